@@ -1,0 +1,306 @@
+"""Benchmark of the headline workload: bit-exact 1024-bit (32-limb) 16-step multiplication
+chains over 65,536 values, every step rounded to nearest-even (the resident chain of the
+reference's CommandBatch::run(mul, x, f_s, x) x16, engine.mm:332-346).
+
+One step = one pass of the chain over the whole batch = 1,048,576 rounded 1024-bit products.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+``value``   device throughput: inputs resident in HBM, CUDA events on the launching stream.
+``e2e``     the same through the public API (Engine / Buffer / CommandBatch): pinned host arrays
+            uploaded, 16 resident muls submitted and waited, the result downloaded, per step.
+``--impl reference`` times the reference's own CPU implementation (its core.hpp compiled from
+the reference sources into oracle/_ref, or the C oracle where that build is absent) on all
+host cores over a bounded sample of the same workload.
+Under torchrun (N > 1) every rank runs its own 65,536-value chain (weak scaling; the path has
+no exchange step), times it on its device and rank 0 reports the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BITS, COUNT, CHAIN = 1024, 65536, 16
+METRIC = "1024-bit ops/s; exact GEMM MAC/s int8-CRT vs limb kernel, 1 B200, bit-exact"
+UNIT = "1024-bit ops/s"
+WORKLOAD = "1024-bit (32-limb) 16-step RNE multiplication chains over 65,536 values (configs[1])"
+ELEMENT_BYTES = BITS // 8 + 12
+# ncu: dram__bytes_read.sum + dram__bytes_write.sum of one chain_kernel<32> launch
+# (profiles/chain_kernel_1024.md); None until a capture exists.
+TRAFFIC_BYTES = None
+
+
+def make_inputs(seed: int = 20261203):
+    """Seeded synthetic data with the configs[1] distribution: significands uniform with the
+    top bit set, exponents uniform in [-8, 8], 1% exact zeros, 2% sparse significands."""
+    from limbforge_b200 import numbers as nb
+    rng = np.random.default_rng(seed)
+    x = nb.random_numbers(rng, COUNT, BITS, 8, zero_frac=0.01, sparse_frac=0.02)
+    f = np.stack([nb.random_numbers(rng, COUNT, BITS, 8, zero_frac=0.01, sparse_frac=0.02) for _ in range(CHAIN)])
+    return x, f
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML every 5 ms while running."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap",
+               0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, device: int):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                break
+            time.sleep(0.005)
+
+    def __enter__(self):
+        if self.nv:
+            self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self.nv:
+            self._t.join()
+
+    def summary(self):
+        return {"sm_mhz": float(np.median(self.samples)) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_reference_rate(x, f, sample: int, threads: int | None = None):
+    """The reference's CPU chain (its core.hpp mul, or the C oracle where the reference build
+    is absent) over `sample` values on all host cores; returns (ops/s, kind, cores)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle.oracle import Oracle, Reference
+    threads = threads or os.cpu_count() or 1
+    xs = np.ascontiguousarray(x[:sample])
+    fs = np.ascontiguousarray(f[:, :sample])
+    if Reference.available():
+        ref, kind = Reference(), "reference"
+
+        def work(lo, hi):
+            v = np.ascontiguousarray(xs[lo:hi])
+            for s in range(CHAIN):
+                v = ref.elementwise(BITS, 2, v, np.ascontiguousarray(fs[s, lo:hi]))
+            return v
+        chunks = np.linspace(0, sample, threads + 1).astype(int)
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(lambda i: work(chunks[i], chunks[i + 1]), range(threads)))
+        dt = time.perf_counter() - t0
+    else:
+        orc, kind = Oracle(), "port"
+        t0 = time.perf_counter()
+        orc.mul_chain(BITS, xs, fs)
+        dt = time.perf_counter() - t0
+    return sample * CHAIN / dt, kind, threads
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU path on the host cores, rank 0 only."""
+    if rank != 0:
+        return
+    x, f = make_inputs()
+    sample = int(os.environ.get("LF_CPU_SAMPLE", "8192"))
+    rates = []
+    for i in range(args.warmup + args.steps):
+        r, kind, cores = cpu_reference_rate(x, f, sample)
+        if i >= args.warmup:
+            rates.append(r)
+    value = float(np.median(rates))
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": COUNT * CHAIN / value * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 limbs (1024-bit RNE)", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "count": COUNT, "steps_per_chain": CHAIN, "bits": BITS},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{sample} of {COUNT} values x {CHAIN} steps per step, extrapolated"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from limbforge_b200 import api
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_
+        dist = dist_
+    x, f = make_inputs(20261203 + rank)
+    E = BITS // 32 + 3
+    # device-resident inputs (torch only as the allocator and stream owner)
+    dx = torch.from_numpy(x.view(np.int32)).cuda()
+    df = torch.from_numpy(np.ascontiguousarray(f).view(np.int32)).cuda()
+    dout = torch.empty_like(dx)
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+
+    def step():
+        api.dev_mul_chain(BITS, dx.data_ptr(), df.data_ptr(), COUNT, CHAIN, dout.data_ptr(), COUNT, stream=sp)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    # correctness of the timed kernel on this rank's data: a sample against the oracle
+    got = dout.cpu().numpy().view(np.uint32)
+    if rank == 0:
+        from oracle.oracle import Oracle
+        idx = slice(0, 2048)
+        want = Oracle().mul_chain(BITS, np.ascontiguousarray(x[idx]), np.ascontiguousarray(f[:, idx]))
+        assert (got[idx] == want).all(), "chain result differs from the oracle"
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            for _ in range(args.steps):
+                step()
+            ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t = torch.tensor([ms], device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = world * COUNT * CHAIN / (ms_step * 1e-3)
+
+    # ---- end to end through the public API with pinned host buffers
+    hx = api.PinnedArray(x.shape)
+    hf = api.PinnedArray(f.shape)
+    ho = api.PinnedArray(x.shape)
+    hx.array[...] = x
+    hf.array[...] = f
+    eng = api.Engine(device=local_rank)
+    X = eng.make_buffer(COUNT, BITS)
+    F = [eng.make_buffer(COUNT, BITS) for _ in range(CHAIN)]
+
+    def e2e_step():
+        X.upload(hx.array)
+        for s in range(CHAIN):
+            F[s].upload(hf.array[s])
+        b = eng.batch()
+        for s in range(CHAIN):
+            b.run(api.Operation.mul, X, F[s], None, X)
+        b.submit().wait()
+        X.download(out=ho.array)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    assert (ho.array == got).all(), "public-API chain differs from the device entry point"
+    e2e_steps = max(3, min(args.steps, 20))
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    te = torch.tensor([e2e_s], device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * COUNT * CHAIN / float(te.item())
+
+    if rank != 0:
+        return
+    hbm_peak, peak_kind = peaks()
+    bytes_per_launch = COUNT * (CHAIN + 2) * ELEMENT_BYTES          # x, 16 factors read; result written
+    achieved = bytes_per_launch / (ms_step * 1e-3) / 1e9
+    word_macs = COUNT * CHAIN * (BITS // 32) ** 2
+    sample = int(os.environ.get("LF_CPU_SAMPLE", "8192"))
+    cpu_rate, kind, cores = cpu_reference_rate(x, f, sample)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32 limbs (1024-bit RNE)", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "count": COUNT, "steps_per_chain": CHAIN, "bits": BITS,
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (%.0f MB resident per step)" % (bytes_per_launch / 1e6)},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(x.nbytes + f.nbytes),
+                "d2h_bytes_per_step": int(x.nbytes), "ms_per_step": e2e_s * 1e3},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                     "traffic": TRAFFIC_BYTES, "peak_kind": peak_kind,
+                     "note": "chain_kernel<32> is integer-pipe bound; HBM fraction shown per the contract"},
+        "integer_pipe": {"word_macs_per_s": word_macs / (ms_step * 1e-3), "word_macs_per_step": word_macs},
+        "clocks": clocks.summary(),
+        "cpu_baseline": {"value": cpu_rate, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{sample} of {COUNT} values x {CHAIN} steps, extrapolated"},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

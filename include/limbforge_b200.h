@@ -1,0 +1,123 @@
+/* C ABI of the B200 implementation of the LimbForge/WolfNum batched multiprecision path.
+ *
+ * The reference exposes a C++17 header API (namespace limbforge, include/limbforge/engine.hpp,
+ * linalg.hpp, batched_linalg.hpp) and no C ABI.  This header is the language-neutral boundary
+ * those classes map onto one to one; include/limbforge/*.hpp in this repository are the
+ * thin inline C++ wrappers that keep user code source compatible.  Each entry point cites the
+ * reference interface it replaces (file:line, paths inside the reference project).
+ *
+ * Conventions
+ *   - Every function returns LF_OK (0) or an error class mirroring the reference's exceptions:
+ *     LF_INVALID_ARGUMENT (std::invalid_argument), LF_LOGIC_ERROR (std::logic_error),
+ *     LF_RUNTIME_ERROR (std::runtime_error).  lf_last_error() returns the message of the last
+ *     failure on the calling thread.  Arithmetic errors are never reported here: they are the
+ *     per-element status bits (division_by_zero=1, exponent_overflow=2, invalid=4).
+ *   - Elements are the reference's structs, byte for byte: a real element of `bits` (64..1024,
+ *     multiple of 32) is bits/32 little-endian uint32 limbs, int32 exponent, int32 sign,
+ *     uint32 status (bits/8+12 bytes); a complex element is {re, im}.
+ *   - Host-array calls take host pointers, copy in and out and return after completion.
+ *   - Operation codes are limbforge::Operation (engine.hpp:13).
+ */
+#ifndef LIMBFORGE_B200_H
+#define LIMBFORGE_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { LF_OK = 0, LF_INVALID_ARGUMENT = 1, LF_LOGIC_ERROR = 2, LF_RUNTIME_ERROR = 3 };
+enum lf_operation {
+    LF_ADD = 0, LF_SUB = 1, LF_MUL = 2, LF_DIV = 3, LF_COMPLEX_ADD = 4, LF_COMPLEX_MUL = 5, LF_COMPLEX_DIV = 6,
+    LF_SQUARE = 7, LF_SQRT = 8, LF_FMA = 9, LF_FMS = 10, LF_COMPLEX_FMA = 11, LF_COMPLEX_FMS = 12
+};
+
+typedef struct lf_timing { double gpu_seconds, wall_seconds; } lf_timing;              /* engine.hpp:18 */
+typedef struct lf_broadcast { size_t stride, period; } lf_broadcast;                   /* engine.hpp:21 */
+typedef struct lf_engine_options {                                                      /* engine.hpp:28 */
+    unsigned threads_per_threadgroup; int cooperative_reductions, cooperative_recurrence; int device;
+} lf_engine_options;
+typedef struct lf_batched4 { size_t count; unsigned rhs; int inverse, determinant, fused; } lf_batched4; /* engine.hpp:36 */
+typedef struct lf_strided_gemm {                                                        /* batched_linalg.hpp:11-14 */
+    size_t count, m, n, k, stride_a, stride_b, stride_c; int accumulate, fused, negative;
+} lf_strided_gemm;
+
+typedef struct lf_engine lf_engine;
+typedef struct lf_buffer lf_buffer;
+typedef struct lf_batch lf_batch;
+typedef struct lf_submission lf_submission;
+
+const char* lf_last_error(void);
+/* library version string and the GPU architecture the kernels were built for */
+const char* lf_version(void);
+
+/* ---- Engine (engine.hpp:184-227) ---- */
+int lf_engine_create(const lf_engine_options* options, lf_engine** out);               /* Engine::Engine */
+void lf_engine_destroy(lf_engine* engine);                                              /* Engine::~Engine */
+int lf_engine_device_name(lf_engine* engine, char* name, size_t capacity);              /* Engine::device_name */
+/* Engine::run (engine.hpp:202): out[i] = op(a[i], b[(i/stride)%period]) for binary real/complex ops */
+int lf_engine_run(lf_engine* engine, int bits, int op, const void* a, const void* b, void* out, size_t count,
+                  lf_broadcast b_index, lf_timing* timing);
+/* Engine::run_unary (engine.hpp:203): square, sqrt */
+int lf_engine_run_unary(lf_engine* engine, int bits, int op, const void* a, void* out, size_t count, lf_timing* timing);
+/* Engine::run_ternary (engine.hpp:204): fma, fms, complex_fma, complex_fms */
+int lf_engine_run_ternary(lf_engine* engine, int bits, int op, const void* a, const void* b, const void* c, void* out,
+                          size_t count, lf_broadcast b_index, lf_broadcast c_index, lf_timing* timing);
+/* Engine::lu4 (engine.hpp:208): batched 4x4 complex LU solve / inverse / determinant */
+int lf_engine_lu4(lf_engine* engine, int bits, const lf_batched4* shape, const void* A, const void* B, void* X,
+                  void* det, uint32_t* status, lf_timing* timing);
+
+/* ---- BatchedLinalg (batched_linalg.hpp:77-118) ---- */
+/* BatchedLinalg::gemm host form (batched_linalg.hpp:86): sequential ascending-k products, one
+ * rounding per step (composed) or per fused step; C is read (accumulate) and written */
+int lf_batched_gemm(lf_engine* engine, int bits, int complex_, const lf_strided_gemm* shape, const void* A,
+                    const void* B, void* C, lf_timing* timing);
+
+/* ---- Buffers (engine.hpp:74-86, 194-198): device-resident typed storage of one engine ---- */
+int lf_buffer_create(lf_engine* engine, size_t bytes, lf_buffer** out);                /* Engine::make_buffer */
+void lf_buffer_release(lf_buffer* buffer);                                              /* last reference frees */
+size_t lf_buffer_bytes(const lf_buffer* buffer);                                        /* Buffer::size (bytes) */
+int lf_buffer_upload(lf_buffer* buffer, const void* source, size_t bytes);              /* Buffer::upload */
+int lf_buffer_download(lf_buffer* buffer, void* target, size_t bytes);                  /* Buffer::download */
+/* Buffer::mapped (engine.hpp:82): a host view, current as of this call; host writes through it
+ * reach the device at the next submission that uses the buffer. */
+int lf_buffer_mapped(lf_buffer* buffer, void** host);
+/* Page-locked host memory for fast transfers to and from buffers (no reference counterpart:
+ * the reference's unified memory needs none). */
+int lf_host_alloc(size_t bytes, void** host);
+void lf_host_free(void* host);
+/* Device address of the storage (CUDA interop; no reference counterpart). */
+int lf_buffer_device_pointer(lf_buffer* buffer, void** device);
+
+/* ---- Command batches and submissions (engine.hpp:93-182) ---- */
+int lf_batch_create(lf_engine* engine, lf_batch** out);                                 /* Engine::batch */
+void lf_batch_destroy(lf_batch* batch);                                                 /* CommandBatch::~CommandBatch */
+/* CommandBatch::run (engine.hpp:120-147): counts in elements; b/c may be NULL where unused */
+int lf_batch_run(lf_batch* batch, int bits, int complex_, int op, lf_buffer* a, lf_buffer* b, lf_buffer* c,
+                 lf_buffer* out, size_t count, lf_broadcast b_index, lf_broadcast c_index);
+/* CommandBatch::lu4 (engine.hpp:164) */
+int lf_batch_lu4(lf_batch* batch, int bits, const lf_batched4* shape, lf_buffer* A, lf_buffer* B, lf_buffer* X,
+                 lf_buffer* det, lf_buffer* status);
+/* BatchedLinalg::gemm resident form (batched_linalg.hpp:97): C_b (+)= A_b B_b, strides in elements */
+int lf_batch_strided_gemm(lf_batch* batch, int bits, int complex_, const lf_strided_gemm* shape, lf_buffer* A,
+                          lf_buffer* B, lf_buffer* C);
+int lf_batch_submit(lf_batch* batch, lf_submission** out);                             /* CommandBatch::submit */
+int lf_submission_ready(lf_submission* submission, int* ready);                        /* Submission::ready */
+int lf_submission_wait(lf_submission* submission, lf_timing* timing);                  /* Submission::wait */
+void lf_submission_destroy(lf_submission* submission);                                  /* waits, then frees */
+
+/* ---- Device-pointer entry points (resident CUDA memory, caller's stream; no reference
+ *      counterpart: they are the kernels behind the calls above, for CUDA callers) ---- */
+int lf_dev_elementwise(int bits, int op, const void* a, const void* b, const void* c, void* out, size_t count,
+                       lf_broadcast b_index, lf_broadcast c_index, void* stream);
+/* x <- x * f_s for s = 0..steps-1, every step rounded, the running value held in registers:
+ * the fused form of CommandBatch::run(mul, x, f_s, x) repeated (engine.mm:332-346).
+ * factors: steps arrays of count elements at factors + s * factor_stride elements. */
+int lf_dev_mul_chain(int bits, const void* x, const void* factors, size_t factor_stride, unsigned steps, void* out,
+                     size_t count, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

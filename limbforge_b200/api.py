@@ -1,0 +1,431 @@
+"""Python mirror of the limbforge C++ API over the C ABI (include/limbforge_b200.h).
+
+Names, argument meaning and error classes follow the reference's headers
+(include/limbforge/engine.hpp, batched_linalg.hpp, linalg.hpp): ``Engine.run/run_unary/
+run_ternary/lu4/make_buffer/batch``, ``Buffer.size/mapped/upload/download``,
+``CommandBatch.run/lu4/submit``, ``Submission.ready/wait``, ``BatchedLinalg.gemm`` and
+``Linalg.gemm/syrk/cholesky/trsm/cholesky_solve``.  Elements are numpy ``uint32`` arrays in
+the reference's struct layout (see ``limbforge_b200.numbers``).  Errors raise
+``InvalidArgument`` (std::invalid_argument), ``LogicError`` (std::logic_error) and
+``RuntimeFailure`` (std::runtime_error).  Every call goes to the CUDA library; there is no
+CPU fallback: a missing or unloadable library raises at import.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from .numbers import check_bits, element_words
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY = os.path.join(HERE, "liblimbforge_b200.so")
+
+
+class LogicError(Exception):
+    """std::logic_error"""
+
+
+class InvalidArgument(LogicError, ValueError):
+    """std::invalid_argument"""
+
+
+class RuntimeFailure(RuntimeError):
+    """std::runtime_error"""
+
+
+class Operation(enum.IntEnum):                                   # engine.hpp:13
+    add = 0
+    sub = 1
+    mul = 2
+    div = 3
+    complex_add = 4
+    complex_mul = 5
+    complex_div = 6
+    square = 7
+    sqrt = 8
+    fma = 9
+    fms = 10
+    complex_fma = 11
+    complex_fms = 12
+
+
+def operation_is_complex(op) -> bool:
+    op = int(op)
+    return 4 <= op <= 6 or op in (11, 12)
+
+
+def operation_is_unary(op) -> bool:
+    return int(op) in (7, 8)
+
+
+def operation_is_ternary(op) -> bool:
+    return 9 <= int(op) <= 12
+
+
+@dataclass
+class Broadcast:                                                 # engine.hpp:21
+    stride: int = 1
+    period: int = 0
+
+
+def broadcast_elements(count: int, b: Broadcast) -> int:         # engine.hpp:22-25
+    if not b.stride:
+        raise InvalidArgument("broadcast stride must be positive")
+    n = count // b.stride + (count % b.stride != 0)
+    return b.period if b.period and b.period < n else n
+
+
+@dataclass
+class Timing:                                                    # engine.hpp:18
+    gpu_seconds: float = 0.0
+    wall_seconds: float = 0.0
+
+
+@dataclass
+class Batched4:                                                  # engine.hpp:36
+    count: int = 0
+    rhs: int = 0
+    inverse: bool = False
+    determinant: bool = False
+    fused: bool = False
+
+
+@dataclass
+class StridedGemm:                                               # batched_linalg.hpp:11-14
+    count: int = 1
+    m: int = 0
+    n: int = 0
+    k: int = 0
+    stride_a: int = 0
+    stride_b: int = 0
+    stride_c: int = 0
+    accumulate: bool = False
+    fused: bool = False
+    negative: bool = False
+
+
+class _Timing(C.Structure):
+    _fields_ = [("gpu_seconds", C.c_double), ("wall_seconds", C.c_double)]
+
+
+class _Broadcast(C.Structure):
+    _fields_ = [("stride", C.c_size_t), ("period", C.c_size_t)]
+
+
+class _EngineOptions(C.Structure):
+    _fields_ = [("threads_per_threadgroup", C.c_uint), ("cooperative_reductions", C.c_int),
+                ("cooperative_recurrence", C.c_int), ("device", C.c_int)]
+
+
+class _Batched4(C.Structure):
+    _fields_ = [("count", C.c_size_t), ("rhs", C.c_uint), ("inverse", C.c_int), ("determinant", C.c_int), ("fused", C.c_int)]
+
+
+class _StridedGemm(C.Structure):
+    _fields_ = [("count", C.c_size_t), ("m", C.c_size_t), ("n", C.c_size_t), ("k", C.c_size_t),
+                ("stride_a", C.c_size_t), ("stride_b", C.c_size_t), ("stride_c", C.c_size_t),
+                ("accumulate", C.c_int), ("fused", C.c_int), ("negative", C.c_int)]
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIBRARY):
+        raise ImportError(f"{LIBRARY} is missing: run limbforge_b200.build.build() (nvcc, sm_100a)")
+    lib = C.CDLL(LIBRARY)
+    P, V, S, I = C.POINTER, C.c_void_p, C.c_size_t, C.c_int
+    sig = {
+        "lf_last_error": ([], C.c_char_p), "lf_version": ([], C.c_char_p),
+        "lf_engine_create": ([P(_EngineOptions), P(V)], I), "lf_engine_destroy": ([V], None),
+        "lf_engine_device_name": ([V, C.c_char_p, S], I),
+        "lf_engine_run": ([V, I, I, V, V, V, S, _Broadcast, P(_Timing)], I),
+        "lf_engine_run_unary": ([V, I, I, V, V, S, P(_Timing)], I),
+        "lf_engine_run_ternary": ([V, I, I, V, V, V, V, S, _Broadcast, _Broadcast, P(_Timing)], I),
+        "lf_engine_lu4": ([V, I, P(_Batched4), V, V, V, V, V, P(_Timing)], I),
+        "lf_batched_gemm": ([V, I, I, P(_StridedGemm), V, V, V, P(_Timing)], I),
+        "lf_buffer_create": ([V, S, P(V)], I), "lf_buffer_release": ([V], None), "lf_buffer_bytes": ([V], S),
+        "lf_buffer_upload": ([V, V, S], I), "lf_buffer_download": ([V, V, S], I),
+        "lf_buffer_mapped": ([V, P(V)], I), "lf_buffer_device_pointer": ([V, P(V)], I),
+        "lf_batch_create": ([V, P(V)], I), "lf_batch_destroy": ([V], None),
+        "lf_batch_run": ([V, I, I, I, V, V, V, V, S, _Broadcast, _Broadcast], I),
+        "lf_batch_lu4": ([V, I, P(_Batched4), V, V, V, V, V], I),
+        "lf_batch_strided_gemm": ([V, I, I, P(_StridedGemm), V, V, V], I),
+        "lf_batch_submit": ([V, P(V)], I), "lf_submission_ready": ([V, P(I)], I),
+        "lf_submission_wait": ([V, P(_Timing)], I), "lf_submission_destroy": ([V], None),
+        "lf_dev_elementwise": ([I, I, V, V, V, V, S, _Broadcast, _Broadcast, V], I),
+        "lf_host_alloc": ([S, P(V)], I), "lf_host_free": ([V], None),
+        "lf_dev_mul_chain": ([I, V, V, S, C.c_uint, V, S, V], I),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes, f.restype = args, res
+    return lib
+
+
+lib = _load()
+
+
+def check(rc: int) -> None:
+    if rc == 0:
+        return
+    msg = lib.lf_last_error().decode()
+    if rc == 1:
+        raise InvalidArgument(msg)
+    if rc == 2:
+        raise LogicError(msg)
+    raise RuntimeFailure(msg)
+
+
+def _ptr(a) -> C.c_void_p | None:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise InvalidArgument("arrays must be C contiguous")
+        return C.c_void_p(a.ctypes.data)
+    return C.c_void_p(int(a))
+
+
+def _bc(b: Broadcast | None) -> _Broadcast:
+    b = b or Broadcast()
+    return _Broadcast(b.stride, b.period)
+
+
+def _timing(t: _Timing) -> Timing:
+    return Timing(t.gpu_seconds, t.wall_seconds)
+
+
+def _elements(a: np.ndarray) -> int:
+    return a.shape[0] if a.ndim >= 1 else 0
+
+
+class Buffer:
+    """Device-resident typed storage (engine.hpp:74-86).  ``bits=0`` holds uint32 words."""
+
+    def __init__(self, engine: "Engine", count: int, bits: int, complex_: bool):
+        self.engine, self.count, self.bits, self.complex = engine, count, bits, complex_
+        self.words = (element_words(bits) * (2 if complex_ else 1)) if bits else 1
+        h = C.c_void_p()
+        check(lib.lf_buffer_create(engine.handle, 4 * self.words * count, C.byref(h)))
+        self.handle = h
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib.lf_buffer_release(self.handle)
+            self.handle = None
+
+    def size(self) -> int:
+        return self.count
+
+    def _shape(self, n):
+        if not self.bits:
+            return (n,)
+        return (n, 2, self.words // 2) if self.complex else (n, self.words)
+
+    def upload(self, source: np.ndarray, count: int | None = None) -> None:
+        n = _elements(source) if count is None else count
+        if n > self.count:
+            raise InvalidArgument("upload exceeds buffer")
+        src = np.ascontiguousarray(source, dtype=np.uint32)
+        check(lib.lf_buffer_upload(self.handle, _ptr(src), 4 * self.words * n))
+
+    def download(self, count: int | None = None, out: np.ndarray | None = None) -> np.ndarray:
+        n = self.count if count is None else count
+        if n > self.count:
+            raise InvalidArgument("download exceeds buffer")
+        dst = np.empty(self._shape(n), dtype=np.uint32) if out is None else out
+        check(lib.lf_buffer_download(self.handle, _ptr(dst), 4 * self.words * n))
+        return dst
+
+    def mapped(self) -> np.ndarray:
+        """Host view (engine.hpp:82); writes reach the device at the next submission using it."""
+        p = C.c_void_p()
+        check(lib.lf_buffer_mapped(self.handle, C.byref(p)))
+        n = self.count * self.words
+        arr = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint32)), shape=(max(n, 1),))[:n]
+        return arr.reshape(self._shape(self.count))
+
+    def device_pointer(self) -> int:
+        p = C.c_void_p()
+        check(lib.lf_buffer_device_pointer(self.handle, C.byref(p)))
+        return p.value or 0
+
+
+class Submission:
+    def __init__(self, handle):
+        self.handle = handle
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib.lf_submission_destroy(self.handle)
+            self.handle = None
+
+    def ready(self) -> bool:
+        r = C.c_int()
+        check(lib.lf_submission_ready(self.handle, C.byref(r)))
+        return bool(r.value)
+
+    def wait(self) -> Timing:
+        t = _Timing()
+        check(lib.lf_submission_wait(self.handle, C.byref(t)))
+        return _timing(t)
+
+
+class CommandBatch:
+    """Asynchronous batch of resident operations (engine.hpp:104-182)."""
+
+    def __init__(self, engine: "Engine"):
+        self.engine = engine
+        h = C.c_void_p()
+        check(lib.lf_batch_create(engine.handle, C.byref(h)))
+        self.handle = h
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib.lf_batch_destroy(self.handle)
+            self.handle = None
+
+    def run(self, op, a: Buffer, b: Buffer | None = None, c: Buffer | None = None, out: Buffer | None = None,
+            b_index: Broadcast | None = None, c_index: Broadcast | None = None) -> None:
+        """run(op, a, b, out[, b_index]) / run(op, a, b, c, out[, b_index, c_index]) / run(op, a, out)"""
+        op = Operation(op)
+        if operation_is_unary(op):
+            out = out if out is not None else b
+            b = None
+        elif not operation_is_ternary(op):
+            out = out if out is not None else c
+            c = None
+        if out is None:
+            raise InvalidArgument("operation requires a different number of inputs")
+        if b_index is None and c_index is None:
+            same = [x for x in (a, b, c, out) if x is not None]
+            if any(x.count != a.count for x in same):
+                raise InvalidArgument("buffer counts must match")
+        elif a.count != out.count:
+            raise InvalidArgument("buffer counts do not match the broadcast")
+        check(lib.lf_batch_run(self.handle, a.bits, int(a.complex), int(op), a.handle, b.handle if b else None,
+                               c.handle if c else None, out.handle, a.count, _bc(b_index), _bc(c_index)))
+
+    def lu4(self, shape: Batched4, A: Buffer, B: Buffer | None, X: Buffer, det: Buffer | None, status: Buffer) -> None:
+        s = _Batched4(shape.count, shape.rhs, int(shape.inverse), int(shape.determinant), int(shape.fused))
+        check(lib.lf_batch_lu4(self.handle, A.bits, C.byref(s), A.handle, B.handle if B else None, X.handle if X else None,
+                               det.handle if det else None, status.handle))
+
+    def submit(self) -> Submission:
+        h = C.c_void_p()
+        check(lib.lf_batch_submit(self.handle, C.byref(h)))
+        return Submission(h)
+
+
+class Engine:
+    """One CUDA device (engine.hpp:184-227).  One Engine per host thread."""
+
+    def __init__(self, device: int = 0):
+        opts = _EngineOptions(0, 1, 1, device)
+        h = C.c_void_p()
+        check(lib.lf_engine_create(C.byref(opts), C.byref(h)))
+        self.handle = h
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib.lf_engine_destroy(self.handle)
+            self.handle = None
+
+    def device_name(self) -> str:
+        buf = C.create_string_buffer(256)
+        check(lib.lf_engine_device_name(self.handle, buf, 256))
+        return buf.value.decode()
+
+    def make_buffer(self, count: int, bits: int = 0, complex_: bool = False) -> Buffer:
+        if bits:
+            check_bits(bits)
+        return Buffer(self, count, bits, complex_)
+
+    def batch(self) -> CommandBatch:
+        return CommandBatch(self)
+
+    def run(self, bits, op, a, b, count=None, b_index: Broadcast | None = None, out=None):
+        n = _elements(a) if count is None else count
+        out = np.empty_like(a[:n]) if out is None else out
+        t = _Timing()
+        check(lib.lf_engine_run(self.handle, bits, int(op), _ptr(a), _ptr(b), _ptr(out), n, _bc(b_index), C.byref(t)))
+        return out, _timing(t)
+
+    def run_unary(self, bits, op, a, count=None, out=None):
+        n = _elements(a) if count is None else count
+        out = np.empty_like(a[:n]) if out is None else out
+        t = _Timing()
+        check(lib.lf_engine_run_unary(self.handle, bits, int(op), _ptr(a), _ptr(out), n, C.byref(t)))
+        return out, _timing(t)
+
+    def run_ternary(self, bits, op, a, b, c, count=None, b_index=None, c_index=None, out=None):
+        n = _elements(a) if count is None else count
+        out = np.empty_like(a[:n]) if out is None else out
+        t = _Timing()
+        check(lib.lf_engine_run_ternary(self.handle, bits, int(op), _ptr(a), _ptr(b), _ptr(c), _ptr(out), n,
+                                        _bc(b_index), _bc(c_index), C.byref(t)))
+        return out, _timing(t)
+
+    def lu4(self, bits, shape: Batched4, A, B=None):
+        n = check_bits(bits)
+        R = 4 if shape.inverse else shape.rhs
+        X = np.zeros((shape.count * 4 * R, 2, n + 3), dtype=np.uint32)
+        det = np.zeros((shape.count, 2, n + 3), dtype=np.uint32)
+        st = np.zeros(shape.count, dtype=np.uint32)
+        s = _Batched4(shape.count, shape.rhs, int(shape.inverse), int(shape.determinant), int(shape.fused))
+        t = _Timing()
+        check(lib.lf_engine_lu4(self.handle, bits, C.byref(s), _ptr(A), _ptr(B), _ptr(X), _ptr(det), _ptr(st), C.byref(t)))
+        return X, det, st, _timing(t)
+
+
+class BatchedLinalg:
+    """Sequential batched products (batched_linalg.hpp:63-118)."""
+
+    def __init__(self, engine: Engine):
+        self.engine = engine
+
+    @staticmethod
+    def _shape(s: StridedGemm) -> _StridedGemm:
+        return _StridedGemm(s.count, s.m, s.n, s.k, s.stride_a, s.stride_b, s.stride_c, int(s.accumulate), int(s.fused),
+                            int(s.negative))
+
+    def gemm(self, bits, complex_, s: StridedGemm, A, B, C_):
+        """Host form: C_ is read and overwritten in place; returns Timing."""
+        t = _Timing()
+        sh = self._shape(s)
+        check(lib.lf_batched_gemm(self.engine.handle, bits, int(complex_), C.byref(sh), _ptr(A), _ptr(B), _ptr(C_), C.byref(t)))
+        return _timing(t)
+
+    def gemm_resident(self, batch: CommandBatch, s: StridedGemm, A: Buffer, B: Buffer, C_: Buffer) -> None:
+        sh = self._shape(s)
+        check(lib.lf_batch_strided_gemm(batch.handle, A.bits, int(A.complex), C.byref(sh), A.handle, B.handle, C_.handle))
+
+
+class PinnedArray:
+    """numpy array over page-locked host memory (lf_host_alloc); freed with the object."""
+
+    def __init__(self, shape, dtype=np.uint32):
+        self.nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        p = C.c_void_p()
+        check(lib.lf_host_alloc(self.nbytes, C.byref(p)))
+        self._p = p
+        buf = (C.c_char * max(self.nbytes, 1)).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+
+    def __del__(self):
+        if getattr(self, "_p", None):
+            self.array = None
+            lib.lf_host_free(self._p)
+            self._p = None
+
+
+def dev_elementwise(bits, op, a_ptr, b_ptr, c_ptr, out_ptr, count, b_index=None, c_index=None, stream=0) -> None:
+    check(lib.lf_dev_elementwise(bits, int(op), _ptr(a_ptr), _ptr(b_ptr), _ptr(c_ptr), _ptr(out_ptr), count,
+                                 _bc(b_index), _bc(c_index), C.c_void_p(stream)))
+
+
+def dev_mul_chain(bits, x_ptr, factors_ptr, factor_stride, steps, out_ptr, count, stream=0) -> None:
+    check(lib.lf_dev_mul_chain(bits, _ptr(x_ptr), _ptr(factors_ptr), factor_stride, steps, _ptr(out_ptr), count,
+                               C.c_void_p(stream)))

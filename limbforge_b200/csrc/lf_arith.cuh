@@ -1,0 +1,582 @@
+// Device arithmetic on 32-bit limb numbers: correctly rounded (round to nearest, ties to even)
+// add/sub/mul/div/sqrt/fma and the exact multi-term sums behind complex fused operations.
+//
+// Element contract (the reference's include/limbforge/core.hpp:22-34): Number<N> is
+// {u32 limb[N] little endian, top bit set when nonzero; i32 exponent; i32 sign; u32 status},
+// value = sign * int(limb) * 2^(exponent-(32N-1)); canonical zero; any input status gives zero
+// carrying the OR of the statuses; a rounded exponent outside [-1e9, 1e9] gives zero with
+// exponent_overflow (core.hpp:77-85).  Every routine here computes the exact result (in a
+// bounded window when a far term can only act as a sticky bit) and rounds it once, so the bits
+// equal the reference's and MPFR's; the algorithms are this file's own (fixed windows and
+// branch-free barrel shifts that keep every index static, so arrays live in registers).
+#pragma once
+#include <stdint.h>
+
+namespace lfd {
+
+typedef uint32_t u32;
+typedef uint64_t u64;
+typedef int64_t i64;
+
+constexpr i64 kEmax = 1000000000;
+enum : u32 { kDivZero = 1, kOverflow = 2, kInvalid = 4 };
+
+template <int N> struct Num { u32 m[N]; int e; int s; u32 st; };
+
+template <int N> __device__ __forceinline__ Num<N> zero(u32 st = 0) {
+    Num<N> r;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.m[i] = 0;
+    r.e = 0; r.s = 0; r.st = st;
+    return r;
+}
+template <int N> __device__ __forceinline__ Num<N> negate(Num<N> a) { a.s = -a.s; return a; }
+
+// ---------------------------------------------------------------- element load / store
+template <int N> __device__ __forceinline__ Num<N> load(const u32* __restrict__ p) {
+    Num<N> r;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.m[i] = __ldg(p + i);
+    r.e = (int)__ldg(p + N); r.s = (int)__ldg(p + N + 1); r.st = __ldg(p + N + 2);
+    return r;
+}
+template <int N> __device__ __forceinline__ Num<N> load_plain(const u32* p) {   // for buffers written in the same kernel
+    Num<N> r;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.m[i] = p[i];
+    r.e = (int)p[N]; r.s = (int)p[N + 1]; r.st = p[N + 2];
+    return r;
+}
+template <int N> __device__ __forceinline__ void store(u32* p, const Num<N>& r) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) p[i] = r.m[i];
+    p[N] = (u32)r.e; p[N + 1] = (u32)r.s; p[N + 2] = r.st;
+}
+
+// ---------------------------------------------------------------- small helpers
+template <int N> __device__ __forceinline__ Num<N> pick(bool c, const Num<N>& a, const Num<N>& b) {
+    Num<N> r;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.m[i] = c ? a.m[i] : b.m[i];
+    r.e = c ? a.e : b.e; r.s = c ? a.s : b.s; r.st = c ? a.st : b.st;
+    return r;
+}
+template <int N> __device__ __forceinline__ int mag_cmp(const Num<N>& a, const Num<N>& b) {
+    if (!a.s) return b.s ? -1 : 0;
+    if (!b.s) return 1;
+    if (a.e != b.e) return a.e > b.e ? 1 : -1;
+    int c = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) c = (a.m[i] != b.m[i]) ? (a.m[i] > b.m[i] ? 1 : -1) : c;   // highest differing word wins
+    return c;
+}
+// Rounded result r = sign * m * 2^(e-(32N-1)) with the increment decided by the caller.
+template <int N> __device__ __forceinline__ Num<N> finish(u32 (&m)[N], i64 e, int sign, bool up, u32 status) {
+    u32 c = up ? 1u : 0u;
+#pragma unroll
+    for (int i = 0; i < N; ++i) { u32 t = m[i] + c; c = (c && t == 0) ? 1u : 0u; m[i] = t; }
+    if (c) { m[N - 1] = 0x80000000u; e += 1; }
+    if (e > kEmax || e < -kEmax) return zero<N>(status | kOverflow);
+    Num<N> r;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.m[i] = m[i];
+    r.e = (int)e; r.s = sign; r.st = status;
+    return r;
+}
+
+// Words of x moved up by q words (q in [0, 2^stages)), zeros shifted in: a branch-free barrel
+// shifter, so the array stays register resident whatever q is.
+template <int W, int STAGES> __device__ __forceinline__ void shift_up_words(u32 (&x)[W], u32 q) {
+#pragma unroll
+    for (int b = 0; b < STAGES; ++b) {
+        const int s = 1 << b;
+        if (s >= W) { if ((q >> b) & 1u) {
+#pragma unroll
+                for (int k = 0; k < W; ++k) x[k] = 0; }
+            continue; }
+        const bool on = (q >> b) & 1u;
+#pragma unroll
+        for (int k = W - 1; k >= 0; --k) x[k] = on ? (k >= s ? x[k - s] : 0u) : x[k];
+    }
+}
+// x <<= r bits (0 <= r < 32) over W words
+template <int W> __device__ __forceinline__ void shift_up_bits(u32 (&x)[W], u32 r) {
+#pragma unroll
+    for (int k = W - 1; k > 0; --k) x[k] = __funnelshift_l(x[k - 1], x[k], r);
+    x[0] = x[0] << r;   // r < 32
+}
+template <int W> __host__ __device__ constexpr int stages_for() { return W <= 1 ? 1 : W <= 2 ? 1 : W <= 4 ? 2 : W <= 8 ? 3 : W <= 16 ? 4 : W <= 32 ? 5 : W <= 64 ? 6 : W <= 128 ? 7 : 8; }
+
+// RN(sign * int(x) * 2^scale) for a W-word magnitude with the top bit anywhere (x is clobbered).
+template <int N, int W> __device__ __forceinline__ Num<N> round_general(u32 (&x)[W], i64 scale, int sign, u32 status) {
+    static_assert(W >= N + 1, "window narrower than the result");
+    int t = -1;
+#pragma unroll
+    for (int k = 0; k < W; ++k) t = x[k] ? k : t;
+    if (t < 0) return zero<N>(status);
+    u32 top = 0;
+#pragma unroll
+    for (int k = 0; k < W; ++k) top = (k == t) ? x[k] : top;
+    const int lz = __clz(top);
+    const i64 e = scale + 32 * (i64)t + 31 - lz;
+    shift_up_words<W, stages_for<W>()>(x, (u32)(W - 1 - t));
+    shift_up_bits<W>(x, (u32)lz);
+    u32 m[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) m[i] = x[W - N + i];
+    u32 below = (W > N) ? x[W - N - 1] : 0u;
+    bool rb = below >> 31;
+    u32 sticky = below & 0x7fffffffu;
+#pragma unroll
+    for (int k = 0; k < W - N - 1; ++k) sticky |= x[k];
+    return finish<N>(m, e, sign, rb && (sticky || (m[0] & 1u)), status);
+}
+
+// ---------------------------------------------------------------- mul
+// p (2N words) = a * b, schoolbook rows with 64-bit multiply-accumulate (IMAD.WIDE).
+template <int N> __device__ __forceinline__ void mant_mul(const u32 (&a)[N], const u32 (&b)[N], u32 (&p)[2 * N]) {
+#pragma unroll
+    for (int k = 0; k < 2 * N; ++k) p[k] = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        u64 c = 0;
+#pragma unroll
+        for (int j = 0; j < N; ++j) { u64 t = (u64)a[i] * b[j] + p[i + j] + c; p[i + j] = (u32)t; c = t >> 32; }
+        p[i + N] = (u32)c;
+    }
+}
+// Round a product of two normalized mantissas: its top bit is bit 64N-1 or 64N-2.
+template <int N> __device__ __forceinline__ Num<N> round_product(const u32 (&p)[2 * N], i64 e_sum, int sign, u32 status) {
+    const u32 s = (p[2 * N - 1] >> 31) ? 0u : 1u;      // normalizing left shift
+    u32 m[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) m[i] = __funnelshift_l(p[N + i - 1], p[N + i], s);
+    const u32 low = p[N - 1] << s;                    // round bit is its top bit
+    u32 sticky = low & 0x7fffffffu;
+#pragma unroll
+    for (int k = 0; k < N - 1; ++k) sticky |= p[k];
+    // (when s = 1 the bit shifted out of p[N-1] went into m[0], not lost)
+    return finish<N>(m, e_sum + 1 - (i64)s, sign, (low >> 31) && (sticky || (m[0] & 1u)), status);
+}
+template <int N> __device__ __forceinline__ Num<N> mul(const Num<N>& a, const Num<N>& b) {
+    const u32 st = a.st | b.st;
+    if (st || !a.s || !b.s) return zero<N>(st);
+    u32 p[2 * N];
+    mant_mul<N>(a.m, b.m, p);
+    return round_product<N>(p, (i64)a.e + b.e, a.s * b.s, 0);
+}
+
+// ---------------------------------------------------------------- add / sub
+// x = larger magnitude, y = smaller; window of 2N+3 words: x at words [N+2, 2N+1], y below it
+// at bit offset 32(N+2)-gap (gap <= 32N+2 keeps y whole); one rounding of the exact sum.
+template <int N> __device__ __forceinline__ Num<N> add(const Num<N>& a, const Num<N>& b) {
+    const u32 st = a.st | b.st;
+    if (st) return zero<N>(st);
+    if (!a.s) return b;
+    if (!b.s) return a;
+    const bool swap = mag_cmp<N>(a, b) < 0;
+    const Num<N> x = pick<N>(swap, b, a);
+    const Num<N> y = pick<N>(swap, a, b);
+    const i64 gap = (i64)x.e - y.e;
+    if (gap > 32 * N + 2) return x;
+    constexpr int W = 2 * N + 3;
+    u32 w[W], v[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) { w[k] = (k >= N + 2 && k < 2 * N + 2) ? x.m[k - N - 2] : 0u; v[k] = k < N ? y.m[k] : 0u; }
+    const u32 sh = (u32)(32 * (N + 2) - gap);           // in [62, 32N+64]
+    shift_up_bits<W>(v, sh & 31u);
+    shift_up_words<W, stages_for<W>()>(v, sh >> 5);
+    if (x.s == y.s) {
+        u64 c = 0;
+#pragma unroll
+        for (int k = 0; k < W; ++k) { u64 t = (u64)w[k] + v[k] + c; w[k] = (u32)t; c = t >> 32; }
+    } else {
+        u32 bo = 0;
+#pragma unroll
+        for (int k = 0; k < W; ++k) { u64 t = (u64)v[k] + bo; u32 old = w[k]; w[k] = (u32)((u64)old - t); bo = (u64)old < t; }
+    }
+    return round_general<N, W>(w, (i64)x.e - (32 * N - 1) - 32 * (N + 2), x.s, 0);
+}
+template <int N> __device__ __forceinline__ Num<N> sub(const Num<N>& a, const Num<N>& b) { return add<N>(a, negate<N>(b)); }
+
+// ---------------------------------------------------------------- div
+// Two-by-one word division with a reused reciprocal (Moller & Granlund, "Improved division by
+// invariant integers", IEEE TC 2011, algorithm 4).  d normalized, u1 < d, v = floor((2^64-1)/d)-2^32.
+__device__ __forceinline__ u32 div2by1(u32 u1, u32 u0, u32 d, u32 v, u32& rem) {
+    u64 p = (u64)v * u1;
+    u64 s = (p & 0xffffffffull) + u0;
+    u32 q0 = (u32)s;
+    u32 q1 = (u32)((p >> 32) + u1 + 1 + (s >> 32));
+    u32 r = u0 - q1 * d;
+    if (r > q0) { --q1; r += d; }
+    if (r >= d) { ++q1; r -= d; }
+    rem = r;
+    return q1;
+}
+// Quotient Q = floor(A * 2^(32N-1+c) / B), c = (A < B), has exactly 32N bits; schoolbook long
+// division by 32-bit digits (Knuth, TAOCP vol. 2, 4.3.1 algorithm D) with the digit estimate
+// above; RNE from the remainder: 2R > B rounds up, 2R == B is a tie.
+template <int N> __device__ __forceinline__ Num<N> div(const Num<N>& a, const Num<N>& b) {
+    const u32 st = a.st | b.st;
+    if (st) return zero<N>(st);
+    if (!b.s) return zero<N>(kDivZero);
+    if (!a.s) return zero<N>();
+    int cmp = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) cmp = (a.m[i] != b.m[i]) ? (a.m[i] > b.m[i] ? 1 : -1) : cmp;
+    const int c = cmp < 0 ? 1 : 0;
+    const i64 e = (i64)a.e - b.e - c;
+    if (e > kEmax || e < -kEmax - 1) return zero<N>(kOverflow);
+    u32 u[2 * N + 1];
+#pragma unroll
+    for (int k = 0; k <= 2 * N; ++k) u[k] = 0;
+    if (c) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) u[N + i] = a.m[i];
+    } else {
+        u[N - 1] = a.m[0] << 31;
+#pragma unroll
+        for (int i = 0; i < N; ++i) u[N + i] = (a.m[i] >> 1) | (i + 1 < N ? a.m[i + 1] << 31 : 0u);
+    }
+    const u32 d = b.m[N - 1], d2 = b.m[N - 2];
+    const u32 v = (u32)(0xffffffffffffffffull / d - 0x100000000ull);
+    u32 q[N];
+#pragma unroll
+    for (int j = N - 1; j >= 0; --j) {
+        const u32 u1 = u[j + N], u0 = u[j + N - 1];
+        u32 qh, rh;
+        bool rbig;                                   // r-hat >= 2^32: the refinement cannot trigger
+        if (u1 >= d) { qh = 0xffffffffu; u64 r = ((u64)u1 << 32 | u0) - (u64)qh * d; rbig = (r >> 32) != 0; rh = (u32)r; }
+        else { qh = div2by1(u1, u0, d, v, rh); rbig = false; }
+        const u32 u2 = u[j + N - 2];
+#pragma unroll 1
+        for (int it = 0; it < 2 && !rbig; ++it) {
+            if ((u64)qh * d2 > (((u64)rh << 32) | u2)) { --qh; u64 nr = (u64)rh + d; rbig = (nr >> 32) != 0; rh = (u32)nr; }
+            else break;
+        }
+        // u[j .. j+N] -= qh * B
+        u64 borrow = 0;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            u64 p = (u64)qh * b.m[i] + borrow;
+            u32 lo = (u32)p, old = u[j + i];
+            u[j + i] = old - lo;
+            borrow = (p >> 32) + (old < lo ? 1u : 0u);
+        }
+        const bool under = (u64)u[j + N] < borrow;
+        u[j + N] = (u32)((u64)u[j + N] - borrow);
+        if (under) {
+            --qh;
+            u64 cy = 0;
+#pragma unroll
+            for (int i = 0; i < N; ++i) { u64 t = (u64)u[j + i] + b.m[i] + cy; u[j + i] = (u32)t; cy = t >> 32; }
+            u[j + N] += (u32)cy;
+        }
+        q[j] = qh;
+    }
+    // remainder u[0..N-1]; compare 2R with B
+    int half = 0;
+    const bool topbit = u[N - 1] >> 31;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        u32 tw = (u[i] << 1) | (i ? u[i - 1] >> 31 : 0u);
+        half = (tw != b.m[i]) ? (tw > b.m[i] ? 1 : -1) : half;
+    }
+    if (topbit) half = 1;
+    return finish<N>(q, e, a.s * b.s, half > 0 || (half == 0 && (q[0] & 1u)), 0);
+}
+
+// ---------------------------------------------------------------- sqrt
+// Restoring digit-by-digit root of the 64N-bit radicand M * 2^(32N-1+odd); the root has 32N bits
+// and no tie is possible: round up exactly when the remainder exceeds the root.
+template <int N> __device__ __forceinline__ Num<N> sqrt(const Num<N>& a) {
+    if (a.st || !a.s) return zero<N>(a.st);
+    if (a.s < 0) return zero<N>(kInvalid);
+    int e = a.e / 2; if (a.e < 0 && (a.e % 2)) --e;
+    const int odd = a.e - 2 * e;                    // 0 or 1
+    // radicand Z = M << (32N - 1 + odd): 2N words
+    u32 z[2 * N];
+#pragma unroll
+    for (int k = 0; k < 2 * N; ++k) z[k] = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) z[N + i] = a.m[i];
+    // shift right by 1 - odd bits (0 or 1)
+    if (!odd) {
+#pragma unroll
+        for (int k = 0; k < 2 * N; ++k) z[k] = (z[k] >> 1) | (k + 1 < 2 * N ? z[k + 1] << 31 : 0u);
+    }
+    u32 root[N + 1], rem[N + 2];
+#pragma unroll
+    for (int k = 0; k <= N; ++k) root[k] = 0;
+#pragma unroll
+    for (int k = 0; k < N + 2; ++k) rem[k] = 0;
+#pragma unroll 1
+    for (int pi = 32 * N - 1; pi >= 0; --pi) {
+        // bring down two bits of z at position 2*pi
+        u32 wsel = 0;
+#pragma unroll
+        for (int k = 0; k < 2 * N; ++k) wsel = (k == (2 * pi) / 32) ? z[k] : wsel;
+        const u32 pair = (wsel >> ((2 * pi) % 32)) & 3u;
+#pragma unroll
+        for (int k = N + 1; k > 0; --k) rem[k] = (rem[k] << 2) | (rem[k - 1] >> 30);
+        rem[0] = (rem[0] << 2) | pair;
+        // trial = 4*root + 1, compared with rem
+        u32 tr[N + 2];
+        tr[0] = (root[0] << 2) | 1u;
+#pragma unroll
+        for (int k = 1; k <= N; ++k) tr[k] = (root[k] << 2) | (root[k - 1] >> 30);
+        tr[N + 1] = root[N] >> 30;
+        int c = 0;
+#pragma unroll
+        for (int k = 0; k < N + 2; ++k) c = (rem[k] != tr[k]) ? (rem[k] > tr[k] ? 1 : -1) : c;
+#pragma unroll
+        for (int k = N; k > 0; --k) root[k] = (root[k] << 1) | (root[k - 1] >> 31);
+        root[0] <<= 1;
+        if (c >= 0) {
+            u32 bo = 0;
+#pragma unroll
+            for (int k = 0; k < N + 2; ++k) { u64 t = (u64)tr[k] + bo; u32 old = rem[k]; rem[k] = (u32)((u64)old - t); bo = (u64)old < t; }
+            root[0] |= 1u;
+        }
+    }
+    // round up iff rem > root
+    int c = 0;
+#pragma unroll
+    for (int k = 0; k < N + 2; ++k) { u32 rk = k <= N ? root[k] : 0u; c = (rem[k] != rk) ? (rem[k] > rk ? 1 : -1) : c; }
+    u32 m[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) m[i] = root[i];
+    return finish<N>(m, e, 1, c > 0, 0);
+}
+
+// ---------------------------------------------------------------- fma
+// RN(a*b + c) with one rounding.  One two's-complement window of F = 3N+4 exact words above one
+// sticky word, anchored 2 bits above the larger term's top bit.  A term that does not fit lies
+// more than 100 bits below the other term's lowest bit (shown by the window sizes), so only its
+// sign matters: it becomes +-1 in the sticky word, below every rounding decision.
+template <int W, int LEN> __device__ __forceinline__ void place_words(u32 (&v)[W], const u32 (&t)[LEN], i64 offset) {
+    // v = t << offset (offset >= 0, the term fits: callers guarantee)
+#pragma unroll
+    for (int k = 0; k < W; ++k) v[k] = k < LEN ? t[k] : 0u;
+    shift_up_bits<W>(v, (u32)(offset & 31));
+    shift_up_words<W, stages_for<W>()>(v, (u32)(offset >> 5));
+}
+template <int W> __device__ __forceinline__ void accumulate(u32 (&acc)[W], const u32 (&t)[W], bool negative) {
+    if (!negative) { u64 cy = 0;
+#pragma unroll
+        for (int k = 0; k < W; ++k) { u64 x = (u64)acc[k] + t[k] + cy; acc[k] = (u32)x; cy = x >> 32; } }
+    else { u32 bo = 0;
+#pragma unroll
+        for (int k = 0; k < W; ++k) { u64 x = (u64)t[k] + bo; u32 old = acc[k]; acc[k] = (u32)((u64)old - x); bo = (u64)old < x; } }
+}
+template <int N> __device__ __forceinline__ Num<N> fma(const Num<N>& a, const Num<N>& b, const Num<N>& c) {
+    const u32 st = a.st | b.st | c.st;
+    if (st) return zero<N>(st);
+    const bool pz = !a.s || !b.s;
+    if (pz) return c.s ? c : zero<N>();
+    u32 p[2 * N];
+    mant_mul<N>(a.m, b.m, p);
+    const int ps = a.s * b.s;
+    if (!c.s) return round_product<N>(p, (i64)a.e + b.e, ps, 0);
+    constexpr int F = 3 * N + 4, W = F + 1;
+    const i64 sp = (i64)a.e + b.e - 2 * (32 * N - 1);
+    const i64 tp = sp + 64 * N - 1 - ((p[2 * N - 1] >> 31) ? 0 : 1);
+    const i64 sc = (i64)c.e - (32 * N - 1), tc = c.e;
+    const i64 hi = tp > tc ? tp : tc;
+    const i64 lo = hi + 3 - 32 * (i64)F;            // exponent of window bit 32
+    u32 acc[W], t[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) acc[k] = 0;
+    if (sp >= lo) place_words<W, 2 * N>(t, p, 32 + (sp - lo));
+    else {
+#pragma unroll
+        for (int k = 0; k < W; ++k) t[k] = k == 0 ? 1u : 0u;
+    }
+    accumulate<W>(acc, t, ps < 0);
+    if (sc >= lo) place_words<W, N>(t, c.m, 32 + (sc - lo));
+    else {
+#pragma unroll
+        for (int k = 0; k < W; ++k) t[k] = k == 0 ? 1u : 0u;
+    }
+    accumulate<W>(acc, t, c.s < 0);
+    int sign = 1;
+    if (acc[W - 1] >> 31) {
+        sign = -1; u64 cy = 1;
+#pragma unroll
+        for (int k = 0; k < W; ++k) { u64 x = (u64)(u32)~acc[k] + cy; acc[k] = (u32)x; cy = x >> 32; }
+    }
+    return round_general<N, W>(acc, lo - 32, sign, 0);
+}
+template <int N> __device__ __forceinline__ Num<N> fms(const Num<N>& a, const Num<N>& b, const Num<N>& c) { return fma<N>(a, b, negate<N>(c)); }
+
+// ---------------------------------------------------------------- exact sums of up to three terms
+// An exact term sign * int(w) * 2^scale of at most XW words (local array; the routines below use
+// runtime lengths, which keeps the rarely used wide paths compact).
+template <int XW> struct Exact { u32 w[XW]; int len; i64 scale; int sign; };
+
+template <int XW> __device__ __forceinline__ i64 ex_msb(const Exact<XW>& x) {
+    for (int k = x.len - 1; k >= 0; --k) if (x.w[k]) return x.scale + 32 * (i64)k + 31 - __clz(x.w[k]);
+    return x.scale - 1;
+}
+template <int XW> __device__ __forceinline__ void ex_add_into(u32* acc, int len, const Exact<XW>& x, i64 off, bool subtract) {
+    // acc (len words) +/-= x.w << off
+    const i64 ws = off >> 5; const int bs = (int)(off & 31);
+    if (!subtract) {
+        u64 cy = 0;
+        for (int k = (int)ws; k < len; ++k) {
+            const i64 src = k - ws;
+            u32 v = 0;
+            if (src < x.len) v = x.w[src] << bs;
+            if (bs && src >= 1 && src - 1 < x.len) v |= x.w[src - 1] >> (32 - bs);
+            if (src > x.len && !cy) break;
+            u64 t = (u64)acc[k] + v + cy; acc[k] = (u32)t; cy = t >> 32;
+        }
+    } else {
+        u32 bo = 0;
+        for (int k = (int)ws; k < len; ++k) {
+            const i64 src = k - ws;
+            u32 v = 0;
+            if (src < x.len) v = x.w[src] << bs;
+            if (bs && src >= 1 && src - 1 < x.len) v |= x.w[src - 1] >> (32 - bs);
+            if (src > x.len && !bo) break;
+            u64 t = (u64)v + bo; u32 old = acc[k]; acc[k] = (u32)((u64)old - t); bo = (u64)old < t;
+        }
+    }
+}
+// x + y exactly, or with y replaced by a sticky unit when y lies wholly more than one bit below
+// x's window [msb(x) - (32N+33), msb(x)] (and below x's lowest bit): then only y's sign can
+// matter to a 32N-bit rounding.  The ordered pairwise structure follows core.hpp:251-275.
+template <int N, int XW> __device__ __noinline__ Exact<XW> ex_add(const Exact<XW>& a, const Exact<XW>& b) {
+    if (!b.sign) return a;
+    if (!a.sign) return b;
+    const bool sw = ex_msb(a) < ex_msb(b);
+    const Exact<XW>& x = sw ? b : a;
+    const Exact<XW>& y = sw ? a : b;
+    const i64 mx = ex_msb(x), my = ex_msb(y);
+    i64 low = mx - (32 * N + 33);
+    if (x.scale < low) low = x.scale;
+    Exact<XW> r;
+    for (int k = 0; k < XW; ++k) r.w[k] = 0;
+    if (my < low - 1) {
+        r.scale = low - 32;
+        r.len = (int)((mx - r.scale) / 32) + 2;
+        ex_add_into<XW>(r.w, r.len, x, x.scale - r.scale, false);
+        if (x.sign == y.sign) r.w[0] |= 1u;              // the word below x is empty
+        else { for (int k = 0; k < r.len; ++k) { u32 old = r.w[k]; r.w[k] = old - 1; if (old) break; } }
+        r.sign = x.sign;
+        return r;
+    }
+    r.scale = x.scale < y.scale ? x.scale : y.scale;
+    r.len = (int)((mx - r.scale) / 32) + 2;
+    u32 t[XW];
+    for (int k = 0; k < XW; ++k) t[k] = 0;
+    ex_add_into<XW>(r.w, r.len, x, x.scale - r.scale, false);
+    ex_add_into<XW>(t, r.len, y, y.scale - r.scale, false);
+    if (x.sign == y.sign) {
+        u64 cy = 0;
+        for (int k = 0; k < r.len; ++k) { u64 s = (u64)r.w[k] + t[k] + cy; r.w[k] = (u32)s; cy = s >> 32; }
+        r.sign = x.sign;
+        return r;
+    }
+    int c = 0;
+    for (int k = r.len - 1; k >= 0 && !c; --k) if (r.w[k] != t[k]) c = r.w[k] > t[k] ? 1 : -1;
+    if (!c) { r.sign = 0; r.scale = 0; r.len = 1; for (int k = 0; k < XW; ++k) r.w[k] = 0; return r; }
+    u32 bo = 0;
+    for (int k = 0; k < r.len; ++k) {
+        u32 p = c > 0 ? r.w[k] : t[k], q = c > 0 ? t[k] : r.w[k];
+        u64 s = (u64)q + bo; r.w[k] = (u32)((u64)p - s); bo = (u64)p < s;
+    }
+    r.sign = c > 0 ? x.sign : y.sign;
+    return r;
+}
+template <int N, int XW> __device__ __noinline__ Num<N> ex_round(const Exact<XW>& x) {
+    if (!x.sign) return zero<N>();
+    int t = -1;
+    for (int k = x.len - 1; k >= 0; --k) if (x.w[k]) { t = k; break; }
+    if (t < 0) return zero<N>();
+    const int h = 32 * t + 31 - __clz(x.w[t]);
+    i64 e = x.scale + h;
+    const int shift = h - (32 * N - 1);             // bit of x that becomes bit 0 of the result
+    u32 m[N];
+    for (int i = 0; i < N; ++i) {
+        const int p = shift + 32 * i;
+        u32 v = 0;
+        if (p <= -32) v = 0;
+        else if (p < 0) v = x.w[0] << (-p);
+        else { const int wi = p >> 5, bi = p & 31; v = wi < x.len ? x.w[wi] >> bi : 0u; if (bi && wi + 1 < x.len) v |= x.w[wi + 1] << (32 - bi); }
+        m[i] = v;
+    }
+    bool up = false;
+    if (shift > 0) {
+        const int rbp = shift - 1;
+        const bool rb = (x.w[rbp >> 5] >> (rbp & 31)) & 1u;
+        bool st = (rbp & 31) && (x.w[rbp >> 5] & ((1u << (rbp & 31)) - 1u));
+        for (int k = 0; k < (rbp >> 5) && !st; ++k) st = x.w[k] != 0;
+        up = rb && (st || (m[0] & 1u));
+    }
+    return finish<N>(m, e, x.sign, up, 0);
+}
+// RN(a*b + c*d + e) with one rounding: terms ordered by msb; either the two smaller terms are
+// far below the largest and summed first, or the largest two overlap and are summed exactly
+// first; each pairwise step is exact or a valid sticky collapse (core.hpp:330-351).
+template <int N> __device__ __noinline__ Num<N> dot2_add(const Num<N>& a, const Num<N>& b, const Num<N>& c, const Num<N>& d, const Num<N>& e) {
+    const u32 st = a.st | b.st | c.st | d.st | e.st;
+    if (st) return zero<N>(st);
+    constexpr int XW = 6 * N + 10;
+    Exact<XW> t[3];
+    for (int q = 0; q < 3; ++q) { for (int k = 0; k < XW; ++k) t[q].w[k] = 0; t[q].len = 1; t[q].scale = 0; t[q].sign = 0; }
+    if (a.s && b.s) { u32 p[2 * N]; mant_mul<N>(a.m, b.m, p); for (int k = 0; k < 2 * N; ++k) t[0].w[k] = p[k];
+        t[0].len = 2 * N; t[0].scale = (i64)a.e + b.e - 2 * (32 * N - 1); t[0].sign = a.s * b.s; }
+    if (c.s && d.s) { u32 p[2 * N]; mant_mul<N>(c.m, d.m, p); for (int k = 0; k < 2 * N; ++k) t[1].w[k] = p[k];
+        t[1].len = 2 * N; t[1].scale = (i64)c.e + d.e - 2 * (32 * N - 1); t[1].sign = c.s * d.s; }
+    if (e.s) { for (int k = 0; k < N; ++k) t[2].w[k] = e.m[k]; t[2].len = N; t[2].scale = (i64)e.e - (32 * N - 1); t[2].sign = e.s; }
+    i64 key[3];
+    for (int q = 0; q < 3; ++q) key[q] = t[q].sign ? ex_msb(t[q]) : -((i64)1 << 62);
+    const int i1 = key[0] >= key[1] ? (key[0] >= key[2] ? 0 : 2) : (key[1] >= key[2] ? 1 : 2);
+    int i3 = key[0] < key[1] ? (key[0] < key[2] ? 0 : 2) : (key[1] < key[2] ? 1 : 2);
+    if (i3 == i1) i3 = (i1 + 1) % 3;
+    const int i2 = 3 - i1 - i3;
+    if (!t[i1].sign) return zero<N>();
+    i64 low = key[i1] - (32 * N + 33);
+    if (t[i1].scale < low) low = t[i1].scale;
+    if (!t[i2].sign || key[i2] < low - 1) {
+        Exact<XW> s = ex_add<N, XW>(t[i2], t[i3]);
+        return ex_round<N, XW>(ex_add<N, XW>(t[i1], s));
+    }
+    Exact<XW> r = ex_add<N, XW>(t[i1], t[i2]);
+    return ex_round<N, XW>(ex_add<N, XW>(r, t[i3]));
+}
+
+// ---------------------------------------------------------------- out-of-line forms
+// Composite sequences (complex ops, batched LU, strided GEMM) call the wide routines through
+// these non-inlined wrappers above 8 limbs: one copy of each routine per kernel keeps code size
+// and compile time bounded, while a call costs little next to an N^2-word product.
+template <int N> __device__ __noinline__ Num<N> mul_call(const Num<N> a, const Num<N> b) { return mul<N>(a, b); }
+template <int N> __device__ __noinline__ Num<N> add_call(const Num<N> a, const Num<N> b) { return add<N>(a, b); }
+template <int N> __device__ __noinline__ Num<N> div_call(const Num<N> a, const Num<N> b) { return div<N>(a, b); }
+template <int N> __device__ __forceinline__ Num<N> mulx(const Num<N>& a, const Num<N>& b) { if constexpr (N > 8) return mul_call<N>(a, b); else return mul<N>(a, b); }
+template <int N> __device__ __forceinline__ Num<N> addx(const Num<N>& a, const Num<N>& b) { if constexpr (N > 8) return add_call<N>(a, b); else return add<N>(a, b); }
+template <int N> __device__ __forceinline__ Num<N> subx(const Num<N>& a, const Num<N>& b) { return addx<N>(a, negate<N>(b)); }
+template <int N> __device__ __forceinline__ Num<N> divx(const Num<N>& a, const Num<N>& b) { if constexpr (N > 8) return div_call<N>(a, b); else return div<N>(a, b); }
+
+// ---------------------------------------------------------------- complex (composed, core.hpp:353-419)
+template <int N> struct Cpx { Num<N> re, im; };
+template <int N> __device__ __forceinline__ Cpx<N> cadd(const Cpx<N>& a, const Cpx<N>& b) { return {addx<N>(a.re, b.re), addx<N>(a.im, b.im)}; }
+template <int N> __device__ __forceinline__ Cpx<N> cmul(const Cpx<N>& a, const Cpx<N>& b) {
+    return {subx<N>(mulx<N>(a.re, b.re), mulx<N>(a.im, b.im)), addx<N>(mulx<N>(a.re, b.im), mulx<N>(a.im, b.re))};
+}
+template <int N> __device__ __forceinline__ Cpx<N> cdiv(const Cpx<N>& a, const Cpx<N>& b) {
+    const Num<N> d = addx<N>(mulx<N>(b.re, b.re), mulx<N>(b.im, b.im));
+    return {divx<N>(addx<N>(mulx<N>(a.re, b.re), mulx<N>(a.im, b.im)), d), divx<N>(subx<N>(mulx<N>(a.im, b.re), mulx<N>(a.re, b.im)), d)};
+}
+template <int N> __device__ __forceinline__ Cpx<N> cfma(const Cpx<N>& a, const Cpx<N>& b, const Cpx<N>& c) {
+    return {dot2_add<N>(a.re, b.re, negate<N>(a.im), b.im, c.re), dot2_add<N>(a.re, b.im, a.im, b.re, c.im)};
+}
+template <int N> __device__ __forceinline__ Cpx<N> cfms(const Cpx<N>& a, const Cpx<N>& b, const Cpx<N>& c) {
+    return cfma<N>(a, b, Cpx<N>{negate<N>(c.re), negate<N>(c.im)});
+}
+template <int N> __device__ __forceinline__ Cpx<N> cload(const u32* p) { return {load<N>(p), load<N>(p + N + 3)}; }
+template <int N> __device__ __forceinline__ Cpx<N> cload_plain(const u32* p) { return {load_plain<N>(p), load_plain<N>(p + N + 3)}; }
+template <int N> __device__ __forceinline__ void cstore(u32* p, const Cpx<N>& z) { store<N>(p, z.re); store<N>(p + N + 3, z.im); }
+
+}  // namespace lfd

@@ -1,0 +1,6 @@
+// Batched small-matrix kernel instantiations for limb counts 25..28.
+#include "lf_batched.cuh"
+LF_BATCHED_INSTANTIATE(25)
+LF_BATCHED_INSTANTIATE(26)
+LF_BATCHED_INSTANTIATE(27)
+LF_BATCHED_INSTANTIATE(28)

@@ -1,0 +1,123 @@
+// Element-wise kernels: one value per thread, the reference's element layout (AoS) in HBM.
+// Broadcast operands are read at (i / stride) % period (kernels.metal:7).  Op codes follow
+// limbforge::Operation (engine.hpp:13).  The mul-chain kernel keeps the running value in
+// registers across every step (the fused form of a resident CommandBatch chain).
+#pragma once
+#include "lf_arith.cuh"
+#include <cuda_runtime.h>
+
+namespace lfd {
+
+struct EwParams {
+    const u32* a; const u32* b; const u32* c; u32* out;
+    u64 count, bs, bp, cs, cp;
+};
+struct ChainStep { const u32* b; u32* out; u64 bs, bp; int op; int pad; };
+constexpr int kMaxChain = 32;
+struct ChainParams {
+    const u32* a; u64 count; int steps; int pad;
+    ChainStep step[kMaxChain];
+};
+
+__device__ __forceinline__ u64 bidx(u64 i, u64 s, u64 p) { u64 j = s > 1 ? i / s : i; return p ? j % p : j; }
+
+constexpr int kEwThreads = 128;
+
+template <int N, int OP> __global__ void __launch_bounds__(kEwThreads) ew_kernel(EwParams p) {
+    const u64 i = (u64)blockIdx.x * kEwThreads + threadIdx.x;
+    if (i >= p.count) return;
+    constexpr u64 E = N + 3;
+    if constexpr (OP == 4 || OP == 5 || OP == 6 || OP == 11 || OP == 12) {
+        const Cpx<N> x = cload<N>(p.a + 2 * E * i);
+        const Cpx<N> y = cload<N>(p.b + 2 * E * bidx(i, p.bs, p.bp));
+        Cpx<N> z;
+        if constexpr (OP == 4) z = cadd<N>(x, y);
+        else if constexpr (OP == 5) z = cmul<N>(x, y);
+        else if constexpr (OP == 6) z = cdiv<N>(x, y);
+        else {
+            const Cpx<N> w = cload<N>(p.c + 2 * E * bidx(i, p.cs, p.cp));
+            z = OP == 11 ? cfma<N>(x, y, w) : cfms<N>(x, y, w);
+        }
+        cstore<N>(p.out + 2 * E * i, z);
+    } else {
+        const Num<N> x = load<N>(p.a + E * i);
+        Num<N> z;
+        if constexpr (OP == 7) z = mul<N>(x, x);
+        else if constexpr (OP == 8) z = lfd::sqrt<N>(x);
+        else {
+            const Num<N> y = load<N>(p.b + E * bidx(i, p.bs, p.bp));
+            if constexpr (OP == 0) z = add<N>(x, y);
+            else if constexpr (OP == 1) z = sub<N>(x, y);
+            else if constexpr (OP == 2) z = mul<N>(x, y);
+            else if constexpr (OP == 3) z = div<N>(x, y);
+            else {
+                const Num<N> w = load<N>(p.c + E * bidx(i, p.cs, p.cp));
+                z = OP == 9 ? fma<N>(x, y, w) : fms<N>(x, y, w);
+            }
+        }
+        store<N>(p.out + E * i, z);
+    }
+}
+
+// v <- op_s(v, b_s[...]) for every step; out_s written where non-null.  Steps are uniform across
+// the grid, so the switch never diverges.
+template <int N> __global__ void __launch_bounds__(kEwThreads) chain_kernel(const __grid_constant__ ChainParams p) {
+    const u64 i = (u64)blockIdx.x * kEwThreads + threadIdx.x;
+    if (i >= p.count) return;
+    constexpr u64 E = N + 3;
+    Num<N> v = load_plain<N>(p.a + E * i);
+#pragma unroll 1
+    for (int s = 0; s < p.steps; ++s) {
+        const ChainStep& st = p.step[s];
+        const Num<N> y = load_plain<N>(st.b + E * bidx(i, st.bs, st.bp));
+        switch (st.op) {
+        case 0: v = add<N>(v, y); break;
+        case 1: v = sub<N>(v, y); break;
+        case 2: v = mul<N>(v, y); break;
+        default: v = div<N>(v, y); break;
+        }
+        if (st.out) store<N>(st.out + E * i, v);
+    }
+}
+
+template <int N> int launch_ew(int op, const EwParams& p, cudaStream_t s) {
+    if (!p.count) return 0;
+    const unsigned blocks = (unsigned)((p.count + kEwThreads - 1) / kEwThreads);
+    switch (op) {
+    case 0: ew_kernel<N, 0><<<blocks, kEwThreads, 0, s>>>(p); break;
+    case 1: ew_kernel<N, 1><<<blocks, kEwThreads, 0, s>>>(p); break;
+    case 2: ew_kernel<N, 2><<<blocks, kEwThreads, 0, s>>>(p); break;
+    case 3: ew_kernel<N, 3><<<blocks, kEwThreads, 0, s>>>(p); break;
+    case 4: ew_kernel<N, 4><<<blocks, kEwThreads, 0, s>>>(p); break;
+    case 5: ew_kernel<N, 5><<<blocks, kEwThreads, 0, s>>>(p); break;
+    case 6: ew_kernel<N, 6><<<blocks, kEwThreads, 0, s>>>(p); break;
+    case 7: ew_kernel<N, 7><<<blocks, kEwThreads, 0, s>>>(p); break;
+    case 8: ew_kernel<N, 8><<<blocks, kEwThreads, 0, s>>>(p); break;
+    case 9: ew_kernel<N, 9><<<blocks, kEwThreads, 0, s>>>(p); break;
+    case 10: ew_kernel<N, 10><<<blocks, kEwThreads, 0, s>>>(p); break;
+    case 11: ew_kernel<N, 11><<<blocks, kEwThreads, 0, s>>>(p); break;
+    case 12: ew_kernel<N, 12><<<blocks, kEwThreads, 0, s>>>(p); break;
+    default: return 1;
+    }
+    return 0;
+}
+template <int N> int launch_chain(const ChainParams& p, cudaStream_t s) {
+    if (!p.count) return 0;
+    const unsigned blocks = (unsigned)((p.count + kEwThreads - 1) / kEwThreads);
+    chain_kernel<N><<<blocks, kEwThreads, 0, s>>>(p);
+    return 0;
+}
+
+// Dispatch tables filled by the per-width translation units (lf_ew_*.cu).
+typedef int (*EwLauncher)(int, const EwParams&, cudaStream_t);
+typedef int (*ChainLauncher)(const ChainParams&, cudaStream_t);
+EwLauncher ew_launcher(int limbs);
+ChainLauncher chain_launcher(int limbs);
+
+}  // namespace lfd
+
+#define LF_EW_INSTANTIATE(N)                                                             \
+    namespace lfd {                                                                      \
+    int ew_launch_##N(int op, const EwParams& p, cudaStream_t s) { return launch_ew<N>(op, p, s); } \
+    int chain_launch_##N(const ChainParams& p, cudaStream_t s) { return launch_chain<N>(p, s); } \
+    }

@@ -1,0 +1,623 @@
+/*
+ * CPU oracle for the LimbForge batched multiprecision path.  TEST INFRASTRUCTURE ONLY:
+ * nothing in the product (the limbforge_b200 package or its shared library) links, loads
+ * or calls this file; tests/, __graft_entry__.smoke() and bench.py's CPU baseline use it
+ * as the checker.
+ *
+ * This is a restatement, in plain C, of the arithmetic contract of the reference
+ * (WolfNum/LimbForge include/limbforge/core.hpp and linalg.hpp::exact_dot_add), not a copy:
+ * every operation is computed as an exact big integer and rounded ONCE with round to
+ * nearest, ties to even.  Because each reference operation is a single correct rounding,
+ * any exact method gives the same bits; the conventions that are not implied by correct
+ * rounding are restated explicitly and cited:
+ *
+ *   element layout  Number<N> = {u32 limb[N] (little endian, top bit set when nonzero),
+ *                   i32 exponent, i32 sign (-1,0,+1), u32 status}           core.hpp:23-28
+ *                   value = sign * int(limb) * 2^(exponent - (32N-1))
+ *   statuses        division_by_zero=1, exponent_overflow=2, invalid=4      core.hpp:22
+ *                   any input status -> zero carrying the OR of the statuses core.hpp:124,138,186,318
+ *   exponent range  the rounded result's exponent must lie in [-1e9, 1e9],
+ *                   otherwise zero with exponent_overflow                   core.hpp:77-85
+ *   zero            canonical: limbs 0, exponent 0, sign 0                  core.hpp:46-49
+ *   add shortcuts   add(0,b) returns b unchanged, add(a,0) returns a;
+ *                   an operand more than 32N+2 bits below returns the larger core.hpp:125-129
+ *   div             b == 0 -> division_by_zero; a == 0 -> zero              core.hpp:187
+ *   sqrt            negative -> invalid                                     core.hpp:218
+ *   exact_dot_add   no nonzero product -> the addend itself (or zero)      linalg.hpp:281
+ *
+ * Sums of several exact terms (fma, dot2_add, exact dots) are rounded with the cluster
+ * argument of linalg.hpp:269-273: terms sorted by magnitude are summed exactly in clusters;
+ * everything after the first nonzero cluster sum S is below 2^(lsb(S)-32N-4) and only its
+ * sign matters, which is the sign of the next nonzero cluster sum.
+ *
+ * Sequences built on these operations (complex ops, blocked Cholesky and triangular
+ * solves, batched 4x4 LU, strided batched GEMM) follow the cited reference sequences.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef uint32_t word;
+typedef uint64_t dword;
+
+enum { ST_DIV0 = 1, ST_OVF = 2, ST_INVALID = 4 };
+#define EMAX 1000000000LL
+
+/* ---------------------------------------------------------------- element access */
+typedef struct { word* w; int n; } num;           /* view of one element */
+static inline int32_t* EXP(word* e, int n) { return (int32_t*)&e[n]; }
+static inline int32_t* SGN(word* e, int n) { return (int32_t*)&e[n + 1]; }
+static inline word* STS(word* e, int n) { return &e[n + 2]; }
+static inline int32_t gexp(const word* e, int n) { return (int32_t)e[n]; }
+static inline int32_t gsgn(const word* e, int n) { return (int32_t)e[n + 1]; }
+static inline word gsts(const word* e, int n) { return e[n + 2]; }
+
+static void set_zero(word* out, int n, word status) {
+    memset(out, 0, sizeof(word) * (size_t)(n + 3));
+    *STS(out, n) = status;
+}
+static void copy_num(word* out, const word* in, int n) { memmove(out, in, sizeof(word) * (size_t)(n + 3)); }
+static void neg_copy(word* out, const word* in, int n) { copy_num(out, in, n); *SGN(out, n) = -gsgn(in, n); }
+
+/* ---------------------------------------------------------------- big integer helpers */
+static int top_bit(const word* x, int W) {           /* index of the highest set bit, -1 if zero */
+    for (int i = W - 1; i >= 0; --i)
+        if (x[i]) return 32 * i + 31 - __builtin_clz(x[i]);
+    return -1;
+}
+static int get_bit(const word* x, int W, long b) {
+    if (b < 0 || b >= 32L * W) return 0;
+    return (x[b / 32] >> (b % 32)) & 1;
+}
+static word bits32(const word* x, int W, long p) {    /* 32 bits of x starting at bit p */
+    word r = 0;
+    if (p <= -32) return 0;
+    if (p < 0) return x[0] << (-p);
+    long i = p / 32; int s = (int)(p % 32);
+    if (i < W) r = x[i] >> s;
+    if (s && i + 1 < W) r |= x[i + 1] << (32 - s);
+    return r;
+}
+static int any_below(const word* x, int W, long b) {  /* any set bit strictly below bit b */
+    if (b <= 0) return 0;
+    long whole = b / 32;
+    for (long i = 0; i < whole && i < W; ++i) if (x[i]) return 1;
+    if (whole < W && (b % 32) && (x[whole] & ((1u << (b % 32)) - 1))) return 1;
+    return 0;
+}
+/* x += y << shift (x has W words, enough room) */
+static void add_shifted(word* x, int W, const word* y, int Wy, long shift) {
+    long ws = shift / 32; int s = (int)(shift % 32); dword c = 0;
+    for (long i = 0; i + ws < W; ++i) {
+        word v = 0;
+        if (i < Wy) v = y[i] << s;
+        if (s && i > 0 && i - 1 < Wy) v |= y[i - 1] >> (32 - s);
+        if (i > Wy && !c) break;
+        dword t = (dword)x[i + ws] + v + c; x[i + ws] = (word)t; c = t >> 32;
+    }
+}
+/* x -= y << shift, two's complement in W words */
+static void sub_shifted(word* x, int W, const word* y, int Wy, long shift) {
+    long ws = shift / 32; int s = (int)(shift % 32); int borrow = 0;
+    for (long i = 0; i + ws < W; ++i) {
+        word v = 0;
+        if (i < Wy) v = y[i] << s;
+        if (s && i > 0 && i - 1 < Wy) v |= y[i - 1] >> (32 - s);
+        if (i > Wy && !borrow) break;
+        dword t = (dword)v + (dword)borrow; word old = x[i + ws];
+        x[i + ws] = (word)((dword)old - t); borrow = (dword)old < t;
+    }
+}
+static void negate_words(word* x, int W) { dword c = 1; for (int i = 0; i < W; ++i) { dword t = (dword)(word)~x[i] + c; x[i] = (word)t; c = t >> 32; } }
+static int is_zero(const word* x, int W) { for (int i = 0; i < W; ++i) if (x[i]) return 0; return 1; }
+static int cmp_words(const word* a, const word* b, int W) { for (int i = W - 1; i >= 0; --i) if (a[i] != b[i]) return a[i] > b[i] ? 1 : -1; return 0; }
+
+/* ---------------------------------------------------------------- the one rounding
+ * out = RN(sign * int(x) * 2^scale) to n words, or zero.  x is not modified. */
+static void round_to(word* out, int n, const word* x, int W, int64_t scale, int sign, word status) {
+    int h = top_bit(x, W);
+    if (h < 0) { set_zero(out, n, status); return; }
+    int64_t e = scale + h;
+    long shift = (long)h - (32L * n - 1);              /* bit of x that becomes bit 0 of the result */
+    word limb[32];
+    for (int i = 0; i < n; ++i) limb[i] = bits32(x, W, shift + 32L * i);
+    if (shift > 0) {
+        int rb = get_bit(x, W, shift - 1);
+        int st = any_below(x, W, shift - 1);
+        if (rb && (st || (limb[0] & 1))) {
+            int i = 0;
+            while (i < n && ++limb[i] == 0) ++i;
+            if (i == n) { limb[n - 1] = 0x80000000u; ++e; }
+        }
+    }
+    if (e > EMAX || e < -EMAX) { set_zero(out, n, status | ST_OVF); return; }
+    set_zero(out, n, status);
+    memcpy(out, limb, sizeof(word) * (size_t)n);
+    *EXP(out, n) = (int32_t)e; *SGN(out, n) = sign;
+}
+
+/* ---------------------------------------------------------------- add / sub */
+static int mag_cmp(const word* a, const word* b, int n) {
+    int sa = gsgn(a, n), sb = gsgn(b, n);
+    if (!sa) return sb ? -1 : 0;
+    if (!sb) return 1;
+    if (gexp(a, n) != gexp(b, n)) return gexp(a, n) > gexp(b, n) ? 1 : -1;
+    return cmp_words(a, b, n);
+}
+void lfo_add(int n, const word* a, const word* b, word* out) {
+    word st = gsts(a, n) | gsts(b, n);
+    if (st) { set_zero(out, n, st); return; }
+    if (!gsgn(a, n)) { copy_num(out, b, n); return; }
+    if (!gsgn(b, n)) { copy_num(out, a, n); return; }
+    const word* x = a; const word* y = b;
+    if (mag_cmp(a, b, n) < 0) { x = b; y = a; }
+    int64_t gap = (int64_t)gexp(x, n) - gexp(y, n);
+    if (gap > 32L * n + 2) { copy_num(out, x, n); return; }
+    int W = 2 * n + 3; word acc[67]; memset(acc, 0, sizeof acc);
+    add_shifted(acc, W, x, n, (long)gap);
+    if (gsgn(x, n) == gsgn(y, n)) add_shifted(acc, W, y, n, 0);
+    else sub_shifted(acc, W, y, n, 0);               /* |x| >= |y|, never negative */
+    round_to(out, n, acc, W, (int64_t)gexp(y, n) - (32L * n - 1), gsgn(x, n), 0);
+}
+void lfo_sub(int n, const word* a, const word* b, word* out) {
+    word t[35]; neg_copy(t, b, n); lfo_add(n, a, t, out);
+}
+
+/* ---------------------------------------------------------------- mul */
+static void mant_mul(const word* a, const word* b, int n, word* p) {   /* p: 2n words */
+    memset(p, 0, sizeof(word) * (size_t)(2 * n));
+    for (int i = 0; i < n; ++i) {
+        dword c = 0;
+        for (int j = 0; j < n; ++j) { dword t = (dword)a[i] * b[j] + p[i + j] + c; p[i + j] = (word)t; c = t >> 32; }
+        p[i + n] = (word)c;
+    }
+}
+void lfo_mul(int n, const word* a, const word* b, word* out) {
+    word st = gsts(a, n) | gsts(b, n);
+    if (st || !gsgn(a, n) || !gsgn(b, n)) { set_zero(out, n, st); return; }
+    word p[64]; mant_mul(a, b, n, p);
+    round_to(out, n, p, 2 * n, (int64_t)gexp(a, n) + gexp(b, n) - 2 * (32L * n - 1), gsgn(a, n) * gsgn(b, n), 0);
+}
+void lfo_square(int n, const word* a, word* out) { lfo_mul(n, a, a, out); }
+
+/* ---------------------------------------------------------------- div
+ * q = floor(A * 2^(32n+1) / B) by binary long division; q has 32n+1 or 32n+2 bits, the
+ * remainder only decides the sticky bit, appended as one extra low bit of q. */
+void lfo_div(int n, const word* a, const word* b, word* out) {
+    word st = gsts(a, n) | gsts(b, n);
+    if (st) { set_zero(out, n, st); return; }
+    if (!gsgn(b, n)) { set_zero(out, n, ST_DIV0); return; }
+    if (!gsgn(a, n)) { set_zero(out, n, 0); return; }
+    int W = n + 2;                                    /* remainder and divisor words */
+    word r[34], d[34], q[68];
+    memset(r, 0, sizeof r); memset(d, 0, sizeof d); memset(q, 0, sizeof q);
+    memcpy(d, b, sizeof(word) * (size_t)n);
+    long total = 32L * n + 32L * n + 1;                /* numerator bits: A then 32n+1 zeros */
+    for (long i = total - 1; i >= 0; --i) {
+        word carry = 0;                               /* r = 2r + bit */
+        for (int k = 0; k < W; ++k) { word nv = (r[k] << 1) | carry; carry = r[k] >> 31; r[k] = nv; }
+        long src = i - (32L * n + 1);
+        if (src >= 0) r[0] |= get_bit(a, n, src);
+        if (cmp_words(r, d, W) >= 0) { sub_shifted(r, W, d, W, 0); q[(i + 1) / 32] |= 1u << ((i + 1) % 32); }
+    }
+    if (!is_zero(r, W)) q[0] |= 1;                    /* sticky below the quotient */
+    round_to(out, n, q, 2 * n + 2, (int64_t)gexp(a, n) - gexp(b, n) - (32L * n + 1) - 1,
+             gsgn(a, n) * gsgn(b, n), 0);
+}
+
+/* ---------------------------------------------------------------- sqrt
+ * Z = M * 2^t with (exponent - (32n-1) - t) even and Z of at least 64n+1 bits; the integer
+ * root has at least 32n+1 bits and the sticky bit says Z is not a perfect square. */
+void lfo_sqrt(int n, const word* a, word* out) {
+    word st = gsts(a, n);
+    if (st || !gsgn(a, n)) { set_zero(out, n, st); return; }
+    if (gsgn(a, n) < 0) { set_zero(out, n, ST_INVALID); return; }
+    int64_t sc = (int64_t)gexp(a, n) - (32L * n - 1);
+    long t = 32L * n + 2;                              /* Z = M << t, then fix the parity */
+    if ((sc - t) & 1) ++t;
+    int W = 2 * n + 2;                                 /* bits of Z <= 64n + 3 */
+    word Z[66], root[34], rem[68], trial[68];
+    memset(Z, 0, sizeof Z); memset(root, 0, sizeof root); memset(rem, 0, sizeof rem);
+    add_shifted(Z, W, a, n, t);
+    int h = top_bit(Z, W); int pairs = h / 2 + 1;
+    int RW = n + 2;                                    /* root words (root < 2^(33n)) */
+    for (int pi = pairs - 1; pi >= 0; --pi) {
+        /* rem = 4 rem + next two bits */
+        word carry = 0;
+        for (int k = 0; k < W; ++k) { word nv = (rem[k] << 2) | carry; carry = rem[k] >> 30; rem[k] = nv; }
+        rem[0] |= (word)(get_bit(Z, W, 2L * pi) | (get_bit(Z, W, 2L * pi + 1) << 1));
+        /* trial = 4 root + 1 */
+        memset(trial, 0, sizeof trial);
+        carry = 0;
+        for (int k = 0; k < RW; ++k) { word nv = (root[k] << 2) | carry; carry = root[k] >> 30; trial[k] = nv; }
+        trial[RW] = carry; trial[0] |= 1;
+        /* root = 2 root */
+        carry = 0;
+        for (int k = 0; k < RW; ++k) { word nv = (root[k] << 1) | carry; carry = root[k] >> 31; root[k] = nv; }
+        if (cmp_words(rem, trial, W) >= 0) { sub_shifted(rem, W, trial, W, 0); root[0] |= 1; }
+    }
+    word r2[36]; memset(r2, 0, sizeof r2);
+    memcpy(r2 + 1, root, sizeof(word) * (size_t)RW);  /* shift left one word for the sticky bit */
+    if (!is_zero(rem, W)) r2[0] = 1;
+    round_to(out, n, r2, RW + 1, (sc - t) / 2 - 32, 1, 0);
+}
+
+/* ---------------------------------------------------------------- exact sums */
+typedef struct { const word* w; int nw; int64_t scale; int sign; } term;
+
+static int term_cmp(const void* x, const void* y) {
+    const term* a = (const term*)x; const term* b = (const term*)y;
+    int64_t ta = a->scale + 32L * a->nw, tb = b->scale + 32L * b->nw;
+    return ta < tb ? 1 : ta > tb ? -1 : 0;
+}
+/* out = RN(sum of terms); the terms array is reordered.  Returns nothing; zero -> canonical. */
+static void round_sum(word* out, int n, term* t, size_t count) {
+    size_t m = 0;
+    for (size_t i = 0; i < count; ++i) if (t[i].sign) t[m++] = t[i];
+    if (!m) { set_zero(out, n, 0); return; }
+    qsort(t, m, sizeof(term), term_cmp);
+    int logc = 0; while (((size_t)1 << logc) < m + 1) ++logc;
+    const int64_t gap = 32L * n + logc + 4;
+    word* first = NULL; int first_w = 0; int64_t first_low = 0; int first_sign = 0; int follow = 0;
+    for (size_t i = 0; i < m;) {
+        size_t j = i + 1; int64_t low = t[i].scale, top = t[i].scale + 32L * t[i].nw;
+        while (j < m && t[j].scale + 32L * t[j].nw > low - gap) { if (t[j].scale < low) low = t[j].scale; ++j; }
+        int W = (int)((top - low) / 32) + 3 + (logc + 31) / 32;
+        word* acc = (word*)calloc((size_t)W, sizeof(word));
+        for (size_t q = i; q < j; ++q) {
+            if (t[q].sign > 0) add_shifted(acc, W, t[q].w, t[q].nw, (long)(t[q].scale - low));
+            else sub_shifted(acc, W, t[q].w, t[q].nw, (long)(t[q].scale - low));
+        }
+        int sign = 1;
+        if (acc[W - 1] >> 31) { sign = -1; negate_words(acc, W); }
+        if (is_zero(acc, W)) { free(acc); i = j; continue; }
+        if (!first) { first = acc; first_w = W; first_low = low; first_sign = sign; i = j; continue; }
+        follow = sign; free(acc); break;
+    }
+    if (!first) { set_zero(out, n, 0); return; }
+    if (!follow) { round_to(out, n, first, first_w, first_low, first_sign, 0); free(first); return; }
+    /* S * 2^D + sign(F) * 1 with D = 32n + 64: the unit lies below every rounding decision */
+    const int D = 32 * n + 64;
+    int W = first_w + D / 32 + 1;
+    word* ext = (word*)calloc((size_t)W, sizeof(word));
+    memcpy(ext + D / 32, first, sizeof(word) * (size_t)first_w);
+    word one = 1;
+    if (follow == first_sign) add_shifted(ext, W, &one, 1, 0); else sub_shifted(ext, W, &one, 1, 0);
+    round_to(out, n, ext, W, first_low - D, first_sign, 0);
+    free(ext); free(first);
+}
+
+/* RN(a*b + c) / RN(a*b - c), one rounding (mpfr_fma / mpfr_fms contract, core.hpp:317-329) */
+void lfo_fma(int n, const word* a, const word* b, const word* c, int negate_c, word* out) {
+    word st = gsts(a, n) | gsts(b, n) | gsts(c, n);
+    if (st) { set_zero(out, n, st); return; }
+    word p[64]; term t[2]; size_t k = 0;
+    if (gsgn(a, n) && gsgn(b, n)) {
+        mant_mul(a, b, n, p);
+        t[k].w = p; t[k].nw = 2 * n; t[k].scale = (int64_t)gexp(a, n) + gexp(b, n) - 2 * (32L * n - 1);
+        t[k].sign = gsgn(a, n) * gsgn(b, n); ++k;
+    }
+    if (gsgn(c, n)) { t[k].w = c; t[k].nw = n; t[k].scale = (int64_t)gexp(c, n) - (32L * n - 1); t[k].sign = negate_c ? -gsgn(c, n) : gsgn(c, n); ++k; }
+    round_sum(out, n, t, k);
+}
+/* RN(a*b + c*d + e), one rounding (core.hpp:334-351) */
+void lfo_dot2_add(int n, const word* a, const word* b, const word* c, const word* d, const word* e, word* out) {
+    word st = gsts(a, n) | gsts(b, n) | gsts(c, n) | gsts(d, n) | gsts(e, n);
+    if (st) { set_zero(out, n, st); return; }
+    word p[64], q[64]; term t[3]; size_t k = 0;
+    if (gsgn(a, n) && gsgn(b, n)) { mant_mul(a, b, n, p); t[k].w = p; t[k].nw = 2 * n; t[k].scale = (int64_t)gexp(a, n) + gexp(b, n) - 2 * (32L * n - 1); t[k].sign = gsgn(a, n) * gsgn(b, n); ++k; }
+    if (gsgn(c, n) && gsgn(d, n)) { mant_mul(c, d, n, q); t[k].w = q; t[k].nw = 2 * n; t[k].scale = (int64_t)gexp(c, n) + gexp(d, n) - 2 * (32L * n - 1); t[k].sign = gsgn(c, n) * gsgn(d, n); ++k; }
+    if (gsgn(e, n)) { t[k].w = e; t[k].nw = n; t[k].scale = (int64_t)gexp(e, n) - (32L * n - 1); t[k].sign = gsgn(e, n); ++k; }
+    round_sum(out, n, t, k);
+}
+/* RN(c -/+ sum_k a[k*sa] * b[k*sb]) with one rounding (linalg.hpp:274-318); c may be NULL. */
+void lfo_exact_dot_add(int n, const word* c, int subtract, const word* a, long sa, const word* b, long sb, size_t K, word* out) {
+    const size_t E = (size_t)n + 3;
+    word st = c ? gsts(c, n) : 0;
+    for (size_t k = 0; k < K; ++k) st |= gsts(a + (long)k * sa * (long)E, n) | gsts(b + (long)k * sb * (long)E, n);
+    if (st) { set_zero(out, n, st); return; }
+    term* t = (term*)malloc(sizeof(term) * (K + 1));
+    word* prod = (word*)malloc(sizeof(word) * (2 * (size_t)n) * (K ? K : 1));
+    size_t m = 0;
+    for (size_t k = 0; k < K; ++k) {
+        const word* x = a + (long)k * sa * (long)E; const word* y = b + (long)k * sb * (long)E;
+        if (!gsgn(x, n) || !gsgn(y, n)) continue;
+        word* p = prod + 2 * (size_t)n * m;
+        mant_mul(x, y, n, p);
+        t[m].w = p; t[m].nw = 2 * n; t[m].scale = (int64_t)gexp(x, n) + gexp(y, n) - 2 * (32L * n - 1);
+        t[m].sign = subtract ? -gsgn(x, n) * gsgn(y, n) : gsgn(x, n) * gsgn(y, n); ++m;
+    }
+    if (!m) {
+        if (c) copy_num(out, c, n); else set_zero(out, n, 0);
+        free(t); free(prod); return;
+    }
+    word cc[35];
+    if (c && gsgn(c, n)) { copy_num(cc, c, n); t[m].w = cc; t[m].nw = n; t[m].scale = (int64_t)gexp(c, n) - (32L * n - 1); t[m].sign = gsgn(c, n); ++m; }
+    round_sum(out, n, t, m);
+    free(t); free(prod);
+}
+
+/* ---------------------------------------------------------------- complex (core.hpp:353-419) */
+/* complex element: re then im, each n+3 words */
+void lfo_cadd(int n, const word* a, const word* b, word* out) {
+    const int E = n + 3; word r[35], i[35];
+    lfo_add(n, a, b, r); lfo_add(n, a + E, b + E, i);
+    copy_num(out, r, n); copy_num(out + E, i, n);
+}
+void lfo_cmul(int n, const word* a, const word* b, word* out) {
+    const int E = n + 3; word p1[35], p2[35], r[35], i[35];
+    lfo_mul(n, a, b, p1); lfo_mul(n, a + E, b + E, p2); lfo_sub(n, p1, p2, r);
+    lfo_mul(n, a, b + E, p1); lfo_mul(n, a + E, b, p2); lfo_add(n, p1, p2, i);
+    copy_num(out, r, n); copy_num(out + E, i, n);
+}
+void lfo_cdiv(int n, const word* a, const word* b, word* out) {
+    const int E = n + 3; word p1[35], p2[35], d[35], x[35], r[35], i[35];
+    lfo_mul(n, b, b, p1); lfo_mul(n, b + E, b + E, p2); lfo_add(n, p1, p2, d);
+    lfo_mul(n, a, b, p1); lfo_mul(n, a + E, b + E, p2); lfo_add(n, p1, p2, x); lfo_div(n, x, d, r);
+    lfo_mul(n, a + E, b, p1); lfo_mul(n, a, b + E, p2); lfo_sub(n, p1, p2, x); lfo_div(n, x, d, i);
+    copy_num(out, r, n); copy_num(out + E, i, n);
+}
+/* cfma: re = RN(a.re b.re - a.im b.im + c.re), im = RN(a.re b.im + a.im b.re + c.im); cfms negates c */
+void lfo_cfma(int n, const word* a, const word* b, const word* c, int negate_c, word* out) {
+    const int E = n + 3; word m[35], cr[35], ci[35], r[35], i[35];
+    neg_copy(m, a + E, n);
+    if (negate_c) { neg_copy(cr, c, n); neg_copy(ci, c + E, n); } else { copy_num(cr, c, n); copy_num(ci, c + E, n); }
+    lfo_dot2_add(n, a, b, m, b + E, cr, r);
+    lfo_dot2_add(n, a, b + E, a + E, b, ci, i);
+    copy_num(out, r, n); copy_num(out + E, i, n);
+}
+
+/* ---------------------------------------------------------------- batched element-wise driver
+ * op codes follow limbforge::Operation (engine.hpp:13): add sub mul div complex_add complex_mul
+ * complex_div square sqrt fma fms complex_fma complex_fms.  Broadcast index (i/stride)%period
+ * (kernels.metal:7). */
+static size_t bidx(size_t i, size_t stride, size_t period) { size_t j = stride > 1 ? i / stride : i; return period ? j % period : j; }
+int lfo_elementwise(int bits, int op, const word* a, const word* b, const word* c, word* out, size_t count,
+                    size_t bs, size_t bp, size_t cs, size_t cp) {
+    if (bits < 64 || bits > 1024 || bits % 32) return 1;
+    const int n = bits / 32; const size_t E = (size_t)n + 3;
+    const int cx = (op >= 4 && op <= 6) || op == 11 || op == 12;
+    const size_t S = cx ? 2 * E : E;
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(|:bad)
+    for (size_t i = 0; i < count; ++i) {
+        const word* x = a + i * S; word* o = out + i * S;
+        const word* y = b ? b + bidx(i, bs, bp) * S : NULL;
+        const word* z = c ? c + bidx(i, cs, cp) * S : NULL;
+        word tmp[70];
+        switch (op) {
+        case 0: lfo_add(n, x, y, tmp); break;
+        case 1: lfo_sub(n, x, y, tmp); break;
+        case 2: lfo_mul(n, x, y, tmp); break;
+        case 3: lfo_div(n, x, y, tmp); break;
+        case 4: lfo_cadd(n, x, y, tmp); break;
+        case 5: lfo_cmul(n, x, y, tmp); break;
+        case 6: lfo_cdiv(n, x, y, tmp); break;
+        case 7: lfo_square(n, x, tmp); break;
+        case 8: lfo_sqrt(n, x, tmp); break;
+        case 9: lfo_fma(n, x, y, z, 0, tmp); break;
+        case 10: lfo_fma(n, x, y, z, 1, tmp); break;
+        case 11: lfo_cfma(n, x, y, z, 0, tmp); break;
+        case 12: lfo_cfma(n, x, y, z, 1, tmp); break;
+        default: bad = 1; continue;
+        }
+        memcpy(o, tmp, sizeof(word) * S);
+    }
+    return bad;
+}
+/* value <- value * f_s for s = 0..steps-1, each step rounded (the resident mul chain);
+ * factors are [steps][count] */
+int lfo_mul_chain(int bits, const word* x, const word* factors, size_t steps, word* out, size_t count) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (size_t i = 0; i < count; ++i) {
+        word v[35]; copy_num(v, x + i * E, n);
+        for (size_t s = 0; s < steps; ++s) { word r[35]; lfo_mul(n, v, factors + (s * count + i) * E, r); copy_num(v, r, n); }
+        copy_num(out + i * E, v, n);
+    }
+    return 0;
+}
+int lfo_exact_dot_add_bits(int bits, const word* c, int subtract, const word* a, long sa, const word* b, long sb, size_t K, word* out) {
+    lfo_exact_dot_add(bits / 32, c, subtract, a, sa, b, sb, K, out); return 0;
+}
+
+/* ---------------------------------------------------------------- dense products
+ * C (m x nc) = op(A) B, or RN(C - op(A) B) with subtract; every entry one exact_dot_add
+ * (the contract of Linalg::gemm/syrk, linalg.hpp:149-155).  Rows [r0, r1) only, so tests
+ * can sample. */
+int lfo_gemm_rows(int bits, int transpose_a, const word* A, const word* B, size_t m, size_t nc, size_t k,
+                  word* C, int subtract, size_t r0, size_t r1) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3;
+    if (r1 > m) r1 = m;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (size_t i = r0; i < r1; ++i)
+        for (size_t j = 0; j < nc; ++j) {
+            const word* x = transpose_a ? A + i * E : A + i * k * E;
+            long sx = transpose_a ? (long)m : 1;
+            word* o = C + (i * nc + j) * E; word old[35]; copy_num(old, o, n);
+            lfo_exact_dot_add(n, subtract ? old : NULL, subtract, x, sx, B + j * E, (long)nc, k, o);
+        }
+    return 0;
+}
+/* C (cols x cols) = A^T A (lower triangle; full when lower_only == 0; subtract requires lower) */
+int lfo_syrk_rows(int bits, const word* A, size_t rows, size_t cols, word* C, int lower_only, int subtract, size_t r0, size_t r1) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3;
+    if (r1 > cols) r1 = cols;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (size_t i = r0; i < r1; ++i)
+        for (size_t j = 0; j <= i; ++j) {
+            word* o = C + (i * cols + j) * E; word old[35]; copy_num(old, o, n);
+            lfo_exact_dot_add(n, subtract ? old : NULL, subtract, A + i * E, (long)cols, A + j * E, (long)cols, rows, o);
+            if (!lower_only && j < i) copy_num(C + (j * cols + i) * E, o, n);
+        }
+    return 0;
+}
+
+/* ---------------------------------------------------------------- blocked Cholesky (linalg.mm:411-457)
+ * D(c; x, y; K) = exact_dot_add(c, subtract).  Right-looking with block nb: the panel of
+ * block [k0,k1) is factored row by row (l_ij = RN(D(a_ij; l_i, l_j; [k0, j)) / l_jj),
+ * l_ii = sqrt(D(a_ii; l_i, l_i; [k0, i)))), then every trailing lower entry is updated by
+ * one D over [k0, k1).  info[0] = pivot, info[1] = pivot sign, info[2] = pivot status. */
+int lfo_cholesky(int bits, const word* A, size_t nn, word* L, size_t block, long* info) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3;
+    size_t nb = block ? (block < nn ? block : nn) : nn;
+    word* W = L;
+    for (size_t i = 0; i < nn; ++i) for (size_t j = 0; j < nn; ++j) {
+        if (j > i) set_zero(W + (i * nn + j) * E, n, 0); else copy_num(W + (i * nn + j) * E, A + (i * nn + j) * E, n);
+    }
+    info[0] = (long)nn; info[1] = 0; info[2] = 0;
+#define AT(i, j) (W + ((i) * nn + (j)) * E)
+    size_t p = nn;
+    for (size_t k0 = 0; k0 < nn && p == nn; k0 += nb) {
+        size_t k1 = k0 + nb < nn ? k0 + nb : nn;
+        /* panel: diagonal block row by row */
+        size_t fail = k1;
+        for (size_t i = k0; i < k1 && fail == k1; ++i) {
+            for (size_t j = k0; j < i; ++j) { word d[35]; lfo_exact_dot_add(n, AT(i, j), 1, AT(i, k0), 1, AT(j, k0), 1, j - k0, d); lfo_div(n, d, AT(j, j), AT(i, j)); }
+            word s[35]; lfo_exact_dot_add(n, AT(i, i), 1, AT(i, k0), 1, AT(i, k0), 1, i - k0, s);
+            if (gsts(s, n) || gsgn(s, n) <= 0) { fail = i; info[0] = (long)i; info[1] = gsts(s, n) ? 0 : gsgn(s, n); info[2] = (long)gsts(s, n); }
+            else lfo_sqrt(n, s, AT(i, i));
+        }
+        size_t first = fail < k1 ? fail + 1 : k1;
+        for (size_t i = first; i < nn; ++i)
+            for (size_t j = k0; j < fail; ++j) { word d[35]; lfo_exact_dot_add(n, AT(i, j), 1, AT(i, k0), 1, AT(j, k0), 1, j - k0, d); lfo_div(n, d, AT(j, j), AT(i, j)); }
+        if (fail < k1) { p = fail; break; }
+        /* trailing update by block [k0, k1) */
+        for (size_t i = k1; i < nn; ++i)
+            for (size_t j = k1; j <= i; ++j) { word d[35]; lfo_exact_dot_add(n, AT(i, j), 1, AT(i, k0), 1, AT(j, k0), 1, k1 - k0, d); copy_num(AT(i, j), d, n); }
+    }
+    if (p < nn) for (size_t i = p; i < nn; ++i) for (size_t j = p; j <= i; ++j) set_zero(AT(i, j), n, ST_INVALID);
+#undef AT
+    return 0;
+}
+/* Triangular solves (linalg.mm:459-488).  passes: 1 forward L X = B, 2 backward L^T X = B,
+ * 3 both.  X holds B on entry (n x nrhs, row-major). */
+int lfo_solve(int bits, const word* L, size_t nn, word* X, size_t nrhs, size_t block, int passes) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3;
+    size_t nb = block ? (block < nn ? block : nn) : nn;
+    if (!nn || !nrhs) return 0;
+#define LL(i, j) (L + ((i) * nn + (j)) * E)
+#define XX(i, c) (X + ((i) * nrhs + (c)) * E)
+    if (passes & 1)
+        for (size_t r0 = 0; r0 < nn; r0 += nb) {
+            size_t r1 = r0 + nb < nn ? r0 + nb : nn;
+            for (size_t c = 0; c < nrhs; ++c)
+                for (size_t i = r0; i < r1; ++i) { word d[35]; lfo_exact_dot_add(n, XX(i, c), 1, LL(i, r0), 1, XX(r0, c), (long)nrhs, i - r0, d); lfo_div(n, d, LL(i, i), XX(i, c)); }
+            for (size_t i = r1; i < nn; ++i)
+                for (size_t c = 0; c < nrhs; ++c) { word d[35]; lfo_exact_dot_add(n, XX(i, c), 1, LL(i, r0), 1, XX(r0, c), (long)nrhs, r1 - r0, d); copy_num(XX(i, c), d, n); }
+        }
+    if (passes & 2)
+        for (size_t r0 = (nn - 1) / nb * nb;; r0 -= nb) {
+            size_t r1 = r0 + nb < nn ? r0 + nb : nn;
+            for (size_t c = 0; c < nrhs; ++c)
+                for (size_t i = r1; i-- > r0;) {
+                    word d[35];
+                    if (i + 1 < r1) lfo_exact_dot_add(n, XX(i, c), 1, LL(i + 1, i), (long)nn, XX(i + 1, c), (long)nrhs, r1 - i - 1, d);
+                    else copy_num(d, XX(i, c), n);
+                    lfo_div(n, d, LL(i, i), XX(i, c));
+                }
+            for (size_t i = 0; i < r0; ++i)
+                for (size_t c = 0; c < nrhs; ++c) { word d[35]; lfo_exact_dot_add(n, XX(i, c), 1, LL(r0, i), (long)nn, XX(r0, c), (long)nrhs, r1 - r0, d); copy_num(XX(i, c), d, n); }
+            if (!r0) break;
+        }
+#undef LL
+#undef XX
+    return 0;
+}
+
+/* ---------------------------------------------------------------- batched 4x4 complex LU (kernels.metal:210-249)
+ * flags: 1 fused (cfms elimination), 2 determinant, 4 inverse.  A [count][16], B [count][4][rhs],
+ * X [count][4][R] (R = 4 for the inverse), det [count], status [count]. */
+static void c_minus(int n, int fused, const word* c, const word* a, const word* b, word* out) {   /* c - a*b */
+    const int E = n + 3;
+    if (fused) { word r[70]; lfo_cfma(n, a, b, c, 1, r); neg_copy(out, r, n); neg_copy(out + E, r + E, n); }
+    else { word q[70], re[35], im[35]; lfo_cmul(n, a, b, q); lfo_sub(n, c, q, re); lfo_sub(n, c + E, q + E, im); copy_num(out, re, n); copy_num(out + E, im, n); }
+}
+int lfo_lu4(int bits, size_t count, unsigned rhs, int flags, const word* A, const word* B, word* X, word* det, word* status) {
+    const int n = bits / 32; const int E = n + 3; const int CE = 2 * E;
+    const int fused = flags & 1, want_det = flags & 2, inverse = flags & 4;
+    unsigned R = inverse ? 4 : rhs;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (size_t m = 0; m < count; ++m) {
+        word a[16][70]; unsigned perm[4] = {0, 1, 2, 3}, st = 0, swaps = 0;
+        for (int i = 0; i < 16; ++i) memcpy(a[i], A + (m * 16 + (size_t)i) * (size_t)CE, sizeof(word) * (size_t)CE);
+        for (unsigned k = 0; k < 4 && !st; ++k) {
+            unsigned piv = k;
+            for (unsigned r = k + 1; r < 4; ++r) {
+                const word* x = mag_cmp(a[r * 4 + k], a[r * 4 + k] + E, n) >= 0 ? a[r * 4 + k] : a[r * 4 + k] + E;
+                const word* y = mag_cmp(a[piv * 4 + k], a[piv * 4 + k] + E, n) >= 0 ? a[piv * 4 + k] : a[piv * 4 + k] + E;
+                if (mag_cmp(x, y, n) > 0) piv = r;
+            }
+            if (!gsgn(a[piv * 4 + k], n) && !gsgn(a[piv * 4 + k] + E, n)) { st = k + 1; break; }
+            if (piv != k) {
+                for (unsigned c = 0; c < 4; ++c) { word t[70]; memcpy(t, a[k * 4 + c], sizeof t); memcpy(a[k * 4 + c], a[piv * 4 + c], sizeof t); memcpy(a[piv * 4 + c], t, sizeof t); }
+                unsigned t = perm[k]; perm[k] = perm[piv]; perm[piv] = t; ++swaps;
+            }
+            for (unsigned r = k + 1; r < 4; ++r) {
+                word l[70]; lfo_cdiv(n, a[r * 4 + k], a[k * 4 + k], l); memcpy(a[r * 4 + k], l, sizeof l);
+                for (unsigned c = k + 1; c < 4; ++c) { word v[70]; c_minus(n, fused, a[r * 4 + c], l, a[k * 4 + c], v); memcpy(a[r * 4 + c], v, sizeof v); }
+            }
+        }
+        status[m] = st;
+        if (want_det) {
+            word d[70]; memset(d, 0, sizeof d);
+            if (!st) {
+                memcpy(d, a[0], sizeof d);
+                for (int k = 1; k < 4; ++k) { word t[70]; lfo_cmul(n, d, a[k * 5], t); memcpy(d, t, sizeof d); }
+                if (swaps & 1) { *SGN(d, n) = -gsgn(d, n); *SGN(d + E, n) = -gsgn(d + E, n); }
+            }
+            memcpy(det + m * (size_t)CE, d, sizeof(word) * (size_t)CE);
+        }
+        for (unsigned j = 0; j < R; ++j) {
+            word y[4][70];
+            for (unsigned i = 0; i < 4; ++i) {
+                memset(y[i], 0, sizeof y[i]);
+                if (inverse) { if (perm[i] == j) { y[i][n - 1] = 0x80000000u; *SGN(y[i], n) = 1; } }
+                else memcpy(y[i], B + ((m * 4 + perm[i]) * R + j) * (size_t)CE, sizeof(word) * (size_t)CE);
+            }
+            if (st) {
+                for (unsigned i = 0; i < 4; ++i) { word* o = X + ((m * 4 + i) * R + j) * (size_t)CE; set_zero(o, n, ST_DIV0); set_zero(o + E, n, ST_DIV0); }
+                continue;
+            }
+            for (unsigned i = 1; i < 4; ++i) for (unsigned t = 0; t < i; ++t) { word v[70]; c_minus(n, fused, y[i], a[i * 4 + t], y[t], v); memcpy(y[i], v, sizeof v); }
+            for (int i = 3; i >= 0; --i) {
+                for (unsigned t = (unsigned)i + 1; t < 4; ++t) { word v[70]; c_minus(n, fused, y[i], a[i * 4 + t], y[t], v); memcpy(y[i], v, sizeof v); }
+                word v[70]; lfo_cdiv(n, y[i], a[i * 5], v); memcpy(y[i], v, sizeof v);
+            }
+            for (unsigned i = 0; i < 4; ++i) memcpy(X + ((m * 4 + i) * R + j) * (size_t)CE, y[i], sizeof(word) * (size_t)CE);
+        }
+    }
+    return 0;
+}
+
+/* ---------------------------------------------------------------- strided batched GEMM
+ * (batched_linalg.hpp:7-14, batched_linalg.metal:16-17,24-37,145-157): C_b (+)= A_b B_b over
+ * ascending k, composed (add(mul(a,b), sum) / cadd(cmul(a,b), sum)) or fused (fma / cfma),
+ * negated at the end with `negative`.  Strides in elements. */
+int lfo_strided_gemm(int bits, int complex_, size_t count, size_t m, size_t nc, size_t k,
+                     size_t sa, size_t sb, size_t sc, int accumulate, int fused, int negative,
+                     const word* A, const word* B, word* C) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3; const size_t S = complex_ ? 2 * E : E;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (size_t t = 0; t < count; ++t)
+        for (size_t i = 0; i < m; ++i)
+            for (size_t j = 0; j < nc; ++j) {
+                word sum[70]; word* o = C + (t * sc + i * nc + j) * S;
+                if (accumulate) memcpy(sum, o, sizeof(word) * S); else memset(sum, 0, sizeof(word) * S);
+                for (size_t q = 0; q < k; ++q) {
+                    const word* x = A + (t * sa + i * k + q) * S; const word* y = B + (t * sb + q * nc + j) * S;
+                    word r[70];
+                    if (complex_) {
+                        if (fused) lfo_cfma(n, x, y, sum, 0, r);
+                        else { word p[70]; lfo_cmul(n, x, y, p); lfo_cadd(n, p, sum, r); }
+                    } else {
+                        if (fused) lfo_fma(n, x, y, sum, 0, r);
+                        else { word p[35]; lfo_mul(n, x, y, p); lfo_add(n, p, sum, r); }
+                    }
+                    memcpy(sum, r, sizeof(word) * S);
+                }
+                if (negative) { *SGN(sum, n) = -gsgn(sum, n); if (complex_) *SGN(sum + E, n) = -gsgn(sum + E, n); }
+                memcpy(o, sum, sizeof(word) * S);
+            }
+    return 0;
+}

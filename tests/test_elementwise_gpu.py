@@ -1,0 +1,237 @@
+"""GPU parity of the element-wise path through the C ABI (host-array calls, resident batches
+with chain fusion, device-pointer entry points) against the golden vectors and the C oracle,
+bit for bit; plus the reference's ownership and argument errors
+(tests/test_arithmetic.cpp, test_fused.cpp, test_broadcast.cpp, test_buffers.cpp)."""
+import numpy as np
+import pytest
+
+from limbforge_b200 import numbers as nb
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN_WIDTHS = [64, 96, 128, 224, 256, 384, 512, 1024]
+ALL_WIDTHS = list(range(64, 1025, 32))
+
+
+def same(x, y):
+    return x.shape == y.shape and bool((x == y).all())
+
+
+def first_bad(x, y):
+    d = np.nonzero((x != y).reshape(x.shape[0], -1).any(axis=1))[0]
+    return d[:5]
+
+
+@pytest.mark.parametrize("bits", GOLDEN_WIDTHS)
+def test_golden_real(engine, golden, bits):
+    from limbforge_b200.api import Operation
+    a, b, roots = golden[f"real_{bits}_a"], golden[f"real_{bits}_b"], golden[f"real_{bits}_roots"]
+    for op in (0, 1, 2, 3):
+        out, _ = engine.run(bits, Operation(op), a, b)
+        want = golden[f"real_{bits}_{op}_out"]
+        assert same(out, want), f"op {op} bad cases {first_bad(out, want)}"
+    for op, x in ((7, a), (8, roots)):
+        out, _ = engine.run_unary(bits, Operation(op), x)
+        want = golden[f"real_{bits}_{op}_out"]
+        assert same(out, want), f"op {op} bad cases {first_bad(out, want)}"
+
+
+@pytest.mark.parametrize("bits", GOLDEN_WIDTHS)
+def test_golden_fused_and_complex(engine, golden, bits):
+    from limbforge_b200.api import Operation
+    fa, fb, fc = golden[f"fused_{bits}_a"], golden[f"fused_{bits}_b"], golden[f"fused_{bits}_c"]
+    for op in (9, 10):
+        out, _ = engine.run_ternary(bits, Operation(op), fa, fb, fc)
+        want = golden[f"fused_{bits}_{op}_out"]
+        assert same(out, want), f"op {op} bad cases {first_bad(out, want)}"
+    ca, cb, cc = golden[f"cx_{bits}_a"], golden[f"cx_{bits}_b"], golden[f"cx_{bits}_c"]
+    for op in (4, 5, 6):
+        out, _ = engine.run(bits, Operation(op), ca, cb)
+        want = golden[f"cx_{bits}_{op}_out"]
+        assert same(out, want), f"op {op} bad cases {first_bad(out, want)}"
+    for op in (11, 12):
+        out, _ = engine.run_ternary(bits, Operation(op), ca, cb, cc)
+        want = golden[f"cx_{bits}_{op}_out"]
+        assert same(out, want), f"op {op} bad cases {first_bad(out, want)}"
+
+
+@pytest.mark.parametrize("bits", ALL_WIDTHS)
+def test_every_width_vs_oracle(engine, oracle, bits):
+    from limbforge_b200.api import Operation
+    rng = np.random.default_rng(1000 + bits)
+    n = bits // 32
+    cnt = 1024
+    a = nb.random_numbers(rng, cnt, bits, 1000, zero_frac=0.03, sparse_frac=0.05)
+    b = nb.random_numbers(rng, cnt, bits, 1000, zero_frac=0.03, sparse_frac=0.05)
+    c = nb.random_numbers(rng, cnt, bits, 1500, zero_frac=0.03, sparse_frac=0.05)
+    b[::3, n] = (nb.exponent(a[::3]) - rng.integers(0, bits + 80, size=a[::3].shape[0])).astype(np.int32).view(np.uint32)
+    b[1::9] = nb.negate(a[1::9])
+    b[1::9, 0] ^= np.uint32(3)
+    c[2::7] = nb.negate(oracle.elementwise(bits, 2, a[2::7].copy(), b[2::7].copy()))
+    a[5::97, n + 2] = nb.INVALID
+    for op in (0, 1, 2, 3, 7):
+        out = engine.run(bits, Operation(op), a, b)[0] if op != 7 else engine.run_unary(bits, Operation(op), a)[0]
+        want = oracle.elementwise(bits, op, a, b)
+        assert same(out, want), f"op {op} bad {first_bad(out, want)}"
+    r = a.copy()
+    r[:, n + 1] = np.abs(nb.sign(r)).astype(np.int32).view(np.uint32)
+    assert same(engine.run_unary(bits, Operation.sqrt, r)[0], oracle.elementwise(bits, 8, r))
+    for op in (9, 10):
+        out = engine.run_ternary(bits, Operation(op), a, b, c)[0]
+        want = oracle.elementwise(bits, op, a, b, c)
+        assert same(out, want), f"op {op} bad {first_bad(out, want)}"
+    ca, cb, cc = (nb.random_complex(rng, 96, bits, 30) for _ in range(3))
+    cb[::5, 0], cb[::5, 1] = ca[::5, 1], ca[::5, 0]
+    for op in (4, 5, 6):
+        assert same(engine.run(bits, Operation(op), ca, cb)[0], oracle.elementwise(bits, op, ca, cb)), f"complex op {op}"
+    for op in (11, 12):
+        assert same(engine.run_ternary(bits, Operation(op), ca, cb, cc)[0], oracle.elementwise(bits, op, ca, cb, cc)), f"op {op}"
+
+
+@pytest.mark.parametrize("bits", [64, 224, 256, 384, 1024])
+def test_broadcast_operands(engine, oracle, bits):
+    """tests/test_broadcast.cpp: b (and c) read at (i / stride) % period."""
+    from limbforge_b200.api import Broadcast, Operation, broadcast_elements
+    rng = np.random.default_rng(bits + 9)
+    n = 1001
+    for bb in (Broadcast(4, 0), Broadcast(1, 7), Broadcast(3, 5), Broadcast(n, 0)):
+        m = broadcast_elements(n, bb)
+        a = nb.random_numbers(rng, n, bits, 9)
+        b = nb.random_numbers(rng, m, bits, 9)
+        out, _ = engine.run(bits, Operation.mul, a, b, b_index=bb)
+        assert same(out, oracle.elementwise(bits, 2, a, b, b_index=(bb.stride, bb.period)))
+        A, B, O = engine.make_buffer(n, bits), engine.make_buffer(m, bits), engine.make_buffer(n, bits)
+        A.upload(a)
+        B.upload(b)
+        batch = engine.batch()
+        batch.run(Operation.div, A, B, None, O, b_index=bb)
+        batch.submit().wait()
+        assert same(O.download(), oracle.elementwise(bits, 3, a, b, b_index=(bb.stride, bb.period)))
+        cb = Broadcast(2, 3)
+        mc = broadcast_elements(n, cb)
+        x, y, z = nb.random_complex(rng, n, bits, 5), nb.random_complex(rng, m, bits, 5), nb.random_complex(rng, mc, bits, 8)
+        out, _ = engine.run(bits, Operation.complex_mul, x, y, b_index=bb)
+        assert same(out, oracle.elementwise(bits, 5, x, y, b_index=(bb.stride, bb.period)))
+        out, _ = engine.run_ternary(bits, Operation.complex_fma, x, y, z, b_index=bb, c_index=cb)
+        assert same(out, oracle.elementwise(bits, 11, x, y, z, b_index=(bb.stride, bb.period), c_index=(cb.stride, cb.period)))
+
+
+def test_resident_mul_chain_is_fused_and_exact(engine, oracle):
+    """Config-1 shape at reduced count: x <- x * f_s, 16 steps at 1024 bits, in one batch; the
+    batch fuses the steps into one register-resident kernel."""
+    from limbforge_b200.api import Operation
+    bits, count, steps = 1024, 4096, 16
+    rng = np.random.default_rng(7)
+    x = nb.random_numbers(rng, count, bits, 8, zero_frac=0.01, sparse_frac=0.02)
+    f = np.stack([nb.random_numbers(rng, count, bits, 8, zero_frac=0.01, sparse_frac=0.02) for _ in range(steps)])
+    want = oracle.mul_chain(bits, x, f)
+    X = engine.make_buffer(count, bits)
+    X.upload(x)
+    F = [engine.make_buffer(count, bits) for _ in range(steps)]
+    for s in range(steps):
+        F[s].upload(f[s])
+    batch = engine.batch()
+    for s in range(steps):
+        batch.run(Operation.mul, X, F[s], None, X)
+    t = batch.submit().wait()
+    assert same(X.download(), want)
+    assert t.gpu_seconds > 0
+    # observable intermediates: y1 = x*f0, y2 = y1*f1 written to separate buffers
+    Y1, Y2 = engine.make_buffer(count, bits), engine.make_buffer(count, bits)
+    X.upload(x)
+    batch = engine.batch()
+    batch.run(Operation.mul, X, F[0], None, Y1)
+    batch.run(Operation.add, Y1, F[1], None, Y2)
+    batch.run(Operation.div, Y2, F[2], None, Y2)
+    batch.submit().wait()
+    y1 = oracle.elementwise(bits, 2, x, f[0])
+    y2 = oracle.elementwise(bits, 3, oracle.elementwise(bits, 0, y1, f[1]), f[2])
+    assert same(Y1.download(), y1)
+    assert same(Y2.download(), y2)
+
+
+def test_device_pointer_chain_entry(oracle):
+    import ctypes
+    from limbforge_b200 import api
+    bits, count, steps = 512, 3000, 5
+    rng = np.random.default_rng(11)
+    x = nb.random_numbers(rng, count, bits, 8)
+    f = np.stack([nb.random_numbers(rng, count, bits, 8) for _ in range(steps)])
+    want = oracle.mul_chain(bits, x, f)
+    e = api.Engine()
+    X, F, O = e.make_buffer(count, bits), e.make_buffer(count * steps, bits), e.make_buffer(count, bits)
+    X.upload(x)
+    F.upload(f.reshape(count * steps, -1))
+    api.dev_mul_chain(bits, X.device_pointer(), F.device_pointer(), count, steps, O.device_pointer(), count)
+    cudart = ctypes.CDLL("libcudart.so")
+    assert cudart.cudaDeviceSynchronize() == 0
+    assert same(O.download(), want)
+
+
+def test_buffer_ownership_and_batch_errors(engine):
+    """tests/test_buffers.cpp: busy buffers, foreign engines, single-use batches, short operands."""
+    from limbforge_b200 import api
+    from limbforge_b200.api import Broadcast, InvalidArgument, LogicError, Operation
+    bits, n = 256, 64
+    rng = np.random.default_rng(2)
+    a = nb.random_numbers(rng, n, bits, 9)
+    A, B, O = engine.make_buffer(n, bits), engine.make_buffer(n, bits), engine.make_buffer(n, bits)
+    A.upload(a)
+    B.upload(a)
+    batch = engine.batch()
+    batch.run(Operation.mul, A, B, None, O)
+    sub = batch.submit()
+    with pytest.raises(LogicError):
+        batch.submit()
+    with pytest.raises(LogicError):
+        batch.run(Operation.mul, A, B, None, O)
+    sub.wait()
+    assert sub.ready()
+    sub.wait()                                        # repeated waits are fine
+    other = api.Engine()
+    foreign = other.make_buffer(n, bits)
+    with pytest.raises(InvalidArgument):
+        b2 = engine.batch()
+        b2.run(Operation.add, A, foreign, None, O)
+    with pytest.raises(InvalidArgument):
+        short = engine.make_buffer(1, bits)
+        b3 = engine.batch()
+        b3.run(Operation.add, engine.make_buffer(8, bits), short, None, engine.make_buffer(8, bits), b_index=Broadcast(4, 0))
+    with pytest.raises(InvalidArgument):
+        engine.run(100, Operation.add, a, a)
+    with pytest.raises(InvalidArgument):
+        engine.run(bits, Operation.fma, a, a)
+    with pytest.raises(InvalidArgument):
+        engine.run_ternary(bits, Operation.add, a, a, a)
+    # mapped(): a host view; writes reach the device at the next submission
+    view = A.mapped()
+    view[:] = 0
+    view[:, bits // 32 - 1] = 0x80000000
+    view[:, bits // 32 + 1] = 1                       # every value = 1
+    batch = engine.batch()
+    batch.run(Operation.mul, A, B, None, O)
+    sub = batch.submit()
+    with pytest.raises(LogicError):
+        A.mapped()
+    with pytest.raises(LogicError):
+        A.upload(a)
+    sub.wait()
+    assert same(O.download(), a)
+    # empty batches and zero counts are accepted
+    engine.batch().submit().wait()
+    out, t = engine.run(bits, Operation.add, a[:0], a[:0])
+    assert out.shape[0] == 0
+
+
+def test_dense_1024_complex_repeats(engine, oracle):
+    """tests/test_arithmetic.cpp:115-129: 65,536 dense 1024-bit complex values, three GPU repeats."""
+    from limbforge_b200.api import Operation
+    bits, count = 1024, 65536
+    rng = np.random.default_rng(20261007 + bits)
+    a = nb.random_complex(rng, count, bits, 5)
+    b = nb.random_complex(rng, count, bits, 5)
+    for op in (4, 5, 6):
+        want = oracle.elementwise(bits, op, a, b)
+        for _ in range(3):
+            out, _ = engine.run(bits, Operation(op), a, b)
+            assert same(out, want), f"op {op} bad {first_bad(out, want)}"
