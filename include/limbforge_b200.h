@@ -43,7 +43,23 @@ typedef struct lf_strided_gemm {                                                
     size_t count, m, n, k, stride_a, stride_b, stride_c; int accumulate, fused, negative;
 } lf_strided_gemm;
 
+typedef struct lf_linalg_options {                                                      /* linalg.hpp:18-25 */
+    int band_bits, max_bands, max_spread; unsigned host_threads; int force_fallback, resident_bands;
+    int method;   /* 0 auto (residue engine where it applies), 1 generic limb kernel, 2 residue engine only */
+} lf_linalg_options;
+typedef struct lf_factor_options { size_t block; double host_macs, solve_host_macs; int gpu; } lf_factor_options; /* linalg.hpp:73-78 */
+typedef struct lf_cholesky_info {                                                       /* linalg.hpp:82-87 */
+    size_t pivot; int pivot_sign; uint32_t pivot_status; lf_timing timing;
+    size_t blocks, gpu_updates, host_updates; double panel_seconds, update_seconds;
+} lf_cholesky_info;
+typedef struct lf_linalg_report {                                                       /* linalg.hpp:35-45 (subset) */
+    size_t m, n, k, gpu_outputs, trivial_outputs, gemm_rows, gemm_cols, int8_gemms, moduli, band_bits;
+    double analysis_seconds, gpu_seconds;
+    int method;   /* 1 generic limb kernel, 2 residue engine */
+} lf_linalg_report;
+
 typedef struct lf_engine lf_engine;
+typedef struct lf_linalg lf_linalg;
 typedef struct lf_buffer lf_buffer;
 typedef struct lf_batch lf_batch;
 typedef struct lf_submission lf_submission;
@@ -73,6 +89,31 @@ int lf_engine_lu4(lf_engine* engine, int bits, const lf_batched4* shape, const v
  * rounding per step (composed) or per fused step; C is read (accumulate) and written */
 int lf_batched_gemm(lf_engine* engine, int bits, int complex_, const lf_strided_gemm* shape, const void* A,
                     const void* B, void* C, lf_timing* timing);
+
+/* ---- Linalg (linalg.hpp:141-218): exact products, blocked Cholesky, triangular solves ---- */
+int lf_linalg_create(lf_engine* engine, const lf_linalg_options* options, lf_linalg** out); /* Linalg::Linalg (engine may be NULL) */
+void lf_linalg_destroy(lf_linalg* linalg);
+int lf_linalg_get_report(lf_linalg* linalg, lf_linalg_report* report);                 /* Linalg::report */
+/* Linalg::gemm (linalg.hpp:155): C (m x n) = op(A) B, or RN(C - op(A) B) with subtract */
+int lf_linalg_gemm(lf_linalg* linalg, int bits, int transpose_a, const void* A, const void* B, size_t m, size_t n, size_t k,
+                   void* C, int subtract, lf_timing* timing);
+/* Linalg::syrk (linalg.hpp:152): C (cols x cols) = A^T A, lower triangle or full */
+int lf_linalg_syrk(lf_linalg* linalg, int bits, const void* A, size_t rows, size_t cols, void* C, int lower_only,
+                   int subtract, lf_timing* timing);
+/* Linalg::cholesky (linalg.hpp:158) */
+int lf_linalg_cholesky(lf_linalg* linalg, int bits, const void* A, size_t n, void* L, const lf_factor_options* options,
+                       lf_cholesky_info* info);
+/* Linalg::trsm (linalg.hpp:161) */
+int lf_linalg_trsm(lf_linalg* linalg, int bits, int transpose, const void* L, size_t n, const void* B, size_t nrhs, void* X,
+                   const lf_factor_options* options, lf_timing* timing);
+/* Linalg::cholesky_solve (linalg.hpp:163) */
+int lf_linalg_cholesky_solve(lf_linalg* linalg, int bits, const void* L, size_t n, const void* B, size_t nrhs, void* X,
+                             const lf_factor_options* options, lf_timing* timing);
+/* Exact product on device line views (CUDA callers; no reference counterpart): element (line, k)
+ * at base + (line * ls + k * ks) elements; C element (i, j) at C + i * ldc + j elements. */
+int lf_dev_exact_product(lf_linalg* linalg, int bits, const void* left, size_t left_ls, size_t left_ks, const void* right,
+                         size_t right_ls, size_t right_ks, size_t M, size_t N, size_t K, void* C, size_t ldc, int subtract,
+                         int lower, void* stream);
 
 /* ---- Buffers (engine.hpp:74-86, 194-198): device-resident typed storage of one engine ---- */
 int lf_buffer_create(lf_engine* engine, size_t bytes, lf_buffer** out);                /* Engine::make_buffer */

@@ -108,6 +108,38 @@ class StridedGemm:                                               # batched_linal
     negative: bool = False
 
 
+@dataclass
+class LinalgOptions:                                             # linalg.hpp:18-25
+    band_bits: int = 64
+    max_bands: int = 4
+    max_spread: int = 512
+    host_threads: int = 0
+    force_fallback: bool = False
+    resident_bands: int = 2
+    method: int = 0          # 0 auto (residue engine where it applies), 1 generic limb kernel, 2 residue only
+
+
+@dataclass
+class FactorOptions:                                             # linalg.hpp:73-78
+    block: int = 32
+    host_macs: float = 5e4
+    solve_host_macs: float = 4e5
+    gpu: bool = True
+
+
+@dataclass
+class CholeskyInfo:                                              # linalg.hpp:82-87
+    pivot: int = 0
+    pivot_sign: int = 0
+    pivot_status: int = 0
+    timing: "Timing" = None
+    blocks: int = 0
+    gpu_updates: int = 0
+    host_updates: int = 0
+    panel_seconds: float = 0.0
+    update_seconds: float = 0.0
+
+
 class _Timing(C.Structure):
     _fields_ = [("gpu_seconds", C.c_double), ("wall_seconds", C.c_double)]
 
@@ -129,6 +161,27 @@ class _StridedGemm(C.Structure):
     _fields_ = [("count", C.c_size_t), ("m", C.c_size_t), ("n", C.c_size_t), ("k", C.c_size_t),
                 ("stride_a", C.c_size_t), ("stride_b", C.c_size_t), ("stride_c", C.c_size_t),
                 ("accumulate", C.c_int), ("fused", C.c_int), ("negative", C.c_int)]
+
+
+class _LinalgOptions(C.Structure):
+    _fields_ = [("band_bits", C.c_int), ("max_bands", C.c_int), ("max_spread", C.c_int), ("host_threads", C.c_uint),
+                ("force_fallback", C.c_int), ("resident_bands", C.c_int), ("method", C.c_int)]
+
+
+class _FactorOptions(C.Structure):
+    _fields_ = [("block", C.c_size_t), ("host_macs", C.c_double), ("solve_host_macs", C.c_double), ("gpu", C.c_int)]
+
+
+class _CholeskyInfo(C.Structure):
+    _fields_ = [("pivot", C.c_size_t), ("pivot_sign", C.c_int), ("pivot_status", C.c_uint32), ("timing", _Timing),
+                ("blocks", C.c_size_t), ("gpu_updates", C.c_size_t), ("host_updates", C.c_size_t),
+                ("panel_seconds", C.c_double), ("update_seconds", C.c_double)]
+
+
+class _LinalgReport(C.Structure):
+    _fields_ = [(f, C.c_size_t) for f in ("m", "n", "k", "gpu_outputs", "trivial_outputs", "gemm_rows", "gemm_cols",
+                                          "int8_gemms", "moduli", "band_bits")] + \
+               [("analysis_seconds", C.c_double), ("gpu_seconds", C.c_double), ("method", C.c_int)]
 
 
 def _load() -> C.CDLL:
@@ -157,6 +210,14 @@ def _load() -> C.CDLL:
         "lf_dev_elementwise": ([I, I, V, V, V, V, S, _Broadcast, _Broadcast, V], I),
         "lf_host_alloc": ([S, P(V)], I), "lf_host_free": ([V], None),
         "lf_dev_mul_chain": ([I, V, V, S, C.c_uint, V, S, V], I),
+        "lf_linalg_create": ([V, P(_LinalgOptions), P(V)], I), "lf_linalg_destroy": ([V], None),
+        "lf_linalg_get_report": ([V, P(_LinalgReport)], I),
+        "lf_linalg_gemm": ([V, I, I, V, V, S, S, S, V, I, P(_Timing)], I),
+        "lf_linalg_syrk": ([V, I, V, S, S, V, I, I, P(_Timing)], I),
+        "lf_linalg_cholesky": ([V, I, V, S, V, P(_FactorOptions), P(_CholeskyInfo)], I),
+        "lf_linalg_trsm": ([V, I, I, V, S, V, S, V, P(_FactorOptions), P(_Timing)], I),
+        "lf_linalg_cholesky_solve": ([V, I, V, S, V, S, V, P(_FactorOptions), P(_Timing)], I),
+        "lf_dev_exact_product": ([V, I, V, S, S, V, S, S, S, S, S, V, S, I, I, V], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -419,6 +480,76 @@ class PinnedArray:
             self.array = None
             lib.lf_host_free(self._p)
             self._p = None
+
+
+class Linalg:
+    """Exact dense products and factorizations (linalg.hpp:141-218).  One Linalg per host thread."""
+
+    def __init__(self, engine: "Engine | None" = None, options: LinalgOptions | None = None):
+        o = options or LinalgOptions()
+        self.options = o
+        self.engine = engine
+        co = _LinalgOptions(o.band_bits, o.max_bands, o.max_spread, o.host_threads, int(o.force_fallback),
+                            o.resident_bands, o.method)
+        h = C.c_void_p()
+        check(lib.lf_linalg_create(engine.handle if engine else None, C.byref(co), C.byref(h)))
+        self.handle = h
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib.lf_linalg_destroy(self.handle)
+            self.handle = None
+
+    def report(self) -> dict:
+        r = _LinalgReport()
+        check(lib.lf_linalg_get_report(self.handle, C.byref(r)))
+        return {f: getattr(r, f) for f, _ in r._fields_}
+
+    def gemm(self, bits, transpose_a, A, B, m, n, k, C_, subtract=False) -> Timing:
+        t = _Timing()
+        check(lib.lf_linalg_gemm(self.handle, bits, int(transpose_a), _ptr(A), _ptr(B), m, n, k, _ptr(C_), int(subtract),
+                                 C.byref(t)))
+        return _timing(t)
+
+    def syrk(self, bits, A, rows, cols, C_, lower_only=True, subtract=False) -> Timing:
+        t = _Timing()
+        check(lib.lf_linalg_syrk(self.handle, bits, _ptr(A), rows, cols, _ptr(C_), int(lower_only), int(subtract), C.byref(t)))
+        return _timing(t)
+
+    @staticmethod
+    def _fo(o: FactorOptions | None):
+        o = o or FactorOptions()
+        return _FactorOptions(o.block, o.host_macs, o.solve_host_macs, int(o.gpu))
+
+    def cholesky(self, bits, A, n, L, options: FactorOptions | None = None) -> CholeskyInfo:
+        i = _CholeskyInfo()
+        fo = self._fo(options)
+        check(lib.lf_linalg_cholesky(self.handle, bits, _ptr(A), n, _ptr(L), C.byref(fo), C.byref(i)))
+        return CholeskyInfo(i.pivot, i.pivot_sign, i.pivot_status, _timing(i.timing), i.blocks, i.gpu_updates,
+                            i.host_updates, i.panel_seconds, i.update_seconds)
+
+    def trsm(self, bits, transpose, L, n, B, nrhs, X, options: FactorOptions | None = None) -> Timing:
+        t = _Timing()
+        fo = self._fo(options)
+        check(lib.lf_linalg_trsm(self.handle, bits, int(transpose), _ptr(L), n, _ptr(B), nrhs, _ptr(X), C.byref(fo), C.byref(t)))
+        return _timing(t)
+
+    def cholesky_solve(self, bits, L, n, B, nrhs, X, options: FactorOptions | None = None) -> Timing:
+        t = _Timing()
+        fo = self._fo(options)
+        check(lib.lf_linalg_cholesky_solve(self.handle, bits, _ptr(L), n, _ptr(B), nrhs, _ptr(X), C.byref(fo), C.byref(t)))
+        return _timing(t)
+
+    # explicit contract names (linalg.hpp:203-210)
+    gemm_exact = gemm
+    syrk_exact = syrk
+    cholesky_blocked = cholesky
+    cholesky_solve_blocked = cholesky_solve
+
+    def dev_exact_product(self, bits, left, left_ls, left_ks, right, right_ls, right_ks, M, N, K, C_, ldc,
+                          subtract=False, lower=False, stream=0) -> None:
+        check(lib.lf_dev_exact_product(self.handle, bits, _ptr(left), left_ls, left_ks, _ptr(right), right_ls, right_ks,
+                                       M, N, K, _ptr(C_), ldc, int(subtract), int(lower), C.c_void_p(stream)))
 
 
 def dev_elementwise(bits, op, a_ptr, b_ptr, c_ptr, out_ptr, count, b_index=None, c_index=None, stream=0) -> None:

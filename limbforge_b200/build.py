@@ -27,14 +27,22 @@ def _headers() -> list[str]:
 
 
 def _stale(src: str, obj: str, newest_header: float) -> bool:
-    if not os.path.exists(obj):
+    """An object is stale when it, or the dependency list nvcc wrote beside it, is missing, or
+    when the source or any header it included is newer."""
+    dep = obj + ".d"
+    if not os.path.exists(obj) or not os.path.exists(dep):
         return True
     t = os.path.getmtime(obj)
-    return os.path.getmtime(src) > t or newest_header > t
+    text = open(dep).read().replace("\\\n", " ")
+    files = text.split(":", 1)[1].split() if ":" in text else []
+    for f in [src] + files:
+        if not os.path.exists(f) or os.path.getmtime(f) > t:
+            return True
+    return False
 
 
 def _compile(src: str, obj: str, verbose: bool) -> str:
-    cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
+    cmd = [NVCC, *ARCH, *FLAGS, "-MD", "-MF", obj + ".d", "-c", src, "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

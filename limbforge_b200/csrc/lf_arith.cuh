@@ -17,6 +17,7 @@ namespace lfd {
 typedef uint32_t u32;
 typedef uint64_t u64;
 typedef int64_t i64;
+typedef uint16_t u16;
 
 constexpr i64 kEmax = 1000000000;
 enum : u32 { kDivZero = 1, kOverflow = 2, kInvalid = 4 };
@@ -133,16 +134,30 @@ template <int N, int W> __device__ __forceinline__ Num<N> round_general(u32 (&x)
 }
 
 // ---------------------------------------------------------------- mul
-// p (2N words) = a * b, schoolbook rows with 64-bit multiply-accumulate (IMAD.WIDE).
+// Carry-chain primitives (PTX add/mad with .cc): one IMAD per half word product.
+__device__ __forceinline__ u32 mad_lo_cc(u32 a, u32 b, u32 c) { u32 r; asm volatile("mad.lo.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+__device__ __forceinline__ u32 madc_lo_cc(u32 a, u32 b, u32 c) { u32 r; asm volatile("madc.lo.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+__device__ __forceinline__ u32 mad_hi_cc(u32 a, u32 b, u32 c) { u32 r; asm volatile("mad.hi.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+__device__ __forceinline__ u32 madc_hi_cc(u32 a, u32 b, u32 c) { u32 r; asm volatile("madc.hi.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+__device__ __forceinline__ u32 madc_hi(u32 a, u32 b, u32 c) { u32 r; asm volatile("madc.hi.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+__device__ __forceinline__ u32 carry_out() { u32 r; asm volatile("addc.u32 %0, 0, 0;" : "=r"(r)); return r; }
+
+// p (2N words) = a * b, schoolbook by rows: for row i a low-half carry chain adds
+// lo(a_i b_j) into p[i+j] and a high-half chain adds hi(a_i b_j) into p[i+j+1]; the running
+// sum never exceeds 2^(32(i+N+1)), so the last high-half step cannot carry out.
 template <int N> __device__ __forceinline__ void mant_mul(const u32 (&a)[N], const u32 (&b)[N], u32 (&p)[2 * N]) {
 #pragma unroll
     for (int k = 0; k < 2 * N; ++k) p[k] = 0;
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-        u64 c = 0;
+        p[i] = mad_lo_cc(a[i], b[0], p[i]);
 #pragma unroll
-        for (int j = 0; j < N; ++j) { u64 t = (u64)a[i] * b[j] + p[i + j] + c; p[i + j] = (u32)t; c = t >> 32; }
-        p[i + N] = (u32)c;
+        for (int j = 1; j < N; ++j) p[i + j] = madc_lo_cc(a[i], b[j], p[i + j]);
+        p[i + N] = carry_out();
+        p[i + 1] = mad_hi_cc(a[i], b[0], p[i + 1]);
+#pragma unroll
+        for (int j = 1; j < N - 1; ++j) p[i + j + 1] = madc_hi_cc(a[i], b[j], p[i + j + 1]);
+        p[i + N] = madc_hi(a[i], b[N - 1], p[i + N]);
     }
 }
 // Round a product of two normalized mantissas: its top bit is bit 64N-1 or 64N-2.

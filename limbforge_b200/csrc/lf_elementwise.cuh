@@ -61,7 +61,7 @@ template <int N, int OP> __global__ void __launch_bounds__(kEwThreads) ew_kernel
 
 // v <- op_s(v, b_s[...]) for every step; out_s written where non-null.  Steps are uniform across
 // the grid, so the switch never diverges.
-template <int N> __global__ void __launch_bounds__(kEwThreads) chain_kernel(const __grid_constant__ ChainParams p) {
+template <int N, bool MUL_ONLY> __global__ void __launch_bounds__(kEwThreads) chain_kernel(const __grid_constant__ ChainParams p) {
     const u64 i = (u64)blockIdx.x * kEwThreads + threadIdx.x;
     if (i >= p.count) return;
     constexpr u64 E = N + 3;
@@ -70,7 +70,8 @@ template <int N> __global__ void __launch_bounds__(kEwThreads) chain_kernel(cons
     for (int s = 0; s < p.steps; ++s) {
         const ChainStep& st = p.step[s];
         const Num<N> y = load_plain<N>(st.b + E * bidx(i, st.bs, st.bp));
-        switch (st.op) {
+        if constexpr (MUL_ONLY) v = mul<N>(v, y);
+        else switch (st.op) {
         case 0: v = add<N>(v, y); break;
         case 1: v = sub<N>(v, y); break;
         case 2: v = mul<N>(v, y); break;
@@ -104,7 +105,10 @@ template <int N> int launch_ew(int op, const EwParams& p, cudaStream_t s) {
 template <int N> int launch_chain(const ChainParams& p, cudaStream_t s) {
     if (!p.count) return 0;
     const unsigned blocks = (unsigned)((p.count + kEwThreads - 1) / kEwThreads);
-    chain_kernel<N><<<blocks, kEwThreads, 0, s>>>(p);
+    bool mul_only = true;
+    for (int k = 0; k < p.steps; ++k) mul_only = mul_only && p.step[k].op == 2;
+    if (mul_only) chain_kernel<N, true><<<blocks, kEwThreads, 0, s>>>(p);     // registers of mul alone
+    else chain_kernel<N, false><<<blocks, kEwThreads, 0, s>>>(p);
     return 0;
 }
 

@@ -1,0 +1,382 @@
+// C ABI of the exact dense products and factorizations (the reference's Linalg, linalg.hpp:141-218,
+// linalg.mm:176-488): host-array and device-resident forms of gemm/syrk, blocked Cholesky with the
+// reference's fixed rounding sequence, and multi-RHS triangular solves.  Every product runs on the
+// GPU (no host fallback): the residue/CRT tensor-core engine where it applies, the generic exact limb
+// kernel otherwise; both give identical bits.
+#include "lf_runtime.h"
+#include "lf_linalg.cuh"
+#include "lf_residue.h"
+
+#include <algorithm>
+#include <chrono>
+
+namespace lfr {
+
+struct Linalg {
+    Engine* engine = nullptr;
+    bool own_engine = false;
+    lf_linalg_options options{};
+    lf_linalg_report report{};
+    DevBuf work[6];
+    DevBuf info_buf, error_buf, lines;
+    ResidueEngine residue;
+};
+
+using Clock = std::chrono::steady_clock;
+static double since(Clock::time_point t) { return std::chrono::duration<double>(Clock::now() - t).count(); }
+static void check_bits(int bits) { if (bits < 64 || bits > 1024 || bits % 32) throw invalid_argument("bits must be a multiple of 32 in [64,1024]"); }
+
+// C (M x Nc at ldc) <- RN(C - L R^T) (subtract) or RN(L R^T), L/R given as line views; lower: only j <= i.
+void exact_product(Linalg& la, int bits, lfd::LineView left, lfd::LineView right, uint64_t M, uint64_t Nc, uint64_t K,
+                   uint32_t* C, uint64_t ldc, bool subtract, bool lower, cudaStream_t s, int* method_used) {
+    if (!M || !Nc) return;
+    const int n = bits / 32;
+    uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));
+    cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
+    int method = la.options.method;                    // 0 auto, 1 limb kernel, 2 residue engine
+    bool used_residue = false;
+    if (method != 1 && !la.options.force_fallback)
+        used_residue = la.residue.run(bits, left, right, M, Nc, K, C, ldc, subtract, lower, err, s, method == 2, la.report);
+    if (!used_residue) {
+        lfd::DotParams p{};
+        p.left = left; p.right = right; p.C = C; p.ldc = ldc; p.M = M; p.Nc = Nc; p.K = K;
+        p.row0 = 0; p.col0 = 0; p.subtract = subtract; p.lower = lower; p.error = err;
+        lfd::linalg_kernels(n)->dot(p, s);
+        cuda_check(cudaGetLastError(), "exact product launch");
+    }
+    if (method_used) *method_used = used_residue ? 2 : 1;
+    uint32_t e = 0;
+    cuda_check(cudaMemcpyAsync(&e, err, 4, cudaMemcpyDeviceToHost, s), "error flag");
+    cuda_check(cudaStreamSynchronize(s), "exact product");
+    if (e) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+}
+
+static void validate_dims(size_t M, size_t Nc, size_t K, size_t stride) {
+    const size_t limit = size_t(1) << 31;
+    if (M >= limit || Nc >= limit || K >= limit || M * stride >= limit) throw invalid_argument("matrix dimensions exceed 32-bit indexing");
+}
+
+}  // namespace lfr
+
+using namespace lfr;
+struct lf_engine : Engine {};
+struct lf_buffer : Buffer {};
+struct lf_batch : Batch {};
+struct lf_linalg : Linalg {};
+
+extern "C" {
+
+int lf_linalg_create(lf_engine* engine, const lf_linalg_options* options, lf_linalg** out) {
+    LF_API_BEGIN
+    if (!out) throw invalid_argument("null handle");
+    lf_linalg_options o{64, 4, 512, 0, 0, 2, 0};
+    if (options) o = *options;
+    if (o.band_bits < 0 || o.band_bits > 1024 || o.max_bands < 0 || o.max_spread < 0 || o.max_spread > 8192)
+        throw invalid_argument("linalg options: band_bits in [0,1024], max_bands >= 0, max_spread in [0,8192]");
+    auto* la = new lf_linalg();
+    la->options = o;
+    if (engine) la->engine = engine;
+    else {
+        lf_engine* e = nullptr;
+        int rc = lf_engine_create(nullptr, &e);
+        if (rc) { delete la; throw runtime_error(lf_last_error()); }
+        la->engine = e; la->own_engine = true;
+    }
+    *out = la;
+    LF_API_END
+}
+void lf_linalg_destroy(lf_linalg* la) {
+    if (!la) return;
+    if (la->own_engine) lf_engine_destroy(static_cast<lf_engine*>(la->engine));
+    delete la;
+}
+int lf_linalg_get_report(lf_linalg* la, lf_linalg_report* r) {
+    LF_API_BEGIN
+    if (!la || !r) throw invalid_argument("null argument");
+    *r = la->report;
+    LF_API_END
+}
+
+// Linalg::gemm (linalg.hpp:155; linalg.mm:181-185): C (m x n) = op(A) B, or RN(C - op(A) B).
+int lf_linalg_gemm(lf_linalg* la, int bits, int transpose_a, const void* A, const void* B, size_t m, size_t n, size_t k,
+                   void* C, int subtract, lf_timing* timing) {
+    LF_API_BEGIN
+    if (!la) throw invalid_argument("null linalg");
+    check_bits(bits);
+    validate_dims(m, n, k, n);
+    if (m && n && !C) throw invalid_argument("null output");
+    if (m * n && k && (!A || !B)) throw invalid_argument("null input");
+    auto w0 = Clock::now();
+    la->report = lf_linalg_report{};
+    la->report.m = m; la->report.n = n; la->report.k = k;
+    if (timing) *timing = {0, 0};
+    if (!m || !n) return LF_OK;
+    Engine& e = *la->engine;
+    e.activate();
+    const size_t E = bits / 32 + 3, eb = 4 * E;
+    cudaStream_t s = e.stream;
+    uint32_t* dA = static_cast<uint32_t*>(la->work[0].get(m * k * eb + 16));
+    uint32_t* dB = static_cast<uint32_t*>(la->work[1].get(k * n * eb + 16));
+    uint32_t* dC = static_cast<uint32_t*>(la->work[2].get(m * n * eb));
+    if (k) {
+        cuda_check(cudaMemcpyAsync(dA, A, m * k * eb, cudaMemcpyHostToDevice, s), "upload");
+        cuda_check(cudaMemcpyAsync(dB, B, k * n * eb, cudaMemcpyHostToDevice, s), "upload");
+    }
+    if (subtract) cuda_check(cudaMemcpyAsync(dC, C, m * n * eb, cudaMemcpyHostToDevice, s), "upload");
+    lfd::LineView lv = transpose_a ? lfd::LineView{dA, 1, m} : lfd::LineView{dA, k, 1};
+    lfd::LineView rv{dB, 1, n};
+    cuda_check(cudaEventRecord(e.e0, s), "event");
+    int method = 1;
+    exact_product(*la, bits, lv, rv, m, n, k, dC, n, subtract != 0, false, s, &method);
+    cuda_check(cudaEventRecord(e.e1, s), "event");
+    cuda_check(cudaMemcpyAsync(C, dC, m * n * eb, cudaMemcpyDeviceToHost, s), "download");
+    cuda_check(cudaStreamSynchronize(s), "execution");
+    float ms = 0; cudaEventElapsedTime(&ms, e.e0, e.e1);
+    la->report.gpu_seconds = ms * 1e-3; la->report.gpu_outputs = m * n; la->report.method = method;
+    if (timing) *timing = {ms * 1e-3, since(w0)};
+    LF_API_END
+}
+
+// Linalg::syrk (linalg.hpp:152; linalg.mm:176-180): C (cols x cols) = A^T A, lower or full.
+int lf_linalg_syrk(lf_linalg* la, int bits, const void* A, size_t rows, size_t cols, void* C, int lower_only, int subtract,
+                   lf_timing* timing) {
+    LF_API_BEGIN
+    if (!la) throw invalid_argument("null linalg");
+    check_bits(bits);
+    if (subtract && !lower_only) throw invalid_argument("syrk: subtract updates the lower triangle only (lower_only)");
+    validate_dims(cols, cols, rows, cols);
+    if (cols && !C) throw invalid_argument("null output");
+    if (cols && rows && !A) throw invalid_argument("null input");
+    auto w0 = Clock::now();
+    la->report = lf_linalg_report{};
+    la->report.m = cols; la->report.n = cols; la->report.k = rows;
+    if (timing) *timing = {0, 0};
+    if (!cols) return LF_OK;
+    Engine& e = *la->engine;
+    e.activate();
+    const size_t E = bits / 32 + 3, eb = 4 * E;
+    cudaStream_t s = e.stream;
+    uint32_t* dA = static_cast<uint32_t*>(la->work[0].get(rows * cols * eb + 16));
+    uint32_t* dC = static_cast<uint32_t*>(la->work[2].get(cols * cols * eb));
+    if (rows) cuda_check(cudaMemcpyAsync(dA, A, rows * cols * eb, cudaMemcpyHostToDevice, s), "upload");
+    cuda_check(cudaMemcpyAsync(dC, C, cols * cols * eb, cudaMemcpyHostToDevice, s), "upload");   // keeps the untouched triangle
+    lfd::LineView v{dA, 1, cols};
+    cuda_check(cudaEventRecord(e.e0, s), "event");
+    int method = 1;
+    exact_product(*la, bits, v, v, cols, cols, rows, dC, cols, subtract != 0, true, s, &method);
+    if (!lower_only) lfd::linalg_kernels(bits / 32)->mirror(dC, cols, cols, s);
+    cuda_check(cudaEventRecord(e.e1, s), "event");
+    cuda_check(cudaMemcpyAsync(C, dC, cols * cols * eb, cudaMemcpyDeviceToHost, s), "download");
+    cuda_check(cudaStreamSynchronize(s), "execution");
+    float ms = 0; cudaEventElapsedTime(&ms, e.e0, e.e1);
+    la->report.gpu_seconds = ms * 1e-3; la->report.gpu_outputs = cols * (cols + 1) / 2; la->report.method = method;
+    if (timing) *timing = {ms * 1e-3, since(w0)};
+    LF_API_END
+}
+
+}  // extern "C"
+
+namespace lfr {
+
+// Blocked right-looking Cholesky of the device matrix W (n x n, already holding A's lower triangle):
+// panels on the GPU (diagonal block, then the rows below), trailing updates as exact SYRK products
+// of one rounding per entry (linalg.mm:411-457 sequence).
+static lf_cholesky_info cholesky_device(Linalg& la, int bits, uint32_t* W, size_t n, size_t block) {
+    lf_cholesky_info info{};
+    info.pivot = n;
+    auto w0 = Clock::now();
+    Engine& e = *la.engine;
+    cudaStream_t s = e.stream;
+    const int limbs = bits / 32;
+    const size_t E = limbs + 3;
+    const auto* fk = lfd::factor_kernels(limbs);
+    const size_t nb = block ? std::min(block, n) : n;
+    long long* dinfo = static_cast<long long*>(la.info_buf.get(64));
+    uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));
+    cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
+    cudaEvent_t g0, g1;
+    cuda_check(cudaEventCreate(&g0), "event"); cuda_check(cudaEventCreate(&g1), "event");
+    cuda_check(cudaEventRecord(g0, s), "event");
+    size_t fail = n;
+    for (size_t k0 = 0; k0 < n && fail == n; k0 += nb) {
+        const size_t k1 = std::min(n, k0 + nb);
+        auto t = Clock::now();
+        long long init[3] = {(long long)n, 0, 0};
+        cuda_check(cudaMemcpyAsync(dinfo, init, sizeof init, cudaMemcpyHostToDevice, s), "info");
+        lfd::CholParams p{W, n, k0, k1, dinfo, err};
+        fk->diag(p, s);
+        long long got[3];
+        cuda_check(cudaMemcpyAsync(got, dinfo, sizeof got, cudaMemcpyDeviceToHost, s), "info");
+        cuda_check(cudaStreamSynchronize(s), "panel");
+        ++info.blocks;
+        if ((size_t)got[0] < n) {
+            fail = (size_t)got[0];
+            info.pivot = fail; info.pivot_sign = (int)got[1]; info.pivot_status = (uint32_t)got[2];
+            fk->rows(p, k1, fail, s);                   // rows below the block: columns [k0, fail)
+            cuda_check(cudaStreamSynchronize(s), "panel");
+            info.panel_seconds += since(t);
+            break;
+        }
+        fk->rows(p, k1, k1, s);
+        cuda_check(cudaGetLastError(), "panel launch");
+        cuda_check(cudaStreamSynchronize(s), "panel");
+        info.panel_seconds += since(t);
+        if (k1 < n) {
+            t = Clock::now();
+            const size_t m = n - k1;
+            lfd::LineView v{W + (k1 * n + k0) * E, n, 1};
+            exact_product(la, bits, v, v, m, m, k1 - k0, W + (k1 * n + k1) * E, n, true, true, s, nullptr);
+            ++info.gpu_updates;
+            info.update_seconds += since(t);
+        }
+    }
+    if (fail < n) fk->prep(nullptr, W, n, fail, s);
+    cuda_check(cudaEventRecord(g1, s), "event");
+    uint32_t ev = 0;
+    cuda_check(cudaMemcpyAsync(&ev, err, 4, cudaMemcpyDeviceToHost, s), "error flag");
+    cuda_check(cudaStreamSynchronize(s), "cholesky");
+    float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
+    cudaEventDestroy(g0); cudaEventDestroy(g1);
+    if (ev) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    info.timing = {ms * 1e-3, since(w0)};
+    return info;
+}
+
+// X (device, n x nrhs) holds B; passes 1 forward, 2 backward (L^T), 3 both (linalg.mm:459-488).
+static double solve_device(Linalg& la, int bits, const uint32_t* L, size_t n, uint32_t* X, size_t nrhs, size_t block, int passes) {
+    if (!n || !nrhs) return 0;
+    Engine& e = *la.engine;
+    cudaStream_t s = e.stream;
+    const int limbs = bits / 32;
+    const size_t E = limbs + 3;
+    const auto* fk = lfd::factor_kernels(limbs);
+    const size_t nb = block ? std::min(block, n) : n;
+    uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));
+    cudaEvent_t g0, g1;
+    cuda_check(cudaEventCreate(&g0), "event"); cuda_check(cudaEventCreate(&g1), "event");
+    cuda_check(cudaEventRecord(g0, s), "event");
+    if (passes & 1)
+        for (size_t r0 = 0; r0 < n; r0 += nb) {
+            const size_t r1 = std::min(n, r0 + nb);
+            cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
+            fk->solve(lfd::SolveParams{L, X, n, nrhs, r0, r1, 0, err}, true, s);
+            if (r1 < n) {
+                lfd::LineView lv{L + (r1 * n + r0) * E, n, 1};
+                lfd::LineView xv{X + r0 * nrhs * E, 1, nrhs};
+                exact_product(la, bits, lv, xv, n - r1, nrhs, r1 - r0, X + r1 * nrhs * E, nrhs, true, false, s, nullptr);
+            }
+        }
+    if (passes & 2)
+        for (size_t r0 = (n - 1) / nb * nb;; r0 -= nb) {
+            const size_t r1 = std::min(n, r0 + nb);
+            cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
+            fk->solve(lfd::SolveParams{L, X, n, nrhs, r0, r1, 0, err}, false, s);
+            if (r0) {
+                lfd::LineView lv{L + (r0 * n) * E, 1, n};           // line i: column i of L from row r0
+                lfd::LineView xv{X + r0 * nrhs * E, 1, nrhs};
+                exact_product(la, bits, lv, xv, r0, nrhs, r1 - r0, X, nrhs, true, false, s, nullptr);
+            }
+            if (!r0) break;
+        }
+    cuda_check(cudaEventRecord(g1, s), "event");
+    uint32_t ev = 0;
+    cuda_check(cudaMemcpyAsync(&ev, err, 4, cudaMemcpyDeviceToHost, s), "error flag");
+    cuda_check(cudaStreamSynchronize(s), "solve");
+    float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
+    cudaEventDestroy(g0); cudaEventDestroy(g1);
+    if (ev) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    return ms * 1e-3;
+}
+
+static bool overlap(const void* a, size_t na, const void* b, size_t nb) {
+    auto x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+    return na && nb && x < y + nb && y < x + na;
+}
+
+}  // namespace lfr
+
+extern "C" {
+
+// Linalg::cholesky (linalg.hpp:158): L may equal A; otherwise they must not overlap.
+int lf_linalg_cholesky(lf_linalg* la, int bits, const void* A, size_t n, void* L, const lf_factor_options* fo,
+                       lf_cholesky_info* out) {
+    LF_API_BEGIN
+    if (!la) throw invalid_argument("null linalg");
+    check_bits(bits);
+    validate_dims(n, n, n, n);
+    const size_t eb = size_t(bits / 8 + 12);
+    if (n && (!A || !L)) throw invalid_argument("null matrix");
+    if (A != L && overlap(A, n * n * eb, L, n * n * eb)) throw invalid_argument("cholesky: L overlaps A");
+    const size_t block = fo ? fo->block : 32;
+    lf_cholesky_info info{};
+    info.pivot = n;
+    if (n) {
+        Engine& e = *la->engine;
+        e.activate();
+        uint32_t* dA = static_cast<uint32_t*>(la->work[3].get(n * n * eb));
+        uint32_t* W = static_cast<uint32_t*>(la->work[4].get(n * n * eb));
+        auto w0 = Clock::now();
+        cuda_check(cudaMemcpyAsync(dA, A, n * n * eb, cudaMemcpyHostToDevice, e.stream), "upload");
+        lfd::factor_kernels(bits / 32)->prep(dA, W, n, n, e.stream);
+        info = cholesky_device(*la, bits, W, n, block);
+        cuda_check(cudaMemcpyAsync(L, W, n * n * eb, cudaMemcpyDeviceToHost, e.stream), "download");
+        cuda_check(cudaStreamSynchronize(e.stream), "download");
+        info.timing.wall_seconds = since(w0);
+    }
+    if (out) *out = info;
+    LF_API_END
+}
+
+static int solve_common(lf_linalg* la, int bits, int passes, const void* L, size_t n, const void* B, size_t nrhs, void* X,
+                        const lf_factor_options* fo, lf_timing* timing) {
+    LF_API_BEGIN
+    if (!la) throw invalid_argument("null linalg");
+    check_bits(bits);
+    validate_dims(n, nrhs, n, nrhs);
+    const size_t eb = size_t(bits / 8 + 12);
+    if (timing) *timing = {0, 0};
+    if (!n || !nrhs) return LF_OK;
+    if (!L || !B || !X) throw invalid_argument("null matrix");
+    if (X != B && (overlap(X, n * nrhs * eb, B, n * nrhs * eb) || overlap(X, n * nrhs * eb, L, n * n * eb)))
+        throw invalid_argument("trsm: X overlaps B or L");
+    Engine& e = *la->engine;
+    e.activate();
+    auto w0 = Clock::now();
+    uint32_t* dL = static_cast<uint32_t*>(la->work[3].get(n * n * eb));
+    uint32_t* dX = static_cast<uint32_t*>(la->work[5].get(n * nrhs * eb));
+    cuda_check(cudaMemcpyAsync(dL, L, n * n * eb, cudaMemcpyHostToDevice, e.stream), "upload");
+    cuda_check(cudaMemcpyAsync(dX, B, n * nrhs * eb, cudaMemcpyHostToDevice, e.stream), "upload");
+    const double g = solve_device(*la, bits, dL, n, dX, nrhs, fo ? fo->block : 32, passes);
+    cuda_check(cudaMemcpyAsync(X, dX, n * nrhs * eb, cudaMemcpyDeviceToHost, e.stream), "download");
+    cuda_check(cudaStreamSynchronize(e.stream), "download");
+    if (timing) *timing = {g, since(w0)};
+    LF_API_END
+}
+// Linalg::trsm (linalg.hpp:161): L X = B, or L^T X = B with transpose.
+int lf_linalg_trsm(lf_linalg* la, int bits, int transpose, const void* L, size_t n, const void* B, size_t nrhs, void* X,
+                   const lf_factor_options* fo, lf_timing* timing) {
+    return solve_common(la, bits, transpose ? 2 : 1, L, n, B, nrhs, X, fo, timing);
+}
+// Linalg::cholesky_solve (linalg.hpp:163): L L^T X = B.
+int lf_linalg_cholesky_solve(lf_linalg* la, int bits, const void* L, size_t n, const void* B, size_t nrhs, void* X,
+                             const lf_factor_options* fo, lf_timing* timing) {
+    return solve_common(la, bits, 3, L, n, B, nrhs, X, fo, timing);
+}
+
+// Device-pointer exact product for CUDA callers (no reference counterpart): C <- RN(C -/+ L R^T)
+// over line views (element (line, k) at base + (line * ls + k * ks) elements).
+int lf_dev_exact_product(lf_linalg* la, int bits, const void* left, size_t left_ls, size_t left_ks, const void* right,
+                         size_t right_ls, size_t right_ks, size_t M, size_t Nc, size_t K, void* C, size_t ldc, int subtract,
+                         int lower, void* stream) {
+    LF_API_BEGIN
+    if (!la) throw invalid_argument("null linalg");
+    check_bits(bits);
+    lfd::LineView lv{static_cast<const uint32_t*>(left), left_ls, left_ks}, rv{static_cast<const uint32_t*>(right), right_ls, right_ks};
+    int method = 1;
+    exact_product(*la, bits, lv, rv, M, Nc, K, static_cast<uint32_t*>(C), ldc, subtract != 0, lower != 0,
+                  stream ? static_cast<cudaStream_t>(stream) : la->engine->stream, &method);
+    la->report.method = method;
+    LF_API_END
+}
+
+}  // extern "C"

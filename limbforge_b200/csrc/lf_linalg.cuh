@@ -1,0 +1,367 @@
+// Exact dense products on the GPU: C[i][j] = RN(c_ij -/+ sum_k L(i,k) R(j,k)) with one rounding per
+// output (the contract of the reference's Linalg::gemm/syrk and exact_dot_add, linalg.hpp:1-7,
+// 268-318).  Operands are strided "line" views of AoS element matrices: element (line, k) of a view
+// sits at base + (line * ls + k * ks) elements.
+//
+// This file holds the per-line analysis and the generic limb kernel: one thread per output sums
+// the exact 2N-word limb products cluster by cluster (terms sorted implicitly by scanning for the
+// next-highest term; a new cluster starts where every remaining term lies more than
+// 32N + ceil(log2(count+1)) + 4 bits below the current cluster's lowest bit, linalg.hpp:269-273),
+// keeps the first nonzero cluster sum S exactly and only the sign of the next nonzero cluster, and
+// rounds S once.  It serves every input (any exponent spread, statuses, zeros) and is the plain
+// limb-kernel baseline of the residue/CRT engine (lf_residue.cu), which must match it bit for bit.
+#pragma once
+#include "lf_arith.cuh"
+#include <cuda_runtime.h>
+
+namespace lfd {
+
+struct LineView { const u32* base; u64 ls, ks; };
+struct LineInfo { u32 status; int top; int bottom; u32 nonzero; };
+
+// One warp per line: OR of statuses, largest and smallest exponent of the nonzero, status-free
+// entries (linalg.mm:82-112 pass 1).
+template <int N> __global__ void analyze_kernel(LineView v, u64 lines, u64 K, LineInfo* out) {
+    const u64 line = (u64)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    const int lane = threadIdx.x & 31;
+    if (line >= lines) return;
+    constexpr u64 E = N + 3;
+    u32 st = 0, nz = 0;
+    int top = INT_MIN, bottom = INT_MAX;
+    for (u64 k = lane; k < K; k += 32) {
+        const u32* p = v.base + (line * v.ls + k * v.ks) * E;
+        const u32 s = __ldg(p + N + 2);
+        const int sg = (int)__ldg(p + N + 1), e = (int)__ldg(p + N);
+        st |= s;
+        if (!s && sg) { nz += 1; top = max(top, e); bottom = min(bottom, e); }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        st |= __shfl_xor_sync(0xffffffffu, st, o);
+        nz += __shfl_xor_sync(0xffffffffu, nz, o);
+        top = max(top, __shfl_xor_sync(0xffffffffu, top, o));
+        bottom = min(bottom, __shfl_xor_sync(0xffffffffu, bottom, o));
+    }
+    if (!lane) out[line] = LineInfo{st, top, bottom, nz};
+}
+
+struct DotParams {
+    LineView left, right;
+    const LineInfo* linfo; const LineInfo* rinfo;
+    u32* C; u64 ldc;                 // output element (i, j) at C + (i * ldc + j) * E
+    u64 M, Nc, K;
+    u64 row0, col0;                  // output offsets of this launch (tiles of a larger product)
+    int subtract, lower;             // lower: only j <= i (global indices i = row0 + r, j = col0 + c)
+    u32* error;                      // set to 1 when a cluster exceeds the accumulator
+};
+
+constexpr int kClusterWords = 192;   // 6144-bit exact window per cluster (pos/neg magnitudes)
+
+// acc (len words) += t << off; t has tw words; acc wide enough (caller checks)
+__device__ __forceinline__ void acc_add(u32* acc, int len, const u32* t, int tw, i64 off) {
+    const int ws = (int)(off >> 5), bs = (int)(off & 31);
+    u64 cy = 0;
+    int k = ws;
+    for (int q = 0; q <= tw && k < len; ++q, ++k) {
+        u32 v = q < tw ? t[q] << bs : 0u;
+        if (bs && q > 0) v |= t[q - 1] >> (32 - bs);
+        u64 s = (u64)acc[k] + v + cy; acc[k] = (u32)s; cy = s >> 32;
+    }
+    for (; cy && k < len; ++k) { u64 s = (u64)acc[k] + cy; acc[k] = (u32)s; cy = s >> 32; }
+}
+
+// Rounding record of a nonzero exact magnitude: N result words, exponent, round and sticky bits.
+template <int N> struct Rounded { u32 m[N]; i64 e; bool rb, sb; };
+template <int N> __device__ bool round_info(const u32* x, int len, i64 scale, Rounded<N>& r) {
+    int t = -1;
+    for (int k = len - 1; k >= 0; --k) if (x[k]) { t = k; break; }
+    if (t < 0) return false;
+    const int h = 32 * t + 31 - __clz(x[t]);
+    r.e = scale + h;
+    const int shift = h - (32 * N - 1);
+    for (int i = 0; i < N; ++i) {
+        const int p = shift + 32 * i;
+        u32 v = 0;
+        if (p <= -32) v = 0;
+        else if (p < 0) v = x[0] << (-p);
+        else { const int wi = p >> 5, bi = p & 31; v = wi < len ? x[wi] >> bi : 0u; if (bi && wi + 1 < len) v |= x[wi + 1] << (32 - bi); }
+        r.m[i] = v;
+    }
+    r.rb = false; r.sb = false;
+    if (shift > 0) {
+        const int rbp = shift - 1;
+        r.rb = (x[rbp >> 5] >> (rbp & 31)) & 1u;
+        bool st = (rbp & 31) && (x[rbp >> 5] & ((1u << (rbp & 31)) - 1u));
+        for (int k = 0; k < (rbp >> 5) && !st; ++k) st = x[k] != 0;
+        r.sb = st;
+    }
+    return true;
+}
+
+// RN(c -/+ sum_{k<K} x[k*sx] y[k*sy]) with one rounding, c == nullptr a zero addend: the contract
+// of exact_dot_add (linalg.hpp:268-318).  Statuses: zero carrying the OR of c's and every x[k],
+// y[k] status; no nonzero product returns c itself (or zero).  `error` is set when one cluster
+// is wider than kClusterWords words (the result is then zero with status invalid).
+template <int N> __device__ Num<N> exact_dot_add_dev(const u32* cp, bool subtract, const u32* x, i64 sx, const u32* y, i64 sy,
+                                                     u64 K, u32* error) {
+    constexpr i64 E = N + 3;
+    const Num<N> c = cp ? load_plain<N>(cp) : zero<N>();
+    u32 st = c.st;
+    for (u64 k = 0; k < K; ++k) st |= __ldg(x + (i64)k * sx * E + N + 2) | __ldg(y + (i64)k * sy * E + N + 2);
+    if (st) return zero<N>(st);
+    // term k < K: product x_k y_k (< 2^(scale+64N)); k == K: the addend (< 2^(scale+32N))
+    auto term = [&](u64 k, i64& scale, i64& top, int& sign) -> bool {
+        if (k == K) {
+            if (!c.s) return false;
+            scale = (i64)c.e - (32 * N - 1); top = scale + 32 * N; sign = c.s;
+            return true;
+        }
+        const u32* a = x + (i64)k * sx * E; const u32* b = y + (i64)k * sy * E;
+        const int sa = (int)__ldg(a + N + 1), sb = (int)__ldg(b + N + 1);
+        if (!sa || !sb) return false;
+        scale = (i64)(int)__ldg(a + N) + (int)__ldg(b + N) - 2 * (32 * N - 1);
+        top = scale + 64 * N;
+        sign = subtract ? -sa * sb : sa * sb;
+        return true;
+    };
+    int count = 0, products = 0;
+    i64 T = INT64_MIN;
+    for (u64 k = 0; k <= K; ++k) {
+        i64 s, tp; int sg;
+        if (!term(k, s, tp, sg)) continue;
+        T = tp > T ? tp : T;
+        ++count; products += k < K;
+    }
+    if (!products) return cp ? c : zero<N>();
+    int logc = 0;
+    while ((1 << logc) < count + 1) ++logc;
+    const i64 gap = 32 * N + logc + 4;
+    u32 pos[kClusterWords], neg[kClusterWords];
+    i64 cutoff = T;                        // inclusive bound on the tops still to visit
+    bool have = false;
+    Rounded<N> R; int rsign = 0, sigma = 0;
+    for (;;) {
+        i64 Tc = INT64_MIN;                // top of the next cluster
+        for (u64 k = 0; k <= K; ++k) {
+            i64 s, tp; int sg;
+            if (term(k, s, tp, sg) && tp <= cutoff && tp > Tc) Tc = tp;
+        }
+        if (Tc == INT64_MIN) break;
+        i64 low = INT64_MAX;               // lowest bit: grow while a remaining term reaches within `gap`
+        for (u64 k = 0; k <= K; ++k) {
+            i64 s, tp; int sg;
+            if (term(k, s, tp, sg) && tp == Tc && s < low) low = s;
+        }
+        for (;;) {
+            i64 nl = low;
+            for (u64 k = 0; k <= K; ++k) {
+                i64 s, tp; int sg;
+                if (term(k, s, tp, sg) && tp <= cutoff && tp > low - gap && s < nl) nl = s;
+            }
+            if (nl == low) break;
+            low = nl;
+        }
+        const int len = (int)((Tc - low + logc + 2 + 31) / 32) + 1;
+        if (len > kClusterWords) { if (error) atomicExch(error, 1u); return zero<N>(kInvalid); }
+        for (int w = 0; w < len; ++w) { pos[w] = 0; neg[w] = 0; }
+        for (u64 k = 0; k <= K; ++k) {
+            i64 s, tp; int sg;
+            if (!term(k, s, tp, sg) || !(tp <= cutoff && tp > low - gap)) continue;
+            if (k == K) acc_add(sg > 0 ? pos : neg, len, c.m, N, s - low);
+            else {
+                const Num<N> a = load<N>(x + (i64)k * sx * E), b = load<N>(y + (i64)k * sy * E);
+                u32 prod[2 * N];
+                mant_mul<N>(a.m, b.m, prod);
+                acc_add(sg > 0 ? pos : neg, len, prod, 2 * N, s - low);
+            }
+        }
+        cutoff = low - gap;
+        int cmp = 0;
+        for (int w = len - 1; w >= 0 && !cmp; --w) if (pos[w] != neg[w]) cmp = pos[w] > neg[w] ? 1 : -1;
+        if (!cmp) continue;                // the cluster cancels exactly
+        u32* big = cmp > 0 ? pos : neg;
+        const u32* small = cmp > 0 ? neg : pos;
+        u32 bo = 0;
+        for (int w = 0; w < len; ++w) { u64 d = (u64)small[w] + bo; u32 o = big[w]; big[w] = (u32)((u64)o - d); bo = (u64)o < d; }
+        if (!have) { round_info<N>(big, len, low, R); rsign = cmp; have = true; continue; }
+        sigma = cmp == rsign ? 1 : -1;     // sign of everything below, relative to S
+        break;
+    }
+    if (!have) return zero<N>();
+    // RN(S + sigma * tiny): the tail decides only exact ties and exact S
+    const bool up = R.rb && (R.sb || sigma > 0 || (sigma == 0 && (R.m[0] & 1u)));
+    return finish<N>(R.m, R.e, rsign, up, 0);
+}
+
+template <int N> __global__ void __launch_bounds__(128) exact_dot_kernel(DotParams p) {
+    const u64 r = (u64)blockIdx.y * blockDim.y + threadIdx.y;
+    const u64 q = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= p.M || q >= p.Nc) return;
+    const u64 i = p.row0 + r, j = p.col0 + q;
+    if (p.lower && j > i) return;
+    constexpr u64 E = N + 3;
+    u32* out = p.C + (r * p.ldc + q) * E;
+    const Num<N> v = exact_dot_add_dev<N>(p.subtract ? out : nullptr, p.subtract, p.left.base + i * p.left.ls * E, (i64)p.left.ks,
+                                          p.right.base + j * p.right.ls * E, (i64)p.right.ks, p.K, p.error);
+    store<N>(out, v);
+}
+
+// Lower triangle mirrored into the upper one (full SYRK output).
+template <int N> __global__ void mirror_kernel(u32* C, u64 n, u64 ldc) {
+    const u64 i = (u64)blockIdx.y * blockDim.y + threadIdx.y, j = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || j >= n || j <= i) return;
+    constexpr u64 E = N + 3;
+    const u32* src = C + (j * ldc + i) * E;
+    u32* dst = C + (i * ldc + j) * E;
+    for (int w = 0; w < (int)E; ++w) dst[w] = src[w];
+}
+
+typedef void (*AnalyzeFn)(LineView, u64, u64, LineInfo*, cudaStream_t);
+typedef void (*DotFn)(const DotParams&, cudaStream_t);
+typedef void (*MirrorFn)(u32*, u64, u64, cudaStream_t);
+struct LinalgKernels { AnalyzeFn analyze; DotFn dot; MirrorFn mirror; };
+const LinalgKernels* linalg_kernels(int limbs);
+
+template <int N> void analyze_launch(LineView v, u64 lines, u64 K, LineInfo* out, cudaStream_t s) {
+    if (!lines) return;
+    analyze_kernel<N><<<(unsigned)((lines + 3) / 4), 128, 0, s>>>(v, lines, K, out);
+}
+template <int N> void dot_launch(const DotParams& p, cudaStream_t s) {
+    if (!p.M || !p.Nc) return;
+    dim3 block(32, 4), grid((unsigned)((p.Nc + 31) / 32), (unsigned)((p.M + 3) / 4));
+    exact_dot_kernel<N><<<grid, block, 0, s>>>(p);
+}
+template <int N> void mirror_launch(u32* C, u64 n, u64 ldc, cudaStream_t s) {
+    if (n < 2) return;
+    dim3 block(32, 4), grid((unsigned)((n + 31) / 32), (unsigned)((n + 3) / 4));
+    mirror_kernel<N><<<grid, block, 0, s>>>(C, n, ldc);
+}
+
+}  // namespace lfd
+
+#define LF_LINALG_INSTANTIATE(N)                                                                      \
+    namespace lfd {                                                                                   \
+    extern const LinalgKernels linalg_kernels_##N; const LinalgKernels linalg_kernels_##N = {analyze_launch<N>, dot_launch<N>, mirror_launch<N>};    \
+    }
+
+namespace lfd {
+
+// ---------------------------------------------------------------- blocked Cholesky pieces
+// W: n x n row-major work matrix (element stride E).  D(c; x, y; K) = exact_dot_add_dev(c, subtract).
+struct CholParams { u32* W; u64 n, k0, k1; long long* info; u32* error; };
+
+// Diagonal block [k0, k1) column by column: s_jj = D(w_jj; row j [k0,j)), l_jj = sqrt(s_jj) (or the
+// failing pivot recorded in info = {pivot, sign, status}); l_ij = RN(D(w_ij; row i, row j; [k0,j)) / l_jj)
+// for the block rows i > j.  The same formulas in the same dependency order as the row-by-row host
+// panel of linalg.mm:418-430, so every entry gets identical bits.
+template <int N> __global__ void chol_diag_kernel(CholParams p) {
+    constexpr u64 E = N + 3;
+    __shared__ int failed;
+    if (!threadIdx.x) failed = 0;
+    __syncthreads();
+    for (u64 j = p.k0; j < p.k1; ++j) {
+        u32* wjj = p.W + (j * p.n + j) * E;
+        if (!threadIdx.x) {
+            const Num<N> s = exact_dot_add_dev<N>(wjj, true, p.W + (j * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
+            if (s.st || s.s <= 0) { p.info[0] = (long long)j; p.info[1] = s.st ? 0 : s.s; p.info[2] = s.st; failed = 1; }
+            else store<N>(wjj, lfd::sqrt<N>(s));
+        }
+        __syncthreads();
+        if (failed) return;
+        const Num<N> d = load_plain<N>(wjj);
+        for (u64 i = j + 1 + threadIdx.x; i < p.k1; i += blockDim.x) {
+            u32* wij = p.W + (i * p.n + j) * E;
+            const Num<N> v = exact_dot_add_dev<N>(wij, true, p.W + (i * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
+            store<N>(wij, div<N>(v, d));
+        }
+        __syncthreads();
+    }
+}
+// Rows i in [r0, n) below the diagonal block: l_ij = RN(D(w_ij; row i, row j; [k0,j)) / l_jj) for
+// j in [k0, jend), left to right (jend = the failing pivot, or k1).  One thread per row.
+template <int N> __global__ void chol_rows_kernel(CholParams p, u64 r0, u64 jend) {
+    constexpr u64 E = N + 3;
+    const u64 i = r0 + (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    for (u64 j = p.k0; j < jend; ++j) {
+        u32* wij = p.W + (i * p.n + j) * E;
+        const Num<N> v = exact_dot_add_dev<N>(wij, true, p.W + (i * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
+        store<N>(wij, div<N>(v, load_plain<N>(p.W + (j * p.n + j) * E)));
+    }
+}
+// W = lower triangle of A (upper zero); after a failure at pivot p: entries (i, j), p <= j <= i, are
+// zero with status invalid.
+template <int N> __global__ void chol_prepare_kernel(const u32* A, u32* W, u64 n, u64 fail) {
+    constexpr u64 E = N + 3;
+    const u64 i = (u64)blockIdx.y * blockDim.y + threadIdx.y, j = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || j >= n) return;
+    u32* w = W + (i * n + j) * E;
+    if (fail < n) {
+        if (j >= fail && j <= i) store<N>(w, zero<N>(kInvalid));
+        return;
+    }
+    if (j > i) store<N>(w, zero<N>());
+    else if (A != W) { const u32* a = A + (i * n + j) * E; for (int q = 0; q < (int)E; ++q) w[q] = a[q]; }
+}
+
+// ---------------------------------------------------------------- triangular solves (linalg.mm:459-488)
+// X: n x nrhs, L: n x n lower.  Forward block [r0, r1): x_i = RN(D(x_i; l_i[r0,i), x[r0,i)) / l_ii),
+// i ascending; backward block: x_i = RN(D(x_i; column i of L below i within (i, r1), x(i, r1)) / l_ii),
+// i descending (upper: R = L^T stored by rows).  One thread per right-hand side.
+struct SolveParams { const u32* L; u32* X; u64 n, nrhs, r0, r1; int upper; u32* error; };
+template <int N> __global__ void solve_forward_kernel(SolveParams p) {
+    constexpr u64 E = N + 3;
+    const u64 c = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= p.nrhs) return;
+    for (u64 i = p.r0; i < p.r1; ++i) {
+        u32* x = p.X + (i * p.nrhs + c) * E;
+        const Num<N> v = exact_dot_add_dev<N>(x, true, p.L + (i * p.n + p.r0) * E, 1, p.X + (p.r0 * p.nrhs + c) * E, (i64)p.nrhs, i - p.r0, p.error);
+        store<N>(x, div<N>(v, load<N>(p.L + (i * p.n + i) * E)));
+    }
+}
+template <int N> __global__ void solve_backward_kernel(SolveParams p) {
+    constexpr u64 E = N + 3;
+    const u64 c = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= p.nrhs) return;
+    for (u64 i = p.r1; i-- > p.r0;) {
+        u32* x = p.X + (i * p.nrhs + c) * E;
+        Num<N> v = load_plain<N>(x);
+        if (i + 1 < p.r1) {
+            const u32* col = p.upper ? p.L + (i * p.n + i + 1) * E : p.L + ((i + 1) * p.n + i) * E;
+            v = exact_dot_add_dev<N>(x, true, col, p.upper ? 1 : (i64)p.n, p.X + ((i + 1) * p.nrhs + c) * E, (i64)p.nrhs, p.r1 - i - 1, p.error);
+        }
+        store<N>(x, div<N>(v, load<N>(p.L + (i * p.n + i) * E)));
+    }
+}
+
+typedef void (*CholDiagFn)(const CholParams&, cudaStream_t);
+typedef void (*CholRowsFn)(const CholParams&, u64, u64, cudaStream_t);
+typedef void (*CholPrepFn)(const u32*, u32*, u64, u64, cudaStream_t);
+typedef void (*SolveFn)(const SolveParams&, bool, cudaStream_t);
+struct FactorKernels { CholDiagFn diag; CholRowsFn rows; CholPrepFn prep; SolveFn solve; };
+const FactorKernels* factor_kernels(int limbs);
+
+template <int N> void chol_diag_launch(const CholParams& p, cudaStream_t s) { chol_diag_kernel<N><<<1, 128, 0, s>>>(p); }
+template <int N> void chol_rows_launch(const CholParams& p, u64 r0, u64 jend, cudaStream_t s) {
+    if (r0 >= p.n || jend <= p.k0) return;
+    const u64 rows = p.n - r0;
+    chol_rows_kernel<N><<<(unsigned)((rows + 63) / 64), 64, 0, s>>>(p, r0, jend);
+}
+template <int N> void chol_prep_launch(const u32* A, u32* W, u64 n, u64 fail, cudaStream_t s) {
+    if (!n) return;
+    dim3 block(32, 4), grid((unsigned)((n + 31) / 32), (unsigned)((n + 3) / 4));
+    chol_prepare_kernel<N><<<grid, block, 0, s>>>(A, W, n, fail);
+}
+template <int N> void solve_launch(const SolveParams& p, bool forward, cudaStream_t s) {
+    if (!p.nrhs || p.r1 <= p.r0) return;
+    const unsigned blocks = (unsigned)((p.nrhs + 63) / 64);
+    if (forward) solve_forward_kernel<N><<<blocks, 64, 0, s>>>(p);
+    else solve_backward_kernel<N><<<blocks, 64, 0, s>>>(p);
+}
+
+}  // namespace lfd
+
+#define LF_FACTOR_INSTANTIATE(N)                                                                               \
+    namespace lfd {                                                                                            \
+    extern const FactorKernels factor_kernels_##N; const FactorKernels factor_kernels_##N = {chol_diag_launch<N>, chol_rows_launch<N>, chol_prep_launch<N>, solve_launch<N>}; \
+    }

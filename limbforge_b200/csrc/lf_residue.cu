@@ -1,0 +1,189 @@
+// Host driver of the int8-residue / CRT exact product engine (kernels in lf_residue.cuh).
+//
+// Domain: every nonzero, status-free line of each side fits one exponent band of width
+// G <= kMaxBand bits (G = the widest such line's exponent spread) and K <= kMaxK.  Outside it the
+// caller runs the generic limb kernel, which gives the same bits.
+//
+// Moduli: primes <= 65279, descending (as the reference, linalg.mm:39-40: a balanced residue
+// |r| <= 32639 then splits into two int8 digits); L is the smallest count whose product exceeds
+// 2^(2(32N+G) + ceil(log2 K) + 3) > 4 K max|entry|^2, so the signed CRT value and the rounding of
+// the fixed-point quotient are both unambiguous.
+#include "lf_residue.h"
+#define LF_RESIDUE_MMA_KERNEL
+#include "lf_residue.cuh"
+
+#include <cuda.h>
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <vector>
+
+namespace lfr {
+
+namespace {
+constexpr int kMaxBand = 192;
+constexpr uint64_t kMaxK = 65472;
+
+const std::vector<uint32_t>& primes() {
+    static const std::vector<uint32_t> p = [] {
+        std::vector<uint32_t> r;
+        for (uint32_t q = 65279; r.size() < (size_t)lfd::kResMaxModuli; --q) {
+            bool prime = q > 1;
+            for (uint32_t d = 2; d * d <= q && prime; ++d) prime = q % d != 0;
+            if (prime) r.push_back(q);
+        }
+        return r;
+    }();
+    return p;
+}
+uint32_t inverse_mod(uint64_t a, uint64_t m) {                // extended Euclid
+    int64_t t = 0, nt = 1, r = (int64_t)m, nr = (int64_t)(a % m);
+    while (nr) { int64_t q = r / nr, x = t - q * nt; t = nt; nt = x; x = r - q * nr; r = nr; nr = x; }
+    return (uint32_t)(t < 0 ? t + (int64_t)m : t);
+}
+// Multiword helpers for the host-side tables.
+void mul_small(std::vector<uint32_t>& x, uint32_t m) {
+    uint64_t c = 0;
+    for (auto& w : x) { uint64_t t = (uint64_t)w * m + c; w = (uint32_t)t; c = t >> 32; }
+    if (c) x.push_back((uint32_t)c);
+}
+uint32_t mod_small(const std::vector<uint32_t>& x, uint32_t m) {
+    uint64_t r = 0;
+    for (size_t i = x.size(); i-- > 0;) r = ((r << 32) | x[i]) % m;
+    return (uint32_t)r;
+}
+
+struct TableSet { lfd::ResTables* dev = nullptr; int L = 0, qwords = 0; };
+std::mutex g_table_mutex;
+std::map<std::pair<int, int>, TableSet> g_tables;            // (device, L)
+
+TableSet tables_for(int device, int L) {
+    std::lock_guard<std::mutex> lock(g_table_mutex);
+    auto key = std::make_pair(device, L);
+    auto it = g_tables.find(key);
+    if (it != g_tables.end()) return it->second;
+    auto* h = new lfd::ResTables();
+    const auto& m = primes();
+    std::vector<uint32_t> M{1};
+    for (int l = 0; l < L; ++l) mul_small(M, m[l]);
+    int qwords = 0;
+    for (int l = 0; l < L; ++l) {
+        h->m[l] = m[l];
+        h->barrett[l] = ~0ull / m[l] + ((~0ull % m[l]) + 1 == m[l] ? 1 : 0);   // floor(2^64 / m)
+        h->frac[l] = (1ull << 48) / m[l];
+        std::vector<uint32_t> q{1};
+        for (int t = 0; t < L; ++t) if (t != l) mul_small(q, m[t]);
+        if ((int)q.size() > lfd::kResMaxQWords) throw runtime_error("residue engine: modulus table too large");
+        qwords = std::max(qwords, (int)q.size());
+        for (size_t w = 0; w < q.size(); ++w) h->q[l][w] = q[w];
+        h->w[l] = inverse_mod(mod_small(q, m[l]), m[l]);
+        uint64_t pw = 1;
+        for (int w = 0; w < 40; ++w) { h->pw[l][w] = (uint32_t)pw; pw = (pw << 32) % m[l]; }
+    }
+    if ((int)M.size() > lfd::kResMaxQWords + 1) throw runtime_error("residue engine: modulus product too large");
+    for (size_t w = 0; w < M.size(); ++w) h->M[w] = M[w];
+    TableSet t;
+    t.L = L; t.qwords = std::max(qwords, (int)M.size() - 1);
+    cuda_check(cudaMalloc(&t.dev, sizeof(lfd::ResTables)), "residue tables");
+    cuda_check(cudaMemcpy(t.dev, h, sizeof(lfd::ResTables), cudaMemcpyHostToDevice), "residue tables");
+    delete h;
+    g_tables[key] = t;
+    return t;
+}
+
+typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                                const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encoder() {
+    static EncodeTiled fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<EncodeTiled>(f);
+    }();
+    if (!fn) throw runtime_error("cuTensorMapEncodeTiled unavailable");
+    return fn;
+}
+// [L][rows_pad][Kp] int8 planes, 128 x 128 boxes with the 128-byte swizzle.
+CUtensorMap plane_map(void* base, uint64_t Kp, uint64_t rows_pad, int L) {
+    CUtensorMap map;
+    const cuuint64_t dims[3] = {Kp, rows_pad, (cuuint64_t)L};
+    const cuuint64_t strides[2] = {Kp, rows_pad * Kp};
+    const cuuint32_t box[3] = {lfd::kTileK, lfd::kTileM, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw runtime_error("cuTensorMapEncodeTiled failed");
+    return map;
+}
+}  // namespace
+
+bool ResidueEngine::run(int bits, lfd::LineView left, lfd::LineView right, uint64_t M, uint64_t Nc, uint64_t K, uint32_t* C,
+                        uint64_t ldc, bool subtract, bool lower, uint32_t* error, cudaStream_t s, bool forced,
+                        lf_linalg_report& report) {
+    const int n = bits / 32;
+    auto refuse = [&](const char* why) -> bool {
+        if (forced) throw runtime_error(std::string("residue engine: ") + why);
+        return false;
+    };
+    if (!K) return refuse("empty inner dimension");
+    if (K > kMaxK) return refuse("inner dimension above 65472");
+    const bool same = left.base == right.base && left.ls == right.ls && left.ks == right.ks && M == Nc;
+    const auto* lk = lfd::linalg_kernels(n);
+    const auto* rk = lfd::residue_kernels(n);
+    auto* linfo = static_cast<lfd::LineInfo*>(lines.get(sizeof(lfd::LineInfo) * (M + Nc) + 64));
+    auto* rinfo = same ? linfo : linfo + M;
+    lk->analyze(left, M, K, linfo, s);
+    if (!same) lk->analyze(right, Nc, K, rinfo, s);
+    std::vector<lfd::LineInfo> h(M + (same ? 0 : Nc));
+    cuda_check(cudaMemcpyAsync(h.data(), linfo, sizeof(lfd::LineInfo) * h.size(), cudaMemcpyDeviceToHost, s), "line info");
+    cuda_check(cudaStreamSynchronize(s), "line analysis");
+    int G = 0;
+    bool any = false;
+    for (const auto& li : h) if (!li.status && li.nonzero) { G = std::max(G, li.top - li.bottom); any = true; }
+    if (!any) return refuse("no nonzero lines");
+    if (G > kMaxBand) return refuse("a line spans more than 192 exponent bits");
+    const int P = 32 * n + G;
+    int logk = 0;
+    while ((1ull << logk) < K) ++logk;
+    const double need = 2.0 * P + logk + 3;
+    double have = 0;
+    int L = 0;
+    while (have <= need) {
+        if (L >= lfd::kResMaxModuli) return refuse("modulus count above the table limit");
+        have += std::log2((double)primes()[L++]);
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    TableSet tab = tables_for(dev, L);
+    const uint64_t Kp = (K + lfd::kTileK - 1) / lfd::kTileK * lfd::kTileK;
+    const uint64_t Mp = (M + lfd::kTileM - 1) / lfd::kTileM * lfd::kTileM, Np = (Nc + lfd::kTileN - 1) / lfd::kTileN * lfd::kTileN;
+    const uint64_t aplane = (uint64_t)L * Mp * Kp, bplane = same ? 0 : (uint64_t)L * Np * Kp;
+    auto* pl = static_cast<signed char*>(planes.get(2 * (aplane + bplane) + 256));
+    signed char *a1 = pl, *a0 = pl + aplane, *b1 = same ? a1 : pl + 2 * aplane, *b0 = same ? a0 : pl + 2 * aplane + bplane;
+    auto* res = static_cast<uint16_t*>(residues.get(sizeof(uint16_t) * (uint64_t)L * M * Nc + 64));
+    const int xwords = n + (G + 31) / 32 + 1;
+    rk->digits(lfd::DigitParams{left, M, K, Kp, Mp, L, xwords, linfo, tab.dev, a1, a0}, s);
+    if (!same) rk->digits(lfd::DigitParams{right, Nc, K, Kp, Np, L, xwords, rinfo, tab.dev, b1, b0}, s);
+    cuda_check(cudaGetLastError(), "digit planes");
+    const CUtensorMap ta1 = plane_map(a1, Kp, Mp, L), ta0 = plane_map(a0, Kp, Mp, L);
+    const CUtensorMap tb1 = plane_map(b1, Kp, same ? Mp : Np, L), tb0 = plane_map(b0, Kp, same ? Mp : Np, L);
+    const size_t smem = lfd::kStages * lfd::kStageBytes + 1024;
+    cuda_check(cudaFuncSetAttribute(lfd::residue_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem");
+    lfd::MmaParams mp{res, tab.dev, M, Nc, Kp, lower ? 1 : 0, error};
+    dim3 grid((unsigned)(Np / lfd::kTileN), (unsigned)(Mp / lfd::kTileM), (unsigned)L);
+    lfd::residue_mma_kernel<<<grid, 128, smem, s>>>(ta1, ta0, tb1, tb0, mp);
+    cuda_check(cudaGetLastError(), "residue products");
+    rk->rec(lfd::RecParams{res, tab.dev, L, tab.qwords, linfo, rinfo, C, ldc, M, Nc, subtract ? 1 : 0, lower ? 1 : 0}, s);
+    cuda_check(cudaGetLastError(), "reconstruction");
+    report.moduli = (size_t)L;
+    report.band_bits = (size_t)G;
+    report.int8_gemms = 4 * (size_t)L;
+    report.gemm_rows = M;
+    report.gemm_cols = Nc;
+    return true;
+}
+
+}  // namespace lfr

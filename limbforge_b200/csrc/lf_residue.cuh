@@ -1,0 +1,369 @@
+// Int8-residue / CRT exact products (the reference's plan D6, linalg.mm:305-404 and
+// linalg.metal:23-152, redesigned for sm_100a):
+//
+//  1. digits: every entry of a line becomes the exact integer X = mantissa * 2^(e - bottom(line))
+//     (< 2^(32N+G), G = widest line spread), reduced modulo L primes m_l < 2^16 to a balanced
+//     residue r = 256 d1 + d0 with int8 digits; planes D1/D0 [L][rows][Kp] (K-major, zero padded).
+//  2. mma: per modulus and 128x128 output tile, tcgen05.mma kind::i8 with int32 accumulators in
+//     TMEM: S11 = D1a D1b^T, S00 = D0a D0b^T, Smid = D1a D0b^T + D0a D1b^T; operands fed by TMA
+//     (128-byte swizzle, no multicast); epilogue r = (65536 S11 + 256 Smid + S00) mod m -> uint16.
+//  3. reconstruct: per output, CRT of the L residues (X = sum_l t_l (M/m_l) - q M, q = round of the
+//     fixed-point sum of t_l/m_l; the modulus product exceeds 4 max|X| so the rounding of q is never
+//     close), then RN(c - X 2^scale) (or RN(X 2^scale)) with one rounding.
+// Every step is exact integer arithmetic, so the outputs equal the generic limb kernel's bit for bit.
+#pragma once
+#include "lf_linalg.cuh"
+#include <cuda.h>
+
+namespace lfd {
+
+constexpr int kResMaxModuli = 160;
+constexpr int kResMaxQWords = 80;          // words of M / m_l
+struct ResTables {
+    u32 m[kResMaxModuli];                  // moduli, descending primes < 2^16
+    u64 barrett[kResMaxModuli];            // floor(2^64 / m)
+    u32 w[kResMaxModuli];                  // (M / m_l)^{-1} mod m_l
+    u64 frac[kResMaxModuli];               // floor(2^48 / m_l)
+    u32 q[kResMaxModuli][kResMaxQWords];   // M / m_l, little-endian words
+    u32 M[kResMaxQWords + 1];              // product of the moduli
+    u32 pw[kResMaxModuli][40];             // 2^(32 w) mod m_l for the integer words (<= 40)
+};
+
+__device__ __forceinline__ u32 mod_barrett(u64 x, u32 m, u64 r) {
+    u64 q = __umul64hi(x, r);
+    u64 t = x - q * m;
+    while (t >= m) t -= m;                 // at most twice
+    return (u32)t;
+}
+
+// ---------------------------------------------------------------- 1. digit planes
+struct DigitParams {
+    LineView v; u64 lines, K, Kp, rows_pad; int L; int xwords;
+    const LineInfo* info; const ResTables* tab;
+    signed char* d1; signed char* d0;      // [L][rows_pad][Kp]
+};
+template <int N> __global__ void __launch_bounds__(128) digits_kernel(DigitParams p) {
+    const u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 line = blockIdx.y;                          // rows_pad lines: padding rows are zero
+    if (k >= p.Kp || line >= p.rows_pad) return;
+    u32 x[40];
+    for (int w = 0; w < 40; ++w) x[w] = 0;
+    bool nz = false, negative = false;
+    if (k < p.K && line < p.lines) {
+        const Num<N> a = load<N>(p.v.base + (line * p.v.ls + k * p.v.ks) * (u64)(N + 3));
+        if (!a.st && a.s) {
+            nz = true; negative = a.s < 0;
+            const int sh = a.e - p.info[line].bottom;       // 0 <= sh <= G
+            const int ws = sh >> 5, bs = sh & 31;
+            for (int i = 0; i <= N; ++i) {
+                u32 v = i < N ? a.m[i] << bs : 0u;
+                if (bs && i > 0) v |= a.m[i - 1] >> (32 - bs);
+                x[i + ws] = v;
+            }
+        }
+    }
+    const u64 plane = p.rows_pad * p.Kp;
+    for (int l = 0; l < p.L; ++l) {
+        int r = 0;
+        if (nz) {
+            const u32 m = p.tab->m[l];
+            u64 acc = 0;
+            for (int w = 0; w < p.xwords; ++w) acc += (u64)x[w] * p.tab->pw[l][w];     // < 2^54
+            u32 u = mod_barrett(acc, m, p.tab->barrett[l]);
+            if (negative && u) u = m - u;                     // residue of -X
+            r = (int)u;
+            if (r > (int)(m >> 1)) r -= (int)m;               // balanced: |r| <= (m-1)/2 <= 32639
+        }
+        const int lo = (int)(signed char)(r & 0xff);
+        const int hi = (r - lo) >> 8;                         // in [-128, 127] because m <= 65279
+        p.d1[l * plane + line * p.Kp + k] = (signed char)hi;
+        p.d0[l * plane + line * p.Kp + k] = (signed char)lo;
+    }
+}
+
+// ---------------------------------------------------------------- 2. tcgen05 residue products
+constexpr int kTileM = 128, kTileN = 128, kTileK = 128;      // K tile in int8 elements = one 128-byte row
+constexpr int kStages = 2;
+constexpr int kTileBytes = kTileM * kTileK;                   // 16 KB per operand tile
+constexpr int kStageBytes = 4 * kTileBytes;                   // D1a, D0a, D1b, D0b
+constexpr u32 kSpinLimit = 1u << 28;                          // bounded mbarrier waits
+
+struct MmaParams {
+    u16* res;                               // [L][M][Nc] residues (0 <= r < m)
+    const ResTables* tab;
+    u64 M, Nc, Kp;
+    int lower;                              // skip tiles strictly above the diagonal (SYRK)
+    u32* error;
+};
+
+__device__ __forceinline__ u32 smem_u32(const void* p) { return (u32)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(u64* bar, u32 count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(u64* bar, u32 bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(u64* bar, u32 phase) {
+    u32 ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(phase) : "memory");
+    return ok != 0;
+}
+// Bounded wait: false (and the error flag set) when the barrier never completes.
+__device__ __forceinline__ bool mbar_wait(u64* bar, u32 phase, u32* error) {
+    for (u32 it = 0; it < kSpinLimit; ++it)
+        if (mbar_try_wait(bar, phase)) return true;
+    atomicExch(error, 2u);
+    return false;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u64* bar, int c0, int c1, int c2) {
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+                 :: "r"(smem_u32(dst)), "l"((u64)map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2) : "memory");
+}
+// K-major operand in 128-byte-swizzled 8-row atoms (1024 B): LBO 16 B, SBO 1024 B, layout SWIZZLE_128B.
+__device__ __forceinline__ u64 smem_desc(const void* p) {
+    const u64 start = (smem_u32(p) >> 4) & 0x3FFFu;
+    return start | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+// kind::i8: D s32, A s8, B s8, both K-major, M = 128, N = 128.
+constexpr u32 kIdesc = (2u << 4) | (1u << 7) | (1u << 10) | ((u32)(kTileN >> 3) << 17) | ((u32)(kTileM >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8(u32 d_tmem, u64 a, u64 b, bool accumulate) {
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+                 :: "r"(d_tmem), "l"(a), "l"(b), "r"(kIdesc), "r"((u32)accumulate), "r"(0u));
+}
+__device__ __forceinline__ void mma_commit(u64* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(u32 taddr, u32 (&r)[32]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                 "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+                   "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+                   "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+}
+
+#ifdef LF_RESIDUE_MMA_KERNEL
+// One CTA = one 128 x 128 output tile of one modulus (grid z).  Warp 0 lane 0 issues TMA loads,
+// warp 1 lane 0 issues the MMAs; all four warps then read their 32 TMEM lanes (rows).
+__global__ void __launch_bounds__(128, 1) residue_mma_kernel(const __grid_constant__ CUtensorMap ta1, const __grid_constant__ CUtensorMap ta0,
+                                                              const __grid_constant__ CUtensorMap tb1, const __grid_constant__ CUtensorMap tb0,
+                                                              MmaParams p) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    __shared__ __align__(8) u64 full[kStages], empty[kStages], done;
+    __shared__ u32 tmem_slot;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tm = blockIdx.y, tn = blockIdx.x, l = blockIdx.z;
+    if (p.lower && (u64)tn * kTileN > (u64)tm * kTileM + kTileM - 1) return;      // whole tile above the diagonal
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        mbar_init(&done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" :: "r"(smem_u32(&tmem_slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const u32 tmem = tmem_slot;
+    const u32 acc11 = tmem, acc00 = tmem + kTileN, accm = tmem + 2 * kTileN;
+    const int kblocks = (int)(p.Kp / kTileK);
+    __shared__ int abort_flag;
+    if (threadIdx.x == 0) abort_flag = 0;
+    __syncthreads();
+    if (warp == 0 && lane == 0) {
+        // producer
+        for (int kb = 0; kb < kblocks; ++kb) {
+            const int s = kb % kStages;
+            const u32 ph = (u32)((kb / kStages) & 1);
+            if (kb >= kStages && !mbar_wait(&empty[s], ph ^ 1u, p.error)) { abort_flag = 1; break; }
+            unsigned char* st = smem + s * kStageBytes;
+            mbar_expect_tx(&full[s], kStageBytes);
+            tma_load_3d(st, &ta1, &full[s], kb * kTileK, tm * kTileM, l);
+            tma_load_3d(st + kTileBytes, &ta0, &full[s], kb * kTileK, tm * kTileM, l);
+            tma_load_3d(st + 2 * kTileBytes, &tb1, &full[s], kb * kTileK, tn * kTileN, l);
+            tma_load_3d(st + 3 * kTileBytes, &tb0, &full[s], kb * kTileK, tn * kTileN, l);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        bool ok = true;
+        for (int kb = 0; kb < kblocks && ok; ++kb) {
+            const int s = kb % kStages;
+            const u32 ph = (u32)((kb / kStages) & 1);
+            if (!mbar_wait(&full[s], ph, p.error)) { ok = false; abort_flag = 1; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            unsigned char* st = smem + s * kStageBytes;
+            const u64 a1 = smem_desc(st), a0 = smem_desc(st + kTileBytes), b1 = smem_desc(st + 2 * kTileBytes),
+                      b0 = smem_desc(st + 3 * kTileBytes);
+#pragma unroll
+            for (int kk = 0; kk < kTileK / 32; ++kk) {
+                const u64 off = (u64)(kk * 32) >> 4;           // 32 bytes along K inside the swizzled row
+                const bool acc = kb > 0 || kk > 0;
+                mma_i8(acc11, a1 + off, b1 + off, acc);
+                mma_i8(acc00, a0 + off, b0 + off, acc);
+                mma_i8(accm, a1 + off, b0 + off, acc);
+                mma_i8(accm, a0 + off, b1 + off, true);
+            }
+            mma_commit(&empty[s]);                            // stage free once these MMAs have read it
+        }
+        mma_commit(&done);                                    // arrives after every MMA issued above
+    }
+    __syncthreads();
+    const bool fine = mbar_wait(&done, 0, p.error) && !abort_flag;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (fine) {
+        const u32 m = p.tab->m[l];
+        const u64 br = p.tab->barrett[l];
+        const u32 off49 = mod_barrett(1ull << 49, m, br);
+        const u64 row = (u64)tm * kTileM + warp * 32 + lane;
+        const u32 lane_base = (u32)(warp * 32) << 16;
+        for (int c0 = 0; c0 < kTileN; c0 += 32) {
+            u32 s11[32], s00[32], sm[32];
+            tmem_ld32(acc11 + lane_base + c0, s11);
+            tmem_ld32(acc00 + lane_base + c0, s00);
+            tmem_ld32(accm + lane_base + c0, sm);
+            asm volatile("tcgen05.wait::ld.sync.aligned;");
+            if (row < p.M) {
+                u16* out = p.res + ((u64)l * p.M + row) * p.Nc;
+#pragma unroll
+                for (int c = 0; c < 32; ++c) {
+                    const u64 col = (u64)tn * kTileN + c0 + c;
+                    if (col >= p.Nc) break;
+                    // 65536 S11 + 256 Smid + S00 (|.| < 2^48), made nonnegative by 2^49 and reduced
+                    const long long v = (long long)(int)s11[c] * 65536 + (long long)(int)sm[c] * 256 + (long long)(int)s00[c];
+                    const u32 rb = mod_barrett((u64)(v + (1ll << 49)), m, br);
+                    const u64 t = (u64)rb + m - off49;
+                    out[col] = (u16)mod_barrett(t, m, br);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" :: "r"(tmem));
+}
+
+#endif  // LF_RESIDUE_MMA_KERNEL
+
+// ---------------------------------------------------------------- 3. reconstruction and rounding
+struct RecParams {
+    const u16* res; const ResTables* tab; int L; int qwords;
+    const LineInfo* linfo; const LineInfo* rinfo;
+    u32* C; u64 ldc, M, Nc;
+    int subtract, lower;
+};
+// RN(sign_x * X * 2^sx + c) with one rounding for an exact multiword X: both terms in one exact
+// window when they are close, otherwise the far smaller term as a sticky unit (as in fma).
+template <int N> __device__ Num<N> round_sum2(const u32* X, int xw, i64 sx, int signx, const Num<N>& c) {
+    constexpr int CW = kResMaxQWords + 2 * N + 8;
+    u32 pos[CW], neg[CW];
+    // magnitude tops
+    int tx = -1;
+    for (int w = xw - 1; w >= 0; --w) if (X[w]) { tx = w; break; }
+    if (tx < 0) return c;                                       // no product term left
+    const i64 topx = sx + 32 * (i64)tx + 31 - __clz(X[tx]);
+    if (!c.s) {
+        u32 t[kResMaxQWords + 1];
+        for (int w = 0; w < xw; ++w) t[w] = X[w];
+        Rounded<N> R; round_info<N>(t, xw, sx, R);
+        return finish<N>(R.m, R.e, signx, R.rb && (R.sb || (R.m[0] & 1u)), 0);
+    }
+    const i64 sc = (i64)c.e - (32 * N - 1), topc = c.e;
+    const i64 hi = topx > topc ? topx : topc;
+    const i64 lo = hi + 3 - 32 * (i64)(CW - 1);               // exponent of window bit 32
+    for (int w = 0; w < CW; ++w) { pos[w] = 0; neg[w] = 0; }
+    // x
+    if (sx >= lo) acc_add(signx > 0 ? pos : neg, CW, X, xw, 32 + (sx - lo));
+    else (signx > 0 ? pos : neg)[0] |= 1u;
+    if (sc >= lo) acc_add(c.s > 0 ? pos : neg, CW, c.m, N, 32 + (sc - lo));
+    else (c.s > 0 ? pos : neg)[0] |= 1u;
+    int cmp = 0;
+    for (int w = CW - 1; w >= 0 && !cmp; --w) if (pos[w] != neg[w]) cmp = pos[w] > neg[w] ? 1 : -1;
+    if (!cmp) return zero<N>();
+    u32* big = cmp > 0 ? pos : neg;
+    const u32* small = cmp > 0 ? neg : pos;
+    u32 bo = 0;
+    for (int w = 0; w < CW; ++w) { u64 d = (u64)small[w] + bo; u32 o = big[w]; big[w] = (u32)((u64)o - d); bo = (u64)o < d; }
+    Rounded<N> R; round_info<N>(big, CW, lo - 32, R);
+    return finish<N>(R.m, R.e, cmp, R.rb && (R.sb || (R.m[0] & 1u)), 0);
+}
+
+template <int N> __global__ void __launch_bounds__(128) reconstruct_kernel(RecParams p) {
+    const u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (j >= p.Nc || i >= p.M) return;
+    if (p.lower && j > i) return;
+    constexpr u64 E = N + 3;
+    u32* out = p.C + (i * p.ldc + j) * E;
+    const Num<N> c = p.subtract ? load_plain<N>(out) : zero<N>();
+    const LineInfo li = p.linfo[i], ri = p.rinfo[j];
+    const u32 st = (p.subtract ? c.st : 0u) | li.status | ri.status;
+    if (st) { store<N>(out, zero<N>(st)); return; }
+    if (!li.nonzero || !ri.nonzero) { store<N>(out, p.subtract ? c : zero<N>()); return; }
+    // S = sum_l t_l (M/m_l) in 64-bit column sums, F = sum_l t_l floor(2^48/m_l)
+    u64 col[kResMaxQWords + 1];
+    for (int w = 0; w <= p.qwords; ++w) col[w] = 0;
+    u64 F = 0;
+    bool any = false;
+    for (int l = 0; l < p.L; ++l) {
+        const u32 r = p.res[((u64)l * p.M + i) * p.Nc + j];
+        any |= r != 0;
+        const u32 m = p.tab->m[l];
+        const u32 t = mod_barrett((u64)r * p.tab->w[l], m, p.tab->barrett[l]);
+        F += (u64)t * p.tab->frac[l];
+        for (int w = 0; w < p.qwords; ++w) col[w] += (u64)t * p.tab->q[l][w];
+    }
+    if (!any) { store<N>(out, p.subtract ? c : zero<N>()); return; }       // X == 0
+    u32 S[kResMaxQWords + 2];
+    u64 cy = 0;
+    for (int w = 0; w <= p.qwords; ++w) { u64 v = col[w] + cy; S[w] = (u32)v; cy = v >> 32; }
+    S[p.qwords + 1] = (u32)cy;
+    const u64 q = (F + (1ull << 47)) >> 48;                  // round(F): X = S - q M
+    // D = S - q*M (two's complement over qwords+2 words)
+    u64 borrow = 0;
+    for (int w = 0; w <= p.qwords + 1; ++w) {
+        const u64 qm = (w <= p.qwords ? (u64)p.tab->M[w] : 0ull) * q + borrow;
+        const u32 lo = (u32)qm;
+        const u32 old = S[w];
+        S[w] = old - lo;
+        borrow = (qm >> 32) + (old < lo ? 1u : 0u);
+    }
+    int sign = 1;
+    const int xw = p.qwords + 2;
+    if (S[xw - 1] >> 31) {
+        sign = -1; u64 c1 = 1;
+        for (int w = 0; w < xw; ++w) { u64 v = (u64)(u32)~S[w] + c1; S[w] = (u32)v; c1 = v >> 32; }
+    }
+    const i64 scale = (i64)li.bottom + ri.bottom - 2 * (32 * N - 1);
+    const Num<N> v = round_sum2<N>(S, xw, scale, p.subtract ? -sign : sign, c);
+    // a zero exact sum X with the addend falls back to c itself, as exact_dot_add
+    store<N>(out, v);
+}
+
+typedef void (*DigitFn)(const DigitParams&, cudaStream_t);
+typedef void (*RecFn)(const RecParams&, cudaStream_t);
+struct ResidueKernels { DigitFn digits; RecFn rec; };
+const ResidueKernels* residue_kernels(int limbs);
+
+template <int N> void digits_launch(const DigitParams& p, cudaStream_t s) {
+    if (!p.rows_pad || !p.Kp) return;
+    dim3 grid((unsigned)((p.Kp + 127) / 128), (unsigned)p.rows_pad);
+    digits_kernel<N><<<grid, 128, 0, s>>>(p);
+}
+template <int N> void rec_launch(const RecParams& p, cudaStream_t s) {
+    if (!p.M || !p.Nc) return;
+    dim3 grid((unsigned)((p.Nc + 127) / 128), (unsigned)p.M);
+    reconstruct_kernel<N><<<grid, 128, 0, s>>>(p);
+}
+
+}  // namespace lfd
+
+#define LF_RESIDUE_INSTANTIATE(N)                                                                  \
+    namespace lfd {                                                                                \
+    extern const ResidueKernels residue_kernels_##N; const ResidueKernels residue_kernels_##N = {digits_launch<N>, rec_launch<N>}; \
+    }
