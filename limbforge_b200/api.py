@@ -273,7 +273,7 @@ class Buffer:
         self.handle = h
 
     def __del__(self):
-        if getattr(self, "handle", None):
+        if getattr(self, "handle", None) and lib is not None:
             lib.lf_buffer_release(self.handle)
             self.handle = None
 
@@ -319,7 +319,7 @@ class Submission:
         self.handle = handle
 
     def __del__(self):
-        if getattr(self, "handle", None):
+        if getattr(self, "handle", None) and lib is not None:
             lib.lf_submission_destroy(self.handle)
             self.handle = None
 
@@ -344,7 +344,7 @@ class CommandBatch:
         self.handle = h
 
     def __del__(self):
-        if getattr(self, "handle", None):
+        if getattr(self, "handle", None) and lib is not None:
             lib.lf_batch_destroy(self.handle)
             self.handle = None
 
@@ -390,7 +390,7 @@ class Engine:
         self.handle = h
 
     def __del__(self):
-        if getattr(self, "handle", None):
+        if getattr(self, "handle", None) and lib is not None:
             lib.lf_engine_destroy(self.handle)
             self.handle = None
 
@@ -476,7 +476,7 @@ class PinnedArray:
         self.array = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
 
     def __del__(self):
-        if getattr(self, "_p", None):
+        if getattr(self, "_p", None) and lib is not None:
             self.array = None
             lib.lf_host_free(self._p)
             self._p = None
@@ -496,7 +496,7 @@ class Linalg:
         self.handle = h
 
     def __del__(self):
-        if getattr(self, "handle", None):
+        if getattr(self, "handle", None) and lib is not None:
             lib.lf_linalg_destroy(self.handle)
             self.handle = None
 
