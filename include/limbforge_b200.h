@@ -115,6 +115,18 @@ int lf_dev_exact_product(lf_linalg* linalg, int bits, const void* left, size_t l
                          size_t right_ls, size_t right_ks, size_t M, size_t N, size_t K, void* C, size_t ldc, int subtract,
                          int lower, void* stream);
 
+/* Allocation-free form of lf_dev_exact_product (no reference counterpart).  For callers that cannot
+ * allocate device memory when they need a product (a fixed device-memory plan, threads that must not
+ * take the allocator's locks, embedding runtimes that forbid allocation): all temporary device data
+ * lives in a 32 MiB static device array of the library, so no cudaMalloc/cudaFree is called.  Same
+ * operands and result as lf_dev_exact_product; at most 8192 lines (M + N), and products whose residue
+ * planes would exceed the array are rejected with LF_INVALID_ARGUMENT.  Calls share the array: calls
+ * that overlap on the GPU race; the first call on a device resolves the array's address (make it
+ * before any stream capture).  Synchronous on `stream`. */
+int lf_dev_exact_product_static(int bits, const void* left, size_t left_ls, size_t left_ks, const void* right,
+                                size_t right_ls, size_t right_ks, size_t M, size_t N, size_t K, void* C, size_t ldc,
+                                int subtract, int lower, void* stream);
+
 /* ---- Buffers (engine.hpp:74-86, 194-198): device-resident typed storage of one engine ---- */
 int lf_buffer_create(lf_engine* engine, size_t bytes, lf_buffer** out);                /* Engine::make_buffer */
 void lf_buffer_release(lf_buffer* buffer);                                              /* last reference frees */

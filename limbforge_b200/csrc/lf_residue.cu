@@ -187,3 +187,56 @@ bool ResidueEngine::run(int bits, lfd::LineView left, lfd::LineView right, uint6
 }
 
 }  // namespace lfr
+
+// ---------------------------------------------------------------- pieces for the allocation-free entry point
+// (lf_noalloc.cu): the same kernels and tables, with every device buffer supplied by the caller.
+namespace lfr {
+
+int residue_moduli_for(int bits, int G, uint64_t K) {
+    const int P = 32 * (bits / 32) + G;
+    int logk = 0;
+    while ((1ull << logk) < K) ++logk;
+    const double need = 2.0 * P + logk + 3;
+    double have = 0;
+    int L = 0;
+    while (have <= need) {
+        if (L >= lfd::kResMaxModuli) return 0;
+        have += std::log2((double)primes()[L++]);
+    }
+    return L;
+}
+int residue_max_band() { return kMaxBand; }
+uint64_t residue_max_k() { return kMaxK; }
+
+void residue_tables_host(int L, lfd::ResTables& h, int& qwords_out) {
+    const auto& m = primes();
+    std::vector<uint32_t> M{1};
+    for (int l = 0; l < L; ++l) mul_small(M, m[l]);
+    int qwords = 0;
+    for (int l = 0; l < L; ++l) {
+        h.m[l] = m[l];
+        h.barrett[l] = ~0ull / m[l] + ((~0ull % m[l]) + 1 == m[l] ? 1 : 0);
+        h.frac[l] = (1ull << 48) / m[l];
+        std::vector<uint32_t> q{1};
+        for (int t = 0; t < L; ++t) if (t != l) mul_small(q, m[t]);
+        qwords = std::max(qwords, (int)q.size());
+        for (size_t w = 0; w < q.size(); ++w) h.q[l][w] = q[w];
+        h.w[l] = inverse_mod(mod_small(q, m[l]), m[l]);
+        uint64_t pw = 1;
+        for (int w = 0; w < 40; ++w) { h.pw[l][w] = (uint32_t)pw; pw = (pw << 32) % m[l]; }
+    }
+    for (size_t w = 0; w < M.size(); ++w) h.M[w] = M[w];
+    qwords_out = std::max(qwords, (int)M.size() - 1);
+}
+
+CUtensorMap residue_plane_map(void* base, uint64_t Kp, uint64_t rows_pad, int L) { return plane_map(base, Kp, rows_pad, L); }
+
+void residue_mma_launch(dim3 grid, const CUtensorMap& ta1, const CUtensorMap& ta0, const CUtensorMap& tb1, const CUtensorMap& tb0,
+                        const lfd::MmaParams& p, cudaStream_t s) {
+    const size_t smem = lfd::kStages * lfd::kStageBytes + 1024;
+    cuda_check(cudaFuncSetAttribute(lfd::residue_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem");
+    lfd::residue_mma_kernel<<<grid, 128, smem, s>>>(ta1, ta0, tb1, tb0, p);
+    cuda_check(cudaGetLastError(), "residue products");
+}
+
+}  // namespace lfr

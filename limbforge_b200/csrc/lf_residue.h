@@ -14,3 +14,16 @@ struct ResidueEngine {
 };
 
 }  // namespace lfr
+
+// Pieces of the engine for callers that supply every device buffer (the allocation-free entry point).
+#include <cuda.h>
+namespace lfd { struct ResTables; struct MmaParams; }
+namespace lfr {
+int residue_moduli_for(int bits, int G, uint64_t K);      // modulus count L, 0 above the table limit
+int residue_max_band();
+uint64_t residue_max_k();
+void residue_tables_host(int L, lfd::ResTables& tables, int& qwords);
+CUtensorMap residue_plane_map(void* base, uint64_t Kp, uint64_t rows_pad, int L);
+void residue_mma_launch(dim3 grid, const CUtensorMap& ta1, const CUtensorMap& ta0, const CUtensorMap& tb1, const CUtensorMap& tb0,
+                        const lfd::MmaParams& p, cudaStream_t s);
+}  // namespace lfr
