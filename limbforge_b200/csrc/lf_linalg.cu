@@ -205,6 +205,7 @@ static lf_cholesky_info cholesky_device(Linalg& la, int bits, uint32_t* W, size_
         cuda_check(cudaMemcpyAsync(dinfo, init, sizeof init, cudaMemcpyHostToDevice, s), "info");
         lfd::CholParams p{W, n, k0, k1, dinfo, err};
         fk->diag(p, s);
+        cuda_check(cudaGetLastError(), "cholesky diagonal block");
         long long got[3];
         cuda_check(cudaMemcpyAsync(got, dinfo, sizeof got, cudaMemcpyDeviceToHost, s), "info");
         cuda_check(cudaStreamSynchronize(s), "panel");
@@ -213,12 +214,13 @@ static lf_cholesky_info cholesky_device(Linalg& la, int bits, uint32_t* W, size_
             fail = (size_t)got[0];
             info.pivot = fail; info.pivot_sign = (int)got[1]; info.pivot_status = (uint32_t)got[2];
             fk->rows(p, k1, fail, s);                   // rows below the block: columns [k0, fail)
+            cuda_check(cudaGetLastError(), "cholesky panel rows");
             cuda_check(cudaStreamSynchronize(s), "panel");
             info.panel_seconds += since(t);
             break;
         }
         fk->rows(p, k1, k1, s);
-        cuda_check(cudaGetLastError(), "panel launch");
+        cuda_check(cudaGetLastError(), "cholesky panel rows");
         cuda_check(cudaStreamSynchronize(s), "panel");
         info.panel_seconds += since(t);
         if (k1 < n) {
@@ -231,6 +233,7 @@ static lf_cholesky_info cholesky_device(Linalg& la, int bits, uint32_t* W, size_
         }
     }
     if (fail < n) fk->prep(nullptr, W, n, fail, s);
+    cuda_check(cudaGetLastError(), "cholesky clear");
     cuda_check(cudaEventRecord(g1, s), "event");
     uint32_t ev = 0;
     cuda_check(cudaMemcpyAsync(&ev, err, 4, cudaMemcpyDeviceToHost, s), "error flag");
@@ -260,6 +263,7 @@ static double solve_device(Linalg& la, int bits, const uint32_t* L, size_t n, ui
             const size_t r1 = std::min(n, r0 + nb);
             cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
             fk->solve(lfd::SolveParams{L, X, n, nrhs, r0, r1, 0, err}, true, s);
+            cuda_check(cudaGetLastError(), "forward substitution");
             if (r1 < n) {
                 lfd::LineView lv{L + (r1 * n + r0) * E, n, 1};
                 lfd::LineView xv{X + r0 * nrhs * E, 1, nrhs};
@@ -271,6 +275,7 @@ static double solve_device(Linalg& la, int bits, const uint32_t* L, size_t n, ui
             const size_t r1 = std::min(n, r0 + nb);
             cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
             fk->solve(lfd::SolveParams{L, X, n, nrhs, r0, r1, 0, err}, false, s);
+            cuda_check(cudaGetLastError(), "back substitution");
             if (r0) {
                 lfd::LineView lv{L + (r0 * n) * E, 1, n};           // line i: column i of L from row r0
                 lfd::LineView xv{X + r0 * nrhs * E, 1, nrhs};
@@ -318,6 +323,7 @@ int lf_linalg_cholesky(lf_linalg* la, int bits, const void* A, size_t n, void* L
         auto w0 = Clock::now();
         cuda_check(cudaMemcpyAsync(dA, A, n * n * eb, cudaMemcpyHostToDevice, e.stream), "upload");
         lfd::factor_kernels(bits / 32)->prep(dA, W, n, n, e.stream);
+        cuda_check(cudaGetLastError(), "cholesky prepare");
         info = cholesky_device(*la, bits, W, n, block);
         cuda_check(cudaMemcpyAsync(L, W, n * n * eb, cudaMemcpyDeviceToHost, e.stream), "download");
         cuda_check(cudaStreamSynchronize(e.stream), "download");

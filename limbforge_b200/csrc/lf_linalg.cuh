@@ -102,12 +102,22 @@ template <int N> __device__ bool round_info(const u32* x, int len, i64 scale, Ro
 // of exact_dot_add (linalg.hpp:268-318).  Statuses: zero carrying the OR of c's and every x[k],
 // y[k] status; no nonzero product returns c itself (or zero).  `error` is set when one cluster
 // is wider than kClusterWords words (the result is then zero with status invalid).
-template <int N> __device__ Num<N> exact_dot_add_dev(const u32* cp, bool subtract, const u32* x, i64 sx, const u32* y, i64 sy,
+// RO: the operands are read-only for the whole kernel (read-only cache loads); kernels that write
+// entries they read later (the factorization panels and solves) use RO = false, coherent loads.
+template <bool RO> __device__ __forceinline__ u32 ldw(const u32* p) { if constexpr (RO) return __ldg(p); else return *(volatile const u32*)p; }
+template <int N, bool RO> __device__ __forceinline__ Num<N> ldn(const u32* p) {
+    Num<N> r;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.m[i] = ldw<RO>(p + i);
+    r.e = (int)ldw<RO>(p + N); r.s = (int)ldw<RO>(p + N + 1); r.st = ldw<RO>(p + N + 2);
+    return r;
+}
+template <int N, bool RO = true> __device__ Num<N> exact_dot_add_dev(const u32* cp, bool subtract, const u32* x, i64 sx, const u32* y, i64 sy,
                                                      u64 K, u32* error) {
     constexpr i64 E = N + 3;
     const Num<N> c = cp ? load_plain<N>(cp) : zero<N>();
     u32 st = c.st;
-    for (u64 k = 0; k < K; ++k) st |= __ldg(x + (i64)k * sx * E + N + 2) | __ldg(y + (i64)k * sy * E + N + 2);
+    for (u64 k = 0; k < K; ++k) st |= ldw<RO>(x + (i64)k * sx * E + N + 2) | ldw<RO>(y + (i64)k * sy * E + N + 2);
     if (st) return zero<N>(st);
     // term k < K: product x_k y_k (< 2^(scale+64N)); k == K: the addend (< 2^(scale+32N))
     auto term = [&](u64 k, i64& scale, i64& top, int& sign) -> bool {
@@ -117,9 +127,9 @@ template <int N> __device__ Num<N> exact_dot_add_dev(const u32* cp, bool subtrac
             return true;
         }
         const u32* a = x + (i64)k * sx * E; const u32* b = y + (i64)k * sy * E;
-        const int sa = (int)__ldg(a + N + 1), sb = (int)__ldg(b + N + 1);
+        const int sa = (int)ldw<RO>(a + N + 1), sb = (int)ldw<RO>(b + N + 1);
         if (!sa || !sb) return false;
-        scale = (i64)(int)__ldg(a + N) + (int)__ldg(b + N) - 2 * (32 * N - 1);
+        scale = (i64)(int)ldw<RO>(a + N) + (int)ldw<RO>(b + N) - 2 * (32 * N - 1);
         top = scale + 64 * N;
         sign = subtract ? -sa * sb : sa * sb;
         return true;
@@ -169,7 +179,7 @@ template <int N> __device__ Num<N> exact_dot_add_dev(const u32* cp, bool subtrac
             if (!term(k, s, tp, sg) || !(tp <= cutoff && tp > low - gap)) continue;
             if (k == K) acc_add(sg > 0 ? pos : neg, len, c.m, N, s - low);
             else {
-                const Num<N> a = load<N>(x + (i64)k * sx * E), b = load<N>(y + (i64)k * sy * E);
+                const Num<N> a = ldn<N, RO>(x + (i64)k * sx * E), b = ldn<N, RO>(y + (i64)k * sy * E);
                 u32 prod[2 * N];
                 mant_mul<N>(a.m, b.m, prod);
                 acc_add(sg > 0 ? pos : neg, len, prod, 2 * N, s - low);
@@ -246,47 +256,138 @@ template <int N> void mirror_launch(u32* C, u64 n, u64 ldc, cudaStream_t s) {
 
 namespace lfd {
 
+// ---------------------------------------------------------------- warp-cooperative exact dot
+// exact_dot_add with the terms spread over the 32 lanes of a warp (k = lane, lane + 32, ...).  When
+// every nonzero term and the addend fit one two's-complement window of W = 2N + 10 words
+// (64N + 320 bits: products of the same magnitude class, as in factorization panels), each lane sums
+// its terms exactly in the window, the warp adds the windows exactly and lane 0 rounds once;
+// otherwise lane 0 runs the generic cluster routine.  Every lane receives the result.
+template <int N> __device__ __forceinline__ Num<N> warp_broadcast(const Num<N>& v) {
+    Num<N> r;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.m[i] = __shfl_sync(0xffffffffu, v.m[i], 0);
+    r.e = __shfl_sync(0xffffffffu, v.e, 0); r.s = __shfl_sync(0xffffffffu, v.s, 0); r.st = __shfl_sync(0xffffffffu, v.st, 0);
+    return r;
+}
+template <int N, bool RO> __device__ Num<N> warp_exact_dot(const u32* cp, bool subtract, const u32* x, i64 sx, const u32* y, i64 sy,
+                                                          u64 K, u32* error) {
+    constexpr int W = 2 * N + 10;
+    constexpr i64 E = N + 3;
+    const int lane = threadIdx.x & 31;
+    const Num<N> c = cp ? ldn<N, RO>(cp) : zero<N>();
+    u32 st = 0; int cnt = 0;
+    i64 lo = INT64_MAX, hi = INT64_MIN;
+    for (u64 k = lane; k < K; k += 32) {
+        const u32* a = x + (i64)k * sx * E; const u32* b = y + (i64)k * sy * E;
+        st |= ldw<RO>(a + N + 2) | ldw<RO>(b + N + 2);
+        const int sa = (int)ldw<RO>(a + N + 1), sb = (int)ldw<RO>(b + N + 1);
+        if (sa && sb) {
+            const i64 s = (i64)(int)ldw<RO>(a + N) + (int)ldw<RO>(b + N) - 2 * (32 * N - 1);
+            lo = s < lo ? s : lo; hi = s + 64 * N > hi ? s + 64 * N : hi; ++cnt;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        st |= __shfl_xor_sync(0xffffffffu, st, o);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        const i64 l2 = __shfl_xor_sync(0xffffffffu, lo, o), h2 = __shfl_xor_sync(0xffffffffu, hi, o);
+        lo = l2 < lo ? l2 : lo; hi = h2 > hi ? h2 : hi;
+    }
+    st |= c.st;
+    if (st) return zero<N>(st);
+    if (!cnt) return cp ? c : zero<N>();
+    if (c.s) {
+        const i64 sc = (i64)c.e - (32 * N - 1);
+        lo = sc < lo ? sc : lo; hi = (i64)c.e + 1 > hi ? (i64)c.e + 1 : hi;
+    }
+    int logc = 0;
+    while ((1 << logc) < cnt + 2) ++logc;
+    if (hi - lo + logc + 1 >= 32 * (i64)W) {
+        Num<N> r = zero<N>();
+        if (lane == 0) r = exact_dot_add_dev<N, RO>(cp, subtract, x, sx, y, sy, K, error);
+        return warp_broadcast<N>(r);
+    }
+    u32 acc[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) acc[w] = 0;
+    for (u64 k = lane; k < K; k += 32) {
+        const Num<N> a = ldn<N, RO>(x + (i64)k * sx * E), b = ldn<N, RO>(y + (i64)k * sy * E);
+        if (!a.s || !b.s) continue;
+        u32 p[2 * N], t[W];
+        mant_mul<N>(a.m, b.m, p);
+        place_words<W, 2 * N>(t, p, (i64)a.e + b.e - 2 * (32 * N - 1) - lo);
+        accumulate<W>(acc, t, (subtract ? -a.s * b.s : a.s * b.s) < 0);
+    }
+    if (lane == 0 && c.s) {
+        u32 t[W];
+        place_words<W, N>(t, c.m, (i64)c.e - (32 * N - 1) - lo);
+        accumulate<W>(acc, t, c.s < 0);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        u32 other[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) other[w] = __shfl_down_sync(0xffffffffu, acc[w], o);
+        accumulate<W>(acc, other, false);
+    }
+    Num<N> r = zero<N>();
+    if (lane == 0) {
+        int sign = 1;
+        if (acc[W - 1] >> 31) {
+            sign = -1; u64 cy = 1;
+#pragma unroll
+            for (int w = 0; w < W; ++w) { u64 v = (u64)(u32)~acc[w] + cy; acc[w] = (u32)v; cy = v >> 32; }
+        }
+        r = round_general<N, W>(acc, lo, sign, 0);
+    }
+    return warp_broadcast<N>(r);
+}
+
 // ---------------------------------------------------------------- blocked Cholesky pieces
-// W: n x n row-major work matrix (element stride E).  D(c; x, y; K) = exact_dot_add_dev(c, subtract).
+// W: n x n row-major work matrix (element stride E).  D(c; x, y; K) = RN(c - sum x_k y_k), one rounding.
 struct CholParams { u32* W; u64 n, k0, k1; long long* info; u32* error; };
 
 // Diagonal block [k0, k1) column by column: s_jj = D(w_jj; row j [k0,j)), l_jj = sqrt(s_jj) (or the
 // failing pivot recorded in info = {pivot, sign, status}); l_ij = RN(D(w_ij; row i, row j; [k0,j)) / l_jj)
 // for the block rows i > j.  The same formulas in the same dependency order as the row-by-row host
-// panel of linalg.mm:418-430, so every entry gets identical bits.
-template <int N> __global__ void chol_diag_kernel(CholParams p) {
+// panel of linalg.mm:418-430, so every entry gets identical bits.  One warp per dot product.
+template <int N> __global__ void __launch_bounds__(128) chol_diag_kernel(CholParams p) {
     constexpr u64 E = N + 3;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     __shared__ int failed;
     if (!threadIdx.x) failed = 0;
     __syncthreads();
     for (u64 j = p.k0; j < p.k1; ++j) {
         u32* wjj = p.W + (j * p.n + j) * E;
-        if (!threadIdx.x) {
-            const Num<N> s = exact_dot_add_dev<N>(wjj, true, p.W + (j * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
-            if (s.st || s.s <= 0) { p.info[0] = (long long)j; p.info[1] = s.st ? 0 : s.s; p.info[2] = s.st; failed = 1; }
-            else store<N>(wjj, lfd::sqrt<N>(s));
+        if (warp == 0) {
+            const Num<N> s = warp_exact_dot<N, false>(wjj, true, p.W + (j * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
+            if (lane == 0) {
+                if (s.st || s.s <= 0) { p.info[0] = (long long)j; p.info[1] = s.st ? 0 : s.s; p.info[2] = s.st; failed = 1; }
+                else store<N>(wjj, lfd::sqrt<N>(s));
+            }
         }
         __syncthreads();
         if (failed) return;
-        const Num<N> d = load_plain<N>(wjj);
-        for (u64 i = j + 1 + threadIdx.x; i < p.k1; i += blockDim.x) {
+        for (u64 i = j + 1 + warp; i < p.k1; i += nw) {
             u32* wij = p.W + (i * p.n + j) * E;
-            const Num<N> v = exact_dot_add_dev<N>(wij, true, p.W + (i * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
-            store<N>(wij, div<N>(v, d));
+            const Num<N> v = warp_exact_dot<N, false>(wij, true, p.W + (i * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
+            if (lane == 0) store<N>(wij, div<N>(v, ldn<N, false>(wjj)));
         }
         __syncthreads();
     }
 }
 // Rows i in [r0, n) below the diagonal block: l_ij = RN(D(w_ij; row i, row j; [k0,j)) / l_jj) for
-// j in [k0, jend), left to right (jend = the failing pivot, or k1).  One thread per row.
-template <int N> __global__ void chol_rows_kernel(CholParams p, u64 r0, u64 jend) {
+// j in [k0, jend), left to right (jend = the failing pivot, or k1).  One warp per row.
+template <int N> __global__ void __launch_bounds__(128) chol_rows_kernel(CholParams p, u64 r0, u64 jend) {
     constexpr u64 E = N + 3;
-    const u64 i = r0 + (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 i = r0 + ((u64)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x & 31;
     if (i >= p.n) return;
     for (u64 j = p.k0; j < jend; ++j) {
         u32* wij = p.W + (i * p.n + j) * E;
-        const Num<N> v = exact_dot_add_dev<N>(wij, true, p.W + (i * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
-        store<N>(wij, div<N>(v, load_plain<N>(p.W + (j * p.n + j) * E)));
+        const Num<N> v = warp_exact_dot<N, false>(wij, true, p.W + (i * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
+        if (lane == 0) store<N>(wij, div<N>(v, ldn<N, false>(p.W + (j * p.n + j) * E)));
+        __syncwarp();
     }
 }
 // W = lower triangle of A (upper zero); after a failure at pivot p: entries (i, j), p <= j <= i, are
@@ -309,28 +410,35 @@ template <int N> __global__ void chol_prepare_kernel(const u32* A, u32* W, u64 n
 // i ascending; backward block: x_i = RN(D(x_i; column i of L below i within (i, r1), x(i, r1)) / l_ii),
 // i descending (upper: R = L^T stored by rows).  One thread per right-hand side.
 struct SolveParams { const u32* L; u32* X; u64 n, nrhs, r0, r1; int upper; u32* error; };
-template <int N> __global__ void solve_forward_kernel(SolveParams p) {
+// One warp per right-hand side.
+template <int N> __global__ void __launch_bounds__(128) solve_forward_kernel(SolveParams p) {
     constexpr u64 E = N + 3;
-    const u64 c = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 c = ((u64)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x & 31;
     if (c >= p.nrhs) return;
     for (u64 i = p.r0; i < p.r1; ++i) {
         u32* x = p.X + (i * p.nrhs + c) * E;
-        const Num<N> v = exact_dot_add_dev<N>(x, true, p.L + (i * p.n + p.r0) * E, 1, p.X + (p.r0 * p.nrhs + c) * E, (i64)p.nrhs, i - p.r0, p.error);
-        store<N>(x, div<N>(v, load<N>(p.L + (i * p.n + i) * E)));
+        const Num<N> v = warp_exact_dot<N, false>(x, true, p.L + (i * p.n + p.r0) * E, 1, p.X + (p.r0 * p.nrhs + c) * E, (i64)p.nrhs, i - p.r0, p.error);
+        if (lane == 0) store<N>(x, div<N>(v, ldn<N, false>(p.L + (i * p.n + i) * E)));
+        __syncwarp();
     }
 }
-template <int N> __global__ void solve_backward_kernel(SolveParams p) {
+template <int N> __global__ void __launch_bounds__(128) solve_backward_kernel(SolveParams p) {
     constexpr u64 E = N + 3;
-    const u64 c = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 c = ((u64)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x & 31;
     if (c >= p.nrhs) return;
     for (u64 i = p.r1; i-- > p.r0;) {
         u32* x = p.X + (i * p.nrhs + c) * E;
-        Num<N> v = load_plain<N>(x);
+        Num<N> v;
         if (i + 1 < p.r1) {
             const u32* col = p.upper ? p.L + (i * p.n + i + 1) * E : p.L + ((i + 1) * p.n + i) * E;
-            v = exact_dot_add_dev<N>(x, true, col, p.upper ? 1 : (i64)p.n, p.X + ((i + 1) * p.nrhs + c) * E, (i64)p.nrhs, p.r1 - i - 1, p.error);
+            v = warp_exact_dot<N, false>(x, true, col, p.upper ? 1 : (i64)p.n, p.X + ((i + 1) * p.nrhs + c) * E, (i64)p.nrhs, p.r1 - i - 1, p.error);
+        } else {
+            v = ldn<N, false>(x);
         }
-        store<N>(x, div<N>(v, load<N>(p.L + (i * p.n + i) * E)));
+        if (lane == 0) store<N>(x, div<N>(v, ldn<N, false>(p.L + (i * p.n + i) * E)));
+        __syncwarp();
     }
 }
 
@@ -345,7 +453,7 @@ template <int N> void chol_diag_launch(const CholParams& p, cudaStream_t s) { ch
 template <int N> void chol_rows_launch(const CholParams& p, u64 r0, u64 jend, cudaStream_t s) {
     if (r0 >= p.n || jend <= p.k0) return;
     const u64 rows = p.n - r0;
-    chol_rows_kernel<N><<<(unsigned)((rows + 63) / 64), 64, 0, s>>>(p, r0, jend);
+    chol_rows_kernel<N><<<(unsigned)((rows + 3) / 4), 128, 0, s>>>(p, r0, jend);
 }
 template <int N> void chol_prep_launch(const u32* A, u32* W, u64 n, u64 fail, cudaStream_t s) {
     if (!n) return;
@@ -354,9 +462,9 @@ template <int N> void chol_prep_launch(const u32* A, u32* W, u64 n, u64 fail, cu
 }
 template <int N> void solve_launch(const SolveParams& p, bool forward, cudaStream_t s) {
     if (!p.nrhs || p.r1 <= p.r0) return;
-    const unsigned blocks = (unsigned)((p.nrhs + 63) / 64);
-    if (forward) solve_forward_kernel<N><<<blocks, 64, 0, s>>>(p);
-    else solve_backward_kernel<N><<<blocks, 64, 0, s>>>(p);
+    const unsigned blocks = (unsigned)((p.nrhs + 3) / 4);
+    if (forward) solve_forward_kernel<N><<<blocks, 128, 0, s>>>(p);
+    else solve_backward_kernel<N><<<blocks, 128, 0, s>>>(p);
 }
 
 }  // namespace lfd

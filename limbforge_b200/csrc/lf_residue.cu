@@ -85,7 +85,10 @@ TableSet tables_for(int device, int L) {
     TableSet t;
     t.L = L; t.qwords = std::max(qwords, (int)M.size() - 1);
     cuda_check(cudaMalloc(&t.dev, sizeof(lfd::ResTables)), "residue tables");
+    // cudaMemcpy from pageable memory may return before its DMA lands, and the kernels that read the
+    // tables run on non-blocking streams: wait for the copy before the table is handed out.
     cuda_check(cudaMemcpy(t.dev, h, sizeof(lfd::ResTables), cudaMemcpyHostToDevice), "residue tables");
+    cuda_check(cudaStreamSynchronize(0), "residue tables");
     delete h;
     g_tables[key] = t;
     return t;

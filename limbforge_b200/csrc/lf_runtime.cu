@@ -243,6 +243,10 @@ int lf_engine_run_ternary(lf_engine* e, int bits, int op, const void* a, const v
 }
 
 // ---- buffers
+// A cudaMemcpy from pageable host memory may return before its DMA has landed, and work on the
+// engines' non-blocking streams is not ordered after the legacy default stream that carried it:
+// every host-to-device transfer outside a stream is followed by this wait.
+static void landed() { cuda_check(cudaStreamSynchronize(0), "host-to-device transfer"); }
 int lf_buffer_create(lf_engine* e, size_t bytes, lf_buffer** out) {
     LF_API_BEGIN
     if (!e || !out) throw invalid_argument("null argument");
@@ -251,7 +255,9 @@ int lf_buffer_create(lf_engine* e, size_t bytes, lf_buffer** out) {
     b->owner = e->identity; b->device = e->device; b->bytes = bytes;
     cudaError_t r = cudaMalloc(&b->dev, bytes ? bytes : 16);
     if (r != cudaSuccess) { b->dev = nullptr; delete b; throw runtime_error(std::string("CUDA buffer allocation: ") + cudaGetErrorString(r)); }
-    cudaMemset(b->dev, 0, bytes ? bytes : 16);
+    r = cudaMemset(b->dev, 0, bytes ? bytes : 16);
+    if (r == cudaSuccess) r = cudaStreamSynchronize(0);        // the memset is asynchronous to the host
+    if (r != cudaSuccess) { cudaFree(b->dev); b->dev = nullptr; delete b; throw runtime_error(std::string("CUDA buffer clear: ") + cudaGetErrorString(r)); }
     *out = b;
     LF_API_END
 }
@@ -271,6 +277,7 @@ int lf_buffer_upload(lf_buffer* b, const void* src, size_t bytes) {
     }
     b->host_authoritative = false;
     if (bytes) cuda_check(cudaMemcpy(b->dev, src, bytes, cudaMemcpyHostToDevice), "upload");
+    landed();
     LF_API_END
 }
 int lf_buffer_download(lf_buffer* b, void* dst, size_t bytes) {
@@ -307,6 +314,7 @@ int lf_buffer_device_pointer(lf_buffer* b, void** device) {
     if (b->host_authoritative) {
         cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
         cuda_check(cudaMemcpy(b->dev, b->host, b->bytes, cudaMemcpyHostToDevice), "mirror upload");
+        landed();
         b->host_authoritative = false;
     }
     *device = b->dev;
