@@ -170,6 +170,54 @@ int lf_dev_elementwise(int bits, int op, const void* a, const void* b, const voi
 int lf_dev_mul_chain(int bits, const void* x, const void* factors, size_t factor_stride, unsigned steps, void* out,
                      size_t count, void* stream);
 
+/* ---- Ragged mixed-precision batches.  No reference counterpart: the reference's
+ * BatchedLinalg::gemm (batched_linalg.hpp:86; batched_linalg.mm:163-173) runs one StridedGemm per
+ * call, one shape and one precision, so a ragged batch there is a loop of calls grouped by shape.
+ * A plan holds a list of GEMM instances, each with its own precision and shape, and optionally one
+ * batched 4x4 LU job (Engine::lu4 semantics, engine.hpp:164), all over one device arena.  Running it
+ * is one CUDA graph launch: one persistent kernel per precision class (blocks take chunks of output
+ * cells from a counter, heaviest instances first) and the LU kernel, on parallel graph branches.
+ * Block sizes and grids come from an autotuner that times the candidates on the plan itself.
+ * Instance i computes C_i (+)= A_i B_i exactly as a one-instance StridedGemm at bits_i would. */
+typedef struct lf_ragged_gemm {
+    int bits;                  /* 64..1024, multiple of 32 */
+    uint32_t m, n, k;          /* A_i m x k, B_i k x n, C_i m x n, row-major */
+    uint64_t a, b, c;          /* byte offsets in the arena, multiples of 16 */
+    int accumulate, negative;  /* as lf_strided_gemm */
+} lf_ragged_gemm;
+typedef struct lf_ragged_lu4 {
+    int bits; lf_batched4 shape;
+    uint64_t A, B, X, det, status;   /* byte offsets in the arena (multiples of 16); unused ones ignored */
+} lf_ragged_lu4;
+typedef struct lf_ragged_class_info {
+    int bits; size_t items, cells;    /* instances and output entries of this precision */
+    unsigned block, grid;             /* launch shape in use */
+    double trial_ms;                  /* measured time of that shape when tuned, else 0 */
+} lf_ragged_class_info;
+typedef struct lf_ragged_info {
+    size_t classes; lf_ragged_class_info cls[31];
+    unsigned lu4_block, lu4_grid; double lu4_trial_ms;
+    int tuned;
+} lf_ragged_info;
+typedef struct lf_ragged_plan lf_ragged_plan;
+
+/* Host only: assigns packed offsets (A, B, C of each instance in turn, then the LU job's A, B, X,
+ * det, status when lu4 is given), 256-byte aligned, and returns the arena size in bytes. */
+int lf_ragged_pack(int complex_, lf_ragged_gemm* items, size_t count, lf_ragged_lu4* lu4, uint64_t* arena_bytes);
+/* Validates the instances against an arena of arena_bytes (extents, alignment, no output overlapping
+ * another output or any input) and builds the work lists.  lu4 may be null. */
+int lf_ragged_plan_create(lf_engine* engine, int complex_, int fused, const lf_ragged_gemm* items, size_t count,
+                          const lf_ragged_lu4* lu4, uint64_t arena_bytes, lf_ragged_plan** out);
+/* Autotuner: times every candidate block size (and, for the LU job, grid form) of every precision
+ * class on this arena's data, with trial outputs written to plan-owned scratch so the arena is not
+ * modified, and keeps the fastest.  Synchronous.  Until it runs, defaults are used. */
+int lf_ragged_plan_tune(lf_ragged_plan* plan, const void* arena);
+/* One graph launch on `stream` (null = the legacy default stream); asynchronous.  Runs of one plan
+ * are ordered after each other whatever their streams.  The graph is rebuilt when the arena moves. */
+int lf_ragged_plan_run(lf_ragged_plan* plan, void* arena, void* stream);
+int lf_ragged_plan_get_info(const lf_ragged_plan* plan, lf_ragged_info* info);
+void lf_ragged_plan_destroy(lf_ragged_plan* plan);
+
 #ifdef __cplusplus
 }
 #endif

@@ -184,6 +184,27 @@ class _LinalgReport(C.Structure):
                [("analysis_seconds", C.c_double), ("gpu_seconds", C.c_double), ("method", C.c_int)]
 
 
+class _RaggedLu4(C.Structure):
+    _fields_ = [("bits", C.c_int), ("shape", _Batched4), ("A", C.c_uint64), ("B", C.c_uint64), ("X", C.c_uint64),
+                ("det", C.c_uint64), ("status", C.c_uint64)]
+
+
+class _RaggedClassInfo(C.Structure):
+    _fields_ = [("bits", C.c_int), ("items", C.c_size_t), ("cells", C.c_size_t), ("block", C.c_uint), ("grid", C.c_uint),
+                ("trial_ms", C.c_double)]
+
+
+class _RaggedInfo(C.Structure):
+    _fields_ = [("classes", C.c_size_t), ("cls", _RaggedClassInfo * 31), ("lu4_block", C.c_uint), ("lu4_grid", C.c_uint),
+                ("lu4_trial_ms", C.c_double), ("tuned", C.c_int)]
+
+
+# lf_ragged_gemm as a numpy record (one row per instance); offsets a, b, c are bytes in the arena.
+RAGGED_DTYPE = np.dtype({"names": ["bits", "m", "n", "k", "a", "b", "c", "accumulate", "negative"],
+                         "formats": [np.int32, np.uint32, np.uint32, np.uint32, np.uint64, np.uint64, np.uint64, np.int32, np.int32],
+                         "offsets": [0, 4, 8, 12, 16, 24, 32, 40, 44], "itemsize": 48})
+
+
 def _load() -> C.CDLL:
     if not os.path.exists(LIBRARY):
         raise ImportError(f"{LIBRARY} is missing: run limbforge_b200.build.build() (nvcc, sm_100a)")
@@ -218,6 +239,10 @@ def _load() -> C.CDLL:
         "lf_linalg_trsm": ([V, I, I, V, S, V, S, V, P(_FactorOptions), P(_Timing)], I),
         "lf_linalg_cholesky_solve": ([V, I, V, S, V, S, V, P(_FactorOptions), P(_Timing)], I),
         "lf_dev_exact_product": ([V, I, V, S, S, V, S, S, S, S, S, V, S, I, I, V], I),
+        "lf_ragged_pack": ([I, V, S, P(_RaggedLu4), P(C.c_uint64)], I),
+        "lf_ragged_plan_create": ([V, I, I, V, S, P(_RaggedLu4), C.c_uint64, P(V)], I),
+        "lf_ragged_plan_tune": ([V, V], I), "lf_ragged_plan_run": ([V, V, V], I),
+        "lf_ragged_plan_get_info": ([V, P(_RaggedInfo)], I), "lf_ragged_plan_destroy": ([V], None),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -462,6 +487,79 @@ class BatchedLinalg:
     def gemm_resident(self, batch: CommandBatch, s: StridedGemm, A: Buffer, B: Buffer, C_: Buffer) -> None:
         sh = self._shape(s)
         check(lib.lf_batch_strided_gemm(batch.handle, A.bits, int(A.complex), C.byref(sh), A.handle, B.handle, C_.handle))
+
+
+@dataclass
+class RaggedLu4:
+    """The batched 4x4 LU job of a ragged plan: Engine::lu4 semantics (engine.hpp:164) on arena data."""
+    bits: int
+    shape: Batched4
+    A: int = 0
+    B: int = 0
+    X: int = 0
+    det: int = 0
+    status: int = 0
+
+    def _c(self) -> _RaggedLu4:
+        s = self.shape
+        return _RaggedLu4(self.bits, _Batched4(s.count, s.rhs, int(s.inverse), int(s.determinant), int(s.fused)),
+                          self.A, self.B, self.X, self.det, self.status)
+
+
+def ragged_items(bits, m, n, k, accumulate=0, negative=0) -> np.ndarray:
+    """Instance table (RAGGED_DTYPE) from per-instance arrays; offsets are filled by ragged_pack."""
+    bits = np.asarray(bits)
+    t = np.zeros(bits.shape[0], RAGGED_DTYPE)
+    t["bits"], t["m"], t["n"], t["k"] = bits, m, n, k
+    t["accumulate"], t["negative"] = accumulate, negative
+    return t
+
+
+def ragged_pack(complex_: bool, items: np.ndarray, lu4: "RaggedLu4 | None" = None) -> int:
+    """Assigns packed byte offsets in place (and the LU job's); returns the arena size in bytes."""
+    if items.dtype != RAGGED_DTYPE or not items.flags["C_CONTIGUOUS"]:
+        raise InvalidArgument("items must be a contiguous RAGGED_DTYPE array")
+    total = C.c_uint64()
+    cl = lu4._c() if lu4 is not None else None
+    check(lib.lf_ragged_pack(int(complex_), _ptr(items), items.shape[0], C.byref(cl) if cl is not None else None,
+                             C.byref(total)))
+    if lu4 is not None:
+        lu4.A, lu4.B, lu4.X, lu4.det, lu4.status = cl.A, cl.B, cl.X, cl.det, cl.status
+    return int(total.value)
+
+
+class RaggedPlan:
+    """A ragged mixed-precision batch over one device arena, run as one CUDA graph launch
+    (lf_ragged_plan_*; no reference counterpart)."""
+
+    def __init__(self, engine: Engine, complex_: bool, fused: bool, items: np.ndarray, arena_bytes: int,
+                 lu4: "RaggedLu4 | None" = None):
+        if items.dtype != RAGGED_DTYPE or not items.flags["C_CONTIGUOUS"]:
+            raise InvalidArgument("items must be a contiguous RAGGED_DTYPE array")
+        self.engine = engine
+        h = C.c_void_p()
+        cl = lu4._c() if lu4 is not None else None
+        check(lib.lf_ragged_plan_create(engine.handle, int(complex_), int(fused), _ptr(items), items.shape[0],
+                                        C.byref(cl) if cl is not None else None, int(arena_bytes), C.byref(h)))
+        self.handle = h
+
+    def tune(self, arena_ptr: int) -> None:
+        check(lib.lf_ragged_plan_tune(self.handle, C.c_void_p(arena_ptr)))
+
+    def run(self, arena_ptr: int, stream: int = 0) -> None:
+        check(lib.lf_ragged_plan_run(self.handle, C.c_void_p(arena_ptr), C.c_void_p(stream)))
+
+    def info(self) -> dict:
+        i = _RaggedInfo()
+        check(lib.lf_ragged_plan_get_info(self.handle, C.byref(i)))
+        return {"tuned": bool(i.tuned), "lu4_block": i.lu4_block, "lu4_grid": i.lu4_grid, "lu4_trial_ms": i.lu4_trial_ms,
+                "classes": [{"bits": c.bits, "items": c.items, "cells": c.cells, "block": c.block, "grid": c.grid,
+                             "trial_ms": c.trial_ms} for c in i.cls[:i.classes]]}
+
+    def __del__(self):
+        if getattr(self, "handle", None) and lib is not None:
+            lib.lf_ragged_plan_destroy(self.handle)
+            self.handle = None
 
 
 class PinnedArray:

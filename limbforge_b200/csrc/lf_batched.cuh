@@ -23,9 +23,12 @@ template <int N> __device__ __forceinline__ Num<N> mag_of(const Cpx<N>& z) {    
     return mag_cmp<N>(z.re, z.im) >= 0 ? z.re : z.im;
 }
 
-template <int N> __global__ void __launch_bounds__(64) lu4_kernel(Lu4Params p) {
-    const u64 m = (u64)blockIdx.x * 64 + threadIdx.x;
-    if (m >= p.count) return;
+// One thread per system; a grid-stride loop, so any grid and block size (up to 256) covers the batch.
+template <int N> __device__ void lu4_system(const Lu4Params& p, u64 m);
+template <int N> __global__ void __launch_bounds__(256) lu4_kernel(Lu4Params p) {
+    for (u64 m = (u64)blockIdx.x * blockDim.x + threadIdx.x; m < p.count; m += (u64)gridDim.x * blockDim.x) lu4_system<N>(p, m);
+}
+template <int N> __device__ void lu4_system(const Lu4Params& p, u64 m) {
     constexpr u64 CE = 2 * (N + 3);
     Cpx<N> a[16];
     for (int i = 0; i < 16; ++i) a[i] = cload<N>(p.A + (m * 16 + i) * CE);
@@ -77,63 +80,105 @@ template <int N> __global__ void __launch_bounds__(64) lu4_kernel(Lu4Params p) {
     }
 }
 
-struct SgParams {
-    const u32* A; const u32* B; u32* C;
-    u64 count, m, n, k, sa, sb, sc;
-    int accumulate, fused, negative;
+// GEMM work of one launch.  Ragged form (items != nullptr): output cells of every item of one
+// precision class numbered consecutively (item t owns cells [cell0, cell0 + m n)), cut into chunks of
+// `chunk` cells, and chunk_item[c] the item that owns the first cell of chunk c; operands are word
+// offsets from `base`.  Uniform form (items == nullptr): the StridedGemm shape below.  With `counter`
+// the kernel is persistent (blocks take chunks from the counter until none are left); without it
+// block b computes chunk b.  With out_override every output cell g goes to out_override + g * S
+// instead of its C (the autotuner's trial runs leave the caller's outputs untouched).
+struct GemmItem { u64 a, b, c, cell0; u32 m, n, k, flags; };          // flags: 1 accumulate, 2 negative
+struct GemmWork {
+    const GemmItem* items; const u32* chunk_item; const u32* base;
+    u64 cells; u32 nchunks, chunk;
+    u32* counter; u32* out_override; u32* out_base;
+    const u32* A; const u32* B; u32* C; u64 m, n, k, sa, sb, sc; int accumulate, negative;
 };
-// One thread per output entry (instance t, row i, column j): sum over ascending k of
-// (composed) add(mul(a,b), sum) / cadd(cmul(a,b), sum), or (fused) fma / cfma; negated at the end.
-template <int N, bool CX, bool FUSED> __global__ void __launch_bounds__(128) strided_gemm_kernel(SgParams p) {
-    const u64 q = (u64)blockIdx.x * 128 + threadIdx.x;
-    const u64 cells = p.m * p.n;
-    if (q >= p.count * cells) return;
-    const u64 t = q / cells, cell = q % cells, i = cell / p.n, j = cell % p.n;
+// One output entry: sum over ascending k of (composed) add(mul(a,b), sum) / cadd(cmul(a,b), sum), or
+// (fused) fma / cfma, starting from C (accumulate) or zero; negated at the end.
+template <int N, bool CX, bool FUSED> __device__ __forceinline__ void gemm_cell(const u32* A, const u32* B, const u32* in, u32* out,
+                                                                              u64 n, u64 k, u64 i, u64 j, bool accumulate, bool negative) {
     constexpr u64 E = N + 3, S = CX ? 2 * E : E;
-    u32* out = p.C + (t * p.sc + cell) * S;
     if constexpr (CX) {
-        Cpx<N> sum = p.accumulate ? cload_plain<N>(out) : Cpx<N>{zero<N>(), zero<N>()};
-        for (u64 kk = 0; kk < p.k; ++kk) {
-            const Cpx<N> x = cload<N>(p.A + (t * p.sa + i * p.k + kk) * S);
-            const Cpx<N> y = cload<N>(p.B + (t * p.sb + kk * p.n + j) * S);
+        Cpx<N> sum = accumulate ? cload_plain<N>(in) : Cpx<N>{zero<N>(), zero<N>()};
+        for (u64 kk = 0; kk < k; ++kk) {
+            const Cpx<N> x = cload<N>(A + (i * k + kk) * S);
+            const Cpx<N> y = cload<N>(B + (kk * n + j) * S);
             if constexpr (FUSED) sum = cfma<N>(x, y, sum); else sum = cadd<N>(cmul<N>(x, y), sum);
         }
-        if (p.negative) sum = {negate<N>(sum.re), negate<N>(sum.im)};
+        if (negative) sum = {negate<N>(sum.re), negate<N>(sum.im)};
         cstore<N>(out, sum);
     } else {
-        Num<N> sum = p.accumulate ? load_plain<N>(out) : zero<N>();
-        for (u64 kk = 0; kk < p.k; ++kk) {
-            const Num<N> x = load<N>(p.A + (t * p.sa + i * p.k + kk) * S);
-            const Num<N> y = load<N>(p.B + (t * p.sb + kk * p.n + j) * S);
+        Num<N> sum = accumulate ? load_plain<N>(in) : zero<N>();
+        for (u64 kk = 0; kk < k; ++kk) {
+            const Num<N> x = load<N>(A + (i * k + kk) * S);
+            const Num<N> y = load<N>(B + (kk * n + j) * S);
             if constexpr (FUSED) sum = fma<N>(x, y, sum); else sum = addx<N>(mulx<N>(x, y), sum);
         }
-        if (p.negative) sum = negate<N>(sum);
+        if (negative) sum = negate<N>(sum);
         store<N>(out, sum);
     }
 }
+template <int N, bool CX, bool FUSED> __global__ void __launch_bounds__(256) gemm_kernel(GemmWork p) {
+    constexpr u64 E = N + 3, S = CX ? 2 * E : E;
+    __shared__ u32 s_chunk;
+    for (u32 round = 0;; ++round) {
+        u32 c;
+        if (p.counter) {
+            __syncthreads();                                        // everyone has read the previous chunk index
+            if (threadIdx.x == 0) s_chunk = atomicAdd(p.counter, 1u);
+            __syncthreads();
+            c = s_chunk;
+        } else {
+            if (round) return;
+            c = blockIdx.x;
+        }
+        if (c >= p.nchunks) return;
+        const u64 g = (u64)c * p.chunk + threadIdx.x;
+        if (threadIdx.x >= p.chunk || g >= p.cells) continue;
+        if (p.items) {
+            u32 t = p.chunk_item[c];
+            GemmItem it = p.items[t];
+            while (g >= it.cell0 + (u64)it.m * it.n) it = p.items[++t];   // owner of cell g (empty items skipped)
+            const u64 cell = g - it.cell0, i = cell / it.n, j = cell % it.n;
+            const u32* in = p.base + it.c + cell * S;
+            u32* out = p.out_override ? p.out_override + g * S : p.out_base + it.c + cell * S;
+            gemm_cell<N, CX, FUSED>(p.base + it.a, p.base + it.b, in, out, it.n, it.k, i, j, it.flags & 1, it.flags & 2);
+        } else {
+            const u64 cells = p.m * p.n, t = g / cells, cell = g % cells;
+            u32* out = p.C + (t * p.sc + cell) * S;
+            gemm_cell<N, CX, FUSED>(p.A + t * p.sa * S, p.B + t * p.sb * S, out, out, p.n, p.k, cell / p.n, cell % p.n,
+                                    p.accumulate, p.negative);
+        }
+    }
+}
 
-template <int N> int launch_lu4_n(const Lu4Params& p, cudaStream_t s) {
+// Launchers.  grid == 0 asks for the number of resident blocks per SM at this block size instead.
+template <int N> int launch_lu4_n(const Lu4Params& p, unsigned grid, unsigned block, cudaStream_t s) {
+    if (!grid) { int b = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lu4_kernel<N>, (int)block, 0); return b; }
     if (!p.count) return 0;
-    lu4_kernel<N><<<(unsigned)((p.count + 63) / 64), 64, 0, s>>>(p);
+    lu4_kernel<N><<<grid, block, 0, s>>>(p);
     return 0;
 }
-template <int N> int launch_sg_n(bool cx, const SgParams& p, cudaStream_t s) {
-    const u64 total = p.count * p.m * p.n;
-    if (!total) return 0;
-    const unsigned blocks = (unsigned)((total + 127) / 128);
-    if (cx) { if (p.fused) strided_gemm_kernel<N, true, true><<<blocks, 128, 0, s>>>(p); else strided_gemm_kernel<N, true, false><<<blocks, 128, 0, s>>>(p); }
-    else { if (p.fused) strided_gemm_kernel<N, false, true><<<blocks, 128, 0, s>>>(p); else strided_gemm_kernel<N, false, false><<<blocks, 128, 0, s>>>(p); }
+template <int N, bool CX, bool FUSED> int launch_gemm_v(const GemmWork& p, unsigned grid, unsigned block, cudaStream_t s) {
+    if (!grid) { int b = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, gemm_kernel<N, CX, FUSED>, (int)block, 0); return b; }
+    if (!p.nchunks) return 0;
+    gemm_kernel<N, CX, FUSED><<<grid, block, 0, s>>>(p);
     return 0;
 }
-typedef int (*Lu4Launcher)(const Lu4Params&, cudaStream_t);
-typedef int (*SgLauncher)(bool, const SgParams&, cudaStream_t);
+template <int N> int launch_gemm_n(bool cx, bool fused, const GemmWork& p, unsigned grid, unsigned block, cudaStream_t s) {
+    if (cx) return fused ? launch_gemm_v<N, true, true>(p, grid, block, s) : launch_gemm_v<N, true, false>(p, grid, block, s);
+    return fused ? launch_gemm_v<N, false, true>(p, grid, block, s) : launch_gemm_v<N, false, false>(p, grid, block, s);
+}
+typedef int (*Lu4Launcher)(const Lu4Params&, unsigned grid, unsigned block, cudaStream_t);
+typedef int (*GemmLauncher)(bool cx, bool fused, const GemmWork&, unsigned grid, unsigned block, cudaStream_t);
 Lu4Launcher lu4_launcher(int limbs);
-SgLauncher sg_launcher(int limbs);
+GemmLauncher gemm_launcher(int limbs);
 
 }  // namespace lfd
 
 #define LF_BATCHED_INSTANTIATE(N)                                                                   \
     namespace lfd {                                                                                 \
-    int lu4_launch_##N(const Lu4Params& p, cudaStream_t s) { return launch_lu4_n<N>(p, s); }        \
-    int sg_launch_##N(bool cx, const SgParams& p, cudaStream_t s) { return launch_sg_n<N>(cx, p, s); } \
+    int lu4_launch_##N(const Lu4Params& p, unsigned g, unsigned b, cudaStream_t s) { return launch_lu4_n<N>(p, g, b, s); } \
+    int gemm_launch_##N(bool cx, bool f, const GemmWork& p, unsigned g, unsigned b, cudaStream_t s) { return launch_gemm_n<N>(cx, f, p, g, b, s); } \
     }

@@ -11,19 +11,24 @@ void launch_lu4(int bits, const lf_batched4& s, const void* A, const void* B, vo
     if (!s.count) return;
     lfd::Lu4Params p{static_cast<const uint32_t*>(A), static_cast<const uint32_t*>(B), static_cast<uint32_t*>(X),
                      static_cast<uint32_t*>(det), status, s.count, s.rhs, s.fused, s.determinant, s.inverse};
-    lfd::lu4_launcher(bits / 32)(p, st);
+    lfd::lu4_launcher(bits / 32)(p, (unsigned)((s.count + 63) / 64), 64, st);
     cuda_check(cudaGetLastError(), "lu4 launch");
 }
 void launch_strided_gemm(int bits, bool complex, const lf_strided_gemm& s, const void* A, const void* B, void* C,
                          cudaStream_t st) {
-    lfd::SgParams p{static_cast<const uint32_t*>(A), static_cast<const uint32_t*>(B), static_cast<uint32_t*>(C),
-                    s.count, s.m, s.n, s.k, s.stride_a, s.stride_b, s.stride_c, s.accumulate, s.fused, s.negative};
-    lfd::sg_launcher(bits / 32)(complex, p, st);
+    lfd::GemmWork p{};
+    p.A = static_cast<const uint32_t*>(A); p.B = static_cast<const uint32_t*>(B); p.C = static_cast<uint32_t*>(C);
+    p.m = s.m; p.n = s.n; p.k = s.k; p.sa = s.stride_a; p.sb = s.stride_b; p.sc = s.stride_c;
+    p.accumulate = s.accumulate; p.negative = s.negative;
+    p.cells = (uint64_t)s.count * s.m * s.n;
+    p.chunk = 128;
+    p.nchunks = (uint32_t)((p.cells + 127) / 128);
+    if (!p.nchunks) return;
+    lfd::gemm_launcher(bits / 32)(complex, s.fused != 0, p, p.nchunks, 128, st);
     cuda_check(cudaGetLastError(), "strided gemm launch");
 }
 
-struct Lu4Sizes { size_t A, B, X, det, status; };
-static Lu4Sizes lu4_elements(int bits, const lf_batched4& s) {                         // engine.mm lu4_elements
+Lu4Sizes lu4_elements(int bits, const lf_batched4& s) {                         // engine.mm lu4_elements
     validate(bits, s.count);
     if (s.count > 0xffffffffull / 16) throw invalid_argument("batched 4x4 exceeds 32-bit indexing");
     if (s.inverse && s.rhs) throw invalid_argument("inverse uses no right-hand sides");

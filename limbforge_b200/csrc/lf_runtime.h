@@ -43,6 +43,14 @@ inline size_t element_bytes(int bits, bool complex) { return size_t(bits / 8 + 1
 // Grow-only device allocation owned by one engine (scratch for host-array calls).
 struct DevBuf {
     void* p = nullptr; size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { if (p) cudaFree(p); p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0; }
+        return *this;
+    }
     void* get(size_t n) {
         if (n > bytes) {
             if (p) cudaFree(p);
@@ -120,6 +128,10 @@ void launch_lu4(int bits, const lf_batched4& shape, const void* A, const void* B
                 cudaStream_t s);
 void launch_strided_gemm(int bits, bool complex, const lf_strided_gemm& s, const void* A, const void* B, void* C,
                          cudaStream_t st);
+// Element counts of the operands of a batched 4x4 job (A, B, X, det, status), validated as
+// Engine::lu4 validates them (engine.mm lu4_elements).
+struct Lu4Sizes { size_t A, B, X, det, status; };
+Lu4Sizes lu4_elements(int bits, const lf_batched4& s);
 
 }  // namespace lfr
 
