@@ -32,7 +32,7 @@ sys.path.insert(0, ROOT)
 BITS, COUNT, CHAIN = 1024, 65536, 16
 METRIC = "1024-bit ops/s; exact GEMM MAC/s int8-CRT vs limb kernel, 1 B200, bit-exact"
 UNIT = "1024-bit ops/s"
-WORKLOAD = "1024-bit (32-limb) 16-step RNE multiplication chains over 65,536 values (configs[1])"
+WORKLOAD = "1024-bit (32-limb) 16-step RNE multiplication chains over 65,536 values"
 ELEMENT_BYTES = BITS // 8 + 12
 # ncu: dram__bytes_read.sum + dram__bytes_write.sum of one chain_kernel<32> launch
 # (profiles/chain_kernel_1024.md); None until a capture exists.
@@ -40,7 +40,7 @@ TRAFFIC_BYTES = None
 
 
 def make_inputs(seed: int = 20261203):
-    """Seeded synthetic data with the configs[1] distribution: significands uniform with the
+    """Seeded synthetic data of the chain workload: significands uniform with the
     top bit set, exponents uniform in [-8, 8], 1% exact zeros, 2% sparse significands."""
     from limbforge_b200 import numbers as nb
     rng = np.random.default_rng(seed)
@@ -154,6 +154,302 @@ def run_reference(args, rank, world):
                          "sample": f"{sample} of {COUNT} values x {CHAIN} steps per step, extrapolated"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+# ---------------------------------------------------------------- secondary workloads
+# Secondary measurements printed inside the same JSON line under "workloads" (1 GPU only): each one
+# is timed on device-resident data and checked against the oracle on a sample.
+
+def _log(msg):
+    print(f"[bench] {msg}", file=sys.stderr, flush=True)
+
+
+def _event_ms(torch, stream, fn, reps):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def _threads_rate(fn, total, threads):
+    """Runs fn(lo, hi) over [0, total) split across host threads; returns seconds."""
+    from concurrent.futures import ThreadPoolExecutor
+    cuts = np.linspace(0, total, threads + 1).astype(int)
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(lambda i: fn(cuts[i], cuts[i + 1]), range(threads)))
+    return time.perf_counter() - t0
+
+
+def elementwise_256(torch, api, hbm_peak):
+    """256-bit RNE mul, div and fma on 65,536 elements (exponents U[-256,256], 1% zeros, 2% sparse)."""
+    from limbforge_b200 import numbers as nb
+    from oracle.oracle import Oracle, Reference
+    bits, cnt = 256, 65536
+    rng = np.random.default_rng(100)
+    a, b, c = (nb.random_numbers(rng, cnt, bits, 256, zero_frac=0.01, sparse_frac=0.02) for _ in range(3))
+    da, db, dc = (torch.from_numpy(x.view(np.int32)).cuda() for x in (a, b, c))
+    do = torch.empty_like(da)
+    st = torch.cuda.Stream()
+    orc = Oracle()
+    ref = Reference() if Reference.available() else None
+    threads = os.cpu_count() or 1
+    out = {}
+    for op, name, nin in ((2, "mul", 2), (3, "div", 2), (9, "fma", 3)):
+        def go():
+            api.dev_elementwise(bits, op, da.data_ptr(), db.data_ptr(), dc.data_ptr() if nin == 3 else None, do.data_ptr(), cnt,
+                                stream=st.cuda_stream)
+        for _ in range(5):
+            go()
+        ms = _event_ms(torch, st, go, 200)
+        got = do.cpu().numpy().view(np.uint32)
+        want = orc.elementwise(bits, op, a, b, c if nin == 3 else None)
+        moved = cnt * nb.element_bytes(bits) * (nin + 1)
+        cpu = None
+        if ref is not None:
+            dt = _threads_rate(lambda lo, hi: ref.elementwise(bits, op, np.ascontiguousarray(a[lo:hi]), np.ascontiguousarray(b[lo:hi]),
+                                                              np.ascontiguousarray(c[lo:hi]) if nin == 3 else None), cnt, threads)
+            cpu = {"ops_per_s": cnt / dt, "cores": threads, "kind": "reference"}
+        out[name] = {"us": ms * 1e3, "ops_per_s": cnt / (ms * 1e-3), "GB_per_s": moved / (ms * 1e-3) / 1e9,
+                     "hbm_frac": moved / (ms * 1e-3) / 1e9 / hbm_peak, "bit_exact": bool((got == want).all()),
+                     "cpu_reference": cpu}
+    out["workload"] = "256-bit mul/div/fma, 65,536 elements per operand, device resident (launch-latency bound at this size)"
+    return out
+
+
+def cdiv_1024(torch, api):
+    """1024-bit complex division on 65,536 pairs (components as the chain's values)."""
+    from limbforge_b200 import numbers as nb
+    from oracle.oracle import Oracle
+    bits, cnt = 1024, 65536
+    rng = np.random.default_rng(101)
+    x = nb.random_complex(rng, cnt, bits, 8, zero_frac=0.01, sparse_frac=0.02)
+    y = nb.random_complex(rng, cnt, bits, 8, zero_frac=0.01, sparse_frac=0.02)
+    dx, dy = (torch.from_numpy(v.view(np.int32)).cuda() for v in (x, y))
+    dz = torch.empty_like(dx)
+    st = torch.cuda.Stream()
+
+    def go():
+        api.dev_elementwise(bits, 6, dx.data_ptr(), dy.data_ptr(), None, dz.data_ptr(), cnt, stream=st.cuda_stream)
+    for _ in range(3):
+        go()
+    ms = _event_ms(torch, st, go, 20)
+    got = dz.cpu().numpy().view(np.uint32)
+    want = Oracle().elementwise(bits, 6, np.ascontiguousarray(x[:4096]), np.ascontiguousarray(y[:4096]))
+    return {"workload": "1024-bit complex division, 65,536 pairs", "ms": ms, "pairs_per_s": cnt / (ms * 1e-3),
+            "bit_exact_sample": bool((got[:4096] == want).all()), "sample": 4096}
+
+
+def exact_gemm_512(torch, api):
+    """512-bit C <- RN(C - A^T B), A, B 1024 x 1024 (exponents U[-40,40], 0.5% zeros), residue engine
+    vs the plain limb kernel on the same device data; SYRK A^T A (lower)."""
+    from limbforge_b200 import numbers as nb
+    from oracle.oracle import Oracle, Reference
+    bits, n = 512, 1024
+    rng = np.random.default_rng(102)
+    A = nb.random_numbers(rng, n * n, bits, 40, zero_frac=0.005)
+    B = nb.random_numbers(rng, n * n, bits, 40, zero_frac=0.005)
+    C0 = nb.random_numbers(rng, n * n, bits, 40, zero_frac=0.005)
+    dA, dB, dC0 = (torch.from_numpy(v.view(np.int32)).cuda() for v in (A, B, C0))
+    eng = api.Engine()
+    la = {m: api.Linalg(eng, api.LinalgOptions(method=m)) for m in (1, 2)}
+    res, outs = {}, {}
+    for m, name in ((2, "residue"), (1, "limb")):
+        dC = dC0.clone()
+        reps = 3 if m == 2 else 1
+        times = []
+        for r in range(reps + 1):
+            dC.copy_(dC0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            la[m].dev_exact_product(bits, dA.data_ptr(), 1, n, dB.data_ptr(), 1, n, n, n, n, dC.data_ptr(), n, subtract=True)
+            torch.cuda.synchronize()
+            if r:
+                times.append(time.perf_counter() - t0)
+        t = float(np.median(times))
+        outs[name] = dC
+        res[name] = {"s": t, "mac_per_s": n ** 3 / t, "report": la[m].report()}
+    res["identical_bits"] = bool(torch.equal(outs["residue"], outs["limb"]))
+    res["speedup_residue_vs_limb"] = res["limb"]["s"] / res["residue"]["s"]
+    rep = res["residue"]["report"]
+    kp = (n + 127) // 128 * 128
+    int8_macs = 4 * rep["moduli"] * kp * kp * kp
+    res["residue"]["int8_tops_whole_call"] = 2 * int8_macs / res["residue"]["s"] / 1e12
+    # oracle on one full output row
+    got = outs["residue"].cpu().numpy().view(np.uint32)
+    row = 517
+    want = Oracle().gemm(bits, True, A, B, n, n, n, C=C0, subtract=True, rows=(row, row + 1))
+    res["oracle_row_match"] = bool((got[row * n:(row + 1) * n] == want[row * n:(row + 1) * n]).all())
+    # SYRK A^T A lower, residue engine
+    dS = torch.zeros_like(dC0)
+    times = []
+    for r in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        la[2].dev_exact_product(bits, dA.data_ptr(), 1, n, dA.data_ptr(), 1, n, n, n, n, dS.data_ptr(), n, lower=True)
+        torch.cuda.synchronize()
+        if r:
+            times.append(time.perf_counter() - t0)
+    ts = float(np.median(times))
+    res["syrk_residue"] = {"s": ts, "mac_per_s": n * n * (n + 1) / 2 / ts}
+    # the reference's exact_dot_add on all host cores over sampled outputs
+    if Reference.available():
+        ref = Reference()
+        At = np.ascontiguousarray(A.reshape(n, n, -1).transpose(1, 0, 2))        # column i of A as a row
+        Bt = np.ascontiguousarray(B.reshape(n, n, -1).transpose(1, 0, 2))
+        sample = 256
+        idx = rng.integers(0, n, size=(sample, 2))
+        threads = os.cpu_count() or 1
+
+        def work(lo, hi):
+            for i, j in idx[lo:hi]:
+                ref.exact_dot_add(bits, C0[i * n + j], True, At[i], 1, Bt[j], 1, n)
+        dt = _threads_rate(work, sample, threads)
+        res["cpu_reference"] = {"mac_per_s": sample * n / dt, "cores": threads, "kind": "reference",
+                                "sample": f"{sample} outputs of {n * n}"}
+    res["workload"] = "512-bit exact GEMM C <- RN(C - A^T B), 1024 x 1024 x 1024, device-pointer entry, synchronous call"
+    return res
+
+
+def cholesky_2048(torch, api):
+    """256-bit SPD A = RN(G^T G) + n I (n = 2048, G uniform in [-1, 1]), blocked Cholesky (block 32),
+    64 right-hand sides; scaled residual ||B - A X|| / (||A|| ||X||) from an exact residual product."""
+    from limbforge_b200 import numbers as nb
+    from oracle.oracle import Oracle
+    bits, n, nrhs = 256, 2048, 64
+    rng = np.random.default_rng(103)
+
+    def uniform(count):
+        x = nb.random_numbers(rng, count, bits, 0)
+        x[:, bits // 32] = (-rng.geometric(0.5, size=count)).astype(np.int32).view(np.uint32)
+        return x
+    G = uniform(n * n)
+    eng = api.Engine()
+    la = api.Linalg(eng)
+    A = np.zeros_like(G)
+    t0 = time.perf_counter()
+    la.syrk(bits, G, n, n, A, lower_only=False)
+    t_syrk = time.perf_counter() - t0
+    diag = np.ascontiguousarray(A[np.arange(n) * (n + 1)])
+    nn = nb.random_numbers(rng, n, bits, 0)
+    nn[:] = 0
+    nn[:, bits // 32 - 1] = 0x80000000
+    nn[:, bits // 32] = np.uint32(11)                     # 2048 = 2^11
+    nn[:, bits // 32 + 1] = 1
+    d2, _ = eng.run(bits, api.Operation.add, diag, nn)
+    A[np.arange(n) * (n + 1)] = d2
+    L = np.zeros_like(A)
+    info = la.cholesky(bits, A, n, L)
+    Bm = uniform(n * nrhs)
+    X = np.zeros_like(Bm)
+    ts = la.cholesky_solve(bits, L, n, Bm, nrhs, X)
+    # residual R = RN(B - A X) with one rounding per entry (exact GEMM), norms from the rounded values
+    R = Bm.copy()
+    la.gemm(bits, False, A, X, n, nrhs, n, R, subtract=True)
+
+    def fro(x):
+        e = nb.exponent(x).astype(np.float64)
+        top = x[:, bits // 32 - 1].astype(np.float64) / 2.0 ** 31
+        v = np.where(nb.sign(x) != 0, top * np.exp2(e - np.max(e)), 0.0)
+        return np.sqrt(np.sum(v * v)) * 2.0 ** float(np.max(e))
+    scaled = fro(R) / (fro(A) * fro(X))
+    # oracle on the leading 96 x 96 block (it depends on A's leading block only)
+    k = 96
+    Ak = np.ascontiguousarray(A.reshape(n, n, -1)[:k, :k].reshape(k * k, -1))
+    WL, winfo = Oracle().cholesky(bits, Ak, k, 32)
+    lead = np.ascontiguousarray(L.reshape(n, n, -1)[:k, :k].reshape(k * k, -1))
+    return {"workload": "256-bit blocked Cholesky n=2048 (block 32) + 64-RHS solve", "syrk_s": t_syrk,
+            "cholesky_s": info.timing.wall_seconds, "cholesky_gpu_s": info.timing.gpu_seconds,
+            "panel_s": info.panel_seconds, "update_s": info.update_seconds, "pivot": info.pivot,
+            "cholesky_mac_per_s": n ** 3 / 6 / info.timing.wall_seconds,
+            "solve_s": ts.wall_seconds, "solve_mac_per_s": n * n * nrhs / ts.wall_seconds,
+            "scaled_residual": scaled, "oracle_leading_block_match": bool((lead == WL).all() and winfo[0] == k)}
+
+
+def ragged_batch(torch, api):
+    """20,000 complex GEMMs, m, n, k uniform in {4..48}, precision uniform in {128, 256, 512, 1024},
+    plus 200,000 4x4 complex LU solves at 512 bits, as one CUDA graph launch of a tuned ragged plan."""
+    from limbforge_b200 import numbers as nb
+    from oracle.oracle import Oracle
+    rng = np.random.default_rng(104)
+    count, lu_count = 20000, 200000
+    bits = rng.choice([128, 256, 512, 1024], size=count)
+    m, n, k = (rng.integers(4, 49, size=count) for _ in range(3))
+    items = api.ragged_items(bits, m, n, k)
+    lu = api.RaggedLu4(512, api.Batched4(count=lu_count, rhs=1))
+    total = api.ragged_pack(True, items, lu)
+    arena = np.zeros(total // 4, np.uint32)
+    for it in items:
+        b, mm, nn, kk = int(it["bits"]), int(it["m"]), int(it["n"]), int(it["k"])
+        x = nb.random_complex(rng, mm * kk + kk * nn, b, 32)
+        w = x.shape[1] * x.shape[2]
+        a0, b0 = int(it["a"]) // 4, int(it["b"]) // 4
+        arena[a0:a0 + mm * kk * w] = x[:mm * kk].ravel()
+        arena[b0:b0 + kk * nn * w] = x[mm * kk:].ravel()
+    LA = nb.random_complex(rng, lu_count * 16, 512, 32).ravel()
+    LB = nb.random_complex(rng, lu_count * 4, 512, 32).ravel()
+    arena[lu.A // 4:lu.A // 4 + LA.size] = LA
+    arena[lu.B // 4:lu.B // 4 + LB.size] = LB
+    eng = api.Engine()
+    plan = api.RaggedPlan(eng, True, False, items, total, lu)
+    dev = torch.from_numpy(arena.view(np.int32)).cuda()
+    ptr = dev.data_ptr()
+    t0 = time.perf_counter()
+    plan.tune(ptr)
+    t_tune = time.perf_counter() - t0
+    st = torch.cuda.current_stream()
+    for _ in range(2):
+        plan.run(ptr, st.cuda_stream)
+    ms = _event_ms(torch, st, lambda: plan.run(ptr, st.cuda_stream), 5)
+    out = dev.cpu().numpy().view(np.uint32)
+    orc = Oracle()
+    bad, sample = 0, rng.choice(count, size=16, replace=False)
+    for t in sample:
+        it = items[t]
+        b, mm, nn, kk = int(it["bits"]), int(it["m"]), int(it["n"]), int(it["k"])
+        w = 2 * (b // 32 + 3)
+        Am = arena[int(it["a"]) // 4:int(it["a"]) // 4 + mm * kk * w].reshape(-1, 2, w // 2)
+        Bm = arena[int(it["b"]) // 4:int(it["b"]) // 4 + kk * nn * w].reshape(-1, 2, w // 2)
+        want = orc.strided_gemm(b, True, {"count": 1, "m": mm, "n": nn, "k": kk, "stride_a": 0, "stride_b": 0, "stride_c": 0},
+                                np.ascontiguousarray(Am), np.ascontiguousarray(Bm), np.zeros((mm * nn, 2, w // 2), np.uint32))
+        bad += int(not (out[int(it["c"]) // 4:int(it["c"]) // 4 + want.size] == want.ravel()).all())
+    ls = rng.choice(lu_count, size=64, replace=False)
+    Aall = arena[lu.A // 4:lu.A // 4 + LA.size].reshape(lu_count, 16, 2, 19)
+    Ball = arena[lu.B // 4:lu.B // 4 + LB.size].reshape(lu_count, 4, 2, 19)
+    X, _, stt = orc.lu4(512, 64, 1, 0, np.ascontiguousarray(Aall[ls]), np.ascontiguousarray(Ball[ls]))
+    Xg = out[lu.X // 4:lu.X // 4 + lu_count * 4 * 38].reshape(lu_count, 4, 2, 19)[ls]
+    Sg = out[lu.status // 4:lu.status // 4 + lu_count][ls]
+    lu_ok = bool((Xg.reshape(64, -1) == X.reshape(64, -1)).all() and (Sg == stt).all())
+    word_macs = float(np.sum(m.astype(np.float64) * n * k * 4 * (bits // 32) ** 2))
+    return {"workload": "20,000 ragged complex GEMMs (m,n,k U{4..48}, bits U{128,256,512,1024}) + 200,000 4x4 LU at 512 bits, one graph launch",
+            "graph_ms": ms, "instances_per_s": count / (ms * 1e-3), "lu4_systems_per_s_if_alone": None,
+            "gemm_word_macs_per_s": word_macs / (ms * 1e-3), "complex_macs": float(np.sum(m.astype(np.float64) * n * k)),
+            "arena_bytes": int(total), "tune_s": t_tune, "plan": plan.info(),
+            "oracle_sample_mismatches": bad, "oracle_sample": int(len(sample)), "lu4_oracle_sample_match": lu_ok}
+
+
+def run_workloads(args):
+    import torch
+    from limbforge_b200 import api
+    hbm_peak, _ = peaks()
+    out = {}
+    for name, fn in (("mul_div_fma_256bit_65536", lambda: elementwise_256(torch, api, hbm_peak)),
+                     ("cdiv_1024bit_65536", lambda: cdiv_1024(torch, api)),
+                     ("exact_gemm_512bit_1024", lambda: exact_gemm_512(torch, api)),
+                     ("cholesky_256bit_2048", lambda: cholesky_2048(torch, api)),
+                     ("ragged_batch_20000", lambda: ragged_batch(torch, api))):
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn()
+        except Exception as e:                       # reported, never hidden
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        _log(f"{name} done in {time.perf_counter() - t0:.1f} s")
+        torch.cuda.empty_cache()
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -272,6 +568,8 @@ def run_ours(args, rank, world, local_rank):
         "cpu_baseline": {"value": cpu_rate, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": f"{sample} of {COUNT} values x {CHAIN} steps, extrapolated"},
     }
+    if world == 1 and not args.no_workloads:
+        line["workloads"] = run_workloads(args)
     print(json.dumps(line), flush=True)
 
 
@@ -281,7 +579,8 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--count", type=int, default=65536, help="values per chain (65,536 is the configs[1] workload)")
+    ap.add_argument("--count", type=int, default=65536, help="values per chain (65,536 is the headline workload)")
+    ap.add_argument("--no-workloads", action="store_true", help="skip the secondary workloads")
     args = ap.parse_args()
     global COUNT
     COUNT = args.count

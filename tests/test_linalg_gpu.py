@@ -120,9 +120,9 @@ def test_saturated_sums_and_tight_bounds(la, oracle):
         K = K * 2 + (K % 3 == 1)
 
 
-def test_config2_gemm_update_sampled(la, oracle):
-    """512-bit A^T B update on a 1024 x 1024 x 1024 problem with exponents in [-40, 40] and 0.5% zeros
-    (configs[2]): every output computed on the GPU, 16 full rows checked against the oracle, and the
+def test_gemm_update_512bit_1024_sampled(la, oracle):
+    """512-bit A^T B update on a 1024 x 1024 x 1024 problem with exponents in [-40, 40] and 0.5% zeros:
+    every output computed on the GPU, 16 full rows checked against the oracle, and the
     SYRK lower triangle sampled too."""
     bits, n = 512, 1024
     rng = np.random.default_rng(2)
