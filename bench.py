@@ -34,9 +34,9 @@ METRIC = "1024-bit ops/s; exact GEMM MAC/s int8-CRT vs limb kernel, 1 B200, bit-
 UNIT = "1024-bit ops/s"
 WORKLOAD = "1024-bit (32-limb) 16-step RNE multiplication chains over 65,536 values"
 ELEMENT_BYTES = BITS // 8 + 12
-# ncu: dram__bytes_read.sum + dram__bytes_write.sum of one chain_kernel<32> launch
-# (profiles/chain_kernel_1024.md); None until a capture exists.
-TRAFFIC_BYTES = None
+# ncu: dram__bytes_read.sum + dram__bytes_write.sum of one chain_kernel<32> launch of this workload
+# (profiles/chain_kernel_1024bit_65536.md: 155,325,440 + 4,717,312 bytes).
+TRAFFIC_BYTES = 160042752
 
 
 def make_inputs(seed: int = 20261203):
@@ -370,13 +370,14 @@ def cholesky_2048(torch, api):
             "scaled_residual": scaled, "oracle_leading_block_match": bool((lead == WL).all() and winfo[0] == k)}
 
 
-def ragged_batch(torch, api):
+def ragged_batch(torch, api, scale=1.0):
     """20,000 complex GEMMs, m, n, k uniform in {4..48}, precision uniform in {128, 256, 512, 1024},
-    plus 200,000 4x4 complex LU solves at 512 bits, as one CUDA graph launch of a tuned ragged plan."""
+    plus 200,000 4x4 complex LU solves at 512 bits, as one CUDA graph launch of a tuned ragged plan
+    (`scale` shrinks both counts, for profiling captures)."""
     from limbforge_b200 import numbers as nb
     from oracle.oracle import Oracle
     rng = np.random.default_rng(104)
-    count, lu_count = 20000, 200000
+    count, lu_count = max(16, int(20000 * scale)), max(64, int(200000 * scale))
     bits = rng.choice([128, 256, 512, 1024], size=count)
     m, n, k = (rng.integers(4, 49, size=count) for _ in range(3))
     items = api.ragged_items(bits, m, n, k)
@@ -425,7 +426,7 @@ def ragged_batch(torch, api):
     Sg = out[lu.status // 4:lu.status // 4 + lu_count][ls]
     lu_ok = bool((Xg.reshape(64, -1) == X.reshape(64, -1)).all() and (Sg == stt).all())
     word_macs = float(np.sum(m.astype(np.float64) * n * k * 4 * (bits // 32) ** 2))
-    return {"workload": "20,000 ragged complex GEMMs (m,n,k U{4..48}, bits U{128,256,512,1024}) + 200,000 4x4 LU at 512 bits, one graph launch",
+    return {"workload": f"{count} ragged complex GEMMs (m,n,k U{{4..48}}, bits U{{128,256,512,1024}}) + {lu_count} 4x4 LU at 512 bits, one graph launch",
             "graph_ms": ms, "instances_per_s": count / (ms * 1e-3), "lu4_systems_per_s_if_alone": None,
             "gemm_word_macs_per_s": word_macs / (ms * 1e-3), "complex_macs": float(np.sum(m.astype(np.float64) * n * k)),
             "arena_bytes": int(total), "tune_s": t_tune, "plan": plan.info(),
@@ -441,7 +442,9 @@ def run_workloads(args):
                      ("cdiv_1024bit_65536", lambda: cdiv_1024(torch, api)),
                      ("exact_gemm_512bit_1024", lambda: exact_gemm_512(torch, api)),
                      ("cholesky_256bit_2048", lambda: cholesky_2048(torch, api)),
-                     ("ragged_batch_20000", lambda: ragged_batch(torch, api))):
+                     ("ragged_batch_20000", lambda: ragged_batch(torch, api, args.scale))):
+        if args.workload and name != args.workload:
+            continue
         t0 = time.perf_counter()
         try:
             out[name] = fn()
@@ -581,6 +584,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--count", type=int, default=65536, help="values per chain (65,536 is the headline workload)")
     ap.add_argument("--no-workloads", action="store_true", help="skip the secondary workloads")
+    ap.add_argument("--workload", default="", help="run only this secondary workload and print its JSON (profiling)")
+    ap.add_argument("--scale", type=float, default=1.0, help="size factor of the ragged batch (profiling captures)")
     args = ap.parse_args()
     global COUNT
     COUNT = args.count
@@ -589,6 +594,11 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload:
+        import torch
+        torch.cuda.set_device(local_rank)
+        print(json.dumps(run_workloads(args)), flush=True)
         return
     if world > 1:
         import datetime
