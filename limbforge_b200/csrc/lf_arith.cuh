@@ -173,17 +173,97 @@ template <int N> __device__ __forceinline__ Num<N> round_product(const u32 (&p)[
     // (when s = 1 the bit shifted out of p[N-1] went into m[0], not lost)
     return finish<N>(m, e_sum + 1 - (i64)s, sign, (low >> 31) && (sticky || (m[0] & 1u)), status);
 }
-template <int N> __device__ __forceinline__ Num<N> mul(const Num<N>& a, const Num<N>& b) {
+// RN(a * b) from the full 2N-word product.
+template <int N> __device__ __forceinline__ Num<N> mul_exact(const Num<N>& a, const Num<N>& b) {
     const u32 st = a.st | b.st;
     if (st || !a.s || !b.s) return zero<N>(st);
     u32 p[2 * N];
     mant_mul<N>(a.m, b.m, p);
     return round_product<N>(p, (i64)a.e + b.e, a.s * b.s, 0);
 }
+template <int N> __device__ __noinline__ Num<N> mul_exact_call(const Num<N> a, const Num<N> b) { return mul_exact<N>(a, b); }
+
+// Upper part of the product: h = T / 2^(32(N-2)) with T = sum of a_i b_j 2^(32(i+j)) over i + j >= N-2
+// (words N-2 .. 2N-1; about 58% of the word products at N = 32).  The omitted products sum to
+// D = sum_{i+j <= N-3} a_i b_j 2^(32(i+j)) < (N-2) 2^(32(N-1)) (1 + 2^-31), so the full product is T + D
+// with D less than N units of word N-1.  Row carries follow mant_mul: T through row i is at most the
+// full partial product, below 2^(32(i+N+1)), so the last high-half step of a row cannot carry out.
+template <int N> __device__ __forceinline__ void mant_mul_high(const u32 (&a)[N], const u32 (&b)[N], u32 (&h)[N + 2]) {
+    constexpr int B = N - 2;
+#pragma unroll
+    for (int k = 0; k < N + 2; ++k) h[k] = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const int j0 = B - i > 0 ? B - i : 0;
+        h[i + j0 - B] = mad_lo_cc(a[i], b[j0], h[i + j0 - B]);
+#pragma unroll
+        for (int j = j0 + 1; j < N; ++j) h[i + j - B] = madc_lo_cc(a[i], b[j], h[i + j - B]);
+        h[i + N - B] = carry_out();
+        h[i + j0 + 1 - B] = mad_hi_cc(a[i], b[j0], h[i + j0 + 1 - B]);
+#pragma unroll
+        for (int j = j0 + 1; j < N - 1; ++j) h[i + j + 1 - B] = madc_hi_cc(a[i], b[j], h[i + j + 1 - B]);
+        h[i + N - B] = madc_hi(a[i], b[N - 1], h[i + N - B]);
+    }
+}
+
+// RN(a * b).  From N = 12 limbs on, the rounding is decided from the upper part T of the product when
+// that is safe, and from the full product otherwise.  With s the normalizing shift, word N-1 of T
+// shifted left by s holds the round bit (bit 31) and, below it, `low`.  The omitted part D adds less
+// than N units to word N-1 (at most 2N after the shift), so when low + 2N stays below 2^31 every bit
+// from the round bit up is exact.  Then a clear round bit rounds down, and a set round bit with low != 0
+// rounds up: the discarded bits are nonzero, so there is no tie.  Any other case (a carry could reach
+// the round bit, or the sticky bits depend on D) takes the full product: for random operands about
+// once in 2^25 products.
+constexpr int kShortMulLimbs = 12;
+template <int N> __device__ __forceinline__ Num<N> mul(const Num<N>& a, const Num<N>& b) {
+    if constexpr (N < kShortMulLimbs) {
+        return mul_exact<N>(a, b);
+    } else {
+        const u32 st = a.st | b.st;
+        if (st || !a.s || !b.s) return zero<N>(st);
+        u32 h[N + 2];
+        mant_mul_high<N>(a.m, b.m, h);
+        const u32 s = (h[N + 1] >> 31) ? 0u : 1u;
+        const u32 lw = h[1] << s;
+        const u32 low = lw & 0x7fffffffu;
+        const bool rb = lw >> 31;
+        if (low >= 0x80000000u - ((u32)N << s) || (rb && low == 0)) return mul_exact_call<N>(a, b);
+        u32 m[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) m[i] = __funnelshift_l(h[i + 1], h[i + 2], s);
+        return finish<N>(m, (i64)a.e + b.e + 1 - (i64)s, a.s * b.s, rb, 0);
+    }
+}
 
 // ---------------------------------------------------------------- add / sub
-// x = larger magnitude, y = smaller; window of 2N+3 words: x at words [N+2, 2N+1], y below it
-// at bit offset 32(N+2)-gap (gap <= 32N+2 keeps y whole); one rounding of the exact sum.
+// Words of x moved down by q words (q in [0, 2^stages)), zeros shifted in; every word shifted out is
+// ORed into `sticky` (branch-free barrel shifter, like shift_up_words).
+template <int W, int STAGES> __device__ __forceinline__ void shift_down_words(u32 (&x)[W], u32 q, u32& sticky) {
+#pragma unroll
+    for (int b = 0; b < STAGES; ++b) {
+        const int s = 1 << b;
+        const bool on = (q >> b) & 1u;
+#pragma unroll
+        for (int k = 0; k < (s < W ? s : W); ++k) sticky |= on ? x[k] : 0u;
+#pragma unroll
+        for (int k = 0; k < W; ++k) x[k] = on ? (k + s < W ? x[k + s] : 0u) : x[k];
+    }
+}
+template <int W> __device__ __forceinline__ void shift_down_bits(u32 (&x)[W], u32 r, u32& sticky) {   // r < 32
+    sticky |= r ? (x[0] << (32 - r)) : 0u;
+#pragma unroll
+    for (int k = 0; k < W - 1; ++k) x[k] = __funnelshift_r(x[k], x[k + 1], r);
+    x[W - 1] = x[W - 1] >> r;
+}
+
+// RN(a + b).  x = the larger magnitude, y = the smaller, gap = e_x - e_y.  Window of N + 4 words:
+// x's significand at words [3, N+2] (three words below it, one word of headroom above).  y is aligned
+// by shifting it down gap bits from x's position.  When gap <= 96 all of y stays in the window and the
+// sum is exact.  Otherwise the bits shifted out are nonzero only if `lost` is set, and
+// x +- y = V + phi with V = x + y_t or x - y_t - lost (y_t the kept part) and 0 <= phi < 1 (phi > 0 iff
+// lost).  Setting bit 0 of V to lost then gives every bit that the rounding reads.  The result is at least
+// x/2 here, so its round bit lies at bit 94 or higher, far above bit 0.  gap > 32N+2 returns x: y is below a
+// quarter ulp of x, and RN(x +- y) = x.
 template <int N> __device__ __forceinline__ Num<N> add(const Num<N>& a, const Num<N>& b) {
     const u32 st = a.st | b.st;
     if (st) return zero<N>(st);
@@ -194,23 +274,25 @@ template <int N> __device__ __forceinline__ Num<N> add(const Num<N>& a, const Nu
     const Num<N> y = pick<N>(swap, a, b);
     const i64 gap = (i64)x.e - y.e;
     if (gap > 32 * N + 2) return x;
-    constexpr int W = 2 * N + 3;
+    constexpr int W = N + 4;
     u32 w[W], v[W];
 #pragma unroll
-    for (int k = 0; k < W; ++k) { w[k] = (k >= N + 2 && k < 2 * N + 2) ? x.m[k - N - 2] : 0u; v[k] = k < N ? y.m[k] : 0u; }
-    const u32 sh = (u32)(32 * (N + 2) - gap);           // in [62, 32N+64]
-    shift_up_bits<W>(v, sh & 31u);
-    shift_up_words<W, stages_for<W>()>(v, sh >> 5);
+    for (int k = 0; k < W; ++k) { w[k] = (k >= 3 && k < N + 3) ? x.m[k - 3] : 0u; v[k] = (k >= 3 && k < N + 3) ? y.m[k - 3] : 0u; }
+    u32 lost = 0;
+    shift_down_bits<W>(v, (u32)gap & 31u, lost);
+    shift_down_words<W, stages_for<W>()>(v, (u32)gap >> 5, lost);
+    const u32 l = lost ? 1u : 0u;
     if (x.s == y.s) {
         u64 c = 0;
 #pragma unroll
         for (int k = 0; k < W; ++k) { u64 t = (u64)w[k] + v[k] + c; w[k] = (u32)t; c = t >> 32; }
     } else {
-        u32 bo = 0;
+        u32 bo = l;                                         // x - y_t - lost
 #pragma unroll
         for (int k = 0; k < W; ++k) { u64 t = (u64)v[k] + bo; u32 old = w[k]; w[k] = (u32)((u64)old - t); bo = (u64)old < t; }
     }
-    return round_general<N, W>(w, (i64)x.e - (32 * N - 1) - 32 * (N + 2), x.s, 0);
+    w[0] |= l;
+    return round_general<N, W>(w, (i64)x.e - (32 * N - 1) - 96, x.s, 0);
 }
 template <int N> __device__ __forceinline__ Num<N> sub(const Num<N>& a, const Num<N>& b) { return add<N>(a, negate<N>(b)); }
 

@@ -80,9 +80,10 @@ template <int N> __device__ void lu4_system(const Lu4Params& p, u64 m) {
     }
 }
 
-// GEMM work of one launch.  Ragged form (items != nullptr): output cells of every item of one
-// precision class numbered consecutively (item t owns cells [cell0, cell0 + m n)), cut into chunks of
-// `chunk` cells, and chunk_item[c] the item that owns the first cell of chunk c; operands are word
+// GEMM work of one launch.  Work units are output entries (real) or entry components (complex: unit g
+// is component g & 1 of entry g >> 1); `cells` counts units.  Ragged form (items != nullptr): entries of
+// every item of one precision class numbered consecutively (item t owns entries [cell0, cell0 + m n)),
+// units cut into chunks of `chunk`, and chunk_item[c] the item owning the first unit of chunk c; operands are word
 // offsets from `base`.  Uniform form (items == nullptr): the StridedGemm shape below.  With `counter`
 // the kernel is persistent (blocks take chunks from the counter until none are left); without it
 // block b computes chunk b.  With out_override every output cell g goes to out_override + g * S
@@ -94,30 +95,52 @@ struct GemmWork {
     u32* counter; u32* out_override; u32* out_base;
     const u32* A; const u32* B; u32* C; u64 m, n, k, sa, sb, sc; int accumulate, negative;
 };
-// One output entry: sum over ascending k of (composed) add(mul(a,b), sum) / cadd(cmul(a,b), sum), or
-// (fused) fma / cfma, starting from C (accumulate) or zero; negated at the end.
-template <int N, bool CX, bool FUSED> __device__ __forceinline__ void gemm_cell(const u32* A, const u32* B, const u32* in, u32* out,
-                                                                              u64 n, u64 k, u64 i, u64 j, bool accumulate, bool negative) {
-    constexpr u64 E = N + 3, S = CX ? 2 * E : E;
-    if constexpr (CX) {
-        Cpx<N> sum = accumulate ? cload_plain<N>(in) : Cpx<N>{zero<N>(), zero<N>()};
-        for (u64 kk = 0; kk < k; ++kk) {
-            const Cpx<N> x = cload<N>(A + (i * k + kk) * S);
-            const Cpx<N> y = cload<N>(B + (kk * n + j) * S);
-            if constexpr (FUSED) sum = cfma<N>(x, y, sum); else sum = cadd<N>(cmul<N>(x, y), sum);
-        }
-        if (negative) sum = {negate<N>(sum.re), negate<N>(sum.im)};
-        cstore<N>(out, sum);
+// One output entry (real) or one component of one (complex: comp 0 = re, 1 = im), summed over
+// ascending k from C (accumulate) or zero and negated at the end.  The components of a complex entry
+// are independent rounding sequences, so each has its own thread:
+//   composed re: add(sub(mul(ar, br), mul(ai, bi)), sum)   im: add(add(mul(ar, bi), mul(ai, br)), sum)
+//   fused    re: dot2_add(ar, br, -ai, bi, sum)             im: dot2_add(ar, bi, ai, br, sum)
+// exactly the re / im parts of cadd(cmul(a, b), sum) and cfma(a, b, sum).
+// One k step of one complex component: sum <- the composed or fused update with x = a_ik, y = b_kj.
+// Operands are loaded next to their use, so only the running sum lives across products; above 8 limbs
+// the step is an out-of-line call, which keeps the kernel's register allocation to that sum.
+template <int N, bool FUSED> __device__ __forceinline__ void cx_step_body(Num<N>& sum, const u32* x, const u32* y, int comp) {
+    constexpr u64 E = N + 3;
+    const u32* yr = y + (comp ? E : 0);                 // im swaps the roles of br and bi
+    const u32* yi = y + (comp ? 0 : E);
+    if constexpr (FUSED) {
+        const Num<N> xi = load<N>(x + E);
+        sum = dot2_add<N>(load<N>(x), load<N>(yr), comp ? xi : negate<N>(xi), load<N>(yi), sum);
     } else {
-        Num<N> sum = accumulate ? load_plain<N>(in) : zero<N>();
-        for (u64 kk = 0; kk < k; ++kk) {
-            const Num<N> x = load<N>(A + (i * k + kk) * S);
-            const Num<N> y = load<N>(B + (kk * n + j) * S);
-            if constexpr (FUSED) sum = fma<N>(x, y, sum); else sum = addx<N>(mulx<N>(x, y), sum);
-        }
-        if (negative) sum = negate<N>(sum);
-        store<N>(out, sum);
+        const Num<N> p1 = mul<N>(load<N>(x), load<N>(yr));
+        const Num<N> p2 = mul<N>(load<N>(x + E), load<N>(yi));
+        sum = add<N>(comp ? add<N>(p1, p2) : sub<N>(p1, p2), sum);
     }
+}
+template <int N, bool FUSED> __device__ __noinline__ void cx_step_call(Num<N>& sum, const u32* x, const u32* y, int comp) {
+    cx_step_body<N, FUSED>(sum, x, y, comp);
+}
+template <int N, bool FUSED> __device__ __forceinline__ void cx_step(Num<N>& sum, const u32* x, const u32* y, int comp) {
+    if constexpr (N > 8) cx_step_call<N, FUSED>(sum, x, y, comp); else cx_step_body<N, FUSED>(sum, x, y, comp);
+}
+
+template <int N, bool CX, bool FUSED> __device__ __forceinline__ void gemm_cell(const u32* A, const u32* B, const u32* in, u32* out,
+                                                                              u64 n, u64 k, u64 i, u64 j, int comp, bool accumulate,
+                                                                              bool negative) {
+    constexpr u64 E = N + 3, S = CX ? 2 * E : E;
+    Num<N> sum = accumulate ? load_plain<N>(in) : zero<N>();
+    for (u64 kk = 0; kk < k; ++kk) {
+        const u32* x = A + (i * k + kk) * S;
+        const u32* y = B + (kk * n + j) * S;
+        if constexpr (CX) {
+            cx_step<N, FUSED>(sum, x, y, comp);
+        } else {
+            const Num<N> xr = load<N>(x), yr = load<N>(y);
+            if constexpr (FUSED) sum = fma<N>(xr, yr, sum); else sum = addx<N>(mulx<N>(xr, yr), sum);
+        }
+    }
+    if (negative) sum = negate<N>(sum);
+    store<N>(out, sum);
 }
 template <int N, bool CX, bool FUSED> __global__ void __launch_bounds__(256) gemm_kernel(GemmWork p) {
     constexpr u64 E = N + 3, S = CX ? 2 * E : E;
@@ -134,20 +157,22 @@ template <int N, bool CX, bool FUSED> __global__ void __launch_bounds__(256) gem
             c = blockIdx.x;
         }
         if (c >= p.nchunks) return;
-        const u64 g = (u64)c * p.chunk + threadIdx.x;
+        const u64 g = (u64)c * p.chunk + threadIdx.x;              // work unit: an entry, or one component of one
         if (threadIdx.x >= p.chunk || g >= p.cells) continue;
+        const u64 gc = CX ? g >> 1 : g;
+        const int comp = CX ? (int)(g & 1) : 0;
         if (p.items) {
             u32 t = p.chunk_item[c];
             GemmItem it = p.items[t];
-            while (g >= it.cell0 + (u64)it.m * it.n) it = p.items[++t];   // owner of cell g (empty items skipped)
-            const u64 cell = g - it.cell0, i = cell / it.n, j = cell % it.n;
-            const u32* in = p.base + it.c + cell * S;
-            u32* out = p.out_override ? p.out_override + g * S : p.out_base + it.c + cell * S;
-            gemm_cell<N, CX, FUSED>(p.base + it.a, p.base + it.b, in, out, it.n, it.k, i, j, it.flags & 1, it.flags & 2);
+            while (gc >= it.cell0 + (u64)it.m * it.n) it = p.items[++t];   // owner of entry gc (empty items skipped)
+            const u64 cell = gc - it.cell0, i = cell / it.n, j = cell % it.n;
+            const u32* in = p.base + it.c + cell * S + comp * E;
+            u32* out = p.out_override ? p.out_override + gc * S + comp * E : p.out_base + it.c + cell * S + comp * E;
+            gemm_cell<N, CX, FUSED>(p.base + it.a, p.base + it.b, in, out, it.n, it.k, i, j, comp, it.flags & 1, it.flags & 2);
         } else {
-            const u64 cells = p.m * p.n, t = g / cells, cell = g % cells;
-            u32* out = p.C + (t * p.sc + cell) * S;
-            gemm_cell<N, CX, FUSED>(p.A + t * p.sa * S, p.B + t * p.sb * S, out, out, p.n, p.k, cell / p.n, cell % p.n,
+            const u64 cells = p.m * p.n, t = gc / cells, cell = gc % cells;
+            u32* out = p.C + (t * p.sc + cell) * S + comp * E;
+            gemm_cell<N, CX, FUSED>(p.A + t * p.sa * S, p.B + t * p.sb * S, out, out, p.n, p.k, cell / p.n, cell % p.n, comp,
                                     p.accumulate, p.negative);
         }
     }

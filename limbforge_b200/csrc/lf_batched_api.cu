@@ -20,7 +20,7 @@ void launch_strided_gemm(int bits, bool complex, const lf_strided_gemm& s, const
     p.A = static_cast<const uint32_t*>(A); p.B = static_cast<const uint32_t*>(B); p.C = static_cast<uint32_t*>(C);
     p.m = s.m; p.n = s.n; p.k = s.k; p.sa = s.stride_a; p.sb = s.stride_b; p.sc = s.stride_c;
     p.accumulate = s.accumulate; p.negative = s.negative;
-    p.cells = (uint64_t)s.count * s.m * s.n;
+    p.cells = (uint64_t)s.count * s.m * s.n * (complex ? 2 : 1);        // work units
     p.chunk = 128;
     p.nchunks = (uint32_t)((p.cells + 127) / 128);
     if (!p.nchunks) return;

@@ -77,15 +77,17 @@ struct RaggedPlan {
 
     uint64_t cell_words(int limbs) const { return uint64_t(limbs + 3) * (cx ? 2 : 1); }
 
-    // Chunk table of a class for block size b: chunk c covers cells [c b, (c+1) b), owned first by item t.
+    uint64_t units(const ClassPlan& c) const { return c.cells * (cx ? 2 : 1); }   // a thread per entry or component
+    // Chunk table of a class for block size b: chunk c covers units [c b, (c+1) b); its first unit belongs
+    // to entry (c b) / (units per entry), owned by item t.
     void build_chunks(ClassPlan& c, unsigned b, cudaStream_t s) {
         if (c.chunk_block == b) return;
-        const uint64_t nch = (c.cells + b - 1) / b;
+        const uint64_t nch = (units(c) + b - 1) / b;
         if (nch > 0x7fffffffull) throw invalid_argument("ragged batch: too many output cells in one precision");
         std::vector<uint32_t> first(nch);
         size_t t = 0;
         for (uint64_t ch = 0; ch < nch; ++ch) {
-            const uint64_t g = ch * b;
+            const uint64_t g = ch * b / (cx ? 2 : 1);
             while (g >= c.items[t].cell0 + (uint64_t)c.items[t].m * c.items[t].n) ++t;
             first[ch] = (uint32_t)t;
         }
@@ -105,7 +107,7 @@ struct RaggedPlan {
         w.chunk_item = static_cast<const uint32_t*>(c.d_chunks.p);
         w.base = static_cast<const uint32_t*>(arena);
         w.out_base = static_cast<uint32_t*>(const_cast<void*>(arena));
-        w.cells = c.cells; w.nchunks = c.nchunks; w.chunk = c.chunk_block;
+        w.cells = units(c); w.nchunks = c.nchunks; w.chunk = c.chunk_block;
         w.counter = counter; w.out_override = override_out;
         return w;
     }

@@ -88,6 +88,42 @@ def test_every_width_vs_oracle(engine, oracle, bits):
         assert same(engine.run_ternary(bits, Operation(op), ca, cb, cc)[0], oracle.elementwise(bits, op, ca, cb, cc)), f"op {op}"
 
 
+@pytest.mark.parametrize("bits", [256, 384, 512, 800, 1024])
+def test_mul_near_rounding_boundaries(engine, oracle, bits):
+    """Products whose bits around the rounding position are runs of zeros or ones, exact ties and
+    exact results: from 12 limbs on, mul decides the rounding from the upper part of the product and
+    must fall back to the full product exactly in these cases."""
+    from limbforge_b200.api import Operation
+    n = bits // 32
+    rng = np.random.default_rng(bits + 5)
+    cnt = 4096
+    a = nb.random_numbers(rng, cnt, bits, 50)
+    b = nb.random_numbers(rng, cnt, bits, 50)
+    q = cnt // 8
+    # a = 2^(32n-1) + u: the product is b shifted plus a small multiple of b
+    a[:q, :n] = 0
+    a[:q, n - 1] = 0x80000000
+    a[:q, 0] = rng.integers(0, 1 << 20, size=q)
+    # trailing words of all zeros / all ones in both operands
+    a[q:2 * q, :n // 2] = 0
+    b[q:2 * q, :n // 2] = 0
+    a[2 * q:3 * q, :n - 1] = 0xFFFFFFFF
+    b[2 * q:3 * q, :n - 1] = 0xFFFFFFFF
+    # b = 2^(32n-1) + 2^(32n-2): exact products 1.5 x a, ties when a is odd
+    b[3 * q:4 * q, :n] = 0
+    b[3 * q:4 * q, n - 1] = 0xC0000000
+    # one limb set below the top, at every position
+    b[4 * q:5 * q, :n - 1] = 0
+    b[4 * q + np.arange(q), np.arange(q) % (n - 1)] = rng.integers(1, 1 << 32, size=q, dtype=np.uint64).astype(np.uint32)
+    # squares of numbers close to a power of two (products just below / above 2^(64n-2))
+    a[5 * q:6 * q, :n] = 0xFFFFFFFF
+    a[5 * q:6 * q, 0] = rng.integers(0, 1 << 32, size=q, dtype=np.uint64).astype(np.uint32)
+    b[5 * q:6 * q] = a[5 * q:6 * q]
+    out, _ = engine.run(bits, Operation.mul, a, b)
+    want = oracle.elementwise(bits, 2, a, b)
+    assert same(out, want), f"first differing element {first_bad(out, want)}"
+
+
 @pytest.mark.parametrize("bits", [64, 224, 256, 384, 1024])
 def test_broadcast_operands(engine, oracle, bits):
     """tests/test_broadcast.cpp: b (and c) read at (i / stride) % period."""
