@@ -386,7 +386,7 @@ template <int N> __device__ __forceinline__ Num<N> div(const Num<N>& a, const Nu
 // ---------------------------------------------------------------- sqrt
 // Restoring digit-by-digit root of the 64N-bit radicand M * 2^(32N-1+odd); the root has 32N bits
 // and no tie is possible: round up exactly when the remainder exceeds the root.
-template <int N> __device__ __forceinline__ Num<N> sqrt(const Num<N>& a) {
+template <int N> __device__ __forceinline__ Num<N> sqrt_restoring(const Num<N>& a) {
     if (a.st || !a.s) return zero<N>(a.st);
     if (a.s < 0) return zero<N>(kInvalid);
     int e = a.e / 2; if (a.e < 0 && (a.e % 2)) --e;
@@ -444,6 +444,137 @@ template <int N> __device__ __forceinline__ Num<N> sqrt(const Num<N>& a) {
 #pragma unroll
     for (int i = 0; i < N; ++i) m[i] = root[i];
     return finish<N>(m, e, 1, c > 0, 0);
+}
+template <int N> __device__ __noinline__ Num<N> sqrt_restoring_call(const Num<N> a) { return sqrt_restoring<N>(a); }
+template <int N> __device__ __noinline__ Num<N> add_call(const Num<N> a, const Num<N> b);
+template <int N> __device__ __noinline__ Num<N> div_call(const Num<N> a, const Num<N> b);
+
+// RN(sqrt(a)) by Newton's iteration x <- (x + RN(a / x)) / 2 from a double-precision start, then an
+// exact check.  With Z the 2N-word radicand of sqrt_restoring and S = sqrt(Z) in [2^(32N-1), 2^(32N)),
+// the result mantissa is the integer C nearest S (there are no ties: S is an integer or irrational),
+// and C is nearest exactly when -C < Z - C^2 <= C.  The candidate from the iteration is moved a unit
+// at a time, with Z - C^2 updated exactly, until it passes.  A candidate that is not within a few
+// units, which the error bounds of the iteration rule out, takes the restoring routine.
+template <int N> __device__ __forceinline__ Num<N> sqrt(const Num<N>& a) {
+    if (a.st || !a.s) return zero<N>(a.st);
+    if (a.s < 0) return zero<N>(kInvalid);
+    int e = a.e / 2; if (a.e < 0 && (a.e % 2)) --e;
+    const int odd = a.e - 2 * e;                    // 0 or 1
+    // start: the top 64 bits of the mantissa as a double in [1, 2), its root in [1, 2)
+    const double f = (double)(((u64)a.m[N - 1] << 32) | a.m[N - 2]) * 0x1p-63;
+    const double r0 = fmin(__dsqrt_rn(odd ? 2.0 * f : f), 0x1.fffffffffffffp0);   // f may round up to 2
+    const u64 rb = (u64)(r0 * 0x1p63);              // top bit set: r0 >= 1
+    Num<N> x;
+#pragma unroll
+    for (int i = 0; i < N; ++i) x.m[i] = 0;
+    x.m[N - 1] = (u32)(rb >> 32); x.m[N - 2] = (u32)rb;
+    x.e = e; x.s = 1; x.st = 0;
+    constexpr int iters = 32 * N <= 104 ? 2 : 32 * N <= 208 ? 3 : 32 * N <= 416 ? 4 : 32 * N <= 832 ? 5 : 6;
+#pragma unroll 1
+    for (int it = 0; it < iters; ++it) {
+        Num<N> y;
+        if constexpr (N > 8) y = add_call<N>(x, div_call<N>(a, x)); else y = add<N>(x, div<N>(a, x));
+        y.e -= 1;
+        x = y;
+    }
+    // candidate C (N words + carry word), aligned to the exponent e
+    u32 c[N + 1];
+    if (x.e == e) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) c[i] = x.m[i];
+    } else if (x.e == e + 1) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) c[i] = 0xffffffffu;
+    } else if (x.e == e - 1) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) c[i] = i == N - 1 ? 0x80000000u : 0u;
+    } else {
+        return sqrt_restoring_call<N>(a);
+    }
+    c[N] = 0;
+    // Z (2N words) and D = Z - C^2 (2N + 1 words, two's complement)
+    u32 z[2 * N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) z[k] = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) z[N + i] = a.m[i];
+    if (!odd) {
+#pragma unroll
+        for (int k = 0; k < 2 * N; ++k) z[k] = (z[k] >> 1) | (k + 1 < 2 * N ? z[k + 1] << 31 : 0u);
+    }
+    u32 cm[N], p[2 * N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) cm[i] = c[i];
+    mant_mul<N>(cm, cm, p);
+    // D within N + 2 words: the words above must be the sign extension
+    u32 d[N + 2];
+    u32 bo = 0, hi_or = 0, hi_and = 0xffffffffu;
+#pragma unroll
+    for (int k = 0; k < 2 * N; ++k) {
+        const u64 t = (u64)p[k] + bo;
+        const u32 r = (u32)((u64)z[k] - t);
+        bo = (u64)z[k] < t;
+        if (k < N + 1) d[k] = r; else { hi_or |= r; hi_and &= r; }
+    }
+    const u32 ext = bo ? 0xffffffffu : 0u;           // sign word of Z - C^2
+    if (N + 1 < 2 * N && (hi_or != ext || hi_and != ext)) return sqrt_restoring_call<N>(a);
+    d[N + 1] = ext;
+    // adjust: while D > C: D -= 2C + 1, C += 1; while D <= -C: D += 2C - 1, C -= 1
+    bool done = false;
+#pragma unroll 1
+    for (int it = 0; it < 6 && !done; ++it) {
+        const bool neg = d[N + 1] >> 31;
+        // cmp = sign(D - C) for D >= 0, or sign(D + C) for D < 0
+        u32 t[N + 2];
+        if (!neg) {
+            u32 b2 = 0;
+#pragma unroll
+            for (int k = 0; k < N + 2; ++k) { const u64 v = (u64)(k <= N ? c[k] : 0u) + b2; t[k] = (u32)((u64)d[k] - v); b2 = (u64)d[k] < v; }
+            u32 o = 0;
+#pragma unroll
+            for (int k = 0; k < N + 2; ++k) o |= t[k];
+            if ((t[N + 1] >> 31) || o == 0) { done = true; break; }   // 0 <= D <= C
+            // D -= 2C + 1; C += 1
+            u32 b3 = 1;
+#pragma unroll
+            for (int k = 0; k < N + 2; ++k) { const u32 ck = k <= N ? c[k] : 0u; const u64 v = (u64)ck + ck + b3;
+                const u64 dv = (u64)d[k] - (u32)v; d[k] = (u32)dv; b3 = (u32)(v >> 32) + (u32)((dv >> 32) & 1u); }
+            u32 cy = 1;
+#pragma unroll
+            for (int k = 0; k <= N; ++k) { const u64 v = (u64)c[k] + cy; c[k] = (u32)v; cy = (u32)(v >> 32); }
+        } else {
+            u64 cy2 = 0;
+#pragma unroll
+            for (int k = 0; k < N + 2; ++k) { const u64 v = (u64)d[k] + (k <= N ? c[k] : 0u) + cy2; t[k] = (u32)v; cy2 = v >> 32; }
+            if (!(t[N + 1] >> 31)) {                     // D + C >= 0 ... D > -C unless D + C == 0
+                u32 o = 0;
+#pragma unroll
+                for (int k = 0; k < N + 2; ++k) o |= t[k];
+                if (o != 0) { done = true; break; }       // -C < D < 0
+            }
+            // D <= -C: D += 2C - 1; C -= 1
+            u64 cy3 = 0;
+#pragma unroll
+            for (int k = 0; k < N + 2; ++k) { const u32 ck = k <= N ? c[k] : 0u; const u64 v = (u64)d[k] + ck + ck + cy3; d[k] = (u32)v; cy3 = v >> 32; }
+            u32 b4 = 1;
+#pragma unroll
+            for (int k = 0; k < N + 2; ++k) { const u64 v = (u64)1u * b4; const u32 old = d[k]; d[k] = old - (u32)v; b4 = old < (u32)v; }
+            u32 b5 = 1;
+#pragma unroll
+            for (int k = 0; k <= N; ++k) { const u32 old = c[k]; c[k] = old - b5; b5 = old < b5; }
+        }
+    }
+    if (!done) return sqrt_restoring_call<N>(a);
+    u32 m[N];
+    if (c[N]) {                                      // C = 2^(32N): rounds up into the next binade
+#pragma unroll
+        for (int i = 0; i < N; ++i) m[i] = 0xffffffffu;
+        return finish<N>(m, e, 1, true, 0);
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) m[i] = c[i];
+    if (!(m[N - 1] >> 31)) return sqrt_restoring_call<N>(a);   // below the binade: not a valid candidate
+    return finish<N>(m, e, 1, false, 0);
 }
 
 // ---------------------------------------------------------------- fma

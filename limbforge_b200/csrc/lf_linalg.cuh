@@ -350,8 +350,12 @@ struct CholParams { u32* W; u64 n, k0, k1; long long* info; u32* error; };
 // Diagonal block [k0, k1) column by column: s_jj = D(w_jj; row j [k0,j)), l_jj = sqrt(s_jj) (or the
 // failing pivot recorded in info = {pivot, sign, status}); l_ij = RN(D(w_ij; row i, row j; [k0,j)) / l_jj)
 // for the block rows i > j.  The same formulas in the same dependency order as the row-by-row host
-// panel of linalg.mm:418-430, so every entry gets identical bits.  One warp per dot product.
-template <int N> __global__ void __launch_bounds__(128) chol_diag_kernel(CholParams p) {
+// panel of linalg.mm:418-430, so every entry gets identical bits.  For each column every dot product
+// (the diagonal's and the rows') runs at once, one warp each, and D is parked in w_ij; the square
+// root follows on the diagonal's warp, then one thread per row divides.  After a failure the column's
+// parked values are overwritten with invalid zeros by chol_prepare_kernel.
+template <int N> constexpr int diag_threads() { return N <= 8 ? 512 : N <= 16 ? 256 : 128; }   // registers per thread
+template <int N> __global__ void __launch_bounds__(diag_threads<N>()) chol_diag_kernel(CholParams p) {
     constexpr u64 E = N + 3;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     __shared__ int failed;
@@ -359,19 +363,21 @@ template <int N> __global__ void __launch_bounds__(128) chol_diag_kernel(CholPar
     __syncthreads();
     for (u64 j = p.k0; j < p.k1; ++j) {
         u32* wjj = p.W + (j * p.n + j) * E;
-        if (warp == 0) {
-            const Num<N> s = warp_exact_dot<N, false>(wjj, true, p.W + (j * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
+        for (u64 u = warp; u < p.k1 - j; u += nw) {                 // u = 0: the diagonal, u > 0: row j + u
+            const u64 i = j + u;
+            u32* wij = p.W + (i * p.n + j) * E;
+            const Num<N> v = warp_exact_dot<N, false>(wij, true, p.W + (i * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
             if (lane == 0) {
-                if (s.st || s.s <= 0) { p.info[0] = (long long)j; p.info[1] = s.st ? 0 : s.s; p.info[2] = s.st; failed = 1; }
-                else store<N>(wjj, lfd::sqrt<N>(s));
+                if (u) store<N>(wij, v);
+                else if (v.st || v.s <= 0) { p.info[0] = (long long)j; p.info[1] = v.st ? 0 : v.s; p.info[2] = v.st; failed = 1; }
+                else store<N>(wjj, lfd::sqrt<N>(v));
             }
         }
         __syncthreads();
         if (failed) return;
-        for (u64 i = j + 1 + warp; i < p.k1; i += nw) {
+        for (u64 i = j + 1 + threadIdx.x; i < p.k1; i += blockDim.x) {
             u32* wij = p.W + (i * p.n + j) * E;
-            const Num<N> v = warp_exact_dot<N, false>(wij, true, p.W + (i * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
-            if (lane == 0) store<N>(wij, div<N>(v, ldn<N, false>(wjj)));
+            store<N>(wij, div<N>(ldn<N, false>(wij), ldn<N, false>(wjj)));
         }
         __syncthreads();
     }
@@ -449,7 +455,7 @@ typedef void (*SolveFn)(const SolveParams&, bool, cudaStream_t);
 struct FactorKernels { CholDiagFn diag; CholRowsFn rows; CholPrepFn prep; SolveFn solve; };
 const FactorKernels* factor_kernels(int limbs);
 
-template <int N> void chol_diag_launch(const CholParams& p, cudaStream_t s) { chol_diag_kernel<N><<<1, 128, 0, s>>>(p); }
+template <int N> void chol_diag_launch(const CholParams& p, cudaStream_t s) { chol_diag_kernel<N><<<1, diag_threads<N>(), 0, s>>>(p); }
 template <int N> void chol_rows_launch(const CholParams& p, u64 r0, u64 jend, cudaStream_t s) {
     if (r0 >= p.n || jend <= p.k0) return;
     const u64 rows = p.n - r0;
