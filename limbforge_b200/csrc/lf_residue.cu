@@ -13,6 +13,7 @@
 #include "lf_residue.cuh"
 
 #include <cuda.h>
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -53,7 +54,13 @@ uint32_t mod_small(const std::vector<uint32_t>& x, uint32_t m) {
     return (uint32_t)r;
 }
 
-struct TableSet { lfd::ResTables* dev = nullptr; int L = 0, qwords = 0; };
+// Device tables of one modulus count: the ResTables and the byte matrix B of the tensor-core CRT
+// (NB rows of byte columns: S bytes 0..NS-1, then 6 bytes of F; Kp = 2L bytes rounded up to 32),
+// stored as the 128-byte-swizzled shared-memory image of each 128-byte K block.
+struct TableSet {
+    lfd::ResTables* dev = nullptr; int L = 0, qwords = 0;
+    unsigned char* bimg = nullptr; int NB = 0, Kp = 0, NS = 0; unsigned tmem_cols = 0;
+};
 std::mutex g_table_mutex;
 std::map<std::pair<int, int>, TableSet> g_tables;            // (device, L)
 
@@ -89,6 +96,26 @@ TableSet tables_for(int device, int L) {
     // tables run on non-blocking streams: wait for the copy before the table is handed out.
     cuda_check(cudaMemcpy(t.dev, h, sizeof(lfd::ResTables), cudaMemcpyHostToDevice), "residue tables");
     cuda_check(cudaStreamSynchronize(0), "residue tables");
+    // tensor-core CRT operand: row b < NS: byte b - h of M/m_l in column 2l + h; row NS + b: byte b - h of
+    // floor(2^48/m_l)
+    t.NS = 4 * t.qwords + 1;
+    t.NB = (t.NS + 6 + 15) / 16 * 16;
+    t.Kp = (2 * L + 31) / 32 * 32;
+    t.tmem_cols = 32;
+    while ((int)t.tmem_cols < t.NB) t.tmem_cols *= 2;
+    const int kblocks = (t.Kp + 127) / 128;
+    std::vector<unsigned char> img((size_t)kblocks * t.NB * 128, 0);
+    auto qbyte = [&](int l, int b) -> unsigned { return b < 0 || b >= 4 * lfd::kResMaxQWords ? 0u : (h->q[l][b / 4] >> (8 * (b % 4))) & 255u; };
+    auto fbyte = [&](int l, int b) -> unsigned { return b < 0 || b >= 8 ? 0u : (unsigned)((h->frac[l] >> (8 * b)) & 255u); };
+    for (int n = 0; n < t.NB; ++n)
+        for (int k = 0; k < 2 * L; ++k) {
+            const int l = k / 2, hb = k % 2;
+            const unsigned v = n < t.NS ? qbyte(l, n - hb) : n < t.NS + 6 ? fbyte(l, n - t.NS - hb) : 0u;
+            img[(size_t)(k / 128) * t.NB * 128 + lfd::sw128_offset((uint32_t)n, (uint32_t)(k % 128))] = (unsigned char)v;
+        }
+    cuda_check(cudaMalloc(&t.bimg, img.size()), "residue CRT operand");
+    cuda_check(cudaMemcpy(t.bimg, img.data(), img.size(), cudaMemcpyHostToDevice), "residue CRT operand");
+    cuda_check(cudaStreamSynchronize(0), "residue CRT operand");
     delete h;
     g_tables[key] = t;
     return t;
@@ -179,8 +206,23 @@ bool ResidueEngine::run(int bits, lfd::LineView left, lfd::LineView right, uint6
     dim3 grid((unsigned)(Np / lfd::kTileN), (unsigned)(Mp / lfd::kTileM), (unsigned)L);
     lfd::residue_mma_kernel<<<grid, 128, smem, s>>>(ta1, ta0, tb1, tb0, mp);
     cuda_check(cudaGetLastError(), "residue products");
-    rk->rec(lfd::RecParams{res, tab.dev, L, tab.qwords, linfo, rinfo, C, ldc, M, Nc, subtract ? 1 : 0, lower ? 1 : 0}, s);
-    cuda_check(cudaGetLastError(), "reconstruction");
+    {
+        // persistent CRT: as many CTAs per SM as TMEM holds (512 columns per SM), shared memory sized
+        // so that no more than that are resident
+        const int kblocks = (tab.Kp + 127) / 128;
+        const int per_sm = (int)(512 / tab.tmem_cols);
+        size_t smem = 1024 + (size_t)kblocks * 16384 + (size_t)kblocks * tab.NB * 128;
+        smem = std::max(smem, (size_t)(228 * 1024) / (per_sm + 1) + 1024);
+        if (smem > 227 * 1024) throw runtime_error("residue engine: CRT operand exceeds shared memory");
+        int sms = 0;
+        cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+        const uint64_t tiles = (M * Nc + 127) / 128;
+        const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * per_sm);
+        lfd::CrtParams cp{res, tab.dev, tab.bimg, L, tab.qwords, tab.NB, tab.Kp, tab.NS, tab.tmem_cols, linfo, rinfo, C, ldc, M, Nc,
+                          subtract ? 1 : 0, lower ? 1 : 0, error};
+        rk->crt(cp, grid, smem, s);
+        cuda_check(cudaGetLastError(), "reconstruction");
+    }
     report.moduli = (size_t)L;
     report.band_bits = (size_t)G;
     report.int8_gemms = 4 * (size_t)L;

@@ -261,8 +261,11 @@ struct RecParams {
 // RN(sign_x * X * 2^sx + c) with one rounding for an exact multiword X: both terms in one exact
 // window when they are close, otherwise the far smaller term as a sticky unit (as in fma).
 template <int N> __device__ Num<N> round_sum2(const u32* X, int xw, i64 sx, int signx, const Num<N>& c) {
-    constexpr int CW = kResMaxQWords + 2 * N + 8;
-    u32 pos[CW], neg[CW];
+    constexpr int CWmax = kResMaxQWords + 2 * N + 10;
+    // window of xw + 2N + 8 words under the larger top: a term below it lies at least 2N + 6 words
+    // under that top, beyond every rounding decision
+    const int CW = xw + 2 * N + 8;
+    u32 pos[CWmax], neg[CWmax];
     // magnitude tops
     int tx = -1;
     for (int w = xw - 1; w >= 0; --w) if (X[w]) { tx = w; break; }
@@ -294,6 +297,32 @@ template <int N> __device__ Num<N> round_sum2(const u32* X, int xw, i64 sx, int 
     return finish<N>(R.m, R.e, cmp, R.rb && (R.sb || (R.m[0] & 1u)), 0);
 }
 
+// From S = sum_l t_l (M / m_l) (qwords + 2 words, clobbered) and F = sum_l t_l floor(2^48 / m_l):
+// X = S - round(F / 2^48) M, the signed exact product sum; returns RN(c -/+ X 2^scale) (subtract) or
+// RN(X 2^scale), one rounding.  The modulus product exceeds 4 max|X|, so the quotient's rounding is
+// never close.
+template <int N> __device__ __forceinline__ Num<N> crt_tail(u32* S, int qwords, u64 F, const ResTables* tab, i64 scale,
+                                                          bool subtract, const Num<N>& c) {
+    const u64 q = (F + (1ull << 47)) >> 48;                  // round(F): X = S - q M
+    // D = S - q*M (two's complement over qwords+2 words)
+    u64 borrow = 0;
+    for (int w = 0; w <= qwords + 1; ++w) {
+        const u64 qm = (w <= qwords ? (u64)tab->M[w] : 0ull) * q + borrow;
+        const u32 lo = (u32)qm;
+        const u32 old = S[w];
+        S[w] = old - lo;
+        borrow = (qm >> 32) + (old < lo ? 1u : 0u);
+    }
+    int sign = 1;
+    const int xw = qwords + 2;
+    if (S[xw - 1] >> 31) {
+        sign = -1; u64 c1 = 1;
+        for (int w = 0; w < xw; ++w) { u64 v = (u64)(u32)~S[w] + c1; S[w] = (u32)v; c1 = v >> 32; }
+    }
+    // a zero exact sum X with the addend falls back to c itself, as exact_dot_add
+    return round_sum2<N>(S, xw, scale, subtract ? -sign : sign, c);
+}
+
 template <int N> __global__ void __launch_bounds__(128) reconstruct_kernel(RecParams p) {
     const u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
     if (j >= p.Nc || i >= p.M) return;
@@ -323,37 +352,168 @@ template <int N> __global__ void __launch_bounds__(128) reconstruct_kernel(RecPa
     u64 cy = 0;
     for (int w = 0; w <= p.qwords; ++w) { u64 v = col[w] + cy; S[w] = (u32)v; cy = v >> 32; }
     S[p.qwords + 1] = (u32)cy;
-    const u64 q = (F + (1ull << 47)) >> 48;                  // round(F): X = S - q M
-    // D = S - q*M (two's complement over qwords+2 words)
-    u64 borrow = 0;
-    for (int w = 0; w <= p.qwords + 1; ++w) {
-        const u64 qm = (w <= p.qwords ? (u64)p.tab->M[w] : 0ull) * q + borrow;
-        const u32 lo = (u32)qm;
-        const u32 old = S[w];
-        S[w] = old - lo;
-        borrow = (qm >> 32) + (old < lo ? 1u : 0u);
+    store<N>(out, crt_tail<N>(S, p.qwords, F, p.tab, (i64)li.bottom + ri.bottom - 2 * (32 * N - 1), p.subtract != 0, c));
+}
+
+// ---------------------------------------------------------------- 3b. CRT on the tensor cores
+// S and F as one unsigned int8 GEMM.  With t_l = 256 th_l + tl_l (bytes) and q_{l,b} the bytes of
+// M/m_l, byte column b of S gets P[b] = sum_l (tl_l q_{l,b} + th_l q_{l,b-1}), so that
+// S = sum_b P[b] 2^(8b); F likewise from the bytes of floor(2^48/m_l).  Row o of the A operand holds
+// (tl_0, th_0, tl_1, th_1, ...) for output o.  B is the constant [NB][Kp] byte matrix of those
+// (shifted) bytes, uploaded once per modulus count already in the 128-byte-swizzled K-major layout
+// of shared memory.  Each P[b] is below 2L * 255^2 < 2^25, so the int32 accumulators are exact.  One
+// CTA computes 128 outputs per tile and is persistent over the tiles:
+//   - all threads build their row of A from the residues (r -> t = r w_l mod m_l);
+//   - one thread issues tcgen05.mma kind::i8 (u8 x u8 -> s32, M = 128, N <= 256 per instruction)
+//     into TMEM;
+//   - each thread reads its TMEM lane, carries the byte columns into S and F, and rounds its output
+//     with crt_tail.
+struct CrtParams {
+    const u16* res; const ResTables* tab; const unsigned char* bimg;
+    int L, qwords, NB, Kp, NS;             // B rows (multiple of 16), K bytes (multiple of 32), S byte columns
+    u32 tmem_cols;
+    const LineInfo* linfo; const LineInfo* rinfo;
+    u32* C; u64 ldc, M, Nc;
+    int subtract, lower;
+    u32* error;
+};
+__device__ __forceinline__ void mma_i8_u(u32 d_tmem, u64 a, u64 b, u32 idesc, bool accumulate) {
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+                 :: "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"((u32)accumulate), "r"(0u));
+}
+__device__ __forceinline__ u64 crt_desc(u32 saddr) {       // K-major, SW128, SBO 1024 B, as smem_desc
+    return (u64)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+// byte offset of (row, k) in a [rows][128-byte K block] tile, 128-byte swizzle (the TMA SW128 image)
+__host__ __device__ __forceinline__ u32 sw128_offset(u32 row, u32 k) {
+    return (row >> 3) * 1024u + (row & 7u) * 128u + ((((k >> 4) ^ row) & 7u) << 4) + (k & 15u);
+}
+template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(CrtParams p) {
+    extern __shared__ __align__(1024) unsigned char crt_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)crt_raw + 1023) & ~(uintptr_t)1023);
+    const int kblocks = p.Kp / 128 + (p.Kp % 128 ? 1 : 0);
+    unsigned char* sA = smem;                                  // kblocks x [128 rows][128 B]
+    unsigned char* sB = smem + kblocks * 16384;                // kblocks x [NB rows][128 B]
+    __shared__ __align__(8) u64 done;
+    __shared__ u32 tmem_slot;
+    const int warp = threadIdx.x >> 5;
+    const u64 bbytes = (u64)kblocks * p.NB * 128;
+    for (u64 o = (u64)threadIdx.x * 16; o < bbytes; o += (u64)blockDim.x * 16)
+        *reinterpret_cast<uint4*>(sB + o) = *reinterpret_cast<const uint4*>(p.bimg + o);
+    if (threadIdx.x == 0) {
+        mbar_init(&done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    int sign = 1;
-    const int xw = p.qwords + 2;
-    if (S[xw - 1] >> 31) {
-        sign = -1; u64 c1 = 1;
-        for (int w = 0; w < xw; ++w) { u64 v = (u64)(u32)~S[w] + c1; S[w] = (u32)v; c1 = v >> 32; }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(smem_u32(&tmem_slot)), "r"(p.tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    const i64 scale = (i64)li.bottom + ri.bottom - 2 * (32 * N - 1);
-    const Num<N> v = round_sum2<N>(S, xw, scale, p.subtract ? -sign : sign, c);
-    // a zero exact sum X with the addend falls back to c itself, as exact_dot_add
-    store<N>(out, v);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const u32 tmem = tmem_slot;
+    const int N1 = p.NB < 256 ? p.NB : 256, N2 = p.NB - N1;
+    const u32 id1 = (2u << 4) | ((u32)(N1 >> 3) << 17) | ((u32)(128 >> 4) << 24);
+    const u32 id2 = (2u << 4) | ((u32)(N2 >> 3) << 17) | ((u32)(128 >> 4) << 24);
+    const u64 outputs = p.M * p.Nc, tiles = (outputs + 127) / 128;
+    const u32 row = threadIdx.x, lane_base = (u32)(warp * 32) << 16;
+    u32 phase = 0;
+    for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        if (p.lower) {                                         // a tile inside one row, wholly above the diagonal
+            const u64 o0 = tile * 128, o1 = (o0 + 127 < outputs ? o0 + 127 : outputs - 1);
+            if (o0 / p.Nc == o1 / p.Nc && o0 % p.Nc > o0 / p.Nc) continue;
+        }
+        const u64 o = tile * 128 + row;
+        const bool valid = o < outputs;
+        bool any = false;
+        for (int l = 0; l < p.L; ++l) {                        // row of A: t_l as two bytes
+            u32 t = 0;
+            if (valid) {
+                const u32 r = p.res[(u64)l * outputs + o];
+                any |= r != 0;
+                t = mod_barrett((u64)r * p.tab->w[l], p.tab->m[l], p.tab->barrett[l]);
+            }
+            const u32 k = 2u * l;
+            *reinterpret_cast<u16*>(sA + (k >> 7) * 16384u + sw128_offset(row, k & 127u)) = (u16)t;
+        }
+        for (u32 k = 2u * p.L; k < (u32)kblocks * 128u; k += 2)
+            *reinterpret_cast<u16*>(sA + (k >> 7) * 16384u + sw128_offset(row, k & 127u)) = 0;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic writes -> tensor core reads
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            for (int ks = 0; ks < p.Kp / 32; ++ks) {
+                const int kb = ks >> 2;
+                const u64 koff = (u64)((ks & 3) * 32) >> 4;
+                const u64 ad = crt_desc(smem_u32(sA + kb * 16384)) + koff;
+                const u32 bbase = smem_u32(sB + (u64)kb * p.NB * 128);
+                mma_i8_u(tmem, ad, crt_desc(bbase) + koff, id1, ks > 0);
+                if (N2) mma_i8_u(tmem + 256, ad, crt_desc(bbase + 256 * 128) + koff, id2, ks > 0);
+            }
+            mma_commit(&done);
+        }
+        const bool fine = __syncthreads_and(mbar_wait(&done, phase, p.error));
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (!fine) break;
+        // S and F from the byte columns of this row (every thread reads its lane: .sync.aligned)
+        u32 S[kResMaxQWords + 2];
+        int sw = 0;
+        u64 acc = 0, F = 0;
+        for (int c0 = 0; c0 < p.NB; c0 += 32) {
+            u32 P[32];
+            tmem_ld32(tmem + lane_base + (u32)c0, P);
+            asm volatile("tcgen05.wait::ld.sync.aligned;");
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                const int col = c0 + c;
+                if (col < p.NS) {
+                    acc += (u64)P[c] << (8 * (col & 3));
+                    if ((col & 3) == 3) { S[sw++] = (u32)acc; acc >>= 32; }
+                } else if (col < p.NS + 6) {
+                    F += (u64)P[c] << (8 * (col - p.NS));
+                }
+            }
+        }
+        while (sw < p.qwords + 2) { S[sw++] = (u32)acc; acc >>= 32; }
+        if (valid) {
+            const u64 i = o / p.Nc, j = o % p.Nc;
+            if (!(p.lower && j > i)) {
+                constexpr u64 E = N + 3;
+                u32* out = p.C + (i * p.ldc + j) * E;
+                const Num<N> c = p.subtract ? load_plain<N>(out) : zero<N>();
+                const LineInfo li = p.linfo[i], ri = p.rinfo[j];
+                const u32 st = (p.subtract ? c.st : 0u) | li.status | ri.status;
+                if (st) store<N>(out, zero<N>(st));
+                else if (!li.nonzero || !ri.nonzero || !any) store<N>(out, p.subtract ? c : zero<N>());
+                else store<N>(out, crt_tail<N>(S, p.qwords, F, p.tab, (i64)li.bottom + ri.bottom - 2 * (32 * N - 1), p.subtract != 0, c));
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();                                        // TMEM and A are free for the next tile
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(p.tmem_cols));
 }
 
 typedef void (*DigitFn)(const DigitParams&, cudaStream_t);
 typedef void (*RecFn)(const RecParams&, cudaStream_t);
-struct ResidueKernels { DigitFn digits; RecFn rec; };
+typedef void (*CrtFn)(const CrtParams&, unsigned grid, size_t smem, cudaStream_t);
+struct ResidueKernels { DigitFn digits; RecFn rec; CrtFn crt; };
 const ResidueKernels* residue_kernels(int limbs);
 
 template <int N> void digits_launch(const DigitParams& p, cudaStream_t s) {
     if (!p.rows_pad || !p.Kp) return;
     dim3 grid((unsigned)((p.Kp + 127) / 128), (unsigned)p.rows_pad);
     digits_kernel<N><<<grid, 128, 0, s>>>(p);
+}
+template <int N> void crt_launch(const CrtParams& p, unsigned grid, size_t smem, cudaStream_t s) {
+    if (!p.M || !p.Nc) return;
+    cudaFuncSetAttribute(crt_mma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    crt_mma_kernel<N><<<grid, 128, smem, s>>>(p);
 }
 template <int N> void rec_launch(const RecParams& p, cudaStream_t s) {
     if (!p.M || !p.Nc) return;
@@ -365,5 +525,5 @@ template <int N> void rec_launch(const RecParams& p, cudaStream_t s) {
 
 #define LF_RESIDUE_INSTANTIATE(N)                                                                  \
     namespace lfd {                                                                                \
-    extern const ResidueKernels residue_kernels_##N; const ResidueKernels residue_kernels_##N = {digits_launch<N>, rec_launch<N>}; \
+    extern const ResidueKernels residue_kernels_##N; const ResidueKernels residue_kernels_##N = {digits_launch<N>, rec_launch<N>, crt_launch<N>}; \
     }
