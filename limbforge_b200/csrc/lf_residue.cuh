@@ -260,19 +260,37 @@ struct RecParams {
 };
 // RN(sign_x * X * 2^sx + c) with one rounding for an exact multiword X: both terms in one exact
 // window when they are close, otherwise the far smaller term as a sticky unit (as in fma).
+// acc (len words, two's complement) -= t << off (t has tw words), borrow carried to the top.
+__device__ __forceinline__ void acc_sub(u32* acc, int len, const u32* t, int tw, i64 off) {
+    const int ws = (int)(off >> 5), bs = (int)(off & 31);
+    u32 bo = 0;
+    int k = ws;
+    for (int q = 0; q <= tw && k < len; ++q, ++k) {
+        u32 v = q < tw ? t[q] << bs : 0u;
+        if (bs && q > 0) v |= t[q - 1] >> (32 - bs);
+        const u64 d = (u64)v + bo;
+        const u32 old = acc[k];
+        acc[k] = (u32)((u64)old - d);
+        bo = (u64)old < d;
+    }
+    for (; bo && k < len; ++k) { const u32 old = acc[k]; acc[k] = old - 1u; bo = old == 0u; }
+}
+__device__ __forceinline__ void acc_unit(u32* acc, int len, bool negative) {   // acc +-= 1
+    if (negative) { for (int k = 0; k < len; ++k) { const u32 old = acc[k]; acc[k] = old - 1u; if (old) break; } }
+    else { for (int k = 0; k < len; ++k) { if (++acc[k]) break; } }
+}
 template <int N> __device__ Num<N> round_sum2(const u32* X, int xw, i64 sx, int signx, const Num<N>& c) {
     constexpr int CWmax = kResMaxQWords + 2 * N + 10;
-    // window of xw + 2N + 8 words under the larger top: a term below it lies at least 2N + 6 words
-    // under that top, beyond every rounding decision
+    // One two's-complement window of xw + 2N + 8 words under the larger top, two bits of headroom
+    // above it: a term below the window lies at least 2N + 6 words under that top, beyond every
+    // rounding decision, and counts as +-1 in the lowest word.
     const int CW = xw + 2 * N + 8;
-    u32 pos[CWmax], neg[CWmax];
-    // magnitude tops
     int tx = -1;
     for (int w = xw - 1; w >= 0; --w) if (X[w]) { tx = w; break; }
     if (tx < 0) return c;                                       // no product term left
     const i64 topx = sx + 32 * (i64)tx + 31 - __clz(X[tx]);
     if (!c.s) {
-        u32 t[kResMaxQWords + 1];
+        u32 t[kResMaxQWords + 2];
         for (int w = 0; w < xw; ++w) t[w] = X[w];
         Rounded<N> R; round_info<N>(t, xw, sx, R);
         return finish<N>(R.m, R.e, signx, R.rb && (R.sb || (R.m[0] & 1u)), 0);
@@ -280,21 +298,17 @@ template <int N> __device__ Num<N> round_sum2(const u32* X, int xw, i64 sx, int 
     const i64 sc = (i64)c.e - (32 * N - 1), topc = c.e;
     const i64 hi = topx > topc ? topx : topc;
     const i64 lo = hi + 3 - 32 * (i64)(CW - 1);               // exponent of window bit 32
-    for (int w = 0; w < CW; ++w) { pos[w] = 0; neg[w] = 0; }
-    // x
-    if (sx >= lo) acc_add(signx > 0 ? pos : neg, CW, X, xw, 32 + (sx - lo));
-    else (signx > 0 ? pos : neg)[0] |= 1u;
-    if (sc >= lo) acc_add(c.s > 0 ? pos : neg, CW, c.m, N, 32 + (sc - lo));
-    else (c.s > 0 ? pos : neg)[0] |= 1u;
-    int cmp = 0;
-    for (int w = CW - 1; w >= 0 && !cmp; --w) if (pos[w] != neg[w]) cmp = pos[w] > neg[w] ? 1 : -1;
-    if (!cmp) return zero<N>();
-    u32* big = cmp > 0 ? pos : neg;
-    const u32* small = cmp > 0 ? neg : pos;
-    u32 bo = 0;
-    for (int w = 0; w < CW; ++w) { u64 d = (u64)small[w] + bo; u32 o = big[w]; big[w] = (u32)((u64)o - d); bo = (u64)o < d; }
-    Rounded<N> R; round_info<N>(big, CW, lo - 32, R);
-    return finish<N>(R.m, R.e, cmp, R.rb && (R.sb || (R.m[0] & 1u)), 0);
+    u32 acc[CWmax];
+    for (int w = 0; w < CW; ++w) acc[w] = 0;
+    if (sx >= lo) { if (signx > 0) acc_add(acc, CW, X, xw, 32 + (sx - lo)); else acc_sub(acc, CW, X, xw, 32 + (sx - lo)); }
+    else acc_unit(acc, CW, signx < 0);
+    if (sc >= lo) { if (c.s > 0) acc_add(acc, CW, c.m, N, 32 + (sc - lo)); else acc_sub(acc, CW, c.m, N, 32 + (sc - lo)); }
+    else acc_unit(acc, CW, c.s < 0);
+    const bool negative = acc[CW - 1] >> 31;
+    if (negative) { u32 cy = 1; for (int w = 0; w < CW; ++w) { const u32 v = ~acc[w] + cy; cy = cy && v == 0; acc[w] = v; } }
+    Rounded<N> R;
+    if (!round_info<N>(acc, CW, lo - 32, R)) return zero<N>();   // exact cancellation
+    return finish<N>(R.m, R.e, negative ? -1 : 1, R.rb && (R.sb || (R.m[0] & 1u)), 0);
 }
 
 // From S = sum_l t_l (M / m_l) (qwords + 2 words, clobbered) and F = sum_l t_l floor(2^48 / m_l):
@@ -428,15 +442,19 @@ template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(CrtParams
         const u64 o = tile * 128 + row;
         const bool valid = o < outputs;
         bool any = false;
-        for (int l = 0; l < p.L; ++l) {                        // row of A: t_l as two bytes
-            u32 t = 0;
-            if (valid) {
-                const u32 r = p.res[(u64)l * outputs + o];
-                any |= r != 0;
-                t = mod_barrett((u64)r * p.tab->w[l], p.tab->m[l], p.tab->barrett[l]);
+        for (int l0 = 0; l0 < p.L; l0 += 16) {                 // row of A: t_l as two bytes; 16 loads in flight
+            u32 r[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) r[q] = (valid && l0 + q < p.L) ? p.res[(u64)(l0 + q) * outputs + o] : 0u;
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const int l = l0 + q;
+                if (l >= p.L) break;
+                any |= r[q] != 0;
+                const u32 t = mod_barrett((u64)r[q] * p.tab->w[l], p.tab->m[l], p.tab->barrett[l]);
+                const u32 k = 2u * l;
+                *reinterpret_cast<u16*>(sA + (k >> 7) * 16384u + sw128_offset(row, k & 127u)) = (u16)t;
             }
-            const u32 k = 2u * l;
-            *reinterpret_cast<u16*>(sA + (k >> 7) * 16384u + sw128_offset(row, k & 127u)) = (u16)t;
         }
         for (u32 k = 2u * p.L; k < (u32)kblocks * 128u; k += 2)
             *reinterpret_cast<u16*>(sA + (k >> 7) * 16384u + sw128_offset(row, k & 127u)) = 0;
