@@ -17,6 +17,7 @@
 #include <cmath>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 namespace lfr {
@@ -121,6 +122,45 @@ TableSet tables_for(int device, int L) {
     return t;
 }
 
+// Digit-plane operand of one (L, xwords): B[2l + h][b] = byte h of 2^(8b) mod m_l, as the swizzled image.
+struct DigitTable { unsigned char* bimg = nullptr; int NB = 0, KB = 0; unsigned tmem_cols = 0; };
+std::map<std::tuple<int, int, int>, DigitTable> g_digit_tables;     // (device, L, xwords)
+DigitTable digit_table_for(int device, int L, int xwords) {
+    std::lock_guard<std::mutex> lock(g_table_mutex);
+    const auto key = std::make_tuple(device, L, xwords);
+    auto it = g_digit_tables.find(key);
+    if (it != g_digit_tables.end()) return it->second;
+    DigitTable t;
+    t.NB = (2 * L + 15) / 16 * 16;
+    t.KB = (4 * xwords + 31) / 32 * 32;
+    t.tmem_cols = 32;
+    while ((int)t.tmem_cols < t.NB) t.tmem_cols *= 2;
+    const int kblocks = (t.KB + 127) / 128;
+    std::vector<unsigned char> img((size_t)kblocks * t.NB * 128, 0);
+    const auto& m = primes();
+    for (int l = 0; l < L; ++l) {
+        uint64_t pw = 1 % m[l];
+        for (int b = 0; b < 4 * xwords; ++b) {
+            for (int h = 0; h < 2; ++h)
+                img[(size_t)(b / 128) * t.NB * 128 + lfd::sw128_offset((uint32_t)(2 * l + h), (uint32_t)(b % 128))] = (unsigned char)(pw >> (8 * h));
+            pw = (pw << 8) % m[l];
+        }
+    }
+    cuda_check(cudaMalloc(&t.bimg, img.size()), "digit operand");
+    cuda_check(cudaMemcpy(t.bimg, img.data(), img.size(), cudaMemcpyHostToDevice), "digit operand");
+    cuda_check(cudaStreamSynchronize(0), "digit operand");
+    g_digit_tables[key] = t;
+    return t;
+}
+// Persistent launch shape of the tcgen05 kernels that hold `tmem_cols` TMEM columns per CTA: as many
+// CTAs per SM as TMEM allows (512 columns), shared memory sized so that no more are resident.
+void tmem_launch_shape(unsigned tmem_cols, size_t smem_need, int sms, uint64_t tiles, unsigned& grid, size_t& smem) {
+    const int per_sm = (int)(512 / tmem_cols);
+    smem = std::max(smem_need, (size_t)(228 * 1024) / (per_sm + 1) + 1024);
+    if (smem > 227 * 1024) throw runtime_error("residue engine: operand tiles exceed shared memory");
+    grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * per_sm);
+}
+
 typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
                                 const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -195,9 +235,21 @@ bool ResidueEngine::run(int bits, lfd::LineView left, lfd::LineView right, uint6
     signed char *a1 = pl, *a0 = pl + aplane, *b1 = same ? a1 : pl + 2 * aplane, *b0 = same ? a0 : pl + 2 * aplane + bplane;
     auto* res = static_cast<uint16_t*>(residues.get(sizeof(uint16_t) * (uint64_t)L * M * Nc + 64));
     const int xwords = n + (G + 31) / 32 + 1;
-    rk->digits(lfd::DigitParams{left, M, K, Kp, Mp, L, xwords, linfo, tab.dev, a1, a0}, s);
-    if (!same) rk->digits(lfd::DigitParams{right, Nc, K, Kp, Np, L, xwords, rinfo, tab.dev, b1, b0}, s);
-    cuda_check(cudaGetLastError(), "digit planes");
+    int sms = 0;
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    {
+        const DigitTable dt = digit_table_for(dev, L, xwords);
+        const int kblocks = (dt.KB + 127) / 128;
+        auto planes_of = [&](lfd::LineView v, uint64_t lines, uint64_t rows_pad, const lfd::LineInfo* info, signed char* d1, signed char* d0) {
+            unsigned grid = 0; size_t smem = 0;
+            tmem_launch_shape(dt.tmem_cols, 1024 + (size_t)kblocks * 16384 + (size_t)kblocks * dt.NB * 128, sms, rows_pad * Kp / 128, grid, smem);
+            rk->digits_mma(lfd::DigitMmaParams{v, lines, K, Kp, rows_pad, L, xwords, info, tab.dev, dt.bimg, dt.NB, dt.KB, dt.tmem_cols,
+                                               d1, d0, error}, grid, smem, s);
+        };
+        planes_of(left, M, Mp, linfo, a1, a0);
+        if (!same) planes_of(right, Nc, Np, rinfo, b1, b0);
+        cuda_check(cudaGetLastError(), "digit planes");
+    }
     const CUtensorMap ta1 = plane_map(a1, Kp, Mp, L), ta0 = plane_map(a0, Kp, Mp, L);
     const CUtensorMap tb1 = plane_map(b1, Kp, same ? Mp : Np, L), tb0 = plane_map(b0, Kp, same ? Mp : Np, L);
     const size_t smem = lfd::kStages * lfd::kStageBytes + 1024;
@@ -210,14 +262,9 @@ bool ResidueEngine::run(int bits, lfd::LineView left, lfd::LineView right, uint6
         // persistent CRT: as many CTAs per SM as TMEM holds (512 columns per SM), shared memory sized
         // so that no more than that are resident
         const int kblocks = (tab.Kp + 127) / 128;
-        const int per_sm = (int)(512 / tab.tmem_cols);
-        size_t smem = 1024 + (size_t)kblocks * 16384 + (size_t)kblocks * tab.NB * 128;
-        smem = std::max(smem, (size_t)(228 * 1024) / (per_sm + 1) + 1024);
-        if (smem > 227 * 1024) throw runtime_error("residue engine: CRT operand exceeds shared memory");
-        int sms = 0;
-        cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-        const uint64_t tiles = (M * Nc + 127) / 128;
-        const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * per_sm);
+        unsigned grid = 0; size_t smem = 0;
+        tmem_launch_shape(tab.tmem_cols, 1024 + (size_t)kblocks * 16384 + (size_t)kblocks * tab.NB * 128, sms, (M * Nc + 127) / 128,
+                          grid, smem);
         lfd::CrtParams cp{res, tab.dev, tab.bimg, L, tab.qwords, tab.NB, tab.Kp, tab.NS, tab.tmem_cols, linfo, rinfo, C, ldc, M, Nc,
                           subtract ? 1 : 0, lower ? 1 : 0, error};
         rk->crt(cp, grid, smem, s);

@@ -517,10 +517,130 @@ template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(CrtParams
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(p.tmem_cols));
 }
 
+// ---------------------------------------------------------------- 1b. digit planes on the tensor cores
+// X mod m_l for all L moduli as one unsigned int8 GEMM: with x_b the bytes of X (4 xwords of them) and
+// T_l[b] = 2^(8b) mod m_l = 256 th + tl, the columns 2l, 2l+1 of P = [x bytes] x [tl; th] give
+// X == P_2l + 256 P_2l+1 (mod m_l), each P below 160 * 255^2 < 2^24.  Rows are the padded entries
+// (line, k) in plane order, 128 per tile; B is the constant [2L][4 xwords] byte table, uploaded per
+// (L, xwords) as its swizzled shared-memory image.  The epilogue reduces, negates for negative
+// entries, balances and splits each residue into the two int8 digits, and writes them to the planes
+// (consecutive rows are consecutive plane bytes).
+struct DigitMmaParams {
+    LineView v; u64 lines, K, Kp, rows_pad; int L; int xwords;
+    const LineInfo* info; const ResTables* tab;
+    const unsigned char* bimg; int NB, KB; u32 tmem_cols;
+    signed char* d1; signed char* d0;
+    u32* error;
+};
+template <int N> __global__ void __launch_bounds__(128) digits_mma_kernel(DigitMmaParams p) {
+    extern __shared__ __align__(1024) unsigned char dig_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)dig_raw + 1023) & ~(uintptr_t)1023);
+    const int kblocks = p.KB / 128 + (p.KB % 128 ? 1 : 0);
+    unsigned char* sA = smem;
+    unsigned char* sB = smem + kblocks * 16384;
+    __shared__ __align__(8) u64 done;
+    __shared__ u32 tmem_slot;
+    const int warp = threadIdx.x >> 5;
+    const u64 bbytes = (u64)kblocks * p.NB * 128;
+    for (u64 o = (u64)threadIdx.x * 16; o < bbytes; o += (u64)blockDim.x * 16)
+        *reinterpret_cast<uint4*>(sB + o) = *reinterpret_cast<const uint4*>(p.bimg + o);
+    if (threadIdx.x == 0) {
+        mbar_init(&done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(smem_u32(&tmem_slot)), "r"(p.tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const u32 tmem = tmem_slot;
+    const int N1 = p.NB < 256 ? p.NB : 256, N2 = p.NB - N1;
+    const u32 id1 = (2u << 4) | ((u32)(N1 >> 3) << 17) | ((u32)(128 >> 4) << 24);
+    const u32 id2 = (2u << 4) | ((u32)(N2 >> 3) << 17) | ((u32)(128 >> 4) << 24);
+    const u64 plane = p.rows_pad * p.Kp, tiles = plane / 128;     // Kp is a multiple of 128
+    const u32 row = threadIdx.x, lane_base = (u32)(warp * 32) << 16;
+    u32 phase = 0;
+    for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const u64 e = tile * 128 + row, line = e / p.Kp, k = e % p.Kp;
+        u32 x[40];
+#pragma unroll
+        for (int w = 0; w < 40; ++w) x[w] = 0;
+        bool negative = false;
+        if (k < p.K && line < p.lines) {
+            const Num<N> a = load<N>(p.v.base + (line * p.v.ls + k * p.v.ks) * (u64)(N + 3));
+            if (!a.st && a.s) {
+                negative = a.s < 0;
+                const int sh = a.e - p.info[line].bottom;       // 0 <= sh <= G
+                const int ws = sh >> 5, bs = sh & 31;
+                for (int i = 0; i <= N; ++i) {
+                    u32 v = i < N ? a.m[i] << bs : 0u;
+                    if (bs && i > 0) v |= a.m[i - 1] >> (32 - bs);
+                    x[i + ws] = v;
+                }
+            }
+        }
+        // row of A: the bytes of X, 16 at a time, zero beyond 4 xwords
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {                          // up to 2 K blocks of 8 chunks
+            if (c >= kblocks * 8) break;
+            const int w0 = c * 4;
+            uint4 v;
+            v.x = w0 < p.xwords ? x[w0] : 0u; v.y = w0 + 1 < p.xwords ? x[w0 + 1] : 0u;
+            v.z = w0 + 2 < p.xwords ? x[w0 + 2] : 0u; v.w = w0 + 3 < p.xwords ? x[w0 + 3] : 0u;
+            *reinterpret_cast<uint4*>(sA + (c >> 3) * 16384u + sw128_offset(row, (u32)(c & 7) * 16u)) = v;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            for (int ks = 0; ks < p.KB / 32; ++ks) {
+                const int kb = ks >> 2;
+                const u64 koff = (u64)((ks & 3) * 32) >> 4;
+                const u64 ad = crt_desc(smem_u32(sA + kb * 16384)) + koff;
+                const u32 bbase = smem_u32(sB + (u64)kb * p.NB * 128);
+                mma_i8_u(tmem, ad, crt_desc(bbase) + koff, id1, ks > 0);
+                if (N2) mma_i8_u(tmem + 256, ad, crt_desc(bbase + 256 * 128) + koff, id2, ks > 0);
+            }
+            mma_commit(&done);
+        }
+        const bool fine = __syncthreads_and(mbar_wait(&done, phase, p.error));
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (!fine) break;
+        for (int c0 = 0; c0 < 2 * p.L; c0 += 32) {
+            u32 P[32];
+            tmem_ld32(tmem + lane_base + (u32)c0, P);
+            asm volatile("tcgen05.wait::ld.sync.aligned;");
+#pragma unroll
+            for (int c = 0; c < 32; c += 2) {
+                const int l = (c0 + c) >> 1;
+                if (l >= p.L) break;
+                const u32 m = p.tab->m[l];
+                u32 u = mod_barrett((u64)P[c] + ((u64)P[c + 1] << 8), m, p.tab->barrett[l]);
+                if (negative && u) u = m - u;                   // residue of -X
+                int r = (int)u;
+                if (r > (int)(m >> 1)) r -= (int)m;              // balanced: |r| <= 32639
+                const int lo = (int)(signed char)(r & 0xff);
+                p.d1[l * plane + e] = (signed char)((r - lo) >> 8);
+                p.d0[l * plane + e] = (signed char)lo;
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(p.tmem_cols));
+}
+
 typedef void (*DigitFn)(const DigitParams&, cudaStream_t);
 typedef void (*RecFn)(const RecParams&, cudaStream_t);
 typedef void (*CrtFn)(const CrtParams&, unsigned grid, size_t smem, cudaStream_t);
-struct ResidueKernels { DigitFn digits; RecFn rec; CrtFn crt; };
+typedef void (*DigitMmaFn)(const DigitMmaParams&, unsigned grid, size_t smem, cudaStream_t);
+struct ResidueKernels { DigitFn digits; RecFn rec; CrtFn crt; DigitMmaFn digits_mma; };
 const ResidueKernels* residue_kernels(int limbs);
 
 template <int N> void digits_launch(const DigitParams& p, cudaStream_t s) {
@@ -533,6 +653,11 @@ template <int N> void crt_launch(const CrtParams& p, unsigned grid, size_t smem,
     cudaFuncSetAttribute(crt_mma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     crt_mma_kernel<N><<<grid, 128, smem, s>>>(p);
 }
+template <int N> void digits_mma_launch(const DigitMmaParams& p, unsigned grid, size_t smem, cudaStream_t s) {
+    if (!p.rows_pad || !p.Kp) return;
+    cudaFuncSetAttribute(digits_mma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    digits_mma_kernel<N><<<grid, 128, smem, s>>>(p);
+}
 template <int N> void rec_launch(const RecParams& p, cudaStream_t s) {
     if (!p.M || !p.Nc) return;
     dim3 grid((unsigned)((p.Nc + 127) / 128), (unsigned)p.M);
@@ -543,5 +668,5 @@ template <int N> void rec_launch(const RecParams& p, cudaStream_t s) {
 
 #define LF_RESIDUE_INSTANTIATE(N)                                                                  \
     namespace lfd {                                                                                \
-    extern const ResidueKernels residue_kernels_##N; const ResidueKernels residue_kernels_##N = {digits_launch<N>, rec_launch<N>, crt_launch<N>}; \
+    extern const ResidueKernels residue_kernels_##N; const ResidueKernels residue_kernels_##N = {digits_launch<N>, rec_launch<N>, crt_launch<N>, digits_mma_launch<N>}; \
     }
