@@ -457,7 +457,7 @@ def run_workloads(args):
 
 def run_ours(args, rank, world, local_rank):
     import torch
-    from limbforge_b200 import api
+    from limbforge_b200 import api, shard
 
     torch.cuda.set_device(local_rank)
     dist = None
@@ -503,10 +503,7 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    t = torch.tensor([ms], device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_total = float(t.item())
+    ms_total = shard.max_over_ranks(ms, dist, "cuda")            # the job's time is its slowest rank's
     ms_step = ms_total / args.steps
     value = world * COUNT * CHAIN / (ms_step * 1e-3)
 
@@ -539,11 +536,8 @@ def run_ours(args, rank, world, local_rank):
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         e2e_step()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    te = torch.tensor([e2e_s], device="cuda")
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * COUNT * CHAIN / float(te.item())
+    e2e_s = shard.max_over_ranks((time.perf_counter() - t0) / e2e_steps, dist, "cuda")
+    e2e_value = world * COUNT * CHAIN / e2e_s
 
     if rank != 0:
         return
