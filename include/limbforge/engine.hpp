@@ -137,6 +137,18 @@ public:
         lf_batched4 sh{s.count, s.rhs, s.inverse, s.determinant, s.fused};
         detail::check(lf_batch_lu4(open(), detail::Format<T>::bits, &sh, A.handle(), B.handle(), X.handle(), det.handle(), status.handle()));
     }
+    // Precision cast (exact widening, RNE narrowing, complex componentwise) and the adjacent-pair tree sum.
+    template <class From, class To> void cast(const Buffer<From>& in, Buffer<To>& out) {
+        static_assert(detail::Format<From>::complex == detail::Format<To>::complex, "cast keeps real or complex");
+        if (in.size() != out.size()) throw std::invalid_argument("cast buffer counts must match");
+        detail::check(lf_batch_cast(open(), detail::Format<From>::bits, detail::Format<To>::bits, detail::Format<To>::complex,
+                                    in.handle(), out.handle(), in.size()));
+    }
+    template <class T> void tree_sum(const Buffer<T>& input, Buffer<T>& out) {
+        if (out.size() != 1) throw std::invalid_argument("tree_sum output must contain one element");
+        detail::check(lf_batch_tree_sum(open(), detail::Format<T>::bits, detail::Format<T>::complex, input.handle(), out.handle(),
+                                        input.size()));
+    }
     Submission submit() {
         lf_submission* s = nullptr;
         detail::check(lf_batch_submit(open(), &s));
@@ -182,6 +194,10 @@ public:
         detail::check(lf_engine_run_ternary(e_.get(), bits, int(op), a, b, c, out, count, {b_index.stride, b_index.period},
                                             {c_index.stride, c_index.period}, &t));
         return detail::timing(t);
+    }
+    // Host-array precision cast between any two supported widths (complex: componentwise).
+    Timing cast(int from_bits, int to_bits, bool complex, const void* in, void* out, std::size_t count) {
+        lf_timing t{}; detail::check(lf_engine_cast(e_.get(), from_bits, to_bits, complex, in, out, count, &t)); return detail::timing(t);
     }
     Timing lu4(int bits, const Batched4& s, const void* A, const void* B, void* X, void* det, std::uint32_t* status) {
         lf_batched4 sh{s.count, s.rhs, s.inverse, s.determinant, s.fused};

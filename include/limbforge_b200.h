@@ -170,6 +170,21 @@ int lf_dev_elementwise(int bits, int op, const void* a, const void* b, const voi
 int lf_dev_mul_chain(int bits, const void* x, const void* factors, size_t factor_stride, unsigned steps, void* out,
                      size_t count, void* stream);
 
+/* ---- Precision casts and tree sums (engine.hpp:150-175,205; kernels.metal:60-112,251-266).
+ * cast: exact widening, round-to-nearest-even narrowing, complex componentwise; a status element or a
+ * zero becomes a zero with that status.  tree_sum: the fixed adjacent-pair tree (elements 2i and 2i+1
+ * added, an odd last element carried unrounded, repeated to one element; empty input -> zero). */
+int lf_engine_cast(lf_engine* engine, int from_bits, int to_bits, int complex_, const void* in, void* out, size_t count,
+                   lf_timing* timing);                                                   /* Engine::cast */
+int lf_batch_cast(lf_batch* batch, int from_bits, int to_bits, int complex_, lf_buffer* in, lf_buffer* out,
+                  size_t count);                                                         /* CommandBatch::cast */
+int lf_batch_tree_sum(lf_batch* batch, int bits, int complex_, lf_buffer* in, lf_buffer* out,
+                      size_t count);                                                     /* CommandBatch::tree_sum */
+/* Device-pointer forms (no reference counterpart), asynchronous on `stream`; tree_sum's scratch holds
+ * 2 * ceil(count / 2) elements (unused for count <= 2). */
+int lf_dev_cast(int from_bits, int to_bits, int complex_, const void* in, void* out, size_t count, void* stream);
+int lf_dev_tree_sum(int bits, int complex_, const void* in, size_t count, void* out, void* scratch, void* stream);
+
 /* ---- Ragged mixed-precision batches.  No reference counterpart: the reference's
  * BatchedLinalg::gemm (batched_linalg.hpp:86; batched_linalg.mm:163-173) runs one StridedGemm per
  * call, one shape and one precision, so a ragged batch there is a loop of calls grouped by shape.

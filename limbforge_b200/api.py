@@ -239,6 +239,9 @@ def _load() -> C.CDLL:
         "lf_linalg_trsm": ([V, I, I, V, S, V, S, V, P(_FactorOptions), P(_Timing)], I),
         "lf_linalg_cholesky_solve": ([V, I, V, S, V, S, V, P(_FactorOptions), P(_Timing)], I),
         "lf_dev_exact_product": ([V, I, V, S, S, V, S, S, S, S, S, V, S, I, I, V], I),
+        "lf_engine_cast": ([V, I, I, I, V, V, S, P(_Timing)], I),
+        "lf_batch_cast": ([V, I, I, I, V, V, S], I), "lf_batch_tree_sum": ([V, I, I, V, V, S], I),
+        "lf_dev_cast": ([I, I, I, V, V, S, V], I), "lf_dev_tree_sum": ([I, I, V, S, V, V, V], I),
         "lf_ragged_pack": ([I, V, S, P(_RaggedLu4), P(C.c_uint64)], I),
         "lf_ragged_plan_create": ([V, I, I, V, S, P(_RaggedLu4), C.c_uint64, P(V)], I),
         "lf_ragged_plan_tune": ([V, V], I), "lf_ragged_plan_run": ([V, V, V], I),
@@ -399,6 +402,20 @@ class CommandBatch:
         check(lib.lf_batch_lu4(self.handle, A.bits, C.byref(s), A.handle, B.handle if B else None, X.handle if X else None,
                                det.handle if det else None, status.handle))
 
+    def cast(self, a: Buffer, out: Buffer) -> None:
+        """CommandBatch::cast (engine.hpp:171): a's elements rounded to out's width."""
+        if a.complex != out.complex or a.count != out.count or not a.bits or not out.bits:
+            raise InvalidArgument("cast buffers must have the same count and format")
+        check(lib.lf_batch_cast(self.handle, a.bits, out.bits, int(a.complex), a.handle, out.handle, a.count))
+
+    def tree_sum(self, a: Buffer, out: Buffer) -> None:
+        """CommandBatch::tree_sum (engine.hpp:150): the adjacent-pair tree sum of a into out[0]."""
+        if out.count != 1:
+            raise InvalidArgument("tree_sum output must contain one element")
+        if a.bits != out.bits or a.complex != out.complex:
+            raise InvalidArgument("tree_sum buffers must have the same format")
+        check(lib.lf_batch_tree_sum(self.handle, a.bits, int(a.complex), a.handle, out.handle, a.count))
+
     def submit(self) -> Submission:
         h = C.c_void_p()
         check(lib.lf_batch_submit(self.handle, C.byref(h)))
@@ -452,6 +469,16 @@ class Engine:
         t = _Timing()
         check(lib.lf_engine_run_ternary(self.handle, bits, int(op), _ptr(a), _ptr(b), _ptr(c), _ptr(out), n,
                                         _bc(b_index), _bc(c_index), C.byref(t)))
+        return out, _timing(t)
+
+    def cast(self, from_bits, to_bits, complex_, x):
+        """Engine::cast (engine.hpp:205), host arrays; returns (out, Timing)."""
+        count = _elements(x)
+        n = to_bits // 32
+        out = np.zeros((count, 2, n + 3) if complex_ else (count, n + 3), dtype=np.uint32)
+        t = _Timing()
+        check(lib.lf_engine_cast(self.handle, from_bits, to_bits, int(complex_), _ptr(np.ascontiguousarray(x)), _ptr(out), count,
+                                 C.byref(t)))
         return out, _timing(t)
 
     def lu4(self, bits, shape: Batched4, A, B=None):
@@ -658,3 +685,13 @@ def dev_elementwise(bits, op, a_ptr, b_ptr, c_ptr, out_ptr, count, b_index=None,
 def dev_mul_chain(bits, x_ptr, factors_ptr, factor_stride, steps, out_ptr, count, stream=0) -> None:
     check(lib.lf_dev_mul_chain(bits, _ptr(x_ptr), _ptr(factors_ptr), factor_stride, steps, _ptr(out_ptr), count,
                                C.c_void_p(stream)))
+
+
+def dev_cast(from_bits, to_bits, complex_, in_ptr, out_ptr, count, stream=0) -> None:
+    check(lib.lf_dev_cast(from_bits, to_bits, int(complex_), C.c_void_p(in_ptr), C.c_void_p(out_ptr), count, C.c_void_p(stream)))
+
+
+def dev_tree_sum(bits, complex_, in_ptr, count, out_ptr, scratch_ptr, stream=0) -> None:
+    """scratch: 2 * ceil(count / 2) elements (unused for count <= 2)."""
+    check(lib.lf_dev_tree_sum(bits, int(complex_), C.c_void_p(in_ptr), count, C.c_void_p(out_ptr),
+                              C.c_void_p(scratch_ptr), C.c_void_p(stream)))

@@ -621,3 +621,49 @@ int lfo_strided_gemm(int bits, int complex_, size_t count, size_t m, size_t nc, 
             }
     return 0;
 }
+
+/* ---------------------------------------------------------------- casts and tree sums
+ * Precision cast (kernels.metal:251-266): a status element or a zero becomes a zero with that status;
+ * otherwise RN(sign * int(limbs) * 2^(e - (32W - 1))) at the target width; complex componentwise
+ * (count counts elements; complex elements are two components). */
+int lfo_cast(int from_bits, int to_bits, int complex_, const word* in, word* out, size_t count) {
+    const int W = from_bits / 32, n = to_bits / 32;
+    const size_t comps = count * (complex_ ? 2 : 1);
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < comps; ++i) {
+        const word* src = in + i * (size_t)(W + 3);
+        word* dst = out + i * (size_t)(n + 3);
+        const word st = src[W + 2];
+        const int32_t sign = (int32_t)src[W + 1];
+        if (st || !sign) { set_zero(dst, n, st); continue; }
+        round_to(dst, n, src, W, (int64_t)(int32_t)src[W] - (32LL * W - 1), sign, 0);
+    }
+    return 0;
+}
+/* Tree sum (kernels.metal:60-112): each level adds elements 2i and 2i+1 (cadd for complex), an odd
+ * last element carried unrounded, until one element; an empty input sums to zero. */
+int lfo_tree_sum(int bits, int complex_, const word* in, size_t count, word* out) {
+    const int n = bits / 32; const size_t S = (size_t)(n + 3) * (complex_ ? 2 : 1);
+    if (!count) { memset(out, 0, sizeof(word) * S); return 0; }
+    word* cur = (word*)malloc(sizeof(word) * S * count);
+    if (!cur) return 1;
+    memcpy(cur, in, sizeof(word) * S * count);
+    size_t c = count;
+    while (c > 1) {
+        const size_t next = (c + 1) / 2;
+        for (size_t i = 0; i < next; ++i) {
+            word r[70];
+            if (2 * i + 1 < c) {
+                if (complex_) lfo_cadd(n, cur + 2 * i * S, cur + (2 * i + 1) * S, r);
+                else lfo_add(n, cur + 2 * i * S, cur + (2 * i + 1) * S, r);
+            } else {
+                memcpy(r, cur + 2 * i * S, sizeof(word) * S);
+            }
+            memcpy(cur + i * S, r, sizeof(word) * S);
+        }
+        c = next;
+    }
+    memcpy(out, cur, sizeof(word) * S);
+    free(cur);
+    return 0;
+}

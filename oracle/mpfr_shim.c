@@ -31,6 +31,7 @@ extern int mpfr_sqrt(mpfr_ptr, mpfr_ptr, int);
 extern int mpfr_fma(mpfr_ptr, mpfr_ptr, mpfr_ptr, mpfr_ptr, int);
 extern int mpfr_fms(mpfr_ptr, mpfr_ptr, mpfr_ptr, mpfr_ptr, int);
 extern int mpfr_neg(mpfr_ptr, mpfr_ptr, int);
+extern int mpfr_set(mpfr_ptr, mpfr_ptr, int);
 extern int mpfr_sum(mpfr_ptr, mpfr_ptr*, unsigned long, int);
 extern void mpfr_set_zero(mpfr_ptr, int);
 extern int mpfr_set_emin(mpfr_exp_t);
@@ -164,5 +165,22 @@ int mpo_dot2_add(int bits, const word* a, const word* b, const word* c, const wo
         from_mp(o, &r, n);
     }
     mpfr_clear(&xa); mpfr_clear(&xb); mpfr_clear(&xc); mpfr_clear(&xd); mpfr_clear(&xe); mpfr_clear(&p); mpfr_clear(&q); mpfr_clear(&r);
+    return 0;
+}
+
+/* Precision cast: the source value exactly at its own precision, mpfr_set into the target precision
+ * RNDN; a status element or a zero gives a zero with that status.  count counts components. */
+int mpo_cast(int from_bits, int to_bits, const word* in, word* out, size_t count) {
+    const int W = from_bits / 32, n = to_bits / 32;
+    widen_range();
+    mpfr_struct x, r; mpfr_init2(&x, from_bits); mpfr_init2(&r, to_bits);
+    for (size_t i = 0; i < count; ++i) {
+        const word* a = in + i * (size_t)(W + 3); word* o = out + i * (size_t)(n + 3);
+        if (a[W + 2] || !(int32_t)a[W + 1]) { zero_num(o, n, a[W + 2]); continue; }
+        to_mp(&x, a, W);
+        mpfr_set(&r, &x, RNDN);
+        from_mp(o, &r, n);
+    }
+    mpfr_clear(&x); mpfr_clear(&r);
     return 0;
 }

@@ -64,6 +64,8 @@ class Oracle:
         lib.lfo_lu4.argtypes = [I, S, C.c_uint, I, V, V, V, V, V]
         lib.lfo_strided_gemm.argtypes = [I, I, S, S, S, S, S, S, S, I, I, I, V, V, V]
         lib.lfo_dot2_add.argtypes = [I, V, V, V, V, V, V]
+        lib.lfo_cast.argtypes = [I, I, I, V, V, S]
+        lib.lfo_tree_sum.argtypes = [I, I, V, S, V]
         self.lib = lib
 
     def elementwise(self, bits, op, a, b=None, c=None, b_index=(1, 0), c_index=(1, 0)):
@@ -125,6 +127,21 @@ class Oracle:
                                   _ptr(A), _ptr(B), _ptr(out))
         return out
 
+    def cast(self, from_bits, to_bits, complex_, x):
+        """x: [count, N+3] or [count, 2, N+3] at from_bits; returns the same shape at to_bits."""
+        count = x.shape[0]
+        n = to_bits // 32
+        out = np.zeros((count, 2, n + 3) if complex_ else (count, n + 3), dtype=np.uint32)
+        assert self.lib.lfo_cast(from_bits, to_bits, int(complex_), _ptr(x), _ptr(out), count) == 0
+        return out
+
+    def tree_sum(self, bits, complex_, x):
+        n = bits // 32
+        out = np.zeros((2, n + 3) if complex_ else (n + 3,), dtype=np.uint32)
+        src = np.ascontiguousarray(x) if x.shape[0] else np.zeros((1,) + out.shape, dtype=np.uint32)
+        assert self.lib.lfo_tree_sum(bits, int(complex_), _ptr(src), x.shape[0], _ptr(out)) == 0
+        return out
+
 
 class Reference:
     """The reference's own CPU arithmetic (core.hpp, exact_dot_add) built into oracle/_ref."""
@@ -170,7 +187,14 @@ class Mpfr:
         lib.mpo_fused.argtypes = [I, I, V, V, V, V, S]
         lib.mpo_dot.argtypes = [I, V, I, V, L, V, L, S, V]
         lib.mpo_dot2_add.argtypes = [I, V, V, V, V, V, V, S]
+        lib.mpo_cast.argtypes = [I, I, V, V, S]
         self.lib = lib
+
+    def cast(self, from_bits, to_bits, x):
+        """Real components x [count, N+3] at from_bits, rounded to to_bits."""
+        out = np.zeros((x.shape[0], to_bits // 32 + 3), dtype=np.uint32)
+        assert self.lib.mpo_cast(from_bits, to_bits, _ptr(x), _ptr(out), x.shape[0]) == 0
+        return out
 
     def real(self, bits, op, a, b=None):
         out = np.zeros_like(a)

@@ -28,6 +28,20 @@ int main() {
         x.download(out.data(), 64);
         for (int i = 0; i < 64; ++i) if (out[i].exponent != i + 8) { std::printf("chain FAILED at %d\n", i); return 1; }
         std::printf("engine ok\n");
+        // cast 256 -> 1024 bits (exact) and the tree sum of 2^1..2^64: sum of powers, exactly representable
+        auto wide = e.make_buffer<Float<1024>>(64), total = e.make_buffer<Float<1024>>(1);
+        auto rb = e.batch();
+        rb.cast(x, wide);
+        rb.tree_sum(wide, total);
+        rb.submit().wait();
+        Float<1024> t{};
+        total.download(&t, 1);
+        // sum_{i=8}^{71} 2^i = 2^72 - 2^8: top bit 2^71, exponent 71, and the 1024-bit mantissa holds it exactly
+        if (t.exponent != 71 || t.sign != 1 || t.limb[31] != 0xffffffffu || t.limb[30] != 0xffffffffu) { std::printf("cast/tree_sum FAILED\n"); return 1; }
+        std::vector<Float<128>> narrow(64);
+        e.cast(B, 128, false, a.data(), narrow.data(), 64);
+        for (int i = 0; i < 64; ++i) if (narrow[i].exponent != i || narrow[i].limb[3] != 0x80000000u) { std::printf("host cast FAILED at %d\n", i); return 1; }
+        std::printf("cast and tree_sum ok\n");
         // exact products: (A^T A) with A = identity-like powers
         Linalg la(e);
         std::vector<Float<B>> A(9, zero<B / 32>()), C(9);
