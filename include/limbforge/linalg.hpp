@@ -24,6 +24,27 @@ struct LinalgReport {
     int method = 0;
 };
 
+// Handle of a resident product (linalg.hpp:60-66): C is final after the batch's Submission::wait().
+class LinalgTicket {
+    struct Del { void operator()(lf_linalg_ticket* t) const { lf_linalg_ticket_destroy(t); } };
+    std::shared_ptr<lf_linalg_ticket> t_;
+    mutable LinalgReport r_;
+    explicit LinalgTicket(lf_linalg_ticket* t) : t_(t, Del{}) {}
+    friend class Linalg;
+public:
+    LinalgTicket() = default;
+    bool resolved() const { int r = 0; detail::check(lf_linalg_ticket_resolved(t_.get(), &r)); return r != 0; }
+    const LinalgReport& report() const {
+        lf_linalg_report c{};
+        detail::check(lf_linalg_ticket_report(t_.get(), &c));
+        r_ = {c.m, c.n, c.k, c.gpu_outputs, c.trivial_outputs, c.gemm_rows, c.gemm_cols, c.int8_gemms, c.moduli, c.band_bits,
+              c.analysis_seconds, c.gpu_seconds, c.method};
+        return r_;
+    }
+    // Later operations of the batch read C in stream order after the product, so no read is provisional.
+    bool provisional_reads() const { (void)report(); return false; }
+};
+
 // One Linalg per host thread.
 class Linalg {
     struct Del { void operator()(lf_linalg* l) const { lf_linalg_destroy(l); } };
@@ -73,6 +94,28 @@ public:
         lf_factor_options o = fo(options);
         lf_timing t{}; detail::check(lf_linalg_cholesky_solve(l_.get(), bits, L, n, B, nrhs, X, &o, &t)); return detail::timing(t);
     }
+    // Resident products (linalg.hpp:190-195): recorded into the batch; analysis, engine choice and modulus
+    // count are GPU passes of the batch.
+    template <class T> LinalgTicket syrk(CommandBatch& batch, const Buffer<T>& A, std::size_t rows, std::size_t cols, Buffer<T>& C,
+                                         bool lower_only = true, bool subtract = false) {
+        static_assert(detail::Format<T>::bits && !detail::Format<T>::complex, "dense linear algebra uses real Float<bits> buffers");
+        lf_linalg_ticket* t = nullptr;
+        detail::check(lf_linalg_batch_syrk(l_.get(), batch.handle(), detail::Format<T>::bits, A.handle(), rows, cols, C.handle(),
+                                           lower_only, subtract, &t));
+        return LinalgTicket(t);
+    }
+    template <class T> LinalgTicket gemm(CommandBatch& batch, bool transpose_a, const Buffer<T>& A, const Buffer<T>& B, std::size_t m,
+                                         std::size_t n, std::size_t k, Buffer<T>& C, bool subtract = false) {
+        static_assert(detail::Format<T>::bits && !detail::Format<T>::complex, "dense linear algebra uses real Float<bits> buffers");
+        lf_linalg_ticket* t = nullptr;
+        detail::check(lf_linalg_batch_gemm(l_.get(), batch.handle(), detail::Format<T>::bits, transpose_a, A.handle(), B.handle(), m, n, k,
+                                           C.handle(), subtract, &t));
+        return LinalgTicket(t);
+    }
+    template <class T> LinalgTicket gemm_exact(CommandBatch& b, bool ta, const Buffer<T>& A, const Buffer<T>& B, std::size_t m, std::size_t n,
+                                               std::size_t k, Buffer<T>& C, bool sub = false) { return gemm(b, ta, A, B, m, n, k, C, sub); }
+    template <class T> LinalgTicket syrk_exact(CommandBatch& b, const Buffer<T>& A, std::size_t rows, std::size_t cols, Buffer<T>& C,
+                                               bool lower_only = true, bool sub = false) { return syrk(b, A, rows, cols, C, lower_only, sub); }
     // explicit contract names (linalg.hpp:203-208)
     Timing gemm_exact(int bits, bool ta, const void* A, const void* B, std::size_t m, std::size_t n, std::size_t k, void* C, bool sub = false) {
         return gemm(bits, ta, A, B, m, n, k, C, sub);

@@ -170,6 +170,19 @@ int lf_dev_elementwise(int bits, int op, const void* a, const void* b, const voi
 int lf_dev_mul_chain(int bits, const void* x, const void* factors, size_t factor_stride, unsigned steps, void* out,
                      size_t count, void* stream);
 
+/* ---- Resident products (linalg.hpp:60-66,190-195): Linalg::syrk / gemm recorded into a CommandBatch on
+ * buffers of the Linalg's engine (row-major, sizes as the host calls).  Line analysis, the choice of engine
+ * and the modulus count are GPU passes of the batch (no host round trip); after the submission is waited C
+ * equals the host-array call bit for bit.  C must not be A or B. */
+typedef struct lf_linalg_ticket lf_linalg_ticket;                                        /* LinalgTicket */
+int lf_linalg_batch_gemm(lf_linalg* la, lf_batch* batch, int bits, int transpose_a, lf_buffer* A, lf_buffer* B, size_t m,
+                         size_t n, size_t k, lf_buffer* C, int subtract, lf_linalg_ticket** out);
+int lf_linalg_batch_syrk(lf_linalg* la, lf_batch* batch, int bits, lf_buffer* A, size_t rows, size_t cols, lf_buffer* C,
+                         int lower_only, int subtract, lf_linalg_ticket** out);
+int lf_linalg_ticket_resolved(lf_linalg_ticket* ticket, int* resolved);                 /* LinalgTicket::resolved */
+int lf_linalg_ticket_report(lf_linalg_ticket* ticket, lf_linalg_report* report);         /* LinalgTicket::report */
+void lf_linalg_ticket_destroy(lf_linalg_ticket* ticket);
+
 /* ---- Precision casts and tree sums (engine.hpp:150-175,205; kernels.metal:60-112,251-266).
  * cast: exact widening, round-to-nearest-even narrowing, complex componentwise; a status element or a
  * zero becomes a zero with that status.  tree_sum: the fixed adjacent-pair tree (elements 2i and 2i+1

@@ -239,6 +239,10 @@ def _load() -> C.CDLL:
         "lf_linalg_trsm": ([V, I, I, V, S, V, S, V, P(_FactorOptions), P(_Timing)], I),
         "lf_linalg_cholesky_solve": ([V, I, V, S, V, S, V, P(_FactorOptions), P(_Timing)], I),
         "lf_dev_exact_product": ([V, I, V, S, S, V, S, S, S, S, S, V, S, I, I, V], I),
+        "lf_linalg_batch_gemm": ([V, V, I, I, V, V, S, S, S, V, I, P(V)], I),
+        "lf_linalg_batch_syrk": ([V, V, I, V, S, S, V, I, I, P(V)], I),
+        "lf_linalg_ticket_resolved": ([V, P(I)], I), "lf_linalg_ticket_report": ([V, P(_LinalgReport)], I),
+        "lf_linalg_ticket_destroy": ([V], None),
         "lf_engine_cast": ([V, I, I, I, V, V, S, P(_Timing)], I),
         "lf_batch_cast": ([V, I, I, I, V, V, S], I), "lf_batch_tree_sum": ([V, I, I, V, V, S], I),
         "lf_dev_cast": ([I, I, I, V, V, S, V], I), "lf_dev_tree_sum": ([I, I, V, S, V, V, V], I),
@@ -607,6 +611,28 @@ class PinnedArray:
             self._p = None
 
 
+class LinalgTicket:
+    """Handle of a resident product (linalg.hpp:60-66)."""
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    def resolved(self) -> bool:
+        r = C.c_int()
+        check(lib.lf_linalg_ticket_resolved(self.handle, C.byref(r)))
+        return bool(r.value)
+
+    def report(self) -> dict:
+        r = _LinalgReport()
+        check(lib.lf_linalg_ticket_report(self.handle, C.byref(r)))
+        return {f: getattr(r, f) for f, _ in _LinalgReport._fields_}
+
+    def __del__(self):
+        if getattr(self, "handle", None) and lib is not None:
+            lib.lf_linalg_ticket_destroy(self.handle)
+            self.handle = None
+
+
 class Linalg:
     """Exact dense products and factorizations (linalg.hpp:141-218).  One Linalg per host thread."""
 
@@ -670,6 +696,21 @@ class Linalg:
     syrk_exact = syrk
     cholesky_blocked = cholesky
     cholesky_solve_blocked = cholesky_solve
+
+    # resident products (linalg.hpp:190-195): recorded into a batch, planned and run on the GPU at submit
+    def gemm_resident(self, batch: "CommandBatch", transpose_a, A: "Buffer", B: "Buffer", m, n, k, C_: "Buffer",
+                      subtract=False) -> "LinalgTicket":
+        h = C.c_void_p()
+        check(lib.lf_linalg_batch_gemm(self.handle, batch.handle, A.bits, int(transpose_a), A.handle, B.handle, m, n, k, C_.handle,
+                                       int(subtract), C.byref(h)))
+        return LinalgTicket(h)
+
+    def syrk_resident(self, batch: "CommandBatch", A: "Buffer", rows, cols, C_: "Buffer", lower_only=True,
+                      subtract=False) -> "LinalgTicket":
+        h = C.c_void_p()
+        check(lib.lf_linalg_batch_syrk(self.handle, batch.handle, A.bits, A.handle, rows, cols, C_.handle, int(lower_only),
+                                       int(subtract), C.byref(h)))
+        return LinalgTicket(h)
 
     def dev_exact_product(self, bits, left, left_ls, left_ks, right, right_ls, right_ks, M, N, K, C_, ldc,
                           subtract=False, lower=False, stream=0) -> None:

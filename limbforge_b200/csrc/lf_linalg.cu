@@ -386,3 +386,90 @@ int lf_dev_exact_product(lf_linalg* la, int bits, const void* left, size_t left_
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- resident products (linalg.hpp:190-195)
+// Linalg::syrk / gemm on a CommandBatch: recorded now, planned and run on the GPU at submit (line analysis,
+// engine choice and modulus count are kernels of the batch), final after Submission::wait.  C equals the
+// host-array call bit for bit.  The ticket reports the engine and modulus count once the batch has run.
+struct lf_linalg_ticket { std::shared_ptr<lfr::ResidentProduct> prod; };
+
+namespace {
+void resident_common(lf_linalg* la, lf_batch* bt, lf_buffer* C) {
+    if (!la) throw invalid_argument("null linalg");
+    if (!bt || bt->submitted) throw logic_error("batch already submitted or moved");
+    if (la->engine != bt->engine) throw invalid_argument("resident product: the batch belongs to another engine than the Linalg");
+    if (!C) throw invalid_argument("missing output buffer");
+}
+void resident_record(lf_batch* bt, std::shared_ptr<ResidentProduct> prod, lf_linalg_ticket** out) {
+    Op o;
+    o.kind = kCustom;
+    o.custom = [prod](cudaStream_t s) { resident_product_launch(*prod, s); };
+    bt->ops.push_back(o);
+    *out = new lf_linalg_ticket{std::move(prod)};
+}
+}  // namespace
+
+extern "C" {
+
+int lf_linalg_batch_gemm(lf_linalg* la, lf_batch* bt, int bits, int transpose_a, lf_buffer* A, lf_buffer* B, size_t m, size_t n,
+                         size_t k, lf_buffer* C, int subtract, lf_linalg_ticket** out) {
+    LF_API_BEGIN
+    resident_common(la, bt, C);
+    if (!out) throw invalid_argument("null ticket");
+    check_bits(bits);
+    validate_dims(m, n, k, n);
+    const size_t eb = size_t(bits / 8 + 12);
+    if (!A || !B) throw invalid_argument("missing input buffer");
+    if (A == C || B == C) throw invalid_argument("resident product: C must not be A or B");
+    if (A->bytes < m * k * eb || B->bytes < k * n * eb || C->bytes < m * n * eb) throw invalid_argument("resident product: undersized buffer");
+    bt->retain(A); bt->retain(B); bt->retain(C, true);
+    bt->engine->activate();
+    const bool limb = la->options.method == 1 || la->options.force_fallback;
+    const auto* a = static_cast<const uint32_t*>(A->dev);
+    lfd::LineView lv = transpose_a ? lfd::LineView{a, 1, m} : lfd::LineView{a, k, 1};
+    lfd::LineView rv{static_cast<const uint32_t*>(B->dev), 1, n};
+    resident_record(bt, resident_product_create(bits, lv, rv, m, n, k, static_cast<uint32_t*>(C->dev), n, subtract != 0, false, false, limb),
+                    out);
+    LF_API_END
+}
+
+int lf_linalg_batch_syrk(lf_linalg* la, lf_batch* bt, int bits, lf_buffer* A, size_t rows, size_t cols, lf_buffer* C, int lower_only,
+                         int subtract, lf_linalg_ticket** out) {
+    LF_API_BEGIN
+    resident_common(la, bt, C);
+    if (!out) throw invalid_argument("null ticket");
+    check_bits(bits);
+    if (subtract && !lower_only) throw invalid_argument("syrk: subtract updates the lower triangle only (lower_only)");
+    validate_dims(cols, cols, rows, cols);
+    const size_t eb = size_t(bits / 8 + 12);
+    if (!A) throw invalid_argument("missing input buffer");
+    if (A == C) throw invalid_argument("resident product: C must not be A");
+    if (A->bytes < rows * cols * eb || C->bytes < cols * cols * eb) throw invalid_argument("resident product: undersized buffer");
+    bt->retain(A); bt->retain(C, true);
+    bt->engine->activate();
+    const bool limb = la->options.method == 1 || la->options.force_fallback;
+    lfd::LineView v{static_cast<const uint32_t*>(A->dev), 1, cols};
+    resident_record(bt, resident_product_create(bits, v, v, cols, cols, rows, static_cast<uint32_t*>(C->dev), cols, subtract != 0, true,
+                                                !lower_only, limb), out);
+    LF_API_END
+}
+
+// LinalgTicket::resolved (linalg.hpp:61): the product has run (its submission completed).
+int lf_linalg_ticket_resolved(lf_linalg_ticket* t, int* resolved) {
+    LF_API_BEGIN
+    if (!t || !resolved) throw invalid_argument("null argument");
+    *resolved = resident_product_done(*t->prod) ? 1 : 0;
+    LF_API_END
+}
+// LinalgTicket::report (linalg.hpp:62): the engine, modulus count and band the GPU chose; logic_error before
+// the product has run, runtime_error when a cluster of terms overflowed the exact window.
+int lf_linalg_ticket_report(lf_linalg_ticket* t, lf_linalg_report* rep) {
+    LF_API_BEGIN
+    if (!t || !rep) throw invalid_argument("null argument");
+    if (!resident_product_done(*t->prod)) throw logic_error("ticket not resolved: wait for the submission first");
+    if (!resident_product_report(*t->prod, *rep)) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    LF_API_END
+}
+void lf_linalg_ticket_destroy(lf_linalg_ticket* t) { delete t; }
+
+}  // extern "C"

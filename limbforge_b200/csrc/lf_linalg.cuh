@@ -45,6 +45,15 @@ template <int N> __global__ void analyze_kernel(LineView v, u64 lines, u64 K, Li
     if (!lane) out[line] = LineInfo{st, top, bottom, nz};
 }
 
+// Plan of a product whose engine is chosen on the GPU (resident products): mode 1 runs the residue
+// engine with the modulus count L and the tables of that count, mode 0 the generic limb kernel.
+struct ResPlan {
+    int mode, G;
+    int L, qwords, NB, Kp, NS; u32 tmem_cols;        // CRT operand of L
+    int dNB; u32 dtmem;                               // digit operand of L
+    const void* tab; const unsigned char* crt_bimg; const unsigned char* dig_bimg;
+};
+
 struct DotParams {
     LineView left, right;
     const LineInfo* linfo; const LineInfo* rinfo;
@@ -53,6 +62,7 @@ struct DotParams {
     u64 row0, col0;                  // output offsets of this launch (tiles of a larger product)
     int subtract, lower;             // lower: only j <= i (global indices i = row0 + r, j = col0 + c)
     u32* error;                      // set to 1 when a cluster exceeds the accumulator
+    const ResPlan* plan;             // planned on the GPU: nothing to do when the plan chose the residue engine
 };
 
 constexpr int kClusterWords = 192;   // 6144-bit exact window per cluster (pos/neg magnitudes)
@@ -204,6 +214,7 @@ template <int N, bool RO = true> __device__ Num<N> exact_dot_add_dev(const u32* 
 }
 
 template <int N> __global__ void __launch_bounds__(128) exact_dot_kernel(DotParams p) {
+    if (p.plan && p.plan->mode == 1) return;
     const u64 r = (u64)blockIdx.y * blockDim.y + threadIdx.y;
     const u64 q = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= p.M || q >= p.Nc) return;

@@ -332,3 +332,168 @@ void residue_mma_launch(dim3 grid, const CUtensorMap& ta1, const CUtensorMap& ta
 }
 
 }  // namespace lfr
+
+// ---------------------------------------------------------------- resident products planned on the GPU
+namespace lfr {
+
+struct ResidentProduct {
+    int bits = 0, n = 0;
+    lfd::LineView left{}, right{};
+    uint64_t M = 0, Nc = 0, K = 0, ldc = 0;
+    uint32_t* C = nullptr;
+    bool subtract = false, lower = false, mirror = false, same = false, residue = false;
+    int device = 0, sms = 0, Lmin = 0, Lmax = 0, xwords = 0;
+    DevBuf lines, planes, res, plan, cands, cum, error;
+    uint64_t Kp = 0, Mp = 0, Np = 0;
+    int maxNB = 0, maxKp = 0, maxDNB = 0, KB = 0; unsigned maxTmem = 0, maxDTmem = 0;
+    CUtensorMap ta1{}, ta0{}, tb1{}, tb0{};
+    cudaEvent_t done = nullptr;
+    bool launched = false;
+    ~ResidentProduct() { if (done) cudaEventDestroy(done); }
+};
+
+static int moduli_for_band(int n, int G, uint64_t K) {
+    int logk = 0;
+    while ((1ull << logk) < K) ++logk;
+    const double need = 2.0 * (32 * n + G) + logk + 3;
+    double have = 0;
+    int L = 0;
+    while (have <= need) {
+        if (L >= lfd::kResMaxModuli) return 0;
+        have += std::log2((double)primes()[L++]);
+    }
+    return L;
+}
+
+std::shared_ptr<ResidentProduct> resident_product_create(int bits, lfd::LineView left, lfd::LineView right, uint64_t M, uint64_t Nc,
+                                                         uint64_t K, uint32_t* C, uint64_t ldc, bool subtract, bool lower,
+                                                         bool mirror, bool limb_only) {
+    auto r = std::make_shared<ResidentProduct>();
+    r->bits = bits; r->n = bits / 32; r->left = left; r->right = right; r->M = M; r->Nc = Nc; r->K = K; r->C = C; r->ldc = ldc;
+    r->subtract = subtract; r->lower = lower; r->mirror = mirror;
+    r->same = left.base == right.base && left.ls == right.ls && left.ks == right.ks && M == Nc;
+    cuda_check(cudaGetDevice(&r->device), "cudaGetDevice");
+    cuda_check(cudaDeviceGetAttribute(&r->sms, cudaDevAttrMultiProcessorCount, r->device), "SM count");
+    cuda_check(cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming), "event");
+    r->error.get(16);
+    r->plan.get(sizeof(lfd::ResPlan));
+    r->lines.get(sizeof(lfd::LineInfo) * (M + Nc) + 64);
+    r->Lmin = moduli_for_band(r->n, 0, K);
+    r->Lmax = moduli_for_band(r->n, kMaxBand, K);
+    r->residue = !limb_only && K && K <= kMaxK && r->Lmin && r->Lmax;
+    if (!r->residue) return r;
+    // candidates: every modulus count a band of 0..kMaxBand bits can need, with their tables
+    r->xwords = r->n + (kMaxBand + 31) / 32 + 1;
+    const int count = r->Lmax - r->Lmin + 1;
+    std::vector<lfd::ResPlan> cand(count);
+    std::vector<double> cum(count);
+    for (int i = 0; i < count; ++i) {
+        const int L = r->Lmin + i;
+        const TableSet t = tables_for(r->device, L);
+        const DigitTable d = digit_table_for(r->device, L, r->xwords);
+        lfd::ResPlan& c = cand[i];
+        c.mode = 1; c.L = L; c.qwords = t.qwords; c.NB = t.NB; c.Kp = t.Kp; c.NS = t.NS; c.tmem_cols = t.tmem_cols;
+        c.dNB = d.NB; c.dtmem = d.tmem_cols; c.tab = t.dev; c.crt_bimg = t.bimg; c.dig_bimg = d.bimg;
+        double have = 0;
+        for (int l = 0; l < L; ++l) have += std::log2((double)primes()[l]);
+        cum[i] = have;
+        r->maxNB = std::max(r->maxNB, t.NB); r->maxKp = std::max(r->maxKp, t.Kp); r->maxTmem = std::max(r->maxTmem, t.tmem_cols);
+        r->maxDNB = std::max(r->maxDNB, d.NB); r->maxDTmem = std::max(r->maxDTmem, d.tmem_cols); r->KB = d.KB;
+    }
+    cuda_check(cudaMemcpy(r->cands.get(sizeof(lfd::ResPlan) * count), cand.data(), sizeof(lfd::ResPlan) * count, cudaMemcpyHostToDevice), "plan candidates");
+    cuda_check(cudaMemcpy(r->cum.get(sizeof(double) * count), cum.data(), sizeof(double) * count, cudaMemcpyHostToDevice), "plan candidates");
+    cuda_check(cudaStreamSynchronize(0), "plan candidates");
+    r->Kp = (K + lfd::kTileK - 1) / lfd::kTileK * lfd::kTileK;
+    r->Mp = (M + lfd::kTileM - 1) / lfd::kTileM * lfd::kTileM;
+    r->Np = (Nc + lfd::kTileN - 1) / lfd::kTileN * lfd::kTileN;
+    const uint64_t aplane = (uint64_t)r->Lmax * r->Mp * r->Kp, bplane = r->same ? 0 : (uint64_t)r->Lmax * r->Np * r->Kp;
+    auto* pl = static_cast<signed char*>(r->planes.get(2 * (aplane + bplane) + 256));
+    signed char *a1 = pl, *a0 = pl + aplane, *b1 = r->same ? a1 : pl + 2 * aplane, *b0 = r->same ? a0 : pl + 2 * aplane + bplane;
+    r->res.get(sizeof(uint16_t) * (uint64_t)r->Lmax * M * Nc + 64);
+    r->ta1 = plane_map(a1, r->Kp, r->Mp, r->Lmax); r->ta0 = plane_map(a0, r->Kp, r->Mp, r->Lmax);
+    r->tb1 = plane_map(b1, r->Kp, r->same ? r->Mp : r->Np, r->Lmax); r->tb0 = plane_map(b0, r->Kp, r->same ? r->Mp : r->Np, r->Lmax);
+    return r;
+}
+
+void resident_product_launch(ResidentProduct& r, cudaStream_t s) {
+    uint32_t* err = static_cast<uint32_t*>(r.error.p);
+    cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
+    const auto* lk = lfd::linalg_kernels(r.n);
+    const lfd::ResPlan* plan = nullptr;
+    auto* linfo = static_cast<lfd::LineInfo*>(r.lines.p);
+    auto* rinfo = r.same ? linfo : linfo + r.M;
+    if (r.residue) {
+        const auto* rk = lfd::residue_kernels(r.n);
+        lk->analyze(r.left, r.M, r.K, linfo, s);
+        if (!r.same) lk->analyze(r.right, r.Nc, r.K, rinfo, s);
+        auto* pdev = static_cast<lfd::ResPlan*>(r.plan.p);
+        lfd::PlanParams pp{linfo, rinfo, r.M, r.Nc, r.K, r.n, static_cast<const lfd::ResPlan*>(r.cands.p),
+                           static_cast<const double*>(r.cum.p), r.Lmin, r.Lmax - r.Lmin + 1, kMaxBand, kMaxK, pdev};
+        lfd::plan_kernel<<<1, 256, 0, s>>>(pp);
+        cuda_check(cudaGetLastError(), "product plan");
+        plan = pdev;
+        const uint64_t aplane = (uint64_t)r.Lmax * r.Mp * r.Kp, bplane = r.same ? 0 : (uint64_t)r.Lmax * r.Np * r.Kp;
+        auto* pl = static_cast<signed char*>(r.planes.p);
+        signed char *a1 = pl, *a0 = pl + aplane, *b1 = r.same ? a1 : pl + 2 * aplane, *b0 = r.same ? a0 : pl + 2 * aplane + bplane;
+        auto* res = static_cast<uint16_t*>(r.res.p);
+        const int kblocks = (r.KB + 127) / 128;
+        auto planes_of = [&](lfd::LineView v, uint64_t lines, uint64_t rows_pad, const lfd::LineInfo* info, signed char* d1, signed char* d0) {
+            unsigned grid = 0; size_t smem = 0;
+            tmem_launch_shape(r.maxDTmem, 1024 + (size_t)kblocks * 16384 + (size_t)kblocks * r.maxDNB * 128, r.sms, rows_pad * r.Kp / 128,
+                              grid, smem);
+            lfd::DigitMmaParams dp{v, lines, r.K, r.Kp, rows_pad, 0, r.xwords, info, nullptr, nullptr, 0, r.KB, 0, d1, d0, err, plan};
+            rk->digits_mma(dp, grid, smem, s);
+        };
+        planes_of(r.left, r.M, r.Mp, linfo, a1, a0);
+        if (!r.same) planes_of(r.right, r.Nc, r.Np, rinfo, b1, b0);
+        cuda_check(cudaGetLastError(), "digit planes");
+        const size_t smem = lfd::kStages * lfd::kStageBytes + 1024;
+        cuda_check(cudaFuncSetAttribute(lfd::residue_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem");
+        lfd::MmaParams mp{res, nullptr, r.M, r.Nc, r.Kp, r.lower ? 1 : 0, err, plan};
+        dim3 grid((unsigned)(r.Np / lfd::kTileN), (unsigned)(r.Mp / lfd::kTileM), (unsigned)r.Lmax);
+        lfd::residue_mma_kernel<<<grid, 128, smem, s>>>(r.ta1, r.ta0, r.tb1, r.tb0, mp);
+        cuda_check(cudaGetLastError(), "residue products");
+        const int ckb = (r.maxKp + 127) / 128;
+        unsigned cgrid = 0; size_t csmem = 0;
+        tmem_launch_shape(r.maxTmem, 1024 + (size_t)ckb * 16384 + (size_t)ckb * r.maxNB * 128, r.sms, (r.M * r.Nc + 127) / 128, cgrid, csmem);
+        lfd::CrtParams cp{res, nullptr, nullptr, 0, 0, 0, 0, 0, 0, linfo, rinfo, r.C, r.ldc, r.M, r.Nc, r.subtract ? 1 : 0, r.lower ? 1 : 0, err, plan};
+        rk->crt(cp, cgrid, csmem, s);
+        cuda_check(cudaGetLastError(), "reconstruction");
+    }
+    // the limb kernel: the whole product when the plan chose it (or there is no residue set-up), else nothing
+    lfd::DotParams dp{};
+    dp.left = r.left; dp.right = r.right; dp.C = r.C; dp.ldc = r.ldc; dp.M = r.M; dp.Nc = r.Nc; dp.K = r.K;
+    dp.subtract = r.subtract; dp.lower = r.lower; dp.error = err; dp.plan = plan;
+    lk->dot(dp, s);
+    cuda_check(cudaGetLastError(), "exact product launch");
+    if (r.mirror) lk->mirror(r.C, r.M, r.ldc, s);
+    cuda_check(cudaEventRecord(r.done, s), "event");
+    r.launched = true;
+}
+
+bool resident_product_done(ResidentProduct& r) {
+    if (!r.launched) return false;
+    const cudaError_t e = cudaEventQuery(r.done);
+    if (e == cudaErrorNotReady) return false;
+    cuda_check(e, "resident product");
+    return true;
+}
+
+bool resident_product_report(ResidentProduct& r, lf_linalg_report& rep) {
+    cuda_check(cudaEventSynchronize(r.done), "resident product");
+    lfd::ResPlan p{};
+    uint32_t e = 0;
+    if (r.residue) cuda_check(cudaMemcpy(&p, r.plan.p, sizeof p, cudaMemcpyDeviceToHost), "plan");
+    cuda_check(cudaMemcpy(&e, r.error.p, 4, cudaMemcpyDeviceToHost), "error word");
+    rep = lf_linalg_report{};
+    rep.m = r.M; rep.n = r.Nc; rep.k = r.K;
+    rep.method = p.mode == 1 ? 2 : 1;
+    if (p.mode == 1) {
+        rep.moduli = (size_t)p.L; rep.band_bits = (size_t)p.G; rep.int8_gemms = 4 * (size_t)p.L;
+        rep.gemm_rows = r.M; rep.gemm_cols = r.Nc;
+    }
+    rep.gpu_outputs = r.lower ? r.M * (r.M + 1) / 2 : r.M * r.Nc;
+    return e == 0;
+}
+
+}  // namespace lfr

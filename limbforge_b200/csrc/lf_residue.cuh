@@ -94,6 +94,7 @@ struct MmaParams {
     u64 M, Nc, Kp;
     int lower;                              // skip tiles strictly above the diagonal (SYRK)
     u32* error;
+    const ResPlan* plan;                    // planned on the GPU: moduli at or above plan->L have no work
 };
 
 __device__ __forceinline__ u32 smem_u32(const void* p) { return (u32)__cvta_generic_to_shared(p); }
@@ -157,6 +158,11 @@ __global__ void __launch_bounds__(128, 1) residue_mma_kernel(const __grid_consta
     __shared__ __align__(8) u64 full[kStages], empty[kStages], done;
     __shared__ u32 tmem_slot;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const ResTables* tab = p.tab;
+    if (p.plan) {
+        if (p.plan->mode != 1 || blockIdx.z >= (unsigned)p.plan->L) return;
+        tab = static_cast<const ResTables*>(p.plan->tab);
+    }
     const int tm = blockIdx.y, tn = blockIdx.x, l = blockIdx.z;
     if (p.lower && (u64)tn * kTileN > (u64)tm * kTileM + kTileM - 1) return;      // whole tile above the diagonal
     if (threadIdx.x == 0) {
@@ -218,8 +224,8 @@ __global__ void __launch_bounds__(128, 1) residue_mma_kernel(const __grid_consta
     const bool fine = mbar_wait(&done, 0, p.error) && !abort_flag;
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (fine) {
-        const u32 m = p.tab->m[l];
-        const u64 br = p.tab->barrett[l];
+        const u32 m = tab->m[l];
+        const u64 br = tab->barrett[l];
         const u32 off49 = mod_barrett(1ull << 49, m, br);
         const u64 row = (u64)tm * kTileM + warp * 32 + lane;
         const u32 lane_base = (u32)(warp * 32) << 16;
@@ -247,6 +253,42 @@ __global__ void __launch_bounds__(128, 1) residue_mma_kernel(const __grid_consta
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" :: "r"(tmem));
+}
+
+// Plans a product on the GPU from its line analysis (the rule of the host driver): the residue engine
+// when some line is nonzero and status free, every such line spans at most max_band bits (G = the
+// widest) and 0 < K <= max_k; L is then the smallest count whose log2 product cum[L] exceeds
+// 2(32 limbs + G) + ceil(log2 K) + 3.  Otherwise the limb kernel.  One block.
+struct PlanParams {
+    const LineInfo* linfo; const LineInfo* rinfo; u64 M, Nc, K; int limbs;
+    const ResPlan* cands; const double* cum; int Lmin, count;     // candidate i is L = Lmin + i
+    int max_band; u64 max_k;
+    ResPlan* out;
+};
+__global__ void __launch_bounds__(256) plan_kernel(PlanParams p) {
+    __shared__ int sg[256], sa[256];
+    int G = 0, any = 0;
+    for (u64 i = threadIdx.x; i < p.M + p.Nc; i += blockDim.x) {
+        const LineInfo li = i < p.M ? p.linfo[i] : p.rinfo[i - p.M];
+        if (!li.status && li.nonzero) { G = max(G, li.top - li.bottom); any = 1; }
+    }
+    sg[threadIdx.x] = G; sa[threadIdx.x] = any;
+    __syncthreads();
+    for (int o = 128; o; o >>= 1) {
+        if ((int)threadIdx.x < o) { sg[threadIdx.x] = max(sg[threadIdx.x], sg[threadIdx.x + o]); sa[threadIdx.x] |= sa[threadIdx.x + o]; }
+        __syncthreads();
+    }
+    if (threadIdx.x) return;
+    ResPlan r{};
+    r.mode = 0; r.G = sg[0];
+    if (sa[0] && sg[0] <= p.max_band && p.K && p.K <= p.max_k) {
+        int logk = 0;
+        while ((1ull << logk) < p.K) ++logk;
+        const double need = 2.0 * (32 * p.limbs + sg[0]) + logk + 3;
+        for (int i = 0; i < p.count; ++i)
+            if (p.cum[i] > need) { r = p.cands[i]; r.mode = 1; r.G = sg[0]; break; }
+    }
+    *p.out = r;
 }
 
 #endif  // LF_RESIDUE_MMA_KERNEL
@@ -390,6 +432,7 @@ struct CrtParams {
     u32* C; u64 ldc, M, Nc;
     int subtract, lower;
     u32* error;
+    const ResPlan* plan;                   // planned on the GPU: L and its operand come from the plan
 };
 __device__ __forceinline__ void mma_i8_u(u32 d_tmem, u64 a, u64 b, u32 idesc, bool accumulate) {
     asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
@@ -403,7 +446,14 @@ __device__ __forceinline__ u64 crt_desc(u32 saddr) {       // K-major, SW128, SB
 __host__ __device__ __forceinline__ u32 sw128_offset(u32 row, u32 k) {
     return (row >> 3) * 1024u + (row & 7u) * 128u + ((((k >> 4) ^ row) & 7u) << 4) + (k & 15u);
 }
-template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(CrtParams p) {
+template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(const CrtParams pin) {
+    CrtParams p = pin;
+    if (pin.plan) {
+        const ResPlan& r = *pin.plan;
+        if (r.mode != 1) return;
+        p.tab = static_cast<const ResTables*>(r.tab); p.bimg = r.crt_bimg; p.L = r.L; p.qwords = r.qwords;
+        p.NB = r.NB; p.Kp = r.Kp; p.NS = r.NS; p.tmem_cols = r.tmem_cols;
+    }
     extern __shared__ __align__(1024) unsigned char crt_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)crt_raw + 1023) & ~(uintptr_t)1023);
     const int kblocks = p.Kp / 128 + (p.Kp % 128 ? 1 : 0);
@@ -531,8 +581,15 @@ struct DigitMmaParams {
     const unsigned char* bimg; int NB, KB; u32 tmem_cols;
     signed char* d1; signed char* d0;
     u32* error;
+    const ResPlan* plan;                   // planned on the GPU: L and its operand come from the plan
 };
-template <int N> __global__ void __launch_bounds__(128) digits_mma_kernel(DigitMmaParams p) {
+template <int N> __global__ void __launch_bounds__(128) digits_mma_kernel(const DigitMmaParams pin) {
+    DigitMmaParams p = pin;
+    if (pin.plan) {
+        const ResPlan& r = *pin.plan;
+        if (r.mode != 1) return;
+        p.tab = static_cast<const ResTables*>(r.tab); p.bimg = r.dig_bimg; p.L = r.L; p.NB = r.dNB; p.tmem_cols = r.dtmem;
+    }
     extern __shared__ __align__(1024) unsigned char dig_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)dig_raw + 1023) & ~(uintptr_t)1023);
     const int kblocks = p.KB / 128 + (p.KB % 128 ? 1 : 0);

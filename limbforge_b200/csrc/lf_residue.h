@@ -2,6 +2,7 @@
 // accumulators, one rounding per output).  run() returns false when the product is outside the
 // engine's domain (the caller then uses the generic limb kernel, which gives identical bits).
 #pragma once
+#include <memory>
 #include "lf_linalg.cuh"
 #include "lf_runtime.h"
 
@@ -26,4 +27,18 @@ void residue_tables_host(int L, lfd::ResTables& tables, int& qwords);
 CUtensorMap residue_plane_map(void* base, uint64_t Kp, uint64_t rows_pad, int L);
 void residue_mma_launch(dim3 grid, const CUtensorMap& ta1, const CUtensorMap& ta0, const CUtensorMap& tb1, const CUtensorMap& tb0,
                         const lfd::MmaParams& p, cudaStream_t s);
+}  // namespace lfr
+
+// Resident products planned on the GPU (Linalg::syrk / gemm on a CommandBatch): set up at record time for
+// every modulus count the product could need; launched at submit with no host round trip (line
+// analysis, plan, digit planes, residue products, CRT or the limb kernel, all on the stream).
+namespace lfr {
+struct ResidentProduct;
+std::shared_ptr<ResidentProduct> resident_product_create(int bits, lfd::LineView left, lfd::LineView right, uint64_t M, uint64_t Nc,
+                                                         uint64_t K, uint32_t* C, uint64_t ldc, bool subtract, bool lower,
+                                                         bool mirror, bool limb_only);
+void resident_product_launch(ResidentProduct& r, cudaStream_t s);
+bool resident_product_done(ResidentProduct& r);              // the launch has completed on the GPU
+// Fills the engine, modulus count and band; returns false when a cluster overflowed the exact window.
+bool resident_product_report(ResidentProduct& r, lf_linalg_report& rep);
 }  // namespace lfr

@@ -48,6 +48,19 @@ int main() {
         for (int i = 0; i < 3; ++i) A[i * 3 + i] = power<B>(i);
         la.syrk(B, A.data(), 3, 3, C.data(), false);
         for (int i = 0; i < 3; ++i) if (C[i * 3 + i].exponent != 2 * i) { std::printf("syrk FAILED\n"); return 1; }
+        {   // the same SYRK resident in a batch: planned on the GPU, identical bits after wait
+            auto bA = e.make_buffer<Float<B>>(9), bC = e.make_buffer<Float<B>>(9);
+            bA.upload(A.data(), 9);
+            auto rb = e.batch();
+            LinalgTicket t = la.syrk(rb, bA, 3, 3, bC, false);
+            rb.submit().wait();
+            std::vector<Float<B>> C2(9);
+            bC.download(C2.data(), 9);
+            if (std::memcmp(C2.data(), C.data(), sizeof(Float<B>) * 9) || !t.resolved() || t.report().m != 3) {
+                std::printf("resident syrk FAILED\n"); return 1;
+            }
+            std::printf("resident syrk ok\n");
+        }
         std::vector<Float<B>> L(9);
         CholeskyInfo info = la.cholesky(B, C.data(), 3, L.data());
         if (info.pivot != 3 || L[4].exponent != 1) { std::printf("cholesky FAILED\n"); return 1; }
