@@ -124,6 +124,41 @@ template <int N, bool FUSED> __device__ __forceinline__ void cx_step(Num<N>& sum
     if constexpr (N > 8) cx_step_call<N, FUSED>(sum, x, y, comp); else cx_step_body<N, FUSED>(sum, x, y, comp);
 }
 
+// Wide composed complex entries park their running sum and first product in shared memory (a slot of
+// 2(N+3) words per thread, word w at slot[w * stride]) while the next product runs.  The kernel then needs
+// the registers of one product or one sum at a time, which doubles the warps an SM holds at 1024 bits.
+template <int N, bool CX, bool FUSED> constexpr bool parked_state() { return CX && !FUSED && N >= 24; }
+template <int N> __device__ __forceinline__ void park(u32* slot, u32 stride, const Num<N>& v) {
+#pragma unroll
+    for (int w = 0; w < N; ++w) slot[w * stride] = v.m[w];
+    slot[N * stride] = (u32)v.e; slot[(N + 1) * stride] = (u32)v.s; slot[(N + 2) * stride] = v.st;
+}
+template <int N> __device__ __forceinline__ Num<N> unpark(const u32* slot, u32 stride) {
+    Num<N> v;
+#pragma unroll
+    for (int w = 0; w < N; ++w) v.m[w] = slot[w * stride];
+    v.e = (int)slot[N * stride]; v.s = (int)slot[(N + 1) * stride]; v.st = slot[(N + 2) * stride];
+    return v;
+}
+template <int N> __device__ void gemm_cell_parked(const u32* A, const u32* B, const u32* in, u32* out, u64 n, u64 k, u64 i, u64 j,
+                                                  int comp, bool accumulate, bool negative, u32* slot, u32 stride) {
+    constexpr u64 E = N + 3, S = 2 * E;
+    u32* ssum = slot;
+    u32* sp1 = slot + E * stride;
+    park<N>(ssum, stride, accumulate ? load_plain<N>(in) : zero<N>());
+    for (u64 kk = 0; kk < k; ++kk) {
+        const u32* x = A + (i * k + kk) * S;
+        const u32* y = B + (kk * n + j) * S;
+        park<N>(sp1, stride, mul<N>(load<N>(x), load<N>(y + (comp ? E : 0))));
+        const Num<N> p2 = mul<N>(load<N>(x + E), load<N>(y + (comp ? 0 : E)));
+        const Num<N> p1 = unpark<N>(sp1, stride);
+        park<N>(sp1, stride, comp ? add<N>(p1, p2) : sub<N>(p1, p2));
+        park<N>(ssum, stride, add<N>(unpark<N>(sp1, stride), unpark<N>(ssum, stride)));
+    }
+    Num<N> sum = unpark<N>(ssum, stride);
+    if (negative) sum = negate<N>(sum);
+    store<N>(out, sum);
+}
 template <int N, bool CX, bool FUSED> __device__ __forceinline__ void gemm_cell(const u32* A, const u32* B, const u32* in, u32* out,
                                                                               u64 n, u64 k, u64 i, u64 j, int comp, bool accumulate,
                                                                               bool negative) {
@@ -142,9 +177,10 @@ template <int N, bool CX, bool FUSED> __device__ __forceinline__ void gemm_cell(
     if (negative) sum = negate<N>(sum);
     store<N>(out, sum);
 }
-template <int N, bool CX, bool FUSED> __global__ void __launch_bounds__(256) gemm_kernel(GemmWork p) {
+template <int N, bool CX, bool FUSED> __global__ void __launch_bounds__(256, (parked_state<N, CX, FUSED>() ? 2 : 1)) gemm_kernel(GemmWork p) {
     constexpr u64 E = N + 3, S = CX ? 2 * E : E;
     __shared__ u32 s_chunk;
+    extern __shared__ u32 gemm_park[];                              // parked_state: 2E words per thread
     for (u32 round = 0;; ++round) {
         u32 c;
         if (p.counter) {
@@ -168,12 +204,20 @@ template <int N, bool CX, bool FUSED> __global__ void __launch_bounds__(256) gem
             const u64 cell = gc - it.cell0, i = cell / it.n, j = cell % it.n;
             const u32* in = p.base + it.c + cell * S + comp * E;
             u32* out = p.out_override ? p.out_override + gc * S + comp * E : p.out_base + it.c + cell * S + comp * E;
-            gemm_cell<N, CX, FUSED>(p.base + it.a, p.base + it.b, in, out, it.n, it.k, i, j, comp, it.flags & 1, it.flags & 2);
+            if constexpr (parked_state<N, CX, FUSED>())
+                gemm_cell_parked<N>(p.base + it.a, p.base + it.b, in, out, it.n, it.k, i, j, comp, it.flags & 1, it.flags & 2,
+                                    gemm_park + threadIdx.x, blockDim.x);
+            else
+                gemm_cell<N, CX, FUSED>(p.base + it.a, p.base + it.b, in, out, it.n, it.k, i, j, comp, it.flags & 1, it.flags & 2);
         } else {
             const u64 cells = p.m * p.n, t = gc / cells, cell = gc % cells;
             u32* out = p.C + (t * p.sc + cell) * S + comp * E;
-            gemm_cell<N, CX, FUSED>(p.A + t * p.sa * S, p.B + t * p.sb * S, out, out, p.n, p.k, cell / p.n, cell % p.n, comp,
-                                    p.accumulate, p.negative);
+            if constexpr (parked_state<N, CX, FUSED>())
+                gemm_cell_parked<N>(p.A + t * p.sa * S, p.B + t * p.sb * S, out, out, p.n, p.k, cell / p.n, cell % p.n, comp,
+                                    p.accumulate, p.negative, gemm_park + threadIdx.x, blockDim.x);
+            else
+                gemm_cell<N, CX, FUSED>(p.A + t * p.sa * S, p.B + t * p.sb * S, out, out, p.n, p.k, cell / p.n, cell % p.n, comp,
+                                        p.accumulate, p.negative);
         }
     }
 }
@@ -186,9 +230,11 @@ template <int N> int launch_lu4_n(const Lu4Params& p, unsigned grid, unsigned bl
     return 0;
 }
 template <int N, bool CX, bool FUSED> int launch_gemm_v(const GemmWork& p, unsigned grid, unsigned block, cudaStream_t s) {
-    if (!grid) { int b = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, gemm_kernel<N, CX, FUSED>, (int)block, 0); return b; }
+    const size_t smem = parked_state<N, CX, FUSED>() ? (size_t)block * 2 * (N + 3) * 4 : 0;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(gemm_kernel<N, CX, FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (!grid) { int b = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, gemm_kernel<N, CX, FUSED>, (int)block, smem); return b; }
     if (!p.nchunks) return 0;
-    gemm_kernel<N, CX, FUSED><<<grid, block, 0, s>>>(p);
+    gemm_kernel<N, CX, FUSED><<<grid, block, smem, s>>>(p);
     return 0;
 }
 template <int N> int launch_gemm_n(bool cx, bool fused, const GemmWork& p, unsigned grid, unsigned block, cudaStream_t s) {
