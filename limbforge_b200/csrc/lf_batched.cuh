@@ -124,10 +124,10 @@ template <int N, bool FUSED> __device__ __forceinline__ void cx_step(Num<N>& sum
     if constexpr (N > 8) cx_step_call<N, FUSED>(sum, x, y, comp); else cx_step_body<N, FUSED>(sum, x, y, comp);
 }
 
-// Wide composed complex entries park their running sum and first product in shared memory (a slot of
+// Composed complex entries of 17+ limbs park their running sum and first product in shared memory (a slot of
 // 2(N+3) words per thread, word w at slot[w * stride]) while the next product runs.  The kernel then needs
-// the registers of one product or one sum at a time, which doubles the warps an SM holds at 1024 bits.
-template <int N, bool CX, bool FUSED> constexpr bool parked_state() { return CX && !FUSED && N >= 24; }
+// the registers of one product or one sum at a time (128), which raises the warps an SM holds from 10 to 16 at 1024 bits.
+template <int N, bool CX, bool FUSED> constexpr bool parked_state() { return CX && !FUSED && N >= 17; }
 template <int N> __device__ __forceinline__ void park(u32* slot, u32 stride, const Num<N>& v) {
 #pragma unroll
     for (int w = 0; w < N; ++w) slot[w * stride] = v.m[w];

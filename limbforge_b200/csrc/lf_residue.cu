@@ -265,8 +265,9 @@ bool ResidueEngine::run(int bits, lfd::LineView left, lfd::LineView right, uint6
         unsigned grid = 0; size_t smem = 0;
         tmem_launch_shape(tab.tmem_cols, 1024 + (size_t)kblocks * 16384 + (size_t)kblocks * tab.NB * 128, sms, (M * Nc + 127) / 128,
                           grid, smem);
+        auto* sf = static_cast<uint32_t*>(misc.get(sizeof(uint32_t) * (uint64_t)(tab.qwords + 4) * M * Nc + 64));
         lfd::CrtParams cp{res, tab.dev, tab.bimg, L, tab.qwords, tab.NB, tab.Kp, tab.NS, tab.tmem_cols, linfo, rinfo, C, ldc, M, Nc,
-                          subtract ? 1 : 0, lower ? 1 : 0, error};
+                          subtract ? 1 : 0, lower ? 1 : 0, error, nullptr, sf};
         rk->crt(cp, grid, smem, s);
         cuda_check(cudaGetLastError(), "reconstruction");
     }
@@ -343,7 +344,7 @@ struct ResidentProduct {
     uint32_t* C = nullptr;
     bool subtract = false, lower = false, mirror = false, same = false, residue = false;
     int device = 0, sms = 0, Lmin = 0, Lmax = 0, xwords = 0;
-    DevBuf lines, planes, res, plan, cands, cum, error;
+    DevBuf lines, planes, res, plan, cands, cum, error, sf;
     uint64_t Kp = 0, Mp = 0, Np = 0;
     int maxNB = 0, maxKp = 0, maxDNB = 0, KB = 0; unsigned maxTmem = 0, maxDTmem = 0;
     CUtensorMap ta1{}, ta0{}, tb1{}, tb0{};
@@ -410,6 +411,9 @@ std::shared_ptr<ResidentProduct> resident_product_create(int bits, lfd::LineView
     auto* pl = static_cast<signed char*>(r->planes.get(2 * (aplane + bplane) + 256));
     signed char *a1 = pl, *a0 = pl + aplane, *b1 = r->same ? a1 : pl + 2 * aplane, *b0 = r->same ? a0 : pl + 2 * aplane + bplane;
     r->res.get(sizeof(uint16_t) * (uint64_t)r->Lmax * M * Nc + 64);
+    int maxq = 0;
+    for (const auto& c : cand) maxq = std::max(maxq, c.qwords);
+    r->sf.get(sizeof(uint32_t) * (uint64_t)(maxq + 4) * M * Nc + 64);
     r->ta1 = plane_map(a1, r->Kp, r->Mp, r->Lmax); r->ta0 = plane_map(a0, r->Kp, r->Mp, r->Lmax);
     r->tb1 = plane_map(b1, r->Kp, r->same ? r->Mp : r->Np, r->Lmax); r->tb0 = plane_map(b0, r->Kp, r->same ? r->Mp : r->Np, r->Lmax);
     return r;
@@ -456,7 +460,8 @@ void resident_product_launch(ResidentProduct& r, cudaStream_t s) {
         const int ckb = (r.maxKp + 127) / 128;
         unsigned cgrid = 0; size_t csmem = 0;
         tmem_launch_shape(r.maxTmem, 1024 + (size_t)ckb * 16384 + (size_t)ckb * r.maxNB * 128, r.sms, (r.M * r.Nc + 127) / 128, cgrid, csmem);
-        lfd::CrtParams cp{res, nullptr, nullptr, 0, 0, 0, 0, 0, 0, linfo, rinfo, r.C, r.ldc, r.M, r.Nc, r.subtract ? 1 : 0, r.lower ? 1 : 0, err, plan};
+        lfd::CrtParams cp{res, nullptr, nullptr, 0, 0, 0, 0, 0, 0, linfo, rinfo, r.C, r.ldc, r.M, r.Nc, r.subtract ? 1 : 0, r.lower ? 1 : 0, err, plan,
+                          static_cast<uint32_t*>(r.sf.p)};
         rk->crt(cp, cgrid, csmem, s);
         cuda_check(cudaGetLastError(), "reconstruction");
     }

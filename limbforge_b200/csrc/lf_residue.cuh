@@ -433,6 +433,8 @@ struct CrtParams {
     int subtract, lower;
     u32* error;
     const ResPlan* plan;                   // planned on the GPU: L and its operand come from the plan
+    u32* sf;                               // not null: S (qwords + 2 words) and F (2 words) go here, word-major
+                                           // (word w of output o at sf[w * M * Nc + o]), and crt_round_kernel rounds
 };
 __device__ __forceinline__ void mma_i8_u(u32 d_tmem, u64 a, u64 b, u32 idesc, bool accumulate) {
     asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
@@ -527,6 +529,34 @@ template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(const Crt
         asm volatile("tcgen05.fence::after_thread_sync;");
         if (!fine) break;
         // S and F from the byte columns of this row (every thread reads its lane: .sync.aligned)
+        if (p.sf) {                                             // S and F to global memory, word-major
+            int sw = 0;
+            u64 acc = 0, F = 0;
+            u32* dst = p.sf + o;
+            for (int c0 = 0; c0 < p.NB; c0 += 32) {
+                u32 P[32];
+                tmem_ld32(tmem + lane_base + (u32)c0, P);
+                asm volatile("tcgen05.wait::ld.sync.aligned;");
+#pragma unroll
+                for (int c = 0; c < 32; ++c) {
+                    const int col = c0 + c;
+                    if (col < p.NS) {
+                        acc += (u64)P[c] << (8 * (col & 3));
+                        if ((col & 3) == 3) { if (valid) dst[(u64)sw * outputs] = (u32)acc; ++sw; acc >>= 32; }
+                    } else if (col < p.NS + 6) {
+                        F += (u64)P[c] << (8 * (col - p.NS));
+                    }
+                }
+            }
+            if (valid) {
+                while (sw < p.qwords + 2) { dst[(u64)sw * outputs] = (u32)acc; ++sw; acc >>= 32; }
+                dst[(u64)(p.qwords + 2) * outputs] = (u32)F;
+                dst[(u64)(p.qwords + 3) * outputs] = (u32)(F >> 32);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            __syncthreads();
+            continue;
+        }
         u32 S[kResMaxQWords + 2];
         int sw = 0;
         u64 acc = 0, F = 0;
@@ -693,6 +723,32 @@ template <int N> __global__ void __launch_bounds__(128) digits_mma_kernel(const 
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(p.tmem_cols));
 }
 
+// The rounding half of the CRT when crt_mma_kernel wrote S and F: one thread per output, so the local-memory
+// work of crt_tail runs at full occupancy.  An output whose residues were all zero has S = F = 0, which
+// crt_tail turns into c itself (or zero), as the fused path does.
+template <int N> __global__ void __launch_bounds__(128) crt_round_kernel(const CrtParams pin) {
+    CrtParams p = pin;
+    if (pin.plan) {
+        if (pin.plan->mode != 1) return;
+        p.tab = static_cast<const ResTables*>(pin.plan->tab); p.qwords = pin.plan->qwords;
+    }
+    const u64 outputs = p.M * p.Nc, o = (u64)blockIdx.x * 128 + threadIdx.x;
+    if (o >= outputs) return;
+    const u64 i = o / p.Nc, j = o % p.Nc;
+    if (p.lower && j > i) return;
+    constexpr u64 E = N + 3;
+    u32* out = p.C + (i * p.ldc + j) * E;
+    const Num<N> c = p.subtract ? load_plain<N>(out) : zero<N>();
+    const LineInfo li = p.linfo[i], ri = p.rinfo[j];
+    const u32 st = (p.subtract ? c.st : 0u) | li.status | ri.status;
+    if (st) { store<N>(out, zero<N>(st)); return; }
+    if (!li.nonzero || !ri.nonzero) { store<N>(out, p.subtract ? c : zero<N>()); return; }
+    u32 S[kResMaxQWords + 2];
+    for (int w = 0; w < p.qwords + 2; ++w) S[w] = p.sf[(u64)w * outputs + o];
+    const u64 F = (u64)p.sf[(u64)(p.qwords + 2) * outputs + o] | ((u64)p.sf[(u64)(p.qwords + 3) * outputs + o] << 32);
+    store<N>(out, crt_tail<N>(S, p.qwords, F, p.tab, (i64)li.bottom + ri.bottom - 2 * (32 * N - 1), p.subtract != 0, c));
+}
+
 typedef void (*DigitFn)(const DigitParams&, cudaStream_t);
 typedef void (*RecFn)(const RecParams&, cudaStream_t);
 typedef void (*CrtFn)(const CrtParams&, unsigned grid, size_t smem, cudaStream_t);
@@ -709,6 +765,7 @@ template <int N> void crt_launch(const CrtParams& p, unsigned grid, size_t smem,
     if (!p.M || !p.Nc) return;
     cudaFuncSetAttribute(crt_mma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     crt_mma_kernel<N><<<grid, 128, smem, s>>>(p);
+    if (p.sf) crt_round_kernel<N><<<(unsigned)((p.M * p.Nc + 127) / 128), 128, 0, s>>>(p);
 }
 template <int N> void digits_mma_launch(const DigitMmaParams& p, unsigned grid, size_t smem, cudaStream_t s) {
     if (!p.rows_pad || !p.Kp) return;
