@@ -182,6 +182,8 @@ template <int N> __device__ __forceinline__ Num<N> mul_exact(const Num<N>& a, co
     return round_product<N>(p, (i64)a.e + b.e, a.s * b.s, 0);
 }
 template <int N> __device__ __noinline__ Num<N> mul_exact_call(const Num<N> a, const Num<N> b) { return mul_exact<N>(a, b); }
+// The same with b read inside the call, so a caller's fast path need not keep b's words live for it.
+template <int N> __device__ __noinline__ Num<N> mul_exact_mem_call(const Num<N> a, const u32* b) { return mul_exact<N>(a, load_plain<N>(b)); }
 
 // Upper part of the product: h = T / 2^(32(N-2)) with T = sum of a_i b_j 2^(32(i+j)) over i + j >= N-2
 // (words N-2 .. 2N-1; about 58% of the word products at N = 32).  The omitted products sum to
@@ -232,6 +234,51 @@ template <int N> __device__ __forceinline__ Num<N> mul(const Num<N>& a, const Nu
 #pragma unroll
         for (int i = 0; i < N; ++i) m[i] = __funnelshift_l(h[i + 1], h[i + 2], s);
         return finish<N>(m, (i64)a.e + b.e + 1 - (i64)s, a.s * b.s, rb, 0);
+    }
+}
+
+// The same upper part T as mant_mul_high with b's words read from memory: row j adds b_j times a into
+// the window through an explicit 32-bit carry (64-bit products, no condition code), so successive rows
+// are plain data dependencies that the compiler can overlap, and only a and the window live in
+// registers.  a_i b_j + h + c <= (2^32 - 1)^2 + 2 (2^32 - 1) = 2^64 - 1, so no step overflows.
+template <int N> __device__ __forceinline__ void mant_mul_high_mem(const u32 (&a)[N], const u32* b, u32 (&h)[N + 2]) {
+    constexpr int B = N - 2;
+#pragma unroll
+    for (int k = 0; k < N + 2; ++k) h[k] = 0;
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        const u32 bj = b[j];
+        const int i0 = B - j > 0 ? B - j : 0;
+        u32 c = 0;
+#pragma unroll
+        for (int i = i0; i < N; ++i) {
+            const u64 t = (u64)a[i] * bj + h[i + j - B] + c;
+            h[i + j - B] = (u32)t;
+            c = (u32)(t >> 32);
+        }
+        h[j + N - B] = c;        // rows before j end at word j + N - B - 1
+    }
+}
+// RN(a * y) for y an element in memory (plain loads: y may have been written earlier in the same
+// kernel).  The rounding rule is mul's, on the same T, so the result is mul(a, y) bit for bit.
+template <int N> __device__ __forceinline__ Num<N> mul_mem(const Num<N>& a, const u32* y) {
+    if constexpr (N < kShortMulLimbs) {
+        return mul_exact<N>(a, load_plain<N>(y));
+    } else {
+        const int ys = (int)y[N + 1];
+        const u32 st = a.st | y[N + 2];
+        if (st || !a.s || !ys) return zero<N>(st);
+        u32 h[N + 2];
+        mant_mul_high_mem<N>(a.m, y, h);
+        const u32 s = (h[N + 1] >> 31) ? 0u : 1u;
+        const u32 lw = h[1] << s;
+        const u32 low = lw & 0x7fffffffu;
+        const bool rb = lw >> 31;
+        if (low >= 0x80000000u - ((u32)N << s) || (rb && low == 0)) return mul_exact_mem_call<N>(a, y);
+        u32 m[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) m[i] = __funnelshift_l(h[i + 1], h[i + 2], s);
+        return finish<N>(m, (i64)a.e + (int)y[N] + 1 - (i64)s, a.s * ys, rb, 0);
     }
 }
 

@@ -60,22 +60,25 @@ template <int N, int OP> __global__ void __launch_bounds__(kEwThreads) ew_kernel
 }
 
 // v <- op_s(v, b_s[...]) for every step; out_s written where non-null.  Steps are uniform across
-// the grid, so the switch never diverges.
-template <int N, bool MUL_ONLY> __global__ void __launch_bounds__(kEwThreads) chain_kernel(const __grid_constant__ ChainParams p) {
-    const u64 i = (u64)blockIdx.x * kEwThreads + threadIdx.x;
+// the grid, so the switch never diverges.  Products read the factor's words from memory inside the
+// product (mul_mem), which keeps the kernel at about 120 registers; 64-thread blocks spread a
+// one-wave grid evenly over the SMs.
+constexpr int kChainThreads = 64;
+template <int N, bool MUL_ONLY> __global__ void __launch_bounds__(kChainThreads) chain_kernel(const __grid_constant__ ChainParams p) {
+    const u64 i = (u64)blockIdx.x * kChainThreads + threadIdx.x;
     if (i >= p.count) return;
     constexpr u64 E = N + 3;
     Num<N> v = load_plain<N>(p.a + E * i);
 #pragma unroll 1
     for (int s = 0; s < p.steps; ++s) {
         const ChainStep& st = p.step[s];
-        const Num<N> y = load_plain<N>(st.b + E * bidx(i, st.bs, st.bp));
-        if constexpr (MUL_ONLY) v = mul<N>(v, y);
+        const u32* y = st.b + E * bidx(i, st.bs, st.bp);
+        if constexpr (MUL_ONLY) v = mul_mem<N>(v, y);
         else switch (st.op) {
-        case 0: v = add<N>(v, y); break;
-        case 1: v = sub<N>(v, y); break;
-        case 2: v = mul<N>(v, y); break;
-        default: v = div<N>(v, y); break;
+        case 0: v = add<N>(v, load_plain<N>(y)); break;
+        case 1: v = sub<N>(v, load_plain<N>(y)); break;
+        case 2: v = mul_mem<N>(v, y); break;
+        default: v = div<N>(v, load_plain<N>(y)); break;
         }
         if (st.out) store<N>(st.out + E * i, v);
     }
@@ -104,11 +107,11 @@ template <int N> int launch_ew(int op, const EwParams& p, cudaStream_t s) {
 }
 template <int N> int launch_chain(const ChainParams& p, cudaStream_t s) {
     if (!p.count) return 0;
-    const unsigned blocks = (unsigned)((p.count + kEwThreads - 1) / kEwThreads);
+    const unsigned blocks = (unsigned)((p.count + kChainThreads - 1) / kChainThreads);
     bool mul_only = true;
     for (int k = 0; k < p.steps; ++k) mul_only = mul_only && p.step[k].op == 2;
-    if (mul_only) chain_kernel<N, true><<<blocks, kEwThreads, 0, s>>>(p);     // registers of mul alone
-    else chain_kernel<N, false><<<blocks, kEwThreads, 0, s>>>(p);
+    if (mul_only) chain_kernel<N, true><<<blocks, kChainThreads, 0, s>>>(p);     // registers of mul alone
+    else chain_kernel<N, false><<<blocks, kChainThreads, 0, s>>>(p);
     return 0;
 }
 

@@ -88,15 +88,11 @@ def test_every_width_vs_oracle(engine, oracle, bits):
         assert same(engine.run_ternary(bits, Operation(op), ca, cb, cc)[0], oracle.elementwise(bits, op, ca, cb, cc)), f"op {op}"
 
 
-@pytest.mark.parametrize("bits", [256, 384, 512, 800, 1024])
-def test_mul_near_rounding_boundaries(engine, oracle, bits):
-    """Products whose bits around the rounding position are runs of zeros or ones, exact ties and
-    exact results: from 12 limbs on, mul decides the rounding from the upper part of the product and
-    must fall back to the full product exactly in these cases."""
-    from limbforge_b200.api import Operation
+def boundary_operands(bits, cnt=4096):
+    """Operand pairs whose products put runs of zeros or ones around the rounding position, exact
+    ties and exact results."""
     n = bits // 32
     rng = np.random.default_rng(bits + 5)
-    cnt = 4096
     a = nb.random_numbers(rng, cnt, bits, 50)
     b = nb.random_numbers(rng, cnt, bits, 50)
     q = cnt // 8
@@ -119,9 +115,56 @@ def test_mul_near_rounding_boundaries(engine, oracle, bits):
     a[5 * q:6 * q, :n] = 0xFFFFFFFF
     a[5 * q:6 * q, 0] = rng.integers(0, 1 << 32, size=q, dtype=np.uint64).astype(np.uint32)
     b[5 * q:6 * q] = a[5 * q:6 * q]
+    return a, b
+
+
+@pytest.mark.parametrize("bits", [256, 384, 512, 800, 1024])
+def test_mul_near_rounding_boundaries(engine, oracle, bits):
+    """From 12 limbs on, mul decides the rounding from the upper part of the product and must fall
+    back to the full product exactly in the boundary cases."""
+    from limbforge_b200.api import Operation
+    a, b = boundary_operands(bits)
     out, _ = engine.run(bits, Operation.mul, a, b)
     want = oracle.elementwise(bits, 2, a, b)
     assert same(out, want), f"first differing element {first_bad(out, want)}"
+
+
+@pytest.mark.parametrize("bits", [384, 512, 800, 1024])
+def test_chain_mul_near_rounding_boundaries(oracle, bits):
+    """The chain kernel's product reads the factor's words from memory inside the product; the same
+    boundary operands through a one-step chain give the oracle's products."""
+    from limbforge_b200 import api
+    a, b = boundary_operands(bits)
+    count = a.shape[0]
+    e = api.Engine()
+    X, F, O = e.make_buffer(count, bits), e.make_buffer(count, bits), e.make_buffer(count, bits)
+    X.upload(a)
+    F.upload(b)
+    api.dev_mul_chain(bits, X.device_pointer(), F.device_pointer(), count, 1, O.device_pointer(), count)
+    assert same(O.download(), oracle.elementwise(bits, 2, a, b))
+
+
+def test_chain_factor_written_earlier_in_the_chain(engine, oracle):
+    """y1 = x * f, y2 = y1 * y1, y3 = y2 * f: the second step's factor is the first step's output,
+    written earlier in the same fused kernel."""
+    from limbforge_b200.api import Operation
+    bits, count = 1024, 2048
+    rng = np.random.default_rng(12)
+    x, f = nb.random_numbers(rng, count, bits, 6), nb.random_numbers(rng, count, bits, 6)
+    X, F = engine.make_buffer(count, bits), engine.make_buffer(count, bits)
+    Y1, Y2, Y3 = (engine.make_buffer(count, bits) for _ in range(3))
+    X.upload(x)
+    F.upload(f)
+    batch = engine.batch()
+    batch.run(Operation.mul, X, F, None, Y1)
+    batch.run(Operation.mul, Y1, Y1, None, Y2)
+    batch.run(Operation.mul, Y2, F, None, Y3)
+    batch.submit().wait()
+    y1 = oracle.elementwise(bits, 2, x, f)
+    y2 = oracle.elementwise(bits, 2, y1, y1)
+    assert same(Y1.download(), y1)
+    assert same(Y2.download(), y2)
+    assert same(Y3.download(), oracle.elementwise(bits, 2, y2, f))
 
 
 @pytest.mark.parametrize("bits", [64, 224, 256, 384, 1024])
