@@ -496,49 +496,178 @@ template <int N> __device__ __noinline__ Num<N> sqrt_restoring_call(const Num<N>
 template <int N> __device__ __noinline__ Num<N> add_call(const Num<N> a, const Num<N> b);
 template <int N> __device__ __noinline__ Num<N> div_call(const Num<N> a, const Num<N> b);
 
-// RN(sqrt(a)) by Newton's iteration x <- (x + RN(a / x)) / 2 from a double-precision start, then an
-// exact check.  With Z the 2N-word radicand of sqrt_restoring and S = sqrt(Z) in [2^(32N-1), 2^(32N)),
-// the result mantissa is the integer C nearest S (there are no ties: S is an integer or irrational),
-// and C is nearest exactly when -C < Z - C^2 <= C.  The candidate from the iteration is moved a unit
-// at a time, with Z - C^2 updated exactly, until it passes.  A candidate that is not within a few
-// units, which the error bounds of the iteration rule out, takes the restoring routine.
+// a (A words) * b (B words) = p (A + B words): schoolbook rows with explicit 32-bit carries.
+template <int A, int B> __device__ __forceinline__ void mul_words(const u32 (&a)[A], const u32 (&b)[B], u32 (&p)[A + B]) {
+#pragma unroll
+    for (int k = 0; k < A + B; ++k) p[k] = 0;
+#pragma unroll
+    for (int j = 0; j < B; ++j) {
+        u32 c = 0;
+#pragma unroll
+        for (int i = 0; i < A; ++i) {
+            const u64 t = (u64)a[i] * b[j] + p[i + j] + c;
+            p[i + j] = (u32)t;
+            c = (u32)(t >> 32);
+        }
+        p[j + A] = c;
+    }
+}
+
+// Reciprocal square root in fixed point, for the candidate of sqrt.  z = Z / 2^(64N) lies in [1/4, 1) and
+// y = 1 / sqrt(z) in (1, 2].  At level M (M words) y is held as Y = y * 2^(32M - 2).  A start of 50 correct
+// bits (a double) is refined by Newton's step y' = y + y (1 - z y^2) / 2 at word counts that double
+// (4, 8, 16, ... capped at N), each giving min(2p - 2, 32M - 8) correct bits, until p >= 16N + 16.
+__host__ __device__ constexpr int rsqrt_next_level(int N, int L) { return L == 2 ? (N < 4 ? N : 4) : (2 * L < N ? 2 * L : N); }
+__host__ __device__ constexpr int rsqrt_prec_after(int p, int M) { return 2 * p - 2 < 32 * M - 8 ? 2 * p - 2 : 32 * M - 8; }
+__host__ __device__ constexpr int rsqrt_final_prec(int N) {
+    int p = 50, L = 2;
+    while (p < 16 * N + 16) { const int M = rsqrt_next_level(N, L); p = rsqrt_prec_after(p, M); L = M; }
+    return p;
+}
+// One Newton step from level L (y[0..L)) to level M >= L.  With Zm the top M words of Z:
+//   P = Y^2 = y^2 2^(64M-4); T = Zm * top_M(P) = z y^2 2^(64M-4); H = 2^(64M-4) - T = (1 - z y^2) 2^(64M-4);
+//   the correction y h / 2 at level M is Y * floor(H / 2^(32M)) / 2^(32M-3).
+template <int N, int L, int M> __device__ __forceinline__ void rsqrt_step(const u32 (&z)[2 * N], u32 (&y)[N]) {
+    u32 Y[M], Zm[M], Pt[M], Ht[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) { Y[i] = i >= M - L ? y[i - (M - L)] : 0u; Zm[i] = z[2 * N - M + i]; }
+    u32 P[2 * M];
+    mul_words<M, M>(Y, Y, P);
+#pragma unroll
+    for (int i = 0; i < M; ++i) Pt[i] = P[M + i];
+    u32 T[2 * M];
+    mul_words<M, M>(Zm, Pt, T);
+    u32 bo = 0;
+#pragma unroll
+    for (int k = 0; k < 2 * M; ++k) {
+        const u64 v = (u64)T[k] + bo;
+        const u32 kw = k == 2 * M - 1 ? 0x10000000u : 0u;
+        const u32 d = (u32)((u64)kw - v);
+        bo = (u64)kw < v;
+        if (k >= M) Ht[k - M] = d;
+    }
+    const bool neg = Ht[M - 1] >> 31;                  // z y^2 > 1: y is too large
+    if (neg) {
+        u32 cy = 1;
+#pragma unroll
+        for (int i = 0; i < M; ++i) { const u64 v = (u64)(~Ht[i]) + cy; Ht[i] = (u32)v; cy = (u32)(v >> 32); }
+    }
+    u32 Q[2 * M];
+    mul_words<M, M>(Y, Ht, Q);
+    u64 cy = 0, bw = 0;
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        const u32 corr = __funnelshift_r(Q[M - 1 + i], M + i < 2 * M ? Q[M + i] : 0u, 29);     // Q >> (32M - 3)
+        if (neg) { const u64 v = (u64)corr + bw; const u32 old = Y[i]; Y[i] = (u32)((u64)old - v); bw = (u64)old < v; }
+        else { const u64 v = (u64)Y[i] + corr + cy; Y[i] = (u32)v; cy = v >> 32; }
+    }
+#pragma unroll
+    for (int i = 0; i < M; ++i) y[i] = Y[i];
+}
+template <int N, int L, int P> __device__ __forceinline__ void rsqrt_ladder(const u32 (&z)[2 * N], u32 (&y)[N]) {
+    if constexpr (P < 16 * N + 16) {
+        constexpr int M = rsqrt_next_level(N, L);
+        rsqrt_step<N, L, M>(z, y);
+        rsqrt_ladder<N, M, rsqrt_prec_after(P, M)>(z, y);
+    } else if constexpr (L < N) {
+#pragma unroll
+        for (int i = N - 1; i >= 0; --i) y[i] = i >= N - L ? y[i - (N - L)] : 0u;     // to level N
+    }
+}
+// Candidate C (N + 1 words, c[N] = 0, C in [2^(32N-1), 2^(32N))) for S = sqrt(Z), within a few units of S.
+// C0 = Zt * Y / 2^(32N-2) (Zt the top N words of Z) is within 2^(32N-p+2) of S; one correction
+// C1 = C0 + (Z - C0^2) / (2 S) = C0 + (Z - C0^2) * Y / 2^(64N-1) leaves a second-order error below a unit
+// (p >= 16N + 16) plus the truncations below, under two units together.  Returns false when Z - C0^2 is
+// larger than these bounds allow (never expected), and the caller takes the restoring routine.
+template <int N> __device__ __forceinline__ bool sqrt_candidate(const u32 (&z)[2 * N], u32 (&c)[N + 1]) {
+    const u64 zt = ((u64)z[2 * N - 1] << 32) | z[2 * N - 2];
+    const double y0 = __drcp_rn(__dsqrt_rn((double)zt * 0x1p-64));                // (1, 2]
+    const u64 Y0 = (u64)(y0 * 0x1p62);
+    u32 y[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) y[i] = 0;
+    y[0] = (u32)Y0; y[1] = (u32)(Y0 >> 32);
+    constexpr int P = rsqrt_final_prec(N);
+    rsqrt_ladder<N, 2, 50>(z, y);
+    // C0
+    u32 Zt[N], R[2 * N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) Zt[i] = z[N + i];
+    mul_words<N, N>(Zt, y, R);
+#pragma unroll
+    for (int i = 0; i <= N; ++i) c[i] = __funnelshift_r(R[N - 1 + i], N + i < 2 * N ? R[N + i] : 0u, 30);
+    const auto clamp = [&c]() {
+        if (c[N]) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) c[i] = 0xffffffffu;
+        } else if (!(c[N - 1] >> 31)) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) c[i] = i == N - 1 ? 0x80000000u : 0u;
+        }
+        c[N] = 0;
+    };
+    clamp();
+    // D0 = Z - C0^2 (sign and magnitude)
+    u32 cm[N], sq[2 * N], d[2 * N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) cm[i] = c[i];
+    mul_words<N, N>(cm, cm, sq);
+    u32 bo = 0;
+#pragma unroll
+    for (int k = 0; k < 2 * N; ++k) { const u64 v = (u64)sq[k] + bo; d[k] = (u32)((u64)z[k] - v); bo = (u64)z[k] < v; }
+    const bool neg = bo != 0;                          // C0^2 > Z
+    if (neg) {
+        u32 cy = 1;
+#pragma unroll
+        for (int k = 0; k < 2 * N; ++k) { const u64 v = (u64)(~d[k]) + cy; d[k] = (u32)v; cy = (u32)(v >> 32); }
+    }
+    // |D0| < 2^(64N - P + 3): words [DL, DH) carry it to within 2^-31 of a unit of the correction;
+    // words [YL, N) of Y carry the product to within a quarter unit.
+    constexpr int DL = N - 1;
+    constexpr int DH = (64 * N - P + 4 + 31) / 32 < 2 * N ? (64 * N - P + 4 + 31) / 32 : 2 * N;
+    constexpr int YL = (P - 6) / 32 < N - 1 ? (P - 6) / 32 : N - 1;
+    static_assert(DH > DL, "correction window");
+    u32 hi = 0;
+#pragma unroll
+    for (int k = DH; k < 2 * N; ++k) hi |= d[k];
+    if (hi) return false;
+    u32 dw[DH - DL], yw[N - YL], pr[DH - DL + N - YL];
+#pragma unroll
+    for (int k = 0; k < DH - DL; ++k) dw[k] = d[DL + k];
+#pragma unroll
+    for (int k = 0; k < N - YL; ++k) yw[k] = y[YL + k];
+    mul_words<DH - DL, N - YL>(dw, yw, pr);
+    // delta = pr >> SH with SH = 64N - 1 - 32 (DL + YL) bits
+    constexpr int SH = 64 * N - 1 - 32 * (DL + YL);
+    constexpr int SW = SH / 32, SB = SH % 32;
+    constexpr int PW = DH - DL + N - YL;
+    u64 cy = 0, bw = 0;
+#pragma unroll
+    for (int i = 0; i <= N; ++i) {
+        const u32 lo = SW + i < PW ? pr[SW + i] : 0u;
+        const u32 up = SW + i + 1 < PW ? pr[SW + i + 1] : 0u;
+        const u32 dl = SB ? __funnelshift_r(lo, up, SB) : lo;
+        if (neg) { const u64 v = (u64)dl + bw; const u32 old = c[i]; c[i] = (u32)((u64)old - v); bw = (u64)old < v; }
+        else { const u64 v = (u64)c[i] + dl + cy; c[i] = (u32)v; cy = v >> 32; }
+    }
+    if (neg && (c[N] >> 31)) {                           // below zero: not reachable from C0 >= 2^(32N-1)
+#pragma unroll
+        for (int i = 0; i <= N; ++i) c[i] = i == N - 1 ? 0x80000000u : 0u;
+    }
+    clamp();
+    return true;
+}
+
+// RN(sqrt(a)).  With Z the 2N-word radicand of sqrt_restoring and S = sqrt(Z) in [2^(32N-1), 2^(32N)),
+// the result mantissa is the integer C nearest S (there are no ties: S is an integer or irrational), and C
+// is nearest exactly when -C < Z - C^2 <= C.  The candidate from sqrt_candidate (multiplications only) is
+// moved a unit at a time, with Z - C^2 updated exactly, until it passes.  A candidate that is not within a
+// few units, which its error bounds rule out, takes the restoring routine.
 template <int N> __device__ __forceinline__ Num<N> sqrt(const Num<N>& a) {
     if (a.st || !a.s) return zero<N>(a.st);
     if (a.s < 0) return zero<N>(kInvalid);
     int e = a.e / 2; if (a.e < 0 && (a.e % 2)) --e;
     const int odd = a.e - 2 * e;                    // 0 or 1
-    // start: the top 64 bits of the mantissa as a double in [1, 2), its root in [1, 2)
-    const double f = (double)(((u64)a.m[N - 1] << 32) | a.m[N - 2]) * 0x1p-63;
-    const double r0 = fmin(__dsqrt_rn(odd ? 2.0 * f : f), 0x1.fffffffffffffp0);   // f may round up to 2
-    const u64 rb = (u64)(r0 * 0x1p63);              // top bit set: r0 >= 1
-    Num<N> x;
-#pragma unroll
-    for (int i = 0; i < N; ++i) x.m[i] = 0;
-    x.m[N - 1] = (u32)(rb >> 32); x.m[N - 2] = (u32)rb;
-    x.e = e; x.s = 1; x.st = 0;
-    constexpr int iters = 32 * N <= 104 ? 2 : 32 * N <= 208 ? 3 : 32 * N <= 416 ? 4 : 32 * N <= 832 ? 5 : 6;
-#pragma unroll 1
-    for (int it = 0; it < iters; ++it) {
-        Num<N> y;
-        if constexpr (N > 8) y = add_call<N>(x, div_call<N>(a, x)); else y = add<N>(x, div<N>(a, x));
-        y.e -= 1;
-        x = y;
-    }
-    // candidate C (N words + carry word), aligned to the exponent e
-    u32 c[N + 1];
-    if (x.e == e) {
-#pragma unroll
-        for (int i = 0; i < N; ++i) c[i] = x.m[i];
-    } else if (x.e == e + 1) {
-#pragma unroll
-        for (int i = 0; i < N; ++i) c[i] = 0xffffffffu;
-    } else if (x.e == e - 1) {
-#pragma unroll
-        for (int i = 0; i < N; ++i) c[i] = i == N - 1 ? 0x80000000u : 0u;
-    } else {
-        return sqrt_restoring_call<N>(a);
-    }
-    c[N] = 0;
     // Z (2N words) and D = Z - C^2 (2N + 1 words, two's complement)
     u32 z[2 * N];
 #pragma unroll
@@ -549,6 +678,8 @@ template <int N> __device__ __forceinline__ Num<N> sqrt(const Num<N>& a) {
 #pragma unroll
         for (int k = 0; k < 2 * N; ++k) z[k] = (z[k] >> 1) | (k + 1 < 2 * N ? z[k + 1] << 31 : 0u);
     }
+    u32 c[N + 1];
+    if (!sqrt_candidate<N>(z, c)) return sqrt_restoring_call<N>(a);
     u32 cm[N], p[2 * N];
 #pragma unroll
     for (int i = 0; i < N; ++i) cm[i] = c[i];

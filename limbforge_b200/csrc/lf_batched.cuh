@@ -102,7 +102,8 @@ struct GemmWork {
 //   fused    re: dot2_add(ar, br, -ai, bi, sum)             im: dot2_add(ar, bi, ai, br, sum)
 // exactly the re / im parts of cadd(cmul(a, b), sum) and cfma(a, b, sum).
 // One k step of one complex component: sum <- the composed or fused update with x = a_ik, y = b_kj.
-// Operands are loaded next to their use, so only the running sum lives across products; above 8 limbs
+// Operands are loaded next to their use (the second factor of a product word by word inside it, mul_mem),
+// so only the running sum lives across products; above 8 limbs
 // the step is an out-of-line call, which keeps the kernel's register allocation to that sum.
 template <int N, bool FUSED> __device__ __forceinline__ void cx_step_body(Num<N>& sum, const u32* x, const u32* y, int comp) {
     constexpr u64 E = N + 3;
@@ -112,8 +113,8 @@ template <int N, bool FUSED> __device__ __forceinline__ void cx_step_body(Num<N>
         const Num<N> xi = load<N>(x + E);
         sum = dot2_add<N>(load<N>(x), load<N>(yr), comp ? xi : negate<N>(xi), load<N>(yi), sum);
     } else {
-        const Num<N> p1 = mul<N>(load<N>(x), load<N>(yr));
-        const Num<N> p2 = mul<N>(load<N>(x + E), load<N>(yi));
+        const Num<N> p1 = mul_mem<N>(load<N>(x), yr);
+        const Num<N> p2 = mul_mem<N>(load<N>(x + E), yi);
         sum = add<N>(comp ? add<N>(p1, p2) : sub<N>(p1, p2), sum);
     }
 }
@@ -149,8 +150,8 @@ template <int N> __device__ void gemm_cell_parked(const u32* A, const u32* B, co
     for (u64 kk = 0; kk < k; ++kk) {
         const u32* x = A + (i * k + kk) * S;
         const u32* y = B + (kk * n + j) * S;
-        park<N>(sp1, stride, mul<N>(load<N>(x), load<N>(y + (comp ? E : 0))));
-        const Num<N> p2 = mul<N>(load<N>(x + E), load<N>(y + (comp ? 0 : E)));
+        park<N>(sp1, stride, mul_mem<N>(load<N>(x), y + (comp ? E : 0)));
+        const Num<N> p2 = mul_mem<N>(load<N>(x + E), y + (comp ? 0 : E));
         const Num<N> p1 = unpark<N>(sp1, stride);
         park<N>(sp1, stride, comp ? add<N>(p1, p2) : sub<N>(p1, p2));
         park<N>(ssum, stride, add<N>(unpark<N>(sp1, stride), unpark<N>(ssum, stride)));

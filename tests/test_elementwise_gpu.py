@@ -167,6 +167,51 @@ def test_chain_factor_written_earlier_in_the_chain(engine, oracle):
     assert same(Y3.download(), oracle.elementwise(bits, 2, y2, f))
 
 
+def sqrt_operands(bits, cnt=2048):
+    """Positive radicands for sqrt: random values of both exponent parities, exact squares, roots just
+    below and just above a half unit (the rounding boundary), and the ends of the binade."""
+    n = bits // 32
+    rng = np.random.default_rng(bits + 77)
+    x = nb.random_numbers(rng, cnt, bits, 60)
+    x[:, n + 1] = 1
+    q = cnt // 8
+
+    def put(row, m, odd):
+        for w in range(n):
+            x[row, w] = (m >> (32 * w)) & 0xFFFFFFFF
+        x[row, n] = np.int32(2 * int(rng.integers(-20, 21)) + odd).view(np.uint32)
+
+    # the radicand is Z = m 2^(32n) for an odd exponent, m 2^(32n-1) for an even one
+    for t in range(q):                                     # exact squares
+        r = (int(rng.integers(1 << 30, 1 << 31)) << (32 * n - 31)) >> (16 * n) << (16 * n)
+        r |= 1 << (32 * n - 1)
+        z = r * r
+        if z >> (64 * n - 1):
+            put(t, z >> (32 * n), 1)
+        else:
+            put(t, z >> (32 * n - 1), 0)
+    for t in range(q, 3 * q):                              # sqrt(Z) within a hair of k + 1/2
+        k = int.from_bytes(rng.bytes(4 * n), "little") | (1 << (32 * n - 1))
+        z = k * k + k                                      # (k + 1/2)^2 - 1/4
+        odd = 1 if z >> (64 * n - 1) else 0
+        sh = 32 * n if odd else 32 * n - 1
+        put(t, (z >> sh) + (t & 1), odd)
+    for t in range(3 * q, 4 * q):                          # binade ends: 2^(32n-1) and 2^(32n) - 1
+        put(t, (1 << (32 * n - 1)) if t & 2 else (1 << (32 * n)) - 1, t & 1)
+    return x
+
+
+@pytest.mark.parametrize("bits", list(range(64, 1025, 32)))
+def test_sqrt_all_widths_and_hard_cases(engine, oracle, bits):
+    """sqrt's candidate comes from a fixed-point reciprocal square root and one exact correction; the
+    exact check must then land on the oracle's correctly rounded root at every width."""
+    from limbforge_b200.api import Operation
+    x = sqrt_operands(bits)
+    out, _ = engine.run_unary(bits, Operation.sqrt, x)
+    want = oracle.elementwise(bits, 8, x)
+    assert same(out, want), f"first differing element {first_bad(out, want)}"
+
+
 @pytest.mark.parametrize("bits", [64, 224, 256, 384, 1024])
 def test_broadcast_operands(engine, oracle, bits):
     """tests/test_broadcast.cpp: b (and c) read at (i / stride) % period."""
