@@ -71,7 +71,11 @@ public:
     }
 };
 namespace detail {
-struct Access { template <class T> static lf_buffer* h(const Buffer<T>& b) { return b.handle(); } };
+struct Access {
+    template <class T> static lf_buffer* h(const Buffer<T>& b) { return b.handle(); }
+    template <class T> static std::shared_ptr<BufferRef> ref(const Buffer<T>& b) { return b.ref_; }
+    template <class T> static Buffer<T> view(std::shared_ptr<BufferRef> r, std::size_t n) { return Buffer<T>(std::move(r), n); }
+};
 }
 
 class Submission {

@@ -18,6 +18,8 @@ struct CholeskyInfo {
     std::size_t blocks = 0, gpu_updates = 0, host_updates = 0;
     double panel_seconds = 0, update_seconds = 0;
 };
+// Device memory a Linalg retains between calls (linalg.hpp:46-52), in bytes.
+struct LinalgWorkspaces { std::size_t scratch_bytes = 0, idle_bytes = 0, busy_bytes = 0, busy_workspaces = 0; };
 struct LinalgReport {
     std::size_t m = 0, n = 0, k = 0, gpu_outputs = 0, trivial_outputs = 0, gemm_rows = 0, gemm_cols = 0, int8_gemms = 0, moduli = 0, band_bits = 0;
     double analysis_seconds = 0, gpu_seconds = 0;
@@ -71,6 +73,17 @@ public:
         r_ = {c.m, c.n, c.k, c.gpu_outputs, c.trivial_outputs, c.gemm_rows, c.gemm_cols, c.int8_gemms, c.moduli, c.band_bits,
               c.analysis_seconds, c.gpu_seconds, c.method};
         return r_;
+    }
+    // Retained memory and its release (linalg.hpp:173-180): scratch and idle resident workspaces are freed now,
+    // busy ones with their batches; the result is what was retained before the release.  Call between this
+    // Linalg's calls, on its host thread.
+    LinalgWorkspaces workspaces() const {
+        lf_linalg_workspaces w{}; detail::check(lf_linalg_get_workspaces(l_.get(), &w));
+        return {w.scratch_bytes, w.idle_bytes, w.busy_bytes, w.busy_workspaces};
+    }
+    LinalgWorkspaces release_workspaces() {
+        lf_linalg_workspaces w{}; detail::check(lf_linalg_release_workspaces(l_.get(), &w));
+        return {w.scratch_bytes, w.idle_bytes, w.busy_bytes, w.busy_workspaces};
     }
     Timing syrk(int bits, const void* A, std::size_t rows, std::size_t cols, void* C, bool lower_only = true, bool subtract = false) {
         lf_timing t{}; detail::check(lf_linalg_syrk(l_.get(), bits, A, rows, cols, C, lower_only, subtract, &t)); return detail::timing(t);

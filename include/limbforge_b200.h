@@ -131,6 +131,7 @@ int lf_dev_exact_product_static(int bits, const void* left, size_t left_ls, size
 int lf_buffer_create(lf_engine* engine, size_t bytes, lf_buffer** out);                /* Engine::make_buffer */
 void lf_buffer_release(lf_buffer* buffer);                                              /* last reference frees */
 size_t lf_buffer_bytes(const lf_buffer* buffer);                                        /* Buffer::size (bytes) */
+int lf_buffer_holders(const lf_buffer* buffer);   /* batches and unwaited submissions holding the buffer (workspace accounting) */
 int lf_buffer_upload(lf_buffer* buffer, const void* source, size_t bytes);              /* Buffer::upload */
 int lf_buffer_download(lf_buffer* buffer, void* target, size_t bytes);                  /* Buffer::download */
 /* Buffer::mapped (engine.hpp:82): a host view, current as of this call; host writes through it
@@ -182,6 +183,13 @@ int lf_linalg_batch_syrk(lf_linalg* la, lf_batch* batch, int bits, lf_buffer* A,
 int lf_linalg_ticket_resolved(lf_linalg_ticket* ticket, int* resolved);                 /* LinalgTicket::resolved */
 int lf_linalg_ticket_report(lf_linalg_ticket* ticket, lf_linalg_report* report);         /* LinalgTicket::report */
 void lf_linalg_ticket_destroy(lf_linalg_ticket* ticket);
+/* Linalg::workspaces / release_workspaces (linalg.hpp:46-52, 173-180): bytes of device memory the Linalg retains:
+ * scratch of the host-array calls and factorizations; resident-product workspaces idle (their batch has run)
+ * or busy (unsubmitted or in flight).  release frees the scratch and the idle workspaces (tickets keep their
+ * reports) and returns what was retained before it; busy workspaces are freed with their batches. */
+typedef struct lf_linalg_workspaces { size_t scratch_bytes, idle_bytes, busy_bytes, busy_workspaces; } lf_linalg_workspaces;
+int lf_linalg_get_workspaces(lf_linalg* linalg, lf_linalg_workspaces* out);
+int lf_linalg_release_workspaces(lf_linalg* linalg, lf_linalg_workspaces* out);
 
 /* ---- Precision casts and tree sums (engine.hpp:150-175,205; kernels.metal:60-112,251-266).
  * cast: exact widening, round-to-nearest-even narrowing, complex componentwise; a status element or a

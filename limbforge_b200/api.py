@@ -178,6 +178,10 @@ class _CholeskyInfo(C.Structure):
                 ("panel_seconds", C.c_double), ("update_seconds", C.c_double)]
 
 
+class _LinalgWorkspaces(C.Structure):
+    _fields_ = [(f, C.c_size_t) for f in ("scratch_bytes", "idle_bytes", "busy_bytes", "busy_workspaces")]
+
+
 class _LinalgReport(C.Structure):
     _fields_ = [(f, C.c_size_t) for f in ("m", "n", "k", "gpu_outputs", "trivial_outputs", "gemm_rows", "gemm_cols",
                                           "int8_gemms", "moduli", "band_bits")] + \
@@ -243,6 +247,8 @@ def _load() -> C.CDLL:
         "lf_linalg_batch_syrk": ([V, V, I, V, S, S, V, I, I, P(V)], I),
         "lf_linalg_ticket_resolved": ([V, P(I)], I), "lf_linalg_ticket_report": ([V, P(_LinalgReport)], I),
         "lf_linalg_ticket_destroy": ([V], None),
+        "lf_linalg_get_workspaces": ([V, P(_LinalgWorkspaces)], I), "lf_linalg_release_workspaces": ([V, P(_LinalgWorkspaces)], I),
+        "lf_buffer_holders": ([V], I),
         "lf_engine_cast": ([V, I, I, I, V, V, S, P(_Timing)], I),
         "lf_batch_cast": ([V, I, I, I, V, V, S], I), "lf_batch_tree_sum": ([V, I, I, V, V, S], I),
         "lf_dev_cast": ([I, I, I, V, V, S, V], I), "lf_dev_tree_sum": ([I, I, V, S, V, V, V], I),
@@ -502,6 +508,7 @@ class BatchedLinalg:
 
     def __init__(self, engine: Engine):
         self.engine = engine
+        self._spaces: list = []
 
     @staticmethod
     def _shape(s: StridedGemm) -> _StridedGemm:
@@ -518,6 +525,40 @@ class BatchedLinalg:
     def gemm_resident(self, batch: CommandBatch, s: StridedGemm, A: Buffer, B: Buffer, C_: Buffer) -> None:
         sh = self._shape(s)
         check(lib.lf_batch_strided_gemm(batch.handle, A.bits, int(A.complex), C.byref(sh), A.handle, B.handle, C_.handle))
+
+    def product3(self, batch: CommandBatch, first: StridedGemm, second: StridedGemm, A: Buffer, B: Buffer, D: Buffer, C_: Buffer,
+                 negative=False) -> None:
+        """C_b = (A_b B_b) D_b (batched_linalg.hpp:99-110) through an intermediate kept by this BatchedLinalg."""
+        import dataclasses
+        if first.count != second.count or first.m != second.m or first.n != second.k or first.accumulate or second.accumulate:
+            raise InvalidArgument("product3: incompatible shapes or accumulation")
+        first = dataclasses.replace(first, stride_c=first.m * first.n)
+        second = dataclasses.replace(second, stride_a=first.m * first.n, negative=bool(negative))
+        count = max(first.count * first.stride_c, 1)
+        tmp = next((b for b in self._spaces if b.bits == A.bits and b.complex == A.complex and b.count >= count
+                    and lib.lf_buffer_holders(b.handle) == 0), None)
+        if tmp is None:
+            tmp = self.engine.make_buffer(count, A.bits, A.complex)
+            self._spaces.append(tmp)
+        self.gemm_resident(batch, first, A, B, tmp)
+        self.gemm_resident(batch, second, tmp, D, C_)
+
+    def workspaces(self) -> dict:
+        """product3 intermediates: idle (held by no batch or unwaited submission) and busy bytes."""
+        w = {"idle_bytes": 0, "busy_bytes": 0, "busy_workspaces": 0}
+        for b in self._spaces:
+            size = 4 * b.words * b.count
+            if lib.lf_buffer_holders(b.handle) == 0:
+                w["idle_bytes"] += size
+            else:
+                w["busy_bytes"] += size
+                w["busy_workspaces"] += 1
+        return w
+
+    def release_workspaces(self) -> dict:
+        w = self.workspaces()
+        self._spaces = []
+        return w
 
 
 @dataclass
@@ -655,6 +696,18 @@ class Linalg:
         r = _LinalgReport()
         check(lib.lf_linalg_get_report(self.handle, C.byref(r)))
         return {f: getattr(r, f) for f, _ in r._fields_}
+
+    def workspaces(self) -> dict:
+        """Device memory retained between calls (linalg.hpp:46-52, 179): scratch, idle and busy resident workspaces."""
+        w = _LinalgWorkspaces()
+        check(lib.lf_linalg_get_workspaces(self.handle, C.byref(w)))
+        return {f: getattr(w, f) for f, _ in w._fields_}
+
+    def release_workspaces(self) -> dict:
+        """Frees the scratch and idle resident workspaces (linalg.hpp:173-180); returns what was retained before."""
+        w = _LinalgWorkspaces()
+        check(lib.lf_linalg_release_workspaces(self.handle, C.byref(w)))
+        return {f: getattr(w, f) for f, _ in w._fields_}
 
     def gemm(self, bits, transpose_a, A, B, m, n, k, C_, subtract=False) -> Timing:
         t = _Timing()

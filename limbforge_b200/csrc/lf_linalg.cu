@@ -20,6 +20,7 @@ struct Linalg {
     DevBuf work[6];
     DevBuf info_buf, error_buf, lines;
     ResidueEngine residue;
+    std::vector<std::weak_ptr<ResidentProduct>> resident;   // recorded resident products, for workspaces()
 };
 
 using Clock = std::chrono::steady_clock;
@@ -400,10 +401,21 @@ void resident_common(lf_linalg* la, lf_batch* bt, lf_buffer* C) {
     if (la->engine != bt->engine) throw invalid_argument("resident product: the batch belongs to another engine than the Linalg");
     if (!C) throw invalid_argument("missing output buffer");
 }
-void resident_record(lf_batch* bt, std::shared_ptr<ResidentProduct> prod, lf_linalg_ticket** out) {
+void resident_record(lf_linalg* la, lf_batch* bt, std::shared_ptr<ResidentProduct> prod, lf_linalg_ticket** out) {
+    auto& list = la->resident;
+    list.erase(std::remove_if(list.begin(), list.end(), [](const std::weak_ptr<ResidentProduct>& w) { return w.expired(); }), list.end());
+    list.push_back(prod);
+    // the product counts as held by the batch until the batch's last copy of the op is gone
+    struct BatchHold {
+        std::shared_ptr<ResidentProduct> p;
+        ~BatchHold() { if (p) resident_product_hold(*p, false); }
+    };
+    auto hold = std::make_shared<BatchHold>();
+    hold->p = prod;
+    resident_product_hold(*prod, true);
     Op o;
     o.kind = kCustom;
-    o.custom = [prod](cudaStream_t s) { resident_product_launch(*prod, s); };
+    o.custom = [hold](cudaStream_t s) { resident_product_launch(*hold->p, s); };
     bt->ops.push_back(o);
     *out = new lf_linalg_ticket{std::move(prod)};
 }
@@ -428,7 +440,7 @@ int lf_linalg_batch_gemm(lf_linalg* la, lf_batch* bt, int bits, int transpose_a,
     const auto* a = static_cast<const uint32_t*>(A->dev);
     lfd::LineView lv = transpose_a ? lfd::LineView{a, 1, m} : lfd::LineView{a, k, 1};
     lfd::LineView rv{static_cast<const uint32_t*>(B->dev), 1, n};
-    resident_record(bt, resident_product_create(bits, lv, rv, m, n, k, static_cast<uint32_t*>(C->dev), n, subtract != 0, false, false, limb),
+    resident_record(la, bt, resident_product_create(bits, lv, rv, m, n, k, static_cast<uint32_t*>(C->dev), n, subtract != 0, false, false, limb),
                     out);
     LF_API_END
 }
@@ -449,7 +461,7 @@ int lf_linalg_batch_syrk(lf_linalg* la, lf_batch* bt, int bits, lf_buffer* A, si
     bt->engine->activate();
     const bool limb = la->options.method == 1 || la->options.force_fallback;
     lfd::LineView v{static_cast<const uint32_t*>(A->dev), 1, cols};
-    resident_record(bt, resident_product_create(bits, v, v, cols, cols, rows, static_cast<uint32_t*>(C->dev), cols, subtract != 0, true,
+    resident_record(la, bt, resident_product_create(bits, v, v, cols, cols, rows, static_cast<uint32_t*>(C->dev), cols, subtract != 0, true,
                                                 !lower_only, limb), out);
     LF_API_END
 }
@@ -471,5 +483,51 @@ int lf_linalg_ticket_report(lf_linalg_ticket* t, lf_linalg_report* rep) {
     LF_API_END
 }
 void lf_linalg_ticket_destroy(lf_linalg_ticket* t) { delete t; }
+
+// Linalg::workspaces / release_workspaces (linalg.hpp:173-180): device memory the Linalg retains between
+// calls.  Scratch is the staging and work memory of the host-array calls and factorizations; a resident
+// product's workspace is idle once its batch has run and busy while the batch is unsubmitted or in flight.
+static lf_linalg_workspaces linalg_workspaces(Linalg& la) {
+    lf_linalg_workspaces w{};
+    for (auto& b : la.work) w.scratch_bytes += b.bytes;
+    w.scratch_bytes += la.info_buf.bytes + la.error_buf.bytes + la.lines.bytes + la.residue.bytes();
+    for (auto& weak : la.resident) {
+        auto r = weak.lock();
+        if (!r) continue;
+        const size_t b = resident_product_bytes(*r);
+        if (!b) continue;                               // released
+        if (resident_product_busy(*r)) { w.busy_bytes += b; ++w.busy_workspaces; }
+        else w.idle_bytes += b;
+    }
+    return w;
+}
+int lf_linalg_get_workspaces(lf_linalg* la, lf_linalg_workspaces* out) {
+    LF_API_BEGIN
+    if (!la || !out) throw invalid_argument("null argument");
+    la->engine->activate();
+    *out = linalg_workspaces(*la);
+    LF_API_END
+}
+// Frees the scratch and the idle resident workspaces now (their tickets keep their reports); busy ones stay
+// with their batches and are freed with them.  Returns what was retained before the release.  Later calls
+// allocate afresh.  Call between this Linalg's calls, on its host thread.
+int lf_linalg_release_workspaces(lf_linalg* la, lf_linalg_workspaces* out) {
+    LF_API_BEGIN
+    if (!la) throw invalid_argument("null linalg");
+    la->engine->activate();
+    cuda_check(cudaStreamSynchronize(la->engine->stream), "release workspaces");
+    const lf_linalg_workspaces w = linalg_workspaces(*la);
+    for (auto& b : la->work) b = DevBuf{};
+    la->info_buf = DevBuf{}; la->error_buf = DevBuf{}; la->lines = DevBuf{};
+    la->residue.release();
+    auto& list = la->resident;
+    for (auto& weak : list) if (auto r = weak.lock()) resident_product_release(*r);
+    list.erase(std::remove_if(list.begin(), list.end(), [](const std::weak_ptr<ResidentProduct>& x) {
+        auto r = x.lock();
+        return !r || resident_product_bytes(*r) == 0;
+    }), list.end());
+    if (out) *out = w;
+    LF_API_END
+}
 
 }  // extern "C"

@@ -350,6 +350,10 @@ struct ResidentProduct {
     CUtensorMap ta1{}, ta0{}, tb1{}, tb0{};
     cudaEvent_t done = nullptr;
     bool launched = false;
+    bool in_batch = false;              // recorded in a batch that still exists
+    bool kept = false;                  // plan and error word copied to the host
+    lfd::ResPlan kept_plan{};
+    uint32_t kept_error = 0;
     ~ResidentProduct() { if (done) cudaEventDestroy(done); }
 };
 
@@ -420,6 +424,7 @@ std::shared_ptr<ResidentProduct> resident_product_create(int bits, lfd::LineView
 }
 
 void resident_product_launch(ResidentProduct& r, cudaStream_t s) {
+    if (!r.error.p) throw std::logic_error("resident product: its workspace was released");
     uint32_t* err = static_cast<uint32_t*>(r.error.p);
     cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
     const auto* lk = lfd::linalg_kernels(r.n);
@@ -484,12 +489,35 @@ bool resident_product_done(ResidentProduct& r) {
     return true;
 }
 
-bool resident_product_report(ResidentProduct& r, lf_linalg_report& rep) {
+static void keep_outcome(ResidentProduct& r) {
+    if (r.kept) return;
     cuda_check(cudaEventSynchronize(r.done), "resident product");
-    lfd::ResPlan p{};
-    uint32_t e = 0;
-    if (r.residue) cuda_check(cudaMemcpy(&p, r.plan.p, sizeof p, cudaMemcpyDeviceToHost), "plan");
-    cuda_check(cudaMemcpy(&e, r.error.p, 4, cudaMemcpyDeviceToHost), "error word");
+    if (r.residue) cuda_check(cudaMemcpy(&r.kept_plan, r.plan.p, sizeof r.kept_plan, cudaMemcpyDeviceToHost), "plan");
+    cuda_check(cudaMemcpy(&r.kept_error, r.error.p, 4, cudaMemcpyDeviceToHost), "error word");
+    r.kept = true;
+}
+
+size_t resident_product_bytes(const ResidentProduct& r) {
+    return r.lines.bytes + r.planes.bytes + r.res.bytes + r.plan.bytes + r.cands.bytes + r.cum.bytes + r.error.bytes + r.sf.bytes;
+}
+
+void resident_product_hold(ResidentProduct& r, bool held) { r.in_batch = held; }
+
+bool resident_product_busy(ResidentProduct& r) { return r.launched ? !resident_product_done(r) : r.in_batch; }
+
+size_t resident_product_release(ResidentProduct& r) {
+    if (resident_product_busy(r)) return 0;
+    if (r.launched) keep_outcome(r);
+    const size_t b = resident_product_bytes(r);
+    r.lines = DevBuf{}; r.planes = DevBuf{}; r.res = DevBuf{}; r.plan = DevBuf{}; r.cands = DevBuf{}; r.cum = DevBuf{};
+    r.error = DevBuf{}; r.sf = DevBuf{};
+    return b;
+}
+
+bool resident_product_report(ResidentProduct& r, lf_linalg_report& rep) {
+    keep_outcome(r);
+    const lfd::ResPlan p = r.kept_plan;
+    const uint32_t e = r.kept_error;
     rep = lf_linalg_report{};
     rep.m = r.M; rep.n = r.Nc; rep.k = r.K;
     rep.method = p.mode == 1 ? 2 : 1;

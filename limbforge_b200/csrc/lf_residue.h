@@ -10,6 +10,8 @@ namespace lfr {
 
 struct ResidueEngine {
     DevBuf lines, planes, residues, tables, misc;
+    size_t bytes() const { return lines.bytes + planes.bytes + residues.bytes + tables.bytes + misc.bytes; }
+    void release() { lines = DevBuf{}; planes = DevBuf{}; residues = DevBuf{}; tables = DevBuf{}; misc = DevBuf{}; }
     bool run(int bits, lfd::LineView left, lfd::LineView right, uint64_t M, uint64_t Nc, uint64_t K, uint32_t* C,
              uint64_t ldc, bool subtract, bool lower, uint32_t* error, cudaStream_t s, bool forced, lf_linalg_report& report);
 };
@@ -39,6 +41,13 @@ std::shared_ptr<ResidentProduct> resident_product_create(int bits, lfd::LineView
                                                          bool mirror, bool limb_only);
 void resident_product_launch(ResidentProduct& r, cudaStream_t s);
 bool resident_product_done(ResidentProduct& r);              // the launch has completed on the GPU
+size_t resident_product_bytes(const ResidentProduct& r);     // device workspace the product holds now
+void resident_product_hold(ResidentProduct& r, bool held);  // recorded in a live batch, or that batch is gone
+// Busy: recorded in a live batch and not launched yet, or launched and not completed.
+bool resident_product_busy(ResidentProduct& r);
+// Frees the product's device workspace unless it is busy (a completed product keeps its report on the host);
+// returns the bytes freed.
+size_t resident_product_release(ResidentProduct& r);
 // Fills the engine, modulus count and band; returns false when a cluster overflowed the exact window.
 bool resident_product_report(ResidentProduct& r, lf_linalg_report& rep);
 }  // namespace lfr

@@ -263,6 +263,8 @@ int lf_buffer_create(lf_engine* e, size_t bytes, lf_buffer** out) {
 }
 void lf_buffer_release(lf_buffer* b) { release(b); }
 size_t lf_buffer_bytes(const lf_buffer* b) { return b ? b->bytes : 0; }
+// References to the buffer besides its owner's: batches that recorded it and submissions not yet waited.
+int lf_buffer_holders(const lf_buffer* b) { return b ? b->refs.load(std::memory_order_acquire) - 1 : 0; }
 static void idle(const Buffer* b) {
     if (!b) throw invalid_argument("empty buffer handle");
     if (b->busy.load(std::memory_order_acquire)) throw logic_error("buffer belongs to an unwaited submission");

@@ -64,6 +64,14 @@ int main() {
         std::vector<Float<B>> L(9);
         CholeskyInfo info = la.cholesky(B, C.data(), 3, L.data());
         if (info.pivot != 3 || L[4].exponent != 1) { std::printf("cholesky FAILED\n"); return 1; }
+        {   // retained memory: the calls above left scratch; release frees it and later calls allocate afresh
+            const LinalgWorkspaces w = la.workspaces();
+            const LinalgWorkspaces r = la.release_workspaces();
+            if (!w.scratch_bytes || r.scratch_bytes != w.scratch_bytes || la.workspaces().scratch_bytes) { std::printf("workspaces FAILED\n"); return 1; }
+            std::vector<Float<B>> C3(9);
+            la.syrk(B, A.data(), 3, 3, C3.data(), false);
+            if (std::memcmp(C3.data(), C.data(), sizeof(Float<B>) * 9)) { std::printf("syrk after release FAILED\n"); return 1; }
+        }
         std::printf("linalg ok\n");
         BatchedLinalg bl(e);
         StridedGemm s; s.count = 1; s.m = s.n = s.k = 2; s.stride_a = s.stride_b = s.stride_c = 4;
@@ -72,6 +80,22 @@ int main() {
         for (auto& z : cb) z = {power<B>(1), zero<B / 32>()};
         bl.gemm(B, true, s, ca.data(), cb.data(), cc.data());
         if (cc[0].re.exponent != 2) { std::printf("batched gemm FAILED\n"); return 1; }
+        {   // (A B) D through product3's intermediate: ones x twos = 4 per entry, times ones = 8 = 2^3
+            auto bA = e.make_buffer<Complex<B / 32>>(4), bB = e.make_buffer<Complex<B / 32>>(4);
+            auto bD = e.make_buffer<Complex<B / 32>>(4), bC = e.make_buffer<Complex<B / 32>>(4);
+            bA.upload(ca.data(), 4); bB.upload(cb.data(), 4); bD.upload(ca.data(), 4);
+            auto pb = e.batch();
+            bl.product3(pb, s, s, bA, bB, bD, bC);
+            if (bl.workspaces().busy_workspaces != 1) { std::printf("product3 workspace FAILED\n"); return 1; }
+            pb.submit().wait();
+            std::vector<Complex<B / 32>> c3(4);
+            bC.download(c3.data(), 4);
+            for (auto& z : c3) if (z.re.exponent != 3 || z.im.sign != 0) { std::printf("product3 FAILED\n"); return 1; }
+            const BatchedWorkspaces w = bl.workspaces();
+            if (w.busy_workspaces || !w.idle_bytes || bl.release_workspaces().idle_bytes != w.idle_bytes || bl.workspaces().idle_bytes) {
+                std::printf("batched workspaces FAILED\n"); return 1;
+            }
+        }
         std::printf("batched ok\n");
         bool threw = false;
         try { e.run(100, Operation::add, a.data(), b.data(), out.data(), 1); } catch (const std::invalid_argument&) { threw = true; }

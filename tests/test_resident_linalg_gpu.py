@@ -109,3 +109,83 @@ def test_resident_errors(engine, la):
     other = api.Engine()
     with pytest.raises(api.InvalidArgument):
         la.gemm_resident(other.batch(), False, b1, b2, 4, 4, 4, engine.make_buffer(16, bits))
+
+
+def test_workspaces_scratch_idle_busy_and_release(engine):
+    """Linalg::workspaces / release_workspaces (linalg.hpp:173-180): host-array calls leave scratch; a resident
+    product's workspace is busy while its batch is unsubmitted and idle once the batch has run; release frees
+    scratch and idle workspaces, returns what was retained, keeps tickets' reports and leaves later calls exact."""
+    bits, m, k = 256, 24, 40
+    rng = np.random.default_rng(3)
+    la = api.Linalg(engine)
+    A = matrix(bits, k, m, "moderate", rng)
+    C1 = np.zeros((m * m, bits // 32 + 3), np.uint32)
+    la.syrk(bits, A, k, m, C1, lower_only=False)
+    w = la.workspaces()
+    assert w["scratch_bytes"] > 0 and w["busy_workspaces"] == 0
+    bA, bC = upload(engine, A, bits), upload(engine, np.zeros_like(C1), bits)
+    batch = engine.batch()
+    ticket = la.syrk_resident(batch, bA, k, m, bC, lower_only=False)
+    w = la.workspaces()
+    assert w["busy_workspaces"] == 1 and w["busy_bytes"] > 0 and w["idle_bytes"] == 0
+    batch.submit().wait()
+    w = la.workspaces()
+    assert w["busy_workspaces"] == 0 and w["idle_bytes"] > 0
+    report = ticket.report()
+    orphan_batch = engine.batch()                             # recorded, then dropped unsubmitted: idle
+    orphan = la.syrk_resident(orphan_batch, bA, k, m, upload(engine, np.zeros_like(C1), bits), lower_only=False)
+    assert la.workspaces()["busy_workspaces"] == 1
+    del orphan_batch
+    before = la.workspaces()
+    assert before["busy_workspaces"] == 0 and before["idle_bytes"] > w["idle_bytes"]
+    assert la.release_workspaces() == before
+    assert la.workspaces() == {"scratch_bytes": 0, "idle_bytes": 0, "busy_bytes": 0, "busy_workspaces": 0}
+    assert ticket.report() == report
+    assert (bC.download() == C1).all()
+    C2 = np.zeros_like(C1)
+    la.syrk(bits, A, k, m, C2, lower_only=False)
+    assert (C2 == C1).all()
+    del orphan
+
+
+def test_product3_equals_two_products_and_reuses_its_workspace(engine):
+    """BatchedLinalg::product3 (batched_linalg.hpp:99-110): C = (A B) D through an intermediate the
+    BatchedLinalg keeps; bits equal two explicit resident products; the intermediate is busy until the
+    batch is waited, then reused; release returns its bytes."""
+    bits, count, m, n, k, q = 384, 7, 5, 4, 6, 3
+    rng = np.random.default_rng(9)
+    A = nb.random_complex(rng, count * m * k, bits, 20)
+    B = nb.random_complex(rng, count * k * n, bits, 20)
+    D = nb.random_complex(rng, count * n * q, bits, 20)
+    first = api.StridedGemm(count, m, n, k, m * k, k * n, 0)
+    second = api.StridedGemm(count, m, q, n, 0, n * q, m * q, negative=False)
+    bl = api.BatchedLinalg(engine)
+
+    def buf(x):
+        b = engine.make_buffer(x.shape[0], bits, True)
+        b.upload(x)
+        return b
+
+    bA, bB, bD = buf(A), buf(B), buf(D)
+    bC = engine.make_buffer(count * m * q, bits, True)
+    batch = engine.batch()
+    bl.product3(batch, first, second, bA, bB, bD, bC, negative=True)
+    assert bl.workspaces()["busy_workspaces"] == 1
+    batch.submit().wait()
+    got = bC.download()
+    T = engine.make_buffer(count * m * n, bits, True)
+    W = engine.make_buffer(count * m * q, bits, True)
+    batch = engine.batch()
+    bl.gemm_resident(batch, api.StridedGemm(count, m, n, k, m * k, k * n, m * n), bA, bB, T)
+    bl.gemm_resident(batch, api.StridedGemm(count, m, q, n, m * n, n * q, m * q, negative=True), T, bD, W)
+    batch.submit().wait()
+    assert (got == W.download()).all()
+    w = bl.workspaces()
+    assert w["busy_workspaces"] == 0 and w["idle_bytes"] > 0
+    batch = engine.batch()
+    bl.product3(batch, first, second, bA, bB, bD, bC)
+    batch.submit().wait()
+    assert bl.workspaces() == w                               # the idle intermediate was reused
+    assert bl.release_workspaces() == w and bl.workspaces()["idle_bytes"] == 0
+    with pytest.raises(api.InvalidArgument):
+        bl.product3(engine.batch(), first, api.StridedGemm(count, m, q, n + 1), bA, bB, bD, bC)
