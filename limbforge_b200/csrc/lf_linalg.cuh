@@ -271,8 +271,11 @@ namespace lfd {
 // exact_dot_add with the terms spread over the 32 lanes of a warp (k = lane, lane + 32, ...).  When
 // every nonzero term and the addend fit one two's-complement window of W = 2N + 10 words
 // (64N + 320 bits: products of the same magnitude class, as in factorization panels), each lane sums
-// its terms exactly in the window, the warp adds the windows exactly and lane 0 rounds once;
-// otherwise lane 0 runs the generic cluster routine.  Every lane receives the result.
+// its terms exactly in the window (the addend goes to lane K mod 32, which has one term fewer when K is
+// not a multiple of 32), the warp adds the windows exactly and rounds once: with shared rows (srow, from
+// the caller's dynamic shared memory) by warp_round_window, otherwise by a shuffle tree and lane 0.  A
+// spread too wide for the window takes the generic cluster routine on lane 0.  Every lane receives the
+// result.
 template <int N> __device__ __forceinline__ Num<N> warp_broadcast(const Num<N>& v) {
     Num<N> r;
 #pragma unroll
@@ -280,8 +283,124 @@ template <int N> __device__ __forceinline__ Num<N> warp_broadcast(const Num<N>& 
     r.e = __shfl_sync(0xffffffffu, v.e, 0); r.s = __shfl_sync(0xffffffffu, v.s, 0); r.st = __shfl_sync(0xffffffffu, v.st, 0);
     return r;
 }
+// Shared memory of the window reduction: one row of dot_row_words words per lane (odd stride: the row
+// writes and the column reads are free of bank conflicts).
+template <int N> __host__ __device__ constexpr int dot_row_words() { return (2 * N + 10) | 1; }
+template <int N> __host__ __device__ constexpr size_t dot_smem_bytes(int warps) { return (size_t)warps * 32 * dot_row_words<N>() * 4; }
+
+// RN(T * 2^lo) for T the sum, mod 2^(32W), of the 32 lanes' two's-complement windows, computed by the whole
+// warp; every lane returns the result.  The windows go to shared memory (srow: 32 rows) and lane l sums
+// column l (+32, +64) over the rows; the column sums' high parts and the carries between columns are
+// resolved with ballots (carries c = ((G|P) + G) ^ (G|P) ^ G for generate G and propagate P); the sign,
+// the magnitude, the top word and the round and sticky bits follow with ballots and shuffles.  The
+// bits equal those of round_general on the summed window.
+template <int N, int W> __device__ __forceinline__ Num<N> warp_round_window(const u32 (&acc)[W], i64 lo, u32* srow) {
+    constexpr int WP = dot_row_words<N>();
+    static_assert(WP >= W, "row shorter than the window");
+    constexpr int R = (W + 31) / 32;
+    constexpr u32 FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    u32* row = srow + lane * WP;
+#pragma unroll
+    for (int w = 0; w < W; ++w) row[w] = acc[w];
+    __syncwarp();
+    u32 v[R], hi[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int w = lane + 32 * r;
+        u64 s0 = 0, s1 = 0;
+        if (w < W) {
+#pragma unroll
+            for (int l = 0; l < 32; l += 2) { s0 += srow[l * WP + w]; s1 += srow[(l + 1) * WP + w]; }
+        }
+        const u64 sum = s0 + s1;
+        v[r] = (u32)sum; hi[r] = (u32)(sum >> 32);
+    }
+    __syncwarp();                                            // the rows may be rewritten by the next call
+    u32 G[R], P[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {                            // u_w = low(S_w) + high(S_{w-1})
+        u32 hp = __shfl_up_sync(FULL, hi[r], 1);
+        const u32 hl = r ? __shfl_sync(FULL, hi[r ? r - 1 : 0], 31) : 0u;
+        if (lane == 0) hp = hl;
+        const u64 u = (u64)v[r] + hp;
+        const bool valid = lane + 32 * r < W;
+        v[r] = valid ? (u32)u : 0u;
+        G[r] = __ballot_sync(FULL, valid && (u >> 32));
+        P[r] = __ballot_sync(FULL, valid && (u32)u == FULL);
+    }
+    u32 cy = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const u32 X = G[r] | P[r];
+        const u64 sum = (u64)X + G[r] + cy;
+        const u32 Cm = (u32)sum ^ X ^ G[r];                  // carry into each column of this round
+        cy = (u32)(sum >> 32);
+        if (lane + 32 * r < W) v[r] += (Cm >> lane) & 1u;     // the carry out of the window is dropped (mod 2^(32W))
+    }
+    constexpr int RT = (W - 1) / 32, LT = (W - 1) % 32;
+    const bool neg = __shfl_sync(FULL, v[RT], LT) >> 31;
+    if (neg) {                                               // magnitude: ~T + 1
+        bool zero_below = true;
+        const u32 lowmask = (1u << lane) - 1u;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const bool valid = lane + 32 * r < W;
+            const u32 Z = __ballot_sync(FULL, !valid || v[r] == 0);
+            const bool cin = zero_below && (Z & lowmask) == lowmask;
+            v[r] = valid ? ~v[r] + (cin ? 1u : 0u) : 0u;
+            zero_below = zero_below && Z == FULL;
+        }
+    }
+    int top = -1;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const u32 T = __ballot_sync(FULL, v[r] != 0);
+        if (T) top = 32 * r + 31 - __clz(T);
+    }
+    if (top < 0) return zero<N>();
+    u32 vt = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) vt = (r == (top >> 5)) ? v[r] : vt;
+    vt = __shfl_sync(FULL, vt, top & 31);
+    const int lz = __clz(vt);
+    u32 sh[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {                            // sh_w = high word of (a_w : a_{w-1}) << lz
+        u32 pv = __shfl_up_sync(FULL, v[r], 1);
+        const u32 pl = r ? __shfl_sync(FULL, v[r ? r - 1 : 0], 31) : 0u;
+        if (lane == 0) pv = pl;
+        sh[r] = __funnelshift_l(pv, v[r], lz);
+    }
+    const int c = top - N;                                   // column whose top bit is the round bit
+    bool any = false;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int w = lane + 32 * r;
+        const u32 part = w < c - 1 ? v[r] : w == c - 1 ? (v[r] << lz) : w == c ? (sh[r] & 0x7fffffffu) : 0u;
+        any = any || part != 0;
+    }
+    const bool sticky = __any_sync(FULL, any);
+    u32 rbw = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) rbw = (r == (c >> 5)) ? sh[r] : rbw;
+    rbw = __shfl_sync(FULL, rbw, c & 31);
+    const bool rb = c >= 0 && (rbw >> 31);
+    u32 m[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const int col = c + 1 + i;
+        u32 x = 0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) x = (r == (col >> 5)) ? sh[r] : x;
+        x = __shfl_sync(FULL, x, col & 31);
+        m[i] = col >= 0 ? x : 0u;
+    }
+    return finish<N>(m, lo + 32 * (i64)top + 31 - lz, neg ? -1 : 1, rb && (sticky || (m[0] & 1u)), 0);
+}
+
 template <int N, bool RO> __device__ Num<N> warp_exact_dot(const u32* cp, bool subtract, const u32* x, i64 sx, const u32* y, i64 sy,
-                                                          u64 K, u32* error) {
+                                                          u64 K, u32* error, u32* srow = nullptr) {
     constexpr int W = 2 * N + 10;
     constexpr i64 E = N + 3;
     const int lane = threadIdx.x & 31;
@@ -329,11 +448,12 @@ template <int N, bool RO> __device__ Num<N> warp_exact_dot(const u32* cp, bool s
         place_words<W, 2 * N>(t, p, (i64)a.e + b.e - 2 * (32 * N - 1) - lo);
         accumulate<W>(acc, t, (subtract ? -a.s * b.s : a.s * b.s) < 0);
     }
-    if (lane == 0 && c.s) {
+    if (lane == (int)(K % 32) && c.s) {                     // the addend goes to a lane with one term fewer
         u32 t[W];
         place_words<W, N>(t, c.m, (i64)c.e - (32 * N - 1) - lo);
         accumulate<W>(acc, t, c.s < 0);
     }
+    if (srow) return warp_round_window<N, W>(acc, lo, srow);
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
         u32 other[W];
@@ -369,6 +489,8 @@ template <int N> constexpr int diag_threads() { return N <= 8 ? 512 : N <= 16 ? 
 template <int N> __global__ void __launch_bounds__(diag_threads<N>()) chol_diag_kernel(CholParams p) {
     constexpr u64 E = N + 3;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    extern __shared__ u32 dot_rows[];
+    u32* srow = dot_rows + warp * 32 * dot_row_words<N>();
     __shared__ int failed;
     if (!threadIdx.x) failed = 0;
     __syncthreads();
@@ -377,7 +499,8 @@ template <int N> __global__ void __launch_bounds__(diag_threads<N>()) chol_diag_
         for (u64 u = warp; u < p.k1 - j; u += nw) {                 // u = 0: the diagonal, u > 0: row j + u
             const u64 i = j + u;
             u32* wij = p.W + (i * p.n + j) * E;
-            const Num<N> v = warp_exact_dot<N, false>(wij, true, p.W + (i * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
+            const Num<N> v = warp_exact_dot<N, false>(wij, true, p.W + (i * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error,
+                                                      srow);
             if (lane == 0) {
                 if (u) store<N>(wij, v);
                 else if (v.st || v.s <= 0) { p.info[0] = (long long)j; p.info[1] = v.st ? 0 : v.s; p.info[2] = v.st; failed = 1; }
@@ -399,10 +522,13 @@ template <int N> __global__ void __launch_bounds__(128) chol_rows_kernel(CholPar
     constexpr u64 E = N + 3;
     const u64 i = r0 + ((u64)blockIdx.x * blockDim.x + threadIdx.x) / 32;
     const int lane = threadIdx.x & 31;
+    extern __shared__ u32 dot_rows[];
+    u32* srow = dot_rows + (threadIdx.x >> 5) * 32 * dot_row_words<N>();
     if (i >= p.n) return;
     for (u64 j = p.k0; j < jend; ++j) {
         u32* wij = p.W + (i * p.n + j) * E;
-        const Num<N> v = warp_exact_dot<N, false>(wij, true, p.W + (i * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error);
+        const Num<N> v = warp_exact_dot<N, false>(wij, true, p.W + (i * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error,
+                                                  srow);
         if (lane == 0) store<N>(wij, div<N>(v, ldn<N, false>(p.W + (j * p.n + j) * E)));
         __syncwarp();
     }
@@ -432,10 +558,13 @@ template <int N> __global__ void __launch_bounds__(128) solve_forward_kernel(Sol
     constexpr u64 E = N + 3;
     const u64 c = ((u64)blockIdx.x * blockDim.x + threadIdx.x) / 32;
     const int lane = threadIdx.x & 31;
+    extern __shared__ u32 dot_rows[];
+    u32* srow = dot_rows + (threadIdx.x >> 5) * 32 * dot_row_words<N>();
     if (c >= p.nrhs) return;
     for (u64 i = p.r0; i < p.r1; ++i) {
         u32* x = p.X + (i * p.nrhs + c) * E;
-        const Num<N> v = warp_exact_dot<N, false>(x, true, p.L + (i * p.n + p.r0) * E, 1, p.X + (p.r0 * p.nrhs + c) * E, (i64)p.nrhs, i - p.r0, p.error);
+        const Num<N> v = warp_exact_dot<N, false>(x, true, p.L + (i * p.n + p.r0) * E, 1, p.X + (p.r0 * p.nrhs + c) * E, (i64)p.nrhs, i - p.r0, p.error,
+                                                  srow);
         if (lane == 0) store<N>(x, div<N>(v, ldn<N, false>(p.L + (i * p.n + i) * E)));
         __syncwarp();
     }
@@ -444,13 +573,16 @@ template <int N> __global__ void __launch_bounds__(128) solve_backward_kernel(So
     constexpr u64 E = N + 3;
     const u64 c = ((u64)blockIdx.x * blockDim.x + threadIdx.x) / 32;
     const int lane = threadIdx.x & 31;
+    extern __shared__ u32 dot_rows[];
+    u32* srow = dot_rows + (threadIdx.x >> 5) * 32 * dot_row_words<N>();
     if (c >= p.nrhs) return;
     for (u64 i = p.r1; i-- > p.r0;) {
         u32* x = p.X + (i * p.nrhs + c) * E;
         Num<N> v;
         if (i + 1 < p.r1) {
             const u32* col = p.upper ? p.L + (i * p.n + i + 1) * E : p.L + ((i + 1) * p.n + i) * E;
-            v = warp_exact_dot<N, false>(x, true, col, p.upper ? 1 : (i64)p.n, p.X + ((i + 1) * p.nrhs + c) * E, (i64)p.nrhs, p.r1 - i - 1, p.error);
+            v = warp_exact_dot<N, false>(x, true, col, p.upper ? 1 : (i64)p.n, p.X + ((i + 1) * p.nrhs + c) * E, (i64)p.nrhs, p.r1 - i - 1, p.error,
+                                         srow);
         } else {
             v = ldn<N, false>(x);
         }
@@ -466,11 +598,15 @@ typedef void (*SolveFn)(const SolveParams&, bool, cudaStream_t);
 struct FactorKernels { CholDiagFn diag; CholRowsFn rows; CholPrepFn prep; SolveFn solve; };
 const FactorKernels* factor_kernels(int limbs);
 
-template <int N> void chol_diag_launch(const CholParams& p, cudaStream_t s) { chol_diag_kernel<N><<<1, diag_threads<N>(), 0, s>>>(p); }
+template <int N> void chol_diag_launch(const CholParams& p, cudaStream_t s) {
+    const size_t smem = dot_smem_bytes<N>(diag_threads<N>() / 32);
+    cudaFuncSetAttribute(chol_diag_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    chol_diag_kernel<N><<<1, diag_threads<N>(), smem, s>>>(p);
+}
 template <int N> void chol_rows_launch(const CholParams& p, u64 r0, u64 jend, cudaStream_t s) {
     if (r0 >= p.n || jend <= p.k0) return;
     const u64 rows = p.n - r0;
-    chol_rows_kernel<N><<<(unsigned)((rows + 3) / 4), 128, 0, s>>>(p, r0, jend);
+    chol_rows_kernel<N><<<(unsigned)((rows + 3) / 4), 128, dot_smem_bytes<N>(4), s>>>(p, r0, jend);
 }
 template <int N> void chol_prep_launch(const u32* A, u32* W, u64 n, u64 fail, cudaStream_t s) {
     if (!n) return;
@@ -480,8 +616,8 @@ template <int N> void chol_prep_launch(const u32* A, u32* W, u64 n, u64 fail, cu
 template <int N> void solve_launch(const SolveParams& p, bool forward, cudaStream_t s) {
     if (!p.nrhs || p.r1 <= p.r0) return;
     const unsigned blocks = (unsigned)((p.nrhs + 3) / 4);
-    if (forward) solve_forward_kernel<N><<<blocks, 128, 0, s>>>(p);
-    else solve_backward_kernel<N><<<blocks, 128, 0, s>>>(p);
+    if (forward) solve_forward_kernel<N><<<blocks, 128, dot_smem_bytes<N>(4), s>>>(p);
+    else solve_backward_kernel<N><<<blocks, 128, dot_smem_bytes<N>(4), s>>>(p);
 }
 
 }  // namespace lfd

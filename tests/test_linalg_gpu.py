@@ -175,6 +175,26 @@ def test_cholesky_and_solves_vs_oracle(la, oracle, bits, kind, n):
             assert same(X, W), f"solve passes={passes} {kind} n={n} {name} bad {bad(X, W)}"
 
 
+@pytest.mark.parametrize("bits,kind,n", [(64, "qsc", 35), (416, "moderate", 40), (416, "graded", 33), (1024, "qsc", 36),
+                                         (1024, "wide", 12)])
+def test_cholesky_and_solves_wide_limbs(la, oracle, bits, kind, n):
+    """Panels and solves at widths whose exact-dot windows span one, two and three columns per lane."""
+    from limbforge_b200.api import FactorOptions
+    rng = np.random.default_rng(bits + n)
+    A = spd(oracle, bits, n, kind, rng)
+    L = np.zeros_like(A)
+    info = la.cholesky(bits, A, n, L, FactorOptions(block=32))
+    WL, winfo = oracle.cholesky(bits, A, n, 32)
+    assert (info.pivot, info.pivot_sign, info.pivot_status) == winfo
+    assert same(L, WL), f"cholesky bad {bad(L, WL)}"
+    if winfo[0] < n:
+        return
+    B = rhs(bits, n, 4, rng)
+    X = np.zeros_like(B)
+    la.cholesky_solve(bits, L, n, B, 4, X, FactorOptions(block=32))
+    assert same(X, oracle.solve(bits, L, n, B, 4, 32, 3))
+
+
 def test_cholesky_failures(la, oracle):
     from limbforge_b200.api import FactorOptions
     bits = 192
