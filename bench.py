@@ -34,9 +34,9 @@ METRIC = "1024-bit ops/s; exact GEMM MAC/s int8-CRT vs limb kernel, 1 B200, bit-
 UNIT = "1024-bit ops/s"
 WORKLOAD = "1024-bit (32-limb) 16-step RNE multiplication chains over 65,536 values"
 ELEMENT_BYTES = BITS // 8 + 12
-# ncu: dram__bytes_read.sum + dram__bytes_write.sum of one chain_kernel<32> launch of this workload
-# (profiles/chain_kernel_1024bit_65536.md: 155,325,440 + 4,717,312 bytes).
-TRAFFIC_BYTES = 160042752
+# ncu: dram__bytes_read.sum + dram__bytes_write.sum of one launch of the 1024-bit chain kernel on this
+# workload, from one capture (156,188,928 + 4,269,568 bytes).
+TRAFFIC_BYTES = 160458496
 
 
 def make_inputs(seed: int = 20261203):
@@ -559,7 +559,7 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      "traffic": TRAFFIC_BYTES, "peak_kind": peak_kind,
-                     "note": "chain_kernel<32> is integer-pipe bound; HBM fraction shown per the contract"},
+                     "note": "the 1024-bit chain kernel is integer-pipe bound; HBM fraction shown per the contract"},
         "integer_pipe": {"word_macs_per_s": word_macs / (ms_step * 1e-3), "word_macs_per_step": word_macs},
         "clocks": clocks.summary(),
         "cpu_baseline": {"value": cpu_rate, "unit": UNIT, "cores": cores, "kind": kind,

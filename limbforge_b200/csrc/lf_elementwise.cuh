@@ -5,6 +5,7 @@
 #pragma once
 #include "lf_arith.cuh"
 #include <cuda_runtime.h>
+#include <cstdint>
 
 namespace lfd {
 
@@ -84,6 +85,67 @@ template <int N, bool MUL_ONLY> __global__ void __launch_bounds__(kChainThreads)
     }
 }
 
+// Multiplication chains whose factors are contiguous (no broadcast) and read nowhere that a step writes:
+// a block of 32 values copies the next step's 32 factors (one contiguous tile of 32 (N+3) words, a
+// multiple of 16 bytes) into shared memory with cp.async while the current products run, so the product
+// reads its factor words from shared memory.  A partial last block reads its factors directly.
+constexpr int kStagedThreads = 32;
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int G> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(G) : "memory"); }
+
+template <int N> __global__ void __launch_bounds__(kStagedThreads) chain_staged_kernel(const __grid_constant__ ChainParams p) {
+    constexpr u64 E = N + 3;
+    constexpr int T = kStagedThreads, TILE = T * (int)E, CH = TILE / 4;
+    static_assert(TILE % 4 == 0, "tiles of whole 16-byte chunks");
+    const u64 base = (u64)blockIdx.x * T, i = base + threadIdx.x;
+    if (base + T > p.count) {
+        if (i >= p.count) return;
+        Num<N> v = load_plain<N>(p.a + E * i);
+#pragma unroll 1
+        for (int s = 0; s < p.steps; ++s) {
+            v = mul_mem<N>(v, p.step[s].b + E * i);
+            if (p.step[s].out) store<N>(p.step[s].out + E * i, v);
+        }
+        return;
+    }
+    extern __shared__ __align__(16) u32 chain_stage[];
+    const auto fetch = [&](int s) {
+        const u32* src = p.step[s].b + E * base;
+        u32* dst = chain_stage + (s & 1) * TILE;
+        for (int c = threadIdx.x; c < CH; c += T) cp_async16(dst + 4 * c, src + 4 * c);
+        cp_async_commit();
+    };
+    fetch(0);
+    Num<N> v = load_plain<N>(p.a + E * i);
+#pragma unroll 1
+    for (int s = 0; s < p.steps; ++s) {
+        if (s + 1 < p.steps) { fetch(s + 1); cp_async_wait<1>(); } else cp_async_wait<0>();
+        __syncthreads();                                     // every thread's chunks of this step's tile
+        v = mul_mem<N>(v, chain_stage + (s & 1) * TILE + threadIdx.x * E);
+        if (p.step[s].out) store<N>(p.step[s].out + E * i, v);
+        __syncthreads();                                     // the tile is refilled for step s + 2
+    }
+}
+// The staged kernel applies when every factor is contiguous, 16-byte aligned and disjoint from every output.
+inline bool chain_can_stage(const ChainParams& p, u64 E) {
+    const u64 bytes = p.count * E * 4;
+    for (int k = 0; k < p.steps; ++k) {
+        const ChainStep& st = p.step[k];
+        if (st.op != 2 || st.bs != 1 || st.bp != 0 || ((uintptr_t)st.b & 15)) return false;
+        const uintptr_t b0 = (uintptr_t)st.b, b1 = b0 + bytes;
+        for (int q = 0; q < p.steps; ++q) {
+            if (!p.step[q].out) continue;
+            const uintptr_t o0 = (uintptr_t)p.step[q].out, o1 = o0 + bytes;
+            if (b0 < o1 && o0 < b1) return false;
+        }
+    }
+    return true;
+}
+
 template <int N> int launch_ew(int op, const EwParams& p, cudaStream_t s) {
     if (!p.count) return 0;
     const unsigned blocks = (unsigned)((p.count + kEwThreads - 1) / kEwThreads);
@@ -110,7 +172,10 @@ template <int N> int launch_chain(const ChainParams& p, cudaStream_t s) {
     const unsigned blocks = (unsigned)((p.count + kChainThreads - 1) / kChainThreads);
     bool mul_only = true;
     for (int k = 0; k < p.steps; ++k) mul_only = mul_only && p.step[k].op == 2;
-    if (mul_only) chain_kernel<N, true><<<blocks, kChainThreads, 0, s>>>(p);     // registers of mul alone
+    if (mul_only && chain_can_stage(p, N + 3)) {
+        const unsigned sb = (unsigned)((p.count + kStagedThreads - 1) / kStagedThreads);
+        chain_staged_kernel<N><<<sb, kStagedThreads, 2 * kStagedThreads * (N + 3) * 4, s>>>(p);
+    } else if (mul_only) chain_kernel<N, true><<<blocks, kChainThreads, 0, s>>>(p);     // registers of mul alone
     else chain_kernel<N, false><<<blocks, kChainThreads, 0, s>>>(p);
     return 0;
 }
