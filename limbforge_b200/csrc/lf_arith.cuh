@@ -755,6 +755,46 @@ template <int N> __device__ __forceinline__ Num<N> sqrt(const Num<N>& a) {
     return finish<N>(m, e, 1, false, 0);
 }
 
+// ---------------------------------------------------------------- division by a known reciprocal
+// r = RN(1 / b) at N + 1 limbs, computed once per divisor (a Cholesky pivot, a triangular solve's diagonal).
+template <int N> __device__ __forceinline__ Num<N + 1> reciprocal(const Num<N>& b) {
+    Num<N + 1> one, w;
+#pragma unroll
+    for (int i = 0; i <= N; ++i) { one.m[i] = 0; w.m[i] = i ? b.m[i - 1] : 0u; }
+    one.m[N] = 0x80000000u; one.e = 0; one.s = 1; one.st = 0;
+    w.e = b.e; w.s = b.s; w.st = b.st;
+    return div<N + 1>(one, w);
+}
+// RN(a / b) from r = reciprocal(b).  r has relative error at most 2^-(32N+32), so the exact product a * r,
+// normalized to N words, puts the quotient's 32 bits below its last place (g) within two units of those of
+// a / b.  Unless g lies within 3 units of 0, of a half or of the wrap (an exact quotient, a tie, a carry into
+// the last place or a power of two), the truncated words are those of a / b and g decides the rounding;
+// those cases, zeros and statuses take the exact division.  The bits always equal div(a, b).
+template <int N> __device__ __forceinline__ Num<N> div_by(const Num<N>& a, const Num<N>& b, const Num<N + 1>& r) {
+    if (a.st || b.st || r.st || !a.s || !b.s) return div_call<N>(a, b);
+    // p = a * r in [2^(64N+30), 2^(64N+32)): the N x N product with r's top N words, shifted one word,
+    // plus a times r's low word
+    u32 rh[N], q[2 * N], p[2 * N + 1];
+#pragma unroll
+    for (int i = 0; i < N; ++i) rh[i] = r.m[i + 1];
+    mant_mul<N>(a.m, rh, q);
+    p[0] = 0;
+#pragma unroll
+    for (int i = 0; i < 2 * N; ++i) p[i + 1] = q[i];
+    u32 c = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) { const u64 t = (u64)a.m[i] * r.m[0] + p[i] + c; p[i] = (u32)t; c = (u32)(t >> 32); }
+#pragma unroll
+    for (int i = N; i < 2 * N + 1; ++i) { const u64 t = (u64)p[i] + c; p[i] = (u32)t; c = (u32)(t >> 32); }
+    const u32 sh = (p[2 * N] >> 31) ? 0u : 1u;
+    const u32 g = __funnelshift_l(p[N - 1], p[N], sh);
+    if (g <= 3u || g >= 0xfffffffcu || (g >= 0x7ffffffdu && g <= 0x80000003u)) return div_call<N>(a, b);
+    u32 m[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) m[i] = __funnelshift_l(p[N + i], p[N + 1 + i], sh);
+    return finish<N>(m, (i64)a.e + r.e + 1 - (i64)sh, a.s * b.s, g > 0x80000000u, 0);
+}
+
 // ---------------------------------------------------------------- fma
 // RN(a*b + c) with one rounding.  One two's-complement window of F = 3N+4 exact words above one
 // sticky word, anchored 2 bits above the larger term's top bit.  A term that does not fit lies

@@ -477,6 +477,7 @@ template <int N, bool RO> __device__ Num<N> warp_exact_dot(const u32* cp, bool s
 // ---------------------------------------------------------------- blocked Cholesky pieces
 // W: n x n row-major work matrix (element stride E).  D(c; x, y; K) = RN(c - sum x_k y_k), one rounding.
 struct CholParams { u32* W; u64 n, k0, k1; long long* info; u32* error; };
+constexpr u64 kRecips = 32;       // pivot reciprocals a panel-row or solve block keeps in shared memory
 
 // Diagonal block [k0, k1) column by column: s_jj = D(w_jj; row j [k0,j)), l_jj = sqrt(s_jj) (or the
 // failing pivot recorded in info = {pivot, sign, status}); l_ij = RN(D(w_ij; row i, row j; [k0,j)) / l_jj)
@@ -518,18 +519,29 @@ template <int N> __global__ void __launch_bounds__(diag_threads<N>()) chol_diag_
 }
 // Rows i in [r0, n) below the diagonal block: l_ij = RN(D(w_ij; row i, row j; [k0,j)) / l_jj) for
 // j in [k0, jend), left to right (jend = the failing pivot, or k1).  One warp per row.
+// The block first forms the reciprocals of its first kRecips pivots l_jj in shared memory, one per thread,
+// and divides through them (div_by: the bits of div); later columns of a wider block use div.
 template <int N> __global__ void __launch_bounds__(128) chol_rows_kernel(CholParams p, u64 r0, u64 jend) {
-    constexpr u64 E = N + 3;
+    constexpr u64 E = N + 3, ER = N + 4;
     const u64 i = r0 + ((u64)blockIdx.x * blockDim.x + threadIdx.x) / 32;
     const int lane = threadIdx.x & 31;
     extern __shared__ u32 dot_rows[];
     u32* srow = dot_rows + (threadIdx.x >> 5) * 32 * dot_row_words<N>();
+    u32* srec = dot_rows + (blockDim.x >> 5) * 32 * dot_row_words<N>();
+    if (threadIdx.x < jend - p.k0 && threadIdx.x < kRecips) {
+        const u64 j = p.k0 + threadIdx.x;
+        store<N + 1>(srec + threadIdx.x * ER, reciprocal<N>(ldn<N, false>(p.W + (j * p.n + j) * E)));
+    }
+    __syncthreads();
     if (i >= p.n) return;
     for (u64 j = p.k0; j < jend; ++j) {
         u32* wij = p.W + (i * p.n + j) * E;
         const Num<N> v = warp_exact_dot<N, false>(wij, true, p.W + (i * p.n + p.k0) * E, 1, p.W + (j * p.n + p.k0) * E, 1, j - p.k0, p.error,
                                                   srow);
-        if (lane == 0) store<N>(wij, div<N>(v, ldn<N, false>(p.W + (j * p.n + j) * E)));
+        if (lane == 0) {
+            const Num<N> ljj = ldn<N, false>(p.W + (j * p.n + j) * E);
+            store<N>(wij, j - p.k0 < kRecips ? div_by<N>(v, ljj, load_plain<N + 1>(srec + (j - p.k0) * ER)) : div<N>(v, ljj));
+        }
         __syncwarp();
     }
 }
@@ -553,6 +565,20 @@ template <int N> __global__ void chol_prepare_kernel(const u32* A, u32* W, u64 n
 // i ascending; backward block: x_i = RN(D(x_i; column i of L below i within (i, r1), x(i, r1)) / l_ii),
 // i descending (upper: R = L^T stored by rows).  One thread per right-hand side.
 struct SolveParams { const u32* L; u32* X; u64 n, nrhs, r0, r1; int upper; u32* error; };
+// Reciprocals of the block's first kRecips diagonal entries l_ii, i in [r0, r1), in shared memory: one per
+// thread, before any thread leaves.  Rows beyond them divide with div.
+template <int N> __device__ __forceinline__ void solve_reciprocals(const SolveParams& p, u32* srec) {
+    constexpr u64 E = N + 3;
+    if (threadIdx.x < p.r1 - p.r0 && threadIdx.x < kRecips) {
+        const u64 i = p.r0 + threadIdx.x;
+        store<N + 1>(srec + threadIdx.x * (N + 4), reciprocal<N>(ldn<N, false>(p.L + (i * p.n + i) * E)));
+    }
+    __syncthreads();
+}
+template <int N> __device__ __forceinline__ Num<N> solve_divide(const SolveParams& p, const Num<N>& v, u64 i, const u32* srec) {
+    const Num<N> lii = ldn<N, false>(p.L + (i * p.n + i) * (N + 3));
+    return i - p.r0 < kRecips ? div_by<N>(v, lii, load_plain<N + 1>(srec + (i - p.r0) * (N + 4))) : div<N>(v, lii);
+}
 // One warp per right-hand side.
 template <int N> __global__ void __launch_bounds__(128) solve_forward_kernel(SolveParams p) {
     constexpr u64 E = N + 3;
@@ -560,12 +586,14 @@ template <int N> __global__ void __launch_bounds__(128) solve_forward_kernel(Sol
     const int lane = threadIdx.x & 31;
     extern __shared__ u32 dot_rows[];
     u32* srow = dot_rows + (threadIdx.x >> 5) * 32 * dot_row_words<N>();
+    u32* srec = dot_rows + (blockDim.x >> 5) * 32 * dot_row_words<N>();
+    solve_reciprocals<N>(p, srec);
     if (c >= p.nrhs) return;
     for (u64 i = p.r0; i < p.r1; ++i) {
         u32* x = p.X + (i * p.nrhs + c) * E;
         const Num<N> v = warp_exact_dot<N, false>(x, true, p.L + (i * p.n + p.r0) * E, 1, p.X + (p.r0 * p.nrhs + c) * E, (i64)p.nrhs, i - p.r0, p.error,
                                                   srow);
-        if (lane == 0) store<N>(x, div<N>(v, ldn<N, false>(p.L + (i * p.n + i) * E)));
+        if (lane == 0) store<N>(x, solve_divide<N>(p, v, i, srec));
         __syncwarp();
     }
 }
@@ -575,6 +603,8 @@ template <int N> __global__ void __launch_bounds__(128) solve_backward_kernel(So
     const int lane = threadIdx.x & 31;
     extern __shared__ u32 dot_rows[];
     u32* srow = dot_rows + (threadIdx.x >> 5) * 32 * dot_row_words<N>();
+    u32* srec = dot_rows + (blockDim.x >> 5) * 32 * dot_row_words<N>();
+    solve_reciprocals<N>(p, srec);
     if (c >= p.nrhs) return;
     for (u64 i = p.r1; i-- > p.r0;) {
         u32* x = p.X + (i * p.nrhs + c) * E;
@@ -586,7 +616,7 @@ template <int N> __global__ void __launch_bounds__(128) solve_backward_kernel(So
         } else {
             v = ldn<N, false>(x);
         }
-        if (lane == 0) store<N>(x, div<N>(v, ldn<N, false>(p.L + (i * p.n + i) * E)));
+        if (lane == 0) store<N>(x, solve_divide<N>(p, v, i, srec));
         __syncwarp();
     }
 }
@@ -606,7 +636,7 @@ template <int N> void chol_diag_launch(const CholParams& p, cudaStream_t s) {
 template <int N> void chol_rows_launch(const CholParams& p, u64 r0, u64 jend, cudaStream_t s) {
     if (r0 >= p.n || jend <= p.k0) return;
     const u64 rows = p.n - r0;
-    chol_rows_kernel<N><<<(unsigned)((rows + 3) / 4), 128, dot_smem_bytes<N>(4), s>>>(p, r0, jend);
+    chol_rows_kernel<N><<<(unsigned)((rows + 3) / 4), 128, dot_smem_bytes<N>(4) + kRecips * (N + 4) * 4, s>>>(p, r0, jend);
 }
 template <int N> void chol_prep_launch(const u32* A, u32* W, u64 n, u64 fail, cudaStream_t s) {
     if (!n) return;
@@ -616,8 +646,9 @@ template <int N> void chol_prep_launch(const u32* A, u32* W, u64 n, u64 fail, cu
 template <int N> void solve_launch(const SolveParams& p, bool forward, cudaStream_t s) {
     if (!p.nrhs || p.r1 <= p.r0) return;
     const unsigned blocks = (unsigned)((p.nrhs + 3) / 4);
-    if (forward) solve_forward_kernel<N><<<blocks, 128, dot_smem_bytes<N>(4), s>>>(p);
-    else solve_backward_kernel<N><<<blocks, 128, dot_smem_bytes<N>(4), s>>>(p);
+    const size_t smem = dot_smem_bytes<N>(4) + kRecips * (N + 4) * 4;
+    if (forward) solve_forward_kernel<N><<<blocks, 128, smem, s>>>(p);
+    else solve_backward_kernel<N><<<blocks, 128, smem, s>>>(p);
 }
 
 }  // namespace lfd
