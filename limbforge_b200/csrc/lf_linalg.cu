@@ -32,7 +32,8 @@ void exact_product(Linalg& la, int bits, lfd::LineView left, lfd::LineView right
                    uint32_t* C, uint64_t ldc, bool subtract, bool lower, cudaStream_t s, int* method_used) {
     if (!M || !Nc) return;
     const int n = bits / 32;
-    uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));
+    // word 1 of the error buffer: word 0 belongs to the panel and solve kernels of a factorization
+    uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16)) + 1;
     cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
     int method = la.options.method;                    // 0 auto, 1 limb kernel, 2 residue engine
     bool used_residue = false;
@@ -255,14 +256,14 @@ static double solve_device(Linalg& la, int bits, const uint32_t* L, size_t n, ui
     const size_t E = limbs + 3;
     const auto* fk = lfd::factor_kernels(limbs);
     const size_t nb = block ? std::min(block, n) : n;
-    uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));
+    uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));      // word 0: the solve kernels' flag
+    cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
     cudaEvent_t g0, g1;
     cuda_check(cudaEventCreate(&g0), "event"); cuda_check(cudaEventCreate(&g1), "event");
     cuda_check(cudaEventRecord(g0, s), "event");
     if (passes & 1)
         for (size_t r0 = 0; r0 < n; r0 += nb) {
             const size_t r1 = std::min(n, r0 + nb);
-            cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
             fk->solve(lfd::SolveParams{L, X, n, nrhs, r0, r1, 0, err}, true, s);
             cuda_check(cudaGetLastError(), "forward substitution");
             if (r1 < n) {
@@ -274,7 +275,6 @@ static double solve_device(Linalg& la, int bits, const uint32_t* L, size_t n, ui
     if (passes & 2)
         for (size_t r0 = (n - 1) / nb * nb;; r0 -= nb) {
             const size_t r1 = std::min(n, r0 + nb);
-            cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
             fk->solve(lfd::SolveParams{L, X, n, nrhs, r0, r1, 0, err}, false, s);
             cuda_check(cudaGetLastError(), "back substitution");
             if (r0) {
