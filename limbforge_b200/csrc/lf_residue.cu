@@ -256,7 +256,7 @@ bool ResidueEngine::run(int bits, lfd::LineView left, lfd::LineView right, uint6
     cuda_check(cudaFuncSetAttribute(lfd::residue_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem");
     lfd::MmaParams mp{res, tab.dev, M, Nc, Kp, lower ? 1 : 0, error};
     dim3 grid((unsigned)(Np / lfd::kTileN), (unsigned)(Mp / lfd::kTileM), (unsigned)L);
-    lfd::residue_mma_kernel<<<grid, 128, smem, s>>>(ta1, ta0, tb1, tb0, mp);
+    lfd::residue_mma_kernel<<<grid, lfd::kMmaThreads, smem, s>>>(ta1, ta0, tb1, tb0, mp);
     cuda_check(cudaGetLastError(), "residue products");
     {
         // persistent CRT: as many CTAs per SM as TMEM holds (512 columns per SM), shared memory sized
@@ -328,7 +328,7 @@ void residue_mma_launch(dim3 grid, const CUtensorMap& ta1, const CUtensorMap& ta
                         const lfd::MmaParams& p, cudaStream_t s) {
     const size_t smem = lfd::kStages * lfd::kStageBytes + 1024;
     cuda_check(cudaFuncSetAttribute(lfd::residue_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem");
-    lfd::residue_mma_kernel<<<grid, 128, smem, s>>>(ta1, ta0, tb1, tb0, p);
+    lfd::residue_mma_kernel<<<grid, lfd::kMmaThreads, smem, s>>>(ta1, ta0, tb1, tb0, p);
     cuda_check(cudaGetLastError(), "residue products");
 }
 
@@ -460,7 +460,7 @@ void resident_product_launch(ResidentProduct& r, cudaStream_t s) {
         cuda_check(cudaFuncSetAttribute(lfd::residue_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem");
         lfd::MmaParams mp{res, nullptr, r.M, r.Nc, r.Kp, r.lower ? 1 : 0, err, plan};
         dim3 grid((unsigned)(r.Np / lfd::kTileN), (unsigned)(r.Mp / lfd::kTileM), (unsigned)r.Lmax);
-        lfd::residue_mma_kernel<<<grid, 128, smem, s>>>(r.ta1, r.ta0, r.tb1, r.tb0, mp);
+        lfd::residue_mma_kernel<<<grid, lfd::kMmaThreads, smem, s>>>(r.ta1, r.ta0, r.tb1, r.tb0, mp);
         cuda_check(cudaGetLastError(), "residue products");
         const int ckb = (r.maxKp + 127) / 128;
         unsigned cgrid = 0; size_t csmem = 0;

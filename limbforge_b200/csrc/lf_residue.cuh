@@ -87,6 +87,7 @@ constexpr int kStages = 2;
 constexpr int kTileBytes = kTileM * kTileK;                   // 16 KB per operand tile
 constexpr int kStageBytes = 4 * kTileBytes;                   // D1a, D0a, D1b, D0b
 constexpr u32 kSpinLimit = 1u << 28;                          // bounded mbarrier waits
+constexpr int kMmaThreads = 256;                              // warps w and w + 4 share TMEM lanes 32 (w % 4) ..
 
 struct MmaParams {
     u16* res;                               // [L][M][Nc] residues (0 <= r < m)
@@ -149,8 +150,10 @@ __device__ __forceinline__ void tmem_ld32(u32 taddr, u32 (&r)[32]) {
 
 #ifdef LF_RESIDUE_MMA_KERNEL
 // One CTA = one 128 x 128 output tile of one modulus (grid z).  Warp 0 lane 0 issues TMA loads,
-// warp 1 lane 0 issues the MMAs; all four warps then read their 32 TMEM lanes (rows).
-__global__ void __launch_bounds__(128, 1) residue_mma_kernel(const __grid_constant__ CUtensorMap ta1, const __grid_constant__ CUtensorMap ta0,
+// warp 1 lane 0 issues the MMAs; then all eight warps reduce the accumulators: warp w reads TMEM lanes
+// 32 (w % 4) .. + 31 (rows) for the columns of half w / 4 and stores 32 residues of a row with four
+// 16-byte stores when the row stride allows.
+__global__ void __launch_bounds__(kMmaThreads, 1) residue_mma_kernel(const __grid_constant__ CUtensorMap ta1, const __grid_constant__ CUtensorMap ta0,
                                                               const __grid_constant__ CUtensorMap tb1, const __grid_constant__ CUtensorMap tb0,
                                                               MmaParams p) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -226,26 +229,38 @@ __global__ void __launch_bounds__(128, 1) residue_mma_kernel(const __grid_consta
     if (fine) {
         const u32 m = tab->m[l];
         const u64 br = tab->barrett[l];
-        const u32 off49 = mod_barrett(1ull << 49, m, br);
-        const u64 row = (u64)tm * kTileM + warp * 32 + lane;
-        const u32 lane_base = (u32)(warp * 32) << 16;
-        for (int c0 = 0; c0 < kTileN; c0 += 32) {
+        const u32 moff = m - mod_barrett(1ull << 49, m, br);  // m - (2^49 mod m), in (0, m]
+        const int q = warp & 3, half = warp >> 2;
+        const u64 row = (u64)tm * kTileM + q * 32 + lane;
+        const u32 lane_base = (u32)(q * 32) << 16;
+        const bool vec = (p.Nc & 7) == 0;                      // rows start on 16-byte boundaries
+        for (int c0 = half * (kTileN / 2); c0 < (half + 1) * (kTileN / 2); c0 += 32) {
             u32 s11[32], s00[32], sm[32];
             tmem_ld32(acc11 + lane_base + c0, s11);
             tmem_ld32(acc00 + lane_base + c0, s00);
             tmem_ld32(accm + lane_base + c0, sm);
             asm volatile("tcgen05.wait::ld.sync.aligned;");
             if (row < p.M) {
-                u16* out = p.res + ((u64)l * p.M + row) * p.Nc;
+                const u64 col0 = (u64)tn * kTileN + c0;
+                u16* out = p.res + ((u64)l * p.M + row) * p.Nc + col0;
+                u32 r[32];
 #pragma unroll
                 for (int c = 0; c < 32; ++c) {
-                    const u64 col = (u64)tn * kTileN + c0 + c;
-                    if (col >= p.Nc) break;
                     // 65536 S11 + 256 Smid + S00 (|.| < 2^48), made nonnegative by 2^49 and reduced
                     const long long v = (long long)(int)s11[c] * 65536 + (long long)(int)sm[c] * 256 + (long long)(int)s00[c];
-                    const u32 rb = mod_barrett((u64)(v + (1ll << 49)), m, br);
-                    const u64 t = (u64)rb + m - off49;
-                    out[col] = (u16)mod_barrett(t, m, br);
+                    const u32 t = mod_barrett((u64)(v + (1ll << 49)), m, br) + moff;     // in (0, 2m)
+                    r[c] = t >= m ? t - m : t;
+                }
+                if (vec && col0 + 32 <= p.Nc) {
+                    uint4* o = reinterpret_cast<uint4*>(out);
+#pragma unroll
+                    for (int v = 0; v < 4; ++v)
+                        o[v] = make_uint4(r[8 * v] | (r[8 * v + 1] << 16), r[8 * v + 2] | (r[8 * v + 3] << 16),
+                                          r[8 * v + 4] | (r[8 * v + 5] << 16), r[8 * v + 6] | (r[8 * v + 7] << 16));
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 32; ++c)
+                        if (col0 + c < p.Nc) out[c] = (u16)r[c];
                 }
             }
         }
