@@ -88,6 +88,7 @@ constexpr int kTileBytes = kTileM * kTileK;                   // 16 KB per opera
 constexpr int kStageBytes = 4 * kTileBytes;                   // D1a, D0a, D1b, D0b
 constexpr u32 kSpinLimit = 1u << 28;                          // bounded mbarrier waits
 constexpr int kMmaThreads = 256;                              // warps w and w + 4 share TMEM lanes 32 (w % 4) ..
+constexpr int kDigitThreads = 256;                            // digit planes: the same lane sharing
 
 struct MmaParams {
     u16* res;                               // [L][M][Nc] residues (0 <= r < m)
@@ -628,7 +629,7 @@ struct DigitMmaParams {
     u32* error;
     const ResPlan* plan;                   // planned on the GPU: L and its operand come from the plan
 };
-template <int N> __global__ void __launch_bounds__(128) digits_mma_kernel(const DigitMmaParams pin) {
+template <int N> __global__ void __launch_bounds__(kDigitThreads, 1) digits_mma_kernel(const DigitMmaParams pin) {
     DigitMmaParams p = pin;
     if (pin.plan) {
         const ResPlan& r = *pin.plan;
@@ -642,10 +643,16 @@ template <int N> __global__ void __launch_bounds__(128) digits_mma_kernel(const 
     unsigned char* sB = smem + kblocks * 16384;
     __shared__ __align__(8) u64 done;
     __shared__ u32 tmem_slot;
+    __shared__ u32 s_m[kResMaxModuli], s_r[kResMaxModuli];     // m_l and floor(2^32 / m_l)
+    __shared__ unsigned char s_neg[128];                       // row holds a negative entry
     const int warp = threadIdx.x >> 5;
     const u64 bbytes = (u64)kblocks * p.NB * 128;
     for (u64 o = (u64)threadIdx.x * 16; o < bbytes; o += (u64)blockDim.x * 16)
         *reinterpret_cast<uint4*>(sB + o) = *reinterpret_cast<const uint4*>(p.bimg + o);
+    for (int l = threadIdx.x; l < p.L; l += blockDim.x) {
+        s_m[l] = p.tab->m[l];
+        s_r[l] = (u32)(p.tab->barrett[l] >> 32);               // floor(2^64 / m) >> 32 = floor(2^32 / m)
+    }
     if (threadIdx.x == 0) {
         mbar_init(&done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -663,36 +670,44 @@ template <int N> __global__ void __launch_bounds__(128) digits_mma_kernel(const 
     const u32 id1 = (2u << 4) | ((u32)(N1 >> 3) << 17) | ((u32)(128 >> 4) << 24);
     const u32 id2 = (2u << 4) | ((u32)(N2 >> 3) << 17) | ((u32)(128 >> 4) << 24);
     const u64 plane = p.rows_pad * p.Kp, tiles = plane / 128;     // Kp is a multiple of 128
-    const u32 row = threadIdx.x, lane_base = (u32)(warp * 32) << 16;
+    const int q = warp & 3, half = warp >> 2;                  // warps q and q + 4 share TMEM lanes 32 q ..
+    const u32 row = (u32)(q * 32 + (threadIdx.x & 31)), lane_base = (u32)(q * 32) << 16;
+    // The first four warps stage the entries of a tile (one row each); the entry of the next tile is
+    // loaded before the current tile's epilogue so that its latency hides behind the digit work.
+    Num<N> a = zero<N>();
+    u64 aline = 0;
+    auto fetch = [&](u64 t) {
+        a = zero<N>();
+        const u64 e = t * 128 + row;
+        aline = e / p.Kp;
+        const u64 k = e % p.Kp;
+        if (t < tiles && k < p.K && aline < p.lines) a = load<N>(p.v.base + (aline * p.v.ls + k * p.v.ks) * (u64)(N + 3));
+    };
+    if (half == 0) fetch(blockIdx.x);
     u32 phase = 0;
     for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const u64 e = tile * 128 + row, line = e / p.Kp, k = e % p.Kp;
-        u32 x[40];
+        const u64 e = tile * 128 + row;
+        if (half == 0) {
+            // row of A: the bytes of X = |entry| 2^(e - bottom) (0 <= shift <= G), zero beyond its words
 #pragma unroll
-        for (int w = 0; w < 40; ++w) x[w] = 0;
-        bool negative = false;
-        if (k < p.K && line < p.lines) {
-            const Num<N> a = load<N>(p.v.base + (line * p.v.ls + k * p.v.ks) * (u64)(N + 3));
+            for (int c = 0; c < 16; ++c) {                      // up to 2 K blocks of 8 chunks
+                if (c >= kblocks * 8) break;
+                *reinterpret_cast<uint4*>(sA + (c >> 3) * 16384u + sw128_offset(row, (u32)(c & 7) * 16u)) = make_uint4(0, 0, 0, 0);
+            }
+            bool negative = false;
             if (!a.st && a.s) {
                 negative = a.s < 0;
-                const int sh = a.e - p.info[line].bottom;       // 0 <= sh <= G
+                const int sh = a.e - p.info[aline].bottom;
                 const int ws = sh >> 5, bs = sh & 31;
+#pragma unroll
                 for (int i = 0; i <= N; ++i) {
                     u32 v = i < N ? a.m[i] << bs : 0u;
                     if (bs && i > 0) v |= a.m[i - 1] >> (32 - bs);
-                    x[i + ws] = v;
+                    const u32 byte = (u32)(i + ws) * 4u;      // word i + ws < xwords <= KB / 4
+                    *reinterpret_cast<u32*>(sA + (byte >> 7) * 16384u + sw128_offset(row, byte & 127u)) = v;
                 }
             }
-        }
-        // row of A: the bytes of X, 16 at a time, zero beyond 4 xwords
-#pragma unroll
-        for (int c = 0; c < 16; ++c) {                          // up to 2 K blocks of 8 chunks
-            if (c >= kblocks * 8) break;
-            const int w0 = c * 4;
-            uint4 v;
-            v.x = w0 < p.xwords ? x[w0] : 0u; v.y = w0 + 1 < p.xwords ? x[w0 + 1] : 0u;
-            v.z = w0 + 2 < p.xwords ? x[w0 + 2] : 0u; v.w = w0 + 3 < p.xwords ? x[w0 + 3] : 0u;
-            *reinterpret_cast<uint4*>(sA + (c >> 3) * 16384u + sw128_offset(row, (u32)(c & 7) * 16u)) = v;
+            s_neg[row] = negative ? 1 : 0;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -712,7 +727,13 @@ template <int N> __global__ void __launch_bounds__(128) digits_mma_kernel(const 
         phase ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;");
         if (!fine) break;
-        for (int c0 = 0; c0 < 2 * p.L; c0 += 32) {
+        if (half == 0) fetch(tile + gridDim.x);                // sA is rewritten only after the barrier below
+        const bool negative = s_neg[row] != 0;
+        signed char* d1 = p.d1 + e;
+        signed char* d0 = p.d0 + e;
+        // X == P_2l + 256 P_2l+1 (mod m_l) with both P below 160 * 255^2, so the sum stays below 2^32 and one
+        // 32-bit Barrett step with floor(2^32 / m) leaves it in [0, 2m).
+        for (int c0 = half * 32; c0 < 2 * p.L; c0 += 64) {
             u32 P[32];
             tmem_ld32(tmem + lane_base + (u32)c0, P);
             asm volatile("tcgen05.wait::ld.sync.aligned;");
@@ -720,14 +741,15 @@ template <int N> __global__ void __launch_bounds__(128) digits_mma_kernel(const 
             for (int c = 0; c < 32; c += 2) {
                 const int l = (c0 + c) >> 1;
                 if (l >= p.L) break;
-                const u32 m = p.tab->m[l];
-                u32 u = mod_barrett((u64)P[c] + ((u64)P[c + 1] << 8), m, p.tab->barrett[l]);
+                const u32 m = s_m[l];
+                const u32 x = P[c] + (P[c + 1] << 8);
+                u32 u = x - __umulhi(x, s_r[l]) * m;
+                if (u >= m) u -= m;
                 if (negative && u) u = m - u;                   // residue of -X
-                int r = (int)u;
-                if (r > (int)(m >> 1)) r -= (int)m;              // balanced: |r| <= 32639
+                const int r = (int)u - (u > (m >> 1) ? (int)m : 0);   // balanced: |r| <= 32639
                 const int lo = (int)(signed char)(r & 0xff);
-                p.d1[l * plane + e] = (signed char)((r - lo) >> 8);
-                p.d0[l * plane + e] = (signed char)lo;
+                d1[(u64)l * plane] = (signed char)((r - lo) >> 8);
+                d0[(u64)l * plane] = (signed char)lo;
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;");
@@ -785,7 +807,7 @@ template <int N> void crt_launch(const CrtParams& p, unsigned grid, size_t smem,
 template <int N> void digits_mma_launch(const DigitMmaParams& p, unsigned grid, size_t smem, cudaStream_t s) {
     if (!p.rows_pad || !p.Kp) return;
     cudaFuncSetAttribute(digits_mma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    digits_mma_kernel<N><<<grid, 128, smem, s>>>(p);
+    digits_mma_kernel<N><<<grid, kDigitThreads, smem, s>>>(p);
 }
 template <int N> void rec_launch(const RecParams& p, cudaStream_t s) {
     if (!p.M || !p.Nc) return;
