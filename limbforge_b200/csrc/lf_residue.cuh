@@ -89,6 +89,7 @@ constexpr int kStageBytes = 4 * kTileBytes;                   // D1a, D0a, D1b, 
 constexpr u32 kSpinLimit = 1u << 28;                          // bounded mbarrier waits
 constexpr int kMmaThreads = 256;                              // warps w and w + 4 share TMEM lanes 32 (w % 4) ..
 constexpr int kDigitThreads = 256;                            // digit planes: the same lane sharing
+constexpr int kCrtThreads = 256;                              // CRT column sums: the same lane sharing
 
 struct MmaParams {
     u16* res;                               // [L][M][Nc] residues (0 <= r < m)
@@ -464,7 +465,7 @@ __device__ __forceinline__ u64 crt_desc(u32 saddr) {       // K-major, SW128, SB
 __host__ __device__ __forceinline__ u32 sw128_offset(u32 row, u32 k) {
     return (row >> 3) * 1024u + (row & 7u) * 128u + ((((k >> 4) ^ row) & 7u) << 4) + (k & 15u);
 }
-template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(const CrtParams pin) {
+template <int N> __global__ void __launch_bounds__(kCrtThreads, 2) crt_mma_kernel(const CrtParams pin) {
     CrtParams p = pin;
     if (pin.plan) {
         const ResPlan& r = *pin.plan;
@@ -479,10 +480,17 @@ template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(const Crt
     unsigned char* sB = smem + kblocks * 16384;                // kblocks x [NB rows][128 B]
     __shared__ __align__(8) u64 done;
     __shared__ u32 tmem_slot;
+    __shared__ u32 s_m[kResMaxModuli], s_w[kResMaxModuli], s_r[kResMaxModuli];   // m_l, (M/m_l)^-1, floor(2^32/m_l)
+    __shared__ unsigned char s_any[2][128];                    // some residue of the row is nonzero, per half
     const int warp = threadIdx.x >> 5;
     const u64 bbytes = (u64)kblocks * p.NB * 128;
     for (u64 o = (u64)threadIdx.x * 16; o < bbytes; o += (u64)blockDim.x * 16)
         *reinterpret_cast<uint4*>(sB + o) = *reinterpret_cast<const uint4*>(p.bimg + o);
+    for (int l = threadIdx.x; l < p.L; l += blockDim.x) {
+        s_m[l] = p.tab->m[l];
+        s_w[l] = p.tab->w[l];
+        s_r[l] = (u32)(p.tab->barrett[l] >> 32);               // floor(2^64 / m) >> 32 = floor(2^32 / m)
+    }
     if (threadIdx.x == 0) {
         mbar_init(&done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -500,7 +508,10 @@ template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(const Crt
     const u32 id1 = (2u << 4) | ((u32)(N1 >> 3) << 17) | ((u32)(128 >> 4) << 24);
     const u32 id2 = (2u << 4) | ((u32)(N2 >> 3) << 17) | ((u32)(128 >> 4) << 24);
     const u64 outputs = p.M * p.Nc, tiles = (outputs + 127) / 128;
-    const u32 row = threadIdx.x, lane_base = (u32)(warp * 32) << 16;
+    // Warps q and q + 4 stage alternate groups of 16 moduli of the same 128 rows; warps 0-3 then carry the
+    // byte columns of their TMEM lanes 32 q .. into S and F.
+    const int half = warp >> 2;
+    const u32 row = (u32)((warp & 3) * 32 + (threadIdx.x & 31)), lane_base = (u32)((warp & 3) * 32) << 16;
     u32 phase = 0;
     for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         if (p.lower) {                                         // a tile inside one row, wholly above the diagonal
@@ -510,7 +521,7 @@ template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(const Crt
         const u64 o = tile * 128 + row;
         const bool valid = o < outputs;
         bool any = false;
-        for (int l0 = 0; l0 < p.L; l0 += 16) {                 // row of A: t_l as two bytes; 16 loads in flight
+        for (int l0 = half * 16; l0 < p.L; l0 += 32) {          // row of A: t_l as two bytes; 16 loads in flight
             u32 r[16];
 #pragma unroll
             for (int q = 0; q < 16; ++q) r[q] = (valid && l0 + q < p.L) ? p.res[(u64)(l0 + q) * outputs + o] : 0u;
@@ -519,13 +530,17 @@ template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(const Crt
                 const int l = l0 + q;
                 if (l >= p.L) break;
                 any |= r[q] != 0;
-                const u32 t = mod_barrett((u64)r[q] * p.tab->w[l], p.tab->m[l], p.tab->barrett[l]);
+                // t = r w mod m: r < m and w < m, so r w < 2^32 and one 32-bit Barrett step leaves [0, 2m)
+                const u32 m = s_m[l], x = r[q] * s_w[l];
+                u32 t = x - __umulhi(x, s_r[l]) * m;
+                if (t >= m) t -= m;
                 const u32 k = 2u * l;
                 *reinterpret_cast<u16*>(sA + (k >> 7) * 16384u + sw128_offset(row, k & 127u)) = (u16)t;
             }
         }
-        for (u32 k = 2u * p.L; k < (u32)kblocks * 128u; k += 2)
+        for (u32 k = 2u * p.L + 2u * half; k < (u32)kblocks * 128u; k += 4)
             *reinterpret_cast<u16*>(sA + (k >> 7) * 16384u + sw128_offset(row, k & 127u)) = 0;
+        s_any[half][row] = any ? 1 : 0;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic writes -> tensor core reads
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -544,8 +559,9 @@ template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(const Crt
         phase ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;");
         if (!fine) break;
-        // S and F from the byte columns of this row (every thread reads its lane: .sync.aligned)
-        if (p.sf) {                                             // S and F to global memory, word-major
+        any = (s_any[0][row] | s_any[1][row]) != 0;
+        // S and F from the byte columns of this row (every thread of warps 0-3 reads its lane: .sync.aligned)
+        if (half == 0 && p.sf) {                                // S and F to global memory, word-major
             int sw = 0;
             u64 acc = 0, F = 0;
             u32* dst = p.sf + o;
@@ -569,10 +585,7 @@ template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(const Crt
                 dst[(u64)(p.qwords + 2) * outputs] = (u32)F;
                 dst[(u64)(p.qwords + 3) * outputs] = (u32)(F >> 32);
             }
-            asm volatile("tcgen05.fence::before_thread_sync;");
-            __syncthreads();
-            continue;
-        }
+        } else if (half == 0) {                                 // S and F in registers, rounded here
         u32 S[kResMaxQWords + 2];
         int sw = 0;
         u64 acc = 0, F = 0;
@@ -604,6 +617,7 @@ template <int N> __global__ void __launch_bounds__(128) crt_mma_kernel(const Crt
                 else if (!li.nonzero || !ri.nonzero || !any) store<N>(out, p.subtract ? c : zero<N>());
                 else store<N>(out, crt_tail<N>(S, p.qwords, F, p.tab, (i64)li.bottom + ri.bottom - 2 * (32 * N - 1), p.subtract != 0, c));
             }
+        }
         }
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncthreads();                                        // TMEM and A are free for the next tile
@@ -801,7 +815,7 @@ template <int N> void digits_launch(const DigitParams& p, cudaStream_t s) {
 template <int N> void crt_launch(const CrtParams& p, unsigned grid, size_t smem, cudaStream_t s) {
     if (!p.M || !p.Nc) return;
     cudaFuncSetAttribute(crt_mma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    crt_mma_kernel<N><<<grid, 128, smem, s>>>(p);
+    crt_mma_kernel<N><<<grid, kCrtThreads, smem, s>>>(p);
     if (p.sf) crt_round_kernel<N><<<(unsigned)((p.M * p.Nc + 127) / 128), 128, 0, s>>>(p);
 }
 template <int N> void digits_mma_launch(const DigitMmaParams& p, unsigned grid, size_t smem, cudaStream_t s) {
