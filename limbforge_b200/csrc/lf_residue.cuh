@@ -83,7 +83,7 @@ template <int N> __global__ void __launch_bounds__(128) digits_kernel(DigitParam
 
 // ---------------------------------------------------------------- 2. tcgen05 residue products
 constexpr int kTileM = 128, kTileN = 128, kTileK = 128;      // K tile in int8 elements = one 128-byte row
-constexpr int kStages = 2;
+constexpr int kStages = 3;                                    // 3 x 64 KB of operand tiles (of 227 KB shared)
 constexpr int kTileBytes = kTileM * kTileK;                   // 16 KB per operand tile
 constexpr int kStageBytes = 4 * kTileBytes;                   // D1a, D0a, D1b, D0b
 constexpr u32 kSpinLimit = 1u << 28;                          // bounded mbarrier waits
