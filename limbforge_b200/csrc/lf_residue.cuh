@@ -436,11 +436,12 @@ template <int N> __global__ void __launch_bounds__(128) reconstruct_kernel(RecPa
 // (shifted) bytes, uploaded once per modulus count already in the 128-byte-swizzled K-major layout
 // of shared memory.  Each P[b] is below 2L * 255^2 < 2^25, so the int32 accumulators are exact.  One
 // CTA computes 128 outputs per tile and is persistent over the tiles:
-//   - all threads build their row of A from the residues (r -> t = r w_l mod m_l);
+//   - eight warps build the rows of A from the residues (r -> t = r w_l mod m_l), warps q and q + 4
+//     taking alternate groups of 16 moduli of the same rows;
 //   - one thread issues tcgen05.mma kind::i8 (u8 x u8 -> s32, M = 128, N <= 256 per instruction)
 //     into TMEM;
-//   - each thread reads its TMEM lane, carries the byte columns into S and F, and rounds its output
-//     with crt_tail.
+//   - each thread of warps 0-3 reads its TMEM lane and carries the byte columns into S and F, which
+//     go to memory for crt_round_kernel (or are rounded here with crt_tail).
 struct CrtParams {
     const u16* res; const ResTables* tab; const unsigned char* bimg;
     int L, qwords, NB, Kp, NS;             // B rows (multiple of 16), K bytes (multiple of 32), S byte columns
