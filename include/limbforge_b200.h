@@ -119,10 +119,13 @@ int lf_dev_exact_product(lf_linalg* linalg, int bits, const void* left, size_t l
  * allocate device memory when they need a product (a fixed device-memory plan, threads that must not
  * take the allocator's locks, embedding runtimes that forbid allocation): all temporary device data
  * lives in a 32 MiB static device array of the library, so no cudaMalloc/cudaFree is called.  Same
- * operands and result as lf_dev_exact_product; at most 8192 lines (M + N), and products whose residue
- * planes would exceed the array are rejected with LF_INVALID_ARGUMENT.  Calls share the array: calls
- * that overlap on the GPU race; the first call on a device resolves the array's address (make it
- * before any stream capture).  Synchronous on `stream`. */
+ * operands and result as lf_dev_exact_product; at most 8192 lines (M + N), larger products are
+ * rejected with LF_INVALID_ARGUMENT.  A product whose residue planes would not fit the array runs on
+ * the generic limb kernel (same bits, slower).  Calls share the array, so calls that overlapped on the
+ * GPU would race: the library serializes them process-wide with one lock held until the product is
+ * done, and each call blocks until then (synchronous on `stream`).  The first call on a device, and
+ * the first after that device's context was recreated (a device reset), resolves the array's address:
+ * make that call before any stream capture. */
 int lf_dev_exact_product_static(int bits, const void* left, size_t left_ls, size_t left_ks, const void* right,
                                 size_t right_ls, size_t right_ks, size_t M, size_t N, size_t K, void* C, size_t ldc,
                                 int subtract, int lower, void* stream);

@@ -10,9 +10,16 @@
 //
 // The array is shared by every call and keeps the last call's contents: whatever must start at zero
 // (the error word) is cleared by each call, and two calls that overlap on the GPU (different streams or
-// threads without ordering between them) race on the array.  The first call on a device looks up the
-// array's device address with cudaGetSymbolAddress (with that device current); make that first call
-// before any stream capture.
+// threads without ordering between them) would race on the array.  Inside this library the calls are
+// serialized process-wide by one lock that is held until the product has completed, so a second host
+// thread waits for the first.  The first call on a device (and the first after that device's context was
+// destroyed and recreated, which the call detects from the context id) looks up the array's device
+// address with cudaGetSymbolAddress (with that device current); make that first call before any stream
+// capture.
+//
+// The residue engine's digit planes and residues must fit the array.  When they do not, the product runs
+// on the generic limb kernel, which needs only the error word and gives the same bits; only products of
+// more than kMaxLines lines (the line table) are refused.
 #include "lf_residue.h"
 #include "lf_residue.cuh"
 
@@ -30,6 +37,7 @@ static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 std::mutex g_mutex;
 unsigned char* g_base[kMaxDevices];                     // device address of g_scratch, per device
+unsigned long long g_context[kMaxDevices];              // id of the context that address belongs to
 int g_tables_L[kMaxDevices];                            // modulus count whose tables the array holds
 int g_tables_qwords[kMaxDevices];                       // their quotient word count
 lfd::ResTables g_host_tables;                           // staging for the table upload (host, static)
@@ -37,12 +45,39 @@ lfd::LineInfo g_host_lines[kMaxLines];
 
 size_t up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-// Device address of the static array on the current device (set-up on the first call per device).
+// Unique id of the current context (cuCtxGetId through the runtime's driver entry points): a device
+// reset or a destroyed primary context gives the next call a new id.
+unsigned long long current_context_id() {
+    typedef CUresult (*GetCurrent)(CUcontext*);
+    typedef CUresult (*GetId)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+            throw lfr::runtime_error("cuCtxGetCurrent unavailable");
+        get_current = reinterpret_cast<GetCurrent>(f);
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+            throw lfr::runtime_error("cuCtxGetId unavailable");
+        get_id = reinterpret_cast<GetId>(f);
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) throw lfr::runtime_error("no current CUDA context");
+    return id;
+}
+
+// Device address of the static array on the current device: set up on the first call per device and
+// again whenever the device's context has changed since (the tables uploaded into the old context are
+// gone with it).
 unsigned char* scratch_base(int device) {
-    if (!g_base[device]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_base[device] || g_context[device] != ctx) {
         void* p = nullptr;
         lfr::cuda_check(cudaGetSymbolAddress(&p, g_scratch), "scratch symbol address");
         g_base[device] = static_cast<unsigned char*>(p);
+        g_context[device] = ctx;
         g_tables_L[device] = 0;
     }
     return g_base[device];
@@ -64,6 +99,7 @@ extern "C" int lf_dev_exact_product_static(int bits, const void* left, size_t le
     int device = 0;
     cuda_check(cudaGetDevice(&device), "cudaGetDevice");
     if (device < 0 || device >= kMaxDevices) throw runtime_error("device index out of range");
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");  // initializes the device's primary context and makes it current
     unsigned char* base = scratch_base(device);
     if (!M || !N) return LF_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -97,15 +133,17 @@ extern "C" int lf_dev_exact_product_static(int bits, const void* left, size_t le
             if (!g_host_lines[i].status && g_host_lines[i].nonzero) { G = std::max(G, g_host_lines[i].top - g_host_lines[i].bottom); any = true; }
         residue = any && G <= residue_max_band() && (L = residue_moduli_for(bits, G, K)) > 0;
     }
+    uint64_t Kp = 0, Mp = 0, Np = 0, aplane = 0, bplane = 0;
+    size_t res_off = 0;
+    if (residue) {                                      // planes and residues must fit the array
+        Kp = up(K, lfd::kTileK); Mp = up(M, lfd::kTileM); Np = up(N, lfd::kTileN);
+        aplane = (uint64_t)L * Mp * Kp; bplane = (uint64_t)L * Np * Kp;
+        res_off = up(planes_off + 2 * (aplane + bplane), 256);
+        residue = res_off + sizeof(uint16_t) * (uint64_t)L * M * N <= kScratchBytes;
+    }
     if (!residue) {
         limb_kernel();
     } else {
-        const uint64_t Kp = up(K, lfd::kTileK), Mp = up(M, lfd::kTileM), Np = up(N, lfd::kTileN);
-        const uint64_t aplane = (uint64_t)L * Mp * Kp, bplane = (uint64_t)L * Np * Kp;
-        const size_t res_off = up(planes_off + 2 * (aplane + bplane), 256);
-        const size_t need = res_off + sizeof(uint16_t) * (uint64_t)L * M * N;
-        if (need > kScratchBytes)
-            throw invalid_argument("static-scratch product needs " + std::to_string(need >> 20) + " MiB of scratch, above the 32 MiB static area");
         if (g_tables_L[device] != L) {
             std::memset(&g_host_tables, 0, sizeof(g_host_tables));
             int qw = 0;

@@ -185,21 +185,23 @@ __global__ void __launch_bounds__(kMmaThreads, 1) residue_mma_kernel(const __gri
     const u32 tmem = tmem_slot;
     const u32 acc11 = tmem, acc00 = tmem + kTileN, accm = tmem + 2 * kTileN;
     const int kblocks = (int)(p.Kp / kTileK);
-    __shared__ int abort_flag;
-    if (threadIdx.x == 0) abort_flag = 0;
+    __shared__ int abort_flag, issued, consumed;          // stages loaded by the producer / read by the MMA issuer
+    if (threadIdx.x == 0) { abort_flag = 0; issued = 0; consumed = kblocks; }
     __syncthreads();
     if (warp == 0 && lane == 0) {
-        // producer
+        // producer; stops issuing once the MMA issuer has given up
         for (int kb = 0; kb < kblocks; ++kb) {
             const int s = kb % kStages;
             const u32 ph = (u32)((kb / kStages) & 1);
             if (kb >= kStages && !mbar_wait(&empty[s], ph ^ 1u, p.error)) { abort_flag = 1; break; }
+            if (*(volatile int*)&abort_flag) break;
             unsigned char* st = smem + s * kStageBytes;
             mbar_expect_tx(&full[s], kStageBytes);
             tma_load_3d(st, &ta1, &full[s], kb * kTileK, tm * kTileM, l);
             tma_load_3d(st + kTileBytes, &ta0, &full[s], kb * kTileK, tm * kTileM, l);
             tma_load_3d(st + 2 * kTileBytes, &tb1, &full[s], kb * kTileK, tn * kTileN, l);
             tma_load_3d(st + 3 * kTileBytes, &tb0, &full[s], kb * kTileK, tn * kTileN, l);
+            issued = kb + 1;
         }
     } else if (warp == 1 && lane == 0) {
         // MMA issuer
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) residue_mma_kernel(const __gri
         for (int kb = 0; kb < kblocks && ok; ++kb) {
             const int s = kb % kStages;
             const u32 ph = (u32)((kb / kStages) & 1);
-            if (!mbar_wait(&full[s], ph, p.error)) { ok = false; abort_flag = 1; break; }
+            if (!mbar_wait(&full[s], ph, p.error)) { ok = false; consumed = kb; *(volatile int*)&abort_flag = 1; break; }
             asm volatile("tcgen05.fence::after_thread_sync;");
             unsigned char* st = smem + s * kStageBytes;
             const u64 a1 = smem_desc(st), a0 = smem_desc(st + kTileBytes), b1 = smem_desc(st + 2 * kTileBytes),
@@ -226,6 +228,11 @@ __global__ void __launch_bounds__(kMmaThreads, 1) residue_mma_kernel(const __gri
         mma_commit(&done);                                    // arrives after every MMA issued above
     }
     __syncthreads();
+    if (abort_flag && threadIdx.x == 0) {
+        // An abandoned wait leaves loads in flight into shared memory: let every stage that was loaded and
+        // not read complete (bounded) before the CTA releases its resources.
+        for (int kb = consumed; kb < issued; ++kb) mbar_wait(&full[kb % kStages], (u32)((kb / kStages) & 1), p.error);
+    }
     const bool fine = mbar_wait(&done, 0, p.error) && !abort_flag;
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (fine) {
