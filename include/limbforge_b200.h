@@ -204,6 +204,20 @@ int lf_batch_cast(lf_batch* batch, int from_bits, int to_bits, int complex_, lf_
                   size_t count);                                                         /* CommandBatch::cast */
 int lf_batch_tree_sum(lf_batch* batch, int bits, int complex_, lf_buffer* in, lf_buffer* out,
                       size_t count);                                                     /* CommandBatch::tree_sum */
+/* Segmented dot products (engine.hpp:30-32,205; kernels.metal:195-207): out[i] is the fused chain s <- fma(a[i*length+k],
+ * b[i*length+k] (or b[k] when shared_right), s) from s = 0 over k = 0..length-1, cfma for complex. */
+typedef struct lf_segmented_dot { size_t segments, length; int shared_right; } lf_segmented_dot;   /* engine.hpp:32 */
+int lf_engine_segmented_dot(lf_engine* engine, int bits, int complex_, const lf_segmented_dot* shape, const void* a, const void* b,
+                            void* out, lf_timing* timing);                               /* Engine::segmented_dot */
+int lf_batch_segmented_dot(lf_batch* batch, int bits, int complex_, const lf_segmented_dot* shape, lf_buffer* a, lf_buffer* b,
+                           lf_buffer* out);                                              /* CommandBatch::segmented_dot */
+/* Engine::recurrence (engine.hpp:218-223; kernels.metal:39-58): complex four-value rings, seeds[j*count+i],
+ * weights[(step*4+j)*(count/states_per_weight)+i/states_per_weight]; each step q <- sum_j w_j q_j as
+ * cadd(cadd(cadd(cadd(0, cmul(w_0, q_0)), ...))) and the ring shifts; out[i] is the last value (the fourth
+ * seed after zero steps). */
+int lf_engine_recurrence(lf_engine* engine, int bits, const void* seeds, const void* weights, void* out, size_t count,
+                         unsigned steps, unsigned states_per_weight, lf_timing* timing);
+
 /* Device-pointer forms (no reference counterpart), asynchronous on `stream`; tree_sum's scratch holds
  * 2 * ceil(count / 2) elements (unused for count <= 2). */
 int lf_dev_cast(int from_bits, int to_bits, int complex_, const void* in, void* out, size_t count, void* stream);
@@ -256,6 +270,11 @@ int lf_ragged_plan_tune(lf_ragged_plan* plan, const void* arena);
 int lf_ragged_plan_run(lf_ragged_plan* plan, void* arena, void* stream);
 int lf_ragged_plan_get_info(const lf_ragged_plan* plan, lf_ragged_info* info);
 void lf_ragged_plan_destroy(lf_ragged_plan* plan);
+
+/* ---- Measurement helper (no reference counterpart): the device's rate of 32 x 32 -> 64-bit integer
+ * multiply-adds, the word product of every limb kernel, measured by a kernel of independent
+ * multiply-add chains on every SM (CUDA events).  The denominator of the integer-pipe roofline. */
+int lf_probe_word_mac_rate(int device, double* word_macs_per_s);
 
 #ifdef __cplusplus
 }

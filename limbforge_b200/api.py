@@ -95,6 +95,13 @@ class Batched4:                                                  # engine.hpp:36
 
 
 @dataclass
+class SegmentedDot:                                              # engine.hpp:30-32
+    segments: int = 0
+    length: int = 0
+    shared_right: bool = False
+
+
+@dataclass
 class StridedGemm:                                               # batched_linalg.hpp:11-14
     count: int = 1
     m: int = 0
@@ -155,6 +162,10 @@ class _EngineOptions(C.Structure):
 
 class _Batched4(C.Structure):
     _fields_ = [("count", C.c_size_t), ("rhs", C.c_uint), ("inverse", C.c_int), ("determinant", C.c_int), ("fused", C.c_int)]
+
+
+class _SegmentedDot(C.Structure):
+    _fields_ = [("segments", C.c_size_t), ("length", C.c_size_t), ("shared_right", C.c_int)]
 
 
 class _StridedGemm(C.Structure):
@@ -256,6 +267,10 @@ def _load() -> C.CDLL:
         "lf_ragged_plan_create": ([V, I, I, V, S, P(_RaggedLu4), C.c_uint64, P(V)], I),
         "lf_ragged_plan_tune": ([V, V], I), "lf_ragged_plan_run": ([V, V, V], I),
         "lf_ragged_plan_get_info": ([V, P(_RaggedInfo)], I), "lf_ragged_plan_destroy": ([V], None),
+        "lf_probe_word_mac_rate": ([I, P(C.c_double)], I),
+        "lf_engine_segmented_dot": ([V, I, I, P(_SegmentedDot), V, V, V, P(_Timing)], I),
+        "lf_batch_segmented_dot": ([V, I, I, P(_SegmentedDot), V, V, V], I),
+        "lf_engine_recurrence": ([V, I, V, V, V, S, C.c_uint, C.c_uint, P(_Timing)], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -412,6 +427,11 @@ class CommandBatch:
         check(lib.lf_batch_lu4(self.handle, A.bits, C.byref(s), A.handle, B.handle if B else None, X.handle if X else None,
                                det.handle if det else None, status.handle))
 
+    def segmented_dot(self, shape: SegmentedDot, a: Buffer, b: Buffer, out: Buffer) -> None:
+        """CommandBatch::segmented_dot (engine.hpp:174)."""
+        sh = _SegmentedDot(shape.segments, shape.length, int(shape.shared_right))
+        check(lib.lf_batch_segmented_dot(self.handle, a.bits, int(a.complex), C.byref(sh), a.handle, b.handle, out.handle))
+
     def cast(self, a: Buffer, out: Buffer) -> None:
         """CommandBatch::cast (engine.hpp:171): a's elements rounded to out's width."""
         if a.complex != out.complex or a.count != out.count or not a.bits or not out.bits:
@@ -489,6 +509,24 @@ class Engine:
         t = _Timing()
         check(lib.lf_engine_cast(self.handle, from_bits, to_bits, int(complex_), _ptr(np.ascontiguousarray(x)), _ptr(out), count,
                                  C.byref(t)))
+        return out, _timing(t)
+
+    def segmented_dot(self, bits, complex_, shape: SegmentedDot, a, b):
+        """Engine::segmented_dot (engine.hpp:205): returns (out [segments], Timing)."""
+        n = check_bits(bits)
+        out = np.zeros((shape.segments, 2, n + 3) if complex_ else (shape.segments, n + 3), dtype=np.uint32)
+        sh = _SegmentedDot(shape.segments, shape.length, int(shape.shared_right))
+        t = _Timing()
+        check(lib.lf_engine_segmented_dot(self.handle, bits, int(complex_), C.byref(sh), _ptr(a), _ptr(b), _ptr(out), C.byref(t)))
+        return out, _timing(t)
+
+    def recurrence(self, bits, seeds, weights, count, steps, states_per_weight=1):
+        """Engine::recurrence (engine.hpp:218-223): returns (out [count] complex, Timing)."""
+        n = check_bits(bits)
+        out = np.zeros((count, 2, n + 3), dtype=np.uint32)
+        t = _Timing()
+        check(lib.lf_engine_recurrence(self.handle, bits, _ptr(seeds), _ptr(weights), _ptr(out), count, steps, states_per_weight,
+                                       C.byref(t)))
         return out, _timing(t)
 
     def lu4(self, bits, shape: Batched4, A, B=None):
@@ -789,3 +827,10 @@ def dev_tree_sum(bits, complex_, in_ptr, count, out_ptr, scratch_ptr, stream=0) 
     """scratch: 2 * ceil(count / 2) elements (unused for count <= 2)."""
     check(lib.lf_dev_tree_sum(bits, int(complex_), C.c_void_p(in_ptr), count, C.c_void_p(out_ptr),
                               C.c_void_p(scratch_ptr), C.c_void_p(stream)))
+
+
+def word_mac_rate(device: int = 0) -> float:
+    """Measured rate of 32 x 32 -> 64-bit integer multiply-adds on `device` (lf_probe_word_mac_rate)."""
+    r = C.c_double()
+    check(lib.lf_probe_word_mac_rate(device, C.byref(r)))
+    return r.value

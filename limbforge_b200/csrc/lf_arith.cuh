@@ -855,142 +855,207 @@ template <int N> __device__ __forceinline__ Num<N> fma(const Num<N>& a, const Nu
 }
 template <int N> __device__ __forceinline__ Num<N> fms(const Num<N>& a, const Num<N>& b, const Num<N>& c) { return fma<N>(a, b, negate<N>(c)); }
 
-// ---------------------------------------------------------------- exact sums of up to three terms
-// An exact term sign * int(w) * 2^scale of at most XW words (local array; the routines below use
-// runtime lengths, which keeps the rarely used wide paths compact).
-template <int XW> struct Exact { u32 w[XW]; int len; i64 scale; int sign; };
+// ---------------------------------------------------------------- exact sums by clusters
+// acc (len words) += t << off; t has tw words; acc wide enough (callers check)
+__device__ __forceinline__ void acc_add(u32* acc, int len, const u32* t, int tw, i64 off) {
+    const int ws = (int)(off >> 5), bs = (int)(off & 31);
+    u64 cy = 0;
+    int k = ws;
+    for (int q = 0; q <= tw && k < len; ++q, ++k) {
+        u32 v = q < tw ? t[q] << bs : 0u;
+        if (bs && q > 0) v |= t[q - 1] >> (32 - bs);
+        u64 s = (u64)acc[k] + v + cy; acc[k] = (u32)s; cy = s >> 32;
+    }
+    for (; cy && k < len; ++k) { u64 s = (u64)acc[k] + cy; acc[k] = (u32)s; cy = s >> 32; }
+}
 
-template <int XW> __device__ __forceinline__ i64 ex_msb(const Exact<XW>& x) {
-    for (int k = x.len - 1; k >= 0; --k) if (x.w[k]) return x.scale + 32 * (i64)k + 31 - __clz(x.w[k]);
-    return x.scale - 1;
-}
-template <int XW> __device__ __forceinline__ void ex_add_into(u32* acc, int len, const Exact<XW>& x, i64 off, bool subtract) {
-    // acc (len words) +/-= x.w << off
-    const i64 ws = off >> 5; const int bs = (int)(off & 31);
-    if (!subtract) {
-        u64 cy = 0;
-        for (int k = (int)ws; k < len; ++k) {
-            const i64 src = k - ws;
-            u32 v = 0;
-            if (src < x.len) v = x.w[src] << bs;
-            if (bs && src >= 1 && src - 1 < x.len) v |= x.w[src - 1] >> (32 - bs);
-            if (src > x.len && !cy) break;
-            u64 t = (u64)acc[k] + v + cy; acc[k] = (u32)t; cy = t >> 32;
-        }
-    } else {
-        u32 bo = 0;
-        for (int k = (int)ws; k < len; ++k) {
-            const i64 src = k - ws;
-            u32 v = 0;
-            if (src < x.len) v = x.w[src] << bs;
-            if (bs && src >= 1 && src - 1 < x.len) v |= x.w[src - 1] >> (32 - bs);
-            if (src > x.len && !bo) break;
-            u64 t = (u64)v + bo; u32 old = acc[k]; acc[k] = (u32)((u64)old - t); bo = (u64)old < t;
-        }
-    }
-}
-// x + y exactly, or with y replaced by a sticky unit when y lies wholly more than one bit below
-// x's window [msb(x) - (32N+33), msb(x)] (and below x's lowest bit): then only y's sign can
-// matter to a 32N-bit rounding.  The ordered pairwise structure follows core.hpp:251-275.
-template <int N, int XW> __device__ __noinline__ Exact<XW> ex_add(const Exact<XW>& a, const Exact<XW>& b) {
-    if (!b.sign) return a;
-    if (!a.sign) return b;
-    const bool sw = ex_msb(a) < ex_msb(b);
-    const Exact<XW>& x = sw ? b : a;
-    const Exact<XW>& y = sw ? a : b;
-    const i64 mx = ex_msb(x), my = ex_msb(y);
-    i64 low = mx - (32 * N + 33);
-    if (x.scale < low) low = x.scale;
-    Exact<XW> r;
-    for (int k = 0; k < XW; ++k) r.w[k] = 0;
-    if (my < low - 1) {
-        r.scale = low - 32;
-        r.len = (int)((mx - r.scale) / 32) + 2;
-        ex_add_into<XW>(r.w, r.len, x, x.scale - r.scale, false);
-        if (x.sign == y.sign) r.w[0] |= 1u;              // the word below x is empty
-        else { for (int k = 0; k < r.len; ++k) { u32 old = r.w[k]; r.w[k] = old - 1; if (old) break; } }
-        r.sign = x.sign;
-        return r;
-    }
-    r.scale = x.scale < y.scale ? x.scale : y.scale;
-    r.len = (int)((mx - r.scale) / 32) + 2;
-    u32 t[XW];
-    for (int k = 0; k < XW; ++k) t[k] = 0;
-    ex_add_into<XW>(r.w, r.len, x, x.scale - r.scale, false);
-    ex_add_into<XW>(t, r.len, y, y.scale - r.scale, false);
-    if (x.sign == y.sign) {
-        u64 cy = 0;
-        for (int k = 0; k < r.len; ++k) { u64 s = (u64)r.w[k] + t[k] + cy; r.w[k] = (u32)s; cy = s >> 32; }
-        r.sign = x.sign;
-        return r;
-    }
-    int c = 0;
-    for (int k = r.len - 1; k >= 0 && !c; --k) if (r.w[k] != t[k]) c = r.w[k] > t[k] ? 1 : -1;
-    if (!c) { r.sign = 0; r.scale = 0; r.len = 1; for (int k = 0; k < XW; ++k) r.w[k] = 0; return r; }
-    u32 bo = 0;
-    for (int k = 0; k < r.len; ++k) {
-        u32 p = c > 0 ? r.w[k] : t[k], q = c > 0 ? t[k] : r.w[k];
-        u64 s = (u64)q + bo; r.w[k] = (u32)((u64)p - s); bo = (u64)p < s;
-    }
-    r.sign = c > 0 ? x.sign : y.sign;
-    return r;
-}
-template <int N, int XW> __device__ __noinline__ Num<N> ex_round(const Exact<XW>& x) {
-    if (!x.sign) return zero<N>();
+// Rounding record of a nonzero exact magnitude: N result words, exponent, round and sticky bits.
+template <int N> struct Rounded { u32 m[N]; i64 e; bool rb, sb; };
+template <int N> __device__ bool round_info(const u32* x, int len, i64 scale, Rounded<N>& r) {
     int t = -1;
-    for (int k = x.len - 1; k >= 0; --k) if (x.w[k]) { t = k; break; }
-    if (t < 0) return zero<N>();
-    const int h = 32 * t + 31 - __clz(x.w[t]);
-    i64 e = x.scale + h;
-    const int shift = h - (32 * N - 1);             // bit of x that becomes bit 0 of the result
-    u32 m[N];
+    for (int k = len - 1; k >= 0; --k) if (x[k]) { t = k; break; }
+    if (t < 0) return false;
+    const int h = 32 * t + 31 - __clz(x[t]);
+    r.e = scale + h;
+    const int shift = h - (32 * N - 1);
     for (int i = 0; i < N; ++i) {
         const int p = shift + 32 * i;
         u32 v = 0;
         if (p <= -32) v = 0;
-        else if (p < 0) v = x.w[0] << (-p);
-        else { const int wi = p >> 5, bi = p & 31; v = wi < x.len ? x.w[wi] >> bi : 0u; if (bi && wi + 1 < x.len) v |= x.w[wi + 1] << (32 - bi); }
-        m[i] = v;
+        else if (p < 0) v = x[0] << (-p);
+        else { const int wi = p >> 5, bi = p & 31; v = wi < len ? x[wi] >> bi : 0u; if (bi && wi + 1 < len) v |= x[wi + 1] << (32 - bi); }
+        r.m[i] = v;
     }
-    bool up = false;
+    r.rb = false; r.sb = false;
     if (shift > 0) {
         const int rbp = shift - 1;
-        const bool rb = (x.w[rbp >> 5] >> (rbp & 31)) & 1u;
-        bool st = (rbp & 31) && (x.w[rbp >> 5] & ((1u << (rbp & 31)) - 1u));
-        for (int k = 0; k < (rbp >> 5) && !st; ++k) st = x.w[k] != 0;
-        up = rb && (st || (m[0] & 1u));
+        r.rb = (x[rbp >> 5] >> (rbp & 31)) & 1u;
+        bool st = (rbp & 31) && (x[rbp >> 5] & ((1u << (rbp & 31)) - 1u));
+        for (int k = 0; k < (rbp >> 5) && !st; ++k) st = x[k] != 0;
+        r.sb = st;
     }
-    return finish<N>(m, e, x.sign, up, 0);
+    return true;
 }
-// RN(a*b + c*d + e) with one rounding: terms ordered by msb; either the two smaller terms are
-// far below the largest and summed first, or the largest two overlap and are summed exactly
-// first; each pairwise step is exact or a valid sticky collapse (core.hpp:330-351).
+
+// RN(sum of the nonzero terms of `src`) with one rounding, for any spread of exponents.  A term source has
+//   u64 count() const;                                          term slots 0 .. count()-1
+//   bool term(u64 k, i64& scale, i64& top, int& sign) const;    false for a zero slot; the term is
+//                                                               sign * T * 2^scale with 0 < T < 2^(top - scale)
+//   void add(u64 k, u32* acc, int len, i64 off) const;          acc (len words) += T << off
+// The terms are summed cluster by cluster from the highest: a cluster holds the highest remaining top and
+// grows downwards while some remaining term reaches within gap = 32N + ceil(log2(count + 1)) + 4 bits of its
+// lowest bit; it is summed exactly as positive and negative magnitudes in CW words.  The first nonzero
+// cluster sum S is kept; everything below it is less than 2^(lowest bit of S - 32N - 2) in magnitude, so of
+// the rest only the sign of the next nonzero cluster can matter (to exact ties and exact S).  A cluster wider
+// than CW words sets *error (when given) and gives zero with status invalid.
+template <int N, int CW, class Src> __device__ Num<N> cluster_round(const Src& src, u32* error) {
+    const u64 n = src.count();
+    int count = 0;
+    i64 T = INT64_MIN;
+    for (u64 k = 0; k < n; ++k) {
+        i64 s, tp; int sg;
+        if (!src.term(k, s, tp, sg)) continue;
+        T = tp > T ? tp : T;
+        ++count;
+    }
+    if (!count) return zero<N>();
+    int logc = 0;
+    while ((1 << logc) < count + 1) ++logc;
+    const i64 gap = 32 * N + logc + 4;
+    u32 pos[CW], neg[CW];
+    i64 cutoff = T;                        // inclusive bound on the tops still to visit
+    bool have = false;
+    Rounded<N> R; int rsign = 0, sigma = 0;
+    for (;;) {
+        i64 Tc = INT64_MIN;                // top of the next cluster
+        for (u64 k = 0; k < n; ++k) {
+            i64 s, tp; int sg;
+            if (src.term(k, s, tp, sg) && tp <= cutoff && tp > Tc) Tc = tp;
+        }
+        if (Tc == INT64_MIN) break;
+        i64 low = INT64_MAX;               // lowest bit: grow while a remaining term reaches within `gap`
+        for (u64 k = 0; k < n; ++k) {
+            i64 s, tp; int sg;
+            if (src.term(k, s, tp, sg) && tp == Tc && s < low) low = s;
+        }
+        for (;;) {
+            i64 nl = low;
+            for (u64 k = 0; k < n; ++k) {
+                i64 s, tp; int sg;
+                if (src.term(k, s, tp, sg) && tp <= cutoff && tp > low - gap && s < nl) nl = s;
+            }
+            if (nl == low) break;
+            low = nl;
+        }
+        const int len = (int)((Tc - low + logc + 2 + 31) / 32) + 1;
+        if (len > CW) { if (error) atomicExch(error, 1u); return zero<N>(kInvalid); }
+        for (int w = 0; w < len; ++w) { pos[w] = 0; neg[w] = 0; }
+        for (u64 k = 0; k < n; ++k) {
+            i64 s, tp; int sg;
+            if (!src.term(k, s, tp, sg) || !(tp <= cutoff && tp > low - gap)) continue;
+            src.add(k, sg > 0 ? pos : neg, len, s - low);
+        }
+        cutoff = low - gap;
+        int cmp = 0;
+        for (int w = len - 1; w >= 0 && !cmp; --w) if (pos[w] != neg[w]) cmp = pos[w] > neg[w] ? 1 : -1;
+        if (!cmp) continue;                // the cluster cancels exactly
+        u32* big = cmp > 0 ? pos : neg;
+        const u32* small = cmp > 0 ? neg : pos;
+        u32 bo = 0;
+        for (int w = 0; w < len; ++w) { u64 d = (u64)small[w] + bo; u32 o = big[w]; big[w] = (u32)((u64)o - d); bo = (u64)o < d; }
+        if (!have) { round_info<N>(big, len, low, R); rsign = cmp; have = true; continue; }
+        sigma = cmp == rsign ? 1 : -1;     // sign of everything below, relative to S
+        break;
+    }
+    if (!have) return zero<N>();
+    // RN(S + sigma * tiny): the tail decides only exact ties and exact S
+    const bool up = R.rb && (R.sb || sigma > 0 || (sigma == 0 && (R.m[0] & 1u)));
+    return finish<N>(R.m, R.e, rsign, up, 0);
+}
+
+// ---------------------------------------------------------------- RN(a*b + c*d + e)
+// The two products and the addend as a term source for cluster_round (words in registers or local memory).
+template <int N> struct Dot2Terms {
+    const u32* w[3]; int len[3]; i64 scale[3]; int sign[3];
+    __device__ u64 count() const { return 3; }
+    __device__ bool term(u64 k, i64& s, i64& tp, int& sg) const {
+        if (!sign[k]) return false;
+        s = scale[k]; tp = scale[k] + 32 * len[k]; sg = sign[k];
+        return true;
+    }
+    __device__ void add(u64 k, u32* acc, int alen, i64 off) const { acc_add(acc, alen, w[k], len[k], off); }
+};
+// One rounding of the exact sum.  Fast path: fma's window, widened to three terms.  One two's-complement window
+// of F = 3N+4 words sits above a sticky word, anchored three bits above the highest term's top bit (three terms
+// below 2^hi sum below 2^(hi+2), plus the sign).  With lo the window's lowest bit, a term whose lowest bit is at
+// or above lo is placed exactly, and a term below 2^(lo-1) in magnitude becomes one unit of the sticky word with
+// its sign.  Let P be the exact sum of the placed terms (a multiple of 2^lo) and R that of the dropped ones
+// (|R| < 2^lo).  When the dropped terms share a sign, the window holds P' = P + u 2^(lo-32) with sign(u) =
+// sign(R).  When moreover |P'| >= 2^(lo+32N), every rounding boundary of the result's binade (representable
+// values and midpoints) is a multiple of 2^lo; P + R and P' lie within 2^lo of P on the same side of it (or both
+// equal P), in the same binade, so they round alike and the window's rounding is RN(ab + cd + e).  Any other
+// case (a term straddling lo, dropped terms of opposite signs, deep cancellation) sums the terms by clusters,
+// the limb kernel's exact method, in 8N+4 words: three chained terms of at most 64N bits and two gaps below.
 template <int N> __device__ __noinline__ Num<N> dot2_add(const Num<N>& a, const Num<N>& b, const Num<N>& c, const Num<N>& d, const Num<N>& e) {
     const u32 st = a.st | b.st | c.st | d.st | e.st;
     if (st) return zero<N>(st);
-    constexpr int XW = 6 * N + 10;
-    Exact<XW> t[3];
-    for (int q = 0; q < 3; ++q) { for (int k = 0; k < XW; ++k) t[q].w[k] = 0; t[q].len = 1; t[q].scale = 0; t[q].sign = 0; }
-    if (a.s && b.s) { u32 p[2 * N]; mant_mul<N>(a.m, b.m, p); for (int k = 0; k < 2 * N; ++k) t[0].w[k] = p[k];
-        t[0].len = 2 * N; t[0].scale = (i64)a.e + b.e - 2 * (32 * N - 1); t[0].sign = a.s * b.s; }
-    if (c.s && d.s) { u32 p[2 * N]; mant_mul<N>(c.m, d.m, p); for (int k = 0; k < 2 * N; ++k) t[1].w[k] = p[k];
-        t[1].len = 2 * N; t[1].scale = (i64)c.e + d.e - 2 * (32 * N - 1); t[1].sign = c.s * d.s; }
-    if (e.s) { for (int k = 0; k < N; ++k) t[2].w[k] = e.m[k]; t[2].len = N; t[2].scale = (i64)e.e - (32 * N - 1); t[2].sign = e.s; }
-    i64 key[3];
-    for (int q = 0; q < 3; ++q) key[q] = t[q].sign ? ex_msb(t[q]) : -((i64)1 << 62);
-    const int i1 = key[0] >= key[1] ? (key[0] >= key[2] ? 0 : 2) : (key[1] >= key[2] ? 1 : 2);
-    int i3 = key[0] < key[1] ? (key[0] < key[2] ? 0 : 2) : (key[1] < key[2] ? 1 : 2);
-    if (i3 == i1) i3 = (i1 + 1) % 3;
-    const int i2 = 3 - i1 - i3;
-    if (!t[i1].sign) return zero<N>();
-    i64 low = key[i1] - (32 * N + 33);
-    if (t[i1].scale < low) low = t[i1].scale;
-    if (!t[i2].sign || key[i2] < low - 1) {
-        Exact<XW> s = ex_add<N, XW>(t[i2], t[i3]);
-        return ex_round<N, XW>(ex_add<N, XW>(t[i1], s));
+    const int s1 = a.s * b.s, s2 = c.s * d.s;
+    if (!s1 && !s2) return e.s ? e : zero<N>();
+    u32 p1[2 * N], p2[2 * N];
+    i64 sc1 = 0, sc2 = 0, top = INT64_MIN;            // scales; top: above the highest term's top bit
+    if (s1) { mant_mul<N>(a.m, b.m, p1); sc1 = (i64)a.e + b.e - 2 * (32 * N - 1); const i64 t = sc1 + 64 * N - ((p1[2 * N - 1] >> 31) ? 0 : 1); top = t > top ? t : top; }
+    if (s2) { mant_mul<N>(c.m, d.m, p2); sc2 = (i64)c.e + d.e - 2 * (32 * N - 1); const i64 t = sc2 + 64 * N - ((p2[2 * N - 1] >> 31) ? 0 : 1); top = t > top ? t : top; }
+    const i64 sce = (i64)e.e - (32 * N - 1);
+    if (e.s) top = (i64)e.e + 1 > top ? (i64)e.e + 1 : top;
+    constexpr int F = 3 * N + 4, W = F + 1;
+    const i64 lo = top + 3 - 32 * (i64)F;
+    u32 acc[W], t[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) acc[k] = 0;
+    bool fast = true;
+    int dropped = 0;                                  // sign of the sticky units so far
+    const auto sticky = [&](int sg) {
+        if (dropped && dropped != sg) fast = false;
+        dropped = sg;
+#pragma unroll
+        for (int k = 0; k < W; ++k) t[k] = k == 0 ? 1u : 0u;
+        accumulate<W>(acc, t, sg < 0);
+    };
+    if (s1) {
+        if (sc1 >= lo) { place_words<W, 2 * N>(t, p1, 32 + (sc1 - lo)); accumulate<W>(acc, t, s1 < 0); }
+        else if (sc1 + 64 * N <= lo - 1) sticky(s1);
+        else fast = false;
     }
-    Exact<XW> r = ex_add<N, XW>(t[i1], t[i2]);
-    return ex_round<N, XW>(ex_add<N, XW>(r, t[i3]));
+    if (s2 && fast) {
+        if (sc2 >= lo) { place_words<W, 2 * N>(t, p2, 32 + (sc2 - lo)); accumulate<W>(acc, t, s2 < 0); }
+        else if (sc2 + 64 * N <= lo - 1) sticky(s2);
+        else fast = false;
+    }
+    if (e.s && fast) {
+        if (sce >= lo) { place_words<W, N>(t, e.m, 32 + (sce - lo)); accumulate<W>(acc, t, e.s < 0); }
+        else if ((i64)e.e + 1 <= lo - 1) sticky(e.s);
+        else fast = false;
+    }
+    if (fast) {
+        int sign = 1;
+        if (acc[W - 1] >> 31) {
+            sign = -1; u64 cy = 1;
+#pragma unroll
+            for (int k = 0; k < W; ++k) { u64 x = (u64)(u32)~acc[k] + cy; acc[k] = (u32)x; cy = x >> 32; }
+        }
+        int hw = -1;
+#pragma unroll
+        for (int k = 0; k < W; ++k) hw = acc[k] ? k : hw;
+        if (hw < 0 && !dropped) return zero<N>();    // exact cancellation
+        if (hw >= 0) {
+            u32 topw = 0;
+#pragma unroll
+            for (int k = 0; k < W; ++k) topw = k == hw ? acc[k] : topw;
+            if (32 * hw + 31 - __clz(topw) >= 32 + 32 * N + 1) return round_general<N, W>(acc, lo - 32, sign, 0);
+        }
+    }
+    Dot2Terms<N> src{{p1, p2, e.m}, {2 * N, 2 * N, N}, {sc1, sc2, sce}, {s1, s2, e.s}};
+    return cluster_round<N, 8 * N + 4>(src, nullptr);
 }
 
 // ---------------------------------------------------------------- out-of-line forms

@@ -1,8 +1,8 @@
-// Batched small-matrix kernels: 4x4 complex LU solve/inverse/determinant (kernels.metal:210-249
-// sequence) and strided batched GEMM with ascending-k composed or fused updates
-// (batched_linalg.metal:16-17, 24-37, 145-157 sequence).  One thread per matrix / per output
-// entry; every arithmetic step is the correctly rounded device routine of lf_arith.cuh, so the
-// bits follow the same rounding sequence as the reference.
+// Batched small-matrix kernels: 4x4 complex LU solve/inverse/determinant (the rounding sequence of
+// kernels.metal:210-249) and strided batched GEMM with ascending-k composed or fused updates
+// (batched_linalg.metal:16-17, 24-37, 145-157 sequence).  Every arithmetic step is the correctly
+// rounded device routine of lf_arith.cuh, applied to the same operands in the same order as the
+// reference's sequence, so the bits are the same however the steps are spread over threads.
 #pragma once
 #include "lf_arith.cuh"
 #include <cuda_runtime.h>
@@ -14,8 +14,8 @@ struct Lu4Params {
     u64 count; unsigned rhs; int fused, want_det, inverse;
 };
 
-template <int N> __device__ __forceinline__ Cpx<N> c_minus(const Cpx<N>& c, const Cpx<N>& a, const Cpx<N>& b, bool fused) {
-    if (fused) { Cpx<N> r = cfms<N>(a, b, c); return {negate<N>(r.re), negate<N>(r.im)}; }   // -(a*b - c), one rounding each
+template <int N, bool FUSED> __device__ __forceinline__ Cpx<N> c_minus(const Cpx<N>& c, const Cpx<N>& a, const Cpx<N>& b) {
+    if constexpr (FUSED) { Cpx<N> r = cfms<N>(a, b, c); return {negate<N>(r.re), negate<N>(r.im)}; }   // -(a*b - c), one rounding each
     const Cpx<N> q = cmul<N>(a, b);
     return {subx<N>(c.re, q.re), subx<N>(c.im, q.im)};
 }
@@ -23,60 +23,97 @@ template <int N> __device__ __forceinline__ Num<N> mag_of(const Cpx<N>& z) {    
     return mag_cmp<N>(z.re, z.im) >= 0 ? z.re : z.im;
 }
 
-// One thread per system; a grid-stride loop, so any grid and block size (up to 256) covers the batch.
-template <int N> __device__ void lu4_system(const Lu4Params& p, u64 m);
-template <int N> __global__ void __launch_bounds__(256) lu4_kernel(Lu4Params p) {
-    for (u64 m = (u64)blockIdx.x * blockDim.x + threadIdx.x; m < p.count; m += (u64)gridDim.x * blockDim.x) lu4_system<N>(p, m);
-}
-template <int N> __device__ void lu4_system(const Lu4Params& p, u64 m) {
+// ---- 4x4 complex LU: one quad of lanes per system.
+// The quad parks its system in shared memory: the 16 matrix entries, then 4 solve values.  Lane r owns row r
+// of the elimination.  At step k every lane finds the same pivot (the row r >= k of largest max(|re|, |im|),
+// ties to the lowest row) by reading column k, lane c swaps column c of the two rows, and lane r > k forms its
+// multiplier l = a_rk / a_kk and updates a_rc -= l a_kc (c > k) from the pivot row.  The solves give lane i
+// row i of the right-hand side: forward, y_i -= a_it y_t in ascending t as each y_t becomes final; backward,
+// y_i -= a_it y_t (t = i+1..3, ascending) then y_i /= a_ii, row after row.  Lane 0 forms the determinant while
+// the other lanes start the forward pass.  A grid-stride loop over systems accepts any grid; the block size
+// must be a multiple of four.
+constexpr unsigned kLuLanes = 4;
+template <int N> constexpr u32 lu_quad_words() { return 20u * 2u * (N + 3); }
+template <int N> __device__ __forceinline__ Cpx<N> lu_get(const u32* q, unsigned idx) { return cload_plain<N>(q + idx * 2 * (N + 3)); }
+template <int N> __device__ __forceinline__ void lu_put(u32* q, unsigned idx, const Cpx<N>& z) { cstore<N>(q + idx * 2 * (N + 3), z); }
+
+template <int N, bool FUSED> __global__ void __launch_bounds__(256) lu4_kernel(Lu4Params p) {
     constexpr u64 CE = 2 * (N + 3);
-    Cpx<N> a[16];
-    for (int i = 0; i < 16; ++i) a[i] = cload<N>(p.A + (m * 16 + i) * CE);
-    unsigned perm[4] = {0, 1, 2, 3}, st = 0, swaps = 0;
-    for (unsigned k = 0; k < 4 && !st; ++k) {
-        unsigned piv = k;
-        for (unsigned r = k + 1; r < 4; ++r)
-            if (mag_cmp<N>(mag_of<N>(a[r * 4 + k]), mag_of<N>(a[piv * 4 + k])) > 0) piv = r;   // ties keep the lowest row
-        if (!a[piv * 4 + k].re.s && !a[piv * 4 + k].im.s) { st = k + 1; break; }
-        if (piv != k) {
-            for (unsigned c = 0; c < 4; ++c) { Cpx<N> t = a[k * 4 + c]; a[k * 4 + c] = a[piv * 4 + c]; a[piv * 4 + c] = t; }
-            unsigned t = perm[k]; perm[k] = perm[piv]; perm[piv] = t; ++swaps;
-        }
-        for (unsigned r = k + 1; r < 4; ++r) {
-            const Cpx<N> l = cdiv<N>(a[r * 4 + k], a[k * 4 + k]);
-            a[r * 4 + k] = l;
-            for (unsigned c = k + 1; c < 4; ++c) a[r * 4 + c] = c_minus<N>(a[r * 4 + c], l, a[k * 4 + c], p.fused);
-        }
-    }
-    p.status[m] = st;
+    extern __shared__ __align__(16) u32 lu_park[];
+    const unsigned lane = threadIdx.x & 3u;
+    u32* const q = lu_park + (threadIdx.x >> 2) * lu_quad_words<N>();
+    u32* const Y = q + 16 * CE;
+    const unsigned qmask = 0xFu << (threadIdx.x & 28u);
+    const u64 quads = ((u64)gridDim.x * blockDim.x) >> 2;
     const Cpx<N> z = {zero<N>(), zero<N>()};
-    if (p.want_det) {
-        Cpx<N> d = z;
-        if (!st) {
-            d = a[0];
-            for (int k = 1; k < 4; ++k) d = cmul<N>(d, a[k * 5]);
-            if (swaps & 1) d = {negate<N>(d.re), negate<N>(d.im)};
+    for (u64 m = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 2; m < p.count; m += quads) {
+        const u32* src = p.A + m * 16 * CE;                  // 16 contiguous entries, copied word by word
+        for (u32 w = lane; w < 16 * CE; w += kLuLanes) q[w] = __ldg(src + w);
+        __syncwarp(qmask);
+        unsigned perm = 0x03020100u, st = 0, swaps = 0;     // row of step i in byte i
+        for (unsigned k = 0; k < 4; ++k) {
+            unsigned piv = k;
+            for (unsigned r = k + 1; r < 4; ++r)
+                if (mag_cmp<N>(mag_of<N>(lu_get<N>(q, r * 4 + k)), mag_of<N>(lu_get<N>(q, piv * 4 + k))) > 0) piv = r;
+            const Cpx<N> pv = lu_get<N>(q, piv * 4 + k);
+            __syncwarp(qmask);                              // column k read by every lane before it moves
+            if (!pv.re.s && !pv.im.s) { st = k + 1; break; }
+            if (piv != k) {
+                const Cpx<N> x = lu_get<N>(q, k * 4 + lane), y = lu_get<N>(q, piv * 4 + lane);
+                lu_put<N>(q, k * 4 + lane, y);
+                lu_put<N>(q, piv * 4 + lane, x);
+                const unsigned a = (perm >> (8 * k)) & 0xffu, b = (perm >> (8 * piv)) & 0xffu;
+                perm ^= ((a ^ b) << (8 * k)) | ((a ^ b) << (8 * piv));
+                ++swaps;
+                __syncwarp(qmask);
+            }
+            if (lane > k) {
+                const Cpx<N> l = cdiv<N>(lu_get<N>(q, lane * 4 + k), lu_get<N>(q, k * 5));
+                lu_put<N>(q, lane * 4 + k, l);
+                for (unsigned c = k + 1; c < 4; ++c) lu_put<N>(q, lane * 4 + c, c_minus<N, FUSED>(lu_get<N>(q, lane * 4 + c), l, lu_get<N>(q, k * 4 + c)));
+            }
+            __syncwarp(qmask);
         }
-        cstore<N>(p.det + m * CE, d);
-    }
-    const unsigned R = p.inverse ? 4 : p.rhs;
-    for (unsigned j = 0; j < R; ++j) {
-        Cpx<N> y[4];
-        for (unsigned i = 0; i < 4; ++i) {
-            if (p.inverse) { y[i] = z; if (perm[i] == j) { y[i].re.m[N - 1] = 0x80000000u; y[i].re.s = 1; } }
-            else y[i] = cload<N>(p.B + ((m * 4 + perm[i]) * R + j) * CE);
+        if (lane == 0) {
+            p.status[m] = st;
+            if (p.want_det) {
+                Cpx<N> d = z;
+                if (!st) {
+                    d = lu_get<N>(q, 0);
+                    for (unsigned k = 1; k < 4; ++k) d = cmul<N>(d, lu_get<N>(q, k * 5));
+                    if (swaps & 1) d = {negate<N>(d.re), negate<N>(d.im)};
+                }
+                cstore<N>(p.det + m * CE, d);
+            }
         }
-        if (st) {
-            const Cpx<N> e = {zero<N>(kDivZero), zero<N>(kDivZero)};
-            for (unsigned i = 0; i < 4; ++i) cstore<N>(p.X + ((m * 4 + i) * R + j) * CE, e);
-            continue;
+        const unsigned R = p.inverse ? 4 : p.rhs;
+        for (unsigned j = 0; j < R; ++j) {
+            u32* xo = p.X + ((m * 4 + lane) * R + j) * CE;
+            if (st) { cstore<N>(xo, Cpx<N>{zero<N>(kDivZero), zero<N>(kDivZero)}); continue; }
+            Cpx<N> y;
+            const unsigned row = (perm >> (8 * lane)) & 0xffu;
+            if (p.inverse) { y = z; if (row == j) { y.re.m[N - 1] = 0x80000000u; y.re.s = 1; } }
+            else y = cload<N>(p.B + ((m * 4 + row) * R + j) * CE);
+            if (lane == 0) lu_put<N>(Y, 0, y);
+            __syncwarp(qmask);
+            for (unsigned t = 0; t < 3; ++t) {                // y_t is final after step t - 1
+                if (lane > t) {
+                    y = c_minus<N, FUSED>(y, lu_get<N>(q, lane * 4 + t), lu_get<N>(Y, t));
+                    if (lane == t + 1) lu_put<N>(Y, lane, y);
+                }
+                __syncwarp(qmask);
+            }
+            for (int i = 3; i >= 0; --i) {
+                if ((int)lane == i) {
+                    for (unsigned t = (unsigned)i + 1; t < 4; ++t) y = c_minus<N, FUSED>(y, lu_get<N>(q, i * 4 + t), lu_get<N>(Y, t));
+                    y = cdiv<N>(y, lu_get<N>(q, (unsigned)i * 5));
+                    lu_put<N>(Y, (unsigned)i, y);
+                }
+                __syncwarp(qmask);
+            }
+            cstore<N>(xo, y);
         }
-        for (unsigned i = 1; i < 4; ++i) for (unsigned t = 0; t < i; ++t) y[i] = c_minus<N>(y[i], a[i * 4 + t], y[t], p.fused);
-        for (int i = 3; i >= 0; --i) {
-            for (unsigned t = (unsigned)i + 1; t < 4; ++t) y[i] = c_minus<N>(y[i], a[i * 4 + t], y[t], p.fused);
-            y[i] = cdiv<N>(y[i], a[i * 5]);
-        }
-        for (unsigned i = 0; i < 4; ++i) cstore<N>(p.X + ((m * 4 + i) * R + j) * CE, y[i]);
+        __syncwarp(qmask);                                  // the parked system is read to the end before the next one
     }
 }
 
@@ -223,12 +260,19 @@ template <int N, bool CX, bool FUSED> __global__ void __launch_bounds__(256, (pa
     }
 }
 
-// Launchers.  grid == 0 asks for the number of resident blocks per SM at this block size instead.
-template <int N> int launch_lu4_n(const Lu4Params& p, unsigned grid, unsigned block, cudaStream_t s) {
-    if (!grid) { int b = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lu4_kernel<N>, (int)block, 0); return b; }
+// Launchers.  grid == 0 asks for the number of resident blocks per SM at this block size instead (0 when
+// the block's parked systems do not fit in shared memory; the LU launcher then refuses the launch too).
+template <int N, bool FUSED> int launch_lu4_v(const Lu4Params& p, unsigned grid, unsigned block, cudaStream_t s) {
+    const size_t smem = (size_t)(block / kLuLanes) * lu_quad_words<N>() * 4;
+    if (block % kLuLanes || smem > 227 * 1024) return grid ? 1 : 0;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(lu4_kernel<N, FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (!grid) { int b = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lu4_kernel<N, FUSED>, (int)block, smem); return b; }
     if (!p.count) return 0;
-    lu4_kernel<N><<<grid, block, 0, s>>>(p);
+    lu4_kernel<N, FUSED><<<grid, block, smem, s>>>(p);
     return 0;
+}
+template <int N> int launch_lu4_n(const Lu4Params& p, unsigned grid, unsigned block, cudaStream_t s) {
+    return p.fused ? launch_lu4_v<N, true>(p, grid, block, s) : launch_lu4_v<N, false>(p, grid, block, s);
 }
 template <int N, bool CX, bool FUSED> int launch_gemm_v(const GemmWork& p, unsigned grid, unsigned block, cudaStream_t s) {
     const size_t smem = parked_state<N, CX, FUSED>() ? (size_t)block * 2 * (N + 3) * 4 : 0;

@@ -1,6 +1,7 @@
 // C ABI of the batched small-matrix paths: Engine::lu4 / CommandBatch::lu4 (engine.hpp:164,208;
 // engine.mm:199-222,363-374,515-521) and BatchedLinalg::gemm host and resident forms
 // (batched_linalg.hpp:86,97; batched_linalg.mm:150-173), with the reference's validation rules.
+#include <algorithm>
 #include "lf_runtime.h"
 #include "lf_batched.cuh"
 
@@ -11,7 +12,9 @@ void launch_lu4(int bits, const lf_batched4& s, const void* A, const void* B, vo
     if (!s.count) return;
     lfd::Lu4Params p{static_cast<const uint32_t*>(A), static_cast<const uint32_t*>(B), static_cast<uint32_t*>(X),
                      static_cast<uint32_t*>(det), status, s.count, s.rhs, s.fused, s.determinant, s.inverse};
-    lfd::lu4_launcher(bits / 32)(p, (unsigned)((s.count + 63) / 64), 64, st);
+    const uint64_t lanes = (uint64_t)s.count * lfd::kLuLanes;           // one quad of lanes per system
+    if (lfd::lu4_launcher(bits / 32)(p, (unsigned)std::min<uint64_t>((lanes + 63) / 64, 1u << 30), 64, st))
+        throw runtime_error("lu4 launch: block does not fit");
     cuda_check(cudaGetLastError(), "lu4 launch");
 }
 void launch_strided_gemm(int bits, bool complex, const lf_strided_gemm& s, const void* A, const void* B, void* C,

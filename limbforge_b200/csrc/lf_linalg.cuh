@@ -67,47 +67,6 @@ struct DotParams {
 
 constexpr int kClusterWords = 192;   // 6144-bit exact window per cluster (pos/neg magnitudes)
 
-// acc (len words) += t << off; t has tw words; acc wide enough (caller checks)
-__device__ __forceinline__ void acc_add(u32* acc, int len, const u32* t, int tw, i64 off) {
-    const int ws = (int)(off >> 5), bs = (int)(off & 31);
-    u64 cy = 0;
-    int k = ws;
-    for (int q = 0; q <= tw && k < len; ++q, ++k) {
-        u32 v = q < tw ? t[q] << bs : 0u;
-        if (bs && q > 0) v |= t[q - 1] >> (32 - bs);
-        u64 s = (u64)acc[k] + v + cy; acc[k] = (u32)s; cy = s >> 32;
-    }
-    for (; cy && k < len; ++k) { u64 s = (u64)acc[k] + cy; acc[k] = (u32)s; cy = s >> 32; }
-}
-
-// Rounding record of a nonzero exact magnitude: N result words, exponent, round and sticky bits.
-template <int N> struct Rounded { u32 m[N]; i64 e; bool rb, sb; };
-template <int N> __device__ bool round_info(const u32* x, int len, i64 scale, Rounded<N>& r) {
-    int t = -1;
-    for (int k = len - 1; k >= 0; --k) if (x[k]) { t = k; break; }
-    if (t < 0) return false;
-    const int h = 32 * t + 31 - __clz(x[t]);
-    r.e = scale + h;
-    const int shift = h - (32 * N - 1);
-    for (int i = 0; i < N; ++i) {
-        const int p = shift + 32 * i;
-        u32 v = 0;
-        if (p <= -32) v = 0;
-        else if (p < 0) v = x[0] << (-p);
-        else { const int wi = p >> 5, bi = p & 31; v = wi < len ? x[wi] >> bi : 0u; if (bi && wi + 1 < len) v |= x[wi + 1] << (32 - bi); }
-        r.m[i] = v;
-    }
-    r.rb = false; r.sb = false;
-    if (shift > 0) {
-        const int rbp = shift - 1;
-        r.rb = (x[rbp >> 5] >> (rbp & 31)) & 1u;
-        bool st = (rbp & 31) && (x[rbp >> 5] & ((1u << (rbp & 31)) - 1u));
-        for (int k = 0; k < (rbp >> 5) && !st; ++k) st = x[k] != 0;
-        r.sb = st;
-    }
-    return true;
-}
-
 // RN(c -/+ sum_{k<K} x[k*sx] y[k*sy]) with one rounding, c == nullptr a zero addend: the contract
 // of exact_dot_add (linalg.hpp:268-318).  Statuses: zero carrying the OR of c's and every x[k],
 // y[k] status; no nonzero product returns c itself (or zero).  `error` is set when one cluster
@@ -122,15 +81,13 @@ template <int N, bool RO> __device__ __forceinline__ Num<N> ldn(const u32* p) {
     r.e = (int)ldw<RO>(p + N); r.s = (int)ldw<RO>(p + N + 1); r.st = ldw<RO>(p + N + 2);
     return r;
 }
-template <int N, bool RO = true> __device__ Num<N> exact_dot_add_dev(const u32* cp, bool subtract, const u32* x, i64 sx, const u32* y, i64 sy,
-                                                     u64 K, u32* error) {
-    constexpr i64 E = N + 3;
-    const Num<N> c = cp ? load_plain<N>(cp) : zero<N>();
-    u32 st = c.st;
-    for (u64 k = 0; k < K; ++k) st |= ldw<RO>(x + (i64)k * sx * E + N + 2) | ldw<RO>(y + (i64)k * sy * E + N + 2);
-    if (st) return zero<N>(st);
-    // term k < K: product x_k y_k (< 2^(scale+64N)); k == K: the addend (< 2^(scale+32N))
-    auto term = [&](u64 k, i64& scale, i64& top, int& sign) -> bool {
+// Terms of one output as a source for cluster_round: slot k < K is the product x_k y_k (top bound
+// scale + 64N), slot K the addend c (top scale + 32N).
+template <int N, bool RO> struct LineTerms {
+    const u32* x; i64 sx; const u32* y; i64 sy; u64 K; bool subtract; Num<N> c;
+    __device__ u64 count() const { return K + 1; }
+    __device__ bool term(u64 k, i64& scale, i64& top, int& sign) const {
+        constexpr i64 E = N + 3;
         if (k == K) {
             if (!c.s) return false;
             scale = (i64)c.e - (32 * N - 1); top = scale + 32 * N; sign = c.s;
@@ -143,74 +100,29 @@ template <int N, bool RO = true> __device__ Num<N> exact_dot_add_dev(const u32* 
         top = scale + 64 * N;
         sign = subtract ? -sa * sb : sa * sb;
         return true;
-    };
-    int count = 0, products = 0;
-    i64 T = INT64_MIN;
-    for (u64 k = 0; k <= K; ++k) {
-        i64 s, tp; int sg;
-        if (!term(k, s, tp, sg)) continue;
-        T = tp > T ? tp : T;
-        ++count; products += k < K;
     }
+    __device__ void add(u64 k, u32* acc, int len, i64 off) const {
+        constexpr i64 E = N + 3;
+        if (k == K) { acc_add(acc, len, c.m, N, off); return; }
+        const Num<N> a = ldn<N, RO>(x + (i64)k * sx * E), b = ldn<N, RO>(y + (i64)k * sy * E);
+        u32 prod[2 * N];
+        mant_mul<N>(a.m, b.m, prod);
+        acc_add(acc, len, prod, 2 * N, off);
+    }
+};
+template <int N, bool RO = true> __device__ Num<N> exact_dot_add_dev(const u32* cp, bool subtract, const u32* x, i64 sx, const u32* y, i64 sy,
+                                                     u64 K, u32* error) {
+    constexpr i64 E = N + 3;
+    const Num<N> c = cp ? load_plain<N>(cp) : zero<N>();
+    u32 st = c.st;
+    for (u64 k = 0; k < K; ++k) st |= ldw<RO>(x + (i64)k * sx * E + N + 2) | ldw<RO>(y + (i64)k * sy * E + N + 2);
+    if (st) return zero<N>(st);
+    bool products = false;
+    for (u64 k = 0; k < K && !products; ++k)
+        products = ldw<RO>(x + (i64)k * sx * E + N + 1) && ldw<RO>(y + (i64)k * sy * E + N + 1);
     if (!products) return cp ? c : zero<N>();
-    int logc = 0;
-    while ((1 << logc) < count + 1) ++logc;
-    const i64 gap = 32 * N + logc + 4;
-    u32 pos[kClusterWords], neg[kClusterWords];
-    i64 cutoff = T;                        // inclusive bound on the tops still to visit
-    bool have = false;
-    Rounded<N> R; int rsign = 0, sigma = 0;
-    for (;;) {
-        i64 Tc = INT64_MIN;                // top of the next cluster
-        for (u64 k = 0; k <= K; ++k) {
-            i64 s, tp; int sg;
-            if (term(k, s, tp, sg) && tp <= cutoff && tp > Tc) Tc = tp;
-        }
-        if (Tc == INT64_MIN) break;
-        i64 low = INT64_MAX;               // lowest bit: grow while a remaining term reaches within `gap`
-        for (u64 k = 0; k <= K; ++k) {
-            i64 s, tp; int sg;
-            if (term(k, s, tp, sg) && tp == Tc && s < low) low = s;
-        }
-        for (;;) {
-            i64 nl = low;
-            for (u64 k = 0; k <= K; ++k) {
-                i64 s, tp; int sg;
-                if (term(k, s, tp, sg) && tp <= cutoff && tp > low - gap && s < nl) nl = s;
-            }
-            if (nl == low) break;
-            low = nl;
-        }
-        const int len = (int)((Tc - low + logc + 2 + 31) / 32) + 1;
-        if (len > kClusterWords) { if (error) atomicExch(error, 1u); return zero<N>(kInvalid); }
-        for (int w = 0; w < len; ++w) { pos[w] = 0; neg[w] = 0; }
-        for (u64 k = 0; k <= K; ++k) {
-            i64 s, tp; int sg;
-            if (!term(k, s, tp, sg) || !(tp <= cutoff && tp > low - gap)) continue;
-            if (k == K) acc_add(sg > 0 ? pos : neg, len, c.m, N, s - low);
-            else {
-                const Num<N> a = ldn<N, RO>(x + (i64)k * sx * E), b = ldn<N, RO>(y + (i64)k * sy * E);
-                u32 prod[2 * N];
-                mant_mul<N>(a.m, b.m, prod);
-                acc_add(sg > 0 ? pos : neg, len, prod, 2 * N, s - low);
-            }
-        }
-        cutoff = low - gap;
-        int cmp = 0;
-        for (int w = len - 1; w >= 0 && !cmp; --w) if (pos[w] != neg[w]) cmp = pos[w] > neg[w] ? 1 : -1;
-        if (!cmp) continue;                // the cluster cancels exactly
-        u32* big = cmp > 0 ? pos : neg;
-        const u32* small = cmp > 0 ? neg : pos;
-        u32 bo = 0;
-        for (int w = 0; w < len; ++w) { u64 d = (u64)small[w] + bo; u32 o = big[w]; big[w] = (u32)((u64)o - d); bo = (u64)o < d; }
-        if (!have) { round_info<N>(big, len, low, R); rsign = cmp; have = true; continue; }
-        sigma = cmp == rsign ? 1 : -1;     // sign of everything below, relative to S
-        break;
-    }
-    if (!have) return zero<N>();
-    // RN(S + sigma * tiny): the tail decides only exact ties and exact S
-    const bool up = R.rb && (R.sb || sigma > 0 || (sigma == 0 && (R.m[0] & 1u)));
-    return finish<N>(R.m, R.e, rsign, up, 0);
+    const LineTerms<N, RO> src{x, sx, y, sy, K, subtract, c};
+    return cluster_round<N, kClusterWords>(src, error);
 }
 
 template <int N> __global__ void __launch_bounds__(128) exact_dot_kernel(DotParams p) {

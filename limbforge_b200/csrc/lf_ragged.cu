@@ -127,13 +127,16 @@ struct RaggedPlan {
     }
     void launch_lu(const void* arena, bool to_scratch, unsigned block, unsigned grid, cudaStream_t s) const {
         const lfd::Lu4Params p = lu_params(arena, to_scratch);
-        lfd::lu4_launcher(lu.bits / 32)(p, grid, block, s);
+        if (lfd::lu4_launcher(lu.bits / 32)(p, grid, block, s)) throw runtime_error("ragged lu4 launch: block does not fit");
         cuda_check(cudaGetLastError(), "ragged lu4 launch");
     }
+    // Grid of the LU job at `block` threads (a quad of lanes per system): one quad per system, or a
+    // persistent grid of resident blocks; 0 when the block's parked systems exceed shared memory.
     unsigned lu_grid_for(unsigned block, bool persistent) const {
-        if (!persistent) return (unsigned)((lu.shape.count + block - 1) / block);
         const int occ = lfd::lu4_launcher(lu.bits / 32)(lfd::Lu4Params{}, 0, block, nullptr);
-        return (unsigned)std::max(1, occ) * (unsigned)sms;
+        if (occ <= 0) return 0;
+        if (!persistent) return (unsigned)std::min<uint64_t>((lu.shape.count * lfd::kLuLanes + block - 1) / block, 1u << 30);
+        return (unsigned)occ * (unsigned)sms;
     }
 };
 
@@ -345,6 +348,7 @@ int lf_ragged_plan_tune(lf_ragged_plan* p, const void* arena) {
             for (unsigned b : kBlocks)
                 for (int persistent = 0; persistent < 2; ++persistent) {
                     const unsigned grid = p->lu_grid_for(b, persistent != 0);
+                    if (!grid) continue;
                     const double ms = timed([&] { p->launch_lu(arena, true, b, grid, s); });
                     if (ms < best) { best = ms; p->lu_block = b; p->lu_grid = grid; }
                 }

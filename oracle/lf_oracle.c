@@ -667,3 +667,44 @@ int lfo_tree_sum(int bits, int complex_, const word* in, size_t count, word* out
     free(cur);
     return 0;
 }
+
+/* ---------------------------------------------------------------- segmented dots and recurrences
+ * Segmented dot (kernels.metal:195-207): out[i] = the chain s <- fma(a[i*len+k], b[..], s) from s = 0 (cfma for
+ * complex), b[k] when shared.  Recurrence (kernels.metal:39-58): four-value complex rings, each step
+ * q = cadd(..cadd(cadd(0, cmul(w0, q0)), cmul(w1, q1)).., cmul(w3, q3)), then the ring shifts. */
+int lfo_segmented_dot(int bits, int complex_, size_t segments, size_t length, int shared, const word* a, const word* b, word* out) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3, S = complex_ ? 2 * E : E;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (size_t i = 0; i < segments; ++i) {
+        word s[70], t[70];
+        memset(s, 0, sizeof s);
+        for (size_t k = 0; k < length; ++k) {
+            const word* x = a + (i * length + k) * S; const word* y = b + (shared ? k : i * length + k) * S;
+            if (complex_) lfo_cfma(n, x, y, s, 0, t); else lfo_fma(n, x, y, s, 0, t);
+            memcpy(s, t, sizeof(word) * S);
+        }
+        memcpy(out + i * S, s, sizeof(word) * S);
+    }
+    return 0;
+}
+int lfo_recurrence(int bits, const word* seeds, const word* weights, word* out, size_t count, unsigned steps, unsigned spw) {
+    const int n = bits / 32; const size_t S = 2 * ((size_t)n + 3);
+    const size_t G = count / spw;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (size_t i = 0; i < count; ++i) {
+        word q[4][70], sum[70], p[70], t[70];
+        for (int j = 0; j < 4; ++j) memcpy(q[j], seeds + ((size_t)j * count + i) * S, sizeof(word) * S);
+        for (unsigned st = 0; st < steps; ++st) {
+            memset(sum, 0, sizeof sum);
+            for (int j = 0; j < 4; ++j) {
+                lfo_cmul(n, weights + (((size_t)st * 4 + (size_t)j) * G + i / spw) * S, q[j], p);
+                lfo_cadd(n, sum, p, t);
+                memcpy(sum, t, sizeof(word) * S);
+            }
+            memcpy(q[0], q[1], sizeof q[0]); memcpy(q[1], q[2], sizeof q[1]); memcpy(q[2], q[3], sizeof q[2]);
+            memcpy(q[3], sum, sizeof(word) * S);
+        }
+        memcpy(out + i * S, q[3], sizeof(word) * S);
+    }
+    return 0;
+}

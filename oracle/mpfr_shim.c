@@ -184,3 +184,57 @@ int mpo_cast(int from_bits, int to_bits, const word* in, word* out, size_t count
     mpfr_clear(&x); mpfr_clear(&r);
     return 0;
 }
+
+/* ---------------------------------------------------------------- CPU baseline: MPFR multiplication chains
+ * The reference's benchmark method (benchmarks/benchmark.cpp:3-94, benchmark_support.hpp:12-45): values and
+ * factors are converted once into preallocated mpfr_t arrays, outside the timed region; a pass computes
+ * r_i <- x_i, then r_i <- RN(r_i * f_{s,i}) for s = 0..steps-1, for every value, serially (threads = 1) or on a
+ * persistent pool of `threads` workers (OpenMP), each taking one contiguous chunk.  mpo_chain_run returns the
+ * pass's wall time in seconds (CLOCK_MONOTONIC); mpo_chain_result converts the last pass's values back to the
+ * limb layout so they can be compared bit for bit. */
+#include <time.h>
+#include <omp.h>
+typedef struct { int bits; size_t steps, count; mpfr_struct *x, *f, *r; } mpo_chain;
+
+void* mpo_chain_setup(int bits, const word* x, const word* f, size_t steps, size_t count) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3; widen_range();
+    mpo_chain* c = (mpo_chain*)calloc(1, sizeof(mpo_chain));
+    c->bits = bits; c->steps = steps; c->count = count;
+    c->x = (mpfr_struct*)malloc(sizeof(mpfr_struct) * count);
+    c->r = (mpfr_struct*)malloc(sizeof(mpfr_struct) * count);
+    c->f = (mpfr_struct*)malloc(sizeof(mpfr_struct) * count * steps);
+    for (size_t i = 0; i < count; ++i) {
+        mpfr_init2(&c->x[i], bits); mpfr_init2(&c->r[i], bits);
+        to_mp(&c->x[i], x + i * E, n);
+    }
+    for (size_t k = 0; k < steps * count; ++k) { mpfr_init2(&c->f[k], bits); to_mp(&c->f[k], f + k * E, n); }
+    return c;
+}
+double mpo_chain_run(void* h, int threads) {
+    mpo_chain* c = (mpo_chain*)h;
+    struct timespec t0, t1;
+    clock_gettime(CLOCK_MONOTONIC, &t0);
+#pragma omp parallel num_threads(threads)
+    {
+        widen_range();
+        const size_t nt = (size_t)omp_get_num_threads(), id = (size_t)omp_get_thread_num();
+        const size_t lo = c->count * id / nt, hi = c->count * (id + 1) / nt;
+        for (size_t i = lo; i < hi; ++i) {
+            mpfr_set(&c->r[i], &c->x[i], RNDN);
+            for (size_t s = 0; s < c->steps; ++s) mpfr_mul(&c->r[i], &c->r[i], &c->f[s * c->count + i], RNDN);
+        }
+    }
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    return (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
+}
+void mpo_chain_result(void* h, word* out) {
+    mpo_chain* c = (mpo_chain*)h;
+    const int n = c->bits / 32;
+    for (size_t i = 0; i < c->count; ++i) from_mp(out + i * ((size_t)n + 3), &c->r[i], n);
+}
+void mpo_chain_free(void* h) {
+    mpo_chain* c = (mpo_chain*)h;
+    for (size_t i = 0; i < c->count; ++i) { mpfr_clear(&c->x[i]); mpfr_clear(&c->r[i]); }
+    for (size_t k = 0; k < c->steps * c->count; ++k) mpfr_clear(&c->f[k]);
+    free(c->x); free(c->r); free(c->f); free(c);
+}

@@ -66,6 +66,8 @@ class Oracle:
         lib.lfo_dot2_add.argtypes = [I, V, V, V, V, V, V]
         lib.lfo_cast.argtypes = [I, I, I, V, V, S]
         lib.lfo_tree_sum.argtypes = [I, I, V, S, V]
+        lib.lfo_segmented_dot.argtypes = [I, I, S, S, I, V, V, V]
+        lib.lfo_recurrence.argtypes = [I, V, V, V, S, C.c_uint, C.c_uint]
         self.lib = lib
 
     def elementwise(self, bits, op, a, b=None, c=None, b_index=(1, 0), c_index=(1, 0)):
@@ -143,6 +145,19 @@ class Oracle:
         return out
 
 
+    def segmented_dot(self, bits, complex_, segments, length, shared, a, b):
+        n = bits // 32
+        out = np.zeros((segments, 2, n + 3) if complex_ else (segments, n + 3), dtype=np.uint32)
+        assert self.lib.lfo_segmented_dot(bits, int(complex_), segments, length, int(shared), _ptr(a), _ptr(b), _ptr(out)) == 0
+        return out
+
+    def recurrence(self, bits, seeds, weights, count, steps, states_per_weight=1):
+        n = bits // 32
+        out = np.zeros((count, 2, n + 3), dtype=np.uint32)
+        assert self.lib.lfo_recurrence(bits, _ptr(seeds), _ptr(weights), _ptr(out), count, steps, states_per_weight) == 0
+        return out
+
+
 class Reference:
     """The reference's own CPU arithmetic (core.hpp, exact_dot_add) built into oracle/_ref."""
 
@@ -188,7 +203,31 @@ class Mpfr:
         lib.mpo_dot.argtypes = [I, V, I, V, L, V, L, S, V]
         lib.mpo_dot2_add.argtypes = [I, V, V, V, V, V, V, S]
         lib.mpo_cast.argtypes = [I, I, V, V, S]
+        lib.mpo_chain_setup.argtypes = [I, V, V, S, S]
+        lib.mpo_chain_setup.restype = V
+        lib.mpo_chain_run.argtypes = [V, I]
+        lib.mpo_chain_run.restype = C.c_double
+        lib.mpo_chain_result.argtypes = [V, V]
+        lib.mpo_chain_free.argtypes = [V]
         self.lib = lib
+
+    def chain_baseline(self, bits, x, factors, threads_list, warmup=2, samples=9):
+        """The MPFR chain baseline (benchmarks/benchmark.cpp method): median pass seconds for each thread
+        count in threads_list (passes of the counts alternate, as the reference alternates serial and
+        parallel runs), and the result values of the last pass."""
+        h = self.lib.mpo_chain_setup(bits, _ptr(x), _ptr(factors), factors.shape[0], x.shape[0])
+        try:
+            times = {t: [] for t in threads_list}
+            for i in range(warmup + samples):
+                for t in threads_list:
+                    s = self.lib.mpo_chain_run(h, t)
+                    if i >= warmup:
+                        times[t].append(s)
+            out = np.zeros_like(x)
+            self.lib.mpo_chain_result(h, _ptr(out))
+        finally:
+            self.lib.mpo_chain_free(h)
+        return {t: float(np.median(v)) for t, v in times.items()}, out
 
     def cast(self, from_bits, to_bits, x):
         """Real components x [count, N+3] at from_bits, rounded to to_bits."""

@@ -247,3 +247,34 @@ def test_cholesky_in_place_and_empty(la, oracle):
     assert same(M, WL)
     info = la.cholesky(bits, np.zeros((1, 11), np.uint32), 0, np.zeros((1, 11), np.uint32))
     assert info.pivot == 0
+
+
+def uniform_pm1(rng, bits, count):
+    """Entries uniform in [-1, 1] at full precision: random sign and significand, exponent -g with g geometric."""
+    x = nb.random_numbers(rng, count, bits, 0)
+    x[:, bits // 32] = (-rng.geometric(0.5, size=count)).astype(np.int32).view(np.uint32)
+    return x
+
+
+def test_cholesky_512_blocked_full_factor(engine, la, oracle):
+    """The benchmark's construction at n = 512 (A = RN(G^T G) + n I, G uniform in [-1, 1], 256 bits, block 32):
+    every entry of the factor and of an 8-RHS solve against the oracle.  Fifteen trailing updates of the
+    residue engine (K = 32) run between the panels."""
+    from limbforge_b200.api import FactorOptions, Operation
+    bits, n, nrhs = 256, 512, 8
+    rng = np.random.default_rng(2048)
+    G = uniform_pm1(rng, bits, n * n)
+    A = np.zeros_like(G)
+    la.syrk(bits, G, n, n, A, lower_only=False)
+    assert same(A[:3 * n], oracle.syrk(bits, G, n, n, lower_only=False, lines=(0, 3))[:3 * n])
+    diag = np.ascontiguousarray(A[np.arange(n) * (n + 1)])
+    A[np.arange(n) * (n + 1)] = engine.run(bits, Operation.add, diag, nb.power(bits, 9, count=n))[0]
+    L = np.zeros_like(A)
+    info = la.cholesky(bits, A, n, L, FactorOptions(block=32))
+    WL, winfo = oracle.cholesky(bits, A, n, 32)
+    assert (info.pivot, info.pivot_sign, info.pivot_status) == winfo == (n, 0, 0)
+    assert same(L, WL), f"factor rows {bad(L, WL)}"
+    B = uniform_pm1(rng, bits, n * nrhs)
+    X = np.zeros_like(B)
+    la.cholesky_solve(bits, L, n, B, nrhs, X, FactorOptions(block=32))
+    assert same(X, oracle.solve(bits, L, n, B, nrhs, 32, 3))

@@ -327,3 +327,56 @@ def test_strided_gemm_oracle_vs_mpfr_replay(oracle):
                     z = cx(bits, 4, z, cx(bits, 5, A[t * 15 + i * 5 + k], B[k * 4 + j]))
                 assert same(got[t * 14 + i * 4 + j], nb.negate(z)), (t, i, j)
     assert same(got[12:14], C0[12:14])               # padding between outputs kept
+
+
+@pytest.mark.parametrize("bits", [64, 128, 256, 480, 1024])
+def test_oracle_fused_three_term_cases(oracle, bits):
+    """Adversarial cfma operands (tests/fused_cases.py): the oracle agrees with an MPFR sum of the two
+    exact products and the addend rounded once per component, and with the reference build."""
+    from fused_cases import dot2_cases
+    rng = np.random.default_rng(4242 + bits)
+    a, b, c = dot2_cases(rng, bits, 160)
+    got = oracle.elementwise(bits, 11, a, b, c)
+    mp = _mp()
+    re = lambda z: np.ascontiguousarray(z[:, 0])
+    im = lambda z: np.ascontiguousarray(z[:, 1])
+    want_re = mp.dot2_add(bits, re(a), re(b), np.ascontiguousarray(nb.negate(im(a))), im(b), re(c))
+    want_im = mp.dot2_add(bits, re(a), im(b), im(a), re(b), im(c))
+    assert same(np.ascontiguousarray(got[:, 0]), want_re), "re vs MPFR"
+    assert same(np.ascontiguousarray(got[:, 1]), want_im), "im vs MPFR"
+    if Reference.available():
+        assert same(got, Reference().elementwise(bits, 11, a, b, c)), "vs reference build"
+
+
+@pytest.mark.skipif(not Reference.available(), reason="reference build (oracle/_ref) absent")
+@pytest.mark.parametrize("bits", [96, 256, 640])
+def test_sequence_oracles_vs_reference_build(oracle, bits):
+    """Segmented dots and recurrences of the oracle equal the same chains stepped with the reference's own
+    fma / cfma / cmul / cadd (its core.hpp, built from its sources)."""
+    ref = Reference()
+    rng = np.random.default_rng(bits + 77)
+    seg, ln = 12, 9
+    for cx in (False, True):
+        make = (lambda c: nb.random_complex(rng, c, bits, 30)) if cx else (lambda c: nb.random_numbers(rng, c, bits, 30, sparse_frac=0.1))
+        a, b = make(seg * ln), make(seg * ln)
+        for shared in (False, True):
+            got = oracle.segmented_dot(bits, cx, seg, ln, shared, a, b)
+            s = np.zeros_like(got)
+            for k in range(ln):
+                x = np.ascontiguousarray(a.reshape(seg, ln, *a.shape[1:])[:, k])
+                y = np.ascontiguousarray(np.broadcast_to(b[k], x.shape) if shared else b.reshape(seg, ln, *b.shape[1:])[:, k])
+                s = ref.elementwise(bits, 11 if cx else 9, x, y, np.ascontiguousarray(s))
+            assert same(got, s), f"segmented dot complex={cx} shared={shared}"
+    count, steps, spw = 16, 5, 2
+    seeds = nb.random_complex(rng, 4 * count, bits, 3)
+    weights = nb.random_complex(rng, steps * 4 * (count // spw), bits, 2)
+    got = oracle.recurrence(bits, seeds, weights, count, steps, spw)
+    q = [np.ascontiguousarray(seeds[j * count:(j + 1) * count]) for j in range(4)]
+    G = count // spw
+    for t in range(steps):
+        s = np.zeros_like(q[0])
+        for j in range(4):
+            w = np.ascontiguousarray(weights[(t * 4 + j) * G:(t * 4 + j + 1) * G][np.arange(count) // spw])
+            s = ref.elementwise(bits, 4, s, ref.elementwise(bits, 5, w, q[j]))
+        q = q[1:] + [s]
+    assert same(got, q[3]), "recurrence"

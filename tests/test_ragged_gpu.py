@@ -15,9 +15,9 @@ from limbforge_b200 import numbers as nb
 pytestmark = pytest.mark.gpu
 
 
-def make_case(rng, count, bits_choices, max_dim, complex_=True, lu_count=0, zero_dims=True):
+def make_case(rng, count, bits_choices, max_dim, complex_=True, lu_count=0, zero_dims=True, min_dim=None):
     bits = rng.choice(bits_choices, size=count)
-    lo = 0 if zero_dims else 1
+    lo = (0 if zero_dims else 1) if min_dim is None else min_dim
     m, n, k = (rng.integers(lo, max_dim + 1, size=count) for _ in range(3))
     acc = rng.integers(0, 2, size=count)
     neg = rng.integers(0, 2, size=count)
@@ -95,6 +95,21 @@ def test_ragged_complex_batch_with_lu_vs_oracle(engine, oracle, fused):
     info = plan.info()
     assert {c["bits"] for c in info["classes"]} == {int(b) for b, m, n in zip(items["bits"], items["m"], items["n"]) if m * n}
     assert sum(c["items"] for c in info["classes"]) == int(np.count_nonzero(items["m"] * items["n"]))
+
+
+@pytest.mark.parametrize("fused", [False, True])
+def test_ragged_benchmark_shapes_vs_oracle(engine, oracle, fused):
+    """The benchmark's shape distribution: m, n, k uniform in {4..48}, precision uniform over
+    {128, 256, 512, 1024} bits, with 1,200 LU systems at 512 bits in the same tuned plan; every output
+    word is compared (the 1024-bit class runs its parked-state kernel at k up to 48)."""
+    rng = np.random.default_rng(48 + fused)
+    items, lu, arena = make_case(rng, 240, [128, 256, 512, 1024], 48, lu_count=1200, min_dim=4)
+    plan = api.RaggedPlan(engine, True, fused, items, arena.size * 4, lu)
+    got = run_plan(engine, plan, arena, tune=True)
+    want = expected(oracle, items, lu, arena, True, fused)
+    bad = np.nonzero(got != want)[0]
+    assert bad.size == 0, f"first differing word {bad[:5]}"
+    assert {c["bits"] for c in plan.info()["classes"]} == {128, 256, 512, 1024}
 
 
 def test_ragged_tuned_equals_untuned_and_arena_is_kept(engine, oracle):
