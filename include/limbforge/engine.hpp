@@ -7,10 +7,12 @@
 #include "../limbforge_b200.h"
 #include <cstddef>
 #include <cstdint>
+#include <future>
 #include <memory>
 #include <stdexcept>
 #include <string>
 #include <utility>
+#include <vector>
 
 namespace limbforge {
 enum class Operation { add, sub, mul, div, complex_add, complex_mul, complex_div, square, sqrt, fma, fms, complex_fma, complex_fms };
@@ -27,6 +29,29 @@ inline std::size_t broadcast_elements(std::size_t count, Broadcast b) {
 }
 struct EngineOptions { unsigned threads_per_threadgroup = 0; bool cooperative_reductions = true; bool cooperative_recurrence = true; };
 struct Batched4 { std::size_t count = 0; unsigned rhs = 0; bool inverse = false, determinant = false, fused = false; };
+struct PipelineInfo { unsigned simd_width, max_threads, threads_per_threadgroup; };
+// Segmented dot products: out[i] = sum_{k<length} a[i*length+k] * b[i*length+k] (or b[k] when shared_right),
+// as the sequential fma / cfma chain from k = 0.
+struct SegmentedDot { std::size_t segments = 0, length = 0; bool shared_right = false; };
+// Shape of Engine::vector_recurrence (the reference's engine.hpp:37-49); that entry point is declared for source
+// compatibility and is not provided by this library (it throws std::runtime_error).
+struct VectorRecurrence {
+    std::size_t lanes = 0; unsigned steps = 0;
+    unsigned lanes_per_weight = 1;
+    bool affine = false, matrix = false, all_steps = false, reverse = false, tangent = false;
+    unsigned lanes_per_base = 1, lanes_per_tangent = 1;
+    bool fused = false;
+};
+// Kernels to prepare ahead of use (Engine::prewarm).  The kernels are compiled ahead for sm_100a; a prewarm
+// validates the widths and operations and loads the element-wise kernels of `operations` for every width.
+struct Prewarm {
+    std::vector<int> bits;
+    std::vector<Operation> operations;
+    bool recurrence = false, reductions = false;
+    std::vector<VectorRecurrence> vector_shapes;
+    std::vector<SegmentedDot> real_dots, complex_dots;
+    std::vector<Batched4> lu4;
+};
 
 namespace detail {
 inline void check(int rc) {
@@ -148,6 +173,19 @@ public:
         detail::check(lf_batch_cast(open(), detail::Format<From>::bits, detail::Format<To>::bits, detail::Format<To>::complex,
                                     in.handle(), out.handle(), in.size()));
     }
+    template <class T> void segmented_dot(const SegmentedDot& shape, const Buffer<T>& a, const Buffer<T>& b, Buffer<T>& out) {
+        static_assert(detail::Format<T>::bits, "segmented dots use arithmetic buffers");
+        lf_segmented_dot d{shape.segments, shape.length, shape.shared_right};
+        detail::check(lf_batch_segmented_dot(open(), detail::Format<T>::bits, detail::Format<T>::complex, &d, a.handle(), b.handle(),
+                                             out.handle()));
+    }
+    // Declared for source compatibility with the reference; not provided by this library.
+    template <class T> void vector_recurrence(const VectorRecurrence&, const Buffer<T>&, const Buffer<T>&, const Buffer<T>&, const Buffer<T>&,
+                                              Buffer<T>&, const Buffer<T>& = Buffer<T>(), const Buffer<T>& = Buffer<T>(),
+                                              const Buffer<T>& = Buffer<T>()) {
+        static_assert(detail::Format<T>::complex, "vector recurrences use complex buffers");
+        throw std::runtime_error("vector_recurrence is not provided by this library");
+    }
     template <class T> void tree_sum(const Buffer<T>& input, Buffer<T>& out) {
         if (out.size() != 1) throw std::invalid_argument("tree_sum output must contain one element");
         detail::check(lf_batch_tree_sum(open(), detail::Format<T>::bits, detail::Format<T>::complex, input.handle(), out.handle(),
@@ -176,6 +214,36 @@ public:
     Engine& operator=(const Engine&) = delete;
     lf_engine* handle() const { return e_.get(); }
     std::string device_name() const { char b[256]; detail::check(lf_engine_device_name(e_.get(), b, sizeof b)); return b; }
+    // Validates the request and loads the element-wise kernels it names; the other fields need no preparation.
+    void prewarm(const Prewarm& request) {
+        std::vector<int> ops;
+        for (Operation op : request.operations) ops.push_back(int(op));
+        detail::check(lf_engine_prewarm(e_.get(), request.bits.data(), request.bits.size(), ops.data(), ops.size()));
+    }
+    // The same on a background thread; errors surface from the future.
+    std::future<void> prewarm_async(Prewarm request) {
+        return std::async(std::launch::async, [this, r = std::move(request)]() { prewarm(r); });
+    }
+    PipelineInfo pipeline_info(int bits, Operation op) {
+        PipelineInfo p{};
+        detail::check(lf_engine_pipeline_info(e_.get(), bits, int(op), &p.simd_width, &p.max_threads, &p.threads_per_threadgroup));
+        return p;
+    }
+    Timing segmented_dot(int bits, bool complex, const SegmentedDot& shape, const void* a, const void* b, void* out) {
+        lf_segmented_dot d{shape.segments, shape.length, shape.shared_right};
+        lf_timing t{}; detail::check(lf_engine_segmented_dot(e_.get(), bits, complex, &d, a, b, out, &t)); return detail::timing(t);
+    }
+    Timing recurrence(int bits, const void* seeds, const void* weights, void* out, std::size_t count, unsigned steps,
+                      unsigned states_per_weight = 1) {
+        lf_timing t{};
+        detail::check(lf_engine_recurrence(e_.get(), bits, seeds, weights, out, count, steps, states_per_weight, &t));
+        return detail::timing(t);
+    }
+    // Declared for source compatibility with the reference; not provided by this library.
+    Timing vector_recurrence(int, const VectorRecurrence&, const void*, const void*, const void*, const void*, void*,
+                             const void* = nullptr, const void* = nullptr, const void* = nullptr) {
+        throw std::runtime_error("vector_recurrence is not provided by this library");
+    }
     template <class T> Buffer<T> make_buffer(std::size_t count) {
         static_assert(!detail::Format<T>::bits || sizeof(T) == std::size_t(detail::Format<T>::bits / 8 + 12) * (detail::Format<T>::complex ? 2 : 1),
                       "buffer layout mismatch");

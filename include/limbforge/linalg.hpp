@@ -3,6 +3,8 @@
 // products with one rounding per output, blocked Cholesky and multi-RHS triangular solves, as
 // inline wrappers over the C ABI.  Every product runs on the GPU.
 #include "engine.hpp"
+#include <cstring>
+#include <future>
 #include <vector>
 
 namespace limbforge {
@@ -20,11 +22,44 @@ struct CholeskyInfo {
 };
 // Device memory a Linalg retains between calls (linalg.hpp:46-52), in bytes.
 struct LinalgWorkspaces { std::size_t scratch_bytes = 0, idle_bytes = 0, busy_bytes = 0, busy_workspaces = 0; };
-struct LinalgReport {
-    std::size_t m = 0, n = 0, k = 0, gpu_outputs = 0, trivial_outputs = 0, gemm_rows = 0, gemm_cols = 0, int8_gemms = 0, moduli = 0, band_bits = 0;
-    double analysis_seconds = 0, gpu_seconds = 0;
-    int method = 0;
+// Kernels to prepare ahead of use (Linalg::prewarm); the widths and inner sizes are validated.
+struct LinalgPrewarm {
+    std::vector<int> bits;
+    std::vector<std::size_t> inner_sizes;
+    bool resident = false;
 };
+struct LinalgPair { unsigned left_band, right_band, rows, cols, moduli; };
+// Diagnostics of the last call (the reference's fields, filled from the GPU analysis: every nonzero, status-free
+// line is one band of the residue engine here, so left_bands[1] / right_bands[1] count them and left_bands[0] /
+// right_bands[0] the zero or status lines; outputs the reference sends to its host fallback run on the GPU, so
+// the *_fallback counts are 0), and the engine used here.
+struct LinalgReport {
+    std::size_t m = 0, n = 0, k = 0;
+    std::vector<std::size_t> left_bands, right_bands;
+    std::size_t left_fallback = 0, right_fallback = 0;
+    std::size_t gpu_outputs = 0, multi_band_outputs = 0, fallback_outputs = 0, trivial_outputs = 0;
+    std::vector<LinalgPair> pairs;
+    std::size_t gemm_rows = 0, gemm_cols = 0, int8_gemms = 0;
+    bool zero_copy_output = false;
+    bool resident_overflow = false;
+    double analysis_seconds = 0, upload_seconds = 0, gpu_seconds = 0, assembly_seconds = 0, fallback_seconds = 0;
+    std::size_t moduli = 0, band_bits = 0;
+    int method = 0;   // 1 generic limb kernel, 2 int8 residue engine
+};
+namespace detail {
+inline LinalgReport report_of(const lf_linalg_report& c) {
+    LinalgReport r;
+    r.m = c.m; r.n = c.n; r.k = c.k;
+    r.gpu_outputs = c.gpu_outputs; r.trivial_outputs = c.trivial_outputs;
+    r.gemm_rows = c.gemm_rows; r.gemm_cols = c.gemm_cols; r.int8_gemms = c.int8_gemms;
+    r.moduli = c.moduli; r.band_bits = c.band_bits; r.method = c.method;
+    r.analysis_seconds = c.analysis_seconds; r.gpu_seconds = c.gpu_seconds;
+    r.left_bands = {c.left_zero_lines, c.left_lines};
+    r.right_bands = {c.right_zero_lines, c.right_lines};
+    if (c.method == 2) r.pairs.push_back({1, 1, (unsigned)c.gemm_rows, (unsigned)c.gemm_cols, (unsigned)c.moduli});
+    return r;
+}
+}  // namespace detail
 
 // Handle of a resident product (linalg.hpp:60-66): C is final after the batch's Submission::wait().
 class LinalgTicket {
@@ -39,8 +74,7 @@ public:
     const LinalgReport& report() const {
         lf_linalg_report c{};
         detail::check(lf_linalg_ticket_report(t_.get(), &c));
-        r_ = {c.m, c.n, c.k, c.gpu_outputs, c.trivial_outputs, c.gemm_rows, c.gemm_cols, c.int8_gemms, c.moduli, c.band_bits,
-              c.analysis_seconds, c.gpu_seconds, c.method};
+        r_ = detail::report_of(c);
         return r_;
     }
     // Later operations of the batch read C in stream order after the product, so no read is provisional.
@@ -54,6 +88,14 @@ class Linalg {
     LinalgOptions o_;
     mutable LinalgReport r_;
     static lf_factor_options fo(const FactorOptions& o) { return {o.block, o.host_macs, o.solve_host_macs, o.gpu}; }
+    template <class T> Timing solve_buffers(int passes, const Buffer<T>& L, std::size_t n, const Buffer<T>& B, std::size_t nrhs, Buffer<T>& X,
+                                            const FactorOptions& options) {
+        static_assert(detail::Format<T>::bits && !detail::Format<T>::complex, "dense linear algebra uses real Float<bits> buffers");
+        lf_factor_options o = fo(options);
+        lf_timing t{};
+        detail::check(lf_linalg_solve_buffers(l_.get(), detail::Format<T>::bits, passes, L.handle(), n, B.handle(), nrhs, X.handle(), &o, &t));
+        return detail::timing(t);
+    }
     void make(lf_engine* e, LinalgOptions o) {
         o_ = o;
         lf_linalg_options c{o.band_bits, o.max_bands, o.max_spread, o.host_threads, o.force_fallback, o.resident_bands, o.method};
@@ -67,11 +109,23 @@ public:
     Linalg(const Linalg&) = delete;
     Linalg& operator=(const Linalg&) = delete;
     const LinalgOptions& options() const { return o_; }
+    // The kernels are compiled ahead for sm_100a; a prewarm validates the widths and inner sizes.
+    void prewarm(const LinalgPrewarm& request) {
+        for (int b : request.bits)
+            if (b < 64 || b > 1024 || b % 32) throw std::invalid_argument("bits must be a multiple of 32 in [64,1024]");
+        for (std::size_t k : request.inner_sizes)
+            if (k > 65472) throw std::invalid_argument("resident inner size above 65472");
+    }
+    std::future<void> prewarm_async(LinalgPrewarm request) {
+        return std::async(std::launch::async, [this, r = std::move(request)]() { prewarm(r); });
+    }
+    std::string device_name() const {
+        char b[256]; detail::check(lf_linalg_device_name(l_.get(), b, sizeof b)); return b;
+    }
     const LinalgReport& report() const {
         lf_linalg_report c{};
         detail::check(lf_linalg_get_report(l_.get(), &c));
-        r_ = {c.m, c.n, c.k, c.gpu_outputs, c.trivial_outputs, c.gemm_rows, c.gemm_cols, c.int8_gemms, c.moduli, c.band_bits,
-              c.analysis_seconds, c.gpu_seconds, c.method};
+        r_ = detail::report_of(c);
         return r_;
     }
     // Retained memory and its release (linalg.hpp:173-180): scratch and idle resident workspaces are freed now,
@@ -107,6 +161,31 @@ public:
         lf_factor_options o = fo(options);
         lf_timing t{}; detail::check(lf_linalg_cholesky_solve(l_.get(), bits, L, n, B, nrhs, X, &o, &t)); return detail::timing(t);
     }
+    // Factorization and solves on Buffer operands of the Linalg's engine (linalg.hpp:194-199): synchronous, outside any
+    // batch, the buffers used in place; they must be idle (logic_error otherwise).  Same bits as the host-array calls.
+    template <class T> CholeskyInfo cholesky(const Buffer<T>& A, std::size_t n, Buffer<T>& L, const FactorOptions& options = {}) {
+        static_assert(detail::Format<T>::bits && !detail::Format<T>::complex, "dense linear algebra uses real Float<bits> buffers");
+        lf_factor_options o = fo(options);
+        lf_cholesky_info i{};
+        detail::check(lf_linalg_cholesky_buffers(l_.get(), detail::Format<T>::bits, A.handle(), n, L.handle(), &o, &i));
+        return {i.pivot, i.pivot_sign, i.pivot_status, detail::timing(i.timing), i.blocks, i.gpu_updates, i.host_updates,
+                i.panel_seconds, i.update_seconds};
+    }
+    template <class T> Timing trsm(bool transpose, const Buffer<T>& L, std::size_t n, const Buffer<T>& B, std::size_t nrhs, Buffer<T>& X,
+                                   const FactorOptions& options = {}) {
+        return solve_buffers<T>(transpose ? 2 : 1, L, n, B, nrhs, X, options);
+    }
+    template <class T> Timing cholesky_solve(const Buffer<T>& L, std::size_t n, const Buffer<T>& B, std::size_t nrhs, Buffer<T>& X,
+                                             const FactorOptions& options = {}) {
+        return solve_buffers<T>(3, L, n, B, nrhs, X, options);
+    }
+    template <class T> CholeskyInfo cholesky_blocked(const Buffer<T>& A, std::size_t n, Buffer<T>& L, const FactorOptions& o = {}) {
+        return cholesky(A, n, L, o);
+    }
+    template <class T> Timing cholesky_solve_blocked(const Buffer<T>& L, std::size_t n, const Buffer<T>& B, std::size_t nrhs, Buffer<T>& X,
+                                                     const FactorOptions& o = {}) {
+        return cholesky_solve(L, n, B, nrhs, X, o);
+    }
     // Resident products (linalg.hpp:190-195): recorded into the batch; analysis, engine choice and modulus
     // count are GPU passes of the batch.
     template <class T> LinalgTicket syrk(CommandBatch& batch, const Buffer<T>& A, std::size_t rows, std::size_t cols, Buffer<T>& C,
@@ -141,4 +220,52 @@ public:
         return cholesky_solve(bits, L, n, B, nrhs, X, o);
     }
 };
+
+// ---- Exact dot products on the host (linalg.hpp:268-321): RN(c -/+ sum_k a[k*sa] b[k*sb]) with one rounding, the
+// contract every GPU product here meets; the same cluster method as the GPU limb kernel.  Statuses: zero carrying the
+// OR of c's and every operand's status; no nonzero product returns c (or zero).
+namespace detail {
+template <int N> struct HostDotTerms {
+    const Number<N>* a; long sa; const Number<N>* b; long sb; std::size_t K; bool subtract; lfd::Num<N> c;
+    lfd::u64 count() const { return K + 1; }
+    bool term(lfd::u64 k, lfd::i64& scale, lfd::i64& top, int& sign) const {
+        if (k == K) {
+            if (!c.s) return false;
+            scale = (lfd::i64)c.e - (32 * N - 1); top = scale + 32 * N; sign = c.s;
+            return true;
+        }
+        const Number<N>& x = a[(long)k * sa];
+        const Number<N>& y = b[(long)k * sb];
+        if (!x.sign || !y.sign) return false;
+        scale = (lfd::i64)x.exponent + y.exponent - 2 * (32 * N - 1); top = scale + 64 * N;
+        sign = subtract ? -x.sign * y.sign : x.sign * y.sign;
+        return true;
+    }
+    void add(lfd::u64 k, lfd::u32* acc, int len, lfd::i64 off) const {
+        if (k == K) { lfd::acc_add(acc, len, c.m, N, off); return; }
+        lfd::u32 p[2 * N];
+        lfd::mant_mul<N>(a[(long)k * sa].limb, b[(long)k * sb].limb, p);
+        lfd::acc_add(acc, len, p, 2 * N, off);
+    }
+};
+}  // namespace detail
+template <int N> inline Number<N> exact_dot_add(const Number<N>& c, bool subtract, const Number<N>* a, long sa, const Number<N>* b, long sb,
+                                                std::size_t K) {
+    word st = c.status;
+    bool products = false;
+    for (std::size_t k = 0; k < K; ++k) {
+        st |= a[(long)k * sa].status | b[(long)k * sb].status;
+        products = products || (a[(long)k * sa].sign && b[(long)k * sb].sign);
+    }
+    if (st) return zero<N>(st);
+    if (!products) return c;
+    const detail::HostDotTerms<N> src{a, sa, b, sb, K, subtract, detail::num(c)};
+    lfd::u32 error = 0;
+    const Number<N> r = detail::number(lfd::cluster_round<N, 8 * N + 64>(src, &error));
+    if (error) throw std::runtime_error("exact_dot_add: a cluster of terms exceeds the exact window");
+    return r;
+}
+template <int N> inline Number<N> exact_dot(const Number<N>* a, long sa, const Number<N>* b, long sb, std::size_t K) {
+    return exact_dot_add<N>(zero<N>(), false, a, sa, b, sb, K);
+}
 }  // namespace limbforge

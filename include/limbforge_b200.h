@@ -2,7 +2,7 @@
  *
  * The reference exposes a C++17 header API (namespace limbforge, include/limbforge/engine.hpp,
  * linalg.hpp, batched_linalg.hpp) and no C ABI.  This header is the language-neutral boundary
- * those classes map onto one to one; include/limbforge/*.hpp in this repository are the
+ * those classes map onto one to one; the headers include/limbforge/NAME.hpp in this repository are the
  * thin inline C++ wrappers that keep user code source compatible.  Each entry point cites the
  * reference interface it replaces (file:line, paths inside the reference project).
  *
@@ -52,10 +52,13 @@ typedef struct lf_cholesky_info {                                               
     size_t pivot; int pivot_sign; uint32_t pivot_status; lf_timing timing;
     size_t blocks, gpu_updates, host_updates; double panel_seconds, update_seconds;
 } lf_cholesky_info;
-typedef struct lf_linalg_report {                                                       /* linalg.hpp:35-45 (subset) */
+typedef struct lf_linalg_report {                                                       /* linalg.hpp:35-45 */
     size_t m, n, k, gpu_outputs, trivial_outputs, gemm_rows, gemm_cols, int8_gemms, moduli, band_bits;
     double analysis_seconds, gpu_seconds;
     int method;   /* 1 generic limb kernel, 2 residue engine */
+    /* lines (rows of the left operand, columns of the right) with a nonzero status-free entry, and the others
+     * (all zero, or a status entry), as the residue engine's analysis found them; 0 when the limb kernel ran */
+    size_t left_lines, left_zero_lines, right_lines, right_zero_lines;
 } lf_linalg_report;
 
 typedef struct lf_engine lf_engine;
@@ -67,11 +70,17 @@ typedef struct lf_submission lf_submission;
 const char* lf_last_error(void);
 /* library version string and the GPU architecture the kernels were built for */
 const char* lf_version(void);
+/* the limbforge API version the library implements (version.hpp: library_version) */
+void lf_api_version(unsigned* major, unsigned* minor, unsigned* patch);
 
 /* ---- Engine (engine.hpp:184-227) ---- */
 int lf_engine_create(const lf_engine_options* options, lf_engine** out);               /* Engine::Engine */
 void lf_engine_destroy(lf_engine* engine);                                              /* Engine::~Engine */
 int lf_engine_device_name(lf_engine* engine, char* name, size_t capacity);              /* Engine::device_name */
+/* Engine::prewarm (engine.hpp:190): validates the widths and operations and loads their element-wise kernels now */
+int lf_engine_prewarm(lf_engine* engine, const int* bits, size_t nbits, const int* ops, size_t nops);
+/* Engine::pipeline_info (engine.hpp:193): warp width, largest block of the kernel, block size it is launched with */
+int lf_engine_pipeline_info(lf_engine* engine, int bits, int op, unsigned* simd_width, unsigned* max_threads, unsigned* threads);
 /* Engine::run (engine.hpp:202): out[i] = op(a[i], b[(i/stride)%period]) for binary real/complex ops */
 int lf_engine_run(lf_engine* engine, int bits, int op, const void* a, const void* b, void* out, size_t count,
                   lf_broadcast b_index, lf_timing* timing);
@@ -94,6 +103,7 @@ int lf_batched_gemm(lf_engine* engine, int bits, int complex_, const lf_strided_
 int lf_linalg_create(lf_engine* engine, const lf_linalg_options* options, lf_linalg** out); /* Linalg::Linalg (engine may be NULL) */
 void lf_linalg_destroy(lf_linalg* linalg);
 int lf_linalg_get_report(lf_linalg* linalg, lf_linalg_report* report);                 /* Linalg::report */
+int lf_linalg_device_name(lf_linalg* linalg, char* name, size_t capacity);              /* Linalg::device_name */
 /* Linalg::gemm (linalg.hpp:155): C (m x n) = op(A) B, or RN(C - op(A) B) with subtract */
 int lf_linalg_gemm(lf_linalg* linalg, int bits, int transpose_a, const void* A, const void* B, size_t m, size_t n, size_t k,
                    void* C, int subtract, lf_timing* timing);
@@ -109,6 +119,12 @@ int lf_linalg_trsm(lf_linalg* linalg, int bits, int transpose, const void* L, si
 /* Linalg::cholesky_solve (linalg.hpp:163) */
 int lf_linalg_cholesky_solve(lf_linalg* linalg, int bits, const void* L, size_t n, const void* B, size_t nrhs, void* X,
                              const lf_factor_options* options, lf_timing* timing);
+/* Buffer forms (linalg.hpp:194-199): Linalg::cholesky / trsm / cholesky_solve on idle buffers of the Linalg's engine,
+ * used in place, synchronous; passes 1 = L X = B, 2 = L^T X = B, 3 = L L^T X = B.  Same results as the host-array calls. */
+int lf_linalg_cholesky_buffers(lf_linalg* linalg, int bits, lf_buffer* A, size_t n, lf_buffer* L, const lf_factor_options* options,
+                               lf_cholesky_info* info);
+int lf_linalg_solve_buffers(lf_linalg* linalg, int bits, int passes, lf_buffer* L, size_t n, lf_buffer* B, size_t nrhs, lf_buffer* X,
+                            const lf_factor_options* options, lf_timing* timing);
 /* Exact product on device line views (CUDA callers; no reference counterpart): element (line, k)
  * at base + (line * ls + k * ks) elements; C element (i, j) at C + i * ldc + j elements. */
 int lf_dev_exact_product(lf_linalg* linalg, int bits, const void* left, size_t left_ls, size_t left_ks, const void* right,

@@ -196,7 +196,8 @@ class _LinalgWorkspaces(C.Structure):
 class _LinalgReport(C.Structure):
     _fields_ = [(f, C.c_size_t) for f in ("m", "n", "k", "gpu_outputs", "trivial_outputs", "gemm_rows", "gemm_cols",
                                           "int8_gemms", "moduli", "band_bits")] + \
-               [("analysis_seconds", C.c_double), ("gpu_seconds", C.c_double), ("method", C.c_int)]
+               [("analysis_seconds", C.c_double), ("gpu_seconds", C.c_double), ("method", C.c_int)] + \
+               [(f, C.c_size_t) for f in ("left_lines", "left_zero_lines", "right_lines", "right_zero_lines")]
 
 
 class _RaggedLu4(C.Structure):

@@ -52,9 +52,12 @@ def _compile(src: str, obj: str, verbose: bool) -> str:
 
 
 def build(jobs: int | None = None, verbose: bool = False, force: bool = False) -> str:
-    os.makedirs(OBJ, exist_ok=True)
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     newest = max((os.path.getmtime(h) for h in _headers()), default=0.0)
+    # a library newer than every source and header is current, whether or not the objects are at hand
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max([newest] + [os.path.getmtime(x) for x in sources]):
+        return LIB
+    os.makedirs(OBJ, exist_ok=True)
     objs, todo = [], []
     for s in sources:
         o = os.path.join(OBJ, os.path.basename(s) + ".o")

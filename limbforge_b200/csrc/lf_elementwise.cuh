@@ -180,11 +180,34 @@ template <int N> int launch_chain(const ChainParams& p, cudaStream_t s) {
     return 0;
 }
 
+// Attributes of the element-wise kernel of one operation (the query also loads the kernel's module, which a
+// first launch would otherwise do): Engine::prewarm and Engine::pipeline_info.
+template <int N> int ew_attributes(int op, cudaFuncAttributes* a) {
+    switch (op) {
+    case 0: return cudaFuncGetAttributes(a, ew_kernel<N, 0>);
+    case 1: return cudaFuncGetAttributes(a, ew_kernel<N, 1>);
+    case 2: return cudaFuncGetAttributes(a, ew_kernel<N, 2>);
+    case 3: return cudaFuncGetAttributes(a, ew_kernel<N, 3>);
+    case 4: return cudaFuncGetAttributes(a, ew_kernel<N, 4>);
+    case 5: return cudaFuncGetAttributes(a, ew_kernel<N, 5>);
+    case 6: return cudaFuncGetAttributes(a, ew_kernel<N, 6>);
+    case 7: return cudaFuncGetAttributes(a, ew_kernel<N, 7>);
+    case 8: return cudaFuncGetAttributes(a, ew_kernel<N, 8>);
+    case 9: return cudaFuncGetAttributes(a, ew_kernel<N, 9>);
+    case 10: return cudaFuncGetAttributes(a, ew_kernel<N, 10>);
+    case 11: return cudaFuncGetAttributes(a, ew_kernel<N, 11>);
+    case 12: return cudaFuncGetAttributes(a, ew_kernel<N, 12>);
+    default: return (int)cudaErrorInvalidValue;
+    }
+}
+
 // Dispatch tables filled by the per-width translation units (lf_ew_*.cu).
 typedef int (*EwLauncher)(int, const EwParams&, cudaStream_t);
 typedef int (*ChainLauncher)(const ChainParams&, cudaStream_t);
+typedef int (*EwAttributes)(int, cudaFuncAttributes*);
 EwLauncher ew_launcher(int limbs);
 ChainLauncher chain_launcher(int limbs);
+EwAttributes ew_attributes_of(int limbs);
 
 }  // namespace lfd
 
@@ -192,4 +215,5 @@ ChainLauncher chain_launcher(int limbs);
     namespace lfd {                                                                      \
     int ew_launch_##N(int op, const EwParams& p, cudaStream_t s) { return launch_ew<N>(op, p, s); } \
     int chain_launch_##N(const ChainParams& p, cudaStream_t s) { return launch_chain<N>(p, s); } \
+    int ew_attr_##N(int op, cudaFuncAttributes* a) { return ew_attributes<N>(op, a); } \
     }

@@ -8,6 +8,7 @@
 #include "lf_residue.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <chrono>
 
 namespace lfr {
@@ -92,6 +93,15 @@ void lf_linalg_destroy(lf_linalg* la) {
     if (la->own_engine) lf_engine_destroy(static_cast<lf_engine*>(la->engine));
     delete la;
 }
+int lf_linalg_device_name(lf_linalg* la, char* name, size_t capacity) {
+    LF_API_BEGIN
+    if (!la || !name || !capacity) throw invalid_argument("null argument");
+    cudaDeviceProp p{};
+    cuda_check(cudaGetDeviceProperties(&p, la->engine->device), "device properties");
+    std::snprintf(name, capacity, "%s", p.name);
+    LF_API_END
+}
+
 int lf_linalg_get_report(lf_linalg* la, lf_linalg_report* r) {
     LF_API_BEGIN
     if (!la || !r) throw invalid_argument("null argument");
@@ -368,6 +378,87 @@ int lf_linalg_trsm(lf_linalg* la, int bits, int transpose, const void* L, size_t
 int lf_linalg_cholesky_solve(lf_linalg* la, int bits, const void* L, size_t n, const void* B, size_t nrhs, void* X,
                              const lf_factor_options* fo, lf_timing* timing) {
     return solve_common(la, bits, 3, L, n, B, nrhs, X, fo, timing);
+}
+
+// Buffer forms of the factorization and the solves (linalg.hpp:194-199): synchronous, outside any batch, on
+// buffers of the Linalg's engine used in place; the buffers must be idle (a buffer in an unwaited submission
+// throws logic_error) and are held like a submission's until the call returns.  Results equal the host-array
+// calls bit for bit.
+namespace {
+struct BufferClaim {
+    std::vector<lf_buffer*> held;
+    void take(lf_buffer* b, uint64_t owner) {
+        if (!b) throw invalid_argument("missing buffer");
+        if (b->owner != owner) throw invalid_argument("buffer belongs to another engine");
+        for (lf_buffer* h : held) if (h == b) return;
+        bool idle = false;
+        if (!b->busy.compare_exchange_strong(idle, true)) throw logic_error("buffer is in use by an unwaited submission");
+        held.push_back(b);
+    }
+    ~BufferClaim() { for (lf_buffer* b : held) b->busy.store(false); }
+};
+}  // namespace
+
+int lf_linalg_cholesky_buffers(lf_linalg* la, int bits, lf_buffer* A, size_t n, lf_buffer* L, const lf_factor_options* fo,
+                               lf_cholesky_info* out) {
+    LF_API_BEGIN
+    if (!la) throw invalid_argument("null linalg");
+    check_bits(bits);
+    validate_dims(n, n, n, n);
+    const size_t eb = size_t(bits / 8 + 12);
+    Engine& e = *la->engine;
+    BufferClaim claim;
+    claim.take(A, e.identity);
+    claim.take(L, e.identity);
+    if (A->bytes < n * n * eb || L->bytes < n * n * eb) throw invalid_argument("cholesky: buffer smaller than n x n");
+    lf_cholesky_info info{};
+    info.pivot = n;
+    if (n) {
+        e.activate();
+        auto w0 = Clock::now();
+        A->sync_to_device(e.stream);
+        if (L != A) L->host_authoritative = false;          // every entry of L is written below
+        uint32_t* W = static_cast<uint32_t*>(L->dev);
+        lfd::factor_kernels(bits / 32)->prep(static_cast<const uint32_t*>(A->dev), W, n, n, e.stream);
+        cuda_check(cudaGetLastError(), "cholesky prepare");
+        info = cholesky_device(*la, bits, W, n, fo ? fo->block : 32);
+        cuda_check(cudaStreamSynchronize(e.stream), "cholesky");
+        info.timing.wall_seconds = since(w0);
+    }
+    if (out) *out = info;
+    LF_API_END
+}
+
+int lf_linalg_solve_buffers(lf_linalg* la, int bits, int passes, lf_buffer* L, size_t n, lf_buffer* B, size_t nrhs, lf_buffer* X,
+                            const lf_factor_options* fo, lf_timing* timing) {
+    LF_API_BEGIN
+    if (!la) throw invalid_argument("null linalg");
+    if (passes < 1 || passes > 3) throw invalid_argument("passes must be 1 (L X = B), 2 (L^T X = B) or 3 (L L^T X = B)");
+    check_bits(bits);
+    validate_dims(n, nrhs, n, nrhs);
+    const size_t eb = size_t(bits / 8 + 12);
+    Engine& e = *la->engine;
+    BufferClaim claim;
+    claim.take(L, e.identity);
+    claim.take(B, e.identity);
+    claim.take(X, e.identity);
+    if (L->bytes < n * n * eb || B->bytes < n * nrhs * eb || X->bytes < n * nrhs * eb) throw invalid_argument("trsm: buffer too small");
+    if (X == L) throw invalid_argument("trsm: X overlaps L");
+    if (timing) *timing = {0, 0};
+    if (!n || !nrhs) return LF_OK;
+    e.activate();
+    auto w0 = Clock::now();
+    L->sync_to_device(e.stream);
+    B->sync_to_device(e.stream);
+    uint32_t* dX = static_cast<uint32_t*>(X->dev);
+    if (X != B) {
+        X->host_authoritative = false;
+        cuda_check(cudaMemcpyAsync(dX, B->dev, n * nrhs * eb, cudaMemcpyDeviceToDevice, e.stream), "right-hand sides");
+    }
+    const double g = solve_device(*la, bits, static_cast<const uint32_t*>(L->dev), n, dX, nrhs, fo ? fo->block : 32, passes);
+    cuda_check(cudaStreamSynchronize(e.stream), "solve");
+    if (timing) *timing = {g, since(w0)};
+    LF_API_END
 }
 
 // Device-pointer exact product for CUDA callers (no reference counterpart): C <- RN(C -/+ L R^T)

@@ -212,7 +212,14 @@ bool ResidueEngine::run(int bits, lfd::LineView left, lfd::LineView right, uint6
     cuda_check(cudaStreamSynchronize(s), "line analysis");
     int G = 0;
     bool any = false;
-    for (const auto& li : h) if (!li.status && li.nonzero) { G = std::max(G, li.top - li.bottom); any = true; }
+    report.left_lines = report.left_zero_lines = report.right_lines = report.right_zero_lines = 0;
+    for (size_t i = 0; i < h.size(); ++i) {
+        const auto& li = h[i];
+        const bool live = !li.status && li.nonzero;
+        if (live) { G = std::max(G, li.top - li.bottom); any = true; }
+        if (i < M) (live ? report.left_lines : report.left_zero_lines) += 1;
+        if (i >= M || same) (live ? report.right_lines : report.right_zero_lines) += 1;
+    }
     if (!any) return refuse("no nonzero lines");
     if (G > kMaxBand) return refuse("a line spans more than 192 exponent bits");
     const int P = 32 * n + G;

@@ -139,7 +139,42 @@ struct lf_submission : Submission {};
 extern "C" {
 
 const char* lf_last_error(void) { return g_error.c_str(); }
-const char* lf_version(void) { return "limbforge_b200 1.0 (sm_100a)"; }
+const char* lf_version(void) { return "limbforge_b200 1.3.1 (sm_100a)"; }
+
+// Engine::prewarm (engine.hpp:190): the kernels are compiled ahead for sm_100a, so preparing a width means
+// validating it and loading the requested element-wise kernels' modules now instead of at their first launch.
+int lf_engine_prewarm(lf_engine* e, const int* bits, size_t nbits, const int* ops, size_t nops) {
+    LF_API_BEGIN
+    if (!e) throw invalid_argument("null engine");
+    for (size_t i = 0; i < nbits; ++i) validate(bits[i], 0);
+    for (size_t j = 0; j < nops; ++j) if (!op_valid(ops[j])) throw invalid_argument("invalid operation");
+    e->activate();
+    for (size_t i = 0; i < nbits; ++i)
+        for (size_t j = 0; j < nops; ++j) {
+            cudaFuncAttributes a{};
+            cuda_check(static_cast<cudaError_t>(lfd::ew_attributes_of(bits[i] / 32)(ops[j], &a)), "kernel load");
+        }
+    LF_API_END
+}
+// Engine::pipeline_info (engine.hpp:193): warp width, the kernel's largest block and the block it is launched with.
+int lf_engine_pipeline_info(lf_engine* e, int bits, int op, unsigned* simd_width, unsigned* max_threads, unsigned* threads) {
+    LF_API_BEGIN
+    if (!e) throw invalid_argument("null engine");
+    validate(bits, 0);
+    if (!op_valid(op)) throw invalid_argument("invalid operation");
+    e->activate();
+    cudaFuncAttributes a{};
+    cuda_check(static_cast<cudaError_t>(lfd::ew_attributes_of(bits / 32)(op, &a)), "kernel attributes");
+    if (simd_width) *simd_width = 32;
+    if (max_threads) *max_threads = (unsigned)a.maxThreadsPerBlock;
+    if (threads) *threads = (unsigned)lfd::kEwThreads;
+    LF_API_END
+}
+void lf_api_version(unsigned* major, unsigned* minor, unsigned* patch) {
+    if (major) *major = 1;
+    if (minor) *minor = 3;
+    if (patch) *patch = 1;
+}
 
 int lf_engine_create(const lf_engine_options* options, lf_engine** out) {
     LF_API_BEGIN

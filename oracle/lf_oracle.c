@@ -255,7 +255,13 @@ static void round_sum(word* out, int n, term* t, size_t count) {
     size_t m = 0;
     for (size_t i = 0; i < count; ++i) if (t[i].sign) t[m++] = t[i];
     if (!m) { set_zero(out, n, 0); return; }
-    qsort(t, m, sizeof(term), term_cmp);
+    if (m <= 64) {                                   /* few terms: insertion sort, the order of term_cmp */
+        for (size_t i = 1; i < m; ++i) {
+            term x = t[i]; size_t j = i;
+            while (j > 0 && term_cmp(&t[j - 1], &x) > 0) { t[j] = t[j - 1]; --j; }
+            t[j] = x;
+        }
+    } else qsort(t, m, sizeof(term), term_cmp);
     int logc = 0; while (((size_t)1 << logc) < m + 1) ++logc;
     const int64_t gap = 32L * n + logc + 4;
     word* first = NULL; int first_w = 0; int64_t first_low = 0; int first_sign = 0; int follow = 0;
@@ -316,8 +322,11 @@ void lfo_exact_dot_add(int n, const word* c, int subtract, const word* a, long s
     word st = c ? gsts(c, n) : 0;
     for (size_t k = 0; k < K; ++k) st |= gsts(a + (long)k * sa * (long)E, n) | gsts(b + (long)k * sb * (long)E, n);
     if (st) { set_zero(out, n, st); return; }
-    term* t = (term*)malloc(sizeof(term) * (K + 1));
-    word* prod = (word*)malloc(sizeof(word) * (2 * (size_t)n) * (K ? K : 1));
+    /* short dots (the factorizations' K <= block) keep their terms on the stack */
+    term t_small[65]; word prod_small[64 * 64];
+    const int small = K <= 64;
+    term* t = small ? t_small : (term*)malloc(sizeof(term) * (K + 1));
+    word* prod = small ? prod_small : (word*)malloc(sizeof(word) * (2 * (size_t)n) * (K ? K : 1));
     size_t m = 0;
     for (size_t k = 0; k < K; ++k) {
         const word* x = a + (long)k * sa * (long)E; const word* y = b + (long)k * sb * (long)E;
@@ -329,12 +338,13 @@ void lfo_exact_dot_add(int n, const word* c, int subtract, const word* a, long s
     }
     if (!m) {
         if (c) copy_num(out, c, n); else set_zero(out, n, 0);
-        free(t); free(prod); return;
+        if (!small) { free(t); free(prod); }
+        return;
     }
     word cc[35];
     if (c && gsgn(c, n)) { copy_num(cc, c, n); t[m].w = cc; t[m].nw = n; t[m].scale = (int64_t)gexp(c, n) - (32L * n - 1); t[m].sign = gsgn(c, n); ++m; }
     round_sum(out, n, t, m);
-    free(t); free(prod);
+    if (!small) { free(t); free(prod); }
 }
 
 /* ---------------------------------------------------------------- complex (core.hpp:353-419) */
@@ -479,10 +489,14 @@ int lfo_cholesky(int bits, const word* A, size_t nn, word* L, size_t block, long
             else lfo_sqrt(n, s, AT(i, i));
         }
         size_t first = fail < k1 ? fail + 1 : k1;
+        /* rows below the diagonal block are independent of one another (each reads its own row and the
+           finished diagonal block), as are the entries of the trailing update: OpenMP over rows */
+#pragma omp parallel for schedule(dynamic, 4)
         for (size_t i = first; i < nn; ++i)
             for (size_t j = k0; j < fail; ++j) { word d[35]; lfo_exact_dot_add(n, AT(i, j), 1, AT(i, k0), 1, AT(j, k0), 1, j - k0, d); lfo_div(n, d, AT(j, j), AT(i, j)); }
         if (fail < k1) { p = fail; break; }
         /* trailing update by block [k0, k1) */
+#pragma omp parallel for schedule(dynamic, 4)
         for (size_t i = k1; i < nn; ++i)
             for (size_t j = k1; j <= i; ++j) { word d[35]; lfo_exact_dot_add(n, AT(i, j), 1, AT(i, k0), 1, AT(j, k0), 1, k1 - k0, d); copy_num(AT(i, j), d, n); }
     }
@@ -501,14 +515,17 @@ int lfo_solve(int bits, const word* L, size_t nn, word* X, size_t nrhs, size_t b
     if (passes & 1)
         for (size_t r0 = 0; r0 < nn; r0 += nb) {
             size_t r1 = r0 + nb < nn ? r0 + nb : nn;
+#pragma omp parallel for schedule(dynamic, 1)
             for (size_t c = 0; c < nrhs; ++c)
                 for (size_t i = r0; i < r1; ++i) { word d[35]; lfo_exact_dot_add(n, XX(i, c), 1, LL(i, r0), 1, XX(r0, c), (long)nrhs, i - r0, d); lfo_div(n, d, LL(i, i), XX(i, c)); }
+#pragma omp parallel for schedule(dynamic, 4)
             for (size_t i = r1; i < nn; ++i)
                 for (size_t c = 0; c < nrhs; ++c) { word d[35]; lfo_exact_dot_add(n, XX(i, c), 1, LL(i, r0), 1, XX(r0, c), (long)nrhs, r1 - r0, d); copy_num(XX(i, c), d, n); }
         }
     if (passes & 2)
         for (size_t r0 = (nn - 1) / nb * nb;; r0 -= nb) {
             size_t r1 = r0 + nb < nn ? r0 + nb : nn;
+#pragma omp parallel for schedule(dynamic, 1)
             for (size_t c = 0; c < nrhs; ++c)
                 for (size_t i = r1; i-- > r0;) {
                     word d[35];
@@ -516,6 +533,7 @@ int lfo_solve(int bits, const word* L, size_t nn, word* X, size_t nrhs, size_t b
                     else copy_num(d, XX(i, c), n);
                     lfo_div(n, d, LL(i, i), XX(i, c));
                 }
+#pragma omp parallel for schedule(dynamic, 4)
             for (size_t i = 0; i < r0; ++i)
                 for (size_t c = 0; c < nrhs; ++c) { word d[35]; lfo_exact_dot_add(n, XX(i, c), 1, LL(r0, i), (long)nn, XX(r0, c), (long)nrhs, r1 - r0, d); copy_num(XX(i, c), d, n); }
             if (!r0) break;

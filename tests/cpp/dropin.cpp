@@ -5,6 +5,7 @@
 #include "limbforge/linalg.hpp"
 #include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 
 using namespace limbforge;
@@ -73,6 +74,64 @@ int main() {
             if (std::memcmp(C3.data(), C.data(), sizeof(Float<B>) * 9)) { std::printf("syrk after release FAILED\n"); return 1; }
         }
         std::printf("linalg ok\n");
+        {   // the rest of the reference's public surface: prewarm, pipeline info, segmented dots, recurrences,
+            // Buffer-form factorization and solves, the full report, host scalar arithmetic, version checks
+            Prewarm pw; pw.bits = {64, 256}; pw.operations = {Operation::mul, Operation::complex_fma};
+            e.prewarm(pw);
+            e.prewarm_async(pw).get();
+            const PipelineInfo pi = e.pipeline_info(256, Operation::mul);
+            if (pi.simd_width != 32 || !pi.max_threads || !pi.threads_per_threadgroup) { std::printf("pipeline_info FAILED\n"); return 1; }
+            LinalgPrewarm lp; lp.bits = {256}; lp.inner_sizes = {32};
+            la.prewarm(lp);
+            la.prewarm_async(lp).get();
+            if (la.device_name().empty()) { std::printf("linalg device_name FAILED\n"); return 1; }
+            SegmentedDot sd; sd.segments = 2; sd.length = 3;
+            std::vector<Float<B>> da(6, power<B>(1)), db(6, power<B>(2)), dout(2);
+            e.segmented_dot(B, false, sd, da.data(), db.data(), dout.data());       // 3 * 2^3 = 2^4 + 2^3
+            if (dout[0].exponent != 4 || dout[1].limb[B / 32 - 1] != 0xC0000000u) { std::printf("segmented_dot FAILED\n"); return 1; }
+            auto ba = e.make_buffer<Float<B>>(6), bb = e.make_buffer<Float<B>>(6), bo = e.make_buffer<Float<B>>(2);
+            ba.upload(da.data(), 6); bb.upload(db.data(), 6);
+            auto sb = e.batch();
+            sb.segmented_dot(sd, ba, bb, bo);
+            sb.submit().wait();
+            std::vector<Float<B>> dout2(2);
+            bo.download(dout2.data(), 2);
+            if (std::memcmp(dout2.data(), dout.data(), sizeof(Float<B>) * 2)) { std::printf("batch segmented_dot FAILED\n"); return 1; }
+            // ring (1, 1, 1, 1) with weights (1, 0, 0, 0): each step moves q0 to the end, so the result is 1
+            std::vector<Complex<B / 32>> seeds(4, {power<B>(0), zero<B / 32>()}), w(4, {zero<B / 32>(), zero<B / 32>()}), q(1);
+            w[0] = {power<B>(0), zero<B / 32>()};
+            e.recurrence(B, seeds.data(), w.data(), q.data(), 1, 1);
+            if (q[0].re.exponent != 0 || q[0].re.sign != 1 || q[0].im.sign) { std::printf("recurrence FAILED\n"); return 1; }
+            bool vr = false;
+            try { e.vector_recurrence(B, VectorRecurrence{}, nullptr, nullptr, nullptr, nullptr, nullptr); } catch (const std::runtime_error&) { vr = true; }
+            if (!vr) { std::printf("vector_recurrence FAILED\n"); return 1; }
+            auto bA = e.make_buffer<Float<B>>(9), bL = e.make_buffer<Float<B>>(9), bR = e.make_buffer<Float<B>>(3), bX = e.make_buffer<Float<B>>(3);
+            bA.upload(C.data(), 9);
+            const CholeskyInfo bi = la.cholesky(bA, 3, bL);
+            std::vector<Float<B>> L2(9);
+            bL.download(L2.data(), 9);
+            if (bi.pivot != 3 || std::memcmp(L2.data(), L.data(), sizeof(Float<B>) * 9)) { std::printf("buffer cholesky FAILED\n"); return 1; }
+            std::vector<Float<B>> rhs = {power<B>(0), power<B>(2), power<B>(4)}, X1(3), X2(3);
+            bR.upload(rhs.data(), 3);
+            la.cholesky_solve(B, L.data(), 3, rhs.data(), 1, X1.data());
+            la.cholesky_solve(bL, 3, bR, 1, bX);
+            bX.download(X2.data(), 3);
+            if (std::memcmp(X1.data(), X2.data(), sizeof(Float<B>) * 3)) { std::printf("buffer cholesky_solve FAILED\n"); return 1; }
+            la.trsm(false, bL, 3, bR, 1, bX);
+            la.cholesky_blocked(bA, 3, bL);
+            la.cholesky_solve_blocked(bL, 3, bR, 1, bX);
+            std::vector<Float<B>> G(4 * 3, power<B>(0)), P(9);
+            la.syrk(B, G.data(), 4, 3, P.data(), false);
+            const LinalgReport& rep = la.report();
+            if (rep.left_bands.size() != 2 || rep.left_bands[1] != 3 || rep.left_fallback || rep.fallback_outputs) { std::printf("report FAILED\n"); return 1; }
+            const Float<B> s = add(power<B>(3), power<B>(3)), p = mul(power<B>(3), power<B>(-5)), f = fma(power<B>(1), power<B>(1), power<B>(2));
+            if (s.exponent != 4 || p.exponent != -2 || f.exponent != 3 || magnitude_compare(s, p) <= 0) { std::printf("host arithmetic FAILED\n"); return 1; }
+            std::vector<Float<B>> xs(3, power<B>(1)), ys(3, power<B>(1));
+            if (exact_dot(xs.data(), 1, ys.data(), 1, 3).limb[B / 32 - 1] != 0xC0000000u) { std::printf("exact_dot FAILED\n"); return 1; }
+            check_library_version();
+            if (!version_compatible(library_version(), header_version) || std::string(library_version_string()).empty()) { std::printf("version FAILED\n"); return 1; }
+            std::printf("full surface ok\n");
+        }
         BatchedLinalg bl(e);
         StridedGemm s; s.count = 1; s.m = s.n = s.k = 2; s.stride_a = s.stride_b = s.stride_c = 4;
         std::vector<Complex<B / 32>> ca(4), cb(4), cc(4);
