@@ -296,12 +296,12 @@ def cdiv_1024(torch, api):
             "cdiv_full_match": bool((got == want).all()), "checked": cnt}
 
 
-def exact_gemm_512(torch, api):
+def exact_gemm_512(torch, api, scale=1.0):
     """512-bit C <- RN(C - A^T B), A, B 1024 x 1024 (exponents U[-40,40], 0.5% zeros), residue engine
-    vs the plain limb kernel on the same device data; SYRK A^T A (lower)."""
+    vs the plain limb kernel on the same device data; SYRK A^T A (lower).  `scale` shrinks n (profiling)."""
     from limbforge_b200 import numbers as nb
     from oracle.oracle import Oracle, Reference
-    bits, n = 512, 1024
+    bits, n = 512, max(128, int(1024 * scale) // 128 * 128)
     rng = np.random.default_rng(102)
     A = nb.random_numbers(rng, n * n, bits, 40, zero_frac=0.005)
     B = nb.random_numbers(rng, n * n, bits, 40, zero_frac=0.005)
@@ -333,7 +333,7 @@ def exact_gemm_512(torch, api):
     res["residue"]["int8_tops_whole_call"] = 2 * int8_macs / res["residue"]["s"] / 1e12
     # oracle on one full output row
     got = outs["residue"].cpu().numpy().view(np.uint32)
-    row = 517
+    row = 517 % n
     want = Oracle().gemm(bits, True, A, B, n, n, n, C=C0, subtract=True, rows=(row, row + 1))
     res["oracle_row_match"] = bool((got[row * n:(row + 1) * n] == want[row * n:(row + 1) * n]).all())
     # SYRK A^T A lower, residue engine
@@ -512,7 +512,7 @@ def run_workloads(args):
     out = {}
     for name, fn in (("mul_div_fma_256bit_65536", lambda: elementwise_256(torch, api, hbm_peak)),
                      ("cdiv_1024bit_65536", lambda: cdiv_1024(torch, api)),
-                     ("exact_gemm_512bit_1024", lambda: exact_gemm_512(torch, api)),
+                     ("exact_gemm_512bit_1024", lambda: exact_gemm_512(torch, api, args.scale)),
                      ("cholesky_256bit_2048", lambda: cholesky_2048(torch, api)),
                      ("ragged_batch_20000", lambda: ragged_batch(torch, api, args.scale))):
         if args.workload and name != args.workload:
@@ -666,7 +666,7 @@ def main():
     ap.add_argument("--count", type=int, default=65536, help="values per chain (65,536 is the headline workload)")
     ap.add_argument("--no-workloads", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--workload", default="", help="run only this secondary workload and print its JSON (profiling)")
-    ap.add_argument("--scale", type=float, default=1.0, help="size factor of the ragged batch (profiling captures)")
+    ap.add_argument("--scale", type=float, default=1.0, help="size factor of the ragged batch and the exact GEMM (profiling captures)")
     args = ap.parse_args()
     global COUNT
     COUNT = args.count

@@ -287,6 +287,11 @@ int lf_ragged_plan_run(lf_ragged_plan* plan, void* arena, void* stream);
 int lf_ragged_plan_get_info(const lf_ragged_plan* plan, lf_ragged_info* info);
 void lf_ragged_plan_destroy(lf_ragged_plan* plan);
 
+/* ---- Failure-detection test hook (no reference counterpart): one tile of the residue products whose loads are
+ * left out, so the first barrier wait of the tensor-core kernel runs out after `polls` polls; the kernel records
+ * error 2, frees its tensor memory and returns, and *error_word receives the kernel's error word. */
+int lf_test_residue_wait_limit(unsigned polls, uint32_t* error_word);
+
 /* ---- Measurement helper (no reference counterpart): the device's rate of 32 x 32 -> 64-bit integer
  * multiply-adds, the word product of every limb kernel, measured by a kernel of independent
  * multiply-add chains on every SM (CUDA events).  The denominator of the integer-pipe roofline. */

@@ -269,6 +269,7 @@ def _load() -> C.CDLL:
         "lf_ragged_plan_tune": ([V, V], I), "lf_ragged_plan_run": ([V, V, V], I),
         "lf_ragged_plan_get_info": ([V, P(_RaggedInfo)], I), "lf_ragged_plan_destroy": ([V], None),
         "lf_probe_word_mac_rate": ([I, P(C.c_double)], I),
+        "lf_test_residue_wait_limit": ([C.c_uint, P(C.c_uint32)], I),
         "lf_engine_segmented_dot": ([V, I, I, P(_SegmentedDot), V, V, V, P(_Timing)], I),
         "lf_batch_segmented_dot": ([V, I, I, P(_SegmentedDot), V, V, V], I),
         "lf_engine_recurrence": ([V, I, V, V, V, S, C.c_uint, C.c_uint, P(_Timing)], I),
@@ -835,3 +836,11 @@ def word_mac_rate(device: int = 0) -> float:
     r = C.c_double()
     check(lib.lf_probe_word_mac_rate(device, C.byref(r)))
     return r.value
+
+
+def residue_wait_limit_test(polls: int) -> int:
+    """Failure-detection hook: a residue-product tile whose first barrier wait runs out after `polls` polls;
+    returns the kernel's error word (2 when the bounded wait gave up)."""
+    e = C.c_uint32()
+    check(lib.lf_test_residue_wait_limit(polls, C.byref(e)))
+    return e.value

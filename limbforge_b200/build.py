@@ -54,8 +54,10 @@ def _compile(src: str, obj: str, verbose: bool) -> str:
 def build(jobs: int | None = None, verbose: bool = False, force: bool = False) -> str:
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     newest = max((os.path.getmtime(h) for h in _headers()), default=0.0)
-    # a library newer than every source and header is current, whether or not the objects are at hand
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max([newest] + [os.path.getmtime(x) for x in sources]):
+    # without the object directory (a copy of the tree that carries only the built library), a library newer
+    # than every source and header is current; with it, every object is checked against its dependencies
+    if not force and not os.path.isdir(OBJ) and os.path.exists(LIB) and \
+            os.path.getmtime(LIB) >= max([newest] + [os.path.getmtime(x) for x in sources]):
         return LIB
     os.makedirs(OBJ, exist_ok=True)
     objs, todo = [], []

@@ -6,6 +6,7 @@
 #include "lf_runtime.h"
 #include "lf_linalg.cuh"
 #include "lf_residue.h"
+#include "lf_residue.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -41,10 +42,16 @@ void exact_product(Linalg& la, int bits, lfd::LineView left, lfd::LineView right
     if (method != 1 && !la.options.force_fallback)
         used_residue = la.residue.run(bits, left, right, M, Nc, K, C, ldc, subtract, lower, err, s, method == 2, la.report);
     if (!used_residue) {
-        lfd::DotParams p{};
+        // the tiled limb kernel: line analysis, then one exact window per output (cluster method for wide outputs)
+        lfd::WinParams wp{};
+        lfd::DotParams& p = wp.d;
         p.left = left; p.right = right; p.C = C; p.ldc = ldc; p.M = M; p.Nc = Nc; p.K = K;
         p.row0 = 0; p.col0 = 0; p.subtract = subtract; p.lower = lower; p.error = err;
-        lfd::linalg_kernels(n)->dot(p, s);
+        auto* linfo = static_cast<lfd::LineInfo*>(la.lines.get(sizeof(lfd::LineInfo) * (M + Nc) + 64));
+        lfd::linalg_kernels(n)->analyze(left, M, K, linfo, s);
+        lfd::linalg_kernels(n)->analyze(right, Nc, K, linfo + M, s);
+        wp.linfo = linfo; wp.rinfo = linfo + M;
+        lfd::residue_kernels(n)->window_dot(wp, s);
         cuda_check(cudaGetLastError(), "exact product launch");
     }
     if (method_used) *method_used = used_residue ? 2 : 1;

@@ -537,3 +537,33 @@ bool resident_product_report(ResidentProduct& r, lf_linalg_report& rep) {
 }
 
 }  // namespace lfr
+
+// ---------------------------------------------------------------- failure detection test hook
+// One 128 x 128 tile of the residue products with the producer's loads left out, so the MMA issuer's first
+// barrier wait never completes and gives up after `polls` polls: the kernel records error 2, frees its TMEM and
+// returns, and the context stays usable.  The value of the error word comes back in *error_word.
+extern "C" int lf_test_residue_wait_limit(unsigned polls, uint32_t* error_word) {
+    using namespace lfr;
+    LF_API_BEGIN
+    if (!error_word || !polls) throw invalid_argument("polls must be positive and error_word not null");
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    const TableSet tab = tables_for(dev, 1);
+    DevBuf planes, res, err;
+    const uint64_t Kp = lfd::kTileK, Mp = lfd::kTileM;
+    auto* pl = static_cast<signed char*>(planes.get(4 * Mp * Kp + 256));
+    cuda_check(cudaMemset(pl, 0, 4 * Mp * Kp + 256), "planes");
+    auto* r16 = static_cast<uint16_t*>(res.get(64));
+    auto* e = static_cast<uint32_t*>(err.get(16));
+    cuda_check(cudaMemset(e, 0, 16), "error word");
+    const CUtensorMap t1 = plane_map(pl, Kp, Mp, 1), t0 = plane_map(pl + Mp * Kp, Kp, Mp, 1);
+    const CUtensorMap u1 = plane_map(pl + 2 * Mp * Kp, Kp, Mp, 1), u0 = plane_map(pl + 3 * Mp * Kp, Kp, Mp, 1);
+    lfd::MmaParams mp{r16, tab.dev, 1, 1, Kp, 0, e, nullptr, polls, 1};
+    const size_t smem = lfd::kStages * lfd::kStageBytes + 1024;
+    cuda_check(cudaFuncSetAttribute(lfd::residue_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem");
+    lfd::residue_mma_kernel<<<dim3(1, 1, 1), lfd::kMmaThreads, smem, nullptr>>>(t1, t0, u1, u0, mp);
+    cuda_check(cudaGetLastError(), "launch");
+    cuda_check(cudaDeviceSynchronize(), "bounded wait");
+    cuda_check(cudaMemcpy(error_word, e, 4, cudaMemcpyDeviceToHost), "error word");
+    LF_API_END
+}

@@ -98,6 +98,8 @@ struct MmaParams {
     int lower;                              // skip tiles strictly above the diagonal (SYRK)
     u32* error;
     const ResPlan* plan;                    // planned on the GPU: moduli at or above plan->L have no work
+    u32 poll_limit;                         // polls of a barrier wait before it gives up (0: kSpinLimit)
+    int no_loads;                           // failure test only: the producer issues no loads, so the first wait runs out
 };
 
 __device__ __forceinline__ u32 smem_u32(const void* p) { return (u32)__cvta_generic_to_shared(p); }
@@ -113,9 +115,9 @@ __device__ __forceinline__ bool mbar_try_wait(u64* bar, u32 phase) {
                  : "=r"(ok) : "r"(smem_u32(bar)), "r"(phase) : "memory");
     return ok != 0;
 }
-// Bounded wait: false (and the error flag set) when the barrier never completes.
-__device__ __forceinline__ bool mbar_wait(u64* bar, u32 phase, u32* error) {
-    for (u32 it = 0; it < kSpinLimit; ++it)
+// Bounded wait: false (and the error flag set) when the barrier has not completed after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(u64* bar, u32 phase, u32* error, u32 limit = kSpinLimit) {
+    for (u32 it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, phase)) return true;
     atomicExch(error, 2u);
     return false;
@@ -185,15 +187,16 @@ __global__ void __launch_bounds__(kMmaThreads, 1) residue_mma_kernel(const __gri
     const u32 tmem = tmem_slot;
     const u32 acc11 = tmem, acc00 = tmem + kTileN, accm = tmem + 2 * kTileN;
     const int kblocks = (int)(p.Kp / kTileK);
+    const u32 polls = p.poll_limit ? p.poll_limit : kSpinLimit;
     __shared__ int abort_flag, issued, consumed;          // stages loaded by the producer / read by the MMA issuer
     if (threadIdx.x == 0) { abort_flag = 0; issued = 0; consumed = kblocks; }
     __syncthreads();
     if (warp == 0 && lane == 0) {
         // producer; stops issuing once the MMA issuer has given up
-        for (int kb = 0; kb < kblocks; ++kb) {
+        for (int kb = 0; kb < kblocks && !p.no_loads; ++kb) {
             const int s = kb % kStages;
             const u32 ph = (u32)((kb / kStages) & 1);
-            if (kb >= kStages && !mbar_wait(&empty[s], ph ^ 1u, p.error)) { abort_flag = 1; break; }
+            if (kb >= kStages && !mbar_wait(&empty[s], ph ^ 1u, p.error, polls)) { abort_flag = 1; break; }
             if (*(volatile int*)&abort_flag) break;
             unsigned char* st = smem + s * kStageBytes;
             mbar_expect_tx(&full[s], kStageBytes);
@@ -209,7 +212,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) residue_mma_kernel(const __gri
         for (int kb = 0; kb < kblocks && ok; ++kb) {
             const int s = kb % kStages;
             const u32 ph = (u32)((kb / kStages) & 1);
-            if (!mbar_wait(&full[s], ph, p.error)) { ok = false; consumed = kb; *(volatile int*)&abort_flag = 1; break; }
+            if (!mbar_wait(&full[s], ph, p.error, polls)) { ok = false; consumed = kb; *(volatile int*)&abort_flag = 1; break; }
             asm volatile("tcgen05.fence::after_thread_sync;");
             unsigned char* st = smem + s * kStageBytes;
             const u64 a1 = smem_desc(st), a0 = smem_desc(st + kTileBytes), b1 = smem_desc(st + 2 * kTileBytes),
@@ -231,9 +234,9 @@ __global__ void __launch_bounds__(kMmaThreads, 1) residue_mma_kernel(const __gri
     if (abort_flag && threadIdx.x == 0) {
         // An abandoned wait leaves loads in flight into shared memory: let every stage that was loaded and
         // not read complete (bounded) before the CTA releases its resources.
-        for (int kb = consumed; kb < issued; ++kb) mbar_wait(&full[kb % kStages], (u32)((kb / kStages) & 1), p.error);
+        for (int kb = consumed; kb < issued; ++kb) mbar_wait(&full[kb % kStages], (u32)((kb / kStages) & 1), p.error, polls);
     }
-    const bool fine = mbar_wait(&done, 0, p.error) && !abort_flag;
+    const bool fine = mbar_wait(&done, 0, p.error, polls) && !abort_flag;
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (fine) {
         const u32 m = tab->m[l];
@@ -345,26 +348,25 @@ __device__ __forceinline__ void acc_unit(u32* acc, int len, bool negative) {   /
     if (negative) { for (int k = 0; k < len; ++k) { const u32 old = acc[k]; acc[k] = old - 1u; if (old) break; } }
     else { for (int k = 0; k < len; ++k) { if (++acc[k]) break; } }
 }
-template <int N> __device__ Num<N> round_sum2(const u32* X, int xw, i64 sx, int signx, const Num<N>& c) {
-    constexpr int CWmax = kResMaxQWords + 2 * N + 10;
+// Scratch words round_sum2 needs for an X of xw words (the window below); callers pass that much.
+template <int N> __host__ __device__ constexpr int round_sum2_words(int xw) { return xw + 2 * N + 8; }
+template <int N> __device__ Num<N> round_sum2(const u32* X, int xw, i64 sx, int signx, const Num<N>& c, u32* acc) {
     // One two's-complement window of xw + 2N + 8 words under the larger top, two bits of headroom
     // above it: a term below the window lies at least 2N + 6 words under that top, beyond every
-    // rounding decision, and counts as +-1 in the lowest word.
-    const int CW = xw + 2 * N + 8;
+    // rounding decision, and counts as +-1 in the lowest word.  The window lives in the caller's
+    // scratch (shared memory in crt_round_kernel).
+    const int CW = round_sum2_words<N>(xw);
     int tx = -1;
     for (int w = xw - 1; w >= 0; --w) if (X[w]) { tx = w; break; }
     if (tx < 0) return c;                                       // no product term left
     const i64 topx = sx + 32 * (i64)tx + 31 - __clz(X[tx]);
     if (!c.s) {
-        u32 t[kResMaxQWords + 2];
-        for (int w = 0; w < xw; ++w) t[w] = X[w];
-        Rounded<N> R; round_info<N>(t, xw, sx, R);
+        Rounded<N> R; round_info<N>(X, xw, sx, R);
         return finish<N>(R.m, R.e, signx, R.rb && (R.sb || (R.m[0] & 1u)), 0);
     }
     const i64 sc = (i64)c.e - (32 * N - 1), topc = c.e;
     const i64 hi = topx > topc ? topx : topc;
     const i64 lo = hi + 3 - 32 * (i64)(CW - 1);               // exponent of window bit 32
-    u32 acc[CWmax];
     for (int w = 0; w < CW; ++w) acc[w] = 0;
     if (sx >= lo) { if (signx > 0) acc_add(acc, CW, X, xw, 32 + (sx - lo)); else acc_sub(acc, CW, X, xw, 32 + (sx - lo)); }
     else acc_unit(acc, CW, signx < 0);
@@ -382,7 +384,7 @@ template <int N> __device__ Num<N> round_sum2(const u32* X, int xw, i64 sx, int 
 // RN(X 2^scale), one rounding.  The modulus product exceeds 4 max|X|, so the quotient's rounding is
 // never close.
 template <int N> __device__ __forceinline__ Num<N> crt_tail(u32* S, int qwords, u64 F, const ResTables* tab, i64 scale,
-                                                          bool subtract, const Num<N>& c) {
+                                                          bool subtract, const Num<N>& c, u32* scratch) {
     const u64 q = (F + (1ull << 47)) >> 48;                  // round(F): X = S - q M
     // D = S - q*M (two's complement over qwords+2 words)
     u64 borrow = 0;
@@ -400,7 +402,115 @@ template <int N> __device__ __forceinline__ Num<N> crt_tail(u32* S, int qwords, 
         for (int w = 0; w < xw; ++w) { u64 v = (u64)(u32)~S[w] + c1; S[w] = (u32)v; c1 = v >> 32; }
     }
     // a zero exact sum X with the addend falls back to c itself, as exact_dot_add
-    return round_sum2<N>(S, xw, scale, subtract ? -sign : sign, c);
+    return round_sum2<N>(S, xw, scale, subtract ? -sign : sign, c, scratch);
+}
+
+// ---------------------------------------------------------------- 4. tiled limb-kernel product
+// The generic limb kernel's fast form: C[i][j] = RN(c -/+ sum_k L(i,k) R(j,k)) with every product summed exactly in
+// one window per output and rounded once (round_sum2 with the old entry), the same bits as exact_dot_add.  The line
+// analysis bounds every product of output (i, j): a nonzero, status-free entry of line i has its exponent in
+// [bottom_i, top_i], so the products' scales lie in [base, base + spread_i + spread_j] with base = bottom_i +
+// bottom_j - 2(32N - 1), each below 2^(scale + 64N), and K of them sum below 2^(base + spread_i + spread_j + 64N +
+// ceil(log2 K)).  When that fits kWinWords(N) words, the output sums its products as two magnitudes, positive and
+// negative, at word offset (scale - base) / 32 (carries run a word or two), then subtracts them once; wider outputs
+// take exact_dot_add_dev's cluster method in the same kernel.  A block computes an 8 x 8 tile of outputs and stages
+// the 8 + 8 lines' next kWinTK entries in shared memory, so each entry is read from memory once per tile instead of
+// once per output; the windows live in shared memory (one odd-stride row per thread).
+constexpr int kWinTM = 8, kWinTN = 8, kWinThreads = kWinTM * kWinTN, kWinTK = 8;
+template <int N> __host__ __device__ constexpr int win_words() { return 2 * N + 8; }
+template <int N> __host__ __device__ constexpr int win_row_words() { return (win_words<N>() + round_sum2_words<N>(win_words<N>())) | 1; }
+template <int N> __host__ __device__ constexpr size_t win_smem_bytes() {
+    return (size_t)4 * ((kWinTM + kWinTN) * kWinTK * (N + 3) + kWinThreads * win_row_words<N>());
+}
+// acc (len words) += t (tw words) << (32 ws + bs), carries to the end of acc
+__device__ __forceinline__ void win_add(u32* acc, int len, const u32* t, int tw, int ws, int bs) {
+    u64 cy = 0;
+    int k = ws;
+    for (int q = 0; q <= tw && k < len; ++q, ++k) {
+        const u32 v = lf_fshl(q ? t[q - 1] : 0u, q < tw ? t[q] : 0u, (u32)bs);
+        const u64 x = (u64)acc[k] + v + cy; acc[k] = (u32)x; cy = x >> 32;
+    }
+    for (; cy && k < len; ++k) { const u64 x = (u64)acc[k] + cy; acc[k] = (u32)x; cy = x >> 32; }
+}
+struct WinParams {
+    DotParams d;                    // operands, output, modes, error word
+    const LineInfo* linfo; const LineInfo* rinfo;   // analysis of the M left and Nc right lines
+};
+template <int N> __global__ void __launch_bounds__(kWinThreads) window_dot_kernel(const WinParams wp) {
+    const DotParams& p = wp.d;
+    constexpr int E = N + 3, W = win_words<N>();
+    extern __shared__ __align__(16) u32 win_park[];
+    u32* sA = win_park;                                  // [kWinTK][kWinTM] entries
+    u32* sB = sA + kWinTK * kWinTM * E;                  // [kWinTK][kWinTN] entries
+    const int t = threadIdx.x, r = t / kWinTN, q = t % kWinTN;
+    u32* pos = sB + kWinTK * kWinTN * E + t * win_row_words<N>();
+    u32* neg = pos + W;                                  // also round_sum2's scratch afterwards
+    const u64 r0 = (u64)blockIdx.y * kWinTM, q0 = (u64)blockIdx.x * kWinTN;
+    const u64 ro = r0 + r, qo = q0 + q;                  // this thread's output (local row, column)
+    const u64 i = p.row0 + ro, j = p.col0 + qo;          // its lines
+    bool live = ro < p.M && qo < p.Nc && !(p.lower && j > i);
+    u32* out = p.C + (ro * p.ldc + qo) * E;
+    const Num<N> c = (live && p.subtract) ? load_plain<N>(out) : zero<N>();
+    LineInfo li{}, ri{};
+    if (live) { li = wp.linfo[ro]; ri = wp.rinfo[qo]; }
+    const u32 st = (p.subtract ? c.st : 0u) | li.status | ri.status;
+    const bool products = li.nonzero && ri.nonzero;
+    int logk = 0;
+    while ((1ull << logk) < p.K) ++logk;
+    const i64 span = products ? (i64)(li.top - li.bottom) + (ri.top - ri.bottom) + 64 * N + logk : 0;
+    const bool window = live && !st && products && span <= 32 * W;
+    if (window) for (int w = 0; w < W; ++w) { pos[w] = 0; neg[w] = 0; }
+    const int ebase = li.bottom + ri.bottom;
+    // all threads stage the tiles (the barriers include threads without a window)
+    for (u64 k0 = 0; k0 < p.K; k0 += kWinTK) {
+        __syncthreads();
+        // word by word over the staged entries, consecutive words to consecutive threads: entries of one k that
+        // are consecutive in memory (unit line stride) make coalesced runs
+        for (int x = t; x < (kWinTM + kWinTN) * kWinTK * E; x += kWinThreads) {
+            const int e = x / E, w = x - e * E;
+            const bool left = e < kWinTM * kWinTK;
+            const int y = left ? e : e - kWinTM * kWinTK;
+            const int kk = y / (left ? kWinTM : kWinTN), line = y - kk * (left ? kWinTM : kWinTN);
+            const u64 lo_line = (left ? r0 : q0) + line, k = k0 + kk;
+            const bool in = k < p.K && lo_line < (left ? p.M : p.Nc);
+            const LineView& v = left ? p.left : p.right;
+            win_park[x] = in ? __ldg(v.base + (((left ? p.row0 : p.col0) + lo_line) * v.ls + k * v.ks) * (u64)E + w) : 0u;
+        }
+        __syncthreads();
+        if (!window) continue;
+        const int kmax = p.K - k0 < (u64)kWinTK ? (int)(p.K - k0) : kWinTK;
+        for (int kk = 0; kk < kmax; ++kk) {
+            const u32* a = sA + (kk * kWinTM + r) * E;
+            const u32* b = sB + (kk * kWinTN + q) * E;
+            const int sa = (int)a[N + 1], sb = (int)b[N + 1];
+            if (!sa || !sb) continue;
+            u32 am[N], bm[N], pr[2 * N];
+#pragma unroll
+            for (int w = 0; w < N; ++w) { am[w] = a[w]; bm[w] = b[w]; }
+            mant_mul<N>(am, bm, pr);
+            const int off = (int)a[N] + (int)b[N] - ebase;           // 0 <= off <= spread_i + spread_j
+            win_add(((sa * sb > 0) != (p.subtract != 0)) ? pos : neg, W, pr, 2 * N, off >> 5, off & 31);
+        }
+    }
+    if (!live) return;
+    if (st) { store<N>(out, zero<N>(st)); return; }
+    if (!products) { store<N>(out, p.subtract ? c : zero<N>()); return; }
+    if (!window) {                                       // wide output: the cluster method, from memory
+        const Num<N> v = exact_dot_add_dev<N>(p.subtract ? out : nullptr, p.subtract, p.left.base + i * p.left.ls * E, (i64)p.left.ks,
+                                              p.right.base + j * p.right.ls * E, (i64)p.right.ks, p.K, p.error);
+        store<N>(out, v);
+        return;
+    }
+    // X = pos - neg as sign and magnitude, then one rounding with the old entry
+    int cmp = 0;
+    for (int w = W - 1; w >= 0 && !cmp; --w) if (pos[w] != neg[w]) cmp = pos[w] > neg[w] ? 1 : -1;
+    u32* big = cmp >= 0 ? pos : neg;
+    const u32* small = cmp >= 0 ? neg : pos;
+    u32 bo = 0;
+    for (int w = 0; w < W; ++w) { const u64 d = (u64)small[w] + bo; const u32 o = big[w]; big[w] = (u32)((u64)o - d); bo = (u64)o < d; }
+    if (big != pos) for (int w = 0; w < W; ++w) pos[w] = big[w];
+    // round_sum2 adds the old entry c with its own sign (it computes RN(sign * X * 2^scale + c))
+    store<N>(out, round_sum2<N>(pos, W, (i64)ebase - 2 * (32 * N - 1), cmp, c, neg));
 }
 
 template <int N> __global__ void __launch_bounds__(128) reconstruct_kernel(RecParams p) {
@@ -432,7 +542,8 @@ template <int N> __global__ void __launch_bounds__(128) reconstruct_kernel(RecPa
     u64 cy = 0;
     for (int w = 0; w <= p.qwords; ++w) { u64 v = col[w] + cy; S[w] = (u32)v; cy = v >> 32; }
     S[p.qwords + 1] = (u32)cy;
-    store<N>(out, crt_tail<N>(S, p.qwords, F, p.tab, (i64)li.bottom + ri.bottom - 2 * (32 * N - 1), p.subtract != 0, c));
+    u32 scratch[round_sum2_words<N>(kResMaxQWords + 2)];
+    store<N>(out, crt_tail<N>(S, p.qwords, F, p.tab, (i64)li.bottom + ri.bottom - 2 * (32 * N - 1), p.subtract != 0, c, scratch));
 }
 
 // ---------------------------------------------------------------- 3b. CRT on the tensor cores
@@ -623,7 +734,10 @@ template <int N> __global__ void __launch_bounds__(kCrtThreads, 2) crt_mma_kerne
                 const u32 st = (p.subtract ? c.st : 0u) | li.status | ri.status;
                 if (st) store<N>(out, zero<N>(st));
                 else if (!li.nonzero || !ri.nonzero || !any) store<N>(out, p.subtract ? c : zero<N>());
-                else store<N>(out, crt_tail<N>(S, p.qwords, F, p.tab, (i64)li.bottom + ri.bottom - 2 * (32 * N - 1), p.subtract != 0, c));
+                else {
+                    u32 scratch[round_sum2_words<N>(kResMaxQWords + 2)];
+                    store<N>(out, crt_tail<N>(S, p.qwords, F, p.tab, (i64)li.bottom + ri.bottom - 2 * (32 * N - 1), p.subtract != 0, c, scratch));
+                }
             }
         }
         }
@@ -782,16 +896,23 @@ template <int N> __global__ void __launch_bounds__(kDigitThreads, 1) digits_mma_
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(p.tmem_cols));
 }
 
-// The rounding half of the CRT when crt_mma_kernel wrote S and F: one thread per output, so the local-memory
-// work of crt_tail runs at full occupancy.  An output whose residues were all zero has S = F = 0, which
-// crt_tail turns into c itself (or zero), as the fused path does.
-template <int N> __global__ void __launch_bounds__(128) crt_round_kernel(const CrtParams pin) {
+// The rounding half of the CRT when crt_mma_kernel wrote S and F: one thread per output.  Each thread's S and
+// rounding window live in shared memory (crt_round_words words per thread, an odd stride so that the 32 lanes of a
+// warp touching the same word index hit 32 banks), so the data-dependent word indexing of crt_tail costs no local-
+// memory traffic to L2 and DRAM.  An output whose residues were all zero has S = F = 0, which crt_tail turns into
+// c itself (or zero), as the fused path does.
+constexpr int kCrtRoundThreads = 64;
+template <int N> __host__ __device__ constexpr int crt_round_words(int qwords) {
+    return ((qwords + 2) + round_sum2_words<N>(qwords + 2)) | 1;
+}
+template <int N> __global__ void __launch_bounds__(kCrtRoundThreads) crt_round_kernel(const CrtParams pin) {
     CrtParams p = pin;
     if (pin.plan) {
         if (pin.plan->mode != 1) return;
         p.tab = static_cast<const ResTables*>(pin.plan->tab); p.qwords = pin.plan->qwords;
     }
-    const u64 outputs = p.M * p.Nc, o = (u64)blockIdx.x * 128 + threadIdx.x;
+    extern __shared__ u32 crt_round_park[];
+    const u64 outputs = p.M * p.Nc, o = (u64)blockIdx.x * kCrtRoundThreads + threadIdx.x;
     if (o >= outputs) return;
     const u64 i = o / p.Nc, j = o % p.Nc;
     if (p.lower && j > i) return;
@@ -802,17 +923,18 @@ template <int N> __global__ void __launch_bounds__(128) crt_round_kernel(const C
     const u32 st = (p.subtract ? c.st : 0u) | li.status | ri.status;
     if (st) { store<N>(out, zero<N>(st)); return; }
     if (!li.nonzero || !ri.nonzero) { store<N>(out, p.subtract ? c : zero<N>()); return; }
-    u32 S[kResMaxQWords + 2];
+    u32* S = crt_round_park + threadIdx.x * crt_round_words<N>(p.qwords);
     for (int w = 0; w < p.qwords + 2; ++w) S[w] = p.sf[(u64)w * outputs + o];
     const u64 F = (u64)p.sf[(u64)(p.qwords + 2) * outputs + o] | ((u64)p.sf[(u64)(p.qwords + 3) * outputs + o] << 32);
-    store<N>(out, crt_tail<N>(S, p.qwords, F, p.tab, (i64)li.bottom + ri.bottom - 2 * (32 * N - 1), p.subtract != 0, c));
+    store<N>(out, crt_tail<N>(S, p.qwords, F, p.tab, (i64)li.bottom + ri.bottom - 2 * (32 * N - 1), p.subtract != 0, c, S + p.qwords + 2));
 }
 
 typedef void (*DigitFn)(const DigitParams&, cudaStream_t);
 typedef void (*RecFn)(const RecParams&, cudaStream_t);
 typedef void (*CrtFn)(const CrtParams&, unsigned grid, size_t smem, cudaStream_t);
 typedef void (*DigitMmaFn)(const DigitMmaParams&, unsigned grid, size_t smem, cudaStream_t);
-struct ResidueKernels { DigitFn digits; RecFn rec; CrtFn crt; DigitMmaFn digits_mma; };
+typedef void (*WindowDotFn)(const WinParams&, cudaStream_t);
+struct ResidueKernels { DigitFn digits; RecFn rec; CrtFn crt; DigitMmaFn digits_mma; WindowDotFn window_dot; };
 const ResidueKernels* residue_kernels(int limbs);
 
 template <int N> void digits_launch(const DigitParams& p, cudaStream_t s) {
@@ -824,12 +946,25 @@ template <int N> void crt_launch(const CrtParams& p, unsigned grid, size_t smem,
     if (!p.M || !p.Nc) return;
     cudaFuncSetAttribute(crt_mma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     crt_mma_kernel<N><<<grid, kCrtThreads, smem, s>>>(p);
-    if (p.sf) crt_round_kernel<N><<<(unsigned)((p.M * p.Nc + 127) / 128), 128, 0, s>>>(p);
+    if (p.sf) {
+        // the planned form learns qwords on the GPU: size the rounding scratch for the largest table
+        const int qw = p.plan ? kResMaxQWords : p.qwords;
+        const size_t rsmem = (size_t)kCrtRoundThreads * crt_round_words<N>(qw) * 4;
+        if (rsmem > 48 * 1024) cudaFuncSetAttribute(crt_round_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem);
+        crt_round_kernel<N><<<(unsigned)((p.M * p.Nc + kCrtRoundThreads - 1) / kCrtRoundThreads), kCrtRoundThreads, rsmem, s>>>(p);
+    }
 }
 template <int N> void digits_mma_launch(const DigitMmaParams& p, unsigned grid, size_t smem, cudaStream_t s) {
     if (!p.rows_pad || !p.Kp) return;
     cudaFuncSetAttribute(digits_mma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     digits_mma_kernel<N><<<grid, kDigitThreads, smem, s>>>(p);
+}
+template <int N> void window_dot_launch(const WinParams& p, cudaStream_t s) {
+    if (!p.d.M || !p.d.Nc) return;
+    const size_t smem = win_smem_bytes<N>();
+    if (smem > 48 * 1024) cudaFuncSetAttribute(window_dot_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 grid((unsigned)((p.d.Nc + kWinTN - 1) / kWinTN), (unsigned)((p.d.M + kWinTM - 1) / kWinTM));
+    window_dot_kernel<N><<<grid, kWinThreads, smem, s>>>(p);
 }
 template <int N> void rec_launch(const RecParams& p, cudaStream_t s) {
     if (!p.M || !p.Nc) return;
@@ -841,5 +976,5 @@ template <int N> void rec_launch(const RecParams& p, cudaStream_t s) {
 
 #define LF_RESIDUE_INSTANTIATE(N)                                                                  \
     namespace lfd {                                                                                \
-    extern const ResidueKernels residue_kernels_##N; const ResidueKernels residue_kernels_##N = {digits_launch<N>, rec_launch<N>, crt_launch<N>, digits_mma_launch<N>}; \
+    extern const ResidueKernels residue_kernels_##N; const ResidueKernels residue_kernels_##N = {digits_launch<N>, rec_launch<N>, crt_launch<N>, digits_mma_launch<N>, window_dot_launch<N>}; \
     }

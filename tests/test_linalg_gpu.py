@@ -74,6 +74,30 @@ def test_products_vs_oracle(la, oracle, bits, kind):
         assert same(Cs, ws), f"syrk update {kind} s={s} bad {bad(Cs, ws)}"
 
 
+@pytest.mark.parametrize("bits", [64, 256, 512, 1024])
+@pytest.mark.parametrize("kind", KINDS)
+def test_limb_kernel_products_vs_oracle(la_limb, oracle, bits, kind):
+    """The tiled limb kernel (per-output exact windows, cluster method for wide outputs) on every matrix kind:
+    GEMM updates with adversarial old entries, plain GEMM and SYRK, against the oracle."""
+    rng = np.random.default_rng(7000 + bits + KINDS.index(kind))
+    for m, n, k in ((9, 13, 21), (17, 8, 40)):
+        L = matrix(bits, k, m, kind, rng)
+        R = matrix(bits, k, n, kind, rng)
+        want = oracle.gemm(bits, True, L, R, m, n, k)
+        C = np.zeros((m * n, bits // 32 + 3), np.uint32)
+        la_limb.gemm(bits, True, L, R, m, n, k, C)
+        assert same(C, want), f"gemm {kind} bad {bad(C, want)}"
+        old = old_entries(bits, want, rng)
+        Cu = old.copy()
+        la_limb.gemm(bits, True, L, R, m, n, k, Cu, subtract=True)
+        wu = oracle.gemm(bits, True, L, R, m, n, k, C=old, subtract=True)
+        assert same(Cu, wu), f"gemm update {kind} bad {bad(Cu, wu)}"
+        S = np.zeros((m * m, bits // 32 + 3), np.uint32)
+        la_limb.syrk(bits, L, k, m, S, lower_only=True)
+        assert same(S, oracle.syrk(bits, L, k, m, C=np.zeros_like(S), lower_only=True)), f"syrk {kind}"
+    assert la_limb.report()["method"] == 1
+
+
 def test_limb_and_auto_engines_agree(la, la_limb, oracle):
     bits, m, n, k = 512, 40, 37, 129
     rng = np.random.default_rng(3)

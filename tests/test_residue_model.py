@@ -29,8 +29,9 @@ def aligned(x, bottom, n):
     return s * (m << (e - bottom)) if s else 0
 
 
-def model_dot(bits, A, B, K):
-    """X = sum_k a_k b_k as the engine computes it, plus its scale."""
+def model_dot(bits, A, B, K, drop=0):
+    """X = sum_k a_k b_k as the engine computes it, plus its scale (drop: use that many moduli fewer than the
+    count rule gives, to show the rule is needed)."""
     n = bits // 32
     ea = [int(v) for v in nb.exponent(A[nb.sign(A) != 0])]
     eb = [int(v) for v in nb.exponent(B[nb.sign(B) != 0])]
@@ -44,6 +45,7 @@ def model_dot(bits, A, B, K):
             break
         mods.append(m)
         have += math.log2(m)
+    mods = mods[:len(mods) - drop]
     X = [aligned(A[k], ba, n) for k in range(K)]
     Y = [aligned(B[k], bb, n) for k in range(K)]
     residues = []
@@ -127,3 +129,20 @@ def test_digit_split_bounds():
     r = (65521 - 1) // 2
     lo = ((r & 0xff) ^ 0x80) - 0x80
     assert (r - lo) >> 8 == 128
+
+
+@pytest.mark.parametrize("bits,K", [(64, 17), (256, 65), (512, 1001)])
+def test_one_modulus_fewer_breaks_a_saturated_sum(bits, K):
+    """Saturated sums (every significand all ones, every line's spread at the band width, all products of one
+    sign: the sum sits just under the bound the count rule covers): the rule's modulus count reconstructs the
+    exact sum and one modulus fewer does not (test_linalg.cpp:175-184, tight-modulus cases)."""
+    n = bits // 32
+    A = np.zeros((K, n + 3), np.uint32)
+    A[:, :n] = 0xFFFFFFFF
+    nb.set_fields(A, 0, 1)
+    A[K - 1, n] = np.int32(-40).view(np.uint32)           # one low entry per line: spread 40
+    exact = sum(aligned(A[k], -40, n) ** 2 for k in range(K))
+    X, _, _ = model_dot(bits, A, A, K)
+    assert X == exact
+    X1, _, _ = model_dot(bits, A, A, K, drop=1)
+    assert X1 != exact
