@@ -573,6 +573,28 @@ def run_ours(args, rank, world, local_rank):
             ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
+    # A/B of the warp-cooperative form: one value per lane pair (same bits), timed the same way on rank 0's data
+    lanes_ab = None
+    if world == 1:
+        dpair = torch.empty_like(dx)
+
+        def pair_step():
+            api.dev_mul_chain_lanes(BITS, 2, dx.data_ptr(), df.data_ptr(), COUNT, CHAIN, dpair.data_ptr(), COUNT, stream=sp)
+        with torch.cuda.stream(stream):
+            for _ in range(max(3, args.warmup)):
+                pair_step()
+        torch.cuda.synchronize()
+        pair_same = bool(torch.equal(dpair, dout))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(args.steps):
+                pair_step()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        lanes_ab = {"one_value_per_thread_ms": ms / args.steps, "one_value_per_lane_pair_ms": e0.elapsed_time(e1) / args.steps,
+                    "lane_pair_bits_identical": pair_same}
+        del dpair
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -648,6 +670,7 @@ def run_ours(args, rank, world, local_rank):
                          "sample": f"{sample} of {COUNT} values x {CHAIN} steps, extrapolated",
                          "mpfr": mpfr},
         "chain_full_match": chain_full_match,
+        "chain_lanes_ab": lanes_ab,
     }
     if mpfr.get("all_core_ops_per_s"):
         line["vs_mpfr_all_core"] = {"value": value / mpfr["all_core_ops_per_s"], "e2e": e2e_value / mpfr["all_core_ops_per_s"],

@@ -189,6 +189,11 @@ int lf_dev_elementwise(int bits, int op, const void* a, const void* b, const voi
  * factors: steps arrays of count elements at factors + s * factor_stride elements. */
 int lf_dev_mul_chain(int bits, const void* x, const void* factors, size_t factor_stride, unsigned steps, void* out,
                      size_t count, void* stream);
+/* The same with a choice of lanes per value (no reference counterpart): 1, one value per thread; 2, one value per
+ * lane pair, each lane forming half of every product's rows and one shuffle exchange per product (even widths of
+ * 384 bits and more, contiguous factors; other chains run one value per thread).  Identical bits either way. */
+int lf_dev_mul_chain_lanes(int bits, int lanes, const void* x, const void* factors, size_t factor_stride, unsigned steps,
+                           void* out, size_t count, void* stream);
 
 /* ---- Resident products (linalg.hpp:60-66,190-195): Linalg::syrk / gemm recorded into a CommandBatch on
  * buffers of the Linalg's engine (row-major, sizes as the host calls).  Line analysis, the choice of engine

@@ -247,6 +247,7 @@ def _load() -> C.CDLL:
         "lf_dev_elementwise": ([I, I, V, V, V, V, S, _Broadcast, _Broadcast, V], I),
         "lf_host_alloc": ([S, P(V)], I), "lf_host_free": ([V], None),
         "lf_dev_mul_chain": ([I, V, V, S, C.c_uint, V, S, V], I),
+        "lf_dev_mul_chain_lanes": ([I, I, V, V, S, C.c_uint, V, S, V], I),
         "lf_linalg_create": ([V, P(_LinalgOptions), P(V)], I), "lf_linalg_destroy": ([V], None),
         "lf_linalg_get_report": ([V, P(_LinalgReport)], I),
         "lf_linalg_gemm": ([V, I, I, V, V, S, S, S, V, I, P(_Timing)], I),
@@ -819,6 +820,11 @@ def dev_elementwise(bits, op, a_ptr, b_ptr, c_ptr, out_ptr, count, b_index=None,
 def dev_mul_chain(bits, x_ptr, factors_ptr, factor_stride, steps, out_ptr, count, stream=0) -> None:
     check(lib.lf_dev_mul_chain(bits, _ptr(x_ptr), _ptr(factors_ptr), factor_stride, steps, _ptr(out_ptr), count,
                                C.c_void_p(stream)))
+
+
+def dev_mul_chain_lanes(bits, lanes, x_ptr, factors_ptr, factor_stride, steps, out_ptr, count, stream=0) -> None:
+    check(lib.lf_dev_mul_chain_lanes(bits, lanes, _ptr(x_ptr), _ptr(factors_ptr), factor_stride, steps, _ptr(out_ptr), count,
+                                     C.c_void_p(stream)))
 
 
 def dev_cast(from_bits, to_bits, complex_, in_ptr, out_ptr, count, stream=0) -> None:

@@ -16,7 +16,7 @@ struct EwParams {
 struct ChainStep { const u32* b; u32* out; u64 bs, bp; int op; int pad; };
 constexpr int kMaxChain = 32;
 struct ChainParams {
-    const u32* a; u64 count; int steps; int pad;
+    const u32* a; u64 count; int steps; int lanes;      // lanes: 2 runs stageable multiplication chains on lane pairs
     ChainStep step[kMaxChain];
 };
 
@@ -130,6 +130,92 @@ template <int N> __global__ void __launch_bounds__(kStagedThreads) chain_staged_
         __syncthreads();                                     // the tile is refilled for step s + 2
     }
 }
+// ---- Lane pairs: one value over two lanes (N even, N >= 12).  Both lanes hold the running value a.  Lane p forms
+// the rows j = 2m + p of the upper part T of a * y (the products a_i y_j with i + j >= N - 2, as mant_mul_high_mem),
+// each row a carry chain, into its own window; lane p's window index w'' stands for word w'' - 1 + p of T, which
+// keeps every index static.  Lane 1's row 2m + 1 starts one product earlier than lane 0's row 2m; lane 0 takes that
+// product with a zero operand.  One exchange of the windows (a shuffle per word) gives both lanes T, and both round
+// it exactly as mul does, so the pair ends the step holding RN(a * y) bit for bit as one thread would.
+template <int N> __device__ __forceinline__ Num<N> mul_pair(const Num<N>& a, const u32* y, int pl) {
+    static_assert(N % 2 == 0 && N >= kShortMulLimbs, "lane pairs need an even width of at least kShortMulLimbs");
+    constexpr int B = N - 2, W = N + 2;
+    const int ys = (int)y[N + 1];
+    const u32 st = a.st | y[N + 2];
+    if (st || !a.s || !ys) return zero<N>(st);
+    u32 h[W + 1];
+#pragma unroll
+    for (int k = 0; k <= W; ++k) h[k] = 0;
+#pragma unroll
+    for (int m = 0; m < N / 2; ++m) {
+        const u32 bj = y[2 * m + pl];
+        const int i1 = B - 2 * m - 1 > 0 ? B - 2 * m - 1 : 0;           // lane 1's first product (static)
+        const bool mask0 = B - 2 * m - 1 >= 0;                           // lane 0 starts one later: zero operand
+        u32 c = 0;
+#pragma unroll
+        for (int i = i1; i < N; ++i) {
+            const u32 ai = (i == i1 && mask0 && !pl) ? 0u : a.m[i];
+            const u64 t = (u64)ai * bj + h[i + 2 * m - B + 1] + c;
+            h[i + 2 * m - B + 1] = (u32)t;
+            c = (u32)(t >> 32);
+        }
+        h[2 * m + 3] = c;                                                // N - 1 + 2m - B + 2
+    }
+    // T word w = h0[w + 1] + h1[w]: each lane sends its share of word w and adds the partner's
+    u32 cy = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+        const u32 mine = pl ? h[w] : h[w + 1];
+        const u32 other = __shfl_xor_sync(0xffffffffu, mine, 1);
+        const u64 t = (u64)mine + other + cy;
+        h[w] = (u32)t;
+        cy = (u32)(t >> 32);
+    }
+    const u32 sh = (h[N + 1] >> 31) ? 0u : 1u;
+    const u32 lw = h[1] << sh;
+    const u32 low = lw & 0x7fffffffu;
+    const bool rb = lw >> 31;
+    if (low >= 0x80000000u - ((u32)N << sh) || (rb && low == 0)) return mul_exact_mem_call<N>(a, y);
+    u32 m[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) m[i] = __funnelshift_l(h[i + 1], h[i + 2], sh);
+    return finish<N>(m, (i64)a.e + (int)y[N] + 1 - (i64)sh, a.s * ys, rb, 0);
+}
+constexpr int kPairThreads = 64;                          // 32 values per block
+template <int N> __global__ void __launch_bounds__(kPairThreads, 10) chain_pair_kernel(const __grid_constant__ ChainParams p) {
+    constexpr u64 E = N + 3;
+    constexpr int V = kPairThreads / 2, TILE = V * (int)E, CH = TILE / 4;
+    static_assert(TILE % 4 == 0, "tiles of whole 16-byte chunks");
+    const int pl = threadIdx.x & 1, vi = threadIdx.x >> 1;
+    const u64 base = (u64)blockIdx.x * V, i = base + vi;
+    if (base + V > p.count) {                                       // partial block: factors straight from memory
+        if (i >= p.count) return;                                    // both lanes of a pair leave together
+        Num<N> v = load_plain<N>(p.a + E * i);
+#pragma unroll 1
+        for (int s = 0; s < p.steps; ++s) {
+            v = mul_pair<N>(v, p.step[s].b + E * i, pl);
+            if (p.step[s].out && !pl) store<N>(p.step[s].out + E * i, v);
+        }
+        return;
+    }
+    extern __shared__ __align__(16) u32 pair_stage[];
+    const auto fetch = [&](int s) {
+        const u32* src = p.step[s].b + E * base;
+        u32* dst = pair_stage + (s & 1) * TILE;
+        for (int c = threadIdx.x; c < CH; c += kPairThreads) cp_async16(dst + 4 * c, src + 4 * c);
+        cp_async_commit();
+    };
+    fetch(0);
+    Num<N> v = load_plain<N>(p.a + E * i);
+#pragma unroll 1
+    for (int s = 0; s < p.steps; ++s) {
+        if (s + 1 < p.steps) { fetch(s + 1); cp_async_wait<1>(); } else cp_async_wait<0>();
+        __syncthreads();
+        v = mul_pair<N>(v, pair_stage + (s & 1) * TILE + vi * E, pl);
+        if (p.step[s].out && !pl) store<N>(p.step[s].out + E * i, v);
+        __syncthreads();
+    }
+}
+
 // The staged kernel applies when every factor is contiguous, 16-byte aligned and disjoint from every output.
 inline bool chain_can_stage(const ChainParams& p, u64 E) {
     const u64 bytes = p.count * E * 4;
@@ -173,6 +259,13 @@ template <int N> int launch_chain(const ChainParams& p, cudaStream_t s) {
     bool mul_only = true;
     for (int k = 0; k < p.steps; ++k) mul_only = mul_only && p.step[k].op == 2;
     if (mul_only && chain_can_stage(p, N + 3)) {
+        if constexpr (N % 2 == 0 && N >= kShortMulLimbs) {
+            if (p.lanes == 2) {
+                const unsigned pb = (unsigned)((p.count + kPairThreads / 2 - 1) / (kPairThreads / 2));
+                chain_pair_kernel<N><<<pb, kPairThreads, 2 * (kPairThreads / 2) * (N + 3) * 4, s>>>(p);
+                return 0;
+            }
+        }
         const unsigned sb = (unsigned)((p.count + kStagedThreads - 1) / kStagedThreads);
         chain_staged_kernel<N><<<sb, kStagedThreads, 2 * kStagedThreads * (N + 3) * 4, s>>>(p);
     } else if (mul_only) chain_kernel<N, true><<<blocks, kChainThreads, 0, s>>>(p);     // registers of mul alone

@@ -1,6 +1,4 @@
-// Element-wise kernel instantiations for limb counts: 25 26 27 28 (split so the widths compile in parallel).
+// Element-wise kernel instantiations for limb counts: 25 26 (split so the widths compile in parallel).
 #include "lf_elementwise.cuh"
 LF_EW_INSTANTIATE(25)
 LF_EW_INSTANTIATE(26)
-LF_EW_INSTANTIATE(27)
-LF_EW_INSTANTIATE(28)

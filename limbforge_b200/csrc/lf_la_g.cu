@@ -1,14 +1,8 @@
-// Exact product, factorization and residue-engine kernel instantiations for limb counts 29..32.
+// Exact product, factorization and residue-engine kernel instantiations for limb counts 26..27.
 #include "lf_residue.cuh"
-LF_LINALG_INSTANTIATE(29)
-LF_FACTOR_INSTANTIATE(29)
-LF_RESIDUE_INSTANTIATE(29)
-LF_LINALG_INSTANTIATE(30)
-LF_FACTOR_INSTANTIATE(30)
-LF_RESIDUE_INSTANTIATE(30)
-LF_LINALG_INSTANTIATE(31)
-LF_FACTOR_INSTANTIATE(31)
-LF_RESIDUE_INSTANTIATE(31)
-LF_LINALG_INSTANTIATE(32)
-LF_FACTOR_INSTANTIATE(32)
-LF_RESIDUE_INSTANTIATE(32)
+LF_LINALG_INSTANTIATE(26)
+LF_FACTOR_INSTANTIATE(26)
+LF_RESIDUE_INSTANTIATE(26)
+LF_LINALG_INSTANTIATE(27)
+LF_FACTOR_INSTANTIATE(27)
+LF_RESIDUE_INSTANTIATE(27)

@@ -22,32 +22,59 @@ struct Linalg {
     DevBuf work[6];
     DevBuf info_buf, error_buf, lines;
     ResidueEngine residue;
+    // the factorizations' second product lane: trailing updates beyond the next block run on `side` while the
+    // next panel runs on the engine's stream (look-ahead), with their own residue-engine workspaces
+    ResidueEngine residue2;
+    DevBuf lines2;
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_panel = nullptr, ev_side = nullptr;
     std::vector<std::weak_ptr<ResidentProduct>> resident;   // recorded resident products, for workspaces()
+    ~Linalg() {
+        if (ev_panel) cudaEventDestroy(ev_panel);
+        if (ev_side) cudaEventDestroy(ev_side);
+        if (side) cudaStreamDestroy(side);
+    }
 };
 
 using Clock = std::chrono::steady_clock;
 static double since(Clock::time_point t) { return std::chrono::duration<double>(Clock::now() - t).count(); }
 static void check_bits(int bits) { if (bits < 64 || bits > 1024 || bits % 32) throw invalid_argument("bits must be a multiple of 32 in [64,1024]"); }
 
-// C (M x Nc at ldc) <- RN(C - L R^T) (subtract) or RN(L R^T), L/R given as line views; lower: only j <= i.
-void exact_product(Linalg& la, int bits, lfd::LineView left, lfd::LineView right, uint64_t M, uint64_t Nc, uint64_t K,
-                   uint32_t* C, uint64_t ldc, bool subtract, bool lower, cudaStream_t s, int* method_used) {
+// Workspaces of one stream of exact products: residue engine, line analysis and the error word.
+struct ProductLane { ResidueEngine* residue; DevBuf* lines; uint32_t* err; };
+// The main lane (the engine's stream; error word 1 of the Linalg's error buffer; word 0 belongs to the panel and
+// solve kernels of a factorization) and the factorizations' side lane (error word 2).
+static ProductLane main_lane(Linalg& la) { return {&la.residue, &la.lines, static_cast<uint32_t*>(la.error_buf.get(16)) + 1}; }
+static ProductLane side_lane(Linalg& la) {
+    if (!la.side) {
+        cuda_check(cudaStreamCreateWithFlags(&la.side, cudaStreamNonBlocking), "stream");
+        cuda_check(cudaEventCreateWithFlags(&la.ev_panel, cudaEventDisableTiming), "event");
+        cuda_check(cudaEventCreateWithFlags(&la.ev_side, cudaEventDisableTiming), "event");
+    }
+    return {&la.residue2, &la.lines2, static_cast<uint32_t*>(la.error_buf.get(16)) + 2};
+}
+
+// C (M x Nc at ldc) <- RN(C - L R^T) (subtract) or RN(L R^T), L/R given as line views; lower: only j <= i.  On `lane`
+// and stream s; with `check`, the call waits for the product and raises a cluster overflow, otherwise the caller reads
+// the lane's error word later (its word is not cleared here then).
+void exact_product_on(Linalg& la, const ProductLane& lane, int bits, lfd::LineView left, lfd::LineView right, uint64_t M,
+                      uint64_t Nc, uint64_t K, uint32_t* C, uint64_t ldc, bool subtract, bool lower, cudaStream_t s,
+                      int* method_used, bool check) {
     if (!M || !Nc) return;
     const int n = bits / 32;
-    // word 1 of the error buffer: word 0 belongs to the panel and solve kernels of a factorization
-    uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16)) + 1;
-    cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
+    uint32_t* err = lane.err;
+    if (check) cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
     int method = la.options.method;                    // 0 auto, 1 limb kernel, 2 residue engine
     bool used_residue = false;
     if (method != 1 && !la.options.force_fallback)
-        used_residue = la.residue.run(bits, left, right, M, Nc, K, C, ldc, subtract, lower, err, s, method == 2, la.report);
+        used_residue = lane.residue->run(bits, left, right, M, Nc, K, C, ldc, subtract, lower, err, s, method == 2, la.report);
     if (!used_residue) {
         // the tiled limb kernel: line analysis, then one exact window per output (cluster method for wide outputs)
         lfd::WinParams wp{};
         lfd::DotParams& p = wp.d;
         p.left = left; p.right = right; p.C = C; p.ldc = ldc; p.M = M; p.Nc = Nc; p.K = K;
         p.row0 = 0; p.col0 = 0; p.subtract = subtract; p.lower = lower; p.error = err;
-        auto* linfo = static_cast<lfd::LineInfo*>(la.lines.get(sizeof(lfd::LineInfo) * (M + Nc) + 64));
+        auto* linfo = static_cast<lfd::LineInfo*>(lane.lines->get(sizeof(lfd::LineInfo) * (M + Nc) + 64));
         lfd::linalg_kernels(n)->analyze(left, M, K, linfo, s);
         lfd::linalg_kernels(n)->analyze(right, Nc, K, linfo + M, s);
         wp.linfo = linfo; wp.rinfo = linfo + M;
@@ -55,10 +82,15 @@ void exact_product(Linalg& la, int bits, lfd::LineView left, lfd::LineView right
         cuda_check(cudaGetLastError(), "exact product launch");
     }
     if (method_used) *method_used = used_residue ? 2 : 1;
+    if (!check) return;
     uint32_t e = 0;
     cuda_check(cudaMemcpyAsync(&e, err, 4, cudaMemcpyDeviceToHost, s), "error flag");
     cuda_check(cudaStreamSynchronize(s), "exact product");
     if (e) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+}
+void exact_product(Linalg& la, int bits, lfd::LineView left, lfd::LineView right, uint64_t M, uint64_t Nc, uint64_t K,
+                   uint32_t* C, uint64_t ldc, bool subtract, bool lower, cudaStream_t s, int* method_used) {
+    exact_product_on(la, main_lane(la), bits, left, right, M, Nc, K, C, ldc, subtract, lower, s, method_used, true);
 }
 
 static void validate_dims(size_t M, size_t Nc, size_t K, size_t stride) {
@@ -199,7 +231,11 @@ namespace lfr {
 
 // Blocked right-looking Cholesky of the device matrix W (n x n, already holding A's lower triangle):
 // panels on the GPU (diagonal block, then the rows below), trailing updates as exact SYRK products
-// of one rounding per entry (linalg.mm:411-457 sequence).
+// of one rounding per entry (linalg.mm:411-457 sequence).  Look-ahead: block k's trailing update is split into
+// the next block column (rows k1.., columns [k1, k2), on the engine's stream, so the next panel follows it there)
+// and the rest (rows and columns k2.., on the side stream), which runs while the next panel is factored.  Every
+// entry still receives block 0's update, then block 1's, ... in order: the next block column's update waits for the
+// previous remainder update, which covered those columns too.
 static lf_cholesky_info cholesky_device(Linalg& la, int bits, uint32_t* W, size_t n, size_t block) {
     lf_cholesky_info info{};
     info.pivot = n;
@@ -212,10 +248,13 @@ static lf_cholesky_info cholesky_device(Linalg& la, int bits, uint32_t* W, size_
     const size_t nb = block ? std::min(block, n) : n;
     long long* dinfo = static_cast<long long*>(la.info_buf.get(64));
     uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));
-    cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
+    cuda_check(cudaMemsetAsync(err, 0, 16, s), "memset");
+    const ProductLane lane_a = main_lane(la), lane_b = side_lane(la);
+    cudaStream_t s2 = la.side;
     cudaEvent_t g0, g1;
     cuda_check(cudaEventCreate(&g0), "event"); cuda_check(cudaEventCreate(&g1), "event");
     cuda_check(cudaEventRecord(g0, s), "event");
+    bool side_pending = false;                           // a remainder update is queued on s2 (ev_side after it)
     size_t fail = n;
     for (size_t k0 = 0; k0 < n && fail == n; k0 += nb) {
         const size_t k1 = std::min(n, k0 + nb);
@@ -240,31 +279,47 @@ static lf_cholesky_info cholesky_device(Linalg& la, int bits, uint32_t* W, size_
         }
         fk->rows(p, k1, k1, s);
         cuda_check(cudaGetLastError(), "cholesky panel rows");
-        cuda_check(cudaStreamSynchronize(s), "panel");
         info.panel_seconds += since(t);
         if (k1 < n) {
             t = Clock::now();
-            const size_t m = n - k1;
-            lfd::LineView v{W + (k1 * n + k0) * E, n, 1};
-            exact_product(la, bits, v, v, m, m, k1 - k0, W + (k1 * n + k1) * E, n, true, true, s, nullptr);
+            const size_t k2 = std::min(n, k1 + nb);
+            cuda_check(cudaEventRecord(la.ev_panel, s), "event");               // panel k0 complete
+            // the next block column: rows [k1, n) x columns [k1, k2), after the previous remainder update
+            if (side_pending) cuda_check(cudaStreamWaitEvent(s, la.ev_side, 0), "event wait");
+            lfd::LineView rows_k1{W + (k1 * n + k0) * E, n, 1}, rows_k1b{W + (k1 * n + k0) * E, n, 1};
+            exact_product_on(la, lane_a, bits, rows_k1, rows_k1b, n - k1, k2 - k1, k1 - k0, W + (k1 * n + k1) * E, n, true, true, s,
+                             nullptr, false);
+            // the rest: rows and columns [k2, n), on the side stream after the panel
+            if (k2 < n) {
+                cuda_check(cudaStreamWaitEvent(s2, la.ev_panel, 0), "event wait");
+                lfd::LineView rows_k2{W + (k2 * n + k0) * E, n, 1};
+                exact_product_on(la, lane_b, bits, rows_k2, rows_k2, n - k2, n - k2, k1 - k0, W + (k2 * n + k2) * E, n, true, true, s2,
+                                 nullptr, false);
+                cuda_check(cudaEventRecord(la.ev_side, s2), "event");
+                side_pending = true;
+            }
             ++info.gpu_updates;
             info.update_seconds += since(t);
         }
     }
+    if (side_pending) cuda_check(cudaStreamWaitEvent(s, la.ev_side, 0), "event wait");
     if (fail < n) fk->prep(nullptr, W, n, fail, s);
     cuda_check(cudaGetLastError(), "cholesky clear");
     cuda_check(cudaEventRecord(g1, s), "event");
-    uint32_t ev = 0;
-    cuda_check(cudaMemcpyAsync(&ev, err, 4, cudaMemcpyDeviceToHost, s), "error flag");
+    uint32_t ev[3] = {0, 0, 0};
+    cuda_check(cudaMemcpyAsync(ev, err, 12, cudaMemcpyDeviceToHost, s), "error flag");
     cuda_check(cudaStreamSynchronize(s), "cholesky");
     float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
     cudaEventDestroy(g0); cudaEventDestroy(g1);
-    if (ev) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    if (ev[0] | ev[1] | ev[2]) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
     info.timing = {ms * 1e-3, since(w0)};
     return info;
 }
 
-// X (device, n x nrhs) holds B; passes 1 forward, 2 backward (L^T), 3 both (linalg.mm:459-488).
+// X (device, n x nrhs) holds B; passes 1 forward, 2 backward (L^T), 3 both (linalg.mm:459-488).  Look-ahead as
+// in the factorization: after the diagonal block of rows [r0, r1), the update of the next block's rows runs on the
+// engine's stream (the next diagonal block follows it there) and the update of the rows beyond on the side stream,
+// while the next diagonal block is solved; each row still receives the blocks' updates in order.
 static double solve_device(Linalg& la, int bits, const uint32_t* L, size_t n, uint32_t* X, size_t nrhs, size_t block, int passes) {
     if (!n || !nrhs) return 0;
     Engine& e = *la.engine;
@@ -274,40 +329,63 @@ static double solve_device(Linalg& la, int bits, const uint32_t* L, size_t n, ui
     const auto* fk = lfd::factor_kernels(limbs);
     const size_t nb = block ? std::min(block, n) : n;
     uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));      // word 0: the solve kernels' flag
-    cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
+    cuda_check(cudaMemsetAsync(err, 0, 16, s), "memset");
+    const ProductLane lane_a = main_lane(la), lane_b = side_lane(la);
+    cudaStream_t s2 = la.side;
     cudaEvent_t g0, g1;
     cuda_check(cudaEventCreate(&g0), "event"); cuda_check(cudaEventCreate(&g1), "event");
     cuda_check(cudaEventRecord(g0, s), "event");
+    bool side_pending = false;
+    // rows [a, b) of X updated by the block [r0, r1): X[a..b) -= L(a..b, r0..r1) X[r0..r1) (forward), or with the
+    // columns of L (backward, line i = column i of L from row r0)
+    auto update = [&](bool forward, size_t r0, size_t r1, size_t a, size_t b, const ProductLane& lane, cudaStream_t st) {
+        if (a >= b) return;
+        const lfd::LineView lv = forward ? lfd::LineView{L + (a * n + r0) * E, n, 1} : lfd::LineView{L + (r0 * n + a) * E, 1, n};
+        const lfd::LineView xv{X + r0 * nrhs * E, 1, nrhs};
+        exact_product_on(la, lane, bits, lv, xv, b - a, nrhs, r1 - r0, X + a * nrhs * E, nrhs, true, false, st, nullptr, false);
+    };
+    // after the diagonal block [r0, r1): the next block's rows [na, nb_) on s, the rest [ra, rb) on s2
+    auto split = [&](bool forward, size_t r0, size_t r1, size_t na, size_t nbb, size_t ra, size_t rb) {
+        cuda_check(cudaEventRecord(la.ev_panel, s), "event");
+        if (side_pending) cuda_check(cudaStreamWaitEvent(s, la.ev_side, 0), "event wait");
+        update(forward, r0, r1, na, nbb, lane_a, s);
+        if (ra < rb) {
+            cuda_check(cudaStreamWaitEvent(s2, la.ev_panel, 0), "event wait");
+            update(forward, r0, r1, ra, rb, lane_b, s2);
+            cuda_check(cudaEventRecord(la.ev_side, s2), "event");
+            side_pending = true;
+        }
+    };
     if (passes & 1)
         for (size_t r0 = 0; r0 < n; r0 += nb) {
             const size_t r1 = std::min(n, r0 + nb);
             fk->solve(lfd::SolveParams{L, X, n, nrhs, r0, r1, 0, err}, true, s);
             cuda_check(cudaGetLastError(), "forward substitution");
             if (r1 < n) {
-                lfd::LineView lv{L + (r1 * n + r0) * E, n, 1};
-                lfd::LineView xv{X + r0 * nrhs * E, 1, nrhs};
-                exact_product(la, bits, lv, xv, n - r1, nrhs, r1 - r0, X + r1 * nrhs * E, nrhs, true, false, s, nullptr);
+                const size_t r2 = std::min(n, r1 + nb);
+                split(true, r0, r1, r1, r2, r2, n);
             }
         }
+    if (side_pending) { cuda_check(cudaStreamWaitEvent(s, la.ev_side, 0), "event wait"); side_pending = false; }
     if (passes & 2)
         for (size_t r0 = (n - 1) / nb * nb;; r0 -= nb) {
             const size_t r1 = std::min(n, r0 + nb);
             fk->solve(lfd::SolveParams{L, X, n, nrhs, r0, r1, 0, err}, false, s);
             cuda_check(cudaGetLastError(), "back substitution");
             if (r0) {
-                lfd::LineView lv{L + (r0 * n) * E, 1, n};           // line i: column i of L from row r0
-                lfd::LineView xv{X + r0 * nrhs * E, 1, nrhs};
-                exact_product(la, bits, lv, xv, r0, nrhs, r1 - r0, X, nrhs, true, false, s, nullptr);
+                const size_t q0 = r0 - nb;                     // the next block (below in the order) is [q0, r0)
+                split(false, r0, r1, q0, r0, 0, q0);
             }
             if (!r0) break;
         }
+    if (side_pending) cuda_check(cudaStreamWaitEvent(s, la.ev_side, 0), "event wait");
     cuda_check(cudaEventRecord(g1, s), "event");
-    uint32_t ev = 0;
-    cuda_check(cudaMemcpyAsync(&ev, err, 4, cudaMemcpyDeviceToHost, s), "error flag");
+    uint32_t ev[3] = {0, 0, 0};
+    cuda_check(cudaMemcpyAsync(ev, err, 12, cudaMemcpyDeviceToHost, s), "error flag");
     cuda_check(cudaStreamSynchronize(s), "solve");
     float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
     cudaEventDestroy(g0); cudaEventDestroy(g1);
-    if (ev) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    if (ev[0] | ev[1] | ev[2]) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
     return ms * 1e-3;
 }
 
@@ -588,7 +666,7 @@ void lf_linalg_ticket_destroy(lf_linalg_ticket* t) { delete t; }
 static lf_linalg_workspaces linalg_workspaces(Linalg& la) {
     lf_linalg_workspaces w{};
     for (auto& b : la.work) w.scratch_bytes += b.bytes;
-    w.scratch_bytes += la.info_buf.bytes + la.error_buf.bytes + la.lines.bytes + la.residue.bytes();
+    w.scratch_bytes += la.info_buf.bytes + la.error_buf.bytes + la.lines.bytes + la.residue.bytes() + la.lines2.bytes + la.residue2.bytes();
     for (auto& weak : la.resident) {
         auto r = weak.lock();
         if (!r) continue;
@@ -616,8 +694,9 @@ int lf_linalg_release_workspaces(lf_linalg* la, lf_linalg_workspaces* out) {
     cuda_check(cudaStreamSynchronize(la->engine->stream), "release workspaces");
     const lf_linalg_workspaces w = linalg_workspaces(*la);
     for (auto& b : la->work) b = DevBuf{};
-    la->info_buf = DevBuf{}; la->error_buf = DevBuf{}; la->lines = DevBuf{};
+    la->info_buf = DevBuf{}; la->error_buf = DevBuf{}; la->lines = DevBuf{}; la->lines2 = DevBuf{};
     la->residue.release();
+    la->residue2.release();
     auto& list = la->resident;
     for (auto& weak : list) if (auto r = weak.lock()) resident_product_release(*r);
     list.erase(std::remove_if(list.begin(), list.end(), [](const std::weak_ptr<ResidentProduct>& x) {

@@ -465,7 +465,12 @@ int lf_dev_elementwise(int bits, int op, const void* a, const void* b, const voi
 }
 int lf_dev_mul_chain(int bits, const void* x, const void* factors, size_t factor_stride, unsigned steps, void* out,
                      size_t count, void* stream) {
+    return lf_dev_mul_chain_lanes(bits, 1, x, factors, factor_stride, steps, out, count, stream);
+}
+int lf_dev_mul_chain_lanes(int bits, int lanes, const void* x, const void* factors, size_t factor_stride, unsigned steps, void* out,
+                           size_t count, void* stream) {
     LF_API_BEGIN
+    if (lanes != 1 && lanes != 2) throw invalid_argument("lanes must be 1 or 2");
     validate(bits, count);
     if (!count) return LF_OK;
     if (!x || !out || (steps && !factors)) throw invalid_argument("null arithmetic buffer");
@@ -481,6 +486,7 @@ int lf_dev_mul_chain(int bits, const void* x, const void* factors, size_t factor
         lfd::ChainParams p{};
         p.a = static_cast<const uint32_t*>(src);
         p.count = count;
+        p.lanes = lanes;
         p.steps = (int)std::min<unsigned>(lfd::kMaxChain, steps - s0);
         for (int k = 0; k < p.steps; ++k) {
             p.step[k].b = f + (size_t)(s0 + k) * factor_stride * E;

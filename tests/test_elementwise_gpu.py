@@ -144,6 +144,30 @@ def test_chain_mul_near_rounding_boundaries(oracle, bits):
     assert same(O.download(), oracle.elementwise(bits, 2, a, b))
 
 
+@pytest.mark.parametrize("bits", [384, 448, 512, 640, 832, 1024])
+def test_chain_on_lane_pairs(oracle, bits):
+    """Chains with one value per lane pair (lf_dev_mul_chain_lanes, lanes = 2): the boundary operands through a
+    one-step chain, and a 9-step chain over a count that leaves a partial block, give the oracle's bits."""
+    from limbforge_b200 import api
+    a, b = boundary_operands(bits)
+    count = a.shape[0]
+    e = api.Engine()
+    X, F, O = e.make_buffer(count, bits), e.make_buffer(count, bits), e.make_buffer(count, bits)
+    X.upload(a)
+    F.upload(b)
+    api.dev_mul_chain_lanes(bits, 2, X.device_pointer(), F.device_pointer(), count, 1, O.device_pointer(), count)
+    assert same(O.download(), oracle.elementwise(bits, 2, a, b))
+    rng = np.random.default_rng(bits + 9)
+    count, steps = 1000 + 17, 9
+    x = nb.random_numbers(rng, count, bits, 8, zero_frac=0.01, sparse_frac=0.02)
+    f = np.stack([nb.random_numbers(rng, count, bits, 8, zero_frac=0.01, sparse_frac=0.02) for _ in range(steps)])
+    X, F, O = e.make_buffer(count, bits), e.make_buffer(count * steps, bits), e.make_buffer(count, bits)
+    X.upload(x)
+    F.upload(f.reshape(count * steps, -1))
+    api.dev_mul_chain_lanes(bits, 2, X.device_pointer(), F.device_pointer(), count, steps, O.device_pointer(), count)
+    assert same(O.download(), oracle.mul_chain(bits, x, f))
+
+
 def test_chain_factor_written_earlier_in_the_chain(engine, oracle):
     """y1 = x * f, y2 = y1 * y1, y3 = y2 * f: the second step's factor is the first step's output,
     written earlier in the same fused kernel."""
