@@ -726,3 +726,297 @@ int lfo_recurrence(int bits, const word* seeds, const word* weights, word* out, 
     }
     return 0;
 }
+
+/* ---------------------------------------------------------------- Householder QR
+ * P(x, y; K) = RN(sum x_k y_k) and D(c; x, y; K) = RN(c - sum x_k y_k), one rounding each.  The
+ * sequences are the column-by-column statements the reference's own test holds its library to, bit
+ * for bit (tests/test_qr.cpp:33-68 unpivoted, :94-135 column-pivoted, :69-77 Q / Q^T, :78-86 and
+ * :137-147 least squares); the blocked right-looking library form (src/linalg.mm:488-790) gives the
+ * same bits.  Layout: A, V (m x n), R (n x n), T (blocks of nb x nb, block b at b*nb*nb, the
+ * compact-WY upper triangles), tau (n), all row-major.  info: rank, reason (0 full rank, 1 zero
+ * column, 2 small column, 3 status column), status, recomputed squared norms (pivoting). */
+static void qr_power2(word* out, int n, int32_t e) { set_zero(out, n, 0); out[n - 1] = 0x80000000u; *EXP(out, n) = e; *SGN(out, n) = 1; }
+/* x * 2^-e exactly; an exponent leaving [-1e9, 1e9] gives zero with exponent_overflow (linalg.mm:492) */
+static void qr_scaled(word* out, const word* x, int n, long e) {
+    if (!gsgn(x, n)) { copy_num(out, x, n); return; }
+    long r = (long)gexp(x, n) - e;
+    if (r > EMAX || r < -EMAX) { set_zero(out, n, gsts(x, n) | ST_OVF); return; }
+    copy_num(out, x, n); *EXP(out, n) = (int32_t)r;
+}
+#define QP(out, a, sa, b, sb, K) lfo_exact_dot_add(n, NULL, 0, (a), (long)(sa), (b), (long)(sb), (K), (out))
+#define QD(out, c, a, sa, b, sb, K) lfo_exact_dot_add(n, (c), 1, (a), (long)(sa), (b), (long)(sb), (K), (out))
+
+/* Reflector of the reduced column x (len entries, x[0] on the diagonal, stride sx): s = P(x, x); beta = -sgn(x0) sqrt(s),
+ * v0 = RN(x0 - beta), v = 2^-e (v0, x1, ...) with e = exponent(v0), tau = RN(2 / P(v, v)); nothing below the diagonal gives
+ * tau = 0, v = (1, 0, ...), beta = x0.  Returns the failure reason (0 none); v is written with stride sv. */
+static int qr_reflector(int n, word* x, long sx, size_t len, word* v, long sv, word* tau, int rank_bits, int* have_top,
+                        long* top, word* status) {
+    const size_t E = (size_t)n + 3;
+    word s[35], beta[35], v0[35], pv[35];
+    QP(s, x, sx, x, sx, len);
+    int below = 0;
+    for (size_t r = 1; r < len; ++r) below |= gsgn(x + (long)r * sx * (long)E, n) != 0;
+    int reason = gsts(s, n) ? 3 : (!gsgn(x, n) && !below) ? 1 : 0;
+    copy_num(beta, x, n); qr_power2(v0, n, 0);
+    if (!reason && below) {
+        lfo_sqrt(n, s, beta);
+        if (gsgn(x, n) >= 0) *SGN(beta, n) = -gsgn(beta, n);
+        lfo_sub(n, x, beta, v0);
+    }
+    if (!reason && rank_bits > 0 && *have_top && (long)gexp(beta, n) + rank_bits < *top) reason = 2;
+    if (reason) { *status = gsts(s, n); return reason; }
+    set_zero(tau, n, 0);
+    if (below) {
+        long e = gexp(v0, n);
+        qr_scaled(v, v0, n, e);
+        for (size_t r = 1; r < len; ++r) qr_scaled(v + (long)r * sv * (long)E, x + (long)r * sx * (long)E, n, e);
+        word two[35]; qr_power2(two, n, 1);
+        QP(pv, v, sv, v, sv, len);
+        lfo_div(n, two, pv, tau);
+    } else qr_power2(v, n, 0);
+    copy_num(x, beta, n);
+    if (!*have_top || (long)gexp(beta, n) > *top) *top = gexp(beta, n);
+    *have_top = 1;
+    return 0;
+}
+/* T column c of the block (Tb, nb x nb): T_cc = tau, T_lc = -RN(tau * P(T_l[l..c), G[l..c))) */
+static void qr_t_column(int n, word* Tb, size_t nb, size_t c, const word* tau, const word* G) {
+    const size_t E = (size_t)n + 3;
+    copy_num(Tb + (c * nb + c) * E, tau, n);
+    for (size_t l = 0; l < c; ++l) {
+        word d[35], p[35];
+        QP(d, Tb + (l * nb + l) * E, 1, G + l * E, 1, c - l);
+        lfo_mul(n, tau, d, p);
+        neg_copy(Tb + (l * nb + c) * E, p, n);
+    }
+}
+static size_t qr_nb(size_t block, size_t nn) { return block && block < nn ? block : nn; }
+
+int lfo_qr(int bits, const word* A, size_t m, size_t nn, size_t block, int rank_bits, word* R, word* V, word* T, word* tau, long* info) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3;
+    const size_t nb = qr_nb(block, nn), blocks = nb ? (nn + nb - 1) / nb : 0;
+    word* a = (word*)malloc(sizeof(word) * E * (m * nn + 1));
+    memcpy(a, A, sizeof(word) * E * m * nn);
+    memset(V, 0, sizeof(word) * E * m * nn); memset(T, 0, sizeof(word) * E * blocks * nb * nb); memset(tau, 0, sizeof(word) * E * nn);
+    word* w = (word*)malloc(sizeof(word) * E * (nb + 1)); word* y = (word*)malloc(sizeof(word) * E * (nb + 1));
+    word* G = (word*)malloc(sizeof(word) * E * (nb + 1));
+    size_t rank = nn; int reason = 0; word status = 0; int have_top = 0; long top = 0;
+#define A_(r, c) (a + ((r) * nn + (c)) * E)
+#define V_(r, c) (V + ((r) * nn + (c)) * E)
+    for (size_t j = 0; j < nn; ++j) {
+        /* column j by the reflectors [0, min(j, rank)) in groups of whole blocks: w, y, one update rounding per entry */
+        const size_t qn = j < rank ? j : rank;
+        for (size_t b0 = 0; b0 < qn; b0 += nb) {
+            const size_t kb = (b0 + nb < qn ? b0 + nb : qn) - b0;
+            const word* Tb = T + (b0 / nb) * nb * nb * E;
+#pragma omp parallel for schedule(dynamic, 1)
+            for (size_t i = 0; i < kb; ++i) QP(w + i * E, V_(b0 + i, b0 + i), nn, A_(b0 + i, j), nn, m - b0 - i);
+            for (size_t i = 0; i < kb; ++i) QP(y + i * E, Tb + i * E, nb, w, 1, i + 1);
+#pragma omp parallel for schedule(dynamic, 16)
+            for (size_t r = 0; r < m - b0; ++r) {
+                word d[35];
+                QD(d, A_(b0 + r, j), V_(b0 + r, b0), 1, y, 1, kb < r + 1 ? kb : r + 1);
+                copy_num(A_(b0 + r, j), d, n);
+            }
+        }
+        if (rank < nn) continue;
+        word t[35];
+        const int why = qr_reflector(n, A_(j, j), (long)nn, m - j, V_(j, j), (long)nn, t, rank_bits, &have_top, &top, &status);
+        if (why) { rank = j; reason = why; continue; }
+        copy_num(tau + j * E, t, n);
+        /* Gram column over the block's rows and T column */
+        const size_t b0 = j / nb * nb, c = j - b0;
+        word* Tb = T + (b0 / nb) * nb * nb * E;
+#pragma omp parallel for schedule(dynamic, 1)
+        for (size_t i = 0; i < c; ++i) QP(G + i * E, V_(b0, b0 + i), nn, V_(b0, j), nn, m - b0);
+        qr_t_column(n, Tb, nb, c, t, G);
+    }
+    for (size_t i = 0; i < nn; ++i)
+        for (size_t j = 0; j < nn; ++j) {
+            if (j >= (i < rank ? i : rank)) copy_num(R + (i * nn + j) * E, A_(i, j), n);
+            else set_zero(R + (i * nn + j) * E, n, 0);
+        }
+#undef A_
+#undef V_
+    info[0] = (long)rank; info[1] = reason; info[2] = (long)status; info[3] = 0;
+    free(a); free(w); free(y); free(G);
+    return 0;
+}
+
+/* Exact order for the pivot choice: +1 if x > y, -1 if x < y, 0 if equal; a status ranks above every value
+ * (two statuses are equal) (linalg.mm:541-547) */
+static int qr_compare(const word* x, const word* y, int n) {
+    const word sx = gsts(x, n), sy = gsts(y, n);
+    if (sx || sy) return (sx != 0) - (sy != 0);
+    const int a = gsgn(x, n), b = gsgn(y, n);
+    if (a != b) return a > b ? 1 : -1;
+    if (!a) return 0;
+    int c = gexp(x, n) != gexp(y, n) ? (gexp(x, n) > gexp(y, n) ? 1 : -1) : cmp_words(x, y, n);
+    return a > 0 ? c : -c;
+}
+static void qr_swap(word* x, word* y, int n) { word t[35]; copy_num(t, x, n); copy_num(x, y, n); copy_num(y, t, n); }
+
+/* Column-pivoted QR (xGEQP3 order, tests/test_qr.cpp:94-135): before step j the remaining column with the largest
+ * downdated squared norm nu (status first, exact comparison, ties to the lowest original index) is swapped in;
+ * column j is reduced by the block's reflectors so far (its Y entries), reflector j as unpivoted; then every
+ * trailing column k gets W_jk = P(v_j, a_k) over rows [j, m), Y_jk = P(T[.][c], W_.k), r_jk = D(a_jk; V_j[block],
+ * Y_.k) and nu_k = D(nu_k; r_jk, r_jk), recomputed from the reduced column when it drops to <= 0 or more than
+ * bits/2 binades below its last exact value.  After the block, X = D(X; V_b, Y) with those W and Y. */
+int lfo_qr_pivoted(int bits, const word* A, size_t m, size_t nn, size_t block, int rank_bits, word* R, word* V, word* T,
+                   word* tau, size_t* perm, long* info) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3;
+    const size_t nb = qr_nb(block, nn), blocks = nb ? (nn + nb - 1) / nb : 0;
+    const size_t cells = m * nn + 1;
+    word* a = (word*)malloc(sizeof(word) * E * cells);
+    memcpy(a, A, sizeof(word) * E * m * nn);
+    memset(V, 0, sizeof(word) * E * m * nn); memset(T, 0, sizeof(word) * E * blocks * nb * nb); memset(tau, 0, sizeof(word) * E * nn);
+    word* nu = (word*)calloc(E * (nn + 1), sizeof(word)); word* nuref = (word*)calloc(E * (nn + 1), sizeof(word));
+    word* Wr = (word*)calloc(E * (nb * nn + 1), sizeof(word)); word* Yr = (word*)calloc(E * (nb * nn + 1), sizeof(word));
+    word* x = (word*)malloc(sizeof(word) * E * (m + 1)); word* G = (word*)malloc(sizeof(word) * E * (nb + 1));
+    char* redo = (char*)calloc(nn + 1, 1);
+    size_t rank = nn; int reason = 0; word status = 0; int have_top = 0; long top = 0; long recomputed = 0;
+#define A_(r, c) (a + ((r) * nn + (c)) * E)
+#define V_(r, c) (V + ((r) * nn + (c)) * E)
+    for (size_t k = 0; k < nn; ++k) perm[k] = k;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (size_t k = 0; k < nn; ++k) { QP(nu + k * E, A_(0, k), nn, A_(0, k), nn, m); copy_num(nuref + k * E, nu + k * E, n); }
+    for (size_t b0 = 0; b0 < nn && rank == nn; b0 += nb) {
+        const size_t kb = (b0 + nb < nn ? b0 + nb : nn) - b0;
+        word* Tb = T + (b0 / nb) * nb * nb * E;
+        size_t g = kb;                                   /* reflectors of this block applied after it */
+        int fresh = 0;
+        for (size_t c = 0; c < kb; ++c) {
+            const size_t j = b0 + c;
+            size_t p = j;
+            for (size_t k = j + 1; k < nn; ++k) {
+                const int cmp = qr_compare(nu + k * E, nu + p * E, n);
+                if (cmp > 0 || (cmp == 0 && perm[k] < perm[p])) p = k;
+            }
+            if (p != j) {
+                for (size_t r = 0; r < m; ++r) qr_swap(A_(r, j), A_(r, p), n);
+                for (size_t i = 0; i < c; ++i) { qr_swap(Wr + (i * nn + j) * E, Wr + (i * nn + p) * E, n); qr_swap(Yr + (i * nn + j) * E, Yr + (i * nn + p) * E, n); }
+                qr_swap(nu + j * E, nu + p * E, n); qr_swap(nuref + j * E, nuref + p * E, n);
+                const size_t t = perm[j]; perm[j] = perm[p]; perm[p] = t;
+            }
+            for (size_t r = 0; r < m - b0; ++r) {
+                if (c) QD(x + r * E, A_(b0 + r, j), V_(b0 + r, b0), 1, Yr + j * E, nn, c < r + 1 ? c : r + 1);
+                else copy_num(x + r * E, A_(b0 + r, j), n);
+            }
+            word t[35];
+            const int why = qr_reflector(n, x + c * E, 1, m - j, V_(j, j), (long)nn, t, rank_bits, &have_top, &top, &status);
+            if (why) { rank = j; reason = why; g = c; fresh = 1; break; }
+            for (size_t r = 0; r < m - b0; ++r) copy_num(A_(b0 + r, j), x + r * E, n);
+            copy_num(tau + j * E, t, n);
+#pragma omp parallel for schedule(dynamic, 1)
+            for (size_t i = 0; i < c; ++i) QP(G + i * E, V_(b0, b0 + i), nn, V_(b0, j), nn, m - b0);
+            qr_t_column(n, Tb, nb, c, t, G);
+            /* trailing columns: W and Y rows c, row j of R, downdated norms */
+#pragma omp parallel for schedule(dynamic, 1)
+            for (size_t k = j + 1; k < nn; ++k) {
+                word rj[35], d[35];
+                QP(Wr + (c * nn + k) * E, V_(j, j), nn, A_(j, k), nn, m - j);
+                QP(Yr + (c * nn + k) * E, Tb + c * E, nb, Wr + k * E, nn, c + 1);
+                QD(rj, A_(j, k), V_(j, b0), 1, Yr + k * E, nn, c + 1);
+                QD(d, nu + k * E, rj, 1, rj, 1, 1);
+                copy_num(nu + k * E, d, n);
+                const word* ref = nuref + k * E;
+                redo[k] = gsgn(ref, n) && !gsts(ref, n) && !gsts(d, n) &&
+                          (gsgn(d, n) <= 0 || (long)gexp(d, n) + 16L * n < (long)gexp(ref, n));
+                if (redo[k]) {
+                    const size_t len = m - j - 1;
+                    word* z = (word*)malloc(sizeof(word) * E * (len + 1));
+                    for (size_t i = 0; i < len; ++i) QD(z + i * E, A_(j + 1 + i, k), V_(j + 1 + i, b0), 1, Yr + k * E, nn, c + 1);
+                    QP(nu + k * E, z, 1, z, 1, len);
+                    copy_num(nuref + k * E, nu + k * E, n);
+                    free(z);
+                }
+            }
+            for (size_t k = j + 1; k < nn; ++k) recomputed += redo[k] != 0;
+        }
+        /* the block's reflectors on the remaining columns: X = D(X; V_b, Y) (after a failure, W and Y formed first) */
+        const size_t c0 = rank == nn ? b0 + kb : rank;
+        if (g && c0 < nn && (rank == nn || fresh)) {
+            if (fresh)
+#pragma omp parallel for schedule(dynamic, 1)
+                for (size_t k = c0; k < nn; ++k) {
+                    for (size_t i = 0; i < g; ++i) QP(Wr + (i * nn + k) * E, V_(b0 + i, b0 + i), nn, A_(b0 + i, k), nn, m - b0 - i);
+                    for (size_t i = 0; i < g; ++i) QP(Yr + (i * nn + k) * E, Tb + i * E, nb, Wr + k * E, nn, i + 1);
+                }
+#pragma omp parallel for schedule(dynamic, 16)
+            for (size_t r = 0; r < m - b0; ++r)
+                for (size_t k = c0; k < nn; ++k) {
+                    word d[35];
+                    QD(d, A_(b0 + r, k), V_(b0 + r, b0), 1, Yr + k * E, nn, g < r + 1 ? g : r + 1);
+                    copy_num(A_(b0 + r, k), d, n);
+                }
+        }
+    }
+    for (size_t i = 0; i < nn; ++i)
+        for (size_t j = 0; j < nn; ++j) {
+            if (j >= (i < rank ? i : rank)) copy_num(R + (i * nn + j) * E, A_(i, j), n);
+            else set_zero(R + (i * nn + j) * E, n, 0);
+        }
+#undef A_
+#undef V_
+    info[0] = (long)rank; info[1] = reason; info[2] = (long)status; info[3] = recomputed;
+    free(a); free(nu); free(nuref); free(Wr); free(Yr); free(x); free(G); free(redo);
+    return 0;
+}
+
+/* C (m x nrhs) <- Q^T C (qt, blocks in order) or Q C (blocks in reverse), the blocks of reflectors [0, rank)
+ * (tests/test_qr.cpp:69-77) */
+int lfo_qr_apply(int bits, size_t m, size_t nn, size_t block, size_t rank, const word* V, const word* T, word* C, size_t nrhs, int qt) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3;
+    const size_t nb = qr_nb(block, nn), blocks = nb ? (rank + nb - 1) / nb : 0;
+    for (size_t s = 0; s < blocks; ++s) {
+        const size_t b = qt ? s : blocks - 1 - s, b0 = b * nb, kb = (b0 + nb < rank ? b0 + nb : rank) - b0;
+        const word* Tb = T + b * nb * nb * E;
+#pragma omp parallel for schedule(dynamic, 1)
+        for (size_t c = 0; c < nrhs; ++c) {
+            word* w = (word*)malloc(sizeof(word) * E * (kb + 1)); word* y = (word*)malloc(sizeof(word) * E * (kb + 1));
+            for (size_t i = 0; i < kb; ++i) QP(w + i * E, V + ((b0 + i) * nn + b0 + i) * E, nn, C + ((b0 + i) * nrhs + c) * E, nrhs, m - b0 - i);
+            for (size_t i = 0; i < kb; ++i) {
+                if (qt) QP(y + i * E, Tb + i * E, nb, w, 1, i + 1);
+                else QP(y + i * E, Tb + (i * nb + i) * E, 1, w + i * E, 1, kb - i);
+            }
+            for (size_t r = b0; r < m; ++r) {
+                word d[35];
+                QD(d, C + (r * nrhs + c) * E, V + (r * nn + b0) * E, 1, y, 1, kb < r - b0 + 1 ? kb : r - b0 + 1);
+                copy_num(C + (r * nrhs + c) * E, d, n);
+            }
+            free(w); free(y);
+        }
+    }
+    return 0;
+}
+/* Least squares X (n x nrhs) from B (m x nrhs): Q^T B, then the blocked backward substitution with R (tests/test_qr.cpp:
+ * 78-86); pivoted (perm != NULL): R[0:p,0:p] z = (Q^T b)[0:p) with blocks min(nb, p), x[perm[i]] = z_i, zero beyond p
+ * (:137-147).  A rank-deficient unpivoted factor gives zero with invalid everywhere, a status column zero with invalid
+ * and its status. */
+int lfo_qr_solve(int bits, size_t m, size_t nn, size_t block, const long* info, const size_t* perm, const word* R,
+                 const word* V, const word* T, const word* B, size_t nrhs, word* X) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3;
+    const size_t p = (size_t)info[0];
+    if (!nn || !nrhs) return 0;
+    if (p < nn && (!perm || info[1] == 3)) {
+        for (size_t q = 0; q < nn * nrhs; ++q) set_zero(X + q * E, n, ST_INVALID | (perm ? (word)info[2] : 0));
+        return 0;
+    }
+    word* C = (word*)malloc(sizeof(word) * E * m * nrhs);
+    memcpy(C, B, sizeof(word) * E * m * nrhs);
+    lfo_qr_apply(bits, m, nn, block, p, V, T, C, nrhs, 1);
+    /* the backward substitution of the upper R is the L^T pass with L = R^T */
+    const size_t nb = qr_nb(block, nn) < p ? qr_nb(block, nn) : p;
+    word* L = (word*)malloc(sizeof(word) * E * (p * p + 1));
+    for (size_t i = 0; i < p; ++i) for (size_t j = 0; j < p; ++j) copy_num(L + (j * p + i) * E, R + (i * nn + j) * E, n);
+    if (p) lfo_solve(bits, L, p, C, nrhs, nb, 2);
+    for (size_t i = 0; i < nn; ++i)
+        for (size_t c = 0; c < nrhs; ++c) {
+            word* out = X + ((perm ? perm[i] : i) * nrhs + c) * E;
+            if (i < p) copy_num(out, C + (i * nrhs + c) * E, n); else set_zero(out, n, 0);
+        }
+    free(C); free(L);
+    return 0;
+}
+#undef QP
+#undef QD

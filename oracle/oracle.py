@@ -68,6 +68,10 @@ class Oracle:
         lib.lfo_tree_sum.argtypes = [I, I, V, S, V]
         lib.lfo_segmented_dot.argtypes = [I, I, S, S, I, V, V, V]
         lib.lfo_recurrence.argtypes = [I, V, V, V, S, C.c_uint, C.c_uint]
+        lib.lfo_qr.argtypes = [I, V, S, S, S, I, V, V, V, V, C.POINTER(C.c_long)]
+        lib.lfo_qr_pivoted.argtypes = [I, V, S, S, S, I, V, V, V, V, C.POINTER(C.c_size_t), C.POINTER(C.c_long)]
+        lib.lfo_qr_apply.argtypes = [I, S, S, S, S, V, V, V, S, I]
+        lib.lfo_qr_solve.argtypes = [I, S, S, S, C.POINTER(C.c_long), C.POINTER(C.c_size_t), V, V, V, V, S, V]
         self.lib = lib
 
     def elementwise(self, bits, op, a, b=None, c=None, b_index=(1, 0), c_index=(1, 0)):
@@ -158,6 +162,49 @@ class Oracle:
         return out
 
 
+    def qr(self, bits, A, m, n, block=32, rank_bits=0, pivot=False):
+        """Householder QR of A (m x n elements); returns a dict with R, V, T, tau, rank, reason, status,
+        recomputed, perm (None unpivoted) and the shape, as the factor the solve and apply calls take."""
+        w = bits // 32 + 3
+        nb = block if block and block < n else n
+        blocks = (n + nb - 1) // nb if nb else 0
+        R = np.zeros((n * n, w), dtype=np.uint32)
+        V = np.zeros((m * n, w), dtype=np.uint32)
+        T = np.zeros((max(blocks * nb * nb, 1), w), dtype=np.uint32)
+        tau = np.zeros((max(n, 1), w), dtype=np.uint32)
+        info = (C.c_long * 4)()
+        A = np.ascontiguousarray(A.reshape(m * n, w)) if m * n else np.zeros((1, w), dtype=np.uint32)
+        perm = None
+        if pivot:
+            pm = (C.c_size_t * max(n, 1))()
+            self.lib.lfo_qr_pivoted(bits, _ptr(A), m, n, block, rank_bits, _ptr(R), _ptr(V), _ptr(T), _ptr(tau), pm, info)
+            perm = [int(pm[i]) for i in range(n)]
+        else:
+            self.lib.lfo_qr(bits, _ptr(A), m, n, block, rank_bits, _ptr(R), _ptr(V), _ptr(T), _ptr(tau), info)
+        return {"bits": bits, "m": m, "n": n, "block": block, "nb": nb, "R": R, "V": V, "T": T[:blocks * nb * nb],
+                "tau": tau[:n], "rank": int(info[0]), "reason": int(info[1]), "status": int(info[2]),
+                "recomputed": int(info[3]), "perm": perm}
+
+    def qr_apply(self, f, B, nrhs, transpose):
+        """B (m x nrhs) -> Q^T B (transpose) or Q B."""
+        out = np.ascontiguousarray(B.copy())
+        if f["m"] and nrhs:
+            self.lib.lfo_qr_apply(f["bits"], f["m"], f["n"], f["block"], f["rank"], _ptr(f["V"]), _ptr(f["T"]),
+                                  _ptr(out), nrhs, int(bool(transpose)))
+        return out
+
+    def qr_solve(self, f, B, nrhs):
+        """Least-squares X (n x nrhs) from B (m x nrhs)."""
+        w = f["bits"] // 32 + 3
+        X = np.zeros((max(f["n"] * nrhs, 1), w), dtype=np.uint32)
+        info = (C.c_long * 4)(f["rank"], f["reason"], f["status"], f["recomputed"])
+        perm = (C.c_size_t * max(f["n"], 1))(*f["perm"]) if f["perm"] is not None else None
+        if f["n"] and nrhs:
+            self.lib.lfo_qr_solve(f["bits"], f["m"], f["n"], f["block"], info, perm, _ptr(f["R"]), _ptr(f["V"]),
+                                  _ptr(f["T"]), _ptr(np.ascontiguousarray(B)), nrhs, _ptr(X))
+        return X[:f["n"] * nrhs]
+
+
 class Reference:
     """The reference's own CPU arithmetic (core.hpp, exact_dot_add) built into oracle/_ref."""
 
@@ -174,6 +221,7 @@ class Reference:
         lib.ref_exact_dot_add.argtypes = [I, V, I, V, L, V, L, S, V]
         lib.ref_dot2_add.argtypes = [I, V, V, V, V, V, V, S]
         lib.ref_divide_word.argtypes = [C.c_uint, C.c_uint, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_uint)]
+        lib.ref_qr_blocked.argtypes = [I, V, S, S, S, I, V, V, V, V, C.POINTER(C.c_long)]
         self.lib = lib
 
     def elementwise(self, bits, op, a, b=None, c=None):
@@ -185,6 +233,21 @@ class Reference:
         out = np.zeros(bits // 32 + 3, dtype=np.uint32)
         self.lib.ref_exact_dot_add(bits, _ptr(c), int(subtract), _ptr(a), sa, _ptr(b), sb, K, _ptr(out))
         return out
+
+    def qr_blocked(self, bits, A, m, n, block=32, rank_bits=0):
+        """Unpivoted QR in the library's blocked right-looking form over the reference's own arithmetic."""
+        w = bits // 32 + 3
+        nb = block if block and block < n else n
+        blocks = (n + nb - 1) // nb if nb else 0
+        R = np.zeros((max(n * n, 1), w), dtype=np.uint32)
+        V = np.zeros((max(m * n, 1), w), dtype=np.uint32)
+        T = np.zeros((max(blocks * nb * nb, 1), w), dtype=np.uint32)
+        tau = np.zeros((max(n, 1), w), dtype=np.uint32)
+        info = (C.c_long * 4)()
+        A = np.ascontiguousarray(A.reshape(m * n, w)) if m * n else np.zeros((1, w), dtype=np.uint32)
+        self.lib.ref_qr_blocked(bits, _ptr(A), m, n, block, rank_bits, _ptr(R), _ptr(V), _ptr(T), _ptr(tau), info)
+        return {"R": R[:n * n], "V": V[:m * n], "T": T[:blocks * nb * nb], "tau": tau[:n], "rank": int(info[0]),
+                "reason": int(info[1]), "status": int(info[2])}
 
     def dot2_add(self, bits, a, b, c, d, e):
         out = np.zeros_like(a)
