@@ -1,7 +1,7 @@
 #pragma once
 // limbforge::Linalg (the reference's include/limbforge/linalg.hpp:141-218 interface): exact dense
-// products with one rounding per output, blocked Cholesky and multi-RHS triangular solves, as
-// inline wrappers over the C ABI.  Every product runs on the GPU.
+// products with one rounding per output, blocked Cholesky, multi-RHS triangular solves and Householder
+// QR, as inline wrappers over the C ABI.  Every product runs on the GPU.
 #include "engine.hpp"
 #include <cstring>
 #include <future>
@@ -81,6 +81,72 @@ public:
     bool provisional_reads() const { (void)report(); return false; }
 };
 
+// Householder QR (linalg.hpp:88-137): FactorOptions (block; the GPU/host split fields only place work and never change
+// a bit) and an optional rank test (rank_bits > 0 also stops at the first column whose |r_jj| lies more than rank_bits
+// binades below the largest earlier |r_kk|); pivot: column pivoting (xGEQP3 order).
+struct QROptions : FactorOptions { int rank_bits = 0; bool pivot = false; };
+struct QRInfo {
+    enum Reason { full_rank = 0, zero_column = 1, small_column = 2, status_column = 3 };
+    std::size_t rank = 0; int reason = full_rank; word status = 0;
+    Timing timing{0, 0};
+    std::size_t blocks = 0, gpu_updates = 0, host_updates = 0;
+    double panel_seconds = 0, update_seconds = 0;
+    std::size_t norm_recomputations = 0;
+};
+class Linalg;
+// Owning QR factor of an m x n matrix (m >= n): Q = H_0 ... H_{n-1}, H_j = I - tau_j v_j v_j^T, and R.  Row-major
+// Float<bits> arrays owned by the factor: R (n x n, upper; with rank p < n rows i >= p hold the remainder in columns
+// j >= p), V (m x n, column j is v_j), tau (n), T (blocks of nb x nb, block b at b*nb*nb).  The Linalg that made it
+// must outlive it; calls follow the Linalg threading rule.
+class QRFactor {
+    struct Del { void operator()(lf_qr* q) const { lf_qr_destroy(q); } };
+    std::unique_ptr<lf_qr, Del> q_;
+    int bits_ = 0; std::size_t m_ = 0, n_ = 0, nb_ = 0; bool pivoted_ = false; QRInfo info_{};
+    explicit QRFactor(lf_qr* q) : q_(q) {
+        lf_qr_info i{}; int piv = 0;
+        detail::check(lf_qr_describe(q, &bits_, &m_, &n_, &nb_, &piv, &i));
+        pivoted_ = piv != 0;
+        info_.rank = i.rank; info_.reason = i.reason; info_.status = i.status; info_.timing = detail::timing(i.timing);
+        info_.blocks = i.blocks; info_.gpu_updates = i.gpu_updates; info_.host_updates = i.host_updates;
+        info_.panel_seconds = i.panel_seconds; info_.update_seconds = i.update_seconds; info_.norm_recomputations = i.norm_recomputations;
+    }
+    const lf_qr* get() const { if (!q_) throw std::logic_error("empty QR factor"); return q_.get(); }
+    friend class Linalg;
+public:
+    QRFactor() = default;
+    QRFactor(QRFactor&&) noexcept = default;
+    QRFactor& operator=(QRFactor&&) noexcept = default;
+    bool empty() const { return !q_; }
+    int bits() const { (void)get(); return bits_; }
+    std::size_t rows() const { (void)get(); return m_; }
+    std::size_t cols() const { (void)get(); return n_; }
+    std::size_t block() const { (void)get(); return nb_; }
+    const QRInfo& info() const { (void)get(); return info_; }
+    bool full_rank() const { (void)get(); return info_.rank == n_; }
+    const void* r() const { return lf_qr_r(get()); }
+    const void* v() const { return lf_qr_v(get()); }
+    const void* tau() const { return lf_qr_tau(get()); }
+    const void* t() const { return lf_qr_t(get()); }
+    bool pivoted() const { (void)get(); return pivoted_; }
+    const std::size_t* permutation() const { return lf_qr_permutation(get()); }
+    // Least squares X (n x nrhs) for B (m x nrhs); X must not overlap B (linalg.hpp:127).
+    Timing solve(const void* B, std::size_t nrhs, void* X) const {
+        lf_timing t{}; detail::check(lf_qr_solve(get(), B, nrhs, X, &t)); return detail::timing(t);
+    }
+    // B (m x nrhs) <- Q^T B (transpose) or Q B, in place (linalg.hpp:129).
+    Timing apply_q(void* B, std::size_t nrhs, bool transpose) const {
+        lf_timing t{}; detail::check(lf_qr_apply_q(get(), B, nrhs, transpose, &t)); return detail::timing(t);
+    }
+    template <class T> Timing solve(const Buffer<T>& B, std::size_t nrhs, Buffer<T>& X) const {
+        static_assert(detail::Format<T>::bits && !detail::Format<T>::complex, "QR uses real Float<bits> buffers");
+        lf_timing t{}; detail::check(lf_qr_solve_buffers(get(), B.handle(), nrhs, X.handle(), &t)); return detail::timing(t);
+    }
+    template <class T> Timing apply_q(Buffer<T>& B, std::size_t nrhs, bool transpose) const {
+        static_assert(detail::Format<T>::bits && !detail::Format<T>::complex, "QR uses real Float<bits> buffers");
+        lf_timing t{}; detail::check(lf_qr_apply_q_buffer(get(), B.handle(), nrhs, transpose, &t)); return detail::timing(t);
+    }
+};
+
 // One Linalg per host thread.
 class Linalg {
     struct Del { void operator()(lf_linalg* l) const { lf_linalg_destroy(l); } };
@@ -88,6 +154,7 @@ class Linalg {
     LinalgOptions o_;
     mutable LinalgReport r_;
     static lf_factor_options fo(const FactorOptions& o) { return {o.block, o.host_macs, o.solve_host_macs, o.gpu}; }
+    static lf_qr_options qo(const QROptions& o) { return {o.block, o.host_macs, o.solve_host_macs, o.gpu, o.rank_bits, o.pivot}; }
     template <class T> Timing solve_buffers(int passes, const Buffer<T>& L, std::size_t n, const Buffer<T>& B, std::size_t nrhs, Buffer<T>& X,
                                             const FactorOptions& options) {
         static_assert(detail::Format<T>::bits && !detail::Format<T>::complex, "dense linear algebra uses real Float<bits> buffers");
@@ -160,6 +227,24 @@ public:
     Timing cholesky_solve(int bits, const void* L, std::size_t n, const void* B, std::size_t nrhs, void* X, const FactorOptions& options = {}) {
         lf_factor_options o = fo(options);
         lf_timing t{}; detail::check(lf_linalg_cholesky_solve(l_.get(), bits, L, n, B, nrhs, X, &o, &t)); return detail::timing(t);
+    }
+    // Householder QR of A (m x n, row-major, m >= n); A is only read (linalg.hpp:164).
+    QRFactor factor_qr(int bits, const void* A, std::size_t m, std::size_t n, const QROptions& options = {}) {
+        lf_qr_options o = qo(options); lf_qr* q = nullptr;
+        detail::check(lf_linalg_factor_qr(l_.get(), bits, A, m, n, &o, &q));
+        return QRFactor(q);
+    }
+    // QR of the augmented Levenberg-Marquardt matrix [J; diag(d)] ((m + n) x n) (linalg.hpp:168).
+    QRFactor factor_qr_augmented(int bits, const void* J, std::size_t m, std::size_t n, const void* d, const QROptions& options = {}) {
+        lf_qr_options o = qo(options); lf_qr* q = nullptr;
+        detail::check(lf_linalg_factor_qr_augmented(l_.get(), bits, J, m, n, d, &o, &q));
+        return QRFactor(q);
+    }
+    template <class T> QRFactor factor_qr(const Buffer<T>& A, std::size_t m, std::size_t n, const QROptions& options = {}) {
+        static_assert(detail::Format<T>::bits && !detail::Format<T>::complex, "QR uses real Float<bits> buffers");
+        lf_qr_options o = qo(options); lf_qr* q = nullptr;
+        detail::check(lf_linalg_factor_qr_buffer(l_.get(), detail::Format<T>::bits, A.handle(), m, n, &o, &q));
+        return QRFactor(q);
     }
     // Factorization and solves on Buffer operands of the Linalg's engine (linalg.hpp:194-199): synchronous, outside any
     // batch, the buffers used in place; they must be idle (logic_error otherwise).  Same bits as the host-array calls.

@@ -125,6 +125,43 @@ int lf_linalg_cholesky_buffers(lf_linalg* linalg, int bits, lf_buffer* A, size_t
                                lf_cholesky_info* info);
 int lf_linalg_solve_buffers(lf_linalg* linalg, int bits, int passes, lf_buffer* L, size_t n, lf_buffer* B, size_t nrhs, lf_buffer* X,
                             const lf_factor_options* options, lf_timing* timing);
+
+/* ---- Householder QR (linalg.hpp:88-137; linalg.mm:488-849).  Options: the FactorOptions fields (block is the
+ * compact-WY block; host_macs, solve_host_macs and gpu only place work and never change a bit), rank_bits (> 0:
+ * the factorization also stops at the first column whose |r_jj| lies more than rank_bits binades below the
+ * largest earlier |r_kk|) and pivot (column pivoting, as xGEQP3).  A factor owns row-major arrays R (n x n, upper;
+ * with rank p < n rows i >= p hold the remainder in columns j >= p), V (m x n, column j is v_j, zero above row j),
+ * tau (n) and T (blocks of nb x nb compact-WY upper triangles, block b at b*nb*nb); it uses the Linalg that made
+ * it, which must outlive it.  info.reason: 0 full rank, 1 zero column, 2 small column, 3 status column. */
+typedef struct lf_qr_options { size_t block; double host_macs, solve_host_macs; int gpu; int rank_bits; int pivot; } lf_qr_options; /* linalg.hpp:94 */
+typedef struct lf_qr_info {                                                               /* linalg.hpp:98-105 */
+    size_t rank; int reason; uint32_t status; lf_timing timing;
+    size_t blocks, gpu_updates, host_updates; double panel_seconds, update_seconds; size_t norm_recomputations;
+} lf_qr_info;
+typedef struct lf_qr lf_qr;                                                               /* QRFactor, linalg.hpp:112 */
+/* Linalg::factor_qr (linalg.hpp:164): A (m x n, m >= n) is only read; *out owns the factor (lf_qr_destroy) */
+int lf_linalg_factor_qr(lf_linalg* linalg, int bits, const void* A, size_t m, size_t n, const lf_qr_options* options, lf_qr** out);
+/* Linalg::factor_qr_augmented (linalg.hpp:168): the factor of [J; diag(d)] ((m + n) x n) */
+int lf_linalg_factor_qr_augmented(lf_linalg* linalg, int bits, const void* J, size_t m, size_t n, const void* d,
+                                  const lf_qr_options* options, lf_qr** out);
+/* Linalg::factor_qr on a Buffer (linalg.hpp:200): synchronous, the buffer idle */
+int lf_linalg_factor_qr_buffer(lf_linalg* linalg, int bits, lf_buffer* A, size_t m, size_t n, const lf_qr_options* options, lf_qr** out);
+void lf_qr_destroy(lf_qr* qr);
+/* QRFactor::bits/rows/cols/block/pivoted/info (linalg.hpp:115-116) */
+int lf_qr_describe(const lf_qr* qr, int* bits, size_t* rows, size_t* cols, size_t* block, int* pivoted, lf_qr_info* info);
+/* QRFactor::r/v/tau/t/permutation (linalg.hpp:121-123): arrays owned by the factor; NULL when empty */
+const void* lf_qr_r(const lf_qr* qr);
+const void* lf_qr_v(const lf_qr* qr);
+const void* lf_qr_tau(const lf_qr* qr);
+const void* lf_qr_t(const lf_qr* qr);
+const size_t* lf_qr_permutation(const lf_qr* qr);
+/* QRFactor::solve (linalg.hpp:127): least-squares X (n x nrhs) from B (m x nrhs); X must not overlap B */
+int lf_qr_solve(const lf_qr* qr, const void* B, size_t nrhs, void* X, lf_timing* timing);
+/* QRFactor::apply_q (linalg.hpp:129): B (m x nrhs) <- Q^T B (transpose) or Q B, in place */
+int lf_qr_apply_q(const lf_qr* qr, void* B, size_t nrhs, int transpose, lf_timing* timing);
+/* Buffer forms of solve / apply_q (linalg.hpp:131-134): synchronous, buffers idle */
+int lf_qr_solve_buffers(const lf_qr* qr, lf_buffer* B, size_t nrhs, lf_buffer* X, lf_timing* timing);
+int lf_qr_apply_q_buffer(const lf_qr* qr, lf_buffer* B, size_t nrhs, int transpose, lf_timing* timing);
 /* Exact product on device line views (CUDA callers; no reference counterpart): element (line, k)
  * at base + (line * ls + k * ks) elements; C element (i, j) at C + i * ldc + j elements. */
 int lf_dev_exact_product(lf_linalg* linalg, int bits, const void* left, size_t left_ls, size_t left_ks, const void* right,

@@ -147,6 +147,26 @@ class CholeskyInfo:                                              # linalg.hpp:82
     update_seconds: float = 0.0
 
 
+@dataclass
+class QROptions(FactorOptions):                                  # linalg.hpp:94
+    rank_bits: int = 0
+    pivot: bool = False
+
+
+@dataclass
+class QRInfo:                                                    # linalg.hpp:98-105
+    rank: int = 0
+    reason: int = 0          # 0 full rank, 1 zero column, 2 small column, 3 status column
+    status: int = 0
+    timing: "Timing" = None
+    blocks: int = 0
+    gpu_updates: int = 0
+    host_updates: int = 0
+    panel_seconds: float = 0.0
+    update_seconds: float = 0.0
+    norm_recomputations: int = 0
+
+
 class _Timing(C.Structure):
     _fields_ = [("gpu_seconds", C.c_double), ("wall_seconds", C.c_double)]
 
@@ -187,6 +207,17 @@ class _CholeskyInfo(C.Structure):
     _fields_ = [("pivot", C.c_size_t), ("pivot_sign", C.c_int), ("pivot_status", C.c_uint32), ("timing", _Timing),
                 ("blocks", C.c_size_t), ("gpu_updates", C.c_size_t), ("host_updates", C.c_size_t),
                 ("panel_seconds", C.c_double), ("update_seconds", C.c_double)]
+
+
+class _QROptions(C.Structure):
+    _fields_ = [("block", C.c_size_t), ("host_macs", C.c_double), ("solve_host_macs", C.c_double), ("gpu", C.c_int),
+                ("rank_bits", C.c_int), ("pivot", C.c_int)]
+
+
+class _QRInfo(C.Structure):
+    _fields_ = [("rank", C.c_size_t), ("reason", C.c_int), ("status", C.c_uint32), ("timing", _Timing),
+                ("blocks", C.c_size_t), ("gpu_updates", C.c_size_t), ("host_updates", C.c_size_t),
+                ("panel_seconds", C.c_double), ("update_seconds", C.c_double), ("norm_recomputations", C.c_size_t)]
 
 
 class _LinalgWorkspaces(C.Structure):
@@ -274,6 +305,15 @@ def _load() -> C.CDLL:
         "lf_engine_segmented_dot": ([V, I, I, P(_SegmentedDot), V, V, V, P(_Timing)], I),
         "lf_batch_segmented_dot": ([V, I, I, P(_SegmentedDot), V, V, V], I),
         "lf_engine_recurrence": ([V, I, V, V, V, S, C.c_uint, C.c_uint, P(_Timing)], I),
+        "lf_linalg_factor_qr": ([V, I, V, S, S, P(_QROptions), P(V)], I),
+        "lf_linalg_factor_qr_augmented": ([V, I, V, S, S, V, P(_QROptions), P(V)], I),
+        "lf_linalg_factor_qr_buffer": ([V, I, V, S, S, P(_QROptions), P(V)], I),
+        "lf_qr_destroy": ([V], None),
+        "lf_qr_describe": ([V, P(I), P(S), P(S), P(S), P(I), P(_QRInfo)], I),
+        "lf_qr_r": ([V], V), "lf_qr_v": ([V], V), "lf_qr_tau": ([V], V), "lf_qr_t": ([V], V),
+        "lf_qr_permutation": ([V], P(S)),
+        "lf_qr_solve": ([V, V, S, V, P(_Timing)], I), "lf_qr_apply_q": ([V, V, S, I, P(_Timing)], I),
+        "lf_qr_solve_buffers": ([V, V, S, V, P(_Timing)], I), "lf_qr_apply_q_buffer": ([V, V, S, I, P(_Timing)], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -785,6 +825,32 @@ class Linalg:
         check(lib.lf_linalg_cholesky_solve(self.handle, bits, _ptr(L), n, _ptr(B), nrhs, _ptr(X), C.byref(fo), C.byref(t)))
         return _timing(t)
 
+    @staticmethod
+    def _qo(o: "QROptions | None"):
+        o = o or QROptions()
+        return _QROptions(o.block, o.host_macs, o.solve_host_macs, int(o.gpu), o.rank_bits, int(o.pivot))
+
+    def factor_qr(self, bits, A, m, n, options: "QROptions | None" = None) -> "QRFactor":
+        """Householder QR of A (m x n, m >= n, row-major) (linalg.hpp:164); A is only read."""
+        h = C.c_void_p()
+        qo = self._qo(options)
+        check(lib.lf_linalg_factor_qr(self.handle, bits, _ptr(A), m, n, C.byref(qo), C.byref(h)))
+        return QRFactor(h, self)
+
+    def factor_qr_augmented(self, bits, J, m, n, d, options: "QROptions | None" = None) -> "QRFactor":
+        """The factor of [J; diag(d)] ((m + n) x n) (linalg.hpp:168)."""
+        h = C.c_void_p()
+        qo = self._qo(options)
+        check(lib.lf_linalg_factor_qr_augmented(self.handle, bits, _ptr(J), m, n, _ptr(d), C.byref(qo), C.byref(h)))
+        return QRFactor(h, self)
+
+    def factor_qr_buffer(self, A: "Buffer", m, n, options: "QROptions | None" = None) -> "QRFactor":
+        """factor_qr on an idle Buffer of this Linalg's engine (linalg.hpp:200)."""
+        h = C.c_void_p()
+        qo = self._qo(options)
+        check(lib.lf_linalg_factor_qr_buffer(self.handle, A.bits, A.handle, m, n, C.byref(qo), C.byref(h)))
+        return QRFactor(h, self)
+
     # explicit contract names (linalg.hpp:203-210)
     gemm_exact = gemm
     syrk_exact = syrk
@@ -810,6 +876,79 @@ class Linalg:
                           subtract=False, lower=False, stream=0) -> None:
         check(lib.lf_dev_exact_product(self.handle, bits, _ptr(left), left_ls, left_ks, _ptr(right), right_ls, right_ks,
                                        M, N, K, _ptr(C_), ldc, int(subtract), int(lower), C.c_void_p(stream)))
+
+
+class QRFactor:
+    """Owning Householder QR factor (linalg.hpp:109-138): Q = H_0 ... H_{n-1}, H_j = I - tau_j v_j v_j^T, and R.  Uses
+    the Linalg that made it (kept alive here)."""
+
+    def __init__(self, handle, linalg: Linalg):
+        self.handle = handle
+        self.linalg = linalg
+        bits, rows, cols, block, piv = C.c_int(), C.c_size_t(), C.c_size_t(), C.c_size_t(), C.c_int()
+        i = _QRInfo()
+        check(lib.lf_qr_describe(handle, C.byref(bits), C.byref(rows), C.byref(cols), C.byref(block), C.byref(piv), C.byref(i)))
+        self.bits, self.rows, self.cols, self.block, self.pivoted = bits.value, rows.value, cols.value, block.value, bool(piv.value)
+        self.info = QRInfo(i.rank, i.reason, i.status, _timing(i.timing), i.blocks, i.gpu_updates, i.host_updates,
+                           i.panel_seconds, i.update_seconds, i.norm_recomputations)
+
+    def __del__(self):
+        if getattr(self, "handle", None) and lib is not None:
+            lib.lf_qr_destroy(self.handle)
+            self.handle = None
+
+    def full_rank(self) -> bool:
+        return self.info.rank == self.cols
+
+    def _array(self, fn, count) -> np.ndarray:
+        w = self.bits // 32 + 3
+        p = fn(self.handle)
+        if not p or not count:
+            return np.zeros((0, w), dtype=np.uint32)
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint32)), shape=(count * w,)).reshape(count, w).copy()
+
+    def r(self) -> np.ndarray:
+        return self._array(lib.lf_qr_r, self.cols * self.cols)
+
+    def v(self) -> np.ndarray:
+        return self._array(lib.lf_qr_v, self.rows * self.cols)
+
+    def tau(self) -> np.ndarray:
+        return self._array(lib.lf_qr_tau, self.cols)
+
+    def t(self) -> np.ndarray:
+        nb = self.block
+        blocks = (self.cols + nb - 1) // nb if nb else 0
+        return self._array(lib.lf_qr_t, blocks * nb * nb)
+
+    def permutation(self) -> list:
+        p = lib.lf_qr_permutation(self.handle)
+        return [int(p[i]) for i in range(self.cols)] if self.cols else []
+
+    def solve(self, B, nrhs, X=None) -> np.ndarray:
+        """Least-squares X (n x nrhs) for B (m x nrhs) (linalg.hpp:127)."""
+        if X is None:
+            X = np.zeros((max(self.cols * nrhs, 0), self.bits // 32 + 3), dtype=np.uint32)
+        t = _Timing()
+        check(lib.lf_qr_solve(self.handle, _ptr(B), nrhs, _ptr(X), C.byref(t)))
+        self.last_timing = _timing(t)
+        return X
+
+    def apply_q(self, B, nrhs, transpose) -> Timing:
+        """B (m x nrhs) <- Q^T B (transpose) or Q B, in place (linalg.hpp:129)."""
+        t = _Timing()
+        check(lib.lf_qr_apply_q(self.handle, _ptr(B), nrhs, int(bool(transpose)), C.byref(t)))
+        return _timing(t)
+
+    def solve_buffers(self, B: "Buffer", nrhs, X: "Buffer") -> Timing:
+        t = _Timing()
+        check(lib.lf_qr_solve_buffers(self.handle, B.handle, nrhs, X.handle, C.byref(t)))
+        return _timing(t)
+
+    def apply_q_buffer(self, B: "Buffer", nrhs, transpose) -> Timing:
+        t = _Timing()
+        check(lib.lf_qr_apply_q_buffer(self.handle, B.handle, nrhs, int(bool(transpose)), C.byref(t)))
+        return _timing(t)
 
 
 def dev_elementwise(bits, op, a_ptr, b_ptr, c_ptr, out_ptr, count, b_index=None, c_index=None, stream=0) -> None:

@@ -7,6 +7,7 @@
 #include "lf_linalg.cuh"
 #include "lf_residue.h"
 #include "lf_residue.cuh"
+#include "lf_qr.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -20,6 +21,7 @@ struct Linalg {
     lf_linalg_options options{};
     lf_linalg_report report{};
     DevBuf work[6];
+    DevBuf qr[11];                  // Householder QR scratch: W/Y blocks, panel, state, right-hand sides
     DevBuf info_buf, error_buf, lines;
     ResidueEngine residue;
     // the factorizations' second product lane: trailing updates beyond the next block run on `side` while the
@@ -320,7 +322,10 @@ static lf_cholesky_info cholesky_device(Linalg& la, int bits, uint32_t* W, size_
 // in the factorization: after the diagonal block of rows [r0, r1), the update of the next block's rows runs on the
 // engine's stream (the next diagonal block follows it there) and the update of the rows beyond on the side stream,
 // while the next diagonal block is solved; each row still receives the blocks' updates in order.
-static double solve_device(Linalg& la, int bits, const uint32_t* L, size_t n, uint32_t* X, size_t nrhs, size_t block, int passes) {
+// upper (backward pass only): L holds an upper triangular R = L^T itself, row i of R in place of column i of L (the
+// least-squares solve of the QR factor; the same sequence, linalg.mm:471-480).
+static double solve_device(Linalg& la, int bits, const uint32_t* L, size_t n, uint32_t* X, size_t nrhs, size_t block, int passes,
+                           bool upper = false) {
     if (!n || !nrhs) return 0;
     Engine& e = *la.engine;
     cudaStream_t s = e.stream;
@@ -340,7 +345,7 @@ static double solve_device(Linalg& la, int bits, const uint32_t* L, size_t n, ui
     // columns of L (backward, line i = column i of L from row r0)
     auto update = [&](bool forward, size_t r0, size_t r1, size_t a, size_t b, const ProductLane& lane, cudaStream_t st) {
         if (a >= b) return;
-        const lfd::LineView lv = forward ? lfd::LineView{L + (a * n + r0) * E, n, 1} : lfd::LineView{L + (r0 * n + a) * E, 1, n};
+        const lfd::LineView lv = forward || upper ? lfd::LineView{L + (a * n + r0) * E, n, 1} : lfd::LineView{L + (r0 * n + a) * E, 1, n};
         const lfd::LineView xv{X + r0 * nrhs * E, 1, nrhs};
         exact_product_on(la, lane, bits, lv, xv, b - a, nrhs, r1 - r0, X + a * nrhs * E, nrhs, true, false, st, nullptr, false);
     };
@@ -370,7 +375,7 @@ static double solve_device(Linalg& la, int bits, const uint32_t* L, size_t n, ui
     if (passes & 2)
         for (size_t r0 = (n - 1) / nb * nb;; r0 -= nb) {
             const size_t r1 = std::min(n, r0 + nb);
-            fk->solve(lfd::SolveParams{L, X, n, nrhs, r0, r1, 0, err}, false, s);
+            fk->solve(lfd::SolveParams{L, X, n, nrhs, r0, r1, upper ? 1 : 0, err}, false, s);
             cuda_check(cudaGetLastError(), "back substitution");
             if (r0) {
                 const size_t q0 = r0 - nb;                     // the next block (below in the order) is [q0, r0)
@@ -666,6 +671,7 @@ void lf_linalg_ticket_destroy(lf_linalg_ticket* t) { delete t; }
 static lf_linalg_workspaces linalg_workspaces(Linalg& la) {
     lf_linalg_workspaces w{};
     for (auto& b : la.work) w.scratch_bytes += b.bytes;
+    for (auto& b : la.qr) w.scratch_bytes += b.bytes;
     w.scratch_bytes += la.info_buf.bytes + la.error_buf.bytes + la.lines.bytes + la.residue.bytes() + la.lines2.bytes + la.residue2.bytes();
     for (auto& weak : la.resident) {
         auto r = weak.lock();
@@ -694,6 +700,7 @@ int lf_linalg_release_workspaces(lf_linalg* la, lf_linalg_workspaces* out) {
     cuda_check(cudaStreamSynchronize(la->engine->stream), "release workspaces");
     const lf_linalg_workspaces w = linalg_workspaces(*la);
     for (auto& b : la->work) b = DevBuf{};
+    for (auto& b : la->qr) b = DevBuf{};
     la->info_buf = DevBuf{}; la->error_buf = DevBuf{}; la->lines = DevBuf{}; la->lines2 = DevBuf{};
     la->residue.release();
     la->residue2.release();
@@ -704,6 +711,454 @@ int lf_linalg_release_workspaces(lf_linalg* la, lf_linalg_workspaces* out) {
         return !r || resident_product_bytes(*r) == 0;
     }), list.end());
     if (out) *out = w;
+    LF_API_END
+}
+
+}  // extern "C"
+
+// ---- Householder QR (linalg.hpp:88-137, linalg.mm:488-849) ----
+namespace lfr {
+
+struct QrFactor {
+    Linalg* owner = nullptr;
+    int bits = 0;
+    size_t m = 0, n = 0, nb = 0, block = 32;    // nb: the factor's block; block: the option the solves use
+    bool pivot = false;
+    lf_qr_info info{};
+    std::vector<uint32_t> R, V, T, tau;          // the accessors' arrays
+    std::vector<size_t> perm;
+    DevBuf dV, dT, dR;                           // device copies for the solves and Q applications
+};
+
+// Factor the device matrix Wk (m x n, reduced in place) into V, T, tau and R (all device).  Right-looking with
+// one block of look-ahead (linalg.mm:721-745): after panel b, block b updates the next panel's columns on the
+// engine's stream, and the rest of the trailing matrix on the side stream while the next panel is factored.
+// After a failing column p in block b, block b (its reflectors before p; the rest of its V and T are zero) is
+// applied to the columns after the block, unless p is the block's first column, and the factorization stops.
+static lf_qr_info qr_device(Linalg& la, int bits, uint32_t* Wk, size_t m, size_t n, size_t nb, int rank_bits, uint32_t* V,
+                            uint32_t* T, uint32_t* tau, uint32_t* R) {
+    lf_qr_info info{};
+    info.rank = n;
+    auto w0 = Clock::now();
+    Engine& e = *la.engine;
+    cudaStream_t s = e.stream;
+    const int limbs = bits / 32;
+    const size_t E = limbs + 3, eb = E * 4;
+    const auto* qk = lfd::qr_kernels(limbs);
+    const size_t blocks = nb ? (n + nb - 1) / nb : 0;
+    cuda_check(cudaMemsetAsync(V, 0, m * n * eb, s), "memset");
+    cuda_check(cudaMemsetAsync(T, 0, blocks * nb * nb * eb, s), "memset");
+    cuda_check(cudaMemsetAsync(tau, 0, n * eb, s), "memset");
+    uint32_t* Wb = static_cast<uint32_t*>(la.qr[0].get(nb * n * eb + 16));
+    uint32_t* Yb = static_cast<uint32_t*>(la.qr[1].get(nb * n * eb + 16));
+    uint32_t* Pt = static_cast<uint32_t*>(la.qr[2].get(nb * m * eb + 16));
+    uint32_t* Vt = static_cast<uint32_t*>(la.qr[3].get(nb * m * eb + 16));
+    uint32_t* Wp = static_cast<uint32_t*>(la.qr[4].get(nb * nb * eb + 16));
+    uint32_t* G = static_cast<uint32_t*>(la.qr[5].get(nb * eb + 16));
+    uint32_t* y = static_cast<uint32_t*>(la.qr[6].get(nb * eb + 16));
+    auto* st = static_cast<lfd::QrState*>(la.qr[7].get(sizeof(lfd::QrState)));
+    lfd::QrState host{};
+    host.rank = (long long)n;
+    cuda_check(cudaMemcpyAsync(st, &host, sizeof host, cudaMemcpyHostToDevice, s), "state");
+    uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));
+    cuda_check(cudaMemsetAsync(err, 0, 16, s), "memset");
+    const ProductLane lane_a = main_lane(la), lane_b = side_lane(la);
+    cudaStream_t s2 = la.side;
+    cudaEvent_t g0, g1;
+    cuda_check(cudaEventCreate(&g0), "event"); cuda_check(cudaEventCreate(&g1), "event");
+    cuda_check(cudaEventRecord(g0, s), "event");
+    lfd::QrPanel P{Wk, m, n, V, T, tau, Pt, Vt, Wp, G, y, 0, 0, nb, 0, rank_bits, st, err};
+    // panel [k0, k1) on the engine's stream; returns min(k1, rank) (the host reads the state once per panel)
+    auto panel = [&](size_t k0, size_t k1) -> size_t {
+        auto t = Clock::now();
+        P.k0 = k0; P.kb = k1 - k0; P.mr = m - k0;
+        qk->load(P, s);
+        for (size_t c = 0; c < P.kb; ++c) {
+            if (c) qk->update(P, c, s);
+            qk->reflect(P, c, s);
+            qk->dots(P, c, s);
+        }
+        qk->store(P, s);
+        cuda_check(cudaGetLastError(), "qr panel");
+        cuda_check(cudaMemcpyAsync(&host, st, sizeof host, cudaMemcpyDeviceToHost, s), "state");
+        cuda_check(cudaStreamSynchronize(s), "qr panel");
+        ++info.blocks;
+        info.panel_seconds += since(t);
+        return std::min(k1, (size_t)host.rank);
+    };
+    // block b on columns [c0, c1): W = P(V_b^T X), Y = P(T_b^T W), X = D(X; V_b, Y) (qr_block, linalg.mm:550-567)
+    auto update = [&](size_t b, size_t c0, size_t c1, const ProductLane& lane, cudaStream_t q) {
+        auto t = Clock::now();
+        const size_t k0 = b * nb, kb = std::min(n, k0 + nb) - k0, mr = m - k0, c = c1 - c0;
+        const uint32_t* Vb = V + (k0 * n + k0) * E;
+        const uint32_t* Tb = T + b * nb * nb * E;
+        exact_product_on(la, lane, bits, {Vb, 1, n}, {Wk + (k0 * n + c0) * E, 1, n}, kb, c, mr, Wb + c0 * E, n, false, false, q,
+                         nullptr, false);
+        exact_product_on(la, lane, bits, {Tb, 1, nb}, {Wb + c0 * E, 1, n}, kb, c, kb, Yb + c0 * E, n, false, false, q, nullptr, false);
+        exact_product_on(la, lane, bits, {Vb, n, 1}, {Yb + c0 * E, 1, n}, mr, c, kb, Wk + (k0 * n + c0) * E, n, true, false, q,
+                         nullptr, false);
+        ++info.gpu_updates;
+        info.update_seconds += since(t);
+    };
+    bool side_pending = false;
+    size_t k0 = 0, k1 = std::min(n, nb), p = n ? panel(0, k1) : 0;
+    while (k1 < n) {
+        const size_t b = k0 / nb;
+        // block b-1's remainder update (side stream) covered the columns from k1 on
+        if (side_pending) cuda_check(cudaStreamWaitEvent(s, la.ev_side, 0), "event wait");
+        if (p < k1) {
+            if (p > k0) update(b, k1, n, lane_a, s);
+            break;
+        }
+        const size_t k2 = std::min(n, k1 + nb);
+        update(b, k1, k2, lane_a, s);
+        if (k2 < n) {
+            // panel b is complete (the host read its state), so the side stream may read V_b and T_b
+            update(b, k2, n, lane_b, s2);
+            cuda_check(cudaEventRecord(la.ev_side, s2), "event");
+            side_pending = true;
+        }
+        p = panel(k1, k2);
+        k0 = k1; k1 = k2;
+    }
+    if (side_pending) cuda_check(cudaStreamWaitEvent(s, la.ev_side, 0), "event wait");
+    qk->extract(Wk, R, n, st, s);
+    cuda_check(cudaGetLastError(), "qr extract");
+    cuda_check(cudaEventRecord(g1, s), "event");
+    uint32_t ev[3] = {0, 0, 0};
+    cuda_check(cudaMemcpyAsync(&host, st, sizeof host, cudaMemcpyDeviceToHost, s), "state");
+    cuda_check(cudaMemcpyAsync(ev, err, 12, cudaMemcpyDeviceToHost, s), "error flag");
+    cuda_check(cudaStreamSynchronize(s), "qr");
+    float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
+    cudaEventDestroy(g0); cudaEventDestroy(g1);
+    if (ev[0] | ev[1] | ev[2]) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    info.rank = (size_t)host.rank; info.reason = host.reason; info.status = host.status;
+    info.timing = {ms * 1e-3, since(w0)};
+    return info;
+}
+
+// C (device, m x nrhs) <- Q^T C (qt: blocks in order) or Q C (blocks in reverse) over the blocks holding reflectors
+// [0, rank) (qr_apply_n, linalg.mm:750-766).  Returns the device seconds.
+static double qr_apply_device(Linalg& la, const QrFactor& f, uint32_t* C, size_t nrhs, bool qt) {
+    const size_t nb = f.nb, blocks = nb ? (f.info.rank + nb - 1) / nb : 0;
+    if (!blocks || !nrhs || !f.m) return 0;
+    Engine& e = *la.engine;
+    cudaStream_t s = e.stream;
+    const size_t E = f.bits / 32 + 3, eb = E * 4, m = f.m, n = f.n;
+    uint32_t* Wb = static_cast<uint32_t*>(la.qr[0].get(nb * nrhs * eb + 16));
+    uint32_t* Yb = static_cast<uint32_t*>(la.qr[1].get(nb * nrhs * eb + 16));
+    uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));
+    cuda_check(cudaMemsetAsync(err, 0, 16, s), "memset");
+    const ProductLane lane = main_lane(la);
+    const uint32_t* V = static_cast<const uint32_t*>(f.dV.p);
+    const uint32_t* T = static_cast<const uint32_t*>(f.dT.p);
+    cudaEvent_t g0, g1;
+    cuda_check(cudaEventCreate(&g0), "event"); cuda_check(cudaEventCreate(&g1), "event");
+    cuda_check(cudaEventRecord(g0, s), "event");
+    for (size_t q = 0; q < blocks; ++q) {
+        const size_t b = qt ? q : blocks - 1 - q, k0 = b * nb, kb = std::min(n, k0 + nb) - k0, mr = m - k0;
+        const uint32_t* Vb = V + (k0 * n + k0) * E;
+        const uint32_t* Tb = T + b * nb * nb * E;
+        uint32_t* X = C + k0 * nrhs * E;
+        exact_product_on(la, lane, f.bits, {Vb, 1, n}, {X, 1, nrhs}, kb, nrhs, mr, Wb, nrhs, false, false, s, nullptr, false);
+        const lfd::LineView tv = qt ? lfd::LineView{Tb, 1, nb} : lfd::LineView{Tb, nb, 1};
+        exact_product_on(la, lane, f.bits, tv, {Wb, 1, nrhs}, kb, nrhs, kb, Yb, nrhs, false, false, s, nullptr, false);
+        exact_product_on(la, lane, f.bits, {Vb, n, 1}, {Yb, 1, nrhs}, mr, nrhs, kb, X, nrhs, true, false, s, nullptr, false);
+    }
+    cuda_check(cudaEventRecord(g1, s), "event");
+    uint32_t ev = 0;
+    cuda_check(cudaMemcpyAsync(&ev, lane.err, 4, cudaMemcpyDeviceToHost, s), "error flag");
+    cuda_check(cudaStreamSynchronize(s), "qr apply");
+    float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
+    cudaEventDestroy(g0); cudaEventDestroy(g1);
+    if (ev) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    return ms * 1e-3;
+}
+
+// Least squares on the device: C (m x nrhs, holding B) <- Q^T C, then the backward substitution with R (upper;
+// pivoted: its leading rank x rank block) on C's first rows (qr_solve_n, linalg.mm:768-786).  Returns the device
+// seconds; the caller reads the first min(rank, n) rows.  Callers handle the rank-deficient cases that write
+// invalid zeros.
+static double qr_solve_device(Linalg& la, const QrFactor& f, uint32_t* C, size_t nrhs) {
+    double g = qr_apply_device(la, f, C, nrhs, true);
+    const size_t p = f.info.rank, n = f.n;
+    if (!p) return g;
+    if (p < n) {
+        const size_t eb = (f.bits / 32 + 3) * 4;
+        uint32_t* R11 = static_cast<uint32_t*>(la.qr[9].get(p * p * eb + 16));
+        lfd::qr_kernels(f.bits / 32)->copy(static_cast<const uint32_t*>(f.dR.p), n, R11, p, p, p, la.engine->stream);
+        cuda_check(cudaGetLastError(), "qr leading block");
+        g += solve_device(la, f.bits, R11, p, C, nrhs, f.block, 2, true);
+    } else {
+        g += solve_device(la, f.bits, static_cast<const uint32_t*>(f.dR.p), n, C, nrhs, f.block, 2, true);
+    }
+    return g;
+}
+
+static void check_qr_size(size_t n, size_t rows) {
+    if (n >= 46341 || n * rows >= (size_t(1) << 31)) throw invalid_argument("matrix dimensions exceed 32-bit indexing");
+}
+
+// Factor the matrix already on the device at dA (m x n, left unchanged) into f's device arrays, then copy the
+// factor to f's host arrays.
+static void qr_factor_common(Linalg& la, QrFactor& f, const uint32_t* dA, int rank_bits) {
+    const size_t eb = size_t(f.bits / 8 + 12), m = f.m, n = f.n;
+    const size_t blocks = f.nb ? (n + f.nb - 1) / f.nb : 0;
+    auto w0 = Clock::now();
+    f.R.assign(n * n * (eb / 4), 0); f.V.assign(m * n * (eb / 4), 0);
+    f.T.assign(blocks * f.nb * f.nb * (eb / 4), 0); f.tau.assign(n * (eb / 4), 0);
+    f.perm.resize(n);
+    for (size_t k = 0; k < n; ++k) f.perm[k] = k;
+    f.info = lf_qr_info{};
+    f.info.rank = n;
+    if (!n) return;
+    if (f.pivot) throw runtime_error("factor_qr: column pivoting is not available on this build");
+    Engine& e = *la.engine;
+    cudaStream_t s = e.stream;
+    uint32_t* Wk = static_cast<uint32_t*>(la.work[4].get(m * n * eb));
+    cuda_check(cudaMemcpyAsync(Wk, dA, m * n * eb, cudaMemcpyDeviceToDevice, s), "work matrix");
+    uint32_t* V = static_cast<uint32_t*>(f.dV.get(m * n * eb));
+    uint32_t* T = static_cast<uint32_t*>(f.dT.get(blocks * f.nb * f.nb * eb + 16));
+    uint32_t* R = static_cast<uint32_t*>(f.dR.get(n * n * eb));
+    uint32_t* tau = static_cast<uint32_t*>(la.qr[10].get(n * eb));
+    f.info = qr_device(la, f.bits, Wk, m, n, f.nb, rank_bits, V, T, tau, R);
+    cuda_check(cudaMemcpyAsync(f.R.data(), R, n * n * eb, cudaMemcpyDeviceToHost, s), "download");
+    cuda_check(cudaMemcpyAsync(f.V.data(), V, m * n * eb, cudaMemcpyDeviceToHost, s), "download");
+    if (blocks) cuda_check(cudaMemcpyAsync(f.T.data(), T, blocks * f.nb * f.nb * eb, cudaMemcpyDeviceToHost, s), "download");
+    cuda_check(cudaMemcpyAsync(f.tau.data(), tau, n * eb, cudaMemcpyDeviceToHost, s), "download");
+    cuda_check(cudaStreamSynchronize(s), "download");
+    f.info.timing.wall_seconds = since(w0);
+}
+
+}  // namespace lfr
+
+struct lf_qr : QrFactor {};
+
+extern "C" {
+
+static QrFactor* qr_prepare(lf_linalg* la, int bits, size_t m, size_t n, const lf_qr_options* o) {
+    if (!la) throw invalid_argument("null linalg");
+    check_bits(bits);
+    if (m < n) throw invalid_argument("factor_qr: rows >= columns required");
+    check_qr_size(n, m);
+    const lf_qr_options opts = o ? *o : lf_qr_options{32, 0, 0, 1, 0, 0};
+    if (opts.rank_bits < 0) throw invalid_argument("factor_qr: rank_bits >= 0");
+    auto* f = new lf_qr();
+    f->owner = la; f->bits = bits; f->m = m; f->n = n;
+    f->block = opts.block; f->nb = opts.block ? std::min(opts.block, n) : n; f->pivot = opts.pivot != 0;
+    return f;
+}
+
+// Linalg::factor_qr (linalg.hpp:164): Householder QR of A (m x n, row-major, m >= n); A is only read.
+int lf_linalg_factor_qr(lf_linalg* la, int bits, const void* A, size_t m, size_t n, const lf_qr_options* o, lf_qr** out) {
+    LF_API_BEGIN
+    if (!out) throw invalid_argument("null output");
+    *out = nullptr;
+    std::unique_ptr<lf_qr> f(static_cast<lf_qr*>(qr_prepare(la, bits, m, n, o)));
+    if (m * n && !A) throw invalid_argument("null matrix");
+    const size_t eb = size_t(bits / 8 + 12);
+    auto w0 = Clock::now();
+    if (n) {
+        Engine& e = *la->engine;
+        e.activate();
+        uint32_t* dA = static_cast<uint32_t*>(la->work[3].get(m * n * eb));
+        cuda_check(cudaMemcpyAsync(dA, A, m * n * eb, cudaMemcpyHostToDevice, e.stream), "upload");
+    }
+    qr_factor_common(*la, *f, static_cast<const uint32_t*>(la->work[3].p), o ? o->rank_bits : 0);
+    f->info.timing.wall_seconds = since(w0);
+    *out = f.release();
+    LF_API_END
+}
+
+// Linalg::factor_qr_augmented (linalg.hpp:168): the factor of [J; diag(d)] ((m + n) x n).
+int lf_linalg_factor_qr_augmented(lf_linalg* la, int bits, const void* J, size_t m, size_t n, const void* d, const lf_qr_options* o,
+                                  lf_qr** out) {
+    LF_API_BEGIN
+    if (!out) throw invalid_argument("null output");
+    *out = nullptr;
+    if (!la) throw invalid_argument("null linalg");
+    check_bits(bits);
+    check_qr_size(n, m + n);
+    if (n && (!d || (m && !J))) throw invalid_argument("null matrix");
+    const size_t eb = size_t(bits / 8 + 12);
+    std::vector<unsigned char> S((m + n) * n * eb, 0);
+    if (m * n) std::memcpy(S.data(), J, m * n * eb);
+    for (size_t i = 0; i < n; ++i) std::memcpy(S.data() + ((m + i) * n + i) * eb, static_cast<const unsigned char*>(d) + i * eb, eb);
+    const int rc = lf_linalg_factor_qr(la, bits, S.data(), m + n, n, o, out);
+    if (rc != LF_OK) return rc;
+    LF_API_END
+}
+
+// Linalg::factor_qr on a Buffer (linalg.hpp:200): synchronous, outside any batch; the buffer must be idle.
+int lf_linalg_factor_qr_buffer(lf_linalg* la, int bits, lf_buffer* A, size_t m, size_t n, const lf_qr_options* o, lf_qr** out) {
+    LF_API_BEGIN
+    if (!out) throw invalid_argument("null output");
+    *out = nullptr;
+    std::unique_ptr<lf_qr> f(static_cast<lf_qr*>(qr_prepare(la, bits, m, n, o)));
+    const size_t eb = size_t(bits / 8 + 12);
+    Engine& e = *la->engine;
+    BufferClaim claim;
+    claim.take(A, e.identity);
+    if (A->bytes < m * n * eb) throw invalid_argument("factor_qr: buffer smaller than m x n");
+    auto w0 = Clock::now();
+    e.activate();
+    A->sync_to_device(e.stream);
+    qr_factor_common(*la, *f, static_cast<const uint32_t*>(A->dev), o ? o->rank_bits : 0);
+    f->info.timing.wall_seconds = since(w0);
+    *out = f.release();
+    LF_API_END
+}
+
+void lf_qr_destroy(lf_qr* f) { delete f; }
+
+int lf_qr_describe(const lf_qr* f, int* bits, size_t* rows, size_t* cols, size_t* block, int* pivoted, lf_qr_info* info) {
+    LF_API_BEGIN
+    if (!f) throw logic_error("empty QR factor");
+    if (bits) *bits = f->bits;
+    if (rows) *rows = f->m;
+    if (cols) *cols = f->n;
+    if (block) *block = f->nb;
+    if (pivoted) *pivoted = f->pivot ? 1 : 0;
+    if (info) *info = f->info;
+    LF_API_END
+}
+const void* lf_qr_r(const lf_qr* f) { return f && !f->R.empty() ? f->R.data() : nullptr; }
+const void* lf_qr_v(const lf_qr* f) { return f && !f->V.empty() ? f->V.data() : nullptr; }
+const void* lf_qr_tau(const lf_qr* f) { return f && !f->tau.empty() ? f->tau.data() : nullptr; }
+const void* lf_qr_t(const lf_qr* f) { return f && !f->T.empty() ? f->T.data() : nullptr; }
+const size_t* lf_qr_permutation(const lf_qr* f) { return f && !f->perm.empty() ? f->perm.data() : nullptr; }
+
+// QRFactor::solve (linalg.hpp:127): X (n x nrhs) = the least-squares solution for each column of B (m x nrhs).
+// A rank-deficient unpivoted factor writes zero with invalid to every entry; a status column zero with invalid and
+// its status.  X must not overlap B.
+int lf_qr_solve(const lf_qr* f, const void* B, size_t nrhs, void* X, lf_timing* timing) {
+    LF_API_BEGIN
+    if (!f) throw logic_error("empty QR factor");
+    check_qr_size(f->n, nrhs);
+    check_qr_size(1, f->m * nrhs);
+    if (timing) *timing = {0, 0};
+    if (!f->n || !nrhs) return LF_OK;
+    if (!B || !X) throw invalid_argument("null matrix");
+    const size_t eb = size_t(f->bits / 8 + 12), E = eb / 4, m = f->m, n = f->n, p = f->info.rank;
+    if (overlap(X, n * nrhs * eb, B, m * nrhs * eb)) throw invalid_argument("solve: X overlaps B");
+    auto w0 = Clock::now();
+    if (p < n && (!f->pivot || f->info.reason == 3)) {
+        const uint32_t st = 4u | (f->pivot ? f->info.status : 0u);
+        auto* x = static_cast<uint32_t*>(X);
+        std::memset(x, 0, n * nrhs * eb);
+        for (size_t q = 0; q < n * nrhs; ++q) x[q * E + E - 1] = st;
+        if (timing) *timing = {0, since(w0)};
+        return LF_OK;
+    }
+    Linalg& la = *f->owner;
+    Engine& e = *la.engine;
+    e.activate();
+    uint32_t* C = static_cast<uint32_t*>(la.qr[8].get(m * nrhs * eb));
+    cuda_check(cudaMemcpyAsync(C, B, m * nrhs * eb, cudaMemcpyHostToDevice, e.stream), "upload");
+    const double g = qr_solve_device(la, *f, C, nrhs);
+    const size_t rows = std::min(p, n);
+    if (f->pivot) {
+        std::vector<uint32_t> Z(rows * nrhs * E);
+        if (rows) cuda_check(cudaMemcpyAsync(Z.data(), C, rows * nrhs * eb, cudaMemcpyDeviceToHost, e.stream), "download");
+        cuda_check(cudaStreamSynchronize(e.stream), "download");
+        auto* x = static_cast<uint32_t*>(X);
+        std::memset(x, 0, n * nrhs * eb);
+        for (size_t i = 0; i < rows; ++i) std::memcpy(x + f->perm[i] * nrhs * E, Z.data() + i * nrhs * E, nrhs * eb);
+    } else {
+        cuda_check(cudaMemcpyAsync(X, C, n * nrhs * eb, cudaMemcpyDeviceToHost, e.stream), "download");
+        cuda_check(cudaStreamSynchronize(e.stream), "download");
+    }
+    if (timing) *timing = {g, since(w0)};
+    LF_API_END
+}
+
+// QRFactor::apply_q (linalg.hpp:129): B (m x nrhs) <- Q^T B (transpose) or Q B, in place.
+int lf_qr_apply_q(const lf_qr* f, void* B, size_t nrhs, int transpose, lf_timing* timing) {
+    LF_API_BEGIN
+    if (!f) throw logic_error("empty QR factor");
+    check_qr_size(f->n, nrhs);
+    check_qr_size(1, f->m * nrhs);
+    if (timing) *timing = {0, 0};
+    if (!f->m || !nrhs) return LF_OK;
+    if (!B) throw invalid_argument("null matrix");
+    const size_t eb = size_t(f->bits / 8 + 12), m = f->m;
+    auto w0 = Clock::now();
+    Linalg& la = *f->owner;
+    Engine& e = *la.engine;
+    e.activate();
+    uint32_t* C = static_cast<uint32_t*>(la.qr[8].get(m * nrhs * eb));
+    cuda_check(cudaMemcpyAsync(C, B, m * nrhs * eb, cudaMemcpyHostToDevice, e.stream), "upload");
+    const double g = qr_apply_device(la, *f, C, nrhs, transpose != 0);
+    cuda_check(cudaMemcpyAsync(B, C, m * nrhs * eb, cudaMemcpyDeviceToHost, e.stream), "download");
+    cuda_check(cudaStreamSynchronize(e.stream), "download");
+    if (timing) *timing = {g, since(w0)};
+    LF_API_END
+}
+
+// QRFactor::solve / apply_q on Buffers (linalg.hpp:131-134): synchronous, outside any batch, buffers idle.
+int lf_qr_solve_buffers(const lf_qr* f, lf_buffer* B, size_t nrhs, lf_buffer* X, lf_timing* timing) {
+    LF_API_BEGIN
+    if (!f) throw logic_error("empty QR factor");
+    check_qr_size(f->n, nrhs);
+    check_qr_size(1, f->m * nrhs);
+    const size_t eb = size_t(f->bits / 8 + 12), E = eb / 4, m = f->m, n = f->n, p = f->info.rank;
+    Linalg& la = *f->owner;
+    Engine& e = *la.engine;
+    BufferClaim claim;
+    claim.take(B, e.identity);
+    claim.take(X, e.identity);
+    if (B->bytes < m * nrhs * eb || X->bytes < n * nrhs * eb) throw invalid_argument("solve: buffer too small");
+    if (X == B) throw invalid_argument("solve: X overlaps B");
+    if (timing) *timing = {0, 0};
+    if (!n || !nrhs) return LF_OK;
+    auto w0 = Clock::now();
+    e.activate();
+    B->sync_to_device(e.stream);
+    X->host_authoritative = false;
+    uint32_t* dX = static_cast<uint32_t*>(X->dev);
+    if (p < n && (!f->pivot || f->info.reason == 3)) {
+        std::vector<uint32_t> z(n * nrhs * E, 0);
+        const uint32_t st = 4u | (f->pivot ? f->info.status : 0u);
+        for (size_t q = 0; q < n * nrhs; ++q) z[q * E + E - 1] = st;
+        cuda_check(cudaMemcpyAsync(dX, z.data(), n * nrhs * eb, cudaMemcpyHostToDevice, e.stream), "invalid solution");
+        cuda_check(cudaStreamSynchronize(e.stream), "solve");
+        if (timing) *timing = {0, since(w0)};
+        return LF_OK;
+    }
+    uint32_t* C = static_cast<uint32_t*>(la.qr[8].get(m * nrhs * eb));
+    cuda_check(cudaMemcpyAsync(C, B->dev, m * nrhs * eb, cudaMemcpyDeviceToDevice, e.stream), "right-hand sides");
+    const double g = qr_solve_device(la, *f, C, nrhs);
+    const size_t rows = std::min(p, n);
+    if (f->pivot) {
+        cuda_check(cudaMemsetAsync(dX, 0, n * nrhs * eb, e.stream), "memset");
+        for (size_t i = 0; i < rows; ++i)
+            cuda_check(cudaMemcpyAsync(dX + f->perm[i] * nrhs * E, C + i * nrhs * E, nrhs * eb, cudaMemcpyDeviceToDevice, e.stream), "permute");
+    } else {
+        cuda_check(cudaMemcpyAsync(dX, C, n * nrhs * eb, cudaMemcpyDeviceToDevice, e.stream), "solution");
+    }
+    cuda_check(cudaStreamSynchronize(e.stream), "solve");
+    if (timing) *timing = {g, since(w0)};
+    LF_API_END
+}
+int lf_qr_apply_q_buffer(const lf_qr* f, lf_buffer* B, size_t nrhs, int transpose, lf_timing* timing) {
+    LF_API_BEGIN
+    if (!f) throw logic_error("empty QR factor");
+    check_qr_size(f->n, nrhs);
+    check_qr_size(1, f->m * nrhs);
+    const size_t eb = size_t(f->bits / 8 + 12), m = f->m;
+    Linalg& la = *f->owner;
+    Engine& e = *la.engine;
+    BufferClaim claim;
+    claim.take(B, e.identity);
+    if (B->bytes < m * nrhs * eb) throw invalid_argument("apply_q: buffer too small");
+    if (timing) *timing = {0, 0};
+    if (!m || !nrhs) return LF_OK;
+    auto w0 = Clock::now();
+    e.activate();
+    B->sync_to_device(e.stream);
+    const double g = qr_apply_device(la, *f, static_cast<uint32_t*>(B->dev), nrhs, transpose != 0);
+    cuda_check(cudaStreamSynchronize(e.stream), "apply_q");
+    if (timing) *timing = {g, since(w0)};
     LF_API_END
 }
 

@@ -1,0 +1,353 @@
+// Householder QR panel kernels (the unpivoted sequence of the reference's src/linalg.mm:488-790; the
+// column-by-column statement its tests/test_qr.cpp:33-68 checks gives the same bits).  P(x, y) = RN(sum x_k y_k)
+// and D(c; x, y) = RN(c - sum x_k y_k) with one rounding each.
+//
+// A panel of kb columns starting at column k0 is copied column-contiguous (Pt: entry (c, r) at c * mr + r,
+// mr = m - k0 rows), its reflectors are built in Vt with the same layout, and every column step runs as three
+// launches with no host round trip: the rows of the column reduced by the panel's earlier reflectors (one warp
+// per row), the reflector (one block: the squared norm, sqrt, the scaled reflector and tau), then the panel W
+// row and Gram column (one block per dot) whose last block to arrive writes the T column and the next column's
+// y.  Failures (zero, small or status columns) are recorded in a device-side state that the following launches
+// and the host read; the trailing matrix is updated by the compact-WY products on the exact GEMM engine.
+#pragma once
+#include "lf_linalg.cuh"
+
+namespace lfd {
+
+// Progress of one factorization, written by the panel kernels and read by the next launches and the host.
+struct QrState {
+    long long rank;      // n while every column so far gave a reflector; the first failing column otherwise
+    int reason;          // 0 full rank, 1 zero column, 2 small column (rank test), 3 status column
+    u32 status;          // the failing column's status
+    long long top;       // the largest exponent of an r_jj so far (valid when have_top)
+    int have_top;
+    u32 arrivals;        // blocks of the current dots launch that have finished
+};
+
+struct QrPanel {
+    u32* Wk; u64 m, n;           // the work matrix (m x n), reduced in place
+    u32* V; u32* T; u32* tau;    // the factor: V (m x n), T (blocks of nb x nb), tau (n)
+    u32* Pt; u32* Vt;            // the panel's columns and reflectors, entry (c, r) at c * mr + r
+    u32* Wp; u32* G; u32* y;     // the panel W rows (nb x nb: Wp[c][c'] = P(v_c, a_c')), Gram column, next y
+    u64 k0, kb, nb, mr;
+    int rank_bits;
+    QrState* st;
+    u32* error;                  // set when an exact sum exceeds the cluster window
+};
+
+constexpr int kQrThreads = 256;
+// Window words of the block-wide exact dot: the product width plus headroom for the spread of the products'
+// exponents (about 800 bits up to 512-bit numbers, 320 bits beyond); wider spreads take the cluster method.
+template <int N> __host__ __device__ constexpr int qr_window() { return 2 * N + 10 + (N <= 16 ? 16 : 4); }
+template <int N> __host__ __device__ constexpr int qr_dot_words() { return (kQrThreads / 32) * (qr_window<N>() + 6) + N + 8; }
+
+template <int N> __device__ __forceinline__ Num<N> qr_pow2(int e) {
+    Num<N> x = zero<N>();
+    x.m[N - 1] = 0x80000000u; x.s = 1; x.e = e;
+    return x;
+}
+// x * 2^-e exactly; a result exponent outside [-1e9, 1e9] gives zero with exponent_overflow (linalg.mm:492).
+template <int N> __device__ __forceinline__ Num<N> qr_scaled(Num<N> x, long long e) {
+    if (!x.s) return x;
+    const long long r = (long long)x.e - e;
+    if (r > kEmax || r < -kEmax) return zero<N>(x.st | kOverflow);
+    x.e = (int)r;
+    return x;
+}
+
+// RN(sum_{k<K} x[k sx] y[k sy]) with one rounding, computed by the whole block (kQrThreads threads) and returned
+// to every thread; the contract of exact_dot (statuses first; no nonzero product gives zero).  Pass 1 reduces the
+// statuses, the number of nonzero products and the range of their scales; each thread then adds its products
+// into a two's-complement window anchored at the lowest scale, the warps sum their windows with shuffles and
+// thread 0 adds the warps' sums and rounds once.  A range wider than the window goes to the cluster method on
+// thread 0.  sm: qr_dot_words<N>() words of shared memory, 8-byte aligned.
+template <int N, bool RO> __device__ Num<N> block_exact_dot(const u32* x, i64 sx, const u32* y, i64 sy, u64 K, u32* sm, u32* error) {
+    constexpr int W = qr_window<N>();
+    constexpr int WARPS = kQrThreads / 32;
+    constexpr i64 E = N + 3;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    u32* s_win = sm;                                                 // WARPS windows
+    long long* s_lo = reinterpret_cast<long long*>(sm + WARPS * W + (WARPS * W) % 2);
+    long long* s_hi = s_lo + WARPS;
+    u32* s_st = reinterpret_cast<u32*>(s_hi + WARPS);
+    u32* s_cnt = s_st + WARPS;
+    u32* s_res = s_cnt + WARPS;                                      // N + 3 words
+    u32 st = 0, cnt = 0;
+    long long lo = INT64_MAX, hi = INT64_MIN;
+    for (u64 k = tid; k < K; k += kQrThreads) {
+        const u32* a = x + (i64)k * sx * E; const u32* b = y + (i64)k * sy * E;
+        st |= ldw<RO>(a + N + 2) | ldw<RO>(b + N + 2);
+        if (ldw<RO>(a + N + 1) && ldw<RO>(b + N + 1)) {
+            const long long s = (long long)(int)ldw<RO>(a + N) + (int)ldw<RO>(b + N) - 2 * (32 * N - 1);
+            lo = s < lo ? s : lo; hi = s + 64 * N > hi ? s + 64 * N : hi; ++cnt;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        st |= __shfl_xor_sync(0xffffffffu, st, o);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        const long long l2 = __shfl_xor_sync(0xffffffffu, lo, o), h2 = __shfl_xor_sync(0xffffffffu, hi, o);
+        lo = l2 < lo ? l2 : lo; hi = h2 > hi ? h2 : hi;
+    }
+    if (lane == 0) { s_lo[warp] = lo; s_hi[warp] = hi; s_st[warp] = st; s_cnt[warp] = cnt; }
+    __syncthreads();
+    st = 0; cnt = 0; lo = INT64_MAX; hi = INT64_MIN;
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) {
+        st |= s_st[w]; cnt += s_cnt[w];
+        lo = s_lo[w] < lo ? s_lo[w] : lo; hi = s_hi[w] > hi ? s_hi[w] : hi;
+    }
+    __syncthreads();                                                 // the slots are reused by the next call
+    if (st) return zero<N>(st);
+    if (!cnt) return zero<N>();
+    int logc = 0;
+    while ((1u << logc) < cnt + 2) ++logc;
+    Num<N> r = zero<N>();
+    if (hi - lo + logc + 1 >= 32 * (long long)W) {
+        if (tid == 0) store<N>(s_res, exact_dot_add_dev<N, RO>(nullptr, false, x, sx, y, sy, K, error));
+        __syncthreads();
+        r = load_plain<N>(s_res);
+        __syncthreads();
+        return r;
+    }
+    u32 acc[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) acc[w] = 0;
+    for (u64 k = tid; k < K; k += kQrThreads) {
+        const Num<N> a = ldn<N, RO>(x + (i64)k * sx * E), b = ldn<N, RO>(y + (i64)k * sy * E);
+        if (!a.s || !b.s) continue;
+        u32 p[2 * N], t[W];
+        mant_mul<N>(a.m, b.m, p);
+        place_words<W, 2 * N>(t, p, (i64)a.e + b.e - 2 * (32 * N - 1) - lo);
+        accumulate<W>(acc, t, a.s * b.s < 0);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        u32 other[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) other[w] = __shfl_down_sync(0xffffffffu, acc[w], o);
+        accumulate<W>(acc, other, false);
+    }
+    if (lane == 0)
+#pragma unroll
+        for (int w = 0; w < W; ++w) s_win[warp * W + w] = acc[w];
+    __syncthreads();
+    if (tid == 0) {
+        for (int v = 1; v < WARPS; ++v) {
+            u32 other[W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) other[w] = s_win[v * W + w];
+            accumulate<W>(acc, other, false);
+        }
+        int sign = 1;
+        if (acc[W - 1] >> 31) {
+            sign = -1; u64 cy = 1;
+#pragma unroll
+            for (int w = 0; w < W; ++w) { const u64 v = (u64)(u32)~acc[w] + cy; acc[w] = (u32)v; cy = v >> 32; }
+        }
+        store<N>(s_res, round_general<N, W>(acc, lo, sign, 0));
+    }
+    __syncthreads();
+    r = load_plain<N>(s_res);
+    __syncthreads();
+    return r;
+}
+
+// Pt <- the panel's columns of Wk, Vt <- 0.
+template <int N> __global__ void qr_load_kernel(QrPanel p) {
+    constexpr u64 E = N + 3;
+    const u64 q = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= p.kb * p.mr) return;
+    const u64 c = q / p.mr, r = q % p.mr;
+    const u32* src = p.Wk + ((p.k0 + r) * p.n + p.k0 + c) * E;
+    u32* dst = p.Pt + q * E;
+    u32* vt = p.Vt + q * E;
+#pragma unroll
+    for (u64 w = 0; w < E; ++w) { dst[w] = src[w]; vt[w] = 0; }
+}
+// The panel's columns and reflectors back into Wk and V.
+template <int N> __global__ void qr_store_kernel(QrPanel p) {
+    constexpr u64 E = N + 3;
+    const u64 q = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= p.kb * p.mr) return;
+    const u64 c = q / p.mr, r = q % p.mr;
+    const u64 at = ((p.k0 + r) * p.n + p.k0 + c) * E;
+#pragma unroll
+    for (u64 w = 0; w < E; ++w) { p.Wk[at + w] = p.Pt[q * E + w]; p.V[at + w] = p.Vt[q * E + w]; }
+}
+
+// Column c (j = k0 + c) by the panel's reflectors so far: x_r = D(x_r; Vt[0..q)[r], y[0..q)) for every row of the
+// panel, q = min(j, rank) - k0.  One warp per row.
+template <int N> __global__ void __launch_bounds__(256) qr_update_kernel(QrPanel p, u64 c) {
+    constexpr u64 E = N + 3;
+    const long long rank = p.st->rank, j = (long long)(p.k0 + c);
+    const long long q = (rank < j ? rank : j) - (long long)p.k0;
+    if (q <= 0) return;
+    const u64 r = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= p.mr) return;
+    u32* x = p.Pt + (c * p.mr + r) * E;
+    const Num<N> v = warp_exact_dot<N, true>(x, true, p.Vt + r * E, (i64)p.mr, p.y, 1, (u64)q, p.error);
+    if ((threadIdx.x & 31) == 0) store<N>(x, v);
+}
+
+// Reflector of column c from its reduced entries x = Pt[c][c..mr) (linalg.mm:675-690): s = P(x, x); a zero or
+// status column, or one failing the rank test, ends the factorization there; otherwise beta = -sgn(x0) sqrt(s),
+// v0 = RN(x0 - beta), v = 2^-e (v0, x1, ...) with e = exponent(v0) and tau = RN(2 / P(v, v)) (nothing below the
+// diagonal: tau = 0, v = e_c, beta = x0); r_jj = beta, T_cc = tau.  One block.
+template <int N> __global__ void __launch_bounds__(kQrThreads) qr_reflect_kernel(QrPanel p, u64 c) {
+    __shared__ __align__(16) u32 sm[qr_dot_words<N>()];
+    __shared__ long long s_e;
+    __shared__ int s_go;
+    constexpr u64 E = N + 3;
+    QrState* st = p.st;
+    if (st->rank < (long long)p.n) return;
+    const u64 j = p.k0 + c, len = p.mr - c;
+    u32* xc = p.Pt + (c * p.mr + c) * E;
+    u32* v = p.Vt + (c * p.mr + c) * E;
+    const Num<N> s = block_exact_dot<N, true>(xc, 1, xc, 1, len, sm, p.error);
+    int below = 0;
+    for (u64 r = 1 + threadIdx.x; r < len; r += kQrThreads) below |= ldw<true>(xc + r * E + N + 1) != 0;
+    below = __syncthreads_or(below);
+    Num<N> beta = zero<N>(), v0 = qr_pow2<N>(0);
+    if (threadIdx.x == 0) {
+        const Num<N> x0 = load_plain<N>(xc);
+        int reason = s.st ? 3 : (!x0.s && !below) ? 1 : 0;
+        beta = x0;
+        if (!reason && below) {
+            beta = sqrt<N>(s);
+            if (x0.s >= 0) beta = negate<N>(beta);
+            v0 = subx<N>(x0, beta);
+        }
+        if (!reason && p.rank_bits > 0 && st->have_top && (long long)beta.e + p.rank_bits < st->top) reason = 2;
+        if (reason) { st->rank = (long long)j; st->reason = reason; st->status = s.st; s_go = 0; }
+        else { s_go = 1; s_e = below ? (long long)v0.e : 0; }
+    }
+    __syncthreads();
+    if (!s_go) return;
+    const long long e = s_e;
+    if (below)
+        for (u64 r = 1 + threadIdx.x; r < len; r += kQrThreads) store<N>(v + r * E, qr_scaled<N>(load_plain<N>(xc + r * E), e));
+    if (threadIdx.x == 0) store<N>(v, below ? qr_scaled<N>(v0, e) : qr_pow2<N>(0));
+    __syncthreads();
+    Num<N> tj = zero<N>();
+    if (below) {
+        const Num<N> pv = block_exact_dot<N, false>(v, 1, v, 1, len, sm, p.error);
+        if (threadIdx.x == 0) tj = divx<N>(qr_pow2<N>(1), pv);
+    }
+    if (threadIdx.x == 0) {
+        store<N>(xc, beta);
+        store<N>(p.tau + j * E, tj);
+        store<N>(p.T + ((p.k0 / p.nb) * p.nb * p.nb + c * p.nb + c) * E, tj);
+        if (!st->have_top || (long long)beta.e > st->top) st->top = beta.e;
+        st->have_top = 1;
+    }
+}
+
+// After reflector c: block u < c gives G[u] = P(v_u, v_c), block u >= c the W row entry Wp[c][u+1] = P(v_c,
+// a_{u+1}) (the block-start column), both over rows [c, mr).  The last block to finish writes the T column,
+// T_lc = -RN(tau * P(T[l][l..c), G[l..c))) (linalg.mm:713), and the next column's y_i = P(T[0..i][i],
+// Wp[0..i][c+1]) for i < min(j + 1, rank) - k0 (linalg.mm:668), one warp per entry.  kb - 1 blocks.
+template <int N> __global__ void __launch_bounds__(kQrThreads) qr_dots_kernel(QrPanel p, u64 c) {
+    __shared__ __align__(16) u32 sm[qr_dot_words<N>()];
+    __shared__ int s_last;
+    constexpr u64 E = N + 3;
+    QrState* st = p.st;
+    const long long rank = st->rank;
+    const bool reflected = rank == (long long)p.n;
+    const u64 j = p.k0 + c, len = p.mr - c, u = blockIdx.x;
+    if (reflected && u + 1 < p.kb) {
+        const u32* v = p.Vt + (c * p.mr + c) * E;
+        const Num<N> d = u < c ? block_exact_dot<N, true>(p.Vt + (u * p.mr + c) * E, 1, v, 1, len, sm, p.error)
+                               : block_exact_dot<N, true>(v, 1, p.Pt + ((u + 1) * p.mr + c) * E, 1, len, sm, p.error);
+        if (threadIdx.x == 0) store<N>(u < c ? p.G + u * E : p.Wp + (c * p.nb + u + 1) * E, d);
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const u32 before = atomicAdd(&st->arrivals, 1u);
+        s_last = before == gridDim.x - 1;
+        if (s_last) st->arrivals = 0;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    u32* Tb = p.T + (p.k0 / p.nb) * p.nb * p.nb * E;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int WARPS = kQrThreads / 32;
+    if (reflected) {
+        const Num<N> tj = ldn<N, false>(p.tau + j * E);
+        for (u64 l = warp; l < c; l += WARPS) {
+            const Num<N> d = warp_exact_dot<N, false>(nullptr, false, Tb + (l * p.nb + l) * E, 1, p.G + l * E, 1, c - l, p.error);
+            if (lane == 0) store<N>(Tb + (l * p.nb + c) * E, negate<N>(mulx<N>(tj, d)));
+        }
+    }
+    __syncthreads();
+    if (c + 1 < p.kb) {
+        const long long qn = (rank < (long long)j + 1 ? rank : (long long)j + 1) - (long long)p.k0;
+        for (long long i = warp; i < qn; i += WARPS) {
+            const Num<N> d = warp_exact_dot<N, false>(nullptr, false, Tb + i * E, (i64)p.nb, p.Wp + (c + 1) * E, (i64)p.nb,
+                                                      (u64)i + 1, p.error);
+            if (lane == 0) store<N>(p.y + i * E, d);
+        }
+    }
+}
+
+// R (n x n) <- the upper triangle of Wk's first n rows; with rank p < n, rows i >= p keep columns j >= p.
+template <int N> __global__ void qr_extract_kernel(const u32* Wk, u32* R, u64 n, const QrState* st) {
+    constexpr u64 E = N + 3;
+    const u64 q = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n * n) return;
+    const u64 i = q / n, j = q % n, rank = (u64)st->rank;
+    const bool keep = j >= (i < rank ? i : rank);
+#pragma unroll
+    for (u64 w = 0; w < E; ++w) R[q * E + w] = keep ? Wk[q * E + w] : 0u;
+}
+// dst (rows x cols, row stride ld_dst) <- src (row stride ld_src), element copies.
+template <int N> __global__ void qr_copy_kernel(const u32* src, u64 ld_src, u32* dst, u64 ld_dst, u64 rows, u64 cols) {
+    constexpr u64 E = N + 3;
+    const u64 q = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= rows * cols) return;
+    const u64 i = q / cols, j = q % cols;
+#pragma unroll
+    for (u64 w = 0; w < E; ++w) dst[(i * ld_dst + j) * E + w] = src[(i * ld_src + j) * E + w];
+}
+
+struct QrKernels {
+    void (*load)(const QrPanel&, cudaStream_t);
+    void (*update)(const QrPanel&, u64 c, cudaStream_t);
+    void (*reflect)(const QrPanel&, u64 c, cudaStream_t);
+    void (*dots)(const QrPanel&, u64 c, cudaStream_t);
+    void (*store)(const QrPanel&, cudaStream_t);
+    void (*extract)(const u32* Wk, u32* R, u64 n, const QrState* st, cudaStream_t);
+    void (*copy)(const u32* src, u64 ld_src, u32* dst, u64 ld_dst, u64 rows, u64 cols, cudaStream_t);
+};
+const QrKernels* qr_kernels(int limbs);
+
+inline unsigned qr_grid(u64 items, unsigned threads) { return (unsigned)((items + threads - 1) / threads); }
+template <int N> void qr_load_launch(const QrPanel& p, cudaStream_t s) {
+    if (p.kb * p.mr) qr_load_kernel<N><<<qr_grid(p.kb * p.mr, 128), 128, 0, s>>>(p);
+}
+template <int N> void qr_store_launch(const QrPanel& p, cudaStream_t s) {
+    if (p.kb * p.mr) qr_store_kernel<N><<<qr_grid(p.kb * p.mr, 128), 128, 0, s>>>(p);
+}
+template <int N> void qr_update_launch(const QrPanel& p, u64 c, cudaStream_t s) {
+    if (p.mr) qr_update_kernel<N><<<qr_grid(p.mr * 32, 256), 256, 0, s>>>(p, c);
+}
+template <int N> void qr_reflect_launch(const QrPanel& p, u64 c, cudaStream_t s) { qr_reflect_kernel<N><<<1, kQrThreads, 0, s>>>(p, c); }
+template <int N> void qr_dots_launch(const QrPanel& p, u64 c, cudaStream_t s) {
+    if (p.kb > 1) qr_dots_kernel<N><<<(unsigned)(p.kb - 1), kQrThreads, 0, s>>>(p, c);
+}
+template <int N> void qr_extract_launch(const u32* Wk, u32* R, u64 n, const QrState* st, cudaStream_t s) {
+    if (n) qr_extract_kernel<N><<<qr_grid(n * n, 128), 128, 0, s>>>(Wk, R, n, st);
+}
+template <int N> void qr_copy_launch(const u32* src, u64 ld_src, u32* dst, u64 ld_dst, u64 rows, u64 cols, cudaStream_t s) {
+    if (rows * cols) qr_copy_kernel<N><<<qr_grid(rows * cols, 128), 128, 0, s>>>(src, ld_src, dst, ld_dst, rows, cols);
+}
+
+}  // namespace lfd
+
+#define LF_QR_INSTANTIATE(N)                                                                                        \
+    namespace lfd {                                                                                                 \
+    extern const QrKernels qr_kernels_##N;                                                                          \
+    const QrKernels qr_kernels_##N = {qr_load_launch<N>, qr_update_launch<N>, qr_reflect_launch<N>, qr_dots_launch<N>, \
+                                      qr_store_launch<N>, qr_extract_launch<N>, qr_copy_launch<N>};                 \
+    }

@@ -128,6 +128,26 @@ int main() {
             if (s.exponent != 4 || p.exponent != -2 || f.exponent != 3 || magnitude_compare(s, p) <= 0) { std::printf("host arithmetic FAILED\n"); return 1; }
             std::vector<Float<B>> xs(3, power<B>(1)), ys(3, power<B>(1));
             if (exact_dot(xs.data(), 1, ys.data(), 1, 3).limb[B / 32 - 1] != 0xC0000000u) { std::printf("exact_dot FAILED\n"); return 1; }
+            {   // Householder QR of diag(2, 2) stacked on a zero row: R = diag(2, 2), Q = I; least squares of (2, 4, 0) is (1, 2)
+                std::vector<Float<B>> qa = {power<B>(1), zero<B / 32>(), zero<B / 32>(), power<B>(1), zero<B / 32>(), zero<B / 32>()};
+                QROptions qopt;
+                qopt.block = 1;
+                QRFactor qf = la.factor_qr(B, qa.data(), 3, 2, qopt);
+                std::vector<Float<B>> qb = {power<B>(1), power<B>(2), zero<B / 32>()}, qx(2);
+                qf.solve(qb.data(), 1, qx.data());
+                if (!qf.full_rank() || qf.rows() != 3 || qf.cols() != 2 || qf.info().reason != QRInfo::full_rank || qx[0].exponent != 0 ||
+                    qx[1].exponent != 1) { std::printf("qr solve FAILED\n"); return 1; }
+                qf.apply_q(qb.data(), 1, true);
+                if (qb[1].exponent != 2) { std::printf("qr apply_q FAILED\n"); return 1; }
+                auto bq = e.make_buffer<Float<B>>(6);
+                bq.upload(qa.data(), 6);
+                QRFactor qg = la.factor_qr(bq, 3, 2, qopt);
+                if (std::memcmp(qg.r(), qf.r(), sizeof(Float<B>) * 4)) { std::printf("buffer qr FAILED\n"); return 1; }
+                QRFactor qm = std::move(qg);
+                if (!qg.empty() || qm.empty() || qm.pivoted() || qm.permutation()[1] != 1) { std::printf("qr move FAILED\n"); return 1; }
+                std::vector<Float<B>> dd(2, power<B>(0));
+                if (la.factor_qr_augmented(B, qa.data(), 3, 2, dd.data(), qopt).rows() != 5) { std::printf("augmented qr FAILED\n"); return 1; }
+            }
             check_library_version();
             if (!version_compatible(library_version(), header_version) || std::string(library_version_string()).empty()) { std::printf("version FAILED\n"); return 1; }
             std::printf("full surface ok\n");
