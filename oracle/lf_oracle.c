@@ -728,13 +728,18 @@ int lfo_recurrence(int bits, const word* seeds, const word* weights, word* out, 
 }
 
 /* ---------------------------------------------------------------- Householder QR
- * P(x, y; K) = RN(sum x_k y_k) and D(c; x, y; K) = RN(c - sum x_k y_k), one rounding each.  The
- * sequences are the column-by-column statements the reference's own test holds its library to, bit
- * for bit (tests/test_qr.cpp:33-68 unpivoted, :94-135 column-pivoted, :69-77 Q / Q^T, :78-86 and
- * :137-147 least squares); the blocked right-looking library form (src/linalg.mm:488-790) gives the
- * same bits.  Layout: A, V (m x n), R (n x n), T (blocks of nb x nb, block b at b*nb*nb, the
- * compact-WY upper triangles), tau (n), all row-major.  info: rank, reason (0 full rank, 1 zero
- * column, 2 small column, 3 status column), status, recomputed squared norms (pivoting). */
+ * P(x, y; K) = RN(sum x_k y_k) and D(c; x, y; K) = RN(c - sum x_k y_k), one rounding each.  Column by
+ * column (the order of the reference's tests/test_qr.cpp:33-135 programs) with the dot products of the
+ * reference library's blocked right-looking sequence (src/linalg.mm:488-790), so every rounding has the
+ * library's term set: a block applied after its panel forms W over all rows from its first row, Y with
+ * the whole block and X's update with the whole block (qr_block, linalg.mm:550-567); within a panel, a
+ * column's y_i has i+1 terms and every row is reduced with all of the panel's reflectors so far
+ * (linalg.mm:668-670).  The two term sets give the same values and differ only in which statuses a
+ * rounding sees: when a reflector after a block's first carries a status (v scaled out of the exponent
+ * range), the library gives the rows above it that status and the test's program does not; this file
+ * follows the library.  Layout: A, V (m x n), R (n x n), T (blocks of nb x nb, block b at b*nb*nb, the
+ * compact-WY upper triangles), tau (n), all row-major.  info: rank, reason (0 full rank, 1 zero column,
+ * 2 small column, 3 status column), status, recomputed squared norms (pivoting). */
 static void qr_power2(word* out, int n, int32_t e) { set_zero(out, n, 0); out[n - 1] = 0x80000000u; *EXP(out, n) = e; *SGN(out, n) = 1; }
 /* x * 2^-e exactly; an exponent leaving [-1e9, 1e9] gives zero with exponent_overflow (linalg.mm:492) */
 static void qr_scaled(word* out, const word* x, int n, long e) {
@@ -804,18 +809,24 @@ int lfo_qr(int bits, const word* A, size_t m, size_t nn, size_t block, int rank_
 #define A_(r, c) (a + ((r) * nn + (c)) * E)
 #define V_(r, c) (V + ((r) * nn + (c)) * E)
     for (size_t j = 0; j < nn; ++j) {
-        /* column j by the reflectors [0, min(j, rank)) in groups of whole blocks: w, y, one update rounding per entry */
-        const size_t qn = j < rank ? j : rank;
+        /* column j by the reflectors [0, min(j, rank)), block by block: an earlier block as its trailing update
+           (W over rows [b0, m), Y and the update with the whole block), j's own block as its panel (w_i over rows
+           [b0 + i, m), y_i with i + 1 terms, every row reduced with the q reflectors so far) */
+        const size_t qn = j < rank ? j : rank, own = j / nb * nb;
         for (size_t b0 = 0; b0 < qn; b0 += nb) {
-            const size_t kb = (b0 + nb < qn ? b0 + nb : qn) - b0;
+            const int panel = b0 == own;
+            const size_t kb = panel ? qn - b0 : (b0 + nb < nn ? b0 + nb : nn) - b0;
             const word* Tb = T + (b0 / nb) * nb * nb * E;
 #pragma omp parallel for schedule(dynamic, 1)
-            for (size_t i = 0; i < kb; ++i) QP(w + i * E, V_(b0 + i, b0 + i), nn, A_(b0 + i, j), nn, m - b0 - i);
-            for (size_t i = 0; i < kb; ++i) QP(y + i * E, Tb + i * E, nb, w, 1, i + 1);
+            for (size_t i = 0; i < kb; ++i) {
+                if (panel) QP(w + i * E, V_(b0 + i, b0 + i), nn, A_(b0 + i, j), nn, m - b0 - i);
+                else QP(w + i * E, V_(b0, b0 + i), nn, A_(b0, j), nn, m - b0);
+            }
+            for (size_t i = 0; i < kb; ++i) QP(y + i * E, Tb + i * E, nb, w, 1, panel ? i + 1 : kb);
 #pragma omp parallel for schedule(dynamic, 16)
             for (size_t r = 0; r < m - b0; ++r) {
                 word d[35];
-                QD(d, A_(b0 + r, j), V_(b0 + r, b0), 1, y, 1, kb < r + 1 ? kb : r + 1);
+                QD(d, A_(b0 + r, j), V_(b0 + r, b0), 1, y, 1, kb);
                 copy_num(A_(b0 + r, j), d, n);
             }
         }
@@ -899,7 +910,7 @@ int lfo_qr_pivoted(int bits, const word* A, size_t m, size_t nn, size_t block, i
                 const size_t t = perm[j]; perm[j] = perm[p]; perm[p] = t;
             }
             for (size_t r = 0; r < m - b0; ++r) {
-                if (c) QD(x + r * E, A_(b0 + r, j), V_(b0 + r, b0), 1, Yr + j * E, nn, c < r + 1 ? c : r + 1);
+                if (c) QD(x + r * E, A_(b0 + r, j), V_(b0 + r, b0), 1, Yr + j * E, nn, c);
                 else copy_num(x + r * E, A_(b0 + r, j), n);
             }
             word t[35];
@@ -933,20 +944,22 @@ int lfo_qr_pivoted(int bits, const word* A, size_t m, size_t nn, size_t block, i
             }
             for (size_t k = j + 1; k < nn; ++k) recomputed += redo[k] != 0;
         }
-        /* the block's reflectors on the remaining columns: X = D(X; V_b, Y) (after a failure, W and Y formed first) */
+        /* the block on the remaining columns, X = D(X; V_b, Y) with the whole block: with the W and Y rows formed
+           during the panel, or after a failure (reflectors [b0, rank), the block's other V and T entries zero)
+           with W over rows [b0, m) and Y formed afresh (linalg.mm:727-729, qr_block) */
         const size_t c0 = rank == nn ? b0 + kb : rank;
         if (g && c0 < nn && (rank == nn || fresh)) {
             if (fresh)
 #pragma omp parallel for schedule(dynamic, 1)
                 for (size_t k = c0; k < nn; ++k) {
-                    for (size_t i = 0; i < g; ++i) QP(Wr + (i * nn + k) * E, V_(b0 + i, b0 + i), nn, A_(b0 + i, k), nn, m - b0 - i);
-                    for (size_t i = 0; i < g; ++i) QP(Yr + (i * nn + k) * E, Tb + i * E, nb, Wr + k * E, nn, i + 1);
+                    for (size_t i = 0; i < kb; ++i) QP(Wr + (i * nn + k) * E, V_(b0, b0 + i), nn, A_(b0, k), nn, m - b0);
+                    for (size_t i = 0; i < kb; ++i) QP(Yr + (i * nn + k) * E, Tb + i * E, nb, Wr + k * E, nn, kb);
                 }
 #pragma omp parallel for schedule(dynamic, 16)
             for (size_t r = 0; r < m - b0; ++r)
                 for (size_t k = c0; k < nn; ++k) {
                     word d[35];
-                    QD(d, A_(b0 + r, k), V_(b0 + r, b0), 1, Yr + k * E, nn, g < r + 1 ? g : r + 1);
+                    QD(d, A_(b0 + r, k), V_(b0 + r, b0), 1, Yr + k * E, nn, kb);
                     copy_num(A_(b0 + r, k), d, n);
                 }
         }
@@ -963,25 +976,26 @@ int lfo_qr_pivoted(int bits, const word* A, size_t m, size_t nn, size_t block, i
     return 0;
 }
 
-/* C (m x nrhs) <- Q^T C (qt, blocks in order) or Q C (blocks in reverse), the blocks of reflectors [0, rank)
- * (tests/test_qr.cpp:69-77) */
+/* C (m x nrhs) <- Q^T C (qt, blocks in order) or Q C (blocks in reverse), the blocks holding reflectors [0, rank)
+ * (qr_apply_n, linalg.mm:750-766; the column form is tests/test_qr.cpp:69-77) */
 int lfo_qr_apply(int bits, size_t m, size_t nn, size_t block, size_t rank, const word* V, const word* T, word* C, size_t nrhs, int qt) {
     const int n = bits / 32; const size_t E = (size_t)n + 3;
     const size_t nb = qr_nb(block, nn), blocks = nb ? (rank + nb - 1) / nb : 0;
     for (size_t s = 0; s < blocks; ++s) {
-        const size_t b = qt ? s : blocks - 1 - s, b0 = b * nb, kb = (b0 + nb < rank ? b0 + nb : rank) - b0;
+        /* qr_block (linalg.mm:550-567): the whole block (V and T are zero beyond the rank), W over rows [b0, m) */
+        const size_t b = qt ? s : blocks - 1 - s, b0 = b * nb, kb = (b0 + nb < nn ? b0 + nb : nn) - b0;
         const word* Tb = T + b * nb * nb * E;
 #pragma omp parallel for schedule(dynamic, 1)
         for (size_t c = 0; c < nrhs; ++c) {
             word* w = (word*)malloc(sizeof(word) * E * (kb + 1)); word* y = (word*)malloc(sizeof(word) * E * (kb + 1));
-            for (size_t i = 0; i < kb; ++i) QP(w + i * E, V + ((b0 + i) * nn + b0 + i) * E, nn, C + ((b0 + i) * nrhs + c) * E, nrhs, m - b0 - i);
+            for (size_t i = 0; i < kb; ++i) QP(w + i * E, V + (b0 * nn + b0 + i) * E, nn, C + (b0 * nrhs + c) * E, nrhs, m - b0);
             for (size_t i = 0; i < kb; ++i) {
-                if (qt) QP(y + i * E, Tb + i * E, nb, w, 1, i + 1);
-                else QP(y + i * E, Tb + (i * nb + i) * E, 1, w + i * E, 1, kb - i);
+                if (qt) QP(y + i * E, Tb + i * E, nb, w, 1, kb);
+                else QP(y + i * E, Tb + (i * nb) * E, 1, w, 1, kb);
             }
             for (size_t r = b0; r < m; ++r) {
                 word d[35];
-                QD(d, C + (r * nrhs + c) * E, V + (r * nn + b0) * E, 1, y, 1, kb < r - b0 + 1 ? kb : r - b0 + 1);
+                QD(d, C + (r * nrhs + c) * E, V + (r * nn + b0) * E, 1, y, 1, kb);
                 copy_num(C + (r * nrhs + c) * E, d, n);
             }
             free(w); free(y);

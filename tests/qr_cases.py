@@ -77,6 +77,12 @@ def special_cases(bits, rng):
             A[r * 12, N] = np.int32(int(np.int32(A[r * 12, N].view(np.int32))) + 10).view(np.uint32)
     A[77 * 12] = nb.power(bits, -999999995)[0]
     out.append(("tiny entry in column 0", A, 150, 12, 0, None))
+    # the same in column 3 with zeros beside it in columns 0..2: reflector 3 carries the status; the rows above it
+    # see it in every later rounding that applies the block (the library's term sets)
+    A = matrix(bits, 60, 12, "moderate", rng)
+    A[37 * 12:37 * 12 + 3] = 0
+    A[37 * 12 + 3] = nb.power(bits, -999999995)[0]
+    out.append(("tiny entry in column 3", A, 60, 12, 0, 4))
     return out
 
 

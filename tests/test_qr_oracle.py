@@ -1,5 +1,5 @@
-"""CPU: pin the oracle's Householder QR (lf_oracle.c, the column-by-column sequence of the reference's
-tests/test_qr.cpp) before the GPU factor is checked against it.
+"""CPU: pin the oracle's Householder QR (lf_oracle.c: the column order of the reference's tests/test_qr.cpp with
+the term sets of its library's blocked sequence, src/linalg.mm:488-790) before the GPU factor is checked against it.
 
 * golden factors (tests/golden/qr_golden.npz) from the library's blocked right-looking sequence evaluated
   with the reference's own arithmetic (oracle/_ref's ref_qr_blocked);
@@ -71,9 +71,15 @@ def test_qr_oracle_fixture_ranks(oracle):
         if f["rank"] == n:
             assert f["reason"] == 0
     # the entry 2^-999999995 leaves the exponent range when v is scaled: tau carries exponent_overflow
-    label, A, m, n, rank_bits, _ = qc.special_cases(bits, rng)[-1]
+    cases = {c[0]: c for c in qc.special_cases(bits, rng)}
+    label, A, m, n, rank_bits, _ = cases["tiny entry in column 0"]
     f = oracle.qr(bits, A, m, n, 16, rank_bits)
     assert nb.status(f["tau"][:1])[0] == nb.EXPONENT_OVERFLOW
+    # reflector 3 carries the status: R's rows 0..2 in later columns see it (the library's term sets)
+    label, A, m, n, rank_bits, _ = cases["tiny entry in column 3"]
+    f = oracle.qr(bits, A, m, n, 16, rank_bits)
+    assert nb.status(f["tau"][3:4])[0] == nb.EXPONENT_OVERFLOW and f["rank"] == 4 and f["reason"] == 3
+    assert (nb.status(f["R"].reshape(n, n, -1)[0, 5:]) == nb.EXPONENT_OVERFLOW).all()
 
 
 def permuted(A, m, n, perm):
