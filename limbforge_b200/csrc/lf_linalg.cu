@@ -21,7 +21,7 @@ struct Linalg {
     lf_linalg_options options{};
     lf_linalg_report report{};
     DevBuf work[6];
-    DevBuf qr[11];                  // Householder QR scratch: W/Y blocks, panel, state, right-hand sides
+    DevBuf qr[13];                  // Householder QR scratch: W/Y blocks, panel, state, right-hand sides, pivoting
     DevBuf info_buf, error_buf, lines;
     ResidueEngine residue;
     // the factorizations' second product lane: trailing updates beyond the next block run on `side` while the
@@ -837,6 +837,114 @@ static lf_qr_info qr_device(Linalg& la, int bits, uint32_t* Wk, size_t m, size_t
     return info;
 }
 
+// Column-pivoted factorization (the pivoted branch of linalg.mm:600-731; no look-ahead: the next panel's columns
+// are chosen during it).  Each step picks the pivot, reduces the column with its Y entries, forms the reflector,
+// the Gram column and the W rows of every trailing column, then their Y rows, row j of R and the downdated norms
+// (recomputed where they collapse).  After the panel the block updates the trailing columns with those Y rows,
+// X = D(X; V_b, Y); after a failing column p it forms W and Y afresh for columns [p, n) and stops.  perm (n) receives
+// the permutation.
+static lf_qr_info qr_device_pivoted(Linalg& la, int bits, uint32_t* Wk, size_t m, size_t n, size_t nb, int rank_bits, uint32_t* V,
+                                    uint32_t* T, uint32_t* tau, uint32_t* R, size_t* perm_out) {
+    lf_qr_info info{};
+    info.rank = n;
+    auto w0 = Clock::now();
+    Engine& e = *la.engine;
+    cudaStream_t s = e.stream;
+    const int limbs = bits / 32;
+    const size_t E = limbs + 3, eb = E * 4;
+    const auto* qk = lfd::qr_kernels(limbs);
+    const size_t blocks = nb ? (n + nb - 1) / nb : 0;
+    cuda_check(cudaMemsetAsync(V, 0, m * n * eb, s), "memset");
+    cuda_check(cudaMemsetAsync(T, 0, blocks * nb * nb * eb, s), "memset");
+    cuda_check(cudaMemsetAsync(tau, 0, n * eb, s), "memset");
+    uint32_t* Wb = static_cast<uint32_t*>(la.qr[0].get(nb * n * eb + 16));
+    uint32_t* Yb = static_cast<uint32_t*>(la.qr[1].get(nb * n * eb + 16));
+    cuda_check(cudaMemsetAsync(Wb, 0, nb * n * eb, s), "memset");
+    cuda_check(cudaMemsetAsync(Yb, 0, nb * n * eb, s), "memset");
+    uint32_t* Pt = static_cast<uint32_t*>(la.qr[2].get(nb * m * eb + 16));
+    uint32_t* Vt = static_cast<uint32_t*>(la.qr[3].get(nb * m * eb + 16));
+    uint32_t* G = static_cast<uint32_t*>(la.qr[5].get(nb * eb + 16));
+    auto* st = static_cast<lfd::QrState*>(la.qr[7].get(sizeof(lfd::QrState)));
+    uint32_t* nu = static_cast<uint32_t*>(la.qr[11].get(2 * n * eb + 16));
+    auto* perm = static_cast<uint64_t*>(la.qr[12].get(n * 12 + 16));
+    uint32_t* flag = reinterpret_cast<uint32_t*>(perm + n);
+    cuda_check(cudaMemsetAsync(flag, 0, n * 4, s), "memset");
+    lfd::QrState host{};
+    host.rank = (long long)n;
+    cuda_check(cudaMemcpyAsync(st, &host, sizeof host, cudaMemcpyHostToDevice, s), "state");
+    uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));
+    cuda_check(cudaMemsetAsync(err, 0, 16, s), "memset");
+    const ProductLane lane = main_lane(la);
+    cudaEvent_t g0, g1;
+    cuda_check(cudaEventCreate(&g0), "event"); cuda_check(cudaEventCreate(&g1), "event");
+    cuda_check(cudaEventRecord(g0, s), "event");
+    lfd::QrPanel P{Wk, m, n, V, T, tau, Pt, Vt, nullptr, G, nullptr, 0, 0, nb, 0, rank_bits, st, err,
+                   1, Wb, Yb, nu, nu + n * E, perm, flag};
+    qk->norms(P, s);
+    for (size_t k0 = 0; k0 < n; k0 += nb) {
+        const size_t k1 = std::min(n, k0 + nb), b = k0 / nb;
+        auto t = Clock::now();
+        P.k0 = k0; P.kb = k1 - k0; P.mr = m - k0;
+        qk->load(P, s);
+        for (size_t c = 0; c < P.kb; ++c) {
+            qk->pivot(P, c, s);
+            qk->column(P, c, s);
+            qk->reflect(P, c, s);
+            qk->gramw(P, c, s);
+            qk->trailing(P, c, s);
+            qk->recompute(P, c, s);
+        }
+        qk->store(P, s);
+        cuda_check(cudaGetLastError(), "pivoted qr panel");
+        cuda_check(cudaMemcpyAsync(&host, st, sizeof host, cudaMemcpyDeviceToHost, s), "state");
+        cuda_check(cudaStreamSynchronize(s), "pivoted qr panel");
+        ++info.blocks;
+        info.panel_seconds += since(t);
+        t = Clock::now();
+        const size_t p = std::min(k1, (size_t)host.rank), kb = k1 - k0, mr = m - k0;
+        const uint32_t* Vb = V + (k0 * n + k0) * E;
+        const uint32_t* Tb = T + b * nb * nb * E;
+        if (p < k1) {
+            // reflectors [k0, p) on columns [p, n) with W and Y formed afresh (qr_block without have_y)
+            if (p > k0) {
+                const size_t c = n - p;
+                exact_product_on(la, lane, bits, {Vb, 1, n}, {Wk + (k0 * n + p) * E, 1, n}, kb, c, mr, Wb + p * E, n, false, false, s,
+                                 nullptr, false);
+                exact_product_on(la, lane, bits, {Tb, 1, nb}, {Wb + p * E, 1, n}, kb, c, kb, Yb + p * E, n, false, false, s, nullptr, false);
+                exact_product_on(la, lane, bits, {Vb, n, 1}, {Yb + p * E, 1, n}, mr, c, kb, Wk + (k0 * n + p) * E, n, true, false, s,
+                                 nullptr, false);
+                ++info.gpu_updates;
+            }
+            info.update_seconds += since(t);
+            break;
+        }
+        if (k1 < n) {
+            // X = D(X; V_b, Y) with the Y rows of the panel
+            exact_product_on(la, lane, bits, {Vb, n, 1}, {Yb + k1 * E, 1, n}, mr, n - k1, kb, Wk + (k0 * n + k1) * E, n, true, false, s,
+                             nullptr, false);
+            ++info.gpu_updates;
+        }
+        info.update_seconds += since(t);
+    }
+    qk->extract(Wk, R, n, st, s);
+    cuda_check(cudaGetLastError(), "qr extract");
+    cuda_check(cudaEventRecord(g1, s), "event");
+    uint32_t ev[3] = {0, 0, 0};
+    std::vector<uint64_t> hp(n);
+    cuda_check(cudaMemcpyAsync(&host, st, sizeof host, cudaMemcpyDeviceToHost, s), "state");
+    cuda_check(cudaMemcpyAsync(hp.data(), perm, n * 8, cudaMemcpyDeviceToHost, s), "permutation");
+    cuda_check(cudaMemcpyAsync(ev, err, 12, cudaMemcpyDeviceToHost, s), "error flag");
+    cuda_check(cudaStreamSynchronize(s), "pivoted qr");
+    float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
+    cudaEventDestroy(g0); cudaEventDestroy(g1);
+    if (ev[0] | ev[1]) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    for (size_t k = 0; k < n; ++k) perm_out[k] = (size_t)hp[k];
+    info.rank = (size_t)host.rank; info.reason = host.reason; info.status = host.status;
+    info.norm_recomputations = host.recomputed;
+    info.timing = {ms * 1e-3, since(w0)};
+    return info;
+}
+
 // C (device, m x nrhs) <- Q^T C (qt: blocks in order) or Q C (blocks in reverse) over the blocks holding reflectors
 // [0, rank) (qr_apply_n, linalg.mm:750-766).  Returns the device seconds.
 static double qr_apply_device(Linalg& la, const QrFactor& f, uint32_t* C, size_t nrhs, bool qt) {
@@ -912,7 +1020,6 @@ static void qr_factor_common(Linalg& la, QrFactor& f, const uint32_t* dA, int ra
     f.info = lf_qr_info{};
     f.info.rank = n;
     if (!n) return;
-    if (f.pivot) throw runtime_error("factor_qr: column pivoting is not available on this build");
     Engine& e = *la.engine;
     cudaStream_t s = e.stream;
     uint32_t* Wk = static_cast<uint32_t*>(la.work[4].get(m * n * eb));
@@ -921,7 +1028,8 @@ static void qr_factor_common(Linalg& la, QrFactor& f, const uint32_t* dA, int ra
     uint32_t* T = static_cast<uint32_t*>(f.dT.get(blocks * f.nb * f.nb * eb + 16));
     uint32_t* R = static_cast<uint32_t*>(f.dR.get(n * n * eb));
     uint32_t* tau = static_cast<uint32_t*>(la.qr[10].get(n * eb));
-    f.info = qr_device(la, f.bits, Wk, m, n, f.nb, rank_bits, V, T, tau, R);
+    f.info = f.pivot ? qr_device_pivoted(la, f.bits, Wk, m, n, f.nb, rank_bits, V, T, tau, R, f.perm.data())
+                     : qr_device(la, f.bits, Wk, m, n, f.nb, rank_bits, V, T, tau, R);
     cuda_check(cudaMemcpyAsync(f.R.data(), R, n * n * eb, cudaMemcpyDeviceToHost, s), "download");
     cuda_check(cudaMemcpyAsync(f.V.data(), V, m * n * eb, cudaMemcpyDeviceToHost, s), "download");
     if (blocks) cuda_check(cudaMemcpyAsync(f.T.data(), T, blocks * f.nb * f.nb * eb, cudaMemcpyDeviceToHost, s), "download");

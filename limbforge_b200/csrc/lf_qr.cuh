@@ -22,6 +22,7 @@ struct QrState {
     long long top;       // the largest exponent of an r_jj so far (valid when have_top)
     int have_top;
     u32 arrivals;        // blocks of the current dots launch that have finished
+    u32 recomputed;      // column pivoting: downdated squared norms recomputed from the reduced column
 };
 
 struct QrPanel {
@@ -33,6 +34,10 @@ struct QrPanel {
     int rank_bits;
     QrState* st;
     u32* error;                  // set when an exact sum exceeds the cluster window
+    // column pivoting (pivot != 0): W and Y rows of the trailing columns (nb x n), squared column norms nu and their
+    // last exact values nuref (n), the permutation (n) and the recomputation flags (n)
+    int pivot;
+    u32* Wr; u32* Yr; u32* nu; u32* nuref; u64* perm; u32* flag;
 };
 
 constexpr int kQrThreads = 256;
@@ -55,16 +60,25 @@ template <int N> __device__ __forceinline__ Num<N> qr_scaled(Num<N> x, long long
     return x;
 }
 
-// RN(sum_{k<K} x[k sx] y[k sy]) with one rounding, computed by the whole block (kQrThreads threads) and returned
-// to every thread; the contract of exact_dot (statuses first; no nonzero product gives zero).  Pass 1 reduces the
-// statuses, the number of nonzero products and the range of their scales; each thread then adds its products
-// into a two's-complement window anchored at the lowest scale, the warps sum their windows with shuffles and
-// thread 0 adds the warps' sums and rounds once.  A range wider than the window goes to the cluster method on
-// thread 0.  sm: qr_dot_words<N>() words of shared memory, 8-byte aligned.
-template <int N, bool RO> __device__ Num<N> block_exact_dot(const u32* x, i64 sx, const u32* y, i64 sy, u64 K, u32* sm, u32* error) {
+// Operands of term k of a strided dot: x[k sx] and y[k sy].  fallback: the cluster method on one thread.
+template <int N, bool RO> struct StridedPair {
+    const u32* x; i64 sx; const u32* y; i64 sy; u64 K;
+    __device__ void operands(u64 k, Num<N>& a, Num<N>& b) const {
+        constexpr i64 E = N + 3;
+        a = ldn<N, RO>(x + (i64)k * sx * E); b = ldn<N, RO>(y + (i64)k * sy * E);
+    }
+    __device__ Num<N> fallback(u32* error) const { return exact_dot_add_dev<N, RO>(nullptr, false, x, sx, y, sy, K, error); }
+};
+
+// RN(sum_{k<K} a_k b_k) with one rounding for the operands a_k, b_k that src gives, computed by the whole block
+// (kQrThreads threads) and returned to every thread; the contract of exact_dot (statuses first; no nonzero product
+// gives zero).  Pass 1 reduces the statuses, the number of nonzero products and the range of their scales; each
+// thread then adds its products into a two's-complement window anchored at the lowest scale, the warps sum their
+// windows with shuffles and thread 0 adds the warps' sums and rounds once.  A range wider than the window goes to
+// src.fallback (the cluster method) on thread 0.  sm: qr_dot_words<N>() words of shared memory, 8-byte aligned.
+template <int N, class Src> __device__ Num<N> block_exact_sum(const Src& src, u64 K, u32* sm, u32* error) {
     constexpr int W = qr_window<N>();
     constexpr int WARPS = kQrThreads / 32;
-    constexpr i64 E = N + 3;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     u32* s_win = sm;                                                 // WARPS windows
     long long* s_lo = reinterpret_cast<long long*>(sm + WARPS * W + (WARPS * W) % 2);
@@ -75,10 +89,11 @@ template <int N, bool RO> __device__ Num<N> block_exact_dot(const u32* x, i64 sx
     u32 st = 0, cnt = 0;
     long long lo = INT64_MAX, hi = INT64_MIN;
     for (u64 k = tid; k < K; k += kQrThreads) {
-        const u32* a = x + (i64)k * sx * E; const u32* b = y + (i64)k * sy * E;
-        st |= ldw<RO>(a + N + 2) | ldw<RO>(b + N + 2);
-        if (ldw<RO>(a + N + 1) && ldw<RO>(b + N + 1)) {
-            const long long s = (long long)(int)ldw<RO>(a + N) + (int)ldw<RO>(b + N) - 2 * (32 * N - 1);
+        Num<N> a, b;
+        src.operands(k, a, b);
+        st |= a.st | b.st;
+        if (a.s && b.s) {
+            const long long s = (long long)a.e + b.e - 2 * (32 * N - 1);
             lo = s < lo ? s : lo; hi = s + 64 * N > hi ? s + 64 * N : hi; ++cnt;
         }
     }
@@ -104,7 +119,7 @@ template <int N, bool RO> __device__ Num<N> block_exact_dot(const u32* x, i64 sx
     while ((1u << logc) < cnt + 2) ++logc;
     Num<N> r = zero<N>();
     if (hi - lo + logc + 1 >= 32 * (long long)W) {
-        if (tid == 0) store<N>(s_res, exact_dot_add_dev<N, RO>(nullptr, false, x, sx, y, sy, K, error));
+        if (tid == 0) store<N>(s_res, src.fallback(error));
         __syncthreads();
         r = load_plain<N>(s_res);
         __syncthreads();
@@ -114,7 +129,8 @@ template <int N, bool RO> __device__ Num<N> block_exact_dot(const u32* x, i64 sx
 #pragma unroll
     for (int w = 0; w < W; ++w) acc[w] = 0;
     for (u64 k = tid; k < K; k += kQrThreads) {
-        const Num<N> a = ldn<N, RO>(x + (i64)k * sx * E), b = ldn<N, RO>(y + (i64)k * sy * E);
+        Num<N> a, b;
+        src.operands(k, a, b);
         if (!a.s || !b.s) continue;
         u32 p[2 * N], t[W];
         mant_mul<N>(a.m, b.m, p);
@@ -152,6 +168,9 @@ template <int N, bool RO> __device__ Num<N> block_exact_dot(const u32* x, i64 sx
     __syncthreads();
     return r;
 }
+template <int N, bool RO> __device__ Num<N> block_exact_dot(const u32* x, i64 sx, const u32* y, i64 sy, u64 K, u32* sm, u32* error) {
+    return block_exact_sum<N>(StridedPair<N, RO>{x, sx, y, sy, K}, K, sm, error);
+}
 
 // Pt <- the panel's columns of Wk, Vt <- 0.
 template <int N> __global__ void qr_load_kernel(QrPanel p) {
@@ -165,12 +184,15 @@ template <int N> __global__ void qr_load_kernel(QrPanel p) {
 #pragma unroll
     for (u64 w = 0; w < E; ++w) { dst[w] = src[w]; vt[w] = 0; }
 }
-// The panel's columns and reflectors back into Wk and V.
+// The panel's columns and reflectors back into Wk and V; with pivoting only the columns before a failing one
+// (linalg.mm:718: the failing column stays as it was at the block start, swapped into place).
 template <int N> __global__ void qr_store_kernel(QrPanel p) {
     constexpr u64 E = N + 3;
     const u64 q = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= p.kb * p.mr) return;
     const u64 c = q / p.mr, r = q % p.mr;
+    const long long rank = p.st->rank;
+    if (p.pivot && rank < (long long)p.n && rank >= (long long)p.k0 && c >= (u64)(rank - (long long)p.k0)) return;
     const u64 at = ((p.k0 + r) * p.n + p.k0 + c) * E;
 #pragma unroll
     for (u64 w = 0; w < E; ++w) { p.Wk[at + w] = p.Pt[q * E + w]; p.V[at + w] = p.Vt[q * E + w]; }
@@ -291,6 +313,195 @@ template <int N> __global__ void __launch_bounds__(kQrThreads) qr_dots_kernel(Qr
     }
 }
 
+// ---- column pivoting (the pivoted branch of linalg.mm:600-719; xGEQP3 order) ----
+// Exact order of two squared norms for the pivot choice: +1 if x > y, -1 if x < y, 0 if equal; a status ranks above
+// every value and two statuses are equal (linalg.mm:541-547).
+template <int N> __device__ __forceinline__ int qr_order(const u32* x, const u32* y) {
+    const u32 sx = x[N + 2], sy = y[N + 2];
+    if (sx || sy) return (sx != 0) - (sy != 0);
+    const int a = (int)x[N + 1], b = (int)y[N + 1];
+    if (a != b) return a > b ? 1 : -1;
+    if (!a) return 0;
+    int c = 0;
+    if (x[N] != y[N]) c = (int)x[N] > (int)y[N] ? 1 : -1;
+    for (int i = N - 1; i >= 0 && !c; --i) if (x[i] != y[i]) c = x[i] > y[i] ? 1 : -1;
+    return a > 0 ? c : -c;
+}
+// nu_k = nuref_k = P(a_k, a_k) over all rows; perm = identity.  One block per column.
+template <int N> __global__ void __launch_bounds__(kQrThreads) qrp_norms_kernel(QrPanel p) {
+    __shared__ __align__(16) u32 sm[qr_dot_words<N>()];
+    constexpr u64 E = N + 3;
+    const u64 k = blockIdx.x;
+    const Num<N> d = block_exact_dot<N, true>(p.Wk + k * E, (i64)p.n, p.Wk + k * E, (i64)p.n, p.m, sm, p.error);
+    if (threadIdx.x == 0) { store<N>(p.nu + k * E, d); store<N>(p.nuref + k * E, d); p.perm[k] = k; }
+}
+// Step j = k0 + c: the remaining column with the largest nu (a status first; ties to the lowest original index) is
+// swapped with column j everywhere: Wk, the W and Y rows of this block's earlier steps, nu, nuref, perm.  One block.
+template <int N> __global__ void __launch_bounds__(kQrThreads) qrp_pivot_kernel(QrPanel p, u64 c) {
+    __shared__ u32 s_best[kQrThreads];
+    constexpr u64 E = N + 3;
+    if (p.st->rank < (long long)p.n) return;
+    const u64 j = p.k0 + c;
+    constexpr u32 kNone = 0xffffffffu;
+    auto better = [&](u32 a, u32 b) {
+        if (b == kNone) return a != kNone;
+        if (a == kNone) return false;
+        const int o = qr_order<N>(p.nu + (u64)a * E, p.nu + (u64)b * E);
+        return o > 0 || (o == 0 && p.perm[a] < p.perm[b]);
+    };
+    u32 best = kNone;
+    for (u64 k = j + threadIdx.x; k < p.n; k += kQrThreads)
+        if (better((u32)k, best)) best = (u32)k;
+    s_best[threadIdx.x] = best;
+    __syncthreads();
+    for (int h = kQrThreads / 2; h; h >>= 1) {
+        if ((int)threadIdx.x < h && better(s_best[threadIdx.x + h], s_best[threadIdx.x])) s_best[threadIdx.x] = s_best[threadIdx.x + h];
+        __syncthreads();
+    }
+    const u64 q = s_best[0];
+    if (q == j || q == kNone) return;
+    for (u64 r = threadIdx.x; r < p.m; r += kQrThreads)
+        for (u64 w = 0; w < E; ++w) {
+            u32* a = p.Wk + (r * p.n + j) * E + w; u32* b = p.Wk + (r * p.n + q) * E + w;
+            const u32 t = *a; *a = *b; *b = t;
+        }
+    for (u64 i = threadIdx.x; i < c; i += kQrThreads)
+        for (u64 w = 0; w < E; ++w) {
+            u32* a = p.Wr + (i * p.n + j) * E + w; u32* b = p.Wr + (i * p.n + q) * E + w;
+            u32 t = *a; *a = *b; *b = t;
+            a = p.Yr + (i * p.n + j) * E + w; b = p.Yr + (i * p.n + q) * E + w;
+            t = *a; *a = *b; *b = t;
+        }
+    if (threadIdx.x == 0) {
+        for (u64 w = 0; w < E; ++w) {
+            u32 t = p.nu[j * E + w]; p.nu[j * E + w] = p.nu[q * E + w]; p.nu[q * E + w] = t;
+            t = p.nuref[j * E + w]; p.nuref[j * E + w] = p.nuref[q * E + w]; p.nuref[q * E + w] = t;
+        }
+        const u64 t = p.perm[j]; p.perm[j] = p.perm[q]; p.perm[q] = t;
+    }
+}
+// Column j reduced by this block's reflectors so far with its Y entries from the earlier steps:
+// Pt[c][r] = D(a_{k0+r,j}; V_{k0+r}[k0, k0+c), Y[0..c)[j]) for every row of the panel (linalg.mm:662, 668-670).
+// One warp per row.
+template <int N> __global__ void __launch_bounds__(256) qrp_column_kernel(QrPanel p, u64 c) {
+    constexpr u64 E = N + 3;
+    if (p.st->rank < (long long)p.n) return;
+    const u64 r = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= p.mr) return;
+    const u64 j = p.k0 + c;
+    const u32* a = p.Wk + ((p.k0 + r) * p.n + j) * E;
+    u32* x = p.Pt + (c * p.mr + r) * E;
+    const Num<N> v = c ? warp_exact_dot<N, true>(a, true, p.Vt + r * E, (i64)p.mr, p.Yr + j * E, (i64)p.n, c, p.error)
+                       : ldn<N, true>(a);
+    if ((threadIdx.x & 31) == 0) store<N>(x, v);
+}
+// After reflector j: block u < c gives the Gram entry G[u] = P(v_u, v_j) over the panel rows [c, mr); block u >= c
+// the W row entry W[c][k] = P(v_j, a_k) over rows [j, m) of trailing column k = j + 1 + (u - c) (block-start values,
+// linalg.mm:636-645).  The last block to arrive writes the T column (linalg.mm:713).
+template <int N> __global__ void __launch_bounds__(kQrThreads) qrp_gramw_kernel(QrPanel p, u64 c) {
+    __shared__ __align__(16) u32 sm[qr_dot_words<N>()];
+    __shared__ int s_last;
+    constexpr u64 E = N + 3;
+    QrState* st = p.st;
+    if (st->rank < (long long)p.n) return;
+    const u64 j = p.k0 + c, len = p.mr - c, u = blockIdx.x;
+    const u32* v = p.Vt + (c * p.mr + c) * E;
+    if (u < c) {
+        const Num<N> d = block_exact_dot<N, true>(p.Vt + (u * p.mr + c) * E, 1, v, 1, len, sm, p.error);
+        if (threadIdx.x == 0) store<N>(p.G + u * E, d);
+    } else if (j + 1 + (u - c) < p.n) {
+        const u64 k = j + 1 + (u - c);
+        const Num<N> d = block_exact_dot<N, true>(v, 1, p.Wk + (j * p.n + k) * E, (i64)p.n, len, sm, p.error);
+        if (threadIdx.x == 0) store<N>(p.Wr + (c * p.n + k) * E, d);
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const u32 before = atomicAdd(&st->arrivals, 1u);
+        s_last = before == gridDim.x - 1;
+        if (s_last) st->arrivals = 0;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    u32* Tb = p.T + (p.k0 / p.nb) * p.nb * p.nb * E;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const Num<N> tj = ldn<N, false>(p.tau + j * E);
+    for (u64 l = warp; l < c; l += kQrThreads / 32) {
+        const Num<N> d = warp_exact_dot<N, false>(nullptr, false, Tb + (l * p.nb + l) * E, 1, p.G + l * E, 1, c - l, p.error);
+        if (lane == 0) store<N>(Tb + (l * p.nb + c) * E, negate<N>(mulx<N>(tj, d)));
+    }
+}
+// Every trailing column k > j: Y[c][k] = P(T[0..c][c], W[0..c][k]), r_jk = D(a_jk; V_j[k0..j], Y[0..c][k]) and
+// nu_k = D(nu_k; r_jk, r_jk); flag_k when nu_k drops to <= 0 or more than bits/2 binades below nuref_k (nuref_k a
+// status-free nonzero, nu_k status-free) (linalg.mm:714-723).  One warp per column.
+template <int N> __global__ void __launch_bounds__(256) qrp_trailing_kernel(QrPanel p, u64 c) {
+    constexpr u64 E = N + 3;
+    if (p.st->rank < (long long)p.n) return;
+    const u64 j = p.k0 + c;
+    const u64 k = j + 1 + (((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (k >= p.n) return;
+    const int lane = threadIdx.x & 31;
+    const u32* Tb = p.T + (p.k0 / p.nb) * p.nb * p.nb * E;
+    const Num<N> y = warp_exact_dot<N, true>(nullptr, false, Tb + c * E, (i64)p.nb, p.Wr + k * E, (i64)p.n, c + 1, p.error);
+    if (lane == 0) store<N>(p.Yr + (c * p.n + k) * E, y);
+    __syncwarp();
+    const Num<N> r = warp_exact_dot<N, false>(p.Wk + (j * p.n + k) * E, true, p.Vt + c * E, (i64)p.mr, p.Yr + k * E, (i64)p.n, c + 1,
+                                              p.error);
+    if (lane == 0) {
+        const Num<N> nu = negate<N>(fms<N>(r, r, ldn<N, false>(p.nu + k * E)));
+        const Num<N> ref = ldn<N, false>(p.nuref + k * E);
+        store<N>(p.nu + k * E, nu);
+        p.flag[k] = ref.s && !ref.st && !nu.st && (nu.s <= 0 || (long long)nu.e + 16 * N < (long long)ref.e);
+    }
+}
+// Operands of the recomputed squared norm: z_i = D(a_{k0+i,k}; V_{k0+i}[k0..j], Y[0..c][k]) for the panel rows i in
+// (c, mr), squared.  The fallback runs the cluster method over the same terms.
+template <int N> struct ReducedSquares {
+    const QrPanel* p; u64 c, k;
+    __device__ Num<N> z(u64 q) const {
+        constexpr u64 E = N + 3;
+        const u64 i = c + 1 + q;
+        return exact_dot_add_dev<N, true>(p->Wk + ((p->k0 + i) * p->n + k) * E, true, p->Vt + i * E, (i64)p->mr, p->Yr + k * E,
+                                          (i64)p->n, c + 1, p->error);
+    }
+    __device__ void operands(u64 q, Num<N>& a, Num<N>& b) const { a = z(q); b = a; }
+    // the cluster-method source: term q is z_q^2
+    __device__ u64 count() const { return p->mr - c - 1; }
+    __device__ bool term(u64 q, i64& scale, i64& top, int& sign) const {
+        const Num<N> a = z(q);
+        if (!a.s) return false;
+        scale = 2 * (i64)a.e - 2 * (32 * N - 1); top = scale + 64 * N; sign = 1;
+        return true;
+    }
+    __device__ void add(u64 q, u32* acc, int len, i64 off) const {
+        const Num<N> a = z(q);
+        u32 prod[2 * N];
+        mant_mul<N>(a.m, a.m, prod);
+        acc_add(acc, len, prod, 2 * N, off);
+    }
+    __device__ Num<N> fallback(u32* error) const {
+        u32 st = 0;
+        for (u64 q = 0; q < count(); ++q) st |= z(q).st;
+        if (st) return zero<N>(st);
+        return cluster_round<N, kClusterWords>(*this, error);
+    }
+};
+// Flagged columns: nu_k = nuref_k = P(z, z) over the reduced column below row j (linalg.mm:724-727).  One block per
+// trailing column; unflagged blocks return at once.
+template <int N> __global__ void __launch_bounds__(kQrThreads) qrp_recompute_kernel(QrPanel p, u64 c) {
+    __shared__ __align__(16) u32 sm[qr_dot_words<N>()];
+    constexpr u64 E = N + 3;
+    if (p.st->rank < (long long)p.n) return;
+    const u64 j = p.k0 + c, k = j + 1 + blockIdx.x;
+    if (k >= p.n || !p.flag[k]) return;
+    const ReducedSquares<N> src{&p, c, k};
+    const Num<N> d = block_exact_sum<N>(src, src.count(), sm, p.error);
+    if (threadIdx.x == 0) {
+        store<N>(p.nu + k * E, d); store<N>(p.nuref + k * E, d);
+        atomicAdd(&p.st->recomputed, 1u);
+    }
+}
+
 // R (n x n) <- the upper triangle of Wk's first n rows; with rank p < n, rows i >= p keep columns j >= p.
 template <int N> __global__ void qr_extract_kernel(const u32* Wk, u32* R, u64 n, const QrState* st) {
     constexpr u64 E = N + 3;
@@ -319,6 +530,13 @@ struct QrKernels {
     void (*store)(const QrPanel&, cudaStream_t);
     void (*extract)(const u32* Wk, u32* R, u64 n, const QrState* st, cudaStream_t);
     void (*copy)(const u32* src, u64 ld_src, u32* dst, u64 ld_dst, u64 rows, u64 cols, cudaStream_t);
+    // column pivoting
+    void (*norms)(const QrPanel&, cudaStream_t);
+    void (*pivot)(const QrPanel&, u64 c, cudaStream_t);
+    void (*column)(const QrPanel&, u64 c, cudaStream_t);
+    void (*gramw)(const QrPanel&, u64 c, cudaStream_t);
+    void (*trailing)(const QrPanel&, u64 c, cudaStream_t);
+    void (*recompute)(const QrPanel&, u64 c, cudaStream_t);
 };
 const QrKernels* qr_kernels(int limbs);
 
@@ -343,11 +561,33 @@ template <int N> void qr_copy_launch(const u32* src, u64 ld_src, u32* dst, u64 l
     if (rows * cols) qr_copy_kernel<N><<<qr_grid(rows * cols, 128), 128, 0, s>>>(src, ld_src, dst, ld_dst, rows, cols);
 }
 
+template <int N> void qrp_norms_launch(const QrPanel& p, cudaStream_t s) {
+    if (p.n) qrp_norms_kernel<N><<<(unsigned)p.n, kQrThreads, 0, s>>>(p);
+}
+template <int N> void qrp_pivot_launch(const QrPanel& p, u64 c, cudaStream_t s) { qrp_pivot_kernel<N><<<1, kQrThreads, 0, s>>>(p, c); }
+template <int N> void qrp_column_launch(const QrPanel& p, u64 c, cudaStream_t s) {
+    if (p.mr) qrp_column_kernel<N><<<qr_grid(p.mr * 32, 256), 256, 0, s>>>(p, c);
+}
+template <int N> void qrp_gramw_launch(const QrPanel& p, u64 c, cudaStream_t s) {
+    const u64 trailing = p.n - (p.k0 + c) - 1, blocks = c + trailing;
+    qrp_gramw_kernel<N><<<(unsigned)(blocks ? blocks : 1), kQrThreads, 0, s>>>(p, c);
+}
+template <int N> void qrp_trailing_launch(const QrPanel& p, u64 c, cudaStream_t s) {
+    const u64 trailing = p.n - (p.k0 + c) - 1;
+    if (trailing) qrp_trailing_kernel<N><<<qr_grid(trailing * 32, 256), 256, 0, s>>>(p, c);
+}
+template <int N> void qrp_recompute_launch(const QrPanel& p, u64 c, cudaStream_t s) {
+    const u64 trailing = p.n - (p.k0 + c) - 1;
+    if (trailing) qrp_recompute_kernel<N><<<(unsigned)trailing, kQrThreads, 0, s>>>(p, c);
+}
+
 }  // namespace lfd
 
 #define LF_QR_INSTANTIATE(N)                                                                                        \
     namespace lfd {                                                                                                 \
     extern const QrKernels qr_kernels_##N;                                                                          \
     const QrKernels qr_kernels_##N = {qr_load_launch<N>, qr_update_launch<N>, qr_reflect_launch<N>, qr_dots_launch<N>, \
-                                      qr_store_launch<N>, qr_extract_launch<N>, qr_copy_launch<N>};                 \
+                                      qr_store_launch<N>, qr_extract_launch<N>, qr_copy_launch<N>, qrp_norms_launch<N>,  \
+                                      qrp_pivot_launch<N>, qrp_column_launch<N>, qrp_gramw_launch<N>,                   \
+                                      qrp_trailing_launch<N>, qrp_recompute_launch<N>};                                 \
     }

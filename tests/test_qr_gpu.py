@@ -37,6 +37,9 @@ def bad(x, y):
 def check_factor(qr, want, label):
     assert (qr.info.rank, qr.info.reason, qr.info.status) == (want["rank"], want["reason"], want["status"]), \
         f"{label}: rank/reason/status {(qr.info.rank, qr.info.reason, qr.info.status)} want {(want['rank'], want['reason'], want['status'])}"
+    if want["perm"] is not None:
+        assert qr.pivoted and qr.permutation() == want["perm"], f"{label}: permutation {qr.permutation()} want {want['perm']}"
+        assert qr.info.norm_recomputations == want["recomputed"], f"{label}: recomputed norms"
     for k, got in (("R", qr.r()), ("V", qr.v()), ("tau", qr.tau()), ("T", qr.t())):
         w = want[k]
         assert got.shape == w.shape and (got == w).all(), f"{label}: {k} differs at {bad(got, w)}"
@@ -183,3 +186,55 @@ def test_qr_empty_and_invalid(la):
         la.factor_qr(bits, A, 4, 3, opts(8, rank_bits=-1))
     with pytest.raises(api.InvalidArgument):
         la.factor_qr(100, A, 4, 3)
+
+
+@pytest.mark.parametrize("bits", [64, 256, 384])
+def test_qr_pivoted_vs_oracle(la, oracle, bits):
+    rng = np.random.default_rng(400 + bits)
+    for i, (m, n, kind) in enumerate([(1, 1, "moderate"), (5, 3, "qsc"), (33, 7, "graded"), (60, 30, "qsc"), (64, 32, "wide"),
+                                      (70, 40, "spread"), (150, 60, "moderate")]):
+        A = qc.matrix(bits, m, n, kind, rng)
+        for block in (16, 7, 0):
+            want = oracle.qr(bits, A, m, n, block, 0, pivot=True)
+            qr = la.factor_qr(bits, A, m, n, opts(block, pivot=True))
+            label = f"pivoted bits={bits} {kind} {m}x{n} block {block}"
+            check_factor(qr, want, label)
+            nrhs = (1, 3, 5)[(i + block) % 3]
+            check_solves(qr, want, oracle, qc.rhs(bits, m, nrhs, rng), nrhs, label)
+
+
+def test_qr_pivoted_fixtures(la, oracle):
+    bits = 256
+    N = bits // 32
+    rng = np.random.default_rng(8)
+    cases = [("dependent", qc.matrix(bits, 41, 7, "dependent", rng), 41, 7, bits // 2, 5),
+             ("dependent 90x40", qc.matrix(bits, 90, 40, "dependent", rng), 90, 40, bits // 2, 38)]
+    A = qc.matrix(bits, 30, 12, "moderate", rng)
+    A[2::12] = 0
+    A[7::12] = 0
+    cases.append(("zero columns 2, 7", A, 30, 12, 0, 10))
+    A = qc.matrix(bits, 25, 9, "moderate", rng)
+    for r in range(25):
+        A[r * 9 + 6] = A[r * 9 + 2]
+        A[r * 9 + 8] = A[r * 9 + 2]
+    cases.append(("duplicate columns", A, 25, 9, bits // 2, 7))
+    A = qc.matrix(bits, 25, 10, "moderate", rng)
+    A[7 * 10 + 4, N + 2] = nb.INVALID
+    cases.append(("status at (7,4)", A, 25, 10, 0, 0))
+    A = qc.matrix(bits, 80, 20, "moderate", rng)
+    for j in (5, 13):
+        t = nb.random_numbers(rng, 80, bits, 4)
+        t[:, N] = (nb.exponent(t) - (bits // 4 + 10)).astype(np.int32).view(np.uint32)
+        A[j::20] = oracle.elementwise(bits, 0, np.ascontiguousarray(A[j - 1::20]), t)
+    cases.append(("nearly parallel columns", A, 80, 20, 0, None))
+    cases.append(("QSC-like", qc.matrix(bits, 300, 150, "qsc", rng), 300, 150, 0, None))
+    for label, A, m, n, rank_bits, expect in cases:
+        for block in (16, 7):
+            want = oracle.qr(bits, A, m, n, block, rank_bits, pivot=True)
+            qr = la.factor_qr(bits, A, m, n, opts(block, rank_bits, pivot=True))
+            check_factor(qr, want, f"{label} block {block}")
+            if expect is not None:
+                assert qr.info.rank == expect, label
+            if label == "nearly parallel columns":
+                assert qr.info.norm_recomputations > 0
+            check_solves(qr, want, oracle, qc.rhs(bits, m, 3, rng), 3, f"{label} block {block}")
