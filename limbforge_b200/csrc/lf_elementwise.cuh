@@ -160,12 +160,15 @@ template <int N> __device__ __forceinline__ Num<N> mul_pair(const Num<N>& a, con
         }
         h[2 * m + 3] = c;                                                // N - 1 + 2m - B + 2
     }
-    // T word w = h0[w + 1] + h1[w]: each lane sends its share of word w and adds the partner's
+    // T word w = h0[w + 1] + h1[w]: each lane sends its share of word w and adds the partner's.  The exchange names
+    // only the two lanes of the pair: other pairs of the warp may have left (a zero or status operand above, or a
+    // value past the end), and both lanes of a pair always take the same path (they hold the same a and y).
+    const u32 pair = 3u << ((threadIdx.x & 31) & ~1u);
     u32 cy = 0;
 #pragma unroll
     for (int w = 0; w < W; ++w) {
         const u32 mine = pl ? h[w] : h[w + 1];
-        const u32 other = __shfl_xor_sync(0xffffffffu, mine, 1);
+        const u32 other = __shfl_xor_sync(pair, mine, 1);
         const u64 t = (u64)mine + other + cy;
         h[w] = (u32)t;
         cy = (u32)(t >> 32);
