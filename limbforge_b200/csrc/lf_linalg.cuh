@@ -110,7 +110,7 @@ template <int N, bool RO> struct LineTerms {
         acc_add(acc, len, prod, 2 * N, off);
     }
 };
-template <int N, bool RO = true> __device__ Num<N> exact_dot_add_dev(const u32* cp, bool subtract, const u32* x, i64 sx, const u32* y, i64 sy,
+template <int N, bool RO = true> __device__ __noinline__ Num<N> exact_dot_add_dev(const u32* cp, bool subtract, const u32* x, i64 sx, const u32* y, i64 sy,
                                                      u64 K, u32* error) {
     constexpr i64 E = N + 3;
     const Num<N> c = cp ? load_plain<N>(cp) : zero<N>();
@@ -311,7 +311,7 @@ template <int N, int W> __device__ __forceinline__ Num<N> warp_round_window(cons
     return finish<N>(m, lo + 32 * (i64)top + 31 - lz, neg ? -1 : 1, rb && (sticky || (m[0] & 1u)), 0);
 }
 
-template <int N, bool RO> __device__ Num<N> warp_exact_dot(const u32* cp, bool subtract, const u32* x, i64 sx, const u32* y, i64 sy,
+template <int N, bool RO> __device__ __noinline__ Num<N> warp_exact_dot(const u32* cp, bool subtract, const u32* x, i64 sx, const u32* y, i64 sy,
                                                           u64 K, u32* error, u32* srow = nullptr) {
     constexpr int W = 2 * N + 10;
     constexpr i64 E = N + 3;

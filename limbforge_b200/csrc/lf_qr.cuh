@@ -76,7 +76,7 @@ template <int N, bool RO> struct StridedPair {
 // thread then adds its products into a two's-complement window anchored at the lowest scale, the warps sum their
 // windows with shuffles and thread 0 adds the warps' sums and rounds once.  A range wider than the window goes to
 // src.fallback (the cluster method) on thread 0.  sm: qr_dot_words<N>() words of shared memory, 8-byte aligned.
-template <int N, class Src> __device__ Num<N> block_exact_sum(const Src& src, u64 K, u32* sm, u32* error) {
+template <int N, class Src> __device__ __noinline__ Num<N> block_exact_sum(const Src& src, u64 K, u32* sm, u32* error) {
     constexpr int W = qr_window<N>();
     constexpr int WARPS = kQrThreads / 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;

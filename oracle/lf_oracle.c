@@ -1034,3 +1034,311 @@ int lfo_qr_solve(int bits, size_t m, size_t nn, size_t block, const long* info, 
 }
 #undef QP
 #undef QD
+
+/* ---------------------------------------------------------------- complex Householder QR
+ * The reference library's complex QR (src/linalg_complex.mm:125-306, zgeqrf convention: H = I - tau v v^H, complex
+ * tau, real beta), restated right-looking as the library runs it.  Every complex dot product or update is two real
+ * exact dot products over the interleaved (re, im) operand sequences, one rounding per component; the trailing
+ * block updates are the real compact-WY update (qr_block, linalg.mm:550-567) of the 2 x 2-block real embeddings
+ * of V and T ([[re, -im], [im, re]]) applied to the work matrix split by rows (row 2r = Re of row r, 2r + 1 = Im).
+ * Complex arrays hold (re, im) element pairs.  pivot: column pivoting with real squared norms downdated by
+ * |r_jk|^2 (linalg_complex.mm:160-255). */
+#define CQP(out, a, sa, b, sb, K) lfo_exact_dot_add(n, NULL, 0, (a), (long)(sa), (b), (long)(sb), (K), (out))
+#define CQD(out, c, a, sa, b, sb, K) lfo_exact_dot_add(n, (c), 1, (a), (long)(sa), (b), (long)(sb), (K), (out))
+/* the real block update of block b on columns [c0, c1) of X (row stride ld): W = P(V_b^T X) over rows [k0, mE),
+   Y = P(T_b^T W) (qt) or P(T_b W), X = D(X; V_b, Y), each with the whole block (have_y: Y given) */
+static void cqr_block(int n, size_t mE, size_t nE, size_t nbE, const word* EV, const word* ET, size_t b, word* X, size_t ld,
+                      size_t c0, size_t c1, int qt, word* Wb, word* Yb, int have_y) {
+    const size_t E = (size_t)n + 3;
+    const size_t k0 = b * nbE, kb = (k0 + nbE < nE ? k0 + nbE : nE) - k0, mr = mE - k0;
+    if (c1 <= c0 || !kb) return;
+    const word* Vb = EV + (k0 * nE + k0) * E; const word* Tb = ET + b * nbE * nbE * E; word* Xb = X + k0 * ld * E;
+    if (!have_y) {
+#pragma omp parallel for schedule(dynamic, 1)
+        for (size_t j = c0; j < c1; ++j) {
+            for (size_t i = 0; i < kb; ++i) CQP(Wb + (i * ld + j) * E, Vb + i * E, nE, Xb + j * E, ld, mr);
+            for (size_t i = 0; i < kb; ++i) {
+                if (qt) CQP(Yb + (i * ld + j) * E, Tb + i * E, nbE, Wb + j * E, ld, kb);
+                else CQP(Yb + (i * ld + j) * E, Tb + i * nbE * E, 1, Wb + j * E, ld, kb);
+            }
+        }
+    }
+#pragma omp parallel for schedule(dynamic, 8)
+    for (size_t r = 0; r < mr; ++r)
+        for (size_t j = c0; j < c1; ++j) {
+            word d[35];
+            CQD(d, Xb + (r * ld + j) * E, Vb + r * nE * E, 1, Yb + j * E, ld, kb);
+            copy_num(Xb + (r * ld + j) * E, d, n);
+        }
+}
+/* the 2 x 2 real block [[re, -im], [im, re]] of z at (2r, 2c) of a real matrix with row stride ld */
+static void cqr_embed(int n, word* M, size_t ld, size_t r, size_t c, const word* z) {
+    const size_t E = (size_t)n + 3;
+    copy_num(M + (2 * r * ld + 2 * c) * E, z, n); neg_copy(M + (2 * r * ld + 2 * c + 1) * E, z + E, n);
+    copy_num(M + ((2 * r + 1) * ld + 2 * c) * E, z + E, n); copy_num(M + ((2 * r + 1) * ld + 2 * c + 1) * E, z, n);
+}
+static void cqr_times_i(int n, word* out, const word* z) { const size_t E = (size_t)n + 3; word t[35]; neg_copy(t, z + E, n); copy_num(out + E, z, n); copy_num(out, t, n); }
+static void cqr_conj(int n, word* out, const word* z) { const size_t E = (size_t)n + 3; copy_num(out, z, n); neg_copy(out + E, z + E, n); }
+static void cqr_i_conj(int n, word* out, const word* z) { const size_t E = (size_t)n + 3; word t[35]; copy_num(t, z + E, n); copy_num(out + E, z, n); copy_num(out, t, n); }
+
+int lfo_qr_complex(int bits, const word* A, size_t m, size_t nn, size_t block, int rank_bits, int pivot, word* R, word* V, word* T,
+                   word* tau, size_t* perm, long* info) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3, C2 = 2 * E;
+    const size_t nb = qr_nb(block, nn), blocks = nb ? (nn + nb - 1) / nb : 0;
+    const size_t mE = 2 * m, nE = 2 * nn, nbE = 2 * nb;
+    word* Wk = (word*)calloc(E * (mE * nn + 1), sizeof(word));
+    word* EV = (word*)calloc(E * (mE * nE + 1), sizeof(word));
+    word* ET = (word*)calloc(E * (blocks * nbE * nbE + 1), sizeof(word));
+    word* Wb = (word*)calloc(E * (nbE * nn + 1), sizeof(word)); word* Yb = (word*)calloc(E * (nbE * nn + 1), sizeof(word));
+    word* Pt = (word*)calloc(C2 * (nb * m + 1), sizeof(word)); word* Vt = (word*)calloc(C2 * (nb * m + 1), sizeof(word));
+    word* Vi = (word*)calloc(C2 * (nb * m + 1), sizeof(word)); word* Vr = (word*)calloc(C2 * (nb * m + 1), sizeof(word));
+    word* Wp = (word*)calloc(C2 * (nb * nb + 1), sizeof(word));
+    word* G = (word*)calloc(C2 * (nb + 1), sizeof(word)); word* Gc = (word*)calloc(C2 * (nb + 1), sizeof(word));
+    word* Gic = (word*)calloc(C2 * (nb + 1), sizeof(word)); word* y = (word*)calloc(C2 * (nb + 1), sizeof(word));
+    word* yc = (word*)calloc(C2 * (nb + 1), sizeof(word)); word* yic = (word*)calloc(C2 * (nb + 1), sizeof(word));
+    word* tcol = (word*)calloc(C2 * (nb + 1), sizeof(word)); word* itcol = (word*)calloc(C2 * (nb + 1), sizeof(word));
+    word* wl = (word*)calloc(C2 * (nb + 1), sizeof(word));
+    word* nu = (word*)calloc(E * (nn + 1), sizeof(word)); word* nuref = (word*)calloc(E * (nn + 1), sizeof(word));
+    char* flag = (char*)calloc(nn + 1, 1);
+    memset(V, 0, sizeof(word) * C2 * m * nn); memset(T, 0, sizeof(word) * C2 * blocks * nb * nb); memset(tau, 0, sizeof(word) * C2 * nn);
+    size_t rank = nn; int reason = 0; word status = 0; int have_top = 0; long top = 0; long recomputed = 0;
+    word one[35], two[35]; qr_power2(one, n, 0); qr_power2(two, n, 1);
+#define W_(r, c) (Wk + ((r) * nn + (c)) * E)
+    for (size_t r = 0; r < m; ++r)
+        for (size_t j = 0; j < nn; ++j) { copy_num(W_(2 * r, j), A + (r * nn + j) * C2, n); copy_num(W_(2 * r + 1, j), A + (r * nn + j) * C2 + E, n); }
+    for (size_t k = 0; k < nn; ++k) perm[k] = k;
+    if (pivot)
+#pragma omp parallel for schedule(dynamic, 1)
+        for (size_t k = 0; k < nn; ++k) { CQP(nu + k * E, W_(0, k), nn, W_(0, k), nn, mE); copy_num(nuref + k * E, nu + k * E, n); }
+    size_t failed_done = 0;
+    for (size_t k0 = 0, first = 1; k0 < nn; first = 0) {
+        const size_t k1 = k0 + nb < nn ? k0 + nb : nn, kb = k1 - k0, mr = m - k0, b = k0 / nb;
+        word* Tb = T + b * nb * nb * C2;
+        (void)first;
+        /* ---- panel [k0, k1) */
+        for (size_t c = 0; c < kb; ++c) {
+            if (!pivot)
+                for (size_t r = 0; r < mr; ++r) { copy_num(Pt + (c * mr + r) * C2, W_(2 * (k0 + r), k0 + c), n); copy_num(Pt + (c * mr + r) * C2 + E, W_(2 * (k0 + r) + 1, k0 + c), n); }
+        }
+        memset(Vt, 0, sizeof(word) * C2 * kb * mr); memset(Vi, 0, sizeof(word) * C2 * kb * mr); memset(Vr, 0, sizeof(word) * C2 * mr * nb);
+        size_t done = kb;
+        for (size_t c = 0; c < kb; ++c) {
+            const size_t j = k0 + c;
+            word* x = Pt + c * mr * C2;
+            if (pivot) {
+                size_t p = j;
+                for (size_t k = j + 1; k < nn; ++k) { const int cmp = qr_compare(nu + k * E, nu + p * E, n); if (cmp > 0 || (cmp == 0 && perm[k] < perm[p])) p = k; }
+                if (p != j) {
+                    for (size_t r = 0; r < mE; ++r) qr_swap(W_(r, j), W_(r, p), n);
+                    for (size_t i = 0; i < 2 * c; ++i) { qr_swap(Wb + (i * nn + j) * E, Wb + (i * nn + p) * E, n); qr_swap(Yb + (i * nn + j) * E, Yb + (i * nn + p) * E, n); }
+                    qr_swap(nu + j * E, nu + p * E, n); qr_swap(nuref + j * E, nuref + p * E, n);
+                    const size_t t = perm[j]; perm[j] = perm[p]; perm[p] = t;
+                }
+                for (size_t r = 0; r < mr; ++r) { copy_num(x + r * C2, W_(2 * (k0 + r), j), n); copy_num(x + r * C2 + E, W_(2 * (k0 + r) + 1, j), n); }
+            }
+            const size_t q = (j < rank ? j : rank) - k0;
+            const int reflect = rank == nn;
+            for (size_t i = 0; i < q; ++i) {
+                if (pivot) { copy_num(y + i * C2, Yb + (2 * i * nn + j) * E, n); copy_num(y + i * C2 + E, Yb + ((2 * i + 1) * nn + j) * E, n); }
+                else {
+                    for (size_t l = 0; l <= i; ++l) { memcpy(tcol + l * C2, Tb + (l * nb + i) * C2, sizeof(word) * C2); cqr_times_i(n, itcol + l * C2, tcol + l * C2); memcpy(wl + l * C2, Wp + (l * nb + c) * C2, sizeof(word) * C2); }
+                    CQP(y + i * C2, tcol, 1, wl, 1, 2 * (i + 1)); CQP(y + i * C2 + E, itcol, 1, wl, 1, 2 * (i + 1));
+                }
+                cqr_conj(n, yc + i * C2, y + i * C2); cqr_i_conj(n, yic + i * C2, y + i * C2);
+            }
+            if (q)
+#pragma omp parallel for schedule(dynamic, 16)
+                for (size_t r = 0; r < mr; ++r) {
+                    word d[35];
+                    CQD(d, x + r * C2, Vr + r * nb * C2, 1, yc, 1, 2 * q); copy_num(x + r * C2, d, n);
+                    CQD(d, x + r * C2 + E, Vr + r * nb * C2, 1, yic, 1, 2 * q); copy_num(x + r * C2 + E, d, n);
+                }
+            if (!reflect) continue;
+            word* xc = x + c * C2; const size_t len = mr - c;
+            word s[35], beta[35], v0[35];
+            CQP(s, xc, 1, xc, 1, 2 * len);
+            int below = 0;
+            for (size_t r = 1; r < len; ++r) below |= gsgn(xc + r * C2, n) != 0 || gsgn(xc + r * C2 + E, n) != 0;
+            const int needs = below || gsgn(xc + E, n) != 0;
+            int why = gsts(s, n) ? 3 : (!gsgn(xc, n) && !gsgn(xc + E, n) && !below) ? 1 : 0;
+            copy_num(beta, xc, n); copy_num(v0, one, n);
+            if (!why && needs) { lfo_sqrt(n, s, beta); if (gsgn(xc, n) >= 0) *SGN(beta, n) = -gsgn(beta, n); lfo_sub(n, xc, beta, v0); }
+            if (!why && rank_bits > 0 && have_top && (long)gexp(beta, n) + rank_bits < top) why = 2;
+            if (why) { rank = j; reason = why; status = gsts(s, n); if (pivot) { done = c; break; } continue; }
+            word* vc = Vt + c * mr * C2; word* ic = Vi + c * mr * C2;
+            word tj[70]; memset(tj, 0, sizeof tj);
+            if (needs) {
+                const long e = gexp(v0, n);
+                qr_scaled(vc + c * C2, v0, n, e); qr_scaled(vc + c * C2 + E, xc + E, n, e);
+                for (size_t r = c + 1; r < mr; ++r) { qr_scaled(vc + r * C2, x + r * C2, n, e); qr_scaled(vc + r * C2 + E, x + r * C2 + E, n, e); }
+                word sv[35];
+                CQP(sv, vc + c * C2, 1, vc + c * C2, 1, 2 * len);
+                const word* vim = vc + c * C2 + E;
+                if (!gsgn(vim, n) && !gsts(vim, n)) lfo_div(n, two, sv, tj);
+                else {
+                    word a[35], sb[35], bb[35], d[35], z[35], t2[35];
+                    qr_scaled(a, sv, n, 1); qr_scaled(sb, beta, n, e); lfo_mul(n, sb, vim, bb);
+                    set_zero(z, n, 0); lfo_dot2_add(n, a, a, bb, bb, z, d);
+                    lfo_div(n, a, d, tj); lfo_div(n, bb, d, t2); neg_copy(tj + E, t2, n);
+                }
+            } else { copy_num(vc + c * C2, one, n); set_zero(vc + c * C2 + E, n, 0); }
+            copy_num(xc, beta, n); set_zero(xc + E, n, 0);
+            memcpy(tau + j * C2, tj, sizeof(word) * C2);
+            if (!have_top || (long)gexp(beta, n) > top) top = gexp(beta, n);
+            have_top = 1;
+            for (size_t r = c; r < mr; ++r) { cqr_times_i(n, ic + r * C2, vc + r * C2); memcpy(Vr + (r * nb + c) * C2, vc + r * C2, sizeof(word) * C2); }
+            /* Gram column and (unpivoted) the panel W row c */
+            const size_t ndots = pivot ? c : kb - 1;
+#pragma omp parallel for schedule(dynamic, 1)
+            for (size_t u = 0; u < ndots; ++u) {
+                if (u < c) {
+                    CQP(G + u * C2, Vt + (u * mr + c) * C2, 1, vc + c * C2, 1, 2 * len);
+                    CQP(G + u * C2 + E, Vi + (u * mr + c) * C2, 1, vc + c * C2, 1, 2 * len);
+                } else {
+                    CQP(Wp + (c * nb + u + 1) * C2, vc + c * C2, 1, Pt + ((u + 1) * mr + c) * C2, 1, 2 * len);
+                    CQP(Wp + (c * nb + u + 1) * C2 + E, ic + c * C2, 1, Pt + ((u + 1) * mr + c) * C2, 1, 2 * len);
+                }
+            }
+            if (pivot)
+#pragma omp parallel for schedule(dynamic, 1)
+                for (size_t k = j + 1; k < nn; ++k) {
+                    CQP(Wb + (2 * c * nn + k) * E, vc + c * C2, 1, W_(2 * (k0 + c), k), nn, 2 * len);
+                    CQP(Wb + ((2 * c + 1) * nn + k) * E, ic + c * C2, 1, W_(2 * (k0 + c), k), nn, 2 * len);
+                }
+            /* T column: T_cc = tau, T_lc = -RN(tau * P(T_b[l][l..c) . G[l..c))) per component */
+            for (size_t l = 0; l < c; ++l) { cqr_conj(n, Gc + l * C2, G + l * C2); cqr_i_conj(n, Gic + l * C2, G + l * C2); }
+            memcpy(Tb + (c * nb + c) * C2, tj, sizeof(word) * C2);
+            for (size_t l = 0; l < c; ++l) {
+                word p[70], z[70], zero2[70];
+                CQP(p, Tb + (l * nb + l) * C2, 1, Gc + l * C2, 1, 2 * (c - l));
+                CQP(p + E, Tb + (l * nb + l) * C2, 1, Gic + l * C2, 1, 2 * (c - l));
+                memset(zero2, 0, sizeof zero2);
+                lfo_cfma(n, tj, p, zero2, 0, z);
+                neg_copy(Tb + (l * nb + c) * C2, z, n); neg_copy(Tb + (l * nb + c) * C2 + E, z + E, n);
+            }
+            if (pivot && j + 1 < nn) {
+                for (size_t l = 0; l <= c; ++l) { memcpy(tcol + l * C2, Tb + (l * nb + c) * C2, sizeof(word) * C2); cqr_times_i(n, itcol + l * C2, tcol + l * C2); }
+#pragma omp parallel for schedule(dynamic, 1)
+                for (size_t k = j + 1; k < nn; ++k) {
+                    word* yk = (word*)malloc(sizeof(word) * C2 * (c + 1)); word* yik = (word*)malloc(sizeof(word) * C2 * (c + 1));
+                    CQP(Yb + (2 * c * nn + k) * E, tcol, 1, Wb + k * E, nn, 2 * (c + 1));
+                    CQP(Yb + ((2 * c + 1) * nn + k) * E, itcol, 1, Wb + k * E, nn, 2 * (c + 1));
+                    for (size_t l = 0; l <= c; ++l) {
+                        word z[70]; copy_num(z, Yb + (2 * l * nn + k) * E, n); copy_num(z + E, Yb + ((2 * l + 1) * nn + k) * E, n);
+                        cqr_conj(n, yk + l * C2, z); cqr_i_conj(n, yik + l * C2, z);
+                    }
+                    word rj[70], d[35];
+                    CQD(rj, W_(2 * j, k), Vr + c * nb * C2, 1, yk, 1, 2 * (c + 1));
+                    CQD(rj + E, W_(2 * j + 1, k), Vr + c * nb * C2, 1, yik, 1, 2 * (c + 1));
+                    CQD(d, nu + k * E, rj, 1, rj, 1, 2);
+                    copy_num(nu + k * E, d, n);
+                    const word* ref = nuref + k * E;
+                    flag[k] = gsgn(ref, n) && !gsts(ref, n) && !gsts(d, n) && (gsgn(d, n) <= 0 || (long)gexp(d, n) + 16L * n < (long)gexp(ref, n));
+                    if (flag[k]) {
+                        const size_t zl = m - j - 1;
+                        word* z = (word*)malloc(sizeof(word) * C2 * (zl + 1));
+                        for (size_t r = j + 1; r < m; ++r) {
+                            CQD(z + (r - j - 1) * C2, W_(2 * r, k), Vr + (r - k0) * nb * C2, 1, yk, 1, 2 * (c + 1));
+                            CQD(z + (r - j - 1) * C2 + E, W_(2 * r + 1, k), Vr + (r - k0) * nb * C2, 1, yik, 1, 2 * (c + 1));
+                        }
+                        CQP(nu + k * E, z, 1, z, 1, 2 * zl);
+                        copy_num(nuref + k * E, nu + k * E, n);
+                        free(z);
+                    }
+                    free(yk); free(yik);
+                }
+                for (size_t k = j + 1; k < nn; ++k) recomputed += flag[k] != 0;
+            }
+        }
+        /* write back the panel (R entries and remainders), V and its embedding, and the embedding of T_b */
+        for (size_t r = 0; r < mr; ++r)
+            for (size_t c = 0; c < done; ++c) {
+                const word* xv = Pt + (c * mr + r) * C2; const word* vv = Vt + (c * mr + r) * C2;
+                copy_num(W_(2 * (k0 + r), k0 + c), xv, n); copy_num(W_(2 * (k0 + r) + 1, k0 + c), xv + E, n);
+                memcpy(V + ((k0 + r) * nn + k0 + c) * C2, vv, sizeof(word) * C2);
+                cqr_embed(n, EV, nE, k0 + r, k0 + c, vv);
+            }
+        word* Eb = ET + b * nbE * nbE * E;
+        for (size_t l = 0; l < kb; ++l) for (size_t c = l; c < kb; ++c) cqr_embed(n, Eb, nbE, l, c, Tb + (l * nb + c) * C2);
+        const size_t p = k1 < rank ? k1 : rank;
+        /* the block on the trailing columns (one update of columns [k1, n) gives the bits of the look-ahead split) */
+        if (pivot) {
+            if (p < k1) { if (p > k0) cqr_block(n, mE, nE, nbE, EV, ET, b, Wk, nn, p, nn, 1, Wb, Yb, 0); break; }
+            if (k1 < nn) cqr_block(n, mE, nE, nbE, EV, ET, b, Wk, nn, k1, nn, 1, Wb, Yb, 1);
+        } else {
+            if (p < k1) { if (p > k0 && k1 < nn) cqr_block(n, mE, nE, nbE, EV, ET, b, Wk, nn, k1, nn, 1, Wb, Yb, 0); break; }
+            if (k1 < nn) cqr_block(n, mE, nE, nbE, EV, ET, b, Wk, nn, k1, nn, 1, Wb, Yb, 0);
+        }
+        k0 = k1;
+        failed_done = done;
+    }
+    (void)failed_done;
+    for (size_t i = 0; i < nn; ++i)
+        for (size_t j = 0; j < nn; ++j) {
+            word* out = R + (i * nn + j) * C2;
+            if (j >= (i < rank ? i : rank)) { copy_num(out, W_(2 * i, j), n); copy_num(out + E, W_(2 * i + 1, j), n); }
+            else { set_zero(out, n, 0); set_zero(out + E, n, 0); }
+        }
+#undef W_
+    info[0] = (long)rank; info[1] = reason; info[2] = (long)status; info[3] = recomputed;
+    free(Wk); free(EV); free(ET); free(Wb); free(Yb); free(Pt); free(Vt); free(Vi); free(Vr); free(Wp); free(G); free(Gc); free(Gic);
+    free(y); free(yc); free(yic); free(tcol); free(itcol); free(wl); free(nu); free(nuref); free(flag);
+    return 0;
+}
+static void cqr_embeddings(int n, size_t m, size_t nn, size_t nb, const word* V, const word* T, word* EV, word* ET) {
+    const size_t E = (size_t)n + 3, C2 = 2 * E, blocks = nb ? (nn + nb - 1) / nb : 0;
+    for (size_t r = 0; r < m; ++r) for (size_t c = 0; c < nn; ++c) cqr_embed(n, EV, 2 * nn, r, c, V + (r * nn + c) * C2);
+    for (size_t b = 0; b < blocks; ++b)
+        for (size_t l = 0; l < nb; ++l) for (size_t c = l; c < nb; ++c) cqr_embed(n, ET + b * 4 * nb * nb * E, 2 * nb, l, c, T + (b * nb * nb + l * nb + c) * C2);
+    (void)C2;
+}
+/* B (m x nrhs complex) <- Q^H B (adjoint, blocks in order) or Q B (reverse) over the blocks holding reflectors [0, rank):
+ * the real block updates of the embeddings on B split by rows (linalg_complex.mm:311-325) */
+int lfo_qr_complex_apply(int bits, size_t m, size_t nn, size_t block, size_t rank, const word* V, const word* T, word* B, size_t nrhs, int adjoint) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3, C2 = 2 * E;
+    const size_t nb = qr_nb(block, nn), blocks = nb ? (rank + nb - 1) / nb : 0, nblk = nb ? (nn + nb - 1) / nb : 0;
+    if (!blocks || !nrhs || !m) return 0;
+    word* EV = (word*)calloc(E * (4 * m * nn + 1), sizeof(word)); word* ET = (word*)calloc(E * (4 * nblk * nb * nb + 1), sizeof(word));
+    word* W = (word*)calloc(E * (2 * m * nrhs + 1), sizeof(word));
+    word* Wb = (word*)calloc(E * (2 * nb * nrhs + 1), sizeof(word)); word* Yb = (word*)calloc(E * (2 * nb * nrhs + 1), sizeof(word));
+    cqr_embeddings(n, m, nn, nb, V, T, EV, ET);
+    for (size_t r = 0; r < m; ++r) for (size_t c = 0; c < nrhs; ++c) { copy_num(W + (2 * r * nrhs + c) * E, B + (r * nrhs + c) * C2, n); copy_num(W + ((2 * r + 1) * nrhs + c) * E, B + (r * nrhs + c) * C2 + E, n); }
+    for (size_t q = 0; q < blocks; ++q) cqr_block(n, 2 * m, 2 * nn, 2 * nb, EV, ET, adjoint ? q : blocks - 1 - q, W, nrhs, 0, nrhs, adjoint, Wb, Yb, 0);
+    for (size_t r = 0; r < m; ++r) for (size_t c = 0; c < nrhs; ++c) { copy_num(B + (r * nrhs + c) * C2, W + (2 * r * nrhs + c) * E, n); copy_num(B + (r * nrhs + c) * C2 + E, W + ((2 * r + 1) * nrhs + c) * E, n); }
+    free(EV); free(ET); free(W); free(Wb); free(Yb);
+    return 0;
+}
+/* X = R^-1 (Q^H B)[0, n): the real backward substitution on the embedding of R (blocks 2 min(nb, p)); pivoted: the leading
+ * 2p x 2p block, x[perm[i]] = z_i, zero beyond p; rank-deficient unpivoted or a status column: invalid zeros
+ * (linalg_complex.mm:331-345) */
+int lfo_qr_complex_solve(int bits, size_t m, size_t nn, size_t block, const long* info, const size_t* perm, const word* R,
+                         const word* V, const word* T, const word* B, size_t nrhs, word* X) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3, C2 = 2 * E;
+    const size_t p = (size_t)info[0];
+    if (!nn || !nrhs) return 0;
+    if (p < nn && (!perm || info[1] == 3)) {
+        for (size_t q = 0; q < nn * nrhs; ++q) { set_zero(X + q * C2, n, ST_INVALID | (perm ? (word)info[2] : 0)); set_zero(X + q * C2 + E, n, ST_INVALID | (perm ? (word)info[2] : 0)); }
+        return 0;
+    }
+    word* C = (word*)malloc(sizeof(word) * C2 * (m * nrhs + 1));
+    memcpy(C, B, sizeof(word) * C2 * m * nrhs);
+    lfo_qr_complex_apply(bits, m, nn, block, p, V, T, C, nrhs, 1);
+    const size_t nb = qr_nb(block, nn), P2 = 2 * p;
+    word* L = (word*)calloc(E * (P2 * P2 + 1), sizeof(word));      /* transpose of the leading 2p x 2p block of R's embedding */
+    word* Cs = (word*)calloc(E * (P2 * nrhs + 1), sizeof(word));
+    word* ER = (word*)calloc(E * (4 * p * p + 1), sizeof(word));
+    for (size_t i = 0; i < p; ++i) for (size_t j = 0; j < p; ++j) cqr_embed(n, ER, P2, i, j, R + (i * nn + j) * C2);
+    for (size_t i = 0; i < P2; ++i) for (size_t j = 0; j < P2; ++j) copy_num(L + (j * P2 + i) * E, ER + (i * P2 + j) * E, n);
+    for (size_t i = 0; i < p; ++i) for (size_t c = 0; c < nrhs; ++c) { copy_num(Cs + (2 * i * nrhs + c) * E, C + (i * nrhs + c) * C2, n); copy_num(Cs + ((2 * i + 1) * nrhs + c) * E, C + (i * nrhs + c) * C2 + E, n); }
+    if (p) lfo_solve(bits, L, P2, Cs, nrhs, 2 * (nb < p ? nb : p), 2);
+    for (size_t i = 0; i < nn; ++i)
+        for (size_t c = 0; c < nrhs; ++c) {
+            word* out = X + ((perm ? perm[i] : i) * nrhs + c) * C2;
+            if (i < p) { copy_num(out, Cs + (2 * i * nrhs + c) * E, n); copy_num(out + E, Cs + ((2 * i + 1) * nrhs + c) * E, n); }
+            else { set_zero(out, n, 0); set_zero(out + E, n, 0); }
+        }
+    free(C); free(L); free(Cs); free(ER);
+    return 0;
+}
+#undef CQP
+#undef CQD

@@ -72,6 +72,9 @@ class Oracle:
         lib.lfo_qr_pivoted.argtypes = [I, V, S, S, S, I, V, V, V, V, C.POINTER(C.c_size_t), C.POINTER(C.c_long)]
         lib.lfo_qr_apply.argtypes = [I, S, S, S, S, V, V, V, S, I]
         lib.lfo_qr_solve.argtypes = [I, S, S, S, C.POINTER(C.c_long), C.POINTER(C.c_size_t), V, V, V, V, S, V]
+        lib.lfo_qr_complex.argtypes = [I, V, S, S, S, I, I, V, V, V, V, C.POINTER(C.c_size_t), C.POINTER(C.c_long)]
+        lib.lfo_qr_complex_apply.argtypes = [I, S, S, S, S, V, V, V, S, I]
+        lib.lfo_qr_complex_solve.argtypes = [I, S, S, S, C.POINTER(C.c_long), C.POINTER(C.c_size_t), V, V, V, V, S, V]
         self.lib = lib
 
     def elementwise(self, bits, op, a, b=None, c=None, b_index=(1, 0), c_index=(1, 0)):
@@ -202,6 +205,43 @@ class Oracle:
         if f["n"] and nrhs:
             self.lib.lfo_qr_solve(f["bits"], f["m"], f["n"], f["block"], info, perm, _ptr(f["R"]), _ptr(f["V"]),
                                   _ptr(f["T"]), _ptr(np.ascontiguousarray(B)), nrhs, _ptr(X))
+        return X[:f["n"] * nrhs]
+
+
+    def qr_complex(self, bits, A, m, n, block=32, rank_bits=0, pivot=False):
+        """Complex Householder QR of A (m * n complex elements, shape [m * n, 2, N + 3]); the factor dict as qr's."""
+        w = bits // 32 + 3
+        nb = block if block and block < n else n
+        blocks = (n + nb - 1) // nb if nb else 0
+        R = np.zeros((max(n * n, 1), 2, w), dtype=np.uint32)
+        V = np.zeros((max(m * n, 1), 2, w), dtype=np.uint32)
+        T = np.zeros((max(blocks * nb * nb, 1), 2, w), dtype=np.uint32)
+        tau = np.zeros((max(n, 1), 2, w), dtype=np.uint32)
+        info = (C.c_long * 4)()
+        pm = (C.c_size_t * max(n, 1))()
+        A = np.ascontiguousarray(A.reshape(m * n, 2, w)) if m * n else np.zeros((1, 2, w), dtype=np.uint32)
+        self.lib.lfo_qr_complex(bits, _ptr(A), m, n, block, rank_bits, int(bool(pivot)), _ptr(R), _ptr(V), _ptr(T), _ptr(tau), pm, info)
+        return {"bits": bits, "m": m, "n": n, "block": block, "nb": nb, "R": R[:n * n], "V": V[:m * n],
+                "T": T[:blocks * nb * nb], "tau": tau[:n], "rank": int(info[0]), "reason": int(info[1]),
+                "status": int(info[2]), "recomputed": int(info[3]), "perm": [int(pm[i]) for i in range(n)] if pivot else None,
+                "complex": True}
+
+    def qr_complex_apply(self, f, B, nrhs, adjoint):
+        out = np.ascontiguousarray(B.copy())
+        if f["m"] and nrhs:
+            self.lib.lfo_qr_complex_apply(f["bits"], f["m"], f["n"], f["block"], f["rank"], _ptr(np.ascontiguousarray(f["V"])),
+                                          _ptr(np.ascontiguousarray(f["T"])), _ptr(out), nrhs, int(bool(adjoint)))
+        return out
+
+    def qr_complex_solve(self, f, B, nrhs):
+        w = f["bits"] // 32 + 3
+        X = np.zeros((max(f["n"] * nrhs, 1), 2, w), dtype=np.uint32)
+        info = (C.c_long * 4)(f["rank"], f["reason"], f["status"], f["recomputed"])
+        perm = (C.c_size_t * max(f["n"], 1))(*f["perm"]) if f["perm"] is not None else None
+        if f["n"] and nrhs:
+            self.lib.lfo_qr_complex_solve(f["bits"], f["m"], f["n"], f["block"], info, perm, _ptr(np.ascontiguousarray(f["R"])),
+                                          _ptr(np.ascontiguousarray(f["V"])), _ptr(np.ascontiguousarray(f["T"])),
+                                          _ptr(np.ascontiguousarray(B)), nrhs, _ptr(X))
         return X[:f["n"] * nrhs]
 
 

@@ -94,3 +94,27 @@ def augmented(bits, J, m, n, d):
     for i in range(n):
         S[(m + i) * n + i] = d[i]
     return S
+
+
+def complex_matrix(bits, m, n, kind, rng):
+    """m x n complex row-major matrix, shape (m * n, 2, N + 3): independent real and imaginary parts of `kind`
+    (the dependent kind keeps its dependence: both parts repeat column 1 in the last column and negate column 0
+    in column n // 2)."""
+    w = bits // 32 + 3
+    A = np.zeros((m * n, 2, w), dtype=np.uint32)
+    A[:, 0] = matrix(bits, m, n, kind, rng)
+    A[:, 1] = matrix(bits, m, n, kind, rng)
+    if kind == "dependent" and n >= 3:
+        for r in range(m):
+            A[r * n + n - 1] = A[r * n + 1]
+            A[r * n + n // 2, 0] = nb.negate(A[r * n, 0][None])[0]
+            A[r * n + n // 2, 1] = nb.negate(A[r * n, 1][None])[0]
+    return A
+
+
+def complex_rhs(bits, m, nrhs, rng):
+    w = bits // 32 + 3
+    B = np.zeros((m * nrhs, 2, w), dtype=np.uint32)
+    B[:, 0] = rhs(bits, m, nrhs, rng)
+    B[:, 1] = rhs(bits, m, nrhs, rng)
+    return B

@@ -177,3 +177,96 @@ def test_qr_planted_mistake_is_caught(oracle, qr_golden):
     f = oracle.qr(bits, qr_golden["c1_A"], m, n, block, rank_bits)
     f["R"][5, 0] ^= 1
     assert not (f["R"] == qr_golden["c1_R"]).all()
+
+
+# ---- complex QR (lf_oracle.c lfo_qr_complex: the library's complex sequence, linalg_complex.mm)
+def test_qr_complex_real_input_is_the_real_qr(oracle):
+    """The reference test's own cross-check (tests/test_qr_complex.cpp:7): a real matrix gives the real QR bit for bit
+    in the real parts and zero imaginary parts, unpivoted and pivoted, with the same solves and Q applications."""
+    bits = 256
+    w = bits // 32 + 3
+    rng = np.random.default_rng(21)
+    for m, n, kind, block in [(33, 7, "graded", 32), (40, 21, "qsc", 8), (50, 33, "spread", 16), (20, 9, "moderate", 4)]:
+        A = qc.matrix(bits, m, n, kind, rng)
+        Ac = np.zeros((m * n, 2, w), np.uint32)
+        Ac[:, 0] = A
+        for pivot in (False, True):
+            fc, fr = oracle.qr_complex(bits, Ac, m, n, block, 0, pivot), oracle.qr(bits, A, m, n, block, 0, pivot)
+            for k in ("R", "V", "tau", "T"):
+                assert (fc[k][:, 0] == fr[k]).all() and (fc[k][:, 1] == 0).all(), f"{kind} {k} pivot={pivot}"
+            assert fc["perm"] == fr["perm"] and fc["rank"] == fr["rank"]
+            B = qc.rhs(bits, m, 3, rng)
+            Bc = np.zeros((m * 3, 2, w), np.uint32)
+            Bc[:, 0] = B
+            X = oracle.qr_complex_solve(fc, Bc, 3)
+            assert (X[:, 0] == oracle.qr_solve(fr, B, 3)).all() and (X[:, 1] == 0).all()
+            for qt in (True, False):
+                C1 = oracle.qr_complex_apply(fc, Bc, 3, qt)
+                assert (C1[:, 0] == oracle.qr_apply(fr, B, 3, qt)).all() and (C1[:, 1] == 0).all()
+
+
+def cfrac(z):
+    return [(nb.to_fraction(v[0]), nb.to_fraction(v[1])) for v in z]
+
+
+def ccheck(x, y, bits, lost):
+    fx, fy = cfrac(x), cfrac(y)
+    scale = max(max(abs(a), abs(b)) for a, b in fy)
+    return all(abs(a - c) <= scale / 2 ** (bits - lost) and abs(b - d) <= scale / 2 ** (bits - lost) for (a, b), (c, d) in zip(fx, fy))
+
+
+def test_qr_complex_properties(oracle):
+    bits = 256
+    N = bits // 32
+    rng = np.random.default_rng(22)
+    m, n, nrhs = 30, 12, 2
+    for pivot in (False, True):
+        A = qc.complex_matrix(bits, m, n, "moderate", rng)
+        f = oracle.qr_complex(bits, A, m, n, 5, 0, pivot)
+        assert f["rank"] == n
+        assert (f["R"].reshape(n, n, 2, -1)[np.arange(n), np.arange(n), 1] == 0).all()      # real diagonal
+        B = qc.complex_rhs(bits, m, nrhs, rng)
+        back = oracle.qr_complex_apply(f, oracle.qr_complex_apply(f, B, nrhs, True), nrhs, False)
+        assert ccheck(back, B, bits, 16)
+        # a consistent system B = A X0 (each component one exact dot), solved back to X0 up to rounding
+        X0 = np.zeros((n * nrhs, 2, N + 3), np.uint32)
+        X0[:, 0] = nb.random_numbers(rng, n * nrhs, bits, 2)
+        X0[:, 1] = nb.random_numbers(rng, n * nrhs, bits, 2)
+        Bc = np.zeros((m * nrhs, 2, N + 3), np.uint32)
+        for r in range(m):
+            a = np.ascontiguousarray(A[r * n:(r + 1) * n].reshape(2 * n, -1))
+            for c in range(nrhs):
+                x = X0[c::nrhs][:n]
+                xr = np.ascontiguousarray(np.stack([x[:, 0], nb.negate(x[:, 1])], 1).reshape(2 * n, -1))
+                xi = np.ascontiguousarray(np.stack([x[:, 1], x[:, 0]], 1).reshape(2 * n, -1))
+                Bc[r * nrhs + c, 0] = oracle.exact_dot_add(bits, None, False, a, 1, xr, 1, 2 * n)
+                Bc[r * nrhs + c, 1] = oracle.exact_dot_add(bits, None, False, a, 1, xi, 1, 2 * n)
+        assert ccheck(oracle.qr_complex_solve(f, Bc, nrhs), X0, bits, 40)
+        if pivot:
+            AP = A.reshape(m, n, 2, -1)[:, f["perm"]].reshape(m * n, 2, -1).copy()
+            u = oracle.qr_complex(bits, AP, m, n, 5)
+            for k in ("R", "V", "tau", "T"):
+                assert (u[k] == f[k]).all(), f"pivoted complex vs A P: {k}"
+
+
+def test_qr_complex_fixture_ranks(oracle):
+    bits = 256
+    N = bits // 32
+    rng = np.random.default_rng(23)
+    A = qc.complex_matrix(bits, 20, 9, "moderate", rng)
+    A[3::9] = 0
+    assert oracle.qr_complex(bits, A, 20, 9, 4)["rank"] == 3
+    A = qc.complex_matrix(bits, 25, 10, "moderate", rng)
+    A[7 * 10 + 4, 1, N + 2] = nb.INVALID
+    f = oracle.qr_complex(bits, A, 25, 10, 4)
+    assert (f["rank"], f["reason"], f["status"]) == (4, 3, nb.INVALID)
+    f = oracle.qr_complex(bits, qc.complex_matrix(bits, 41, 7, "dependent", rng), 41, 7, 16, bits // 2)
+    assert f["rank"] == 3 and f["reason"] == 2
+    f = oracle.qr_complex(bits, qc.complex_matrix(bits, 41, 7, "dependent", rng), 41, 7, 16, bits // 2, True)
+    assert f["rank"] == 5
+    # a column that is purely imaginary on the diagonal and zero below still reflects (tau complex)
+    A = qc.complex_matrix(bits, 6, 3, "moderate", rng)
+    A[0::3] = 0
+    A[0, 1] = nb.power(bits, 3)[0]
+    f = oracle.qr_complex(bits, A, 6, 3, 2)
+    assert f["rank"] == 3 and nb.sign(f["tau"][0, 1][None])[0] != 0
