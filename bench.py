@@ -487,6 +487,127 @@ def qr_2000(torch, api, scale=1.0):
             "normal_equations_residual_binades": ortho_binades}
 
 
+def qr_complex_800(torch, api, scale=1.0):
+    """Complex Householder QR least squares (256 bits, block 32, 4 right-hand sides) on an 800 x 400 complex QSC-like J
+    (real and imaginary parts drawn as the real QR workload's), the shape of the reference's complex QR benchmark; factor +
+    solve through the host-array API, best of 3; the whole factor and solution of a 160 x 80 matrix of the same kind
+    against the oracle."""
+    from oracle.oracle import Oracle
+    from tests import qr_cases as qc
+    bits, nrhs = 256, 4
+    n = max(8, int(round(400 * scale)))
+    m = 2 * n
+    rng = np.random.default_rng(43)
+    A = qc.complex_matrix(bits, m, n, "qsc", rng)
+    B = qc.complex_rhs(bits, m, nrhs, rng)
+    eng = api.Engine()
+    la = api.Linalg(eng)
+    o = api.QROptions(block=32)
+    best = None
+    for _ in range(3):
+        t0 = time.perf_counter()
+        qr = la.factor_qr_complex(bits, A, m, n, o)
+        t1 = time.perf_counter()
+        qr.solve(B, nrhs)
+        t2 = time.perf_counter()
+        run = {"factor_s": t1 - t0, "solve_s": t2 - t1, "e2e_s": t2 - t0, "factor_gpu_s": qr.info.timing.gpu_seconds,
+               "panel_s": qr.info.panel_seconds, "update_s": qr.info.update_seconds}
+        if best is None or run["e2e_s"] < best["e2e_s"]:
+            best = run
+    orc = Oracle()
+    ps = int(os.environ.get("LF_CQR_PARITY_N", "80"))
+    rngp = np.random.default_rng(44)
+    Ap = qc.complex_matrix(bits, 2 * ps, ps, "qsc", rngp)
+    Bp = qc.complex_rhs(bits, 2 * ps, nrhs, rngp)
+    t0 = time.perf_counter()
+    want = orc.qr_complex(bits, Ap, 2 * ps, ps, 32)
+    t_orc = time.perf_counter() - t0
+    got = la.factor_qr_complex(bits, Ap, 2 * ps, ps, o)
+    match = all((a == b).all() for a, b in ((got.r(), want["R"]), (got.v(), want["V"]), (got.tau(), want["tau"]), (got.t(), want["T"])))
+    match = match and (got.info.rank, got.info.reason, got.info.status) == (want["rank"], want["reason"], want["status"])
+    solve_match = bool((got.solve(Bp, nrhs) == orc.qr_complex_solve(want, Bp, nrhs)).all())
+    return {"workload": f"256-bit complex Householder QR least squares, QSC-like J {m}x{n} (block 32), {nrhs} right-hand sides",
+            **best, "rank": qr.info.rank, "reference_m5max_e2e_ms": 259.28 if n == 400 else None,
+            "parity": {"size": f"{2 * ps}x{ps}", "factor_match": bool(match), "solve_match": solve_match, "oracle_s": t_orc}}
+
+
+def exact_gemm4_448(torch, api, scale=1.0):
+    """Exact batched 4 x 4 product, 448-bit complex, 100,000 matrices (the largest configuration of the reference's
+    exact 4 x 4 experiment), accumulate into C: resident batch (device time and wall) and host arrays (wall, transfers
+    included), beside the composed (rounded-per-step) strided GEMM of the same shape; best of 5 each.  Every result of
+    the first 10,000 matrices against the oracle."""
+    from limbforge_b200 import numbers as nb
+    from oracle.oracle import Oracle
+    bits, cx = 448, True
+    count = max(16, int(round(100000 * scale)))
+    rng = np.random.default_rng(77)
+    A, B, C0 = (nb.random_complex(rng, count * 16, bits, 30, zero_frac=0.01, sparse_frac=0.05) for _ in range(3))
+    eng = api.Engine()
+    g = api.ExactGemm4(eng)
+    shape = api.ExactGemm4Shape(count, 16, 16, 16, True, False)
+    bufs = [eng.make_buffer(count * 16, bits, cx) for _ in range(3)]
+    for b, x in zip(bufs, (A, B, C0)):
+        b.upload(x)
+
+    def resident():
+        bt = eng.batch()
+        g.encode(bt, shape, *bufs)
+        return bt.submit().wait()
+    for _ in range(3):
+        resident()
+    res = [resident() for _ in range(5)]
+    host = []
+    for _ in range(3 + 5):
+        C = C0.copy()
+        t0 = time.perf_counter()
+        g.gemm(bits, cx, shape, A, B, C)
+        host.append(time.perf_counter() - t0)
+    host = host[3:]
+    bl = api.BatchedLinalg(eng)
+    sg = api.StridedGemm(count, 4, 4, 4, 16, 16, 16, accumulate=True)
+    composed = []
+    for _ in range(3 + 5):
+        bt = eng.batch()
+        bl.gemm_resident(bt, sg, *bufs)
+        composed.append(bt.submit().wait())
+    composed = composed[3:]
+    pc = min(count, 10000)
+    sh = {"count": pc, "stride_a": 16, "stride_b": 16, "stride_c": 16, "accumulate": True, "negative": False}
+    want = Oracle().exact_gemm4(bits, cx, sh, A[:pc * 16], B[:pc * 16], C0[:pc * 16])
+    match = bool((C[:pc * 16] == want).all())
+    dev_ms = min(t.gpu_seconds for t in res) * 1e3
+    # algorithmic bytes: A, B read and C read + written once, 2 * (N + 3) words per complex element
+    el = 2 * (bits // 32 + 3) * 4
+    moved = count * 16 * el * 4
+    return {"workload": f"exact batched 4x4 product, {bits}-bit complex, {count} matrices, accumulate",
+            "resident_device_ms": dev_ms, "resident_wall_ms": min(t.wall_seconds for t in res) * 1e3,
+            "host_wall_ms": min(host) * 1e3, "composed_device_ms": min(t.gpu_seconds for t in composed) * 1e3,
+            "matrices_per_s": count / (dev_ms * 1e-3), "algorithmic_gb_s": moved / (dev_ms * 1e-3) / 1e9,
+            "reference_m5max_resident_ms": 49.015 if count == 100000 else None,
+            "reference_m5max_host_ms": 49.277 if count == 100000 else None,
+            "parity": {"checked_matrices": pc, "match": match}}
+
+
+def mpfr_bridge():
+    """MPFR bridge throughput (host): ns per value of from_mpfr / to_mpfr arrays on one thread and on every host
+    thread, beside the mpz route, at 224/256/384/1024 bits and MPFR precisions bits, bits + 64 and bits - 32 (the grid
+    of the reference's benchmarks/bridge.cpp), 65,536 values, median of 5.  Built here with g++ against the installed
+    MPFR/GMP runtime libraries."""
+    import subprocess
+    import tempfile
+    root = os.path.dirname(os.path.abspath(__file__))
+    with tempfile.TemporaryDirectory() as d:
+        exe = os.path.join(d, "bridge")
+        subprocess.run(["g++", "-std=c++17", "-O2", f"-I{root}/include", f"-I{root}/tests/cpp/mpfr_decl",
+                        os.path.join(root, "tests", "cpp", "bridge.cpp"), "-o", exe, "-l:libmpfr.so.6", "-l:libgmp.so.10",
+                        "-pthread"], check=True, capture_output=True)
+        ok = subprocess.run([exe, "self"], capture_output=True, text=True, timeout=300)
+        r = subprocess.run([exe, "time", "65536", "5"], capture_output=True, text=True, timeout=600, check=True)
+    rows = [json.loads(line) for line in r.stdout.splitlines() if line.startswith("{")]
+    return {"workload": "MPFR bridge, 65,536 values per array", "self_checks": "bridge ok" in ok.stdout, "rows": rows,
+            "reference_m5max": "2-4 ns/value for threaded arrays on 3-16 threads (docs/optimizations.md, loaded host)"}
+
+
 def ragged_batch(torch, api, scale=1.0):
     """20,000 complex GEMMs, m, n, k uniform in {4..48}, precision uniform in {128, 256, 512, 1024},
     plus 200,000 4x4 complex LU solves at 512 bits, as one CUDA graph launch of a tuned ragged plan
@@ -574,7 +695,10 @@ def run_workloads(args):
                      ("exact_gemm_512bit_1024", lambda: exact_gemm_512(torch, api, args.scale)),
                      ("cholesky_256bit_2048", lambda: cholesky_2048(torch, api)),
                      ("qr_256bit_2000x1000", lambda: qr_2000(torch, api, args.scale)),
-                     ("ragged_batch_20000", lambda: ragged_batch(torch, api, args.scale))):
+                     ("qr_complex_256bit_800x400", lambda: qr_complex_800(torch, api, args.scale)),
+                     ("exact_gemm4_448bit_complex_100000", lambda: exact_gemm4_448(torch, api, args.scale)),
+                     ("ragged_batch_20000", lambda: ragged_batch(torch, api, args.scale)),
+                     ("mpfr_bridge", mpfr_bridge)):
         if args.workload and name != args.workload:
             continue
         t0 = time.perf_counter()

@@ -14,6 +14,15 @@ struct StridedGemm {
 };
 // Intermediate buffers BatchedLinalg keeps for product3 (batched_linalg.hpp:77-79), in bytes.
 struct BatchedWorkspaces { std::size_t idle_bytes = 0, busy_bytes = 0, busy_workspaces = 0; };
+// Metadata for an external allocation of whole aligned pages holding inline MPFR significands
+// (batched_linalg.hpp:53-60): offsets address little-endian 64-bit MPFR limbs of exactly the target width.  The
+// allocation stays alive and unchanged until the batch has been submitted.
+struct InlineComplexRecord {
+    std::uint64_t real_offset = 0, imag_offset = 0;
+    std::int32_t real_exponent = 0, imag_exponent = 0, real_sign = 0, imag_sign = 0;
+    std::uint32_t real_status = 0, imag_status = 0;
+};
+static_assert(sizeof(InlineComplexRecord) == sizeof(lf_inline_complex_record), "record layout is the C ABI's");
 class BatchedLinalg {
     Engine* engine_;
     // product3 intermediates: idle when no batch or unwaited submission holds them, and then reused
@@ -53,6 +62,14 @@ public:
     template <class T> void gemm_sequential(CommandBatch& b, const StridedGemm& s, const Buffer<T>& A, const Buffer<T>& B, Buffer<T>& C) { gemm(b, s, A, B, C); }
     // Two-stage product C_b = (A_b B_b) D_b (batched_linalg.hpp:99-110): the intermediate
     // [first.count][first.m][first.n] lives in a workspace of this BatchedLinalg; neither stage accumulates.
+    // Complex values gathered on the GPU from MPFR significands inside `allocation` (batched_linalg.hpp:146-148).
+    template <class T> void import_inline_complex(CommandBatch& b, const void* allocation, std::size_t bytes,
+                                                  const InlineComplexRecord* records, std::size_t count, Buffer<T>& out) {
+        static_assert(detail::Format<T>::complex, "inline complex staging needs complex output");
+        if (out.size() < count) throw std::invalid_argument("inline staging: undersized buffer");
+        detail::check(lf_batch_import_inline_complex(b.handle(), detail::Format<T>::bits, allocation, bytes,
+                                                     reinterpret_cast<const lf_inline_complex_record*>(records), count, out.handle()));
+    }
     template <class T> void product3(CommandBatch& b, StridedGemm first, StridedGemm second, const Buffer<T>& A, const Buffer<T>& B,
                                      const Buffer<T>& D, Buffer<T>& C, bool negative = false) {
         if (first.count != second.count || first.m != second.m || first.n != second.k || first.accumulate || second.accumulate)

@@ -977,13 +977,172 @@ template <int N> LFD_FN bool round_info(const u32* x, int len, i64 scale, Rounde
 //   bool term(u64 k, i64& scale, i64& top, int& sign) const;    false for a zero slot; the term is
 //                                                               sign * T * 2^scale with 0 < T < 2^(top - scale)
 //   void add(u64 k, u32* acc, int len, i64 off) const;          acc (len words) += T << off
+// ---- over-wide clusters: streaming with a sliding window
+// The terms with top <= cutoff taken one at a time in the order (top descending, index ascending) are added into
+// a window of CW words (positive and negative magnitudes) that covers bits [A - 32 CW, A).  A term that reaches
+// below the window moves the window down when the partial sum is small enough to stay inside (nothing is lost);
+// otherwise the partial sum lies at least 32 CW - 64N - 2 bits above the term and everything after it is tiny
+// against it.
+struct StreamPos { i64 top; u64 k; bool started; };
+// The next term after `at` in the order (top descending, index ascending) among those with top <= cutoff.
+template <class Src> LFD_FN bool stream_next(const Src& src, i64 cutoff, StreamPos& at, i64& scale, i64& top, int& sign) {
+    const u64 n = src.count();
+    bool found = false; i64 bt = 0; u64 bk = 0;
+    for (u64 k = 0; k < n; ++k) {
+        i64 s, tp; int sg;
+        if (!src.term(k, s, tp, sg) || tp > cutoff) continue;
+        if (at.started && (tp > at.top || (tp == at.top && k <= at.k))) continue;
+        if (!found || tp > bt || (tp == bt && k < bk)) { found = true; bt = tp; bk = k; }
+    }
+    if (!found) return false;
+    at.top = bt; at.k = bk; at.started = true;
+    src.term(bk, scale, top, sign);
+    return true;
+}
+// pos <- |pos - neg|, neg <- 0; returns the sign of pos - neg before (0 when equal).
+template <int CW> LFD_FN int stream_normalize(u32* pos, u32* neg) {
+    int cmp = 0;
+    for (int w = CW - 1; w >= 0 && !cmp; --w) if (pos[w] != neg[w]) cmp = pos[w] > neg[w] ? 1 : -1;
+    if (cmp < 0) for (int w = 0; w < CW; ++w) { const u32 t = pos[w]; pos[w] = neg[w]; neg[w] = t; }
+    u32 bo = 0;
+    for (int w = 0; w < CW; ++w) { const u64 d = (u64)neg[w] + bo; const u32 o = pos[w]; pos[w] = (u32)((u64)o - d); bo = (u64)o < d; neg[w] = 0; }
+    return cmp;
+}
+// Index of the highest set bit of x (CW words), -1 when zero.
+template <int CW> LFD_FN int stream_msb(const u32* x) {
+    for (int w = CW - 1; w >= 0; --w) if (x[w]) return 32 * w + 31 - lf_clz(x[w]);
+    return -1;
+}
+// x <- x * 2^d (d >= 0), words shifted out at the top dropped (the caller guarantees they are zero).
+template <int CW> LFD_FN void stream_shift_up(u32* x, i64 d) {
+    const int q = (int)(d >> 5), r = (int)(d & 31);
+    for (int w = CW - 1; w >= 0; --w) {
+        const int a = w - q;
+        u32 v = a >= 0 ? x[a] << r : 0u;
+        if (r && a - 1 >= 0) v |= x[a - 1] >> (32 - r);
+        x[w] = v;
+    }
+}
+// Window state of one stream: magnitudes (pos, neg), sign of the partial sum after normalisation, anchor A.
+template <int CW> struct StreamWin { u32 pos[CW], neg[CW]; i64 A; };
+// Adds the terms after `at` (in order) until they run out (returns true) or one no longer fits while the partial sum
+// is too large to move the window (returns false with that term pending in `at`, its data in scale/top/sign).
+// mult flips every term's sign (-1).  logc: ceil(log2(terms + 2)).
+template <int CW, class Src> LFD_FN bool stream_run(const Src& src, i64 cutoff, int mult, int logc, StreamWin<CW>& W, StreamPos& at,
+                                                    i64& scale, i64& top, int& sign) {
+    for (;;) {
+        StreamPos nx = at;
+        if (!stream_next(src, cutoff, nx, scale, top, sign)) return true;
+        i64 bottom = W.A - 32 * (i64)CW;
+        if (scale < bottom) {
+            const int sg = stream_normalize<CW>(W.pos, W.neg);
+            const int h = stream_msb<CW>(W.pos);
+            if (sg == 0 || h < 0) {
+                W.A = top + logc + 2;                                     // empty window: re-anchor at the term
+            } else {
+                const i64 m = bottom + h;                                 // highest set bit of |partial|
+                const i64 A2 = (m + 2 > top + logc + 2) ? m + 2 : top + logc + 2;
+                if (A2 - 32 * (i64)CW > scale) {                          // the partial sum dominates the rest
+                    if (sg < 0) for (int w = 0; w < CW; ++w) { W.neg[w] = W.pos[w]; W.pos[w] = 0; }
+                    at = nx;
+                    return false;
+                }
+                stream_shift_up<CW>(W.pos, W.A - A2);
+                if (sg < 0) for (int w = 0; w < CW; ++w) { W.neg[w] = W.pos[w]; W.pos[w] = 0; }
+                W.A = A2;
+            }
+            bottom = W.A - 32 * (i64)CW;
+        }
+        src.add(nx.k, sign * mult > 0 ? W.pos : W.neg, CW, scale - bottom);
+        at = nx;
+    }
+}
+// Sign of X * 2^xscale * xsign + mult * (the terms after `at`, and the term at `at` itself when pending), exactly.
+// X: xw words (nullptr when absent).
+template <int CW, class Src> LFD_FN int stream_sign(const Src& src, i64 cutoff, StreamPos at, bool pending, int mult, int logc,
+                                                    const u32* X, int xw, i64 xscale, int xsign) {
+    StreamWin<CW> W;
+    for (int w = 0; w < CW; ++w) { W.pos[w] = 0; W.neg[w] = 0; }
+    i64 xt = INT64_MIN;                                                   // X's highest bit + 1
+    for (int w = xw - 1; w >= 0; --w) if (X[w]) { xt = xscale + 32 * w + 32 - lf_clz(X[w]); break; }
+    i64 s0 = 0, t0 = INT64_MIN; int g0 = 0;
+    if (pending) src.term(at.k, s0, t0, g0);
+    const i64 top = xt > t0 ? xt : t0;
+    W.A = (top == INT64_MIN ? cutoff : top) + logc + 2;
+    const i64 bottom = W.A - 32 * (i64)CW;
+    if (pending) src.add(at.k, g0 * mult > 0 ? W.pos : W.neg, CW, s0 - bottom);
+    if (xt != INT64_MIN) acc_add(xsign > 0 ? W.pos : W.neg, CW, X, xw, xscale - bottom);
+    i64 sc, tp; int sg;
+    stream_run<CW>(src, cutoff, mult, logc, W, at, sc, tp, sg);           // stops early only when the partial sum dominates
+    return stream_normalize<CW>(W.pos, W.neg);
+}
+// RN of the exact sum of the terms with top <= cutoff, by streaming.  When the window cannot follow, the partial sum
+// S is split at bit k = (pending top) + logc + 3 into S_hi (a multiple of 2^k) and S_lo < 2^k; with the tail t (all
+// later terms, |t| < 2^(k - 2)) the rounding of S + t is that of S_hi + carry 2^k plus the sign of the remainder in
+// [0, 2^k), and carry and remainder follow from the exact signs of S_lo + t and S_lo + t - 2^k.
+template <int N, int CW, class Src> LFD_FN Num<N> stream_value(const Src& src, i64 cutoff, int logc) {
+    StreamWin<CW> W;
+    for (int w = 0; w < CW; ++w) { W.pos[w] = 0; W.neg[w] = 0; }
+    StreamPos at{0, 0, false};
+    W.A = cutoff + logc + 2;
+    i64 sc, tp; int sg;
+    const bool done = stream_run<CW>(src, cutoff, 1, logc, W, at, sc, tp, sg);
+    const int ssign = stream_normalize<CW>(W.pos, W.neg);
+    const i64 bottom = W.A - 32 * (i64)CW;
+    if (done) {
+        if (!ssign) return zero<N>();
+        Rounded<N> R;
+        round_info<N>(W.pos, CW, bottom, R);
+        return finish<N>(R.m, R.e, ssign, R.rb && (R.sb || (R.m[0] & 1u)), 0);
+    }
+    const i64 k = tp + logc + 3;                                          // S_lo = |S| mod 2^k
+    u32 lo[CW];
+    for (int w = 0; w < CW; ++w) lo[w] = 0;
+    const i64 kb = k - bottom;                                            // bit index of k in the window (> 0)
+    for (int w = 0; w < CW; ++w) {
+        const i64 b0 = 32 * (i64)w;
+        if (b0 + 32 <= kb) { lo[w] = W.pos[w]; W.pos[w] = 0; }
+        else if (b0 < kb) { const u32 mask = (1u << (kb - b0)) - 1u; lo[w] = W.pos[w] & mask; W.pos[w] &= ~mask; }
+    }
+    // sign of S_lo + ssign * t, and of S_lo - 2^k + ssign * t
+    const int c0 = stream_sign<CW>(src, cutoff, at, true, ssign, logc, lo, CW, bottom, 1);
+    int carry = 0, sigma = 0;
+    if (kb <= 0) {
+        // the pending term lies wholly below the window: S is a multiple of 2^bottom > |t|, so only t's sign matters
+        sigma = c0;
+    } else {
+        u32 hk[CW];                                                       // 2^k - S_lo
+        for (int w = 0; w < CW; ++w) hk[w] = 0;
+        if (kb < 32 * (i64)CW) hk[kb >> 5] = 1u << (kb & 31);
+        u32 bo = 0;
+        for (int w = 0; w < CW; ++w) { const u64 d = (u64)lo[w] + bo; const u32 o = hk[w]; hk[w] = (u32)((u64)o - d); bo = (u64)o < d; }
+        const int c1 = stream_sign<CW>(src, cutoff, at, true, ssign, logc, hk, CW, bottom, -1);
+        if (c0 < 0) { carry = -1; sigma = 1; }
+        else if (c0 == 0) { carry = 0; sigma = 0; }
+        else if (c1 < 0) { carry = 0; sigma = 1; }
+        else if (c1 == 0) { carry = 1; sigma = 0; }
+        else { carry = 1; sigma = 1; }
+    }
+    if (carry) {                                                          // S_hi +- 2^k (S_hi >> 2^k: no sign change)
+        u32 one[1] = {1u};
+        if (carry > 0) acc_add(W.pos, CW, one, 1, kb);
+        else { for (int w = 0; w < CW; ++w) W.neg[w] = 0; acc_add(W.neg, CW, one, 1, kb); stream_normalize<CW>(W.pos, W.neg); }
+    }
+    Rounded<N> R;
+    round_info<N>(W.pos, CW, bottom, R);
+    const bool up = R.rb && (R.sb || sigma > 0 || (sigma == 0 && (R.m[0] & 1u)));
+    return finish<N>(R.m, R.e, ssign, up, 0);
+}
+
 // The terms are summed cluster by cluster from the highest: a cluster holds the highest remaining top and
 // grows downwards while some remaining term reaches within gap = 32N + ceil(log2(count + 1)) + 4 bits of its
 // lowest bit; it is summed exactly as positive and negative magnitudes in CW words.  The first nonzero
 // cluster sum S is kept; everything below it is less than 2^(lowest bit of S - 32N - 2) in magnitude, so of
 // the rest only the sign of the next nonzero cluster can matter (to exact ties and exact S).  A cluster wider
-// than CW words sets *error (when given) and gives zero with status invalid.
-template <int N, int CW, class Src> LFD_FN Num<N> cluster_round(const Src& src, u32* error) {
+// than CW words is streamed (stream_value / stream_sign above), so no input fails.
+// STREAM = false leaves the streaming path out (callers whose clusters provably fit: dot2_add's three terms); an
+// over-wide cluster then sets *error and gives zero with status invalid.
+template <int N, int CW, class Src, bool STREAM = true> LFD_FN Num<N> cluster_round(const Src& src, u32* error) {
     const u64 n = src.count();
     int count = 0;
     i64 T = INT64_MIN;
@@ -1023,7 +1182,18 @@ template <int N, int CW, class Src> LFD_FN Num<N> cluster_round(const Src& src, 
             low = nl;
         }
         const int len = (int)((Tc - low + logc + 2 + 31) / 32) + 1;
-        if (len > CW) { if (error) lf_flag(error, 1u); return zero<N>(kInvalid); }
+        if (len > CW) {
+            if constexpr (STREAM) {
+                // an over-wide cluster: stream everything from here (tops <= cutoff)
+                if (!have) return stream_value<N, CW>(src, cutoff, logc);
+                const int rest = stream_sign<CW>(src, cutoff, StreamPos{0, 0, false}, false, 1, logc, nullptr, 0, 0, 1);
+                sigma = rest == 0 ? 0 : (rest == rsign ? 1 : -1);
+                break;
+            } else {
+                if (error) lf_flag(error, 1u);
+                return zero<N>(kInvalid);
+            }
+        }
         for (int w = 0; w < len; ++w) { pos[w] = 0; neg[w] = 0; }
         for (u64 k = 0; k < n; ++k) {
             i64 s, tp; int sg;
@@ -1130,7 +1300,7 @@ LFD_UNROLL
         }
     }
     Dot2Terms<N> src{{p1, p2, e.m}, {2 * N, 2 * N, N}, {sc1, sc2, sce}, {s1, s2, e.s}};
-    return cluster_round<N, 8 * N + 4>(src, nullptr);
+    return cluster_round<N, 8 * N + 4, Dot2Terms<N>, false>(src, nullptr);
 }
 
 // ---------------------------------------------------------------- out-of-line forms

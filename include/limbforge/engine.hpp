@@ -7,6 +7,7 @@
 #include "../limbforge_b200.h"
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <future>
 #include <memory>
 #include <stdexcept>
@@ -106,7 +107,8 @@ struct Access {
 class Submission {
     struct Del { void operator()(lf_submission* s) const { lf_submission_destroy(s); } };
     std::unique_ptr<lf_submission, Del> s_;
-    explicit Submission(lf_submission* s) : s_(s) {}
+    std::vector<std::function<void()>> done_;     // run once waited for (tickets of operations in the batch)
+    Submission(lf_submission* s, std::vector<std::function<void()>> done) : s_(s), done_(std::move(done)) {}
     friend class CommandBatch;
 public:
     Submission() = default;
@@ -116,13 +118,17 @@ public:
     }
     Timing wait() {
         if (!s_) throw std::logic_error("empty submission");
-        lf_timing t{}; detail::check(lf_submission_wait(s_.get(), &t)); return detail::timing(t);
+        lf_timing t{}; detail::check(lf_submission_wait(s_.get(), &t));
+        for (auto& f : done_) f();
+        done_.clear();
+        return detail::timing(t);
     }
 };
 
 class CommandBatch {
     struct Del { void operator()(lf_batch* b) const { lf_batch_destroy(b); } };
     std::unique_ptr<lf_batch, Del> b_;
+    std::vector<std::function<void()>> done_;
     explicit CommandBatch(lf_batch* b) : b_(b) {}
     friend class Engine;
     lf_batch* open() const { if (!b_) throw std::logic_error("batch already submitted or moved"); return b_.get(); }
@@ -134,6 +140,8 @@ class CommandBatch {
     }
 public:
     lf_batch* handle() const { return b_.get(); }
+    // f runs when the submission of this batch has been waited for.
+    void on_wait(std::function<void()> f) { open(); done_.push_back(std::move(f)); }
     template <class T> void run(Operation op, const Buffer<T>& a, const Buffer<T>& b, Buffer<T>& out) {
         if (operation_is_unary(op) || operation_is_ternary(op)) throw std::invalid_argument("operation requires a different number of inputs");
         if (a.size() != b.size() || a.size() != out.size()) throw std::invalid_argument("buffer counts must match");
@@ -195,7 +203,7 @@ public:
         lf_submission* s = nullptr;
         detail::check(lf_batch_submit(open(), &s));
         b_.reset();
-        return Submission(s);
+        return Submission(s, std::move(done_));
     }
 };
 

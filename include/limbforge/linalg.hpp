@@ -147,6 +147,34 @@ public:
     }
 };
 
+// Owning complex QR factor (linalg.hpp:331-350): H_j = I - tau_j v_j v_j^H with complex tau_j (zgeqrf), R upper with a
+// real diagonal; row-major Complex<bits/32> arrays.  Same options, rank and status rules as QRFactor; column pivoting of
+// complex factors is not built (factor_qr_complex throws std::runtime_error).
+class ComplexQRFactor {
+    QRFactor f_;
+    explicit ComplexQRFactor(QRFactor f) : f_(std::move(f)) {}
+    friend class Linalg;
+public:
+    ComplexQRFactor() = default;
+    bool empty() const { return f_.empty(); }
+    int bits() const { return f_.bits(); }
+    std::size_t rows() const { return f_.rows(); }
+    std::size_t cols() const { return f_.cols(); }
+    std::size_t block() const { return f_.block(); }
+    const QRInfo& info() const { return f_.info(); }
+    bool full_rank() const { return f_.full_rank(); }
+    const void* r() const { return f_.r(); }
+    const void* v() const { return f_.v(); }
+    const void* tau() const { return f_.tau(); }
+    const void* t() const { return f_.t(); }
+    bool pivoted() const { return f_.pivoted(); }
+    const std::size_t* permutation() const { return f_.permutation(); }
+    // X (n x nrhs, complex) = least-squares solution for B (m x nrhs, complex); X must not overlap B.
+    Timing solve(const void* B, std::size_t nrhs, void* X) const { return f_.solve(B, nrhs, X); }
+    // B (m x nrhs, complex) <- Q^H B (adjoint) or Q B, in place.
+    Timing apply_q(void* B, std::size_t nrhs, bool adjoint) const { return f_.apply_q(B, nrhs, adjoint); }
+};
+
 // One Linalg per host thread.
 class Linalg {
     struct Del { void operator()(lf_linalg* l) const { lf_linalg_destroy(l); } };
@@ -233,6 +261,12 @@ public:
         lf_qr_options o = qo(options); lf_qr* q = nullptr;
         detail::check(lf_linalg_factor_qr(l_.get(), bits, A, m, n, &o, &q));
         return QRFactor(q);
+    }
+    // Complex Householder QR of A (m x n Complex<bits/32>, row-major, m >= n) (linalg.hpp:170).
+    ComplexQRFactor factor_qr_complex(int bits, const void* A, std::size_t m, std::size_t n, const QROptions& options = {}) {
+        lf_qr_options o = qo(options); lf_qr* q = nullptr;
+        detail::check(lf_linalg_factor_qr_complex(l_.get(), bits, A, m, n, &o, &q));
+        return ComplexQRFactor(QRFactor(q));
     }
     // QR of the augmented Levenberg-Marquardt matrix [J; diag(d)] ((m + n) x n) (linalg.hpp:168).
     QRFactor factor_qr_augmented(int bits, const void* J, std::size_t m, std::size_t n, const void* d, const QROptions& options = {}) {

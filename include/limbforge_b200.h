@@ -159,9 +159,15 @@ const size_t* lf_qr_permutation(const lf_qr* qr);
 int lf_qr_solve(const lf_qr* qr, const void* B, size_t nrhs, void* X, lf_timing* timing);
 /* QRFactor::apply_q (linalg.hpp:129): B (m x nrhs) <- Q^T B (transpose) or Q B, in place */
 int lf_qr_apply_q(const lf_qr* qr, void* B, size_t nrhs, int transpose, lf_timing* timing);
-/* Buffer forms of solve / apply_q (linalg.hpp:131-134): synchronous, buffers idle */
+/* Buffer forms of solve / apply_q (linalg.hpp:131-134): synchronous, buffers idle (real factors) */
 int lf_qr_solve_buffers(const lf_qr* qr, lf_buffer* B, size_t nrhs, lf_buffer* X, lf_timing* timing);
 int lf_qr_apply_q_buffer(const lf_qr* qr, lf_buffer* B, size_t nrhs, int transpose, lf_timing* timing);
+/* Linalg::factor_qr_complex (linalg.hpp:170, ComplexQRFactor linalg.hpp:331-350): complex A (m x n Complex<bits/32>,
+ * m >= n); the factor's r/v/tau/t are complex arrays (R with a real diagonal), lf_qr_solve and lf_qr_apply_q take
+ * complex matrices (transpose selects Q^H).  Column pivoting of complex factors is not built (runtime error). */
+int lf_linalg_factor_qr_complex(lf_linalg* linalg, int bits, const void* A, size_t m, size_t n, const lf_qr_options* options,
+                                lf_qr** out);
+int lf_qr_is_complex(const lf_qr* qr);
 /* Exact product on device line views (CUDA callers; no reference counterpart): element (line, k)
  * at base + (line * ls + k * ks) elements; C element (i, j) at C + i * ldc + j elements. */
 int lf_dev_exact_product(lf_linalg* linalg, int bits, const void* left, size_t left_ls, size_t left_ks, const void* right,
@@ -275,6 +281,37 @@ int lf_batch_segmented_dot(lf_batch* batch, int bits, int complex_, const lf_seg
  * seed after zero steps). */
 int lf_engine_recurrence(lf_engine* engine, int bits, const void* seeds, const void* weights, void* out, size_t count,
                          unsigned steps, unsigned states_per_weight, lf_timing* timing);
+/* The exact batched 4 x 4 product, wolfnum::experimental::ExactGemm4 (benchmarks/experiments/exact_gemm4/prototype.hpp:
+ * 4-33): row-major 4 x 4 matrices, matrix t of A, B, C at t * stride elements (stride 0 broadcasts an input); each real
+ * component RN(C_old + sum_k a_ik b_kj) with one rounding of the exact sum (C_old left out without accumulate), then
+ * negated when `negative`; complex components sum eight signed real products.  Output matrices may not overlap
+ * (stride_c >= 16 when count > 1), inputs may; the output may not alias an input.  Every component is summed on the
+ * GPU: the report's host_components and provisional_reads are always 0. */
+typedef struct lf_exact_gemm4_shape {
+    size_t count, stride_a, stride_b, stride_c;
+    int accumulate, negative;
+} lf_exact_gemm4_shape;                                                                  /* ExactGemm4Shape */
+typedef struct lf_exact_gemm4_report {
+    size_t gpu_components, host_components;
+    int provisional_reads;
+} lf_exact_gemm4_report;                                                                 /* ExactGemm4Report */
+int lf_engine_exact_gemm4(lf_engine* engine, int bits, int complex_, const lf_exact_gemm4_shape* shape, const void* A,
+                          const void* B, void* C, lf_exact_gemm4_report* report,
+                          lf_timing* timing);                                            /* ExactGemm4::gemm (host arrays) */
+int lf_batch_exact_gemm4(lf_batch* batch, int bits, int complex_, const lf_exact_gemm4_shape* shape, lf_buffer* A,
+                         lf_buffer* B, lf_buffer* C);                                    /* ExactGemm4::gemm (CommandBatch&) */
+/* Import of complex values whose MPFR significands live inside one caller allocation (BatchedLinalg::
+ * import_inline_complex, batched_linalg.hpp:53-60,146-148): offsets address little-endian 64-bit MPFR limbs of a
+ * significand of exactly `bits` bits; the allocation owns whole aligned pages and stays unchanged until the batch has
+ * been submitted.  out[i] gets both parts of record i (a status or a zero sign gives zero with that status). */
+typedef struct lf_inline_complex_record {
+    uint64_t real_offset, imag_offset;
+    int32_t real_exponent, imag_exponent, real_sign, imag_sign;
+    uint32_t real_status, imag_status;
+} lf_inline_complex_record;                                                              /* InlineComplexRecord */
+int lf_batch_import_inline_complex(lf_batch* batch, int bits, const void* allocation, size_t bytes,
+                                   const lf_inline_complex_record* records, size_t count,
+                                   lf_buffer* out);                                      /* import_inline_complex */
 
 /* Device-pointer forms (no reference counterpart), asynchronous on `stream`; tree_sum's scratch holds
  * 2 * ceil(count / 2) elements (unused for count <= 2). */

@@ -102,6 +102,23 @@ class SegmentedDot:                                              # engine.hpp:30
 
 
 @dataclass
+class ExactGemm4Shape:                                           # experiments/exact_gemm4/prototype.hpp:6
+    count: int = 1
+    stride_a: int = 16
+    stride_b: int = 16
+    stride_c: int = 16
+    accumulate: bool = False
+    negative: bool = False
+
+
+@dataclass
+class ExactGemm4Report:                                          # experiments/exact_gemm4/prototype.hpp:7
+    gpu_components: int = 0
+    host_components: int = 0
+    provisional_reads: bool = False
+
+
+@dataclass
 class StridedGemm:                                               # batched_linalg.hpp:11-14
     count: int = 1
     m: int = 0
@@ -188,6 +205,15 @@ class _SegmentedDot(C.Structure):
     _fields_ = [("segments", C.c_size_t), ("length", C.c_size_t), ("shared_right", C.c_int)]
 
 
+class _ExactGemm4Shape(C.Structure):
+    _fields_ = [(f, C.c_size_t) for f in ("count", "stride_a", "stride_b", "stride_c")] + \
+               [("accumulate", C.c_int), ("negative", C.c_int)]
+
+
+class _ExactGemm4Report(C.Structure):
+    _fields_ = [("gpu_components", C.c_size_t), ("host_components", C.c_size_t), ("provisional_reads", C.c_int)]
+
+
 class _StridedGemm(C.Structure):
     _fields_ = [("count", C.c_size_t), ("m", C.c_size_t), ("n", C.c_size_t), ("k", C.c_size_t),
                 ("stride_a", C.c_size_t), ("stride_b", C.c_size_t), ("stride_c", C.c_size_t),
@@ -244,6 +270,21 @@ class _RaggedClassInfo(C.Structure):
 class _RaggedInfo(C.Structure):
     _fields_ = [("classes", C.c_size_t), ("cls", _RaggedClassInfo * 31), ("lu4_block", C.c_uint), ("lu4_grid", C.c_uint),
                 ("lu4_trial_ms", C.c_double), ("tuned", C.c_int)]
+
+
+# lf_inline_complex_record (BatchedLinalg::import_inline_complex) as a numpy record.
+INLINE_RECORD_DTYPE = np.dtype({"names": ["real_offset", "imag_offset", "real_exponent", "imag_exponent", "real_sign", "imag_sign",
+                                          "real_status", "imag_status"],
+                                "formats": [np.uint64, np.uint64, np.int32, np.int32, np.int32, np.int32, np.uint32, np.uint32],
+                                "offsets": [0, 8, 16, 20, 24, 28, 32, 36], "itemsize": 40})
+
+
+def page_aligned(nbytes: int) -> np.ndarray:
+    """A zeroed uint8 array of whole pages at a page boundary (an anonymous mapping), as inline staging requires."""
+    import mmap
+    page = mmap.PAGESIZE
+    size = max(page, (nbytes + page - 1) // page * page)
+    return np.frombuffer(mmap.mmap(-1, size), dtype=np.uint8)
 
 
 # lf_ragged_gemm as a numpy record (one row per instance); offsets a, b, c are bytes in the arena.
@@ -304,6 +345,9 @@ def _load() -> C.CDLL:
         "lf_test_residue_wait_limit": ([C.c_uint, P(C.c_uint32)], I),
         "lf_engine_segmented_dot": ([V, I, I, P(_SegmentedDot), V, V, V, P(_Timing)], I),
         "lf_batch_segmented_dot": ([V, I, I, P(_SegmentedDot), V, V, V], I),
+        "lf_engine_exact_gemm4": ([V, I, I, P(_ExactGemm4Shape), V, V, V, P(_ExactGemm4Report), P(_Timing)], I),
+        "lf_batch_exact_gemm4": ([V, I, I, P(_ExactGemm4Shape), V, V, V], I),
+        "lf_batch_import_inline_complex": ([V, I, V, S, V, S, V], I),
         "lf_engine_recurrence": ([V, I, V, V, V, S, C.c_uint, C.c_uint, P(_Timing)], I),
         "lf_linalg_factor_qr": ([V, I, V, S, S, P(_QROptions), P(V)], I),
         "lf_linalg_factor_qr_augmented": ([V, I, V, S, S, V, P(_QROptions), P(V)], I),
@@ -314,6 +358,7 @@ def _load() -> C.CDLL:
         "lf_qr_permutation": ([V], P(S)),
         "lf_qr_solve": ([V, V, S, V, P(_Timing)], I), "lf_qr_apply_q": ([V, V, S, I, P(_Timing)], I),
         "lf_qr_solve_buffers": ([V, V, S, V, P(_Timing)], I), "lf_qr_apply_q_buffer": ([V, V, S, I, P(_Timing)], I),
+        "lf_linalg_factor_qr_complex": ([V, I, V, S, S, P(_QROptions), P(V)], I), "lf_qr_is_complex": ([V], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -411,8 +456,9 @@ class Buffer:
 
 
 class Submission:
-    def __init__(self, handle):
+    def __init__(self, handle, completions=()):
         self.handle = handle
+        self._completions = list(completions)
 
     def __del__(self):
         if getattr(self, "handle", None) and lib is not None:
@@ -427,6 +473,9 @@ class Submission:
     def wait(self) -> Timing:
         t = _Timing()
         check(lib.lf_submission_wait(self.handle, C.byref(t)))
+        for f in self._completions:
+            f()
+        self._completions = []
         return _timing(t)
 
 
@@ -438,6 +487,7 @@ class CommandBatch:
         h = C.c_void_p()
         check(lib.lf_batch_create(engine.handle, C.byref(h)))
         self.handle = h
+        self._completions = []      # run once the submission has been waited for (tickets)
 
     def __del__(self):
         if getattr(self, "handle", None) and lib is not None:
@@ -492,7 +542,8 @@ class CommandBatch:
     def submit(self) -> Submission:
         h = C.c_void_p()
         check(lib.lf_batch_submit(self.handle, C.byref(h)))
-        return Submission(h)
+        done, self._completions = self._completions, []
+        return Submission(h, done)
 
 
 class Engine:
@@ -584,6 +635,56 @@ class Engine:
         return X, det, st, _timing(t)
 
 
+class ExactGemm4Ticket:
+    """experimental::ExactGemm4Ticket (prototype.hpp:9-16): resolved once the batch's submission has been waited for."""
+
+    def __init__(self, report: ExactGemm4Report):
+        self._report = report
+        self._done = False
+
+    def resolved(self) -> bool:
+        return self._done
+
+    def report(self) -> ExactGemm4Report:
+        if not self._done:
+            raise LogicError("exact GEMM4: wait for submission before reading report")
+        return self._report
+
+
+class ExactGemm4:
+    """experimental::ExactGemm4 (prototype.hpp:21-33): batches of row-major 4 x 4 products, each real component
+    RN(C_old + sum of exact signed products), then optionally negated; complex components sum eight real products with
+    one rounding.  Every component is summed exactly on the GPU, so no host repair is ever pending and outputs read later
+    in the same batch are final."""
+
+    def __init__(self, engine: "Engine"):
+        self.engine = engine
+
+    @staticmethod
+    def _shape(s: ExactGemm4Shape) -> _ExactGemm4Shape:
+        return _ExactGemm4Shape(s.count, s.stride_a, s.stride_b, s.stride_c, int(s.accumulate), int(s.negative))
+
+    def gemm(self, bits, complex_, shape: ExactGemm4Shape, a, b, c):
+        """Host arrays (prototype.hpp:32): c is updated in place; returns (Timing, ExactGemm4Report)."""
+        check_bits(bits)
+        if not (isinstance(c, np.ndarray) and c.flags.c_contiguous and c.dtype == np.uint32):
+            raise InvalidArgument("exact_gemm4 output must be a C-contiguous uint32 array")
+        r, t = _ExactGemm4Report(), _Timing()
+        check(lib.lf_engine_exact_gemm4(self.engine.handle, bits, int(complex_), C.byref(self._shape(shape)),
+                                        _ptr(np.ascontiguousarray(a)), _ptr(np.ascontiguousarray(b)), _ptr(c), C.byref(r), C.byref(t)))
+        return _timing(t), ExactGemm4Report(r.gpu_components, r.host_components, bool(r.provisional_reads))
+
+    def encode(self, batch: CommandBatch, shape: ExactGemm4Shape, a: Buffer, b: Buffer, c: Buffer) -> ExactGemm4Ticket:
+        """Resident buffers recorded into batch (prototype.hpp:28-30)."""
+        if not a.bits or a.bits != b.bits or a.bits != c.bits or a.complex != b.complex or a.complex != c.complex:
+            raise InvalidArgument("exact_gemm4 buffers must share one arithmetic format")
+        check(lib.lf_batch_exact_gemm4(batch.handle, a.bits, int(a.complex), C.byref(self._shape(shape)), a.handle, b.handle,
+                                       c.handle))
+        ticket = ExactGemm4Ticket(ExactGemm4Report(shape.count * 16 * (2 if a.complex else 1), 0, False))
+        batch._completions.append(lambda: setattr(ticket, "_done", True))
+        return ticket
+
+
 class BatchedLinalg:
     """Sequential batched products (batched_linalg.hpp:63-118)."""
 
@@ -606,6 +707,20 @@ class BatchedLinalg:
     def gemm_resident(self, batch: CommandBatch, s: StridedGemm, A: Buffer, B: Buffer, C_: Buffer) -> None:
         sh = self._shape(s)
         check(lib.lf_batch_strided_gemm(batch.handle, A.bits, int(A.complex), C.byref(sh), A.handle, B.handle, C_.handle))
+
+    def import_inline_complex(self, batch: CommandBatch, allocation: np.ndarray, records: np.ndarray, out: Buffer) -> None:
+        """BatchedLinalg::import_inline_complex (batched_linalg.hpp:146-148): out[i] gathered on the GPU from the MPFR
+        significands inside `allocation` (whole aligned pages, see page_aligned) that records[i] (INLINE_RECORD_DTYPE)
+        describes.  The allocation must stay unchanged until the batch has been submitted."""
+        if not out.complex or not out.bits:
+            raise InvalidArgument("inline complex staging needs complex output")
+        if records.dtype != INLINE_RECORD_DTYPE or not records.flags.c_contiguous:
+            raise InvalidArgument("records must be a contiguous INLINE_RECORD_DTYPE array")
+        if out.count < len(records):
+            raise InvalidArgument("inline staging: undersized buffer")
+        check(lib.lf_batch_import_inline_complex(batch.handle, out.bits, allocation.ctypes.data, allocation.nbytes,
+                                                 records.ctypes.data if len(records) else None, len(records), out.handle))
+        batch._completions.append(lambda keep=(allocation, records): None)   # both stay referenced until the wait
 
     def product3(self, batch: CommandBatch, first: StridedGemm, second: StridedGemm, A: Buffer, B: Buffer, D: Buffer, C_: Buffer,
                  negative=False) -> None:
@@ -844,6 +959,14 @@ class Linalg:
         check(lib.lf_linalg_factor_qr_augmented(self.handle, bits, _ptr(J), m, n, _ptr(d), C.byref(qo), C.byref(h)))
         return QRFactor(h, self)
 
+    def factor_qr_complex(self, bits, A, m, n, options: "QROptions | None" = None) -> "QRFactor":
+        """Complex Householder QR of A (m x n complex, shape [m * n, 2, N + 3]) (linalg.hpp:170): H = I - tau v v^H with
+        complex tau, R upper with a real diagonal.  Column pivoting of complex factors is not built."""
+        h = C.c_void_p()
+        qo = self._qo(options)
+        check(lib.lf_linalg_factor_qr_complex(self.handle, bits, _ptr(A), m, n, C.byref(qo), C.byref(h)))
+        return QRFactor(h, self)
+
     def factor_qr_buffer(self, A: "Buffer", m, n, options: "QROptions | None" = None) -> "QRFactor":
         """factor_qr on an idle Buffer of this Linalg's engine (linalg.hpp:200)."""
         h = C.c_void_p()
@@ -889,6 +1012,7 @@ class QRFactor:
         i = _QRInfo()
         check(lib.lf_qr_describe(handle, C.byref(bits), C.byref(rows), C.byref(cols), C.byref(block), C.byref(piv), C.byref(i)))
         self.bits, self.rows, self.cols, self.block, self.pivoted = bits.value, rows.value, cols.value, block.value, bool(piv.value)
+        self.complex = bool(lib.lf_qr_is_complex(handle))
         self.info = QRInfo(i.rank, i.reason, i.status, _timing(i.timing), i.blocks, i.gpu_updates, i.host_updates,
                            i.panel_seconds, i.update_seconds, i.norm_recomputations)
 
@@ -902,10 +1026,12 @@ class QRFactor:
 
     def _array(self, fn, count) -> np.ndarray:
         w = self.bits // 32 + 3
+        shape = (count, 2, w) if self.complex else (count, w)
         p = fn(self.handle)
         if not p or not count:
-            return np.zeros((0, w), dtype=np.uint32)
-        return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint32)), shape=(count * w,)).reshape(count, w).copy()
+            return np.zeros((0,) + shape[1:], dtype=np.uint32)
+        total = count * w * (2 if self.complex else 1)
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint32)), shape=(total,)).reshape(shape).copy()
 
     def r(self) -> np.ndarray:
         return self._array(lib.lf_qr_r, self.cols * self.cols)
@@ -928,7 +1054,8 @@ class QRFactor:
     def solve(self, B, nrhs, X=None) -> np.ndarray:
         """Least-squares X (n x nrhs) for B (m x nrhs) (linalg.hpp:127)."""
         if X is None:
-            X = np.zeros((max(self.cols * nrhs, 0), self.bits // 32 + 3), dtype=np.uint32)
+            w = self.bits // 32 + 3
+            X = np.zeros((self.cols * nrhs, 2, w) if self.complex else (self.cols * nrhs, w), dtype=np.uint32)
         t = _Timing()
         check(lib.lf_qr_solve(self.handle, _ptr(B), nrhs, _ptr(X), C.byref(t)))
         self.last_timing = _timing(t)

@@ -1,0 +1,288 @@
+// Complex Householder QR panel kernels (the reference's src/linalg_complex.mm:125-306: zgeqrf convention,
+// H = I - tau v v^H with complex tau and real beta).  Every complex dot product or update is two real exact dot
+// products over the interleaved (re, im) operand sequences, one rounding per component; a complex array of
+// elements (re, im) is read as such a real sequence with unit stride.  The panel mirrors the real one (lf_qr.cuh):
+// column-contiguous Pt (the panel's columns), Vt (reflectors) and Vi (i v), plus Vr (the reflectors by rows,
+// entry (r, c) at r * nb + c), three launches per column and a device-side state; the trailing updates are the
+// real compact-WY products on the 2 x 2-block real embeddings of V and T ([[re, -im], [im, re]]) applied to the
+// work matrix split by rows (row 2r = Re of row r, 2r + 1 = Im).
+#pragma once
+#include "lf_qr.cuh"
+
+namespace lfd {
+
+struct CqrPanel {
+    u32* Wk; u64 m, n;               // the row-split work matrix (2m x n real), reduced in place
+    u32* V; u32* T; u32* tau;        // the complex factor: V (m x n), T (blocks of nb x nb), tau (n)
+    u32* EV; u32* ET;                // real embeddings: EV (2m x 2n), ET (blocks of 2nb x 2nb)
+    u32* Pt; u32* Vt; u32* Vi; u32* Vr;
+    u32* Wp; u32* G; u32* Gc; u32* Gic; u32* yc; u32* yic;
+    u32* scr;                        // per y entry: the T column, i times it and the W column (3 nb complex)
+    u64 k0, kb, nb, mr;
+    int rank_bits;
+    QrState* st;
+    u32* error;
+};
+
+template <int N> __device__ __forceinline__ void cq_store(u32* p, const Num<N>& re, const Num<N>& im) { store<N>(p, re); store<N>(p + N + 3, im); }
+// i z, conj(z), i conj(z) of the complex element at p, written to q
+template <int N> __device__ __forceinline__ void cq_times_i(u32* q, const u32* p) {
+    const Num<N> re = load_plain<N>(p), im = load_plain<N>(p + N + 3);
+    cq_store<N>(q, negate<N>(im), re);
+}
+template <int N> __device__ __forceinline__ void cq_conj(u32* q, const u32* p) {
+    const Num<N> re = load_plain<N>(p), im = load_plain<N>(p + N + 3);
+    cq_store<N>(q, re, negate<N>(im));
+}
+template <int N> __device__ __forceinline__ void cq_i_conj(u32* q, const u32* p) {
+    const Num<N> re = load_plain<N>(p), im = load_plain<N>(p + N + 3);
+    cq_store<N>(q, im, re);
+}
+// The 2 x 2 real block [[re, -im], [im, re]] of the complex element at z, written at (2r, 2c) of M (row stride ld).
+template <int N> __device__ __forceinline__ void cq_embed(u32* M, u64 ld, u64 r, u64 c, const u32* z) {
+    constexpr u64 E = N + 3;
+    const Num<N> re = load_plain<N>(z), im = load_plain<N>(z + E);
+    store<N>(M + (2 * r * ld + 2 * c) * E, re); store<N>(M + (2 * r * ld + 2 * c + 1) * E, negate<N>(im));
+    store<N>(M + ((2 * r + 1) * ld + 2 * c) * E, im); store<N>(M + ((2 * r + 1) * ld + 2 * c + 1) * E, re);
+}
+
+// Pt <- the panel's columns of the row-split Wk; Vt, Vi, Vr <- 0.
+template <int N> __global__ void cqr_load_kernel(CqrPanel p) {
+    constexpr u64 E = N + 3, C2 = 2 * E;
+    const u64 q = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= p.mr * p.nb) return;
+    for (u64 w = 0; w < C2; ++w) p.Vr[q * C2 + w] = 0;
+    if (q >= p.kb * p.mr) return;
+    const u64 c = q / p.mr, r = q % p.mr;
+    const u32* re = p.Wk + (2 * (p.k0 + r) * p.n + p.k0 + c) * E;
+    const u32* im = re + p.n * E;
+    for (u64 w = 0; w < E; ++w) { p.Pt[q * C2 + w] = re[w]; p.Pt[q * C2 + E + w] = im[w]; }
+    for (u64 w = 0; w < C2; ++w) { p.Vt[q * C2 + w] = 0; p.Vi[q * C2 + w] = 0; }
+}
+// Column c by the panel's reflectors so far: x_r = (D(Re x_r; Vr[r][0..q), conj y), D(Im x_r; Vr[r][0..q), i conj y))
+// over 2q real terms each (linalg_complex.mm:188-193).  One warp per row.
+template <int N> __global__ void __launch_bounds__(256) cqr_update_kernel(CqrPanel p, u64 c) {
+    constexpr u64 E = N + 3, C2 = 2 * E;
+    const long long rank = p.st->rank, j = (long long)(p.k0 + c);
+    const long long q = (rank < j ? rank : j) - (long long)p.k0;
+    if (q <= 0) return;
+    const u64 r = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= p.mr) return;
+    u32* x = p.Pt + (c * p.mr + r) * C2;
+    const u32* vr = p.Vr + r * p.nb * C2;
+    const Num<N> re = warp_exact_dot<N, true>(x, true, vr, 1, p.yc, 1, 2 * (u64)q, p.error);
+    const Num<N> im = warp_exact_dot<N, true>(x + E, true, vr, 1, p.yic, 1, 2 * (u64)q, p.error);
+    if ((threadIdx.x & 31) == 0) cq_store<N>(x, re, im);
+}
+// Reflector of column c (linalg_complex.mm:205-226): s = P(x^H x); a zero or status column, or one failing the rank
+// test, ends the factorization; otherwise, when anything lies below the diagonal or Im alpha != 0, beta =
+// -sgn(Re alpha) sqrt(s), v0 = (RN(Re alpha - beta), Im alpha), v = 2^-e (v0, x_1, ...) with e = exponent(Re v0) and
+// tau = (RN(2 / P(v^H v)), 0) when Im v0 = 0, else with a = P(v^H v) / 2, b = RN(2^-e beta Im v0), d = RN(a^2 + b^2):
+// tau = (RN(a / d), -RN(b / d)); nothing to reflect: tau = 0, v = e_c, r_jj = alpha.  r_jj = (beta, 0), T_cc = tau,
+// and the rows of v and i v from row c (Vt, Vi, Vr).  One block.
+template <int N> __global__ void __launch_bounds__(kQrThreads) cqr_reflect_kernel(CqrPanel p, u64 c) {
+    __shared__ __align__(16) u32 sm[qr_dot_words<N>()];
+    __shared__ long long s_e;
+    __shared__ int s_go, s_needs;
+    constexpr u64 E = N + 3, C2 = 2 * E;
+    QrState* st = p.st;
+    if (st->rank < (long long)p.n) return;
+    const u64 j = p.k0 + c, len = p.mr - c;
+    u32* xc = p.Pt + (c * p.mr + c) * C2;
+    u32* v = p.Vt + (c * p.mr + c) * C2;
+    u32* iv = p.Vi + (c * p.mr + c) * C2;
+    const Num<N> s = block_exact_dot<N, true>(xc, 1, xc, 1, 2 * len, sm, p.error);
+    int below = 0;
+    for (u64 k = 2 + threadIdx.x; k < 2 * len; k += kQrThreads) below |= ldw<true>(xc + k * E + N + 1) != 0;
+    below = __syncthreads_or(below);
+    Num<N> beta = zero<N>(), v0 = qr_pow2<N>(0);
+    if (threadIdx.x == 0) {
+        const Num<N> are = load_plain<N>(xc), aim = load_plain<N>(xc + E);
+        const int needs = below || aim.s;
+        int reason = s.st ? 3 : (!are.s && !aim.s && !below) ? 1 : 0;
+        beta = are;
+        if (!reason && needs) {
+            beta = sqrt<N>(s);
+            if (are.s >= 0) beta = negate<N>(beta);
+            v0 = subx<N>(are, beta);
+        }
+        if (!reason && p.rank_bits > 0 && st->have_top && (long long)beta.e + p.rank_bits < st->top) reason = 2;
+        if (reason) { st->rank = (long long)j; st->reason = reason; st->status = s.st; s_go = 0; }
+        else {
+            s_go = 1; s_needs = needs; s_e = needs ? (long long)v0.e : 0;
+            if (needs) cq_store<N>(v, qr_scaled<N>(v0, s_e), qr_scaled<N>(aim, s_e));
+            else cq_store<N>(v, qr_pow2<N>(0), zero<N>());
+        }
+    }
+    __syncthreads();
+    if (!s_go) return;
+    const long long e = s_e;
+    const bool needs = s_needs;
+    if (needs)
+        for (u64 r = 1 + threadIdx.x; r < len; r += kQrThreads)
+            cq_store<N>(v + r * C2, qr_scaled<N>(load_plain<N>(xc + r * C2), e), qr_scaled<N>(load_plain<N>(xc + r * C2 + E), e));
+    __syncthreads();
+    Num<N> tre = zero<N>(), tim = zero<N>();
+    if (needs) {
+        const Num<N> sv = block_exact_dot<N, false>(v, 1, v, 1, 2 * len, sm, p.error);
+        if (threadIdx.x == 0) {
+            const Num<N> vim = load_plain<N>(v + E);
+            if (!vim.s && !vim.st) tre = divx<N>(qr_pow2<N>(1), sv);
+            else {
+                const Num<N> a = qr_scaled<N>(sv, 1), b = mulx<N>(qr_scaled<N>(beta, e), vim);
+                const Num<N> d = dot2_add<N>(a, a, b, b, zero<N>());
+                tre = divx<N>(a, d); tim = negate<N>(divx<N>(b, d));
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        cq_store<N>(xc, beta, zero<N>());
+        cq_store<N>(p.tau + j * C2, tre, tim);
+        cq_store<N>(p.T + ((p.k0 / p.nb) * p.nb * p.nb + c * p.nb + c) * C2, tre, tim);
+        if (!st->have_top || (long long)beta.e > st->top) st->top = beta.e;
+        st->have_top = 1;
+    }
+    for (u64 r = threadIdx.x; r < len; r += kQrThreads) {
+        cq_times_i<N>(iv + r * C2, v + r * C2);
+        for (u64 w = 0; w < C2; ++w) p.Vr[((c + r) * p.nb + c) * C2 + w] = v[r * C2 + w];
+    }
+}
+// After reflector c: block u < c gives G[u] = P(v_u^H v_c), block u >= c the W row entry Wp[c][u+1] = P(v_c^H a_{u+1})
+// (the block-start column), over rows [c, mr), two real dots each.  The last block to arrive writes the T column,
+// T_lc = -(tau * P(T[l][l..c) G[l..c))) with one rounding per component (cfma, linalg_complex.mm:237), and the next
+// column's conj y and i conj y for y_i = P(T[0..i][i]^H Wp[0..i][c+1]) (linalg_complex.mm:186-187).  kb - 1 blocks.
+template <int N> __global__ void __launch_bounds__(kQrThreads) cqr_dots_kernel(CqrPanel p, u64 c) {
+    __shared__ __align__(16) u32 sm[qr_dot_words<N>()];
+    __shared__ int s_last;
+    constexpr u64 E = N + 3, C2 = 2 * E;
+    QrState* st = p.st;
+    const long long rank = st->rank;
+    const bool reflected = rank == (long long)p.n;
+    const u64 j = p.k0 + c, len = p.mr - c, u = blockIdx.x;
+    if (reflected && u + 1 < p.kb) {
+        const u32* v = p.Vt + (c * p.mr + c) * C2;
+        const u32* iv = p.Vi + (c * p.mr + c) * C2;
+        const u32 *a0, *a1, *b0;
+        u32* out;
+        if (u < c) { a0 = p.Vt + (u * p.mr + c) * C2; a1 = p.Vi + (u * p.mr + c) * C2; b0 = v; out = p.G + u * C2; }
+        else { a0 = v; a1 = iv; b0 = p.Pt + ((u + 1) * p.mr + c) * C2; out = p.Wp + (c * p.nb + u + 1) * C2; }
+        const Num<N> re = block_exact_dot<N, true>(a0, 1, b0, 1, 2 * len, sm, p.error);
+        const Num<N> im = block_exact_dot<N, true>(a1, 1, b0, 1, 2 * len, sm, p.error);
+        if (threadIdx.x == 0) cq_store<N>(out, re, im);
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const u32 before = atomicAdd(&st->arrivals, 1u);
+        s_last = before == gridDim.x - 1;
+        if (s_last) st->arrivals = 0;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    u32* Tb = p.T + (p.k0 / p.nb) * p.nb * p.nb * C2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int WARPS = kQrThreads / 32;
+    if (reflected) {
+        for (u64 l = threadIdx.x; l < c; l += kQrThreads) { cq_conj<N>(p.Gc + l * C2, p.G + l * C2); cq_i_conj<N>(p.Gic + l * C2, p.G + l * C2); }
+        __syncthreads();
+        const Num<N> tre = ldn<N, false>(p.tau + j * C2), tim = ldn<N, false>(p.tau + j * C2 + E);
+        for (u64 l = warp; l < c; l += WARPS) {
+            const u32* trow = Tb + (l * p.nb + l) * C2;
+            const Num<N> pre = warp_exact_dot<N, false>(nullptr, false, trow, 1, p.Gc + l * C2, 1, 2 * (c - l), p.error);
+            const Num<N> pim = warp_exact_dot<N, false>(nullptr, false, trow, 1, p.Gic + l * C2, 1, 2 * (c - l), p.error);
+            if (lane == 0) {
+                const Cpx<N> z = cfma<N>(Cpx<N>{tre, tim}, Cpx<N>{pre, pim}, Cpx<N>{zero<N>(), zero<N>()});
+                cq_store<N>(Tb + (l * p.nb + c) * C2, negate<N>(z.re), negate<N>(z.im));
+            }
+        }
+    }
+    __syncthreads();
+    if (c + 1 < p.kb) {
+        const long long qn = (rank < (long long)j + 1 ? rank : (long long)j + 1) - (long long)p.k0;
+        for (long long i = warp; i < qn; i += WARPS) {
+            u32* tcol = p.scr + (u64)i * 3 * p.nb * C2;
+            u32* itcol = tcol + p.nb * C2;
+            u32* wl = itcol + p.nb * C2;
+            for (long long l = lane; l <= i; l += 32) {
+                const u32* t = Tb + ((u64)l * p.nb + (u64)i) * C2;
+                for (u64 w = 0; w < C2; ++w) { tcol[l * C2 + w] = t[w]; wl[l * C2 + w] = p.Wp[((u64)l * p.nb + c + 1) * C2 + w]; }
+                cq_times_i<N>(itcol + l * C2, t);
+            }
+            __syncwarp();
+            const Num<N> yre = warp_exact_dot<N, false>(nullptr, false, tcol, 1, wl, 1, 2 * ((u64)i + 1), p.error);
+            const Num<N> yim = warp_exact_dot<N, false>(nullptr, false, itcol, 1, wl, 1, 2 * ((u64)i + 1), p.error);
+            if (lane == 0) { cq_store<N>(p.yc + i * C2, yre, negate<N>(yim)); cq_store<N>(p.yic + i * C2, yim, yre); }
+        }
+    }
+}
+// The panel back into the row-split Wk, V (complex) and its embedding EV; the block's T into ET (entries l <= c).
+template <int N> __global__ void cqr_store_kernel(CqrPanel p) {
+    constexpr u64 E = N + 3, C2 = 2 * E;
+    const u64 q = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < p.kb * p.kb) {
+        const u64 l = q / p.kb, c = q % p.kb;
+        if (l <= c) {
+            const u64 b = p.k0 / p.nb;
+            cq_embed<N>(p.ET + b * 4 * p.nb * p.nb * E, 2 * p.nb, l, c, p.T + (b * p.nb * p.nb + l * p.nb + c) * C2);
+        }
+    }
+    if (q >= p.kb * p.mr) return;
+    const u64 c = q / p.mr, r = q % p.mr;
+    const u32* x = p.Pt + q * C2;
+    const u32* v = p.Vt + q * C2;
+    u32* re = p.Wk + (2 * (p.k0 + r) * p.n + p.k0 + c) * E;
+    for (u64 w = 0; w < E; ++w) { re[w] = x[w]; re[p.n * E + w] = x[E + w]; }
+    for (u64 w = 0; w < C2; ++w) p.V[((p.k0 + r) * p.n + p.k0 + c) * C2 + w] = v[w];
+    cq_embed<N>(p.EV, 2 * p.n, p.k0 + r, p.k0 + c, v);
+}
+// R (complex, n x n) <- the upper triangle of the row-split Wk (rows i >= rank keep columns j >= rank), and its
+// real embedding ER (2n x 2n) for the solves.
+template <int N> __global__ void cqr_extract_kernel(const u32* Wk, u32* R, u32* ER, u64 n, const QrState* st) {
+    constexpr u64 E = N + 3, C2 = 2 * E;
+    const u64 q = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n * n) return;
+    const u64 i = q / n, j = q % n, rank = (u64)st->rank;
+    const bool keep = j >= (i < rank ? i : rank);
+    for (u64 w = 0; w < E; ++w) {
+        R[q * C2 + w] = keep ? Wk[(2 * i * n + j) * E + w] : 0u;
+        R[q * C2 + E + w] = keep ? Wk[((2 * i + 1) * n + j) * E + w] : 0u;
+    }
+    cq_embed<N>(ER, 2 * n, i, j, R + q * C2);
+}
+
+struct CqrKernels {
+    void (*load)(const CqrPanel&, cudaStream_t);
+    void (*update)(const CqrPanel&, u64 c, cudaStream_t);
+    void (*reflect)(const CqrPanel&, u64 c, cudaStream_t);
+    void (*dots)(const CqrPanel&, u64 c, cudaStream_t);
+    void (*store)(const CqrPanel&, cudaStream_t);
+    void (*extract)(const u32* Wk, u32* R, u32* ER, u64 n, const QrState* st, cudaStream_t);
+};
+const CqrKernels* cqr_kernels(int limbs);
+
+template <int N> void cqr_load_launch(const CqrPanel& p, cudaStream_t s) {
+    if (p.mr * p.nb) cqr_load_kernel<N><<<qr_grid(p.mr * p.nb, 128), 128, 0, s>>>(p);
+}
+template <int N> void cqr_update_launch(const CqrPanel& p, u64 c, cudaStream_t s) {
+    if (p.mr) cqr_update_kernel<N><<<qr_grid(p.mr * 32, 256), 256, 0, s>>>(p, c);
+}
+template <int N> void cqr_reflect_launch(const CqrPanel& p, u64 c, cudaStream_t s) { cqr_reflect_kernel<N><<<1, kQrThreads, 0, s>>>(p, c); }
+template <int N> void cqr_dots_launch(const CqrPanel& p, u64 c, cudaStream_t s) {
+    if (p.kb > 1) cqr_dots_kernel<N><<<(unsigned)(p.kb - 1), kQrThreads, 0, s>>>(p, c);
+}
+template <int N> void cqr_store_launch(const CqrPanel& p, cudaStream_t s) {
+    const u64 items = p.kb * p.mr > p.kb * p.kb ? p.kb * p.mr : p.kb * p.kb;
+    if (items) cqr_store_kernel<N><<<qr_grid(items, 128), 128, 0, s>>>(p);
+}
+template <int N> void cqr_extract_launch(const u32* Wk, u32* R, u32* ER, u64 n, const QrState* st, cudaStream_t s) {
+    if (n) cqr_extract_kernel<N><<<qr_grid(n * n, 128), 128, 0, s>>>(Wk, R, ER, n, st);
+}
+
+}  // namespace lfd
+
+#define LF_CQR_INSTANTIATE(N)                                                                                   \
+    namespace lfd {                                                                                             \
+    extern const CqrKernels cqr_kernels_##N;                                                                    \
+    const CqrKernels cqr_kernels_##N = {cqr_load_launch<N>, cqr_update_launch<N>, cqr_reflect_launch<N>,        \
+                                        cqr_dots_launch<N>, cqr_store_launch<N>, cqr_extract_launch<N>};        \
+    }

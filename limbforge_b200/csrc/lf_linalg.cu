@@ -8,6 +8,7 @@
 #include "lf_residue.h"
 #include "lf_residue.cuh"
 #include "lf_qr.cuh"
+#include "lf_cqr.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -88,7 +89,7 @@ void exact_product_on(Linalg& la, const ProductLane& lane, int bits, lfd::LineVi
     uint32_t e = 0;
     cuda_check(cudaMemcpyAsync(&e, err, 4, cudaMemcpyDeviceToHost, s), "error flag");
     cuda_check(cudaStreamSynchronize(s), "exact product");
-    if (e) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    if (e) throw runtime_error("exact product: a device error word was set (a bounded wait gave up)");
 }
 void exact_product(Linalg& la, int bits, lfd::LineView left, lfd::LineView right, uint64_t M, uint64_t Nc, uint64_t K,
                    uint32_t* C, uint64_t ldc, bool subtract, bool lower, cudaStream_t s, int* method_used) {
@@ -313,7 +314,7 @@ static lf_cholesky_info cholesky_device(Linalg& la, int bits, uint32_t* W, size_
     cuda_check(cudaStreamSynchronize(s), "cholesky");
     float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
     cudaEventDestroy(g0); cudaEventDestroy(g1);
-    if (ev[0] | ev[1] | ev[2]) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    if (ev[0] | ev[1] | ev[2]) throw runtime_error("exact product: a device error word was set (a bounded wait gave up)");
     info.timing = {ms * 1e-3, since(w0)};
     return info;
 }
@@ -390,7 +391,7 @@ static double solve_device(Linalg& la, int bits, const uint32_t* L, size_t n, ui
     cuda_check(cudaStreamSynchronize(s), "solve");
     float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
     cudaEventDestroy(g0); cudaEventDestroy(g1);
-    if (ev[0] | ev[1] | ev[2]) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    if (ev[0] | ev[1] | ev[2]) throw runtime_error("exact product: a device error word was set (a bounded wait gave up)");
     return ms * 1e-3;
 }
 
@@ -660,7 +661,7 @@ int lf_linalg_ticket_report(lf_linalg_ticket* t, lf_linalg_report* rep) {
     LF_API_BEGIN
     if (!t || !rep) throw invalid_argument("null argument");
     if (!resident_product_done(*t->prod)) throw logic_error("ticket not resolved: wait for the submission first");
-    if (!resident_product_report(*t->prod, *rep)) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    if (!resident_product_report(*t->prod, *rep)) throw runtime_error("exact product: a device error word was set (a bounded wait gave up)");
     LF_API_END
 }
 void lf_linalg_ticket_destroy(lf_linalg_ticket* t) { delete t; }
@@ -724,11 +725,33 @@ struct QrFactor {
     int bits = 0;
     size_t m = 0, n = 0, nb = 0, block = 32;    // nb: the factor's block; block: the option the solves use
     bool pivot = false;
+    bool cplx = false;                           // a complex factor (linalg_complex.mm): complex arrays, real embeddings
     lf_qr_info info{};
     std::vector<uint32_t> R, V, T, tau;          // the accessors' arrays
     std::vector<size_t> perm;
-    DevBuf dV, dT, dR;                           // device copies for the solves and Q applications
+    DevBuf dV, dT, dR;                           // device copies for the solves and Q applications (complex: the embeddings)
 };
+
+// Block b of the compact-WY factor (V: mE x nE, T: blocks of nbE x nbE, all real) applied to columns [c0, c1) of X
+// (row stride ld): W = P(V_b^T X) over rows [k0, mE), Y = P(T_b^T W) (qt) or P(T_b W), X = D(X; V_b, Y), each with the
+// whole block; with have_y, Y is given (qr_block, linalg.mm:550-567).  The complex factor passes its real embeddings
+// with doubled dimensions and its row-split work matrix.
+static void qr_block_update(Linalg& la, const ProductLane& lane, int bits, const uint32_t* V, const uint32_t* T, size_t mE, size_t nE,
+                            size_t nbE, size_t b, uint32_t* X, size_t ld, size_t c0, size_t c1, bool qt, uint32_t* Wb, uint32_t* Yb,
+                            bool have_y, cudaStream_t q) {
+    const size_t E = bits / 32 + 3;
+    const size_t k0 = b * nbE, kb = std::min(nE, k0 + nbE) - k0, mr = mE - k0, c = c1 - c0;
+    if (!c || !kb) return;
+    const uint32_t* Vb = V + (k0 * nE + k0) * E;
+    const uint32_t* Tb = T + b * nbE * nbE * E;
+    uint32_t* Xb = X + (k0 * ld + c0) * E;
+    if (!have_y) {
+        exact_product_on(la, lane, bits, {Vb, 1, nE}, {Xb, 1, ld}, kb, c, mr, Wb + c0 * E, ld, false, false, q, nullptr, false);
+        const lfd::LineView tv = qt ? lfd::LineView{Tb, 1, nbE} : lfd::LineView{Tb, nbE, 1};
+        exact_product_on(la, lane, bits, tv, {Wb + c0 * E, 1, ld}, kb, c, kb, Yb + c0 * E, ld, false, false, q, nullptr, false);
+    }
+    exact_product_on(la, lane, bits, {Vb, nE, 1}, {Yb + c0 * E, 1, ld}, mr, c, kb, Xb, ld, true, false, q, nullptr, false);
+}
 
 // Factor the device matrix Wk (m x n, reduced in place) into V, T, tau and R (all device).  Right-looking with
 // one block of look-ahead (linalg.mm:721-745): after panel b, block b updates the next panel's columns on the
@@ -789,14 +812,7 @@ static lf_qr_info qr_device(Linalg& la, int bits, uint32_t* Wk, size_t m, size_t
     // block b on columns [c0, c1): W = P(V_b^T X), Y = P(T_b^T W), X = D(X; V_b, Y) (qr_block, linalg.mm:550-567)
     auto update = [&](size_t b, size_t c0, size_t c1, const ProductLane& lane, cudaStream_t q) {
         auto t = Clock::now();
-        const size_t k0 = b * nb, kb = std::min(n, k0 + nb) - k0, mr = m - k0, c = c1 - c0;
-        const uint32_t* Vb = V + (k0 * n + k0) * E;
-        const uint32_t* Tb = T + b * nb * nb * E;
-        exact_product_on(la, lane, bits, {Vb, 1, n}, {Wk + (k0 * n + c0) * E, 1, n}, kb, c, mr, Wb + c0 * E, n, false, false, q,
-                         nullptr, false);
-        exact_product_on(la, lane, bits, {Tb, 1, nb}, {Wb + c0 * E, 1, n}, kb, c, kb, Yb + c0 * E, n, false, false, q, nullptr, false);
-        exact_product_on(la, lane, bits, {Vb, n, 1}, {Yb + c0 * E, 1, n}, mr, c, kb, Wk + (k0 * n + c0) * E, n, true, false, q,
-                         nullptr, false);
+        qr_block_update(la, lane, bits, V, T, m, n, nb, b, Wk, n, c0, c1, true, Wb, Yb, false, q);
         ++info.gpu_updates;
         info.update_seconds += since(t);
     };
@@ -831,7 +847,7 @@ static lf_qr_info qr_device(Linalg& la, int bits, uint32_t* Wk, size_t m, size_t
     cuda_check(cudaStreamSynchronize(s), "qr");
     float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
     cudaEventDestroy(g0); cudaEventDestroy(g1);
-    if (ev[0] | ev[1] | ev[2]) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    if (ev[0] | ev[1] | ev[2]) throw runtime_error("exact product: a device error word was set (a bounded wait gave up)");
     info.rank = (size_t)host.rank; info.reason = host.reason; info.status = host.status;
     info.timing = {ms * 1e-3, since(w0)};
     return info;
@@ -937,10 +953,112 @@ static lf_qr_info qr_device_pivoted(Linalg& la, int bits, uint32_t* Wk, size_t m
     cuda_check(cudaStreamSynchronize(s), "pivoted qr");
     float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
     cudaEventDestroy(g0); cudaEventDestroy(g1);
-    if (ev[0] | ev[1]) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    if (ev[0] | ev[1]) throw runtime_error("exact product: a device error word was set (a bounded wait gave up)");
     for (size_t k = 0; k < n; ++k) perm_out[k] = (size_t)hp[k];
     info.rank = (size_t)host.rank; info.reason = host.reason; info.status = host.status;
     info.norm_recomputations = host.recomputed;
+    info.timing = {ms * 1e-3, since(w0)};
+    return info;
+}
+
+// Complex factorization (linalg_complex.mm:125-306) of the row-split device matrix Wk (2m x n real, reduced in place) into
+// V, T, tau, R (complex) and the real embeddings EV (2m x 2n), ET (blocks of 2nb x 2nb), ER (2n x 2n).  The loop and the
+// look-ahead are the real factorization's; the trailing updates are qr_block_update on the embeddings.
+static lf_qr_info cqr_device(Linalg& la, int bits, uint32_t* Wk, size_t m, size_t n, size_t nb, int rank_bits, uint32_t* V, uint32_t* T,
+                             uint32_t* tau, uint32_t* R, uint32_t* EV, uint32_t* ET, uint32_t* ER) {
+    lf_qr_info info{};
+    info.rank = n;
+    auto w0 = Clock::now();
+    Engine& e = *la.engine;
+    cudaStream_t s = e.stream;
+    const int limbs = bits / 32;
+    const size_t E = limbs + 3, eb = E * 4, cb = 2 * eb;
+    const auto* ck = lfd::cqr_kernels(limbs);
+    const size_t blocks = nb ? (n + nb - 1) / nb : 0;
+    cuda_check(cudaMemsetAsync(V, 0, m * n * cb, s), "memset");
+    cuda_check(cudaMemsetAsync(T, 0, blocks * nb * nb * cb, s), "memset");
+    cuda_check(cudaMemsetAsync(tau, 0, n * cb, s), "memset");
+    cuda_check(cudaMemsetAsync(EV, 0, 4 * m * n * eb, s), "memset");
+    cuda_check(cudaMemsetAsync(ET, 0, 4 * blocks * nb * nb * eb, s), "memset");
+    uint32_t* Wb = static_cast<uint32_t*>(la.qr[0].get(2 * nb * n * eb + 16));
+    uint32_t* Yb = static_cast<uint32_t*>(la.qr[1].get(2 * nb * n * eb + 16));
+    uint32_t* Pt = static_cast<uint32_t*>(la.qr[2].get(4 * nb * m * cb + 16));       // Pt, Vt, Vi, Vr
+    uint32_t* Vt = Pt + nb * m * 2 * E;
+    uint32_t* Vi = Vt + nb * m * 2 * E;
+    uint32_t* Vr = Vi + nb * m * 2 * E;
+    uint32_t* Wp = static_cast<uint32_t*>(la.qr[4].get((nb * nb + 6 * nb) * cb + 3 * nb * nb * cb + 16));
+    uint32_t* G = Wp + nb * nb * 2 * E;
+    uint32_t* Gc = G + nb * 2 * E;
+    uint32_t* Gic = Gc + nb * 2 * E;
+    uint32_t* yc = Gic + nb * 2 * E;
+    uint32_t* yic = yc + nb * 2 * E;
+    uint32_t* scr = yic + 2 * nb * 2 * E;
+    auto* st = static_cast<lfd::QrState*>(la.qr[7].get(sizeof(lfd::QrState)));
+    lfd::QrState host{};
+    host.rank = (long long)n;
+    cuda_check(cudaMemcpyAsync(st, &host, sizeof host, cudaMemcpyHostToDevice, s), "state");
+    uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));
+    cuda_check(cudaMemsetAsync(err, 0, 16, s), "memset");
+    const ProductLane lane_a = main_lane(la), lane_b = side_lane(la);
+    cudaStream_t s2 = la.side;
+    cudaEvent_t g0, g1;
+    cuda_check(cudaEventCreate(&g0), "event"); cuda_check(cudaEventCreate(&g1), "event");
+    cuda_check(cudaEventRecord(g0, s), "event");
+    lfd::CqrPanel P{Wk, m, n, V, T, tau, EV, ET, Pt, Vt, Vi, Vr, Wp, G, Gc, Gic, yc, yic, scr, 0, 0, nb, 0, rank_bits, st, err};
+    auto panel = [&](size_t k0, size_t k1) -> size_t {
+        auto t = Clock::now();
+        P.k0 = k0; P.kb = k1 - k0; P.mr = m - k0;
+        ck->load(P, s);
+        for (size_t c = 0; c < P.kb; ++c) {
+            if (c) ck->update(P, c, s);
+            ck->reflect(P, c, s);
+            ck->dots(P, c, s);
+        }
+        ck->store(P, s);
+        cuda_check(cudaGetLastError(), "complex qr panel");
+        cuda_check(cudaMemcpyAsync(&host, st, sizeof host, cudaMemcpyDeviceToHost, s), "state");
+        cuda_check(cudaStreamSynchronize(s), "complex qr panel");
+        ++info.blocks;
+        info.panel_seconds += since(t);
+        return std::min(k1, (size_t)host.rank);
+    };
+    auto update = [&](size_t b, size_t c0, size_t c1, const ProductLane& lane, cudaStream_t q) {
+        auto t = Clock::now();
+        qr_block_update(la, lane, bits, EV, ET, 2 * m, 2 * n, 2 * nb, b, Wk, n, c0, c1, true, Wb, Yb, false, q);
+        ++info.gpu_updates;
+        info.update_seconds += since(t);
+    };
+    bool side_pending = false;
+    size_t k0 = 0, k1 = std::min(n, nb), p = n ? panel(0, k1) : 0;
+    while (k1 < n) {
+        const size_t b = k0 / nb;
+        if (side_pending) cuda_check(cudaStreamWaitEvent(s, la.ev_side, 0), "event wait");
+        if (p < k1) {
+            if (p > k0) update(b, k1, n, lane_a, s);
+            break;
+        }
+        const size_t k2 = std::min(n, k1 + nb);
+        update(b, k1, k2, lane_a, s);
+        if (k2 < n) {
+            update(b, k2, n, lane_b, s2);
+            cuda_check(cudaEventRecord(la.ev_side, s2), "event");
+            side_pending = true;
+        }
+        p = panel(k1, k2);
+        k0 = k1; k1 = k2;
+    }
+    if (side_pending) cuda_check(cudaStreamWaitEvent(s, la.ev_side, 0), "event wait");
+    ck->extract(Wk, R, ER, n, st, s);
+    cuda_check(cudaGetLastError(), "complex qr extract");
+    cuda_check(cudaEventRecord(g1, s), "event");
+    uint32_t ev[3] = {0, 0, 0};
+    cuda_check(cudaMemcpyAsync(&host, st, sizeof host, cudaMemcpyDeviceToHost, s), "state");
+    cuda_check(cudaMemcpyAsync(ev, err, 12, cudaMemcpyDeviceToHost, s), "error flag");
+    cuda_check(cudaStreamSynchronize(s), "complex qr");
+    float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
+    cudaEventDestroy(g0); cudaEventDestroy(g1);
+    if (ev[0] | ev[1] | ev[2]) throw runtime_error("exact product: a device error word was set (a bounded wait gave up)");
+    info.rank = (size_t)host.rank; info.reason = host.reason; info.status = host.status;
     info.timing = {ms * 1e-3, since(w0)};
     return info;
 }
@@ -952,34 +1070,26 @@ static double qr_apply_device(Linalg& la, const QrFactor& f, uint32_t* C, size_t
     if (!blocks || !nrhs || !f.m) return 0;
     Engine& e = *la.engine;
     cudaStream_t s = e.stream;
-    const size_t E = f.bits / 32 + 3, eb = E * 4, m = f.m, n = f.n;
-    uint32_t* Wb = static_cast<uint32_t*>(la.qr[0].get(nb * nrhs * eb + 16));
-    uint32_t* Yb = static_cast<uint32_t*>(la.qr[1].get(nb * nrhs * eb + 16));
+    const size_t k = f.cplx ? 2 : 1;                    // a complex factor applies its real embeddings to row-split C
+    const size_t eb = (f.bits / 32 + 3) * 4;
+    uint32_t* Wb = static_cast<uint32_t*>(la.qr[0].get(k * nb * nrhs * eb + 16));
+    uint32_t* Yb = static_cast<uint32_t*>(la.qr[1].get(k * nb * nrhs * eb + 16));
     uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));
     cuda_check(cudaMemsetAsync(err, 0, 16, s), "memset");
     const ProductLane lane = main_lane(la);
-    const uint32_t* V = static_cast<const uint32_t*>(f.dV.p);
-    const uint32_t* T = static_cast<const uint32_t*>(f.dT.p);
     cudaEvent_t g0, g1;
     cuda_check(cudaEventCreate(&g0), "event"); cuda_check(cudaEventCreate(&g1), "event");
     cuda_check(cudaEventRecord(g0, s), "event");
-    for (size_t q = 0; q < blocks; ++q) {
-        const size_t b = qt ? q : blocks - 1 - q, k0 = b * nb, kb = std::min(n, k0 + nb) - k0, mr = m - k0;
-        const uint32_t* Vb = V + (k0 * n + k0) * E;
-        const uint32_t* Tb = T + b * nb * nb * E;
-        uint32_t* X = C + k0 * nrhs * E;
-        exact_product_on(la, lane, f.bits, {Vb, 1, n}, {X, 1, nrhs}, kb, nrhs, mr, Wb, nrhs, false, false, s, nullptr, false);
-        const lfd::LineView tv = qt ? lfd::LineView{Tb, 1, nb} : lfd::LineView{Tb, nb, 1};
-        exact_product_on(la, lane, f.bits, tv, {Wb, 1, nrhs}, kb, nrhs, kb, Yb, nrhs, false, false, s, nullptr, false);
-        exact_product_on(la, lane, f.bits, {Vb, n, 1}, {Yb, 1, nrhs}, mr, nrhs, kb, X, nrhs, true, false, s, nullptr, false);
-    }
+    for (size_t q = 0; q < blocks; ++q)
+        qr_block_update(la, lane, f.bits, static_cast<const uint32_t*>(f.dV.p), static_cast<const uint32_t*>(f.dT.p), k * f.m, k * f.n,
+                        k * nb, qt ? q : blocks - 1 - q, C, nrhs, 0, nrhs, qt, Wb, Yb, false, s);
     cuda_check(cudaEventRecord(g1, s), "event");
     uint32_t ev = 0;
     cuda_check(cudaMemcpyAsync(&ev, lane.err, 4, cudaMemcpyDeviceToHost, s), "error flag");
     cuda_check(cudaStreamSynchronize(s), "qr apply");
     float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
     cudaEventDestroy(g0); cudaEventDestroy(g1);
-    if (ev) throw runtime_error("exact product: a cluster of terms exceeds the 6144-bit exact window");
+    if (ev) throw runtime_error("exact product: a device error word was set (a bounded wait gave up)");
     return ms * 1e-3;
 }
 
@@ -989,18 +1099,38 @@ static double qr_apply_device(Linalg& la, const QrFactor& f, uint32_t* C, size_t
 // invalid zeros.
 static double qr_solve_device(Linalg& la, const QrFactor& f, uint32_t* C, size_t nrhs) {
     double g = qr_apply_device(la, f, C, nrhs, true);
-    const size_t p = f.info.rank, n = f.n;
+    // complex: the real backward substitution of the 2n x 2n embedding of R, blocks 2 min(nb, p) (linalg_complex.mm:339-342)
+    const size_t k = f.cplx ? 2 : 1, p = k * f.info.rank, n = k * f.n;
+    const size_t block = f.cplx ? 2 * std::min(f.nb, f.info.rank) : f.block;
     if (!p) return g;
     if (p < n) {
         const size_t eb = (f.bits / 32 + 3) * 4;
         uint32_t* R11 = static_cast<uint32_t*>(la.qr[9].get(p * p * eb + 16));
         lfd::qr_kernels(f.bits / 32)->copy(static_cast<const uint32_t*>(f.dR.p), n, R11, p, p, p, la.engine->stream);
         cuda_check(cudaGetLastError(), "qr leading block");
-        g += solve_device(la, f.bits, R11, p, C, nrhs, f.block, 2, true);
+        g += solve_device(la, f.bits, R11, p, C, nrhs, block, 2, true);
     } else {
-        g += solve_device(la, f.bits, static_cast<const uint32_t*>(f.dR.p), n, C, nrhs, f.block, 2, true);
+        g += solve_device(la, f.bits, static_cast<const uint32_t*>(f.dR.p), n, C, nrhs, block, 2, true);
     }
     return g;
+}
+// Complex host arrays <-> the row-split real layout the device works on (row 2r = Re of row r, 2r + 1 = Im).
+static void split_rows(const uint32_t* A, size_t rows, size_t cols, size_t E, std::vector<uint32_t>& out) {
+    out.resize(2 * rows * cols * E);
+    for (size_t r = 0; r < rows; ++r)
+        for (size_t c = 0; c < cols; ++c) {
+            const uint32_t* z = A + (r * cols + c) * 2 * E;
+            std::memcpy(&out[(2 * r * cols + c) * E], z, E * 4);
+            std::memcpy(&out[((2 * r + 1) * cols + c) * E], z + E, E * 4);
+        }
+}
+static void join_rows(const uint32_t* W, size_t rows, size_t cols, size_t E, uint32_t* out) {
+    for (size_t r = 0; r < rows; ++r)
+        for (size_t c = 0; c < cols; ++c) {
+            uint32_t* z = out + (r * cols + c) * 2 * E;
+            std::memcpy(z, W + (2 * r * cols + c) * E, E * 4);
+            std::memcpy(z + E, W + ((2 * r + 1) * cols + c) * E, E * 4);
+        }
 }
 
 static void check_qr_size(size_t n, size_t rows) {
@@ -1142,71 +1272,151 @@ const size_t* lf_qr_permutation(const lf_qr* f) { return f && !f->perm.empty() ?
 int lf_qr_solve(const lf_qr* f, const void* B, size_t nrhs, void* X, lf_timing* timing) {
     LF_API_BEGIN
     if (!f) throw logic_error("empty QR factor");
-    check_qr_size(f->n, nrhs);
-    check_qr_size(1, f->m * nrhs);
+    check_qr_size(f->cplx ? 2 * f->n : f->n, nrhs);
+    check_qr_size(1, (f->cplx ? 4 : 1) * f->m * nrhs);
     if (timing) *timing = {0, 0};
     if (!f->n || !nrhs) return LF_OK;
     if (!B || !X) throw invalid_argument("null matrix");
+    const size_t k = f->cplx ? 2 : 1;                    // components per element
     const size_t eb = size_t(f->bits / 8 + 12), E = eb / 4, m = f->m, n = f->n, p = f->info.rank;
-    if (overlap(X, n * nrhs * eb, B, m * nrhs * eb)) throw invalid_argument("solve: X overlaps B");
+    if (overlap(X, n * nrhs * k * eb, B, m * nrhs * k * eb)) throw invalid_argument("solve: X overlaps B");
     auto w0 = Clock::now();
     if (p < n && (!f->pivot || f->info.reason == 3)) {
         const uint32_t st = 4u | (f->pivot ? f->info.status : 0u);
         auto* x = static_cast<uint32_t*>(X);
-        std::memset(x, 0, n * nrhs * eb);
-        for (size_t q = 0; q < n * nrhs; ++q) x[q * E + E - 1] = st;
+        std::memset(x, 0, n * nrhs * k * eb);
+        for (size_t q = 0; q < k * n * nrhs; ++q) x[q * E + E - 1] = st;
         if (timing) *timing = {0, since(w0)};
         return LF_OK;
     }
     Linalg& la = *f->owner;
     Engine& e = *la.engine;
     e.activate();
-    uint32_t* C = static_cast<uint32_t*>(la.qr[8].get(m * nrhs * eb));
-    cuda_check(cudaMemcpyAsync(C, B, m * nrhs * eb, cudaMemcpyHostToDevice, e.stream), "upload");
+    // the device works on k m real rows (complex: split by rows); the solution is its first k min(p, n) rows
+    uint32_t* C = static_cast<uint32_t*>(la.qr[8].get(k * m * nrhs * eb));
+    std::vector<uint32_t> split;
+    if (f->cplx) {
+        split_rows(static_cast<const uint32_t*>(B), m, nrhs, E, split);
+        cuda_check(cudaMemcpyAsync(C, split.data(), 2 * m * nrhs * eb, cudaMemcpyHostToDevice, e.stream), "upload");
+    } else {
+        cuda_check(cudaMemcpyAsync(C, B, m * nrhs * eb, cudaMemcpyHostToDevice, e.stream), "upload");
+    }
     const double g = qr_solve_device(la, *f, C, nrhs);
     const size_t rows = std::min(p, n);
-    if (f->pivot) {
-        std::vector<uint32_t> Z(rows * nrhs * E);
-        if (rows) cuda_check(cudaMemcpyAsync(Z.data(), C, rows * nrhs * eb, cudaMemcpyDeviceToHost, e.stream), "download");
-        cuda_check(cudaStreamSynchronize(e.stream), "download");
-        auto* x = static_cast<uint32_t*>(X);
-        std::memset(x, 0, n * nrhs * eb);
-        for (size_t i = 0; i < rows; ++i) std::memcpy(x + f->perm[i] * nrhs * E, Z.data() + i * nrhs * E, nrhs * eb);
+    std::vector<uint32_t> Z(k * rows * nrhs * E + 1), Zc;
+    if (rows) cuda_check(cudaMemcpyAsync(Z.data(), C, k * rows * nrhs * eb, cudaMemcpyDeviceToHost, e.stream), "download");
+    cuda_check(cudaStreamSynchronize(e.stream), "download");
+    const uint32_t* z = Z.data();
+    if (f->cplx) {
+        Zc.resize(2 * rows * nrhs * E + 1);
+        join_rows(Z.data(), rows, nrhs, E, Zc.data());
+        z = Zc.data();
+    }
+    auto* x = static_cast<uint32_t*>(X);
+    if (rows < n) std::memset(x, 0, n * nrhs * k * eb);
+    for (size_t i = 0; i < rows; ++i) std::memcpy(x + f->perm[i] * nrhs * k * E, z + i * nrhs * k * E, nrhs * k * eb);
+    if (timing) *timing = {g, since(w0)};
+    LF_API_END
+}
+
+// QRFactor::apply_q (linalg.hpp:129): B (m x nrhs) <- Q^T B (transpose) or Q B, in place; a complex factor's adjoint is Q^H.
+int lf_qr_apply_q(const lf_qr* f, void* B, size_t nrhs, int transpose, lf_timing* timing) {
+    LF_API_BEGIN
+    if (!f) throw logic_error("empty QR factor");
+    check_qr_size(f->cplx ? 2 * f->n : f->n, nrhs);
+    check_qr_size(1, (f->cplx ? 4 : 1) * f->m * nrhs);
+    if (timing) *timing = {0, 0};
+    if (!f->m || !nrhs) return LF_OK;
+    if (!B) throw invalid_argument("null matrix");
+    const size_t k = f->cplx ? 2 : 1;
+    const size_t eb = size_t(f->bits / 8 + 12), E = eb / 4, m = f->m;
+    auto w0 = Clock::now();
+    Linalg& la = *f->owner;
+    Engine& e = *la.engine;
+    e.activate();
+    uint32_t* C = static_cast<uint32_t*>(la.qr[8].get(k * m * nrhs * eb));
+    std::vector<uint32_t> split;
+    if (f->cplx) {
+        split_rows(static_cast<const uint32_t*>(B), m, nrhs, E, split);
+        cuda_check(cudaMemcpyAsync(C, split.data(), 2 * m * nrhs * eb, cudaMemcpyHostToDevice, e.stream), "upload");
     } else {
-        cuda_check(cudaMemcpyAsync(X, C, n * nrhs * eb, cudaMemcpyDeviceToHost, e.stream), "download");
+        cuda_check(cudaMemcpyAsync(C, B, m * nrhs * eb, cudaMemcpyHostToDevice, e.stream), "upload");
+    }
+    const double g = qr_apply_device(la, *f, C, nrhs, transpose != 0);
+    if (f->cplx) {
+        cuda_check(cudaMemcpyAsync(split.data(), C, 2 * m * nrhs * eb, cudaMemcpyDeviceToHost, e.stream), "download");
+        cuda_check(cudaStreamSynchronize(e.stream), "download");
+        join_rows(split.data(), m, nrhs, E, static_cast<uint32_t*>(B));
+    } else {
+        cuda_check(cudaMemcpyAsync(B, C, m * nrhs * eb, cudaMemcpyDeviceToHost, e.stream), "download");
         cuda_check(cudaStreamSynchronize(e.stream), "download");
     }
     if (timing) *timing = {g, since(w0)};
     LF_API_END
 }
 
-// QRFactor::apply_q (linalg.hpp:129): B (m x nrhs) <- Q^T B (transpose) or Q B, in place.
-int lf_qr_apply_q(const lf_qr* f, void* B, size_t nrhs, int transpose, lf_timing* timing) {
+// Linalg::factor_qr_complex (linalg.hpp:170): complex Householder QR of A (m x n Complex<bits/32>, row-major, m >= n);
+// the factor's arrays are complex and its solve and apply_q take complex matrices.  Column pivoting of complex factors
+// is not built.
+int lf_linalg_factor_qr_complex(lf_linalg* la, int bits, const void* A, size_t m, size_t n, const lf_qr_options* o, lf_qr** out) {
     LF_API_BEGIN
-    if (!f) throw logic_error("empty QR factor");
-    check_qr_size(f->n, nrhs);
-    check_qr_size(1, f->m * nrhs);
-    if (timing) *timing = {0, 0};
-    if (!f->m || !nrhs) return LF_OK;
-    if (!B) throw invalid_argument("null matrix");
-    const size_t eb = size_t(f->bits / 8 + 12), m = f->m;
+    if (!out) throw invalid_argument("null output");
+    *out = nullptr;
+    if (!la) throw invalid_argument("null linalg");
+    check_bits(bits);
+    if (m < n) throw invalid_argument("factor_qr_complex: rows >= columns required");
+    if (2 * n >= 46341 || 4 * n * m >= (size_t(1) << 31)) throw invalid_argument("matrix dimensions exceed 32-bit indexing");
+    if (m * n && !A) throw invalid_argument("null matrix");
+    const lf_qr_options opts = o ? *o : lf_qr_options{32, 0, 0, 1, 0, 0};
+    if (opts.rank_bits < 0) throw invalid_argument("factor_qr_complex: rank_bits >= 0");
+    if (opts.pivot) throw runtime_error("factor_qr_complex: column pivoting of complex factors is not built");
+    std::unique_ptr<lf_qr> f(new lf_qr());
+    f->owner = la; f->bits = bits; f->m = m; f->n = n; f->cplx = true;
+    f->block = opts.block; f->nb = opts.block ? std::min(opts.block, n) : n;
+    const size_t eb = size_t(bits / 8 + 12), E = eb / 4, cb = 2 * eb;
+    const size_t blocks = f->nb ? (n + f->nb - 1) / f->nb : 0;
     auto w0 = Clock::now();
-    Linalg& la = *f->owner;
-    Engine& e = *la.engine;
-    e.activate();
-    uint32_t* C = static_cast<uint32_t*>(la.qr[8].get(m * nrhs * eb));
-    cuda_check(cudaMemcpyAsync(C, B, m * nrhs * eb, cudaMemcpyHostToDevice, e.stream), "upload");
-    const double g = qr_apply_device(la, *f, C, nrhs, transpose != 0);
-    cuda_check(cudaMemcpyAsync(B, C, m * nrhs * eb, cudaMemcpyDeviceToHost, e.stream), "download");
-    cuda_check(cudaStreamSynchronize(e.stream), "download");
-    if (timing) *timing = {g, since(w0)};
+    f->R.assign(n * n * 2 * E, 0); f->V.assign(m * n * 2 * E, 0);
+    f->T.assign(blocks * f->nb * f->nb * 2 * E, 0); f->tau.assign(n * 2 * E, 0);
+    f->perm.resize(n);
+    for (size_t k = 0; k < n; ++k) f->perm[k] = k;
+    f->info.rank = n;
+    if (n) {
+        Engine& e = *la->engine;
+        e.activate();
+        cudaStream_t s = e.stream;
+        std::vector<uint32_t> split;
+        split_rows(static_cast<const uint32_t*>(A), m, n, E, split);
+        uint32_t* Wk = static_cast<uint32_t*>(la->work[4].get(2 * m * n * eb));
+        cuda_check(cudaMemcpyAsync(Wk, split.data(), 2 * m * n * eb, cudaMemcpyHostToDevice, s), "upload");
+        DevBuf dVc, dTc, dRc, dtau;
+        uint32_t* V = static_cast<uint32_t*>(dVc.get(m * n * cb));
+        uint32_t* T = static_cast<uint32_t*>(dTc.get(blocks * f->nb * f->nb * cb + 16));
+        uint32_t* R = static_cast<uint32_t*>(dRc.get(n * n * cb));
+        uint32_t* tau = static_cast<uint32_t*>(dtau.get(n * cb));
+        uint32_t* EV = static_cast<uint32_t*>(f->dV.get(4 * m * n * eb));
+        uint32_t* ET = static_cast<uint32_t*>(f->dT.get(4 * blocks * f->nb * f->nb * eb + 16));
+        uint32_t* ER = static_cast<uint32_t*>(f->dR.get(4 * n * n * eb));
+        f->info = cqr_device(*la, bits, Wk, m, n, f->nb, opts.rank_bits, V, T, tau, R, EV, ET, ER);
+        cuda_check(cudaMemcpyAsync(f->R.data(), R, n * n * cb, cudaMemcpyDeviceToHost, s), "download");
+        cuda_check(cudaMemcpyAsync(f->V.data(), V, m * n * cb, cudaMemcpyDeviceToHost, s), "download");
+        if (blocks) cuda_check(cudaMemcpyAsync(f->T.data(), T, blocks * f->nb * f->nb * cb, cudaMemcpyDeviceToHost, s), "download");
+        cuda_check(cudaMemcpyAsync(f->tau.data(), tau, n * cb, cudaMemcpyDeviceToHost, s), "download");
+        cuda_check(cudaStreamSynchronize(s), "download");
+    } else {
+        f->info.rank = 0;
+    }
+    f->info.timing.wall_seconds = since(w0);
+    *out = f.release();
     LF_API_END
 }
+int lf_qr_is_complex(const lf_qr* f) { return f && f->cplx ? 1 : 0; }
 
 // QRFactor::solve / apply_q on Buffers (linalg.hpp:131-134): synchronous, outside any batch, buffers idle.
 int lf_qr_solve_buffers(const lf_qr* f, lf_buffer* B, size_t nrhs, lf_buffer* X, lf_timing* timing) {
     LF_API_BEGIN
     if (!f) throw logic_error("empty QR factor");
+    if (f->cplx) throw invalid_argument("complex QR factors have no Buffer forms");
     check_qr_size(f->n, nrhs);
     check_qr_size(1, f->m * nrhs);
     const size_t eb = size_t(f->bits / 8 + 12), E = eb / 4, m = f->m, n = f->n, p = f->info.rank;
@@ -1251,6 +1461,7 @@ int lf_qr_solve_buffers(const lf_qr* f, lf_buffer* B, size_t nrhs, lf_buffer* X,
 int lf_qr_apply_q_buffer(const lf_qr* f, lf_buffer* B, size_t nrhs, int transpose, lf_timing* timing) {
     LF_API_BEGIN
     if (!f) throw logic_error("empty QR factor");
+    if (f->cplx) throw invalid_argument("complex QR factors have no Buffer forms");
     check_qr_size(f->n, nrhs);
     check_qr_size(1, f->m * nrhs);
     const size_t eb = size_t(f->bits / 8 + 12), m = f->m;

@@ -41,6 +41,7 @@ void Submission::finish() {
     timing.wall_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
     for (auto* r : resources) { r->busy.store(false, std::memory_order_release); release(r); }
     resources.clear();
+    keep.clear();
     done = true;
 }
 Submission::~Submission() {
@@ -428,6 +429,7 @@ int lf_batch_submit(lf_batch* bt, lf_submission** out) {
         throw;
     }
     sub->resources.swap(bt->resources);     // references move to the submission
+    sub->keep.swap(bt->keep);
     bt->submitted = true;
     *out = sub;
     LF_API_END

@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -105,6 +106,7 @@ struct Batch {
     std::vector<Op> ops;
     std::vector<Buffer*> resources;   // each retained once
     std::vector<Buffer*> written;
+    std::vector<std::shared_ptr<void>> keep;   // objects the recorded operations use, freed when the submission completes
     bool submitted = false;
     void retain(Buffer* r, bool write = false);
     ~Batch();
@@ -114,6 +116,7 @@ struct Submission {
     Engine* engine = nullptr;
     cudaEvent_t start = nullptr, end = nullptr;
     std::vector<Buffer*> resources;
+    std::vector<std::shared_ptr<void>> keep;
     bool done = false; std::string error;
     lf_timing timing{0, 0};
     std::chrono::steady_clock::time_point wall0;

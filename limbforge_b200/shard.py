@@ -52,3 +52,48 @@ def max_over_ranks(value: float, dist=None, device: str = "cpu") -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def gemm_row_block(m: int, rank: int, world: int, align: int = 128) -> tuple[int, int]:
+    """Rows [lo, hi) of an m-row exact product's output for `rank`: whole blocks of `align` rows (the residue engine's
+    output tile height) split as evenly as split_range splits units, the last block ragged."""
+    if align < 1:
+        raise ValueError("align must be positive")
+    blocks = (m + align - 1) // align
+    lo, hi = split_range(blocks, rank, world)
+    return min(m, lo * align), min(m, hi * align)
+
+
+def sharded_exact_gemm(gemm, bits: int, transpose_a: bool, A: np.ndarray, B: np.ndarray, m: int, n: int, k: int,
+                       C: np.ndarray | None = None, subtract: bool = False, dist=None, align: int = 128) -> np.ndarray:
+    """C <- RN(C - op(A) B) (or RN(op(A) B)) with C's rows split over the ranks of the default process group: each rank
+    computes its row block with `gemm(bits, transpose_a, A_rows, B, rows, n, k, C_rows, subtract)` (Linalg.gemm, or any
+    function of that signature) from op(A)'s matching rows and all of B, and an all-gather assembles the whole C on
+    every rank.  Every output is one rounding of its own exact dot product, so the result is bit-identical to the
+    unsharded product whatever the split.  Arrays are element words: A [k*m or m*k, W], B [k*n, W], C [m*n, W]."""
+    w = A.shape[-1]
+    world = dist.get_world_size() if dist is not None and dist.is_initialized() else 1
+    rank = dist.get_rank() if world > 1 else 0
+    lo, hi = gemm_row_block(m, rank, world, align)
+    rows = hi - lo
+    if transpose_a:
+        a_rows = np.ascontiguousarray(A.reshape(k, m, w)[:, lo:hi]).reshape(k * rows, w)
+    else:
+        a_rows = np.ascontiguousarray(A.reshape(m, k, w)[lo:hi]).reshape(rows * k, w)
+    c_rows = (np.zeros((rows * n, w), np.uint32) if C is None else
+              np.ascontiguousarray(C.reshape(m, n, w)[lo:hi]).reshape(rows * n, w))
+    if rows:
+        gemm(bits, transpose_a, a_rows, B, rows, n, k, c_rows, subtract)
+    if world == 1:
+        return c_rows
+    import torch
+    most = max(gemm_row_block(m, r, world, align)[1] - gemm_row_block(m, r, world, align)[0] for r in range(world))
+    mine = torch.zeros((most * n, w), dtype=torch.int32)
+    mine[:rows * n] = torch.from_numpy(c_rows.view(np.int32))
+    parts = [torch.zeros_like(mine) for _ in range(world)]
+    dist.all_gather(parts, mine)
+    out = np.empty((m * n, w), np.uint32)
+    for r, t in enumerate(parts):
+        a, b = gemm_row_block(m, r, world, align)
+        out[a * n:b * n] = t[:(b - a) * n].numpy().view(np.uint32)
+    return out

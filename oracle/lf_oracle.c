@@ -1342,3 +1342,42 @@ int lfo_qr_complex_solve(int bits, size_t m, size_t nn, size_t block, const long
 }
 #undef CQP
 #undef CQD
+
+/* ---------------------------------------------------------------- exact batched 4 x 4 products
+ * The exact 4 x 4 batch of the reference's experiment (benchmarks/experiments/exact_gemm4/README.md, prototype.hpp:
+ * 5-24): fixed row-major 4 x 4 matrices, matrix t at A + t*sa, B + t*sb, C + t*sc elements (stride 0 broadcasts an
+ * input); each real output component is RN(C_old + sum_k a_ik b_kj), one rounding of the exact sum (C_old left out
+ * without accumulation), then negated when asked; a complex component sums its eight signed real products.
+ * Statuses: zero with the OR of every operand the component reads (and C_old); no nonzero product gives C_old (or
+ * zero); exact cancellation gives canonical zero. */
+int lfo_exact_gemm4(int bits, int complex_, size_t count, size_t sa, size_t sb, size_t sc, int accumulate, int negative,
+                    const word* A, const word* B, word* C) {
+    const int n = bits / 32; const size_t E = (size_t)n + 3, S = complex_ ? 2 * E : E;
+#pragma omp parallel for schedule(static)
+    for (size_t t = 0; t < count; ++t)
+        for (size_t i = 0; i < 4; ++i)
+            for (size_t j = 0; j < 4; ++j) {
+                word* out = C + (t * sc + i * 4 + j) * S;
+                const word* a = A + (t * sa + i * 4) * S;
+                const word* b = B + (t * sb + j) * S;
+                if (!complex_) {
+                    word r[35];
+                    lfo_exact_dot_add(n, accumulate ? out : NULL, 0, a, 1, b, 4, 4, r);
+                    if (negative) *SGN(r, n) = -gsgn(r, n);
+                    copy_num(out, r, n);
+                } else {
+                    /* re: a.re b.re - a.im b.im; im: a.re b.im + a.im b.re, over the interleaved (re, im) sequence of row i */
+                    word br[8 * 35], bi[8 * 35], r[35], q[35];
+                    for (int k = 0; k < 4; ++k) {
+                        const word* z = b + (size_t)k * 4 * S;
+                        copy_num(br + (2 * k) * E, z, n); neg_copy(br + (2 * k + 1) * E, z + E, n);
+                        copy_num(bi + (2 * k) * E, z + E, n); copy_num(bi + (2 * k + 1) * E, z, n);
+                    }
+                    lfo_exact_dot_add(n, accumulate ? out : NULL, 0, a, 1, br, 1, 8, r);
+                    lfo_exact_dot_add(n, accumulate ? out + E : NULL, 0, a, 1, bi, 1, 8, q);
+                    if (negative) { *SGN(r, n) = -gsgn(r, n); *SGN(q, n) = -gsgn(q, n); }
+                    copy_num(out, r, n); copy_num(out + E, q, n);
+                }
+            }
+    return 0;
+}

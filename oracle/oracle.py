@@ -72,6 +72,7 @@ class Oracle:
         lib.lfo_qr_pivoted.argtypes = [I, V, S, S, S, I, V, V, V, V, C.POINTER(C.c_size_t), C.POINTER(C.c_long)]
         lib.lfo_qr_apply.argtypes = [I, S, S, S, S, V, V, V, S, I]
         lib.lfo_qr_solve.argtypes = [I, S, S, S, C.POINTER(C.c_long), C.POINTER(C.c_size_t), V, V, V, V, S, V]
+        lib.lfo_exact_gemm4.argtypes = [I, I, S, S, S, S, I, I, V, V, V]
         lib.lfo_qr_complex.argtypes = [I, V, S, S, S, I, I, V, V, V, V, C.POINTER(C.c_size_t), C.POINTER(C.c_long)]
         lib.lfo_qr_complex_apply.argtypes = [I, S, S, S, S, V, V, V, S, I]
         lib.lfo_qr_complex_solve.argtypes = [I, S, S, S, C.POINTER(C.c_long), C.POINTER(C.c_size_t), V, V, V, V, S, V]
@@ -208,6 +209,15 @@ class Oracle:
         return X[:f["n"] * nrhs]
 
 
+    def exact_gemm4(self, bits, complex_, shape, A, B, C):
+        """The exact batched 4 x 4 product; shape: dict(count, stride_a, stride_b, stride_c, accumulate, negative).
+        Returns the new C."""
+        out = np.ascontiguousarray(C.copy())
+        assert self.lib.lfo_exact_gemm4(bits, int(complex_), shape["count"], shape["stride_a"], shape["stride_b"], shape["stride_c"],
+                                        int(shape.get("accumulate", False)), int(shape.get("negative", False)),
+                                        _ptr(np.ascontiguousarray(A)), _ptr(np.ascontiguousarray(B)), _ptr(out)) == 0
+        return out
+
     def qr_complex(self, bits, A, m, n, block=32, rank_bits=0, pivot=False):
         """Complex Householder QR of A (m * n complex elements, shape [m * n, 2, N + 3]); the factor dict as qr's."""
         w = bits // 32 + 3
@@ -336,6 +346,12 @@ class Mpfr:
         """Real components x [count, N+3] at from_bits, rounded to to_bits."""
         out = np.zeros((x.shape[0], to_bits // 32 + 3), dtype=np.uint32)
         assert self.lib.mpo_cast(from_bits, to_bits, _ptr(x), _ptr(out), x.shape[0]) == 0
+        return out
+
+    def dot(self, bits, c, subtract, a, sa, b, sb, K):
+        """RN(c -/+ sum_k a[k sa] b[k sb]) by mpfr_sum (c may be None)."""
+        out = np.zeros(bits // 32 + 3, dtype=np.uint32)
+        self.lib.mpo_dot(bits, _ptr(c), int(subtract), _ptr(a), sa, _ptr(b), sb, K, _ptr(out))
         return out
 
     def real(self, bits, op, a, b=None):

@@ -2,6 +2,7 @@
 // CommandBatch, Linalg, BatchedLinalg) compiles unchanged against include/limbforge/*.hpp and runs on
 // the GPU through liblimbforge_b200.so.  Prints one line per check; exit status 0 when all pass.
 #include "limbforge/batched_linalg.hpp"
+#include "limbforge/exact_gemm4.hpp"
 #include "limbforge/linalg.hpp"
 #include <cstdio>
 #include <cstring>
@@ -133,7 +134,7 @@ int main() {
                 QROptions qopt;
                 qopt.block = 1;
                 QRFactor qf = la.factor_qr(B, qa.data(), 3, 2, qopt);
-                std::vector<Float<B>> qb = {power<B>(1), power<B>(2), zero<B / 32>()}, qx(2);
+                std::vector<Float<B>> qb = {power<B>(1), power<B>(2), zero<B / 32>()}, qx(2), qb0 = qb;
                 qf.solve(qb.data(), 1, qx.data());
                 if (!qf.full_rank() || qf.rows() != 3 || qf.cols() != 2 || qf.info().reason != QRInfo::full_rank || qx[0].exponent != 0 ||
                     qx[1].exponent != 1) { std::printf("qr solve FAILED\n"); return 1; }
@@ -147,6 +148,16 @@ int main() {
                 if (!qg.empty() || qm.empty() || qm.pivoted() || qm.permutation()[1] != 1) { std::printf("qr move FAILED\n"); return 1; }
                 std::vector<Float<B>> dd(2, power<B>(0));
                 if (la.factor_qr_augmented(B, qa.data(), 3, 2, dd.data(), qopt).rows() != 5) { std::printf("augmented qr FAILED\n"); return 1; }
+                // complex: the same matrix with zero imaginary parts gives the real factor in the real parts
+                std::vector<Complex<B / 32>> ca(6), cb(3), cx(2);
+                for (int i = 0; i < 6; ++i) ca[i] = {qa[i], zero<B / 32>()};
+                for (int i = 0; i < 3; ++i) cb[i] = {qb0[i], zero<B / 32>()};
+                ComplexQRFactor cq = la.factor_qr_complex(B, ca.data(), 3, 2, qopt);
+                cq.solve(cb.data(), 1, cx.data());
+                if (!cq.full_rank() || cx[0].re.exponent != 0 || cx[1].re.exponent != 1 || cx[0].im.sign || cx[1].im.sign) {
+                    std::printf("complex qr FAILED\n"); return 1;
+                }
+                cq.apply_q(cb.data(), 1, true);
             }
             check_library_version();
             if (!version_compatible(library_version(), header_version) || std::string(library_version_string()).empty()) { std::printf("version FAILED\n"); return 1; }
@@ -176,6 +187,28 @@ int main() {
             }
         }
         std::printf("batched ok\n");
+        {   // exact 4x4: I * 2 = 2 everywhere; accumulated onto itself and negated: -4; resident form with a ticket
+            wolfnum::experimental::ExactGemm4 g(e);
+            std::vector<Float<B>> I4(16, zero<B / 32>()), T4(16, power<B>(1)), C4(16);
+            for (int i = 0; i < 4; ++i) I4[i * 5] = power<B>(0);
+            wolfnum::experimental::ExactGemm4Shape gs;
+            wolfnum::experimental::ExactGemm4Report gr;
+            g.gemm(B, false, gs, I4.data(), T4.data(), C4.data(), &gr);
+            gs.accumulate = gs.negative = true;
+            g.gemm(B, false, gs, I4.data(), T4.data(), C4.data());
+            for (auto& x : C4) if (x.exponent != 2 || x.sign != -1) { std::printf("exact gemm4 FAILED\n"); return 1; }
+            if (gr.gpu_components != 16 || gr.host_components) { std::printf("exact gemm4 report FAILED\n"); return 1; }
+            auto gA = e.make_buffer<Float<B>>(16), gB = e.make_buffer<Float<B>>(16), gC = e.make_buffer<Float<B>>(16);
+            gA.upload(I4.data(), 16); gB.upload(T4.data(), 16); gC.upload(C4.data(), 16);
+            auto gb = e.batch();
+            auto ticket = g.gemm(gb, gs, gA, gB, gC);                 // -(-4 + 2) = 2
+            if (ticket.resolved()) { std::printf("exact gemm4 ticket FAILED\n"); return 1; }
+            gb.submit().wait();
+            gC.download(C4.data(), 16);
+            for (auto& x : C4) if (x.exponent != 1 || x.sign != 1) { std::printf("resident exact gemm4 FAILED\n"); return 1; }
+            if (!ticket.resolved() || ticket.report().gpu_components != 16) { std::printf("exact gemm4 ticket FAILED\n"); return 1; }
+        }
+        std::printf("exact gemm4 ok\n");
         bool threw = false;
         try { e.run(100, Operation::add, a.data(), b.data(), out.data(), 1); } catch (const std::invalid_argument&) { threw = true; }
         if (!threw) { std::printf("error mapping FAILED\n"); return 1; }

@@ -65,3 +65,14 @@ def _dot2(oracle, bits, a, b, c, d, e):
     p = lambda v: np.ascontiguousarray(v).ctypes.data_as(C.c_void_p)
     oracle.lib.lfo_dot2_add(bits // 32, p(a), p(b), p(c), p(d), p(e), out.ctypes.data_as(C.c_void_p))
     return out
+
+
+def test_wide_clusters_stream_exactly(tmp_path):
+    """Exact sums whose clusters are wider than the accumulator window (tests/cpp/wide_sum.cpp): the streaming path of
+    cluster_round with the smallest window (8N + 4 words) gives the same bits as a window wide enough for every cluster,
+    at six widths, over chains of products spaced below the cluster gap, exact cancellations, ties and far terms."""
+    exe = str(tmp_path / "wide_sum")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", f"-I{os.path.join(ROOT, 'include')}",
+                    os.path.join(ROOT, "tests", "cpp", "wide_sum.cpp"), "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "mismatches 0" in r.stdout, r.stdout + r.stderr

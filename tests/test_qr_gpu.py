@@ -238,3 +238,80 @@ def test_qr_pivoted_fixtures(la, oracle):
             if label == "nearly parallel columns":
                 assert qr.info.norm_recomputations > 0
             check_solves(qr, want, oracle, qc.rhs(bits, m, 3, rng), 3, f"{label} block {block}")
+
+
+# ---- complex QR (linalg_complex.mm): the factor, least squares and Q / Q^H against the oracle's complex sequence
+def check_cfactor(qr, want, label):
+    assert qr.complex
+    assert (qr.info.rank, qr.info.reason, qr.info.status) == (want["rank"], want["reason"], want["status"]), label
+    for k, got in (("R", qr.r()), ("V", qr.v()), ("tau", qr.tau()), ("T", qr.t())):
+        w = want[k]
+        assert got.shape == w.shape and (got == w).all(), f"{label}: {k} differs at {bad(got.reshape(got.shape[0], -1), w.reshape(w.shape[0], -1))}"
+
+
+def check_csolves(qr, want, oracle, B, nrhs, label):
+    X = qr.solve(B, nrhs)
+    assert (X == oracle.qr_complex_solve(want, B, nrhs)).all(), f"{label}: solve"
+    for adj in (True, False):
+        C = B.copy()
+        qr.apply_q(C, nrhs, adj)
+        assert (C == oracle.qr_complex_apply(want, B, nrhs, adj)).all(), f"{label}: apply {'Q^H' if adj else 'Q'}"
+
+
+@pytest.mark.parametrize("bits", [64, 256, 416])
+def test_qr_complex_vs_oracle(la, oracle, bits):
+    rng = np.random.default_rng(600 + bits)
+    for i, (m, n, kind) in enumerate([(1, 1, "moderate"), (3, 2, "qsc"), (33, 7, "graded"), (40, 21, "wide"), (50, 24, "spread"),
+                                      (30, 17, "triangular"), (41, 7, "dependent")]):
+        A = qc.complex_matrix(bits, m, n, kind, rng)
+        for block in (16, 5, 0):
+            want = oracle.qr_complex(bits, A, m, n, block)
+            qr = la.factor_qr_complex(bits, A, m, n, opts(block))
+            label = f"complex bits={bits} {kind} {m}x{n} block {block}"
+            check_cfactor(qr, want, label)
+            nrhs = (1, 2, 3)[(i + block) % 3]
+            B = qc.complex_rhs(bits, m, nrhs, rng)
+            if block == 5 and m > 3:
+                B[nrhs + 1, 1, -1] = nb.INVALID
+            check_csolves(qr, want, oracle, B, nrhs, label)
+
+
+def test_qr_complex_special_cases(la, oracle):
+    bits = 256
+    N = bits // 32
+    rng = np.random.default_rng(61)
+    cases = []
+    A = qc.complex_matrix(bits, 20, 9, "moderate", rng)
+    A[3::9] = 0
+    cases.append(("zero column 3", A, 20, 9, 0))
+    A = qc.complex_matrix(bits, 25, 10, "moderate", rng)
+    A[7 * 10 + 4, 1, N + 2] = nb.INVALID
+    cases.append(("status at (7,4)", A, 25, 10, 0))
+    cases.append(("dependent, rank_bits", qc.complex_matrix(bits, 41, 7, "dependent", rng), 41, 7, bits // 2))
+    A = qc.complex_matrix(bits, 6, 3, "moderate", rng)
+    A[0::3] = 0
+    A[0, 1] = nb.power(bits, 3)[0]
+    cases.append(("imaginary diagonal, zero below", A, 6, 3, 0))
+    w = bits // 32 + 3
+    R = qc.matrix(bits, 30, 12, "qsc", rng)
+    A = np.zeros((30 * 12, 2, w), np.uint32)
+    A[:, 0] = R
+    cases.append(("real input", A, 30, 12, 0))
+    for label, A, m, n, rank_bits in cases:
+        for block in (4, 16):
+            want = oracle.qr_complex(bits, A, m, n, block, rank_bits)
+            qr = la.factor_qr_complex(bits, A, m, n, opts(block, rank_bits))
+            check_cfactor(qr, want, f"{label} block {block}")
+            check_csolves(qr, want, oracle, qc.complex_rhs(bits, m, 2, rng), 2, f"{label} block {block}")
+    # the real input gives the real factor in the real parts
+    real = la.factor_qr(bits, R, 30, 12, opts(4))
+    cq = la.factor_qr_complex(bits, cases[-1][1], 30, 12, opts(4))
+    assert (cq.r()[:, 0] == real.r()).all() and (cq.r()[:, 1] == 0).all()
+
+
+def test_qr_complex_pivot_not_built(la):
+    from limbforge_b200 import api
+    bits = 256
+    A = np.zeros((12, 2, bits // 32 + 3), np.uint32)
+    with pytest.raises(api.RuntimeFailure):
+        la.factor_qr_complex(bits, A, 4, 3, opts(8, pivot=True))

@@ -47,6 +47,55 @@ def _rank(rank, world, port, out):
         dist.destroy_process_group()
 
 
+def _gemm_rank(rank, world, port, out):
+    from oracle.oracle import Oracle
+    from limbforge_b200 import numbers as nb
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        orc = Oracle()
+        rng = np.random.default_rng(21)
+        bits, m, n, k = 128, 37, 9, 11
+        A = nb.random_numbers(rng, k * m, bits, 40)
+        B = nb.random_numbers(rng, k * n, bits, 40)
+        C = nb.random_numbers(rng, m * n, bits, 40)
+
+        def gemm(bits_, ta, a, b, rows, n_, k_, c, sub):      # the per-rank product (Linalg.gemm on a GPU)
+            c[:] = orc.gemm(bits_, ta, a, b, rows, n_, k_, c, sub)
+        got = shard.sharded_exact_gemm(gemm, bits, True, A, B, m, n, k, C, True, dist, align=8)
+        got2 = shard.sharded_exact_gemm(gemm, bits, False, A, B, m, n, k, None, False, dist, align=8)
+        out.put((rank, got, got2))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_sharded_exact_gemm():
+    """Row blocks of an exact product on two ranks, all-gathered, equal the whole product bit for bit."""
+    from oracle.oracle import Oracle
+    from limbforge_b200 import numbers as nb
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gemm_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    results = [q.get(timeout=180) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    orc = Oracle()
+    rng = np.random.default_rng(21)
+    bits, m, n, k = 128, 37, 9, 11
+    A = nb.random_numbers(rng, k * m, bits, 40)
+    B = nb.random_numbers(rng, k * n, bits, 40)
+    C = nb.random_numbers(rng, m * n, bits, 40)
+    want = orc.gemm(bits, True, A, B, m, n, k, C, True)
+    want2 = orc.gemm(bits, False, A, B, m, n, k)
+    for _, got, got2 in results:
+        assert (got == want).all() and (got2 == want2).all()
+    assert shard.gemm_row_block(37, 0, 2, 8) == (0, 24) and shard.gemm_row_block(37, 1, 2, 8) == (24, 37)
+
+
 def test_two_gloo_ranks_partition_and_max():
     world, port = 2, _free_port()
     ctx = mp.get_context("spawn")
