@@ -1002,21 +1002,21 @@ template <class Src> LFD_FN bool stream_next(const Src& src, i64 cutoff, StreamP
 // pos <- |pos - neg|, neg <- 0; returns the sign of pos - neg before (0 when equal).
 template <int CW> LFD_FN int stream_normalize(u32* pos, u32* neg) {
     int cmp = 0;
-    for (int w = CW - 1; w >= 0 && !cmp; --w) if (pos[w] != neg[w]) cmp = pos[w] > neg[w] ? 1 : -1;
-    if (cmp < 0) for (int w = 0; w < CW; ++w) { const u32 t = pos[w]; pos[w] = neg[w]; neg[w] = t; }
+    LFD_NOUNROLL for (int w = CW - 1; w >= 0 && !cmp; --w) if (pos[w] != neg[w]) cmp = pos[w] > neg[w] ? 1 : -1;
+    if (cmp < 0) { LFD_NOUNROLL for (int w = 0; w < CW; ++w) { const u32 t = pos[w]; pos[w] = neg[w]; neg[w] = t; } }
     u32 bo = 0;
-    for (int w = 0; w < CW; ++w) { const u64 d = (u64)neg[w] + bo; const u32 o = pos[w]; pos[w] = (u32)((u64)o - d); bo = (u64)o < d; neg[w] = 0; }
+    LFD_NOUNROLL for (int w = 0; w < CW; ++w) { const u64 d = (u64)neg[w] + bo; const u32 o = pos[w]; pos[w] = (u32)((u64)o - d); bo = (u64)o < d; neg[w] = 0; }
     return cmp;
 }
 // Index of the highest set bit of x (CW words), -1 when zero.
 template <int CW> LFD_FN int stream_msb(const u32* x) {
-    for (int w = CW - 1; w >= 0; --w) if (x[w]) return 32 * w + 31 - lf_clz(x[w]);
+    LFD_NOUNROLL for (int w = CW - 1; w >= 0; --w) if (x[w]) return 32 * w + 31 - lf_clz(x[w]);
     return -1;
 }
 // x <- x * 2^d (d >= 0), words shifted out at the top dropped (the caller guarantees they are zero).
 template <int CW> LFD_FN void stream_shift_up(u32* x, i64 d) {
     const int q = (int)(d >> 5), r = (int)(d & 31);
-    for (int w = CW - 1; w >= 0; --w) {
+    LFD_NOUNROLL for (int w = CW - 1; w >= 0; --w) {
         const int a = w - q;
         u32 v = a >= 0 ? x[a] << r : 0u;
         if (r && a - 1 >= 0) v |= x[a - 1] >> (32 - r);
@@ -1028,7 +1028,7 @@ template <int CW> struct StreamWin { u32 pos[CW], neg[CW]; i64 A; };
 // Adds the terms after `at` (in order) until they run out (returns true) or one no longer fits while the partial sum
 // is too large to move the window (returns false with that term pending in `at`, its data in scale/top/sign).
 // mult flips every term's sign (-1).  logc: ceil(log2(terms + 2)).
-template <int CW, class Src> LFD_FN bool stream_run(const Src& src, i64 cutoff, int mult, int logc, StreamWin<CW>& W, StreamPos& at,
+template <int CW, class Src> LFD_FN LFD_NOINLINE bool stream_run(const Src& src, i64 cutoff, int mult, int logc, StreamWin<CW>& W, StreamPos& at,
                                                     i64& scale, i64& top, int& sign) {
     for (;;) {
         StreamPos nx = at;
@@ -1043,12 +1043,12 @@ template <int CW, class Src> LFD_FN bool stream_run(const Src& src, i64 cutoff, 
                 const i64 m = bottom + h;                                 // highest set bit of |partial|
                 const i64 A2 = (m + 2 > top + logc + 2) ? m + 2 : top + logc + 2;
                 if (A2 - 32 * (i64)CW > scale) {                          // the partial sum dominates the rest
-                    if (sg < 0) for (int w = 0; w < CW; ++w) { W.neg[w] = W.pos[w]; W.pos[w] = 0; }
+                    if (sg < 0) { LFD_NOUNROLL for (int w = 0; w < CW; ++w) { W.neg[w] = W.pos[w]; W.pos[w] = 0; } }
                     at = nx;
                     return false;
                 }
                 stream_shift_up<CW>(W.pos, W.A - A2);
-                if (sg < 0) for (int w = 0; w < CW; ++w) { W.neg[w] = W.pos[w]; W.pos[w] = 0; }
+                if (sg < 0) { LFD_NOUNROLL for (int w = 0; w < CW; ++w) { W.neg[w] = W.pos[w]; W.pos[w] = 0; } }
                 W.A = A2;
             }
             bottom = W.A - 32 * (i64)CW;
@@ -1059,12 +1059,12 @@ template <int CW, class Src> LFD_FN bool stream_run(const Src& src, i64 cutoff, 
 }
 // Sign of X * 2^xscale * xsign + mult * (the terms after `at`, and the term at `at` itself when pending), exactly.
 // X: xw words (nullptr when absent).
-template <int CW, class Src> LFD_FN int stream_sign(const Src& src, i64 cutoff, StreamPos at, bool pending, int mult, int logc,
+template <int CW, class Src> LFD_FN LFD_NOINLINE int stream_sign(const Src& src, i64 cutoff, StreamPos at, bool pending, int mult, int logc,
                                                     const u32* X, int xw, i64 xscale, int xsign) {
     StreamWin<CW> W;
-    for (int w = 0; w < CW; ++w) { W.pos[w] = 0; W.neg[w] = 0; }
+    LFD_NOUNROLL for (int w = 0; w < CW; ++w) { W.pos[w] = 0; W.neg[w] = 0; }
     i64 xt = INT64_MIN;                                                   // X's highest bit + 1
-    for (int w = xw - 1; w >= 0; --w) if (X[w]) { xt = xscale + 32 * w + 32 - lf_clz(X[w]); break; }
+    LFD_NOUNROLL for (int w = xw - 1; w >= 0; --w) if (X[w]) { xt = xscale + 32 * w + 32 - lf_clz(X[w]); break; }
     i64 s0 = 0, t0 = INT64_MIN; int g0 = 0;
     if (pending) src.term(at.k, s0, t0, g0);
     const i64 top = xt > t0 ? xt : t0;
@@ -1080,9 +1080,9 @@ template <int CW, class Src> LFD_FN int stream_sign(const Src& src, i64 cutoff, 
 // S is split at bit k = (pending top) + logc + 3 into S_hi (a multiple of 2^k) and S_lo < 2^k; with the tail t (all
 // later terms, |t| < 2^(k - 2)) the rounding of S + t is that of S_hi + carry 2^k plus the sign of the remainder in
 // [0, 2^k), and carry and remainder follow from the exact signs of S_lo + t and S_lo + t - 2^k.
-template <int N, int CW, class Src> LFD_FN Num<N> stream_value(const Src& src, i64 cutoff, int logc) {
+template <int N, int CW, class Src> LFD_FN LFD_NOINLINE Num<N> stream_value(const Src& src, i64 cutoff, int logc) {
     StreamWin<CW> W;
-    for (int w = 0; w < CW; ++w) { W.pos[w] = 0; W.neg[w] = 0; }
+    LFD_NOUNROLL for (int w = 0; w < CW; ++w) { W.pos[w] = 0; W.neg[w] = 0; }
     StreamPos at{0, 0, false};
     W.A = cutoff + logc + 2;
     i64 sc, tp; int sg;
@@ -1097,9 +1097,9 @@ template <int N, int CW, class Src> LFD_FN Num<N> stream_value(const Src& src, i
     }
     const i64 k = tp + logc + 3;                                          // S_lo = |S| mod 2^k
     u32 lo[CW];
-    for (int w = 0; w < CW; ++w) lo[w] = 0;
+    LFD_NOUNROLL for (int w = 0; w < CW; ++w) lo[w] = 0;
     const i64 kb = k - bottom;                                            // bit index of k in the window (> 0)
-    for (int w = 0; w < CW; ++w) {
+    LFD_NOUNROLL for (int w = 0; w < CW; ++w) {
         const i64 b0 = 32 * (i64)w;
         if (b0 + 32 <= kb) { lo[w] = W.pos[w]; W.pos[w] = 0; }
         else if (b0 < kb) { const u32 mask = (1u << (kb - b0)) - 1u; lo[w] = W.pos[w] & mask; W.pos[w] &= ~mask; }
@@ -1112,10 +1112,10 @@ template <int N, int CW, class Src> LFD_FN Num<N> stream_value(const Src& src, i
         sigma = c0;
     } else {
         u32 hk[CW];                                                       // 2^k - S_lo
-        for (int w = 0; w < CW; ++w) hk[w] = 0;
+        LFD_NOUNROLL for (int w = 0; w < CW; ++w) hk[w] = 0;
         if (kb < 32 * (i64)CW) hk[kb >> 5] = 1u << (kb & 31);
         u32 bo = 0;
-        for (int w = 0; w < CW; ++w) { const u64 d = (u64)lo[w] + bo; const u32 o = hk[w]; hk[w] = (u32)((u64)o - d); bo = (u64)o < d; }
+        LFD_NOUNROLL for (int w = 0; w < CW; ++w) { const u64 d = (u64)lo[w] + bo; const u32 o = hk[w]; hk[w] = (u32)((u64)o - d); bo = (u64)o < d; }
         const int c1 = stream_sign<CW>(src, cutoff, at, true, ssign, logc, hk, CW, bottom, -1);
         if (c0 < 0) { carry = -1; sigma = 1; }
         else if (c0 == 0) { carry = 0; sigma = 0; }
@@ -1126,7 +1126,7 @@ template <int N, int CW, class Src> LFD_FN Num<N> stream_value(const Src& src, i
     if (carry) {                                                          // S_hi +- 2^k (S_hi >> 2^k: no sign change)
         u32 one[1] = {1u};
         if (carry > 0) acc_add(W.pos, CW, one, 1, kb);
-        else { for (int w = 0; w < CW; ++w) W.neg[w] = 0; acc_add(W.neg, CW, one, 1, kb); stream_normalize<CW>(W.pos, W.neg); }
+        else { LFD_NOUNROLL for (int w = 0; w < CW; ++w) W.neg[w] = 0; acc_add(W.neg, CW, one, 1, kb); stream_normalize<CW>(W.pos, W.neg); }
     }
     Rounded<N> R;
     round_info<N>(W.pos, CW, bottom, R);

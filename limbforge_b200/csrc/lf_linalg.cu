@@ -800,6 +800,7 @@ static lf_qr_info qr_device(Linalg& la, int bits, uint32_t* Wk, size_t m, size_t
             if (c) qk->update(P, c, s);
             qk->reflect(P, c, s);
             qk->dots(P, c, s);
+            qk->tcol(P, c, s);
         }
         qk->store(P, s);
         cuda_check(cudaGetLastError(), "qr panel");

@@ -3,11 +3,10 @@
 // and D(c; x, y) = RN(c - sum x_k y_k) with one rounding each.
 //
 // A panel of kb columns starting at column k0 is copied column-contiguous (Pt: entry (c, r) at c * mr + r,
-// mr = m - k0 rows), its reflectors are built in Vt with the same layout, and every column step runs as three
+// mr = m - k0 rows), its reflectors are built in Vt with the same layout, and every column step runs as four
 // launches with no host round trip: the rows of the column reduced by the panel's earlier reflectors (one warp
-// per row), the reflector (one block: the squared norm, sqrt, the scaled reflector and tau), then the panel W
-// row and Gram column (one block per dot) whose last block to arrive writes the T column and the next column's
-// y.  Failures (zero, small or status columns) are recorded in a device-side state that the following launches
+// per row), the reflector (one block: the squared norm, sqrt, the scaled reflector and tau), the panel W row and
+// Gram column (one block per dot), then one block that writes the T column and the next column's y.  Failures (zero, small or status columns) are recorded in a device-side state that the following launches
 // and the host read; the trailing matrix is updated by the compact-WY products on the exact GEMM engine.
 #pragma once
 #include "lf_linalg.cuh"
@@ -266,35 +265,33 @@ template <int N> __global__ void __launch_bounds__(kQrThreads) qr_reflect_kernel
 }
 
 // After reflector c: block u < c gives G[u] = P(v_u, v_c), block u >= c the W row entry Wp[c][u+1] = P(v_c,
-// a_{u+1}) (the block-start column), both over rows [c, mr).  The last block to finish writes the T column,
-// T_lc = -RN(tau * P(T[l][l..c), G[l..c))) (linalg.mm:713), and the next column's y_i = P(T[0..i][i],
-// Wp[0..i][c+1]) for i < min(j + 1, rank) - k0 (linalg.mm:668), one warp per entry.  kb - 1 blocks.
+// a_{u+1}) (the block-start column), both over rows [c, mr) (linalg.mm:636-645).  kb - 1 blocks.
 template <int N> __global__ void __launch_bounds__(kQrThreads) qr_dots_kernel(QrPanel p, u64 c) {
     __shared__ __align__(16) u32 sm[qr_dot_words<N>()];
-    __shared__ int s_last;
     constexpr u64 E = N + 3;
     QrState* st = p.st;
     const long long rank = st->rank;
     const bool reflected = rank == (long long)p.n;
-    const u64 j = p.k0 + c, len = p.mr - c, u = blockIdx.x;
+    const u64 len = p.mr - c, u = blockIdx.x;
     if (reflected && u + 1 < p.kb) {
         const u32* v = p.Vt + (c * p.mr + c) * E;
         const Num<N> d = u < c ? block_exact_dot<N, true>(p.Vt + (u * p.mr + c) * E, 1, v, 1, len, sm, p.error)
                                : block_exact_dot<N, true>(v, 1, p.Pt + ((u + 1) * p.mr + c) * E, 1, len, sm, p.error);
         if (threadIdx.x == 0) store<N>(u < c ? p.G + u * E : p.Wp + (c * p.nb + u + 1) * E, d);
     }
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const u32 before = atomicAdd(&st->arrivals, 1u);
-        s_last = before == gridDim.x - 1;
-        if (s_last) st->arrivals = 0;
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
+}
+// T column c, T_lc = -RN(tau * P(T[l][l..c), G[l..c))) (linalg.mm:713), then the next column's y_i = P(T[0..i][i],
+// Wp[0..i][c+1]) for i < min(j + 1, rank) - k0 (linalg.mm:668): one warp per entry, 16 warps (a 32-column block's
+// entries in two rounds).  One block, after the dots kernel.
+constexpr int kQrTcolThreads = 512;
+template <int N> __global__ void __launch_bounds__(kQrTcolThreads) qr_tcol_kernel(QrPanel p, u64 c) {
+    constexpr u64 E = N + 3;
+    const long long rank = p.st->rank;
+    const bool reflected = rank == (long long)p.n;
+    const u64 j = p.k0 + c;
     u32* Tb = p.T + (p.k0 / p.nb) * p.nb * p.nb * E;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int WARPS = kQrThreads / 32;
+    constexpr int WARPS = kQrTcolThreads / 32;
     if (reflected) {
         const Num<N> tj = ldn<N, false>(p.tau + j * E);
         for (u64 l = warp; l < c; l += WARPS) {
@@ -527,6 +524,7 @@ struct QrKernels {
     void (*update)(const QrPanel&, u64 c, cudaStream_t);
     void (*reflect)(const QrPanel&, u64 c, cudaStream_t);
     void (*dots)(const QrPanel&, u64 c, cudaStream_t);
+    void (*tcol)(const QrPanel&, u64 c, cudaStream_t);
     void (*store)(const QrPanel&, cudaStream_t);
     void (*extract)(const u32* Wk, u32* R, u64 n, const QrState* st, cudaStream_t);
     void (*copy)(const u32* src, u64 ld_src, u32* dst, u64 ld_dst, u64 rows, u64 cols, cudaStream_t);
@@ -553,6 +551,9 @@ template <int N> void qr_update_launch(const QrPanel& p, u64 c, cudaStream_t s) 
 template <int N> void qr_reflect_launch(const QrPanel& p, u64 c, cudaStream_t s) { qr_reflect_kernel<N><<<1, kQrThreads, 0, s>>>(p, c); }
 template <int N> void qr_dots_launch(const QrPanel& p, u64 c, cudaStream_t s) {
     if (p.kb > 1) qr_dots_kernel<N><<<(unsigned)(p.kb - 1), kQrThreads, 0, s>>>(p, c);
+}
+template <int N> void qr_tcol_launch(const QrPanel& p, u64 c, cudaStream_t s) {
+    if (p.kb > 1) qr_tcol_kernel<N><<<1, kQrTcolThreads, 0, s>>>(p, c);
 }
 template <int N> void qr_extract_launch(const u32* Wk, u32* R, u64 n, const QrState* st, cudaStream_t s) {
     if (n) qr_extract_kernel<N><<<qr_grid(n * n, 128), 128, 0, s>>>(Wk, R, n, st);
@@ -587,7 +588,7 @@ template <int N> void qrp_recompute_launch(const QrPanel& p, u64 c, cudaStream_t
     namespace lfd {                                                                                                 \
     extern const QrKernels qr_kernels_##N;                                                                          \
     const QrKernels qr_kernels_##N = {qr_load_launch<N>, qr_update_launch<N>, qr_reflect_launch<N>, qr_dots_launch<N>, \
-                                      qr_store_launch<N>, qr_extract_launch<N>, qr_copy_launch<N>, qrp_norms_launch<N>,  \
+                                      qr_tcol_launch<N>, qr_store_launch<N>, qr_extract_launch<N>, qr_copy_launch<N>, qrp_norms_launch<N>,  \
                                       qrp_pivot_launch<N>, qrp_column_launch<N>, qrp_gramw_launch<N>,                   \
                                       qrp_trailing_launch<N>, qrp_recompute_launch<N>};                                 \
     }
