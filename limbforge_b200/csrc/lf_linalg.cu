@@ -1064,6 +1064,117 @@ static lf_qr_info cqr_device(Linalg& la, int bits, uint32_t* Wk, size_t m, size_
     return info;
 }
 
+// Column-pivoted complex QR (linalg_complex.mm:136-139, 160-290): per column step the pivot choice and swap, the
+// column's reduction with its Y rows, the reflector, the Gram entries with the W rows of every trailing column and
+// the T column, the Y rows with the downdated norms, and recomputation of collapsed norms; after each panel the
+// trailing matrix is updated with the panel's Y rows (X = D(X; EV_b, Y)).  No look-ahead, as in the reference.  After
+// a failing column p in block b, block b (formed afresh) is applied to the columns [p, n) and the factorization stops.
+static lf_qr_info cqr_device_pivoted(Linalg& la, int bits, uint32_t* Wk, size_t m, size_t n, size_t nb, int rank_bits, uint32_t* V,
+                                     uint32_t* T, uint32_t* tau, uint32_t* R, uint32_t* EV, uint32_t* ET, uint32_t* ER, size_t* perm_out) {
+    lf_qr_info info{};
+    info.rank = n;
+    auto w0 = Clock::now();
+    Engine& e = *la.engine;
+    cudaStream_t s = e.stream;
+    const int limbs = bits / 32;
+    const size_t E = limbs + 3, eb = E * 4, cb = 2 * eb;
+    const auto* ck = lfd::cqr_kernels(limbs);
+    const auto* qk = lfd::qr_kernels(limbs);
+    const size_t blocks = nb ? (n + nb - 1) / nb : 0;
+    cuda_check(cudaMemsetAsync(V, 0, m * n * cb, s), "memset");
+    cuda_check(cudaMemsetAsync(T, 0, blocks * nb * nb * cb, s), "memset");
+    cuda_check(cudaMemsetAsync(tau, 0, n * cb, s), "memset");
+    cuda_check(cudaMemsetAsync(EV, 0, 4 * m * n * eb, s), "memset");
+    cuda_check(cudaMemsetAsync(ET, 0, 4 * blocks * nb * nb * eb, s), "memset");
+    uint32_t* Wb = static_cast<uint32_t*>(la.qr[0].get(2 * nb * n * eb + 16));
+    uint32_t* Yb = static_cast<uint32_t*>(la.qr[1].get(2 * nb * n * eb + 16));
+    cuda_check(cudaMemsetAsync(Wb, 0, 2 * nb * n * eb, s), "memset");
+    cuda_check(cudaMemsetAsync(Yb, 0, 2 * nb * n * eb, s), "memset");
+    uint32_t* Pt = static_cast<uint32_t*>(la.qr[2].get(4 * nb * m * cb + 16));       // Pt, Vt, Vi, Vr
+    uint32_t* Vt = Pt + nb * m * 2 * E;
+    uint32_t* Vi = Vt + nb * m * 2 * E;
+    uint32_t* Vr = Vi + nb * m * 2 * E;
+    uint32_t* Wp = static_cast<uint32_t*>(la.qr[4].get((nb * nb + 6 * nb) * cb + 3 * nb * nb * cb + 16));
+    uint32_t* G = Wp + nb * nb * 2 * E;
+    uint32_t* Gc = G + nb * 2 * E;
+    uint32_t* Gic = Gc + nb * 2 * E;
+    uint32_t* Vrc = static_cast<uint32_t*>(la.qr[6].get((2 * nb * m + 2 * nb) * cb + 16));   // Vrc, Vri, tc
+    uint32_t* Vri = Vrc + nb * m * 2 * E;
+    uint32_t* tc = Vri + nb * m * 2 * E;
+    auto* st = static_cast<lfd::QrState*>(la.qr[7].get(sizeof(lfd::QrState)));
+    uint32_t* nu = static_cast<uint32_t*>(la.qr[11].get(2 * n * eb + 16));
+    auto* perm = static_cast<uint64_t*>(la.qr[12].get(n * 12 + 16));
+    uint32_t* flag = reinterpret_cast<uint32_t*>(perm + n);
+    cuda_check(cudaMemsetAsync(flag, 0, n * 4, s), "memset");
+    lfd::QrState host{};
+    host.rank = (long long)n;
+    cuda_check(cudaMemcpyAsync(st, &host, sizeof host, cudaMemcpyHostToDevice, s), "state");
+    uint32_t* err = static_cast<uint32_t*>(la.error_buf.get(16));
+    cuda_check(cudaMemsetAsync(err, 0, 16, s), "memset");
+    const ProductLane lane = main_lane(la);
+    cudaEvent_t g0, g1;
+    cuda_check(cudaEventCreate(&g0), "event"); cuda_check(cudaEventCreate(&g1), "event");
+    cuda_check(cudaEventRecord(g0, s), "event");
+    // squared norms over the 2m split rows: the real kernel on the split matrix
+    lfd::QrPanel Q{};
+    Q.Wk = Wk; Q.m = 2 * m; Q.n = n; Q.st = st; Q.error = err; Q.pivot = 1; Q.nu = nu; Q.nuref = nu + n * E; Q.perm = perm;
+    qk->norms(Q, s);
+    lfd::CqrPanel P{Wk, m, n, V, T, tau, EV, ET, Pt, Vt, Vi, Vr, Wp, G, Gc, Gic, nullptr, nullptr, nullptr, 0, 0, nb, 0, rank_bits, st, err,
+                    1, Wb, Yb, nu, nu + n * E, perm, flag, Vrc, Vri, tc};
+    for (size_t k0 = 0; k0 < n; k0 += nb) {
+        const size_t k1 = std::min(n, k0 + nb), b = k0 / nb;
+        auto t = Clock::now();
+        P.k0 = k0; P.kb = k1 - k0; P.mr = m - k0;
+        ck->load(P, s);
+        for (size_t c = 0; c < P.kb; ++c) {
+            ck->pivot(P, c, s);
+            ck->column(P, c, s);
+            ck->reflect(P, c, s);
+            ck->gramw(P, c, s);
+            ck->trailing(P, c, s);
+            ck->recompute(P, c, s);
+        }
+        ck->store(P, s);
+        cuda_check(cudaGetLastError(), "pivoted complex qr panel");
+        cuda_check(cudaMemcpyAsync(&host, st, sizeof host, cudaMemcpyDeviceToHost, s), "state");
+        cuda_check(cudaStreamSynchronize(s), "pivoted complex qr panel");
+        ++info.blocks;
+        info.panel_seconds += since(t);
+        t = Clock::now();
+        const size_t p = std::min(k1, (size_t)host.rank);
+        if (p < k1) {
+            if (p > k0) {
+                qr_block_update(la, lane, bits, EV, ET, 2 * m, 2 * n, 2 * nb, b, Wk, n, p, n, true, Wb, Yb, false, s);
+                ++info.gpu_updates;
+            }
+            info.update_seconds += since(t);
+            break;
+        }
+        if (k1 < n) {
+            qr_block_update(la, lane, bits, EV, ET, 2 * m, 2 * n, 2 * nb, b, Wk, n, k1, n, true, Wb, Yb, true, s);
+            ++info.gpu_updates;
+        }
+        info.update_seconds += since(t);
+    }
+    ck->extract(Wk, R, ER, n, st, s);
+    cuda_check(cudaGetLastError(), "complex qr extract");
+    cuda_check(cudaEventRecord(g1, s), "event");
+    uint32_t ev[3] = {0, 0, 0};
+    std::vector<uint64_t> pm(n);
+    cuda_check(cudaMemcpyAsync(&host, st, sizeof host, cudaMemcpyDeviceToHost, s), "state");
+    cuda_check(cudaMemcpyAsync(ev, err, 12, cudaMemcpyDeviceToHost, s), "error flag");
+    if (n) cuda_check(cudaMemcpyAsync(pm.data(), perm, n * 8, cudaMemcpyDeviceToHost, s), "permutation");
+    cuda_check(cudaStreamSynchronize(s), "pivoted complex qr");
+    float ms = 0; cudaEventElapsedTime(&ms, g0, g1);
+    cudaEventDestroy(g0); cudaEventDestroy(g1);
+    if (ev[0] | ev[1] | ev[2]) throw runtime_error("exact product: a device error word was set (a bounded wait gave up)");
+    for (size_t k = 0; k < n; ++k) perm_out[k] = (size_t)pm[k];
+    info.rank = (size_t)host.rank; info.reason = host.reason; info.status = host.status;
+    info.norm_recomputations = host.recomputed;
+    info.timing = {ms * 1e-3, since(w0)};
+    return info;
+}
+
 // C (device, m x nrhs) <- Q^T C (qt: blocks in order) or Q C (blocks in reverse) over the blocks holding reflectors
 // [0, rank) (qr_apply_n, linalg.mm:750-766).  Returns the device seconds.
 static double qr_apply_device(Linalg& la, const QrFactor& f, uint32_t* C, size_t nrhs, bool qt) {
@@ -1357,8 +1468,8 @@ int lf_qr_apply_q(const lf_qr* f, void* B, size_t nrhs, int transpose, lf_timing
 }
 
 // Linalg::factor_qr_complex (linalg.hpp:170): complex Householder QR of A (m x n Complex<bits/32>, row-major, m >= n);
-// the factor's arrays are complex and its solve and apply_q take complex matrices.  Column pivoting of complex factors
-// is not built.
+// the factor's arrays are complex and its solve and apply_q take complex matrices; with pivoting, column j of the
+// factor is column perm[j] of A.
 int lf_linalg_factor_qr_complex(lf_linalg* la, int bits, const void* A, size_t m, size_t n, const lf_qr_options* o, lf_qr** out) {
     LF_API_BEGIN
     if (!out) throw invalid_argument("null output");
@@ -1370,9 +1481,8 @@ int lf_linalg_factor_qr_complex(lf_linalg* la, int bits, const void* A, size_t m
     if (m * n && !A) throw invalid_argument("null matrix");
     const lf_qr_options opts = o ? *o : lf_qr_options{32, 0, 0, 1, 0, 0};
     if (opts.rank_bits < 0) throw invalid_argument("factor_qr_complex: rank_bits >= 0");
-    if (opts.pivot) throw runtime_error("factor_qr_complex: column pivoting of complex factors is not built");
     std::unique_ptr<lf_qr> f(new lf_qr());
-    f->owner = la; f->bits = bits; f->m = m; f->n = n; f->cplx = true;
+    f->owner = la; f->bits = bits; f->m = m; f->n = n; f->cplx = true; f->pivot = opts.pivot != 0;
     f->block = opts.block; f->nb = opts.block ? std::min(opts.block, n) : n;
     const size_t eb = size_t(bits / 8 + 12), E = eb / 4, cb = 2 * eb;
     const size_t blocks = f->nb ? (n + f->nb - 1) / f->nb : 0;
@@ -1398,7 +1508,8 @@ int lf_linalg_factor_qr_complex(lf_linalg* la, int bits, const void* A, size_t m
         uint32_t* EV = static_cast<uint32_t*>(f->dV.get(4 * m * n * eb));
         uint32_t* ET = static_cast<uint32_t*>(f->dT.get(4 * blocks * f->nb * f->nb * eb + 16));
         uint32_t* ER = static_cast<uint32_t*>(f->dR.get(4 * n * n * eb));
-        f->info = cqr_device(*la, bits, Wk, m, n, f->nb, opts.rank_bits, V, T, tau, R, EV, ET, ER);
+        f->info = f->pivot ? cqr_device_pivoted(*la, bits, Wk, m, n, f->nb, opts.rank_bits, V, T, tau, R, EV, ET, ER, f->perm.data())
+                           : cqr_device(*la, bits, Wk, m, n, f->nb, opts.rank_bits, V, T, tau, R, EV, ET, ER);
         cuda_check(cudaMemcpyAsync(f->R.data(), R, n * n * cb, cudaMemcpyDeviceToHost, s), "download");
         cuda_check(cudaMemcpyAsync(f->V.data(), V, m * n * cb, cudaMemcpyDeviceToHost, s), "download");
         if (blocks) cuda_check(cudaMemcpyAsync(f->T.data(), T, blocks * f->nb * f->nb * cb, cudaMemcpyDeviceToHost, s), "download");

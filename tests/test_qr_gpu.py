@@ -309,9 +309,65 @@ def test_qr_complex_special_cases(la, oracle):
     assert (cq.r()[:, 0] == real.r()).all() and (cq.r()[:, 1] == 0).all()
 
 
-def test_qr_complex_pivot_not_built(la):
-    from limbforge_b200 import api
+def check_cpivot(qr, want, label):
+    assert qr.pivoted and qr.permutation() == want["perm"], f"{label}: permutation {qr.permutation()} want {want['perm']}"
+    assert qr.info.norm_recomputations == want["recomputed"], f"{label}: recomputed norms"
+    check_cfactor(qr, want, label)
+
+
+@pytest.mark.parametrize("bits", [64, 256, 416])
+def test_qr_complex_pivoted_vs_oracle(la, oracle, bits):
+    rng = np.random.default_rng(700 + bits)
+    for i, (m, n, kind) in enumerate([(1, 1, "moderate"), (5, 3, "qsc"), (33, 7, "graded"), (40, 21, "wide"), (50, 24, "spread"),
+                                      (41, 7, "dependent"), (90, 40, "qsc")]):
+        A = qc.complex_matrix(bits, m, n, kind, rng)
+        for block in (16, 5, 0):
+            want = oracle.qr_complex(bits, A, m, n, block, 0, pivot=True)
+            qr = la.factor_qr_complex(bits, A, m, n, opts(block, pivot=True))
+            label = f"pivoted complex bits={bits} {kind} {m}x{n} block {block}"
+            check_cpivot(qr, want, label)
+            nrhs = (1, 2, 3)[(i + block) % 3]
+            check_csolves(qr, want, oracle, qc.complex_rhs(bits, m, nrhs, rng), nrhs, label)
+
+
+def test_qr_complex_pivoted_fixtures(la, oracle):
     bits = 256
-    A = np.zeros((12, 2, bits // 32 + 3), np.uint32)
-    with pytest.raises(api.RuntimeFailure):
-        la.factor_qr_complex(bits, A, 4, 3, opts(8, pivot=True))
+    N = bits // 32
+    rng = np.random.default_rng(71)
+    cases = [("dependent, rank_bits", qc.complex_matrix(bits, 41, 7, "dependent", rng), 41, 7, bits // 2)]
+    A = qc.complex_matrix(bits, 30, 12, "moderate", rng)
+    A[2::12] = 0
+    A[7::12] = 0
+    cases.append(("zero columns 2, 7", A, 30, 12, 0))
+    A = qc.complex_matrix(bits, 25, 9, "moderate", rng)
+    for r in range(25):
+        A[r * 9 + 6] = A[r * 9 + 2]
+    cases.append(("duplicate columns", A, 25, 9, bits // 2))
+    A = qc.complex_matrix(bits, 25, 10, "moderate", rng)
+    A[7 * 10 + 4, 1, N + 2] = nb.INVALID
+    cases.append(("status at (7,4)", A, 25, 10, 0))
+    A = qc.complex_matrix(bits, 80, 20, "moderate", rng)
+    for j in (5, 13):                                          # nearly parallel columns: collapsed norms are recomputed
+        t = nb.random_complex(rng, 80, bits, 4)
+        for part in (0, 1):
+            t[:, part, N] = (nb.exponent(t[:, part]) - (bits // 4 + 10)).astype(np.int32).view(np.uint32)
+        A[j::20] = oracle.elementwise(bits, 4, np.ascontiguousarray(A[j - 1::20]), t)
+    cases.append(("nearly parallel columns", A, 80, 20, 0))
+    w = bits // 32 + 3
+    R = qc.matrix(bits, 30, 12, "qsc", rng)
+    A = np.zeros((30 * 12, 2, w), np.uint32)
+    A[:, 0] = R
+    cases.append(("real input", A, 30, 12, 0))
+    for label, A, m, n, rank_bits in cases:
+        for block in (4, 16):
+            want = oracle.qr_complex(bits, A, m, n, block, rank_bits, pivot=True)
+            qr = la.factor_qr_complex(bits, A, m, n, opts(block, rank_bits, pivot=True))
+            check_cpivot(qr, want, f"{label} block {block}")
+            if label == "nearly parallel columns":
+                assert qr.info.norm_recomputations > 0
+            check_csolves(qr, want, oracle, qc.complex_rhs(bits, m, 2, rng), 2, f"{label} block {block}")
+    # the real input gives the real pivoted factor in the real parts
+    real = la.factor_qr(bits, R, 30, 12, opts(4, pivot=True))
+    cq = la.factor_qr_complex(bits, cases[-1][1], 30, 12, opts(4, pivot=True))
+    assert cq.permutation() == real.permutation()
+    assert (cq.r()[:, 0] == real.r()).all() and (cq.r()[:, 1] == 0).all()
