@@ -666,7 +666,6 @@ class ExactGemm4:
 
     def gemm(self, bits, complex_, shape: ExactGemm4Shape, a, b, c):
         """Host arrays (prototype.hpp:32): c is updated in place; returns (Timing, ExactGemm4Report)."""
-        check_bits(bits)
         if not (isinstance(c, np.ndarray) and c.flags.c_contiguous and c.dtype == np.uint32):
             raise InvalidArgument("exact_gemm4 output must be a C-contiguous uint32 array")
         r, t = _ExactGemm4Report(), _Timing()

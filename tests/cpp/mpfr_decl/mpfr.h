@@ -83,4 +83,15 @@ void mpfr_free_cache2(mpfr_free_cache_t);
 #ifdef __cplusplus
 }
 #endif
+/* The real header also defines the field accessors as macros over the documented layout (zero, NaN and infinity
+ * encoded in the exponent field as its minimum + 1, + 2, + 3), so a build against it inlines them; so does this one. */
+#define LIMBFORGE_TEST_MPFR_EXP_ZERO (-0x7fffffffffffffffL - 1L + 1)
+#define LIMBFORGE_TEST_MPFR_EXP_INF (-0x7fffffffffffffffL - 1L + 3)
+#define mpfr_get_prec(x) ((mpfr_prec_t)(x)->_mpfr_prec)
+#define mpfr_get_exp(x) ((mpfr_exp_t)(x)->_mpfr_exp)
+#define mpfr_signbit(x) ((x)->_mpfr_sign < 0)
+#define mpfr_zero_p(x) ((x)->_mpfr_exp == LIMBFORGE_TEST_MPFR_EXP_ZERO)
+#define mpfr_regular_p(x) ((x)->_mpfr_exp > LIMBFORGE_TEST_MPFR_EXP_INF)
+#define mpfr_number_p(x) ((x)->_mpfr_exp > LIMBFORGE_TEST_MPFR_EXP_INF || (x)->_mpfr_exp == LIMBFORGE_TEST_MPFR_EXP_ZERO)
+#define mpfr_custom_get_significand(x) ((void*)(x)->_mpfr_d)
 #endif
