@@ -4,7 +4,9 @@
 #include "lf_runtime.h"
 #include "lf_eg4.cuh"
 
+#include <algorithm>
 #include <chrono>
+#include <cstring>
 
 namespace lfr {
 
@@ -31,6 +33,95 @@ static void eg4_run(int bits, bool cx, const lf_exact_gemm4_shape& s, const void
     cuda_check(cudaGetLastError(), "exact_gemm4 launch");
 }
 
+// Host copy split over the host threads (large staging copies run at memory bandwidth rather than one core's rate).
+static void par_copy(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kPiece = size_t(1) << 20;
+    const long long pieces = (long long)((bytes + kPiece - 1) / kPiece);
+#pragma omp parallel for schedule(static) if (pieces > 1)
+    for (long long q = 0; q < pieces; ++q) {
+        const size_t off = (size_t)q * kPiece, len = std::min(kPiece, bytes - off);
+        std::memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off, len);
+    }
+}
+
+// Host arrays with dense strides (16 elements, or 0 for a broadcast input): the matrices run in chunks through two
+// pinned staging slots and two streams, so that the host copies of one chunk overlap the transfers and the product
+// of the other.  Returns the summed device time of the products.
+static double eg4_host_pipelined(Engine* e, int bits, bool cx, const lf_exact_gemm4_shape& s, const void* A, const void* B, void* C) {
+    constexpr size_t kChunkBytes = size_t(8) << 20;               // per staged operand and slot
+    const size_t per = 16 * element_bytes(bits, cx);              // one matrix
+    const size_t cm = std::max<size_t>(1, kChunkBytes / per);     // matrices per chunk
+    const size_t chunks = (s.count + cm - 1) / cm;
+    const bool ba = s.stride_a == 0, bb = s.stride_b == 0;
+    const size_t slot = ((ba ? 0 : cm) + (bb ? 0 : cm) + cm) * per;
+    char* pin[2] = {static_cast<char*>(e->staging[0].get(slot)), static_cast<char*>(e->staging[1].get(slot))};
+    char* dev[2] = {static_cast<char*>(e->scratch[0].get(slot)), static_cast<char*>(e->scratch[1].get(slot))};
+    char* da0 = static_cast<char*>(e->scratch[2].get(per)), *db0 = static_cast<char*>(e->scratch[3].get(per));
+    if (ba) cuda_check(cudaMemcpy(da0, A, per, cudaMemcpyHostToDevice), "upload");
+    if (bb) cuda_check(cudaMemcpy(db0, B, per, cudaMemcpyHostToDevice), "upload");
+    cudaStream_t st[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr}, k0[2] = {nullptr, nullptr}, k1[2] = {nullptr, nullptr};
+    double gpu = 0;
+    size_t pending[2] = {SIZE_MAX, SIZE_MAX};                       // chunk whose result sits in slot q
+    auto drain = [&](int q) {                                       // wait for slot q's chunk and copy its C out
+        if (pending[q] == SIZE_MAX) return;
+        cuda_check(cudaEventSynchronize(done[q]), "execution");
+        float ms = 0;
+        cudaEventElapsedTime(&ms, k0[q], k1[q]);
+        gpu += ms * 1e-3;
+        const size_t t0 = pending[q] * cm, nt = std::min(cm, s.count - t0);
+        const size_t coff = ((ba ? 0 : cm) + (bb ? 0 : cm)) * per;
+        par_copy(static_cast<char*>(C) + t0 * per, pin[q] + coff, nt * per);
+        pending[q] = SIZE_MAX;
+    };
+    try {
+        for (int q = 0; q < 2; ++q) {
+            cuda_check(cudaStreamCreateWithFlags(&st[q], cudaStreamNonBlocking), "stream");
+            cuda_check(cudaEventCreate(&done[q]), "event");
+            cuda_check(cudaEventCreate(&k0[q]), "event");
+            cuda_check(cudaEventCreate(&k1[q]), "event");
+        }
+        for (size_t i = 0; i < chunks; ++i) {
+            const int q = int(i & 1);
+            drain(q);
+            const size_t t0 = i * cm, nt = std::min(cm, s.count - t0);
+            char* h = pin[q];
+            size_t off = 0, aoff = 0, boff = 0;
+            if (!ba) { par_copy(h, static_cast<const char*>(A) + t0 * per, nt * per); aoff = off; off += cm * per; }
+            if (!bb) { par_copy(h + off, static_cast<const char*>(B) + t0 * per, nt * per); boff = off; off += cm * per; }
+            const size_t coff = off;
+            if (s.accumulate) par_copy(h + coff, static_cast<const char*>(C) + t0 * per, nt * per);
+            char* d = dev[q];
+            if (!ba) cuda_check(cudaMemcpyAsync(d + aoff, h + aoff, nt * per, cudaMemcpyHostToDevice, st[q]), "upload");
+            if (!bb) cuda_check(cudaMemcpyAsync(d + boff, h + boff, nt * per, cudaMemcpyHostToDevice, st[q]), "upload");
+            if (s.accumulate) cuda_check(cudaMemcpyAsync(d + coff, h + coff, nt * per, cudaMemcpyHostToDevice, st[q]), "upload");
+            lf_exact_gemm4_shape cs = s;
+            cs.count = nt;
+            cuda_check(cudaEventRecord(k0[q], st[q]), "event");
+            eg4_run(bits, cx, cs, ba ? da0 : d + aoff, bb ? db0 : d + boff, d + coff, st[q]);
+            cuda_check(cudaEventRecord(k1[q], st[q]), "event");
+            cuda_check(cudaMemcpyAsync(h + coff, d + coff, nt * per, cudaMemcpyDeviceToHost, st[q]), "download");
+            cuda_check(cudaEventRecord(done[q], st[q]), "event");
+            pending[q] = i;
+        }
+        drain(int(chunks & 1));
+        drain(int((chunks + 1) & 1));
+    } catch (...) {
+        for (int q = 0; q < 2; ++q) if (st[q]) cudaStreamSynchronize(st[q]);
+        for (int q = 0; q < 2; ++q) {
+            if (st[q]) cudaStreamDestroy(st[q]);
+            if (done[q]) cudaEventDestroy(done[q]);
+            if (k0[q]) cudaEventDestroy(k0[q]);
+            if (k1[q]) cudaEventDestroy(k1[q]);
+        }
+        throw;
+    }
+    for (int q = 0; q < 2; ++q) {
+        cudaStreamDestroy(st[q]); cudaEventDestroy(done[q]); cudaEventDestroy(k0[q]); cudaEventDestroy(k1[q]);
+    }
+    return gpu;
+}
+
 }  // namespace lfr
 
 using namespace lfr;
@@ -52,6 +143,16 @@ int lf_engine_exact_gemm4(lf_engine* e, int bits, int complex_, const lf_exact_g
     if (!A || !B || !C) throw invalid_argument("exact_gemm4: null host matrix");
     const auto w0 = std::chrono::steady_clock::now();
     e->activate();
+    const bool dense = (shape->stride_a == 16 || shape->stride_a == 0) && (shape->stride_b == 16 || shape->stride_b == 0) &&
+                       (shape->stride_c == 16 || shape->count == 1);
+    if (dense) {
+        lf_exact_gemm4_shape d = *shape;
+        d.stride_c = 16;
+        const double g = eg4_host_pipelined(e, bits, complex_ != 0, d, A, B, C);
+        if (report) *report = lf_exact_gemm4_report{shape->count * 16 * (complex_ ? 2 : 1), 0, 0};
+        if (timing) *timing = {g, std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count()};
+        return LF_OK;
+    }
     const size_t es = element_bytes(bits, complex_ != 0);
     const size_t ab = checked_size(n[0], es), bb = checked_size(n[1], es), cb = checked_size(n[2], es);
     void* da = e->scratch[0].get(ab + 16);

@@ -63,6 +63,23 @@ struct DevBuf {
     }
     ~DevBuf() { if (p) cudaFree(p); }
 };
+// Pinned host staging that grows on demand (host-array calls that pipeline their transfers).
+struct PinnedBuf {
+    void* p = nullptr; size_t bytes = 0;
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+    void* get(size_t n) {
+        if (n > bytes) {
+            if (p) cudaFreeHost(p);
+            p = nullptr; bytes = 0;
+            cuda_check(cudaMallocHost(&p, n ? n : 16), "pinned staging allocation");
+            bytes = n;
+        }
+        return p;
+    }
+    ~PinnedBuf() { if (p) cudaFreeHost(p); }
+};
 
 struct Engine {
     int device = 0;
@@ -70,6 +87,7 @@ struct Engine {
     cudaStream_t stream = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     DevBuf scratch[6];
+    PinnedBuf staging[2];
     std::string name;
     lf_engine_options options{};
     void activate() const { cuda_check(cudaSetDevice(device), "cudaSetDevice"); }

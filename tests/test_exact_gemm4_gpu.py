@@ -59,6 +59,24 @@ def test_exact_gemm4_strides_broadcast_and_gaps(engine, oracle, bits, cx):
     assert (got[gaps] == Cm[gaps]).all()                      # padding between output matrices untouched
 
 
+@pytest.mark.parametrize("bits,cx,sa,accumulate", [(1024, True, 16, True), (1024, True, 0, False), (64, False, 16, True)])
+def test_exact_gemm4_host_chunks(engine, oracle, bits, cx, sa, accumulate):
+    """Host arrays run through the staged pipeline in several chunks (8 MiB of matrices per operand each)."""
+    rng = np.random.default_rng(bits + sa + accumulate)
+    g = api.ExactGemm4(engine)
+    per = 16 * (bits // 8 + 12) * (2 if cx else 1)
+    count = 2 * ((8 << 20) // per) + 37                        # two whole chunks and a ragged third
+    s = api.ExactGemm4Shape(count, sa, 16, 16, accumulate, False)
+    A = operands(bits, 1 if sa == 0 else count, cx, rng, 50)
+    B, Cm = (operands(bits, count, cx, rng, 50) for _ in range(2))
+    want = oracle.exact_gemm4(bits, cx, shape_dict(s), A, B, Cm)
+    got = Cm.copy()
+    t, rep = g.gemm(bits, cx, s, A, B, got)
+    bad = np.nonzero((got != want).reshape(count * 16, -1).any(axis=1))[0]
+    assert bad.size == 0, f"first differing components {bad[:5]}"
+    assert rep.gpu_components == count * 16 * (2 if cx else 1) and t.gpu_seconds > 0
+
+
 def test_exact_gemm4_statuses_and_empty_sums(engine, oracle):
     bits, w = 256, 11
     rng = np.random.default_rng(9)
