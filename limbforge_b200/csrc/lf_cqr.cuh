@@ -90,8 +90,10 @@ template <int N> __global__ void __launch_bounds__(256) cqr_update_kernel(CqrPan
 // and the rows of v and i v from row c (Vt, Vi, Vr).  One block.
 template <int N> __global__ void __launch_bounds__(kQrThreads) cqr_reflect_kernel(CqrPanel p, u64 c) {
     __shared__ __align__(16) u32 sm[qr_dot_words<N>()];
+    __shared__ u32 s_keep[qr_keep_words<N>()];
+    __shared__ u32 s_sv[N + 3];
     __shared__ long long s_e;
-    __shared__ int s_go, s_needs;
+    __shared__ int s_go, s_needs, s_fast;
     constexpr u64 E = N + 3, C2 = 2 * E;
     QrState* st = p.st;
     if (st->rank < (long long)p.n) return;
@@ -99,7 +101,7 @@ template <int N> __global__ void __launch_bounds__(kQrThreads) cqr_reflect_kerne
     u32* xc = p.Pt + (c * p.mr + c) * C2;
     u32* v = p.Vt + (c * p.mr + c) * C2;
     u32* iv = p.Vi + (c * p.mr + c) * C2;
-    const Num<N> s = block_exact_dot<N, true>(xc, 1, xc, 1, 2 * len, sm, p.error);
+    const Num<N> s = block_exact_dot<N, true>(xc, 1, xc, 1, 2 * len, sm, p.error, s_keep);
     int below = 0;
     for (u64 k = 2 + threadIdx.x; k < 2 * len; k += kQrThreads) below |= ldw<true>(xc + k * E + N + 1) != 0;
     below = __syncthreads_or(below);
@@ -120,6 +122,9 @@ template <int N> __global__ void __launch_bounds__(kQrThreads) cqr_reflect_kerne
             s_go = 1; s_needs = needs; s_e = needs ? (long long)v0.e : 0;
             if (needs) cq_store<N>(v, qr_scaled<N>(v0, s_e), qr_scaled<N>(aim, s_e));
             else cq_store<N>(v, qr_pow2<N>(0), zero<N>());
+            Num<N> sv;
+            s_fast = needs && qr_resum<N>(s_keep, are, v0, (long long)v0.e, sv);
+            if (s_fast) store<N>(s_sv, sv);
         }
     }
     __syncthreads();
@@ -132,7 +137,7 @@ template <int N> __global__ void __launch_bounds__(kQrThreads) cqr_reflect_kerne
     __syncthreads();
     Num<N> tre = zero<N>(), tim = zero<N>();
     if (needs) {
-        const Num<N> sv = block_exact_dot<N, false>(v, 1, v, 1, 2 * len, sm, p.error);
+        const Num<N> sv = s_fast ? load_plain<N>(s_sv) : block_exact_dot<N, false>(v, 1, v, 1, 2 * len, sm, p.error);
         if (threadIdx.x == 0) {
             const Num<N> vim = load_plain<N>(v + E);
             if (!vim.s && !vim.st) tre = divx<N>(qr_pow2<N>(1), sv);

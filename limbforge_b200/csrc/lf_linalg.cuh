@@ -366,7 +366,7 @@ template <int N, bool RO> __device__ __noinline__ Num<N> warp_exact_dot(const u3
         accumulate<W>(acc, t, c.s < 0);
     }
     if (srow) return warp_round_window<N, W>(acc, lo, srow);
-#pragma unroll
+#pragma unroll 1
     for (int o = 16; o; o >>= 1) {
         u32 other[W];
 #pragma unroll

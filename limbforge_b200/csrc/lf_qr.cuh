@@ -75,7 +75,12 @@ template <int N, bool RO> struct StridedPair {
 // thread then adds its products into a two's-complement window anchored at the lowest scale, the warps sum their
 // windows with shuffles and thread 0 adds the warps' sums and rounds once.  A range wider than the window goes to
 // src.fallback (the cluster method) on thread 0.  sm: qr_dot_words<N>() words of shared memory, 8-byte aligned.
-template <int N, class Src> __device__ __noinline__ Num<N> block_exact_sum(const Src& src, u64 K, u32* sm, u32* error) {
+// keep (optional, qr_keep_words<N>() words): thread 0 leaves there the exact window of the sum (valid flag, lo, hi,
+// logc, the two's-complement words) so that it can add terms to the exact sum and round again (qr_resum).
+// The window reductions run as rolled loops: these kernels are latency-bound on one or a few blocks, where the
+// instruction fetch of fully unrolled code, not the arithmetic, sets the time.
+template <int N> __host__ __device__ constexpr int qr_keep_words() { return qr_window<N>() + 6; }
+template <int N, class Src> __device__ __noinline__ Num<N> block_exact_sum(const Src& src, u64 K, u32* sm, u32* error, u32* keep = nullptr) {
     constexpr int W = qr_window<N>();
     constexpr int WARPS = kQrThreads / 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -112,6 +117,7 @@ template <int N, class Src> __device__ __noinline__ Num<N> block_exact_sum(const
         lo = s_lo[w] < lo ? s_lo[w] : lo; hi = s_hi[w] > hi ? s_hi[w] : hi;
     }
     __syncthreads();                                                 // the slots are reused by the next call
+    if (keep && tid == 0) keep[0] = 0;
     if (st) return zero<N>(st);
     if (!cnt) return zero<N>();
     int logc = 0;
@@ -136,7 +142,7 @@ template <int N, class Src> __device__ __noinline__ Num<N> block_exact_sum(const
         place_words<W, 2 * N>(t, p, (i64)a.e + b.e - 2 * (32 * N - 1) - lo);
         accumulate<W>(acc, t, a.s * b.s < 0);
     }
-#pragma unroll
+#pragma unroll 1
     for (int o = 16; o; o >>= 1) {
         u32 other[W];
 #pragma unroll
@@ -148,11 +154,20 @@ template <int N, class Src> __device__ __noinline__ Num<N> block_exact_sum(const
         for (int w = 0; w < W; ++w) s_win[warp * W + w] = acc[w];
     __syncthreads();
     if (tid == 0) {
+#pragma unroll 1
         for (int v = 1; v < WARPS; ++v) {
             u32 other[W];
 #pragma unroll
             for (int w = 0; w < W; ++w) other[w] = s_win[v * W + w];
             accumulate<W>(acc, other, false);
+        }
+        if (keep) {
+            keep[0] = 1;
+            keep[1] = (u32)(u64)lo; keep[2] = (u32)((u64)lo >> 32);
+            keep[3] = (u32)(u64)hi; keep[4] = (u32)((u64)hi >> 32);
+            keep[5] = (u32)logc;
+#pragma unroll 1
+            for (int w = 0; w < W; ++w) keep[6 + w] = acc[w];
         }
         int sign = 1;
         if (acc[W - 1] >> 31) {
@@ -167,8 +182,39 @@ template <int N, class Src> __device__ __noinline__ Num<N> block_exact_sum(const
     __syncthreads();
     return r;
 }
-template <int N, bool RO> __device__ Num<N> block_exact_dot(const u32* x, i64 sx, const u32* y, i64 sy, u64 K, u32* sm, u32* error) {
-    return block_exact_sum<N>(StridedPair<N, RO>{x, sx, y, sy, K}, K, sm, error);
+template <int N, bool RO> __device__ Num<N> block_exact_dot(const u32* x, i64 sx, const u32* y, i64 sy, u64 K, u32* sm, u32* error,
+                                                    u32* keep = nullptr) {
+    return block_exact_sum<N>(StridedPair<N, RO>{x, sx, y, sy, K}, K, sm, error, keep);
+}
+// P(v, v) of a reflector from the kept window of s = P(x, x) (thread 0): v = 2^-e (v0, x_1, ...), so P(v, v) =
+// 2^-2e RN(s_exact - x0^2 + v0^2) exactly, as long as every 2^-e x_r stays inside the exponent range and the window has
+// room for v0^2; false when it does not (the caller then sums v afresh).  For a complex column x0 and v0 are the real
+// parts of alpha and v0 (the imaginary part of v0 is alpha's).
+template <int N> __device__ bool qr_resum(const u32* keep, const Num<N>& x0, const Num<N>& v0, long long e, Num<N>& out) {
+    constexpr int W = qr_window<N>();
+    if (!keep[0] || !v0.s || v0.st || x0.st) return false;
+    const long long lo = (long long)((u64)keep[1] | ((u64)keep[2] << 32));
+    const long long hi = (long long)((u64)keep[3] | ((u64)keep[4] << 32));
+    const int logc = (int)keep[5];
+    const long long xe_lo = (lo + 2 * (32 * N - 1)) / 2 - 1, xe_hi = (hi - 2) / 2 + 1;    // exponents of the entries
+    if (xe_lo - e < -kEmax || xe_hi - e > kEmax) return false;
+    const long long sv = 2 * (long long)v0.e - 2 * (32 * N - 1);
+    const long long top = sv + 64 * N > hi ? sv + 64 * N : hi;
+    if (sv < lo || top - lo + logc + 4 >= 32 * (long long)W) return false;
+    u32 acc[W], p[2 * N], t[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) acc[w] = keep[6 + w];
+    if (x0.s) {
+        mant_mul<N>(x0.m, x0.m, p);
+        place_words<W, 2 * N>(t, p, 2 * (long long)x0.e - 2 * (32 * N - 1) - lo);
+        accumulate<W>(acc, t, true);
+    }
+    mant_mul<N>(v0.m, v0.m, p);
+    place_words<W, 2 * N>(t, p, sv - lo);
+    accumulate<W>(acc, t, false);
+    if (acc[W - 1] >> 31) return false;
+    out = qr_scaled<N>(round_general<N, W>(acc, lo, 1, 0), 2 * e);
+    return true;
 }
 
 // Pt <- the panel's columns of Wk, Vt <- 0.
@@ -217,15 +263,17 @@ template <int N> __global__ void __launch_bounds__(256) qr_update_kernel(QrPanel
 // diagonal: tau = 0, v = e_c, beta = x0); r_jj = beta, T_cc = tau.  One block.
 template <int N> __global__ void __launch_bounds__(kQrThreads) qr_reflect_kernel(QrPanel p, u64 c) {
     __shared__ __align__(16) u32 sm[qr_dot_words<N>()];
+    __shared__ u32 s_keep[qr_keep_words<N>()];
+    __shared__ u32 s_pv[N + 3];
     __shared__ long long s_e;
-    __shared__ int s_go;
+    __shared__ int s_go, s_fast;
     constexpr u64 E = N + 3;
     QrState* st = p.st;
     if (st->rank < (long long)p.n) return;
     const u64 j = p.k0 + c, len = p.mr - c;
     u32* xc = p.Pt + (c * p.mr + c) * E;
     u32* v = p.Vt + (c * p.mr + c) * E;
-    const Num<N> s = block_exact_dot<N, true>(xc, 1, xc, 1, len, sm, p.error);
+    const Num<N> s = block_exact_dot<N, true>(xc, 1, xc, 1, len, sm, p.error, s_keep);
     int below = 0;
     for (u64 r = 1 + threadIdx.x; r < len; r += kQrThreads) below |= ldw<true>(xc + r * E + N + 1) != 0;
     below = __syncthreads_or(below);
@@ -241,7 +289,12 @@ template <int N> __global__ void __launch_bounds__(kQrThreads) qr_reflect_kernel
         }
         if (!reason && p.rank_bits > 0 && st->have_top && (long long)beta.e + p.rank_bits < st->top) reason = 2;
         if (reason) { st->rank = (long long)j; st->reason = reason; st->status = s.st; s_go = 0; }
-        else { s_go = 1; s_e = below ? (long long)v0.e : 0; }
+        else {
+            s_go = 1; s_e = below ? (long long)v0.e : 0;
+            Num<N> pv;
+            s_fast = below && qr_resum<N>(s_keep, x0, v0, (long long)v0.e, pv);
+            if (s_fast) store<N>(s_pv, pv);
+        }
     }
     __syncthreads();
     if (!s_go) return;
@@ -252,7 +305,7 @@ template <int N> __global__ void __launch_bounds__(kQrThreads) qr_reflect_kernel
     __syncthreads();
     Num<N> tj = zero<N>();
     if (below) {
-        const Num<N> pv = block_exact_dot<N, false>(v, 1, v, 1, len, sm, p.error);
+        const Num<N> pv = s_fast ? load_plain<N>(s_pv) : block_exact_dot<N, false>(v, 1, v, 1, len, sm, p.error);
         if (threadIdx.x == 0) tj = divx<N>(qr_pow2<N>(1), pv);
     }
     if (threadIdx.x == 0) {
