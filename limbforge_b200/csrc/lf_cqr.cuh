@@ -3,7 +3,7 @@
 // products over the interleaved (re, im) operand sequences, one rounding per component; a complex array of
 // elements (re, im) is read as such a real sequence with unit stride.  The panel mirrors the real one (lf_qr.cuh):
 // column-contiguous Pt (the panel's columns), Vt (reflectors) and Vi (i v), plus Vr (the reflectors by rows,
-// entry (r, c) at r * nb + c), three launches per column and a device-side state; the trailing updates are the
+// entry (r, c) at r * nb + c), four launches per column and a device-side state; the trailing updates are the
 // real compact-WY products on the 2 x 2-block real embeddings of V and T ([[re, -im], [im, re]]) applied to the
 // work matrix split by rows (row 2r = Re of row r, 2r + 1 = Im).
 #pragma once
@@ -165,17 +165,13 @@ template <int N> __global__ void __launch_bounds__(kQrThreads) cqr_reflect_kerne
     }
 }
 // After reflector c: block u < c gives G[u] = P(v_u^H v_c), block u >= c the W row entry Wp[c][u+1] = P(v_c^H a_{u+1})
-// (the block-start column), over rows [c, mr), two real dots each.  The last block to arrive writes the T column,
-// T_lc = -(tau * P(T[l][l..c) G[l..c))) with one rounding per component (cfma, linalg_complex.mm:237), and the next
-// column's conj y and i conj y for y_i = P(T[0..i][i]^H Wp[0..i][c+1]) (linalg_complex.mm:186-187).  kb - 1 blocks.
+// (the block-start column), over rows [c, mr), two real dots each.  kb - 1 blocks.
 template <int N> __global__ void __launch_bounds__(kQrThreads) cqr_dots_kernel(CqrPanel p, u64 c) {
     __shared__ __align__(16) u32 sm[qr_dot_words<N>()];
-    __shared__ int s_last;
     constexpr u64 E = N + 3, C2 = 2 * E;
-    QrState* st = p.st;
-    const long long rank = st->rank;
+    const long long rank = p.st->rank;
     const bool reflected = rank == (long long)p.n;
-    const u64 j = p.k0 + c, len = p.mr - c, u = blockIdx.x;
+    const u64 len = p.mr - c, u = blockIdx.x;
     if (reflected && u + 1 < p.kb) {
         const u32* v = p.Vt + (c * p.mr + c) * C2;
         const u32* iv = p.Vi + (c * p.mr + c) * C2;
@@ -187,20 +183,22 @@ template <int N> __global__ void __launch_bounds__(kQrThreads) cqr_dots_kernel(C
         const Num<N> im = block_exact_dot<N, true>(a1, 1, b0, 1, 2 * len, sm, p.error);
         if (threadIdx.x == 0) cq_store<N>(out, re, im);
     }
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const u32 before = atomicAdd(&st->arrivals, 1u);
-        s_last = before == gridDim.x - 1;
-        if (s_last) st->arrivals = 0;
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
+}
+
+// T column c, T_lc = -(tau * P(T[l][l..c) G[l..c))) with one rounding per component (cfma, linalg_complex.mm:237),
+// then the next column's conj y and i conj y for y_i = P(T[0..i][i]^H Wp[0..i][c+1]) (linalg_complex.mm:186-187): one
+// warp per entry, 16 warps.  One block, after the dots kernel.
+constexpr int kCqrTcolThreads = 512;
+template <int N> __global__ void __launch_bounds__(kCqrTcolThreads) cqr_tcol_kernel(CqrPanel p, u64 c) {
+    constexpr u64 E = N + 3, C2 = 2 * E;
+    const long long rank = p.st->rank;
+    const bool reflected = rank == (long long)p.n;
+    const u64 j = p.k0 + c;
     u32* Tb = p.T + (p.k0 / p.nb) * p.nb * p.nb * C2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int WARPS = kQrThreads / 32;
+    constexpr int WARPS = kCqrTcolThreads / 32;
     if (reflected) {
-        for (u64 l = threadIdx.x; l < c; l += kQrThreads) { cq_conj<N>(p.Gc + l * C2, p.G + l * C2); cq_i_conj<N>(p.Gic + l * C2, p.G + l * C2); }
+        for (u64 l = threadIdx.x; l < c; l += kCqrTcolThreads) { cq_conj<N>(p.Gc + l * C2, p.G + l * C2); cq_i_conj<N>(p.Gic + l * C2, p.G + l * C2); }
         __syncthreads();
         const Num<N> tre = ldn<N, false>(p.tau + j * C2), tim = ldn<N, false>(p.tau + j * C2 + E);
         for (u64 l = warp; l < c; l += WARPS) {
@@ -469,6 +467,7 @@ struct CqrKernels {
     void (*update)(const CqrPanel&, u64 c, cudaStream_t);
     void (*reflect)(const CqrPanel&, u64 c, cudaStream_t);
     void (*dots)(const CqrPanel&, u64 c, cudaStream_t);
+    void (*tcol)(const CqrPanel&, u64 c, cudaStream_t);
     void (*store)(const CqrPanel&, cudaStream_t);
     void (*extract)(const u32* Wk, u32* R, u32* ER, u64 n, const QrState* st, cudaStream_t);
     void (*pivot)(const CqrPanel&, u64 c, cudaStream_t);
@@ -488,6 +487,9 @@ template <int N> void cqr_update_launch(const CqrPanel& p, u64 c, cudaStream_t s
 template <int N> void cqr_reflect_launch(const CqrPanel& p, u64 c, cudaStream_t s) { cqr_reflect_kernel<N><<<1, kQrThreads, 0, s>>>(p, c); }
 template <int N> void cqr_dots_launch(const CqrPanel& p, u64 c, cudaStream_t s) {
     if (p.kb > 1) cqr_dots_kernel<N><<<(unsigned)(p.kb - 1), kQrThreads, 0, s>>>(p, c);
+}
+template <int N> void cqr_tcol_launch(const CqrPanel& p, u64 c, cudaStream_t s) {
+    if (p.kb > 1) cqr_tcol_kernel<N><<<1, kCqrTcolThreads, 0, s>>>(p, c);
 }
 template <int N> void cqr_store_launch(const CqrPanel& p, cudaStream_t s) {
     const u64 items = p.kb * p.mr > p.kb * p.kb ? p.kb * p.mr : p.kb * p.kb;
@@ -520,7 +522,8 @@ template <int N> void cqrp_recompute_launch(const CqrPanel& p, u64 c, cudaStream
     namespace lfd {                                                                                             \
     extern const CqrKernels cqr_kernels_##N;                                                                    \
     const CqrKernels cqr_kernels_##N = {cqr_load_launch<N>, cqr_update_launch<N>, cqr_reflect_launch<N>,        \
-                                        cqr_dots_launch<N>, cqr_store_launch<N>, cqr_extract_launch<N>,         \
+                                        cqr_dots_launch<N>, cqr_tcol_launch<N>, cqr_store_launch<N>,            \
+                                        cqr_extract_launch<N>,                                                  \
                                         cqrp_pivot_launch<N>, cqrp_column_launch<N>, cqrp_gramw_launch<N>,      \
                                         cqrp_trailing_launch<N>, cqrp_recompute_launch<N>};                     \
     }

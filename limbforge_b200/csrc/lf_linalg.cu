@@ -1014,6 +1014,7 @@ static lf_qr_info cqr_device(Linalg& la, int bits, uint32_t* Wk, size_t m, size_
             if (c) ck->update(P, c, s);
             ck->reflect(P, c, s);
             ck->dots(P, c, s);
+            ck->tcol(P, c, s);
         }
         ck->store(P, s);
         cuda_check(cudaGetLastError(), "complex qr panel");
