@@ -54,3 +54,17 @@ def test_bridge_vs_oracle_cast(bridge, oracle, tmp_path):
         narrow = oracle.cast(1024, w, False, x)
         assert (got_from == narrow).all(), f"from_mpfr<{w}>"
         assert (got_to == oracle.cast(w, 1024, False, narrow)).all(), f"to_mpfr at precision {w}"
+
+
+@pytest.mark.gpu
+def test_bridge_buffers_and_inline_import_on_gpu(tmp_path):
+    """The engine-buffer forms of the bridge and the inline MPC import, through the C++ headers and the library."""
+    from limbforge_b200 import build
+    build.build()
+    exe = str(tmp_path / "bridge_gpu")
+    libdir = os.path.join(ROOT, "limbforge_b200")
+    subprocess.run(["g++", "-std=c++17", "-O2", f"-I{ROOT}/include", f"-I{ROOT}/tests/cpp/mpfr_decl",
+                    os.path.join(ROOT, "tests", "cpp", "bridge_gpu.cpp"), "-o", exe, f"-L{libdir}", "-llimbforge_b200",
+                    f"-Wl,-rpath,{libdir}", "-l:libmpfr.so.6", "-l:libgmp.so.10", "-pthread"], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "bridge gpu ok" in r.stdout, r.stdout + r.stderr
