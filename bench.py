@@ -573,7 +573,9 @@ def exact_gemm4_448(torch, api, scale=1.0):
     composed = composed[3:]
     pc = min(count, 10000)
     sh = {"count": pc, "stride_a": 16, "stride_b": 16, "stride_c": 16, "accumulate": True, "negative": False}
+    t0 = time.perf_counter()
     want = Oracle().exact_gemm4(bits, cx, sh, A[:pc * 16], B[:pc * 16], C0[:pc * 16])
+    t_orc = time.perf_counter() - t0
     match = bool((C[:pc * 16] == want).all())
     dev_ms = min(t.gpu_seconds for t in res) * 1e3
     # algorithmic bytes: A, B read and C read + written once, 2 * (N + 3) words per complex element
@@ -585,7 +587,9 @@ def exact_gemm4_448(torch, api, scale=1.0):
             "matrices_per_s": count / (dev_ms * 1e-3), "algorithmic_gb_s": moved / (dev_ms * 1e-3) / 1e9,
             "reference_m5max_resident_ms": 49.015 if count == 100000 else None,
             "reference_m5max_host_ms": 49.277 if count == 100000 else None,
-            "parity": {"checked_matrices": pc, "match": match}}
+            "parity": {"checked_matrices": pc, "match": match},
+            "cpu_oracle": {"matrices_per_s": pc / t_orc, "cores": os.cpu_count(), "kind": "port",
+                           "sample": f"{pc} of {count} matrices (the C oracle, OpenMP)"}}
 
 
 def mpfr_bridge():

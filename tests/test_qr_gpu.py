@@ -371,3 +371,19 @@ def test_qr_complex_pivoted_fixtures(la, oracle):
     cq = la.factor_qr_complex(bits, cases[-1][1], 30, 12, opts(4, pivot=True))
     assert cq.permutation() == real.permutation()
     assert (cq.r()[:, 0] == real.r()).all() and (cq.r()[:, 1] == 0).all()
+
+
+def test_qr_large_factor_parity(la, oracle):
+    """Whole factors and solutions at bench-like sizes: real 1000 x 500 and complex 400 x 200, QSC-like, block 32."""
+    bits = 256
+    rng = np.random.default_rng(901)
+    A = qc.matrix(bits, 1000, 500, "qsc", rng)
+    want = oracle.qr(bits, A, 1000, 500, 32)
+    qr = la.factor_qr(bits, A, 1000, 500, opts(32))
+    check_factor(qr, want, "real 1000x500")
+    check_solves(qr, want, oracle, qc.rhs(bits, 1000, 4, rng), 4, "real 1000x500")
+    Z = qc.complex_matrix(bits, 400, 200, "qsc", rng)
+    wantc = oracle.qr_complex(bits, Z, 400, 200, 32)
+    cq = la.factor_qr_complex(bits, Z, 400, 200, opts(32))
+    check_cfactor(cq, wantc, "complex 400x200")
+    check_csolves(cq, wantc, oracle, qc.complex_rhs(bits, 400, 4, rng), 4, "complex 400x200")
