@@ -411,26 +411,32 @@ template <int N> __device__ __forceinline__ Num<N> crt_tail(u32* S, int qwords, 
 // analysis bounds every product of output (i, j): a nonzero, status-free entry of line i has its exponent in
 // [bottom_i, top_i], so the products' scales lie in [base, base + spread_i + spread_j] with base = bottom_i +
 // bottom_j - 2(32N - 1), each below 2^(scale + 64N), and K of them sum below 2^(base + spread_i + spread_j + 64N +
-// ceil(log2 K)).  When that fits kWinWords(N) words, the output sums its products as two magnitudes, positive and
-// negative, at word offset (scale - base) / 32 (carries run a word or two), then subtracts them once; wider outputs
-// take exact_dot_add_dev's cluster method in the same kernel.  A block computes an 8 x 8 tile of outputs and stages
-// the 8 + 8 lines' next kWinTK entries in shared memory, so each entry is read from memory once per tile instead of
-// once per output; the windows live in shared memory (one odd-stride row per thread).
+// ceil(log2 K)).  When that fits kWinWords(N) words, the output adds each signed product, shifted to its bit offset
+// (scale - base), word by word into signed 64-bit column sums: no carry runs between the words of a product, so the
+// adds of one product are independent, and K < 2^28 products of 32-bit words cannot overflow a column.  One carry pass
+// at the end turns the columns into a two's-complement window that is rounded once with the old entry; wider
+// outputs take exact_dot_add_dev's cluster method in the same kernel.  A block computes an 8 x 8 tile of outputs and
+// stages the 8 + 8 lines' next kWinTK entries in shared memory, so each entry is read from memory once per tile
+// instead of once per output; the column sums live in shared memory (one row per thread, an odd number of 64-bit
+// words apart).
 constexpr int kWinTM = 8, kWinTN = 8, kWinThreads = kWinTM * kWinTN, kWinTK = 8;
 template <int N> __host__ __device__ constexpr int win_words() { return 2 * N + 8; }
-template <int N> __host__ __device__ constexpr int win_row_words() { return (win_words<N>() + round_sum2_words<N>(win_words<N>())) | 1; }
+// Row of one thread: W 64-bit column sums, later the W-word window (round_sum2's scratch is thread-local, used once
+// per output); the row is an odd number of 64-bit words long.
+template <int N> __host__ __device__ constexpr int win_row_words() { return 2 * (win_words<N>() | 1); }
+constexpr unsigned long long kWinMaxK = 1ull << 28;          // column sums of 32-bit words stay below 2^62
 template <int N> __host__ __device__ constexpr size_t win_smem_bytes() {
     return (size_t)4 * ((kWinTM + kWinTN) * kWinTK * (N + 3) + kWinThreads * win_row_words<N>());
 }
-// acc (len words) += t (tw words) << (32 ws + bs), carries to the end of acc
-__device__ __forceinline__ void win_add(u32* acc, int len, const u32* t, int tw, int ws, int bs) {
-    u64 cy = 0;
-    int k = ws;
-    for (int q = 0; q <= tw && k < len; ++q, ++k) {
-        const u32 v = lf_fshl(q ? t[q - 1] : 0u, q < tw ? t[q] : 0u, (u32)bs);
-        const u64 x = (u64)acc[k] + v + cy; acc[k] = (u32)x; cy = x >> 32;
+// col (len signed 64-bit column sums) +/-= t (TW words) << (32 ws + bs), one independent add per word
+template <int TW> __device__ __forceinline__ void win_add_cols(long long* col, int len, const u32 (&t)[TW], int ws, int bs, bool negative) {
+#pragma unroll
+    for (int q = 0; q <= TW; ++q) {
+        const int k = ws + q;
+        if (k >= len) break;
+        const u32 v = lf_fshl(q ? t[q - 1] : 0u, q < TW ? t[q] : 0u, (u32)bs);
+        col[k] += negative ? -(long long)v : (long long)v;
     }
-    for (; cy && k < len; ++k) { const u64 x = (u64)acc[k] + cy; acc[k] = (u32)x; cy = x >> 32; }
 }
 struct WinParams {
     DotParams d;                    // operands, output, modes, error word
@@ -443,8 +449,8 @@ template <int N> __global__ void __launch_bounds__(kWinThreads) window_dot_kerne
     u32* sA = win_park;                                  // [kWinTK][kWinTM] entries
     u32* sB = sA + kWinTK * kWinTM * E;                  // [kWinTK][kWinTN] entries
     const int t = threadIdx.x, r = t / kWinTN, q = t % kWinTN;
-    u32* pos = sB + kWinTK * kWinTN * E + t * win_row_words<N>();
-    u32* neg = pos + W;                                  // also round_sum2's scratch afterwards
+    u32* row = sB + kWinTK * kWinTN * E + t * win_row_words<N>();
+    long long* col = reinterpret_cast<long long*>(row);  // W column sums; then the window
     const u64 r0 = (u64)blockIdx.y * kWinTM, q0 = (u64)blockIdx.x * kWinTN;
     const u64 ro = r0 + r, qo = q0 + q;                  // this thread's output (local row, column)
     const u64 i = p.row0 + ro, j = p.col0 + qo;          // its lines
@@ -458,8 +464,8 @@ template <int N> __global__ void __launch_bounds__(kWinThreads) window_dot_kerne
     int logk = 0;
     while ((1ull << logk) < p.K) ++logk;
     const i64 span = products ? (i64)(li.top - li.bottom) + (ri.top - ri.bottom) + 64 * N + logk : 0;
-    const bool window = live && !st && products && span <= 32 * W;
-    if (window) for (int w = 0; w < W; ++w) { pos[w] = 0; neg[w] = 0; }
+    const bool window = live && !st && products && span < 32 * W && p.K < kWinMaxK;   // a sign bit above the sum
+    if (window) for (int w = 0; w < W; ++w) col[w] = 0;
     const int ebase = li.bottom + ri.bottom;
     // all threads stage the tiles (the barriers include threads without a window)
     for (u64 k0 = 0; k0 < p.K; k0 += kWinTK) {
@@ -489,7 +495,7 @@ template <int N> __global__ void __launch_bounds__(kWinThreads) window_dot_kerne
             for (int w = 0; w < N; ++w) { am[w] = a[w]; bm[w] = b[w]; }
             mant_mul<N>(am, bm, pr);
             const int off = (int)a[N] + (int)b[N] - ebase;           // 0 <= off <= spread_i + spread_j
-            win_add(((sa * sb > 0) != (p.subtract != 0)) ? pos : neg, W, pr, 2 * N, off >> 5, off & 31);
+            win_add_cols<2 * N>(col, W, pr, off >> 5, off & 31, (sa * sb > 0) == (p.subtract != 0));
         }
     }
     if (!live) return;
@@ -501,16 +507,25 @@ template <int N> __global__ void __launch_bounds__(kWinThreads) window_dot_kerne
         store<N>(out, v);
         return;
     }
-    // X = pos - neg as sign and magnitude, then one rounding with the old entry
-    int cmp = 0;
-    for (int w = W - 1; w >= 0 && !cmp; --w) if (pos[w] != neg[w]) cmp = pos[w] > neg[w] ? 1 : -1;
-    u32* big = cmp >= 0 ? pos : neg;
-    const u32* small = cmp >= 0 ? neg : pos;
-    u32 bo = 0;
-    for (int w = 0; w < W; ++w) { const u64 d = (u64)small[w] + bo; const u32 o = big[w]; big[w] = (u32)((u64)o - d); bo = (u64)o < d; }
-    if (big != pos) for (int w = 0; w < W; ++w) pos[w] = big[w];
+    // one carry pass: the columns become the two's-complement window X (in place: word w is written after column w,
+    // which starts at word 2w, has been read), its sign the final carry's
+    u32* X = row;
+    long long carry = 0;
+    for (int w = 0; w < W; ++w) {
+        const long long v = col[w] + carry;
+        X[w] = (u32)v;
+        carry = v >> 32;
+    }
+    int cmp = carry < 0 ? -1 : 0;
+    if (cmp < 0) {
+        u32 cy = 1;
+        for (int w = 0; w < W; ++w) { const u32 v = ~X[w] + cy; cy = cy && v == 0; X[w] = v; }
+    } else {
+        for (int w = 0; w < W && !cmp; ++w) if (X[w]) cmp = 1;
+    }
     // round_sum2 adds the old entry c with its own sign (it computes RN(sign * X * 2^scale + c))
-    store<N>(out, round_sum2<N>(pos, W, (i64)ebase - 2 * (32 * N - 1), cmp, c, neg));
+    u32 scratch[round_sum2_words<N>(W)];
+    store<N>(out, round_sum2<N>(X, W, (i64)ebase - 2 * (32 * N - 1), cmp, c, scratch));
 }
 
 template <int N> __global__ void __launch_bounds__(128) reconstruct_kernel(RecParams p) {
