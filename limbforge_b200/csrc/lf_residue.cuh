@@ -421,9 +421,9 @@ template <int N> __device__ __forceinline__ Num<N> crt_tail(u32* S, int qwords, 
 // words apart).
 constexpr int kWinTM = 8, kWinTN = 8, kWinThreads = kWinTM * kWinTN, kWinTK = 8;
 template <int N> __host__ __device__ constexpr int win_words() { return 2 * N + 8; }
-// Row of one thread: W 64-bit column sums, later the W-word window (round_sum2's scratch is thread-local, used once
-// per output); the row is an odd number of 64-bit words long.
-template <int N> __host__ __device__ constexpr int win_row_words() { return 2 * (win_words<N>() | 1); }
+// Row of one thread: W + 1 64-bit column sums (the sum's sign in the last), later the window (round_sum2's scratch is
+// thread-local, used once per output); the row is an odd number of 64-bit words long.
+template <int N> __host__ __device__ constexpr int win_row_words() { return 2 * ((win_words<N>() + 1) | 1); }
 constexpr unsigned long long kWinMaxK = 1ull << 28;          // column sums of 32-bit words stay below 2^62
 template <int N> __host__ __device__ constexpr size_t win_smem_bytes() {
     return (size_t)4 * ((kWinTM + kWinTN) * kWinTK * (N + 3) + kWinThreads * win_row_words<N>());
@@ -464,8 +464,9 @@ template <int N> __global__ void __launch_bounds__(kWinThreads) window_dot_kerne
     int logk = 0;
     while ((1ull << logk) < p.K) ++logk;
     const i64 span = products ? (i64)(li.top - li.bottom) + (ri.top - ri.bottom) + 64 * N + logk : 0;
-    const bool window = live && !st && products && span < 32 * W && p.K < kWinMaxK;   // a sign bit above the sum
-    if (window) for (int w = 0; w < W; ++w) col[w] = 0;
+    const bool window = live && !st && products && span <= 32 * W && p.K < kWinMaxK;
+    constexpr int W1 = W + 1;                            // one more column for the sign of the signed sum
+    if (window) for (int w = 0; w < W1; ++w) col[w] = 0;
     const int ebase = li.bottom + ri.bottom;
     // all threads stage the tiles (the barriers include threads without a window)
     for (u64 k0 = 0; k0 < p.K; k0 += kWinTK) {
@@ -495,7 +496,7 @@ template <int N> __global__ void __launch_bounds__(kWinThreads) window_dot_kerne
             for (int w = 0; w < N; ++w) { am[w] = a[w]; bm[w] = b[w]; }
             mant_mul<N>(am, bm, pr);
             const int off = (int)a[N] + (int)b[N] - ebase;           // 0 <= off <= spread_i + spread_j
-            win_add_cols<2 * N>(col, W, pr, off >> 5, off & 31, (sa * sb > 0) == (p.subtract != 0));
+            win_add_cols<2 * N>(col, W1, pr, off >> 5, off & 31, (sa * sb > 0) == (p.subtract != 0));
         }
     }
     if (!live) return;
@@ -511,7 +512,7 @@ template <int N> __global__ void __launch_bounds__(kWinThreads) window_dot_kerne
     // which starts at word 2w, has been read), its sign the final carry's
     u32* X = row;
     long long carry = 0;
-    for (int w = 0; w < W; ++w) {
+    for (int w = 0; w < W1; ++w) {
         const long long v = col[w] + carry;
         X[w] = (u32)v;
         carry = v >> 32;
@@ -519,13 +520,13 @@ template <int N> __global__ void __launch_bounds__(kWinThreads) window_dot_kerne
     int cmp = carry < 0 ? -1 : 0;
     if (cmp < 0) {
         u32 cy = 1;
-        for (int w = 0; w < W; ++w) { const u32 v = ~X[w] + cy; cy = cy && v == 0; X[w] = v; }
+        for (int w = 0; w < W1; ++w) { const u32 v = ~X[w] + cy; cy = cy && v == 0; X[w] = v; }
     } else {
-        for (int w = 0; w < W && !cmp; ++w) if (X[w]) cmp = 1;
+        for (int w = 0; w < W1 && !cmp; ++w) if (X[w]) cmp = 1;
     }
     // round_sum2 adds the old entry c with its own sign (it computes RN(sign * X * 2^scale + c))
-    u32 scratch[round_sum2_words<N>(W)];
-    store<N>(out, round_sum2<N>(X, W, (i64)ebase - 2 * (32 * N - 1), cmp, c, scratch));
+    u32 scratch[round_sum2_words<N>(W1)];
+    store<N>(out, round_sum2<N>(X, W1, (i64)ebase - 2 * (32 * N - 1), cmp, c, scratch));
 }
 
 template <int N> __global__ void __launch_bounds__(128) reconstruct_kernel(RecParams p) {
