@@ -727,9 +727,31 @@ struct QrFactor {
     bool pivot = false;
     bool cplx = false;                           // a complex factor (linalg_complex.mm): complex arrays, real embeddings
     lf_qr_info info{};
-    std::vector<uint32_t> R, V, T, tau;          // the accessors' arrays
+    // The accessors' arrays.  The factor keeps R, V and T on the device and copies them to these arrays the first
+    // time an accessor asks (host_pending): a factorization followed by solves or Q applications moves no factor data
+    // to the host.
+    mutable std::vector<uint32_t> R, V, T, tau;
     std::vector<size_t> perm;
     DevBuf dV, dT, dR;                           // device copies for the solves and Q applications (complex: the embeddings)
+    DevBuf cV, cT, cR;                           // complex: the factor's own complex arrays, for the accessors
+    mutable bool host_pending = false;
+    mutable std::mutex host_mutex;
+    void materialize() const {
+        std::lock_guard<std::mutex> lock(host_mutex);
+        if (!host_pending) return;
+        const size_t E = size_t(bits / 32 + 3) * (cplx ? 2 : 1), eb = 4 * E, blocks = nb ? (n + nb - 1) / nb : 0;
+        const void* sR = cplx ? cR.p : dR.p;
+        const void* sV = cplx ? cV.p : dV.p;
+        const void* sT = cplx ? cT.p : dT.p;
+        Engine& e = *owner->engine;
+        e.activate();
+        R.resize(n * n * E); V.resize(m * n * E); T.resize(blocks * nb * nb * E);
+        cuda_check(cudaMemcpyAsync(R.data(), sR, n * n * eb, cudaMemcpyDeviceToHost, e.stream), "download");
+        cuda_check(cudaMemcpyAsync(V.data(), sV, m * n * eb, cudaMemcpyDeviceToHost, e.stream), "download");
+        if (blocks) cuda_check(cudaMemcpyAsync(T.data(), sT, blocks * nb * nb * eb, cudaMemcpyDeviceToHost, e.stream), "download");
+        cuda_check(cudaStreamSynchronize(e.stream), "download");
+        host_pending = false;
+    }
 };
 
 // Block b of the compact-WY factor (V: mE x nE, T: blocks of nbE x nbE, all real) applied to columns [c0, c1) of X
@@ -1256,8 +1278,9 @@ static void qr_factor_common(Linalg& la, QrFactor& f, const uint32_t* dA, int ra
     const size_t eb = size_t(f.bits / 8 + 12), m = f.m, n = f.n;
     const size_t blocks = f.nb ? (n + f.nb - 1) / f.nb : 0;
     auto w0 = Clock::now();
-    f.R.assign(n * n * (eb / 4), 0); f.V.assign(m * n * (eb / 4), 0);
-    f.T.assign(blocks * f.nb * f.nb * (eb / 4), 0); f.tau.assign(n * (eb / 4), 0);
+    f.R.clear(); f.V.clear(); f.T.clear();
+    f.host_pending = false;
+    f.tau.assign(n * (eb / 4), 0);
     f.perm.resize(n);
     for (size_t k = 0; k < n; ++k) f.perm[k] = k;
     f.info = lf_qr_info{};
@@ -1273,11 +1296,10 @@ static void qr_factor_common(Linalg& la, QrFactor& f, const uint32_t* dA, int ra
     uint32_t* tau = static_cast<uint32_t*>(la.qr[10].get(n * eb));
     f.info = f.pivot ? qr_device_pivoted(la, f.bits, Wk, m, n, f.nb, rank_bits, V, T, tau, R, f.perm.data())
                      : qr_device(la, f.bits, Wk, m, n, f.nb, rank_bits, V, T, tau, R);
-    cuda_check(cudaMemcpyAsync(f.R.data(), R, n * n * eb, cudaMemcpyDeviceToHost, s), "download");
-    cuda_check(cudaMemcpyAsync(f.V.data(), V, m * n * eb, cudaMemcpyDeviceToHost, s), "download");
-    if (blocks) cuda_check(cudaMemcpyAsync(f.T.data(), T, blocks * f.nb * f.nb * eb, cudaMemcpyDeviceToHost, s), "download");
+    (void)R; (void)V; (void)T;                   // kept on the device; copied on the first accessor call
     cuda_check(cudaMemcpyAsync(f.tau.data(), tau, n * eb, cudaMemcpyDeviceToHost, s), "download");
     cuda_check(cudaStreamSynchronize(s), "download");
+    f.host_pending = true;
     f.info.timing.wall_seconds = since(w0);
 }
 
@@ -1373,10 +1395,17 @@ int lf_qr_describe(const lf_qr* f, int* bits, size_t* rows, size_t* cols, size_t
     if (info) *info = f->info;
     LF_API_END
 }
-const void* lf_qr_r(const lf_qr* f) { return f && !f->R.empty() ? f->R.data() : nullptr; }
-const void* lf_qr_v(const lf_qr* f) { return f && !f->V.empty() ? f->V.data() : nullptr; }
+// The first call on a real factor copies R, V and T from the device; a failing copy gives nullptr and the error
+// message (lf_last_error).
+static const QrFactor* qr_host(const lf_qr* f) {
+    if (!f) return nullptr;
+    try { f->materialize(); } catch (const std::exception& e) { set_error(e.what()); return nullptr; }
+    return f;
+}
+const void* lf_qr_r(const lf_qr* f) { const QrFactor* q = qr_host(f); return q && !q->R.empty() ? q->R.data() : nullptr; }
+const void* lf_qr_v(const lf_qr* f) { const QrFactor* q = qr_host(f); return q && !q->V.empty() ? q->V.data() : nullptr; }
 const void* lf_qr_tau(const lf_qr* f) { return f && !f->tau.empty() ? f->tau.data() : nullptr; }
-const void* lf_qr_t(const lf_qr* f) { return f && !f->T.empty() ? f->T.data() : nullptr; }
+const void* lf_qr_t(const lf_qr* f) { const QrFactor* q = qr_host(f); return q && !q->T.empty() ? q->T.data() : nullptr; }
 const size_t* lf_qr_permutation(const lf_qr* f) { return f && !f->perm.empty() ? f->perm.data() : nullptr; }
 
 // QRFactor::solve (linalg.hpp:127): X (n x nrhs) = the least-squares solution for each column of B (m x nrhs).
@@ -1488,8 +1517,7 @@ int lf_linalg_factor_qr_complex(lf_linalg* la, int bits, const void* A, size_t m
     const size_t eb = size_t(bits / 8 + 12), E = eb / 4, cb = 2 * eb;
     const size_t blocks = f->nb ? (n + f->nb - 1) / f->nb : 0;
     auto w0 = Clock::now();
-    f->R.assign(n * n * 2 * E, 0); f->V.assign(m * n * 2 * E, 0);
-    f->T.assign(blocks * f->nb * f->nb * 2 * E, 0); f->tau.assign(n * 2 * E, 0);
+    f->tau.assign(n * 2 * E, 0);
     f->perm.resize(n);
     for (size_t k = 0; k < n; ++k) f->perm[k] = k;
     f->info.rank = n;
@@ -1501,21 +1529,19 @@ int lf_linalg_factor_qr_complex(lf_linalg* la, int bits, const void* A, size_t m
         split_rows(static_cast<const uint32_t*>(A), m, n, E, split);
         uint32_t* Wk = static_cast<uint32_t*>(la->work[4].get(2 * m * n * eb));
         cuda_check(cudaMemcpyAsync(Wk, split.data(), 2 * m * n * eb, cudaMemcpyHostToDevice, s), "upload");
-        DevBuf dVc, dTc, dRc, dtau;
-        uint32_t* V = static_cast<uint32_t*>(dVc.get(m * n * cb));
-        uint32_t* T = static_cast<uint32_t*>(dTc.get(blocks * f->nb * f->nb * cb + 16));
-        uint32_t* R = static_cast<uint32_t*>(dRc.get(n * n * cb));
+        DevBuf dtau;
+        uint32_t* V = static_cast<uint32_t*>(f->cV.get(m * n * cb));
+        uint32_t* T = static_cast<uint32_t*>(f->cT.get(blocks * f->nb * f->nb * cb + 16));
+        uint32_t* R = static_cast<uint32_t*>(f->cR.get(n * n * cb));
         uint32_t* tau = static_cast<uint32_t*>(dtau.get(n * cb));
         uint32_t* EV = static_cast<uint32_t*>(f->dV.get(4 * m * n * eb));
         uint32_t* ET = static_cast<uint32_t*>(f->dT.get(4 * blocks * f->nb * f->nb * eb + 16));
         uint32_t* ER = static_cast<uint32_t*>(f->dR.get(4 * n * n * eb));
         f->info = f->pivot ? cqr_device_pivoted(*la, bits, Wk, m, n, f->nb, opts.rank_bits, V, T, tau, R, EV, ET, ER, f->perm.data())
                            : cqr_device(*la, bits, Wk, m, n, f->nb, opts.rank_bits, V, T, tau, R, EV, ET, ER);
-        cuda_check(cudaMemcpyAsync(f->R.data(), R, n * n * cb, cudaMemcpyDeviceToHost, s), "download");
-        cuda_check(cudaMemcpyAsync(f->V.data(), V, m * n * cb, cudaMemcpyDeviceToHost, s), "download");
-        if (blocks) cuda_check(cudaMemcpyAsync(f->T.data(), T, blocks * f->nb * f->nb * cb, cudaMemcpyDeviceToHost, s), "download");
         cuda_check(cudaMemcpyAsync(f->tau.data(), tau, n * cb, cudaMemcpyDeviceToHost, s), "download");
         cuda_check(cudaStreamSynchronize(s), "download");
+        f->host_pending = true;                  // R, V and T are copied on the first accessor call
     } else {
         f->info.rank = 0;
     }
