@@ -111,6 +111,10 @@ class QRFactor {
         info_.panel_seconds = i.panel_seconds; info_.update_seconds = i.update_seconds; info_.norm_recomputations = i.norm_recomputations;
     }
     const lf_qr* get() const { if (!q_) throw std::logic_error("empty QR factor"); return q_.get(); }
+    const void* host(const void* p) const {
+        if (!p && n_) throw std::runtime_error(std::string("QR factor arrays: ") + lf_last_error());
+        return p;
+    }
     friend class Linalg;
 public:
     QRFactor() = default;
@@ -123,10 +127,11 @@ public:
     std::size_t block() const { (void)get(); return nb_; }
     const QRInfo& info() const { (void)get(); return info_; }
     bool full_rank() const { (void)get(); return info_.rank == n_; }
-    const void* r() const { return lf_qr_r(get()); }
-    const void* v() const { return lf_qr_v(get()); }
+    // R, V and T are copied from the device on the first call; a failed copy throws.
+    const void* r() const { return host(lf_qr_r(get())); }
+    const void* v() const { return host(lf_qr_v(get())); }
     const void* tau() const { return lf_qr_tau(get()); }
-    const void* t() const { return lf_qr_t(get()); }
+    const void* t() const { return host(lf_qr_t(get())); }
     bool pivoted() const { (void)get(); return pivoted_; }
     const std::size_t* permutation() const { return lf_qr_permutation(get()); }
     // Least squares X (n x nrhs) for B (m x nrhs); X must not overlap B (linalg.hpp:127).

@@ -1026,9 +1026,11 @@ class QRFactor:
     def _array(self, fn, count) -> np.ndarray:
         w = self.bits // 32 + 3
         shape = (count, 2, w) if self.complex else (count, w)
-        p = fn(self.handle)
-        if not p or not count:
+        p = fn(self.handle)                      # R, V and T are copied from the device on the first call
+        if not count:
             return np.zeros((0,) + shape[1:], dtype=np.uint32)
+        if not p:
+            raise RuntimeFailure("QR factor arrays: " + lib.lf_last_error().decode())
         total = count * w * (2 if self.complex else 1)
         return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint32)), shape=(total,)).reshape(shape).copy()
 
