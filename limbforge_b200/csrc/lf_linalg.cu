@@ -1249,6 +1249,15 @@ static double qr_solve_device(Linalg& la, const QrFactor& f, uint32_t* C, size_t
     }
     return g;
 }
+// A complex matrix (rows x cols elements of (re, im), E words each) to the row-split real layout, on the device: one
+// thread per word of A.
+__global__ void split_rows_kernel(const uint32_t* A, uint32_t* W, uint64_t rows, uint64_t cols, uint64_t E) {
+    const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= rows * cols * 2 * E) return;
+    const uint64_t el = q / (2 * E), k = q % (2 * E), part = k / E, w = k % E;
+    const uint64_t r = el / cols, c = el % cols;
+    W[((2 * r + part) * cols + c) * E + w] = A[q];
+}
 // Complex host arrays <-> the row-split real layout the device works on (row 2r = Re of row r, 2r + 1 = Im).
 static void split_rows(const uint32_t* A, size_t rows, size_t cols, size_t E, std::vector<uint32_t>& out) {
     out.resize(2 * rows * cols * E);
@@ -1525,10 +1534,13 @@ int lf_linalg_factor_qr_complex(lf_linalg* la, int bits, const void* A, size_t m
         Engine& e = *la->engine;
         e.activate();
         cudaStream_t s = e.stream;
-        std::vector<uint32_t> split;
-        split_rows(static_cast<const uint32_t*>(A), m, n, E, split);
+        // A as it is, then split by rows on the device
+        uint32_t* Ac = static_cast<uint32_t*>(la->qr[8].get(2 * m * n * eb));
         uint32_t* Wk = static_cast<uint32_t*>(la->work[4].get(2 * m * n * eb));
-        cuda_check(cudaMemcpyAsync(Wk, split.data(), 2 * m * n * eb, cudaMemcpyHostToDevice, s), "upload");
+        cuda_check(cudaMemcpyAsync(Ac, A, 2 * m * n * eb, cudaMemcpyHostToDevice, s), "upload");
+        const uint64_t words = 2 * (uint64_t)m * n * E;
+        split_rows_kernel<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(Ac, Wk, m, n, E);
+        cuda_check(cudaGetLastError(), "split rows");
         DevBuf dtau;
         uint32_t* V = static_cast<uint32_t*>(f->cV.get(m * n * cb));
         uint32_t* T = static_cast<uint32_t*>(f->cT.get(blocks * f->nb * f->nb * cb + 16));
