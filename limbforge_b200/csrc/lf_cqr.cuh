@@ -91,7 +91,6 @@ template <int N> __global__ void __launch_bounds__(256) cqr_update_kernel(CqrPan
 template <int N> __global__ void __launch_bounds__(kQrThreads) cqr_reflect_kernel(CqrPanel p, u64 c) {
     __shared__ __align__(16) u32 sm[qr_dot_words<N>()];
     __shared__ u32 s_keep[qr_keep_words<N>()];
-    __shared__ u32 s_sv[N + 3];
     __shared__ long long s_e;
     __shared__ int s_go, s_needs, s_fast;
     constexpr u64 E = N + 3, C2 = 2 * E;
@@ -105,9 +104,9 @@ template <int N> __global__ void __launch_bounds__(kQrThreads) cqr_reflect_kerne
     int below = 0;
     for (u64 k = 2 + threadIdx.x; k < 2 * len; k += kQrThreads) below |= ldw<true>(xc + k * E + N + 1) != 0;
     below = __syncthreads_or(below);
-    Num<N> beta = zero<N>(), v0 = qr_pow2<N>(0);
+    Num<N> beta = zero<N>(), v0 = qr_pow2<N>(0), are = zero<N>(), aim = zero<N>();
     if (threadIdx.x == 0) {
-        const Num<N> are = load_plain<N>(xc), aim = load_plain<N>(xc + E);
+        are = load_plain<N>(xc); aim = load_plain<N>(xc + E);
         const int needs = below || aim.s;
         int reason = s.st ? 3 : (!are.s && !aim.s && !below) ? 1 : 0;
         beta = are;
@@ -122,31 +121,36 @@ template <int N> __global__ void __launch_bounds__(kQrThreads) cqr_reflect_kerne
             s_go = 1; s_needs = needs; s_e = needs ? (long long)v0.e : 0;
             if (needs) cq_store<N>(v, qr_scaled<N>(v0, s_e), qr_scaled<N>(aim, s_e));
             else cq_store<N>(v, qr_pow2<N>(0), zero<N>());
-            Num<N> sv;
-            s_fast = needs && qr_resum<N>(s_keep, are, v0, (long long)v0.e, sv);
-            if (s_fast) store<N>(s_sv, sv);
         }
     }
     __syncthreads();
     if (!s_go) return;
     const long long e = s_e;
     const bool needs = s_needs;
-    if (needs)
-        for (u64 r = 1 + threadIdx.x; r < len; r += kQrThreads)
+    Num<N> tre = zero<N>(), tim = zero<N>();
+    auto tau_of = [&](const Num<N>& sv) {                             // thread 0
+        const Num<N> vim = load_plain<N>(v + E);
+        if (!vim.s && !vim.st) tre = divx<N>(qr_pow2<N>(1), sv);
+        else {
+            const Num<N> a = qr_scaled<N>(sv, 1), b = mulx<N>(qr_scaled<N>(beta, e), vim);
+            const Num<N> d = dot2_add<N>(a, a, b, b, zero<N>());
+            tre = divx<N>(a, d); tim = negate<N>(divx<N>(b, d));
+        }
+    };
+    // Thread 0 forms P(v^H v) from the kept window and tau while warps 1.. scale the rest of the reflector.
+    if (threadIdx.x == 0) {
+        Num<N> sv;
+        const int fast = needs && qr_resum<N>(s_keep, are, v0, e, sv);
+        if (fast) tau_of(sv);
+        s_fast = fast;
+    }
+    if (needs && threadIdx.x >= 32)
+        for (u64 r = 1 + threadIdx.x - 32; r < len; r += kQrThreads - 32)
             cq_store<N>(v + r * C2, qr_scaled<N>(load_plain<N>(xc + r * C2), e), qr_scaled<N>(load_plain<N>(xc + r * C2 + E), e));
     __syncthreads();
-    Num<N> tre = zero<N>(), tim = zero<N>();
-    if (needs) {
-        const Num<N> sv = s_fast ? load_plain<N>(s_sv) : block_exact_dot<N, false>(v, 1, v, 1, 2 * len, sm, p.error);
-        if (threadIdx.x == 0) {
-            const Num<N> vim = load_plain<N>(v + E);
-            if (!vim.s && !vim.st) tre = divx<N>(qr_pow2<N>(1), sv);
-            else {
-                const Num<N> a = qr_scaled<N>(sv, 1), b = mulx<N>(qr_scaled<N>(beta, e), vim);
-                const Num<N> d = dot2_add<N>(a, a, b, b, zero<N>());
-                tre = divx<N>(a, d); tim = negate<N>(divx<N>(b, d));
-            }
-        }
+    if (needs && !s_fast) {
+        const Num<N> sv = block_exact_dot<N, false>(v, 1, v, 1, 2 * len, sm, p.error);
+        if (threadIdx.x == 0) tau_of(sv);
     }
     if (threadIdx.x == 0) {
         cq_store<N>(xc, beta, zero<N>());

@@ -200,6 +200,11 @@ template <int N> __device__ __forceinline__ Num<N> warp_broadcast(const Num<N>& 
 template <int N> __host__ __device__ constexpr int dot_row_words() { return (2 * N + 10) | 1; }
 template <int N> __host__ __device__ constexpr size_t dot_smem_bytes(int warps) { return (size_t)warps * 32 * dot_row_words<N>() * 4; }
 
+// RN(T * 2^lo) for T = sum_w S_w 2^(32w) mod 2^(32W), lane l holding the column sums S_{l+32r} as v[r] (low word)
+// and hi[r] (high word); every lane of the warp returns the result.  keep (optional): the resolved two's-complement
+// words T_w go to keep[w] before the rounding.
+template <int N, int W> __device__ __forceinline__ Num<N> warp_round_columns(u32 (&v)[(W + 31) / 32], const u32 (&hi)[(W + 31) / 32],
+                                                                            i64 lo, u32* keep);
 // RN(T * 2^lo) for T the sum, mod 2^(32W), of the 32 lanes' two's-complement windows, computed by the whole
 // warp; every lane returns the result.  The windows go to shared memory (srow: 32 rows) and lane l sums
 // column l (+32, +64) over the rows; the column sums' high parts and the carries between columns are
@@ -229,6 +234,13 @@ template <int N, int W> __device__ __forceinline__ Num<N> warp_round_window(cons
         v[r] = (u32)sum; hi[r] = (u32)(sum >> 32);
     }
     __syncwarp();                                            // the rows may be rewritten by the next call
+    return warp_round_columns<N, W>(v, hi, lo, nullptr);
+}
+template <int N, int W> __device__ __forceinline__ Num<N> warp_round_columns(u32 (&v)[(W + 31) / 32], const u32 (&hi)[(W + 31) / 32],
+                                                                            i64 lo, u32* keep) {
+    constexpr int R = (W + 31) / 32;
+    constexpr u32 FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     u32 G[R], P[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {                            // u_w = low(S_w) + high(S_{w-1})
@@ -250,6 +262,10 @@ template <int N, int W> __device__ __forceinline__ Num<N> warp_round_window(cons
         cy = (u32)(sum >> 32);
         if (lane + 32 * r < W) v[r] += (Cm >> lane) & 1u;     // the carry out of the window is dropped (mod 2^(32W))
     }
+    if (keep)
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (lane + 32 * r < W) keep[lane + 32 * r] = v[r];
     constexpr int RT = (W - 1) / 32, LT = (W - 1) % 32;
     const bool neg = __shfl_sync(FULL, v[RT], LT) >> 31;
     if (neg) {                                               // magnitude: ~T + 1

@@ -43,7 +43,13 @@ constexpr int kQrThreads = 256;
 // Window words of the block-wide exact dot: the product width plus headroom for the spread of the products'
 // exponents (about 800 bits up to 512-bit numbers, 320 bits beyond); wider spreads take the cluster method.
 template <int N> __host__ __device__ constexpr int qr_window() { return 2 * N + 10 + (N <= 16 ? 16 : 4); }
-template <int N> __host__ __device__ constexpr int qr_dot_words() { return (kQrThreads / 32) * (qr_window<N>() + 6) + N + 8; }
+// The block-wide sums reduce the threads' windows with two shuffle levels to kQrRows partial windows, which go to
+// shared memory as rows of qr_row_words words (odd: conflict-free rows and columns) and are summed by columns.
+constexpr int kQrRows = kQrThreads / 4;
+template <int N> __host__ __device__ constexpr int qr_row_words() { return qr_window<N>() | 1; }
+template <int N> __host__ __device__ constexpr int qr_dot_words() {
+    return kQrRows * qr_row_words<N>() + 1 + 8 * qr_window<N>() + 6 * (kQrThreads / 32) + N + 8;
+}
 
 template <int N> __device__ __forceinline__ Num<N> qr_pow2(int e) {
     Num<N> x = zero<N>();
@@ -83,9 +89,11 @@ template <int N> __host__ __device__ constexpr int qr_keep_words() { return qr_w
 template <int N, class Src> __device__ __noinline__ Num<N> block_exact_sum(const Src& src, u64 K, u32* sm, u32* error, u32* keep = nullptr) {
     constexpr int W = qr_window<N>();
     constexpr int WARPS = kQrThreads / 32;
+    constexpr int WP = qr_row_words<N>(), P0 = (kQrRows * WP + 1) & ~1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    u32* s_win = sm;                                                 // WARPS windows
-    long long* s_lo = reinterpret_cast<long long*>(sm + WARPS * W + (WARPS * W) % 2);
+    u32* s_rows = sm;                                                // kQrRows partial windows
+    u64* s_part = reinterpret_cast<u64*>(sm + P0);                   // 4 column sums of 16 rows each, per column
+    long long* s_lo = reinterpret_cast<long long*>(s_part + 4 * W);
     long long* s_hi = s_lo + WARPS;
     u32* s_st = reinterpret_cast<u32*>(s_hi + WARPS);
     u32* s_cnt = s_st + WARPS;
@@ -143,39 +151,45 @@ template <int N, class Src> __device__ __noinline__ Num<N> block_exact_sum(const
         accumulate<W>(acc, t, a.s * b.s < 0);
     }
 #pragma unroll 1
-    for (int o = 16; o; o >>= 1) {
+    for (int o = 16; o >= 32 / (kQrThreads / kQrRows); o >>= 1) {
         u32 other[W];
 #pragma unroll
         for (int w = 0; w < W; ++w) other[w] = __shfl_down_sync(0xffffffffu, acc[w], o);
         accumulate<W>(acc, other, false);
     }
-    if (lane == 0)
+    constexpr int PER_WARP = kQrRows / WARPS;
+    if (lane < PER_WARP) {
+        u32* row = s_rows + (warp * PER_WARP + lane) * WP;
 #pragma unroll
-        for (int w = 0; w < W; ++w) s_win[warp * W + w] = acc[w];
+        for (int w = 0; w < W; ++w) row[w] = acc[w];
+    }
     __syncthreads();
-    if (tid == 0) {
-#pragma unroll 1
-        for (int v = 1; v < WARPS; ++v) {
-            u32 other[W];
+    for (int job = tid; job < 4 * W; job += kQrThreads) {            // job q * W + col: rows [16q, 16q + 16) of col
+        const int q = job / W, col = job - q * W;
+        const u32* at = s_rows + q * (kQrRows / 4) * WP + col;
+        u64 s0 = 0, s1 = 0;
 #pragma unroll
-            for (int w = 0; w < W; ++w) other[w] = s_win[v * W + w];
-            accumulate<W>(acc, other, false);
+        for (int l = 0; l < kQrRows / 4; l += 2) { s0 += at[l * WP]; s1 += at[(l + 1) * WP]; }
+        s_part[job] = s0 + s1;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        constexpr int R = (W + 31) / 32;
+        u32 v[R], h[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            const int w = lane + 32 * q;
+            const u64 sum = w < W ? s_part[w] + s_part[W + w] + s_part[2 * W + w] + s_part[3 * W + w] : 0;
+            v[q] = (u32)sum; h[q] = (u32)(sum >> 32);
         }
-        if (keep) {
+        if (keep && lane == 0) {
             keep[0] = 1;
             keep[1] = (u32)(u64)lo; keep[2] = (u32)((u64)lo >> 32);
             keep[3] = (u32)(u64)hi; keep[4] = (u32)((u64)hi >> 32);
             keep[5] = (u32)logc;
-#pragma unroll 1
-            for (int w = 0; w < W; ++w) keep[6 + w] = acc[w];
         }
-        int sign = 1;
-        if (acc[W - 1] >> 31) {
-            sign = -1; u64 cy = 1;
-#pragma unroll
-            for (int w = 0; w < W; ++w) { const u64 v = (u64)(u32)~acc[w] + cy; acc[w] = (u32)v; cy = v >> 32; }
-        }
-        store<N>(s_res, round_general<N, W>(acc, lo, sign, 0));
+        const Num<N> res = warp_round_columns<N, W>(v, h, lo, keep ? keep + 6 : nullptr);
+        if (lane == 0) store<N>(s_res, res);
     }
     __syncthreads();
     r = load_plain<N>(s_res);
@@ -264,7 +278,6 @@ template <int N> __global__ void __launch_bounds__(256) qr_update_kernel(QrPanel
 template <int N> __global__ void __launch_bounds__(kQrThreads) qr_reflect_kernel(QrPanel p, u64 c) {
     __shared__ __align__(16) u32 sm[qr_dot_words<N>()];
     __shared__ u32 s_keep[qr_keep_words<N>()];
-    __shared__ u32 s_pv[N + 3];
     __shared__ long long s_e;
     __shared__ int s_go, s_fast;
     constexpr u64 E = N + 3;
@@ -277,9 +290,9 @@ template <int N> __global__ void __launch_bounds__(kQrThreads) qr_reflect_kernel
     int below = 0;
     for (u64 r = 1 + threadIdx.x; r < len; r += kQrThreads) below |= ldw<true>(xc + r * E + N + 1) != 0;
     below = __syncthreads_or(below);
-    Num<N> beta = zero<N>(), v0 = qr_pow2<N>(0);
+    Num<N> beta = zero<N>(), v0 = qr_pow2<N>(0), x0 = zero<N>();
     if (threadIdx.x == 0) {
-        const Num<N> x0 = load_plain<N>(xc);
+        x0 = load_plain<N>(xc);
         int reason = s.st ? 3 : (!x0.s && !below) ? 1 : 0;
         beta = x0;
         if (!reason && below) {
@@ -289,23 +302,25 @@ template <int N> __global__ void __launch_bounds__(kQrThreads) qr_reflect_kernel
         }
         if (!reason && p.rank_bits > 0 && st->have_top && (long long)beta.e + p.rank_bits < st->top) reason = 2;
         if (reason) { st->rank = (long long)j; st->reason = reason; st->status = s.st; s_go = 0; }
-        else {
-            s_go = 1; s_e = below ? (long long)v0.e : 0;
-            Num<N> pv;
-            s_fast = below && qr_resum<N>(s_keep, x0, v0, (long long)v0.e, pv);
-            if (s_fast) store<N>(s_pv, pv);
-        }
+        else { s_go = 1; s_e = below ? (long long)v0.e : 0; }
     }
     __syncthreads();
     if (!s_go) return;
     const long long e = s_e;
-    if (below)
-        for (u64 r = 1 + threadIdx.x; r < len; r += kQrThreads) store<N>(v + r * E, qr_scaled<N>(load_plain<N>(xc + r * E), e));
-    if (threadIdx.x == 0) store<N>(v, below ? qr_scaled<N>(v0, e) : qr_pow2<N>(0));
-    __syncthreads();
+    // Thread 0 forms P(v, v) from the kept window and tau while warps 1.. scale the rest of the reflector.
     Num<N> tj = zero<N>();
-    if (below) {
-        const Num<N> pv = s_fast ? load_plain<N>(s_pv) : block_exact_dot<N, false>(v, 1, v, 1, len, sm, p.error);
+    if (threadIdx.x == 0) {
+        store<N>(v, below ? qr_scaled<N>(v0, e) : qr_pow2<N>(0));
+        Num<N> pv;
+        const int fast = below && qr_resum<N>(s_keep, x0, v0, e, pv);
+        if (fast) tj = divx<N>(qr_pow2<N>(1), pv);
+        s_fast = fast;
+    }
+    if (below && threadIdx.x >= 32)
+        for (u64 r = 1 + threadIdx.x - 32; r < len; r += kQrThreads - 32) store<N>(v + r * E, qr_scaled<N>(load_plain<N>(xc + r * E), e));
+    __syncthreads();
+    if (below && !s_fast) {
+        const Num<N> pv = block_exact_dot<N, false>(v, 1, v, 1, len, sm, p.error);
         if (threadIdx.x == 0) tj = divx<N>(qr_pow2<N>(1), pv);
     }
     if (threadIdx.x == 0) {
